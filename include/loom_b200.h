@@ -1,0 +1,170 @@
+/* loom_b200.h — C ABI of the B200 execution backend for Loom kernels.
+ *
+ * Loom selects a backend by C++ template alias and has no FFI of its own:
+ *   vm::bse::function<K>          Loom src/vm/bse.hpp:648-649
+ *   vm::cuda::function<K>(n)      Loom src/vm/cuda.hpp:1581-1582
+ *   vm::cuda::stream<K>(n)        Loom src/vm/cuda.hpp:1584-1586
+ *   vm::simd::hybrid_function<K>  Loom src/vm/simd.hpp:4311-4318
+ * The functions below are the boundary those aliases bind to on B200: the
+ * C++ front end (loom_b200.hpp) and the Python binding (loom_b200.api) call
+ * only these entry points.  Plain pointers and sizes; no exceptions cross the
+ * ABI; every call returns LOOM_B200_OK (0) or a negative error code.
+ * A handle is not thread-safe: one host thread drives it at a time
+ * (Loom's facades have the same rule, src/vm/mp.hpp:67-132).
+ */
+#ifndef LOOM_B200_H
+#define LOOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LOOM_B200_ABI_VERSION 1
+
+/* ------------------------------------------------------------ error codes */
+#define LOOM_B200_OK 0
+#define LOOM_B200_ERR_INVALID (-1)   /* bad argument */
+#define LOOM_B200_ERR_NOT_FOUND (-2) /* kernel name not compiled in */
+#define LOOM_B200_ERR_CUDA (-3)      /* CUDA runtime error */
+#define LOOM_B200_ERR_OOM (-4)       /* device allocation failed */
+#define LOOM_B200_ERR_DEVICE (-5)    /* device status word non-zero */
+#define LOOM_B200_ERR_BUDGET (-6)    /* request exceeds the memory budget */
+#define LOOM_B200_ERR_NO_DEVICE (-7) /* no CUDA device visible */
+#define LOOM_B200_ERR_CANCELLED (-8) /* request cancelled */
+#define LOOM_B200_ERR_TIMEOUT (-9)   /* host-side watchdog expired */
+
+/* Device status bits (loom_b200_stats.status).  Device code never traps:
+ * it records one of these and finishes the launch. */
+#define LOOM_B200_STATUS_STEP_LIMIT 1u      /* a thread exceeded max_steps */
+#define LOOM_B200_STATUS_ASSERT_FP 2u       /* ops::assert_fp saw NaN/inf */
+#define LOOM_B200_STATUS_QUEUE_OVERRUN 4u   /* a work-queue index was out of range */
+#define LOOM_B200_STATUS_BARRIER_TIMEOUT 8u /* a bounded grid-barrier wait ran out */
+
+/* ------------------------------------------------------------ scalar types */
+enum loom_b200_type
+{
+    LOOM_B200_B8  = 0,
+    LOOM_B200_I8  = 1,
+    LOOM_B200_U8  = 2,
+    LOOM_B200_I16 = 3,
+    LOOM_B200_U16 = 4,
+    LOOM_B200_I32 = 5,
+    LOOM_B200_U32 = 6,
+    LOOM_B200_I64 = 7,
+    LOOM_B200_U64 = 8,
+    LOOM_B200_F32 = 9,
+    LOOM_B200_F64 = 10
+};
+
+/* Static description of a compiled kernel.  Mirrors the compile-time facts
+ * of loom::vm::kernel_blank (Loom src/vm/core.hpp:939-1031): inputs/outputs
+ * (input_vars/output_vars), num_blocks, state_size. */
+typedef struct loom_b200_kernel_info
+{
+    const char*        name;          /* registry name, e.g. "fib_u64" */
+    const char*        ir_digest;     /* sha256 prefix of the kernel's text IR */
+    uint32_t           num_inputs;
+    uint32_t           num_outputs;
+    const int*         input_types;   /* enum loom_b200_type */
+    const int*         output_types;
+    const char* const* input_names;
+    const char* const* output_names;
+    uint32_t           num_blocks;
+    uint32_t           num_regs;      /* Loom registers incl. PC (reg_names) */
+    uint32_t           state_size;    /* K::state_size in bytes */
+    uint32_t           state_cols;    /* registers live at some block entry */
+    const uint32_t*    block_instrs;  /* static instruction count per block */
+    const uint32_t*    block_live_bytes; /* live-in bytes per block */
+} loom_b200_kernel_info;
+
+/* Execution form. */
+#define LOOM_B200_PLAIN 0u   /* one CUDA thread per Loom thread, hardware reconvergence */
+#define LOOM_B200_REGROUP 1u /* persistent megakernel, threads regrouped by PC */
+
+/* Launch options; zero-initialise and set what you need (0 = default). */
+typedef struct loom_b200_opts
+{
+    uint32_t mode;        /* LOOM_B200_PLAIN or LOOM_B200_REGROUP */
+    uint32_t block_size;  /* CUDA threads per CTA (multiple of 32) */
+    uint32_t utr_lanes;   /* regroup: keep running in registers while the
+                             largest same-PC group has >= utr_lanes lanes
+                             (the GPU form of Loom's UTR, simd.hpp:3273-3292) */
+    uint32_t period;      /* regroup: max block steps per tile per round */
+    uint64_t population;  /* regroup: resident thread slots; 0 = all inputs */
+    uint64_t max_steps;   /* per-thread block-step guard; 0 = 2^40 */
+    uint32_t profile;     /* plain: collect lane-efficiency counters */
+    uint32_t no_refill;   /* regroup: do not refill halted lanes in registers */
+    uint32_t ctas_per_sm; /* regroup: resident CTAs per SM; 0 = occupancy max */
+    uint32_t fault_phantom_ctas; /* fault injection for tests: the grid barrier
+                                    also waits for this many CTAs that do not
+                                    exist, so its bounded wait must run out */
+    uint64_t barrier_spins; /* regroup: polls before a barrier wait gives up
+                               (0 = default, about 7 s) */
+} loom_b200_opts;
+
+/* Counters of the launches since the last reset. */
+typedef struct loom_b200_stats
+{
+    uint64_t launches;
+    uint64_t threads;      /* Loom threads completed */
+    uint64_t thread_instr; /* VM instructions executed, summed over threads */
+    uint64_t warp_instr;   /* VM instructions issued, summed over warp steps;
+                              lane efficiency = thread_instr / (32 * warp_instr) */
+    uint64_t rounds;       /* regroup rounds (grid barriers) */
+    uint64_t parks;        /* threads written to the state file */
+    uint64_t state_bytes;  /* algorithmic state bytes moved (saves + restores) */
+    uint32_t status;       /* OR of LOOM_B200_STATUS_* */
+    uint32_t grid;         /* CTAs of the last launch */
+    double   ms;           /* device time of the last launch (CUDA events) */
+} loom_b200_stats;
+
+typedef struct loom_b200_handle loom_b200_handle;
+
+/* ------------------------------------------------------------ registry */
+int         loom_b200_version(void);
+const char* loom_b200_error_string(int code);
+int         loom_b200_kernel_count(void);
+int         loom_b200_kernel_get(int index, const loom_b200_kernel_info** info);
+int         loom_b200_kernel_find(const char* name, const loom_b200_kernel_info** info);
+
+/* ------------------------------------------------------------ function
+ * Replaces vm::cuda::function<K>(n)(inputs...) (Loom src/vm/cuda.hpp:
+ * 1406-1462, MemoryFacade::set_inputs/get_outputs 1060-1148): one handle per
+ * kernel and capacity; inputs are column arrays (one pointer per
+ * K::input_vars entry), outputs likewise; outputs keep input order. */
+int loom_b200_create(const char*             kernel,
+                     uint64_t                capacity,
+                     const loom_b200_opts*   opts,
+                     loom_b200_handle**      out);
+int loom_b200_destroy(loom_b200_handle* h);
+int loom_b200_set_opts(loom_b200_handle* h, const loom_b200_opts* opts);
+int loom_b200_get_opts(const loom_b200_handle* h, loom_b200_opts* opts);
+
+/* Host columns in, host columns out; copies and launch are inside the call,
+ * which returns after the outputs are on the host.  A NULL input column
+ * means "iota": input value = thread index. */
+int loom_b200_run_host(loom_b200_handle*  h,
+                       const void* const* inputs,
+                       void* const*       outputs,
+                       uint64_t           n);
+
+/* Device columns in and out, enqueued on `stream` (a cudaStream_t, NULL =
+ * the handle's own stream); returns without synchronising. */
+int loom_b200_run_device(loom_b200_handle*  h,
+                         const void* const* inputs,
+                         void* const*       outputs,
+                         uint64_t           n,
+                         void*              stream);
+
+int loom_b200_sync(loom_b200_handle* h);
+int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);
+int loom_b200_reset_stats(loom_b200_handle* h);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* LOOM_B200_H */

@@ -1,0 +1,343 @@
+"""Python binding of libloom_b200 (the C ABI in include/loom_b200.h).
+
+Mirrors the call shapes of Loom's backends:
+
+* ``Function(kernel, n)(*inputs)`` is ``vm::cuda::function<K>(n)(inputs...)``
+  (Loom src/vm/cuda.hpp:1406-1462): input columns in, output columns out, in
+  input order;
+* ``Function.run_device`` launches on device columns (torch tensors or raw
+  pointers) without synchronising, for callers that keep data resident.
+
+There is no CPU fallback: if the CUDA library is missing or no device is
+visible, construction raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import pathlib
+from typing import Dict, List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "libloom_b200.so"
+
+PLAIN = 0
+REGROUP = 1
+
+OK = 0
+ERR_INVALID = -1
+ERR_NOT_FOUND = -2
+ERR_CUDA = -3
+ERR_OOM = -4
+ERR_DEVICE = -5
+ERR_BUDGET = -6
+ERR_NO_DEVICE = -7
+ERR_CANCELLED = -8
+ERR_TIMEOUT = -9
+
+STATUS_STEP_LIMIT = 1
+STATUS_ASSERT_FP = 2
+STATUS_QUEUE_OVERRUN = 4
+STATUS_BARRIER_TIMEOUT = 8
+
+TYPE_NAMES = ["b8", "i8", "u8", "i16", "u16", "i32", "u32", "i64", "u64", "f32", "f64"]
+NP_TYPE = {
+    "b8": np.uint8,
+    "i8": np.int8,
+    "u8": np.uint8,
+    "i16": np.int16,
+    "u16": np.uint16,
+    "i32": np.int32,
+    "u32": np.uint32,
+    "i64": np.int64,
+    "u64": np.uint64,
+    "f32": np.float32,
+    "f64": np.float64,
+}
+
+
+class LoomError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"libloom_b200 error {code}: {msg}")
+        self.code = code
+
+
+class KernelInfoC(ctypes.Structure):
+    _fields_ = [
+        ("name", ctypes.c_char_p),
+        ("ir_digest", ctypes.c_char_p),
+        ("num_inputs", ctypes.c_uint32),
+        ("num_outputs", ctypes.c_uint32),
+        ("input_types", ctypes.POINTER(ctypes.c_int)),
+        ("output_types", ctypes.POINTER(ctypes.c_int)),
+        ("input_names", ctypes.POINTER(ctypes.c_char_p)),
+        ("output_names", ctypes.POINTER(ctypes.c_char_p)),
+        ("num_blocks", ctypes.c_uint32),
+        ("num_regs", ctypes.c_uint32),
+        ("state_size", ctypes.c_uint32),
+        ("state_cols", ctypes.c_uint32),
+        ("block_instrs", ctypes.POINTER(ctypes.c_uint32)),
+        ("block_live_bytes", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_uint32),
+        ("block_size", ctypes.c_uint32),
+        ("utr_lanes", ctypes.c_uint32),
+        ("period", ctypes.c_uint32),
+        ("population", ctypes.c_uint64),
+        ("max_steps", ctypes.c_uint64),
+        ("profile", ctypes.c_uint32),
+        ("no_refill", ctypes.c_uint32),
+        ("ctas_per_sm", ctypes.c_uint32),
+        ("fault_phantom_ctas", ctypes.c_uint32),
+        ("barrier_spins", ctypes.c_uint64),
+    ]
+
+
+class StatsC(ctypes.Structure):
+    _fields_ = [
+        ("launches", ctypes.c_uint64),
+        ("threads", ctypes.c_uint64),
+        ("thread_instr", ctypes.c_uint64),
+        ("warp_instr", ctypes.c_uint64),
+        ("rounds", ctypes.c_uint64),
+        ("parks", ctypes.c_uint64),
+        ("state_bytes", ctypes.c_uint64),
+        ("status", ctypes.c_uint32),
+        ("grid", ctypes.c_uint32),
+        ("ms", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+# every symbol include/loom_b200.h declares
+EXPORTS = [
+    "loom_b200_version",
+    "loom_b200_error_string",
+    "loom_b200_kernel_count",
+    "loom_b200_kernel_get",
+    "loom_b200_kernel_find",
+    "loom_b200_create",
+    "loom_b200_destroy",
+    "loom_b200_set_opts",
+    "loom_b200_get_opts",
+    "loom_b200_run_host",
+    "loom_b200_run_device",
+    "loom_b200_sync",
+    "loom_b200_get_stats",
+    "loom_b200_reset_stats",
+]
+
+
+def lib() -> ctypes.CDLL:
+    """Load libloom_b200.so (fails loudly when it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m loom_b200.build` "
+            "(there is no CPU fallback)"
+        )
+    L = ctypes.CDLL(str(LIB_PATH))
+    vp = ctypes.c_void_p
+    L.loom_b200_version.restype = ctypes.c_int
+    L.loom_b200_error_string.restype = ctypes.c_char_p
+    L.loom_b200_error_string.argtypes = [ctypes.c_int]
+    L.loom_b200_kernel_count.restype = ctypes.c_int
+    L.loom_b200_kernel_get.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
+    L.loom_b200_kernel_find.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
+    L.loom_b200_create.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(Opts), ctypes.POINTER(vp)]
+    L.loom_b200_destroy.argtypes = [vp]
+    L.loom_b200_set_opts.argtypes = [vp, ctypes.POINTER(Opts)]
+    L.loom_b200_get_opts.argtypes = [vp, ctypes.POINTER(Opts)]
+    L.loom_b200_run_host.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint64]
+    L.loom_b200_run_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint64, vp]
+    L.loom_b200_sync.argtypes = [vp]
+    L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
+    L.loom_b200_reset_stats.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def check(code: int) -> int:
+    if code != OK:
+        msg = lib().loom_b200_error_string(code)
+        raise LoomError(code, msg.decode() if msg else "?")
+    return code
+
+
+class KernelInfo:
+    def __init__(self, c: KernelInfoC):
+        self.name = c.name.decode()
+        self.ir_digest = c.ir_digest.decode()
+        self.inputs = [
+            (c.input_names[i].decode(), TYPE_NAMES[c.input_types[i]]) for i in range(c.num_inputs)
+        ]
+        self.outputs = [
+            (c.output_names[i].decode(), TYPE_NAMES[c.output_types[i]])
+            for i in range(c.num_outputs)
+        ]
+        self.num_blocks = c.num_blocks
+        self.num_regs = c.num_regs
+        self.state_size = c.state_size
+        self.state_cols = c.state_cols
+        self.block_instrs = [c.block_instrs[i] for i in range(c.num_blocks)]
+        self.block_live_bytes = [c.block_live_bytes[i] for i in range(c.num_blocks)]
+
+    def __repr__(self):
+        return f"KernelInfo({self.name}, in={self.inputs}, out={self.outputs}, blocks={self.num_blocks})"
+
+
+def kernels() -> List[str]:
+    L = lib()
+    out = []
+    for i in range(L.loom_b200_kernel_count()):
+        p = ctypes.POINTER(KernelInfoC)()
+        check(L.loom_b200_kernel_get(i, ctypes.byref(p)))
+        out.append(p.contents.name.decode())
+    return out
+
+
+def info(kernel: str) -> KernelInfo:
+    p = ctypes.POINTER(KernelInfoC)()
+    check(lib().loom_b200_kernel_find(kernel.encode(), ctypes.byref(p)))
+    return KernelInfo(p.contents)
+
+
+def make_opts(
+    mode: Union[int, str] = PLAIN,
+    block_size: int = 0,
+    utr_lanes: int = 0,
+    period: int = 0,
+    population: int = 0,
+    max_steps: int = 0,
+    profile: bool = False,
+    refill: bool = True,
+    ctas_per_sm: int = 0,
+    fault_phantom_ctas: int = 0,
+    barrier_spins: int = 0,
+) -> Opts:
+    if isinstance(mode, str):
+        mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
+    return Opts(
+        mode=mode,
+        block_size=block_size,
+        utr_lanes=utr_lanes,
+        period=period,
+        population=population,
+        max_steps=max_steps,
+        profile=1 if profile else 0,
+        no_refill=0 if refill else 1,
+        ctas_per_sm=ctas_per_sm,
+        fault_phantom_ctas=fault_phantom_ctas,
+        barrier_spins=barrier_spins,
+    )
+
+
+def _ptr(x) -> Optional[int]:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError(f"cannot take a pointer of {type(x)}")
+
+
+class Function:
+    """A kernel bound to a device, a capacity and launch options."""
+
+    def __init__(self, kernel: str, capacity: int, mode: Union[int, str] = PLAIN, **opts):
+        self.kernel = kernel
+        self.info = info(kernel)
+        self.capacity = int(capacity)
+        o = make_opts(mode, **opts)
+        h = ctypes.c_void_p()
+        check(lib().loom_b200_create(kernel.encode(), self.capacity, ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+
+    # -------------------------------------------------------------- options
+    def set_opts(self, mode: Union[int, str] = PLAIN, **opts) -> None:
+        o = make_opts(mode, **opts)
+        check(lib().loom_b200_set_opts(self._h, ctypes.byref(o)))
+
+    def get_opts(self) -> Dict[str, int]:
+        o = Opts()
+        check(lib().loom_b200_get_opts(self._h, ctypes.byref(o)))
+        return {f: getattr(o, f) for f, _ in Opts._fields_}
+
+    # -------------------------------------------------------------- runs
+    def __call__(self, *inputs: Optional[np.ndarray], n: Optional[int] = None):
+        """Host arrays in, host arrays out (blocking).  ``None`` = iota."""
+        ins = []
+        for a, (_, t) in zip(inputs, self.info.inputs):
+            ins.append(None if a is None else np.ascontiguousarray(a, dtype=NP_TYPE[t]))
+        if len(ins) != len(self.info.inputs):
+            raise ValueError(f"{self.kernel} takes {len(self.info.inputs)} input columns")
+        if n is None:
+            sized = [a for a in ins if a is not None]
+            if not sized:
+                raise ValueError("n is required when every input is iota")
+            n = len(sized[0])
+        outs = [np.empty(n, dtype=NP_TYPE[t]) for _, t in self.info.outputs]
+        pin = (ctypes.c_void_p * max(1, len(ins)))(*[_ptr(a) for a in ins])
+        pout = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        check(lib().loom_b200_run_host(self._h, pin, pout, n))
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def run_host_ptrs(self, inputs: Sequence, outputs: Sequence, n: int) -> None:
+        """Host pointers (e.g. pinned torch tensors) in and out, blocking."""
+        pin = (ctypes.c_void_p * max(1, len(inputs)))(*[_ptr(a) for a in inputs])
+        pout = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
+        check(lib().loom_b200_run_host(self._h, pin, pout, n))
+
+    def run_device(self, inputs: Sequence, outputs: Sequence, n: int, stream=None) -> None:
+        """Device columns in and out; asynchronous on `stream` (cudaStream_t
+        handle or torch.cuda.Stream; None = the handle's own stream)."""
+        pin = (ctypes.c_void_p * max(1, len(inputs)))(*[_ptr(a) for a in inputs])
+        pout = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
+        s = getattr(stream, "cuda_stream", stream)
+        check(lib().loom_b200_run_device(self._h, pin, pout, n, s))
+
+    def sync(self) -> None:
+        check(lib().loom_b200_sync(self._h))
+
+    def stats(self, raise_on_device_error: bool = False) -> Dict[str, float]:
+        s = StatsC()
+        check(lib().loom_b200_get_stats(self._h, ctypes.byref(s)))
+        d = {f: getattr(s, f) for f, _ in StatsC._fields_}
+        d["lane_efficiency"] = (
+            s.thread_instr / (32.0 * s.warp_instr) if s.warp_instr else float("nan")
+        )
+        if raise_on_device_error and s.status:
+            raise LoomError(ERR_DEVICE, f"device status {s.status:#x}")
+        return d
+
+    def reset_stats(self) -> None:
+        check(lib().loom_b200_reset_stats(self._h))
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().loom_b200_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,445 @@
+"""Lower a Loom kernel (text IR) to CUDA C++ for the B200 engines.
+
+For every kernel the generator writes one translation unit that defines a
+struct ``K`` with
+
+* ``Regs``            the Loom register file as scalars (kept in CUDA
+                      registers); Union registers (Loom src/common/union.hpp)
+                      are stored as unsigned integers and bit-cast per view;
+* ``run<kProf>``      the whole program as a goto CFG (plain engine);
+* ``exec(b)``         one basic block, returning the next block (regrouping
+                      engine);
+* ``save/restore(b)`` the live-in registers of block b to/from the SoA state
+                      file;
+* ``load_inputs`` / ``store_outputs`` the input/output columns;
+
+plus the host-side descriptor and launchers.  Op semantics follow Loom
+src/vm/operators.hpp and the std:: functors exactly as standard_eval applies
+them (core.hpp:740-750): arguments are converted to the functor's operand
+type, the functor's result type is kept (T for arithmetic, bool for
+comparisons and logic), and the result is converted to the destination
+variable's type.  The TU is compiled with -fmad=false and IEEE division and
+square root so that float arithmetic rounds like the scalar backend.
+"""
+
+from __future__ import annotations
+
+import math
+import struct
+from typing import Dict, List
+
+from .ir import (
+    FLOAT_TYPES,
+    HALT,
+    INT_TYPES,
+    TYPE_BYTES,
+    Compute,
+    Jump,
+    Kernel,
+    Operand,
+    ParmJump,
+)
+
+CTYPE = {
+    "b8": "bool",
+    "i8": "signed char",
+    "u8": "unsigned char",
+    "i16": "short",
+    "u16": "unsigned short",
+    "i32": "int",
+    "u32": "unsigned int",
+    "i64": "long long",
+    "u64": "unsigned long long",
+    "f32": "float",
+    "f64": "double",
+}
+
+ABI_TYPE = {
+    "b8": "LOOM_B200_B8",
+    "i8": "LOOM_B200_I8",
+    "u8": "LOOM_B200_U8",
+    "i16": "LOOM_B200_I16",
+    "u16": "LOOM_B200_U16",
+    "i32": "LOOM_B200_I32",
+    "u32": "LOOM_B200_U32",
+    "i64": "LOOM_B200_I64",
+    "u64": "LOOM_B200_U64",
+    "f32": "LOOM_B200_F32",
+    "f64": "LOOM_B200_F64",
+}
+
+CMP = {"eq": "==", "ne": "!=", "gt": ">", "lt": "<", "ge": ">=", "le": "<="}
+ARITH = {"add": "+", "sub": "-", "mul": "*", "div": "/", "mod": "%"}
+BITS = {"band": "&", "bor": "|", "bxor": "^", "shl": "<<", "shr": ">>"}
+LOGIC = {"land": "&&", "lor": "||"}
+UNARY_FN = {
+    "round": "op_round",
+    "ceil": "op_ceil",
+    "floor": "op_floor",
+    "trunc": "op_trunc",
+    "sqrt": "op_sqrt",
+    "sin": "op_sin",
+    "cos": "op_cos",
+    "rsqrt": "op_rsqrt",
+}
+
+
+def literal(op: Operand) -> str:
+    """Exact C++ spelling of a literal's bit pattern."""
+    t = op.type
+    ct = CTYPE[t]
+    if t == "f32":
+        v = struct.unpack("<f", struct.pack("<I", op.bits & 0xFFFFFFFF))[0]
+        if math.isfinite(v):
+            return f"({v.hex()}f)"
+        return f"__uint_as_float({op.bits & 0xFFFFFFFF:#x}u)"
+    if t == "f64":
+        v = struct.unpack("<d", struct.pack("<Q", op.bits))[0]
+        if math.isfinite(v):
+            return f"({v.hex()})"
+        return f"__longlong_as_double({op.bits:#x}ll)"
+    if t == "b8":
+        return "true" if op.bits & 1 else "false"
+    nbits = TYPE_BYTES[t] * 8
+    bits = op.bits & ((1 << nbits) - 1)
+    return f"(({ct}){bits:#x}ull)"
+
+
+class Lowering:
+    def __init__(self, k: Kernel):
+        self.k = k
+        self.pc = k.pc_reg()
+        self.regs = {r.idx: r for r in k.regs}
+
+    # ------------------------------------------------------------ views
+    def rname(self, idx: int) -> str:
+        return f"R.r{idx}"
+
+    def read(self, op: Operand) -> str:
+        if op.is_literal:
+            return literal(op)
+        reg = self.regs[op.reg]
+        if reg.storage == op.type:
+            return self.rname(op.reg)
+        return f"bitcast<{CTYPE[op.type]}>({self.rname(op.reg)})"
+
+    def write(self, dst: Operand, expr: str) -> str:
+        reg = self.regs[dst.reg]
+        val = f"static_cast<{CTYPE[dst.type]}>({expr})"
+        if reg.storage == dst.type:
+            return f"{self.rname(dst.reg)} = {val};"
+        return f"{self.rname(dst.reg)} = bitcast<{CTYPE[reg.storage]}>({val});"
+
+    # ------------------------------------------------------------ ops
+    def expr(self, ins: Compute) -> str:
+        op = ins.op
+        a = [self.read(x) for x in ins.args]
+        ot = ins.optype
+
+        def cv(i: int, t: str) -> str:
+            return f"static_cast<{CTYPE[t]}>({a[i]})"
+
+        if op == "mov":
+            return a[0]
+        if op == "cmov":
+            return f"(({a[0]}) ? ({a[1]}) : ({a[2]}))"
+        if op in ("fma", "fms"):
+            t = ins.args[0].type
+            z = a[2] if op == "fma" else f"(-({a[2]}))"
+            return f"op_fma({a[0]}, {a[1]}, {z})"
+        if op == "assert_fp":
+            return f"op_assert_fp({a[0]}, ctx)"
+        if op == "sct":
+            t, _ = ot
+            consts = [literal(c) for c in ins.consts]
+            idx = a[0]
+            e = consts[-1]
+            for i in reversed(range(len(consts) - 1)):
+                e = f"(({idx}) == {i} ? {consts[i]} : {e})"
+            return f"static_cast<{CTYPE[t]}>({e})"
+        if op == "slt":
+            t, _ = ot
+            idx = a[0]
+            vals = a[1:]
+            e = f"static_cast<{CTYPE[t]}>({vals[-1]})"
+            for i in reversed(range(len(vals) - 1)):
+                e = f"(({idx}) == {i} ? static_cast<{CTYPE[t]}>({vals[i]}) : {e})"
+            return e
+        if op == "pacc":
+            t, it, acc, cmp = ot
+            c = f"static_cast<{CTYPE[it]}>({cv(1, t)} {CMP[cmp]} {cv(2, t)})"
+            return f"static_cast<{CTYPE[it]}>({cv(0, it)} {LOGIC[acc]} {c})"
+        (t,) = ot
+        ct = CTYPE[t]
+        if op in ARITH:
+            return f"static_cast<{ct}>({cv(0, t)} {ARITH[op]} {cv(1, t)})"
+        if op in BITS:
+            return f"static_cast<{ct}>({cv(0, t)} {BITS[op]} {cv(1, t)})"
+        if op in CMP:
+            return f"static_cast<bool>({cv(0, t)} {CMP[op]} {cv(1, t)})"
+        if op in LOGIC:
+            return f"static_cast<bool>({cv(0, t)} {LOGIC[op]} {cv(1, t)})"
+        if op == "lnot":
+            return f"static_cast<bool>(!{cv(0, t)})"
+        if op == "neg":
+            return f"static_cast<{ct}>(-{cv(0, t)})"
+        if op == "bnot":
+            return f"static_cast<{ct}>(~{cv(0, t)})"
+        if op == "abs":
+            if t in FLOAT_TYPES:
+                return f"op_abs({cv(0, t)})"
+            if t.startswith("u"):
+                return cv(0, t)
+            wide = "long long" if t == "i64" else "int"
+            return f"static_cast<{ct}>(op_abs(static_cast<{wide}>({cv(0, t)})))"
+        if op == "max":
+            return f"op_max<{ct}>({cv(0, t)}, {cv(1, t)})"
+        if op == "min":
+            return f"op_min<{ct}>({cv(0, t)}, {cv(1, t)})"
+        if op == "copysign":
+            return f"op_copysign({cv(0, t)}, {cv(1, t)})"
+        if op in UNARY_FN:
+            return f"{UNARY_FN[op]}({cv(0, t)})"
+        raise NotImplementedError(f"{self.k.name}: op {op}")
+
+    def body(self, instrs, indent: str) -> List[str]:
+        out = []
+        for ins in instrs:
+            if isinstance(ins, Compute):
+                out.append(indent + self.write(ins.dst, self.expr(ins)))
+        return out
+
+    # ------------------------------------------------------------ transfers
+    def next_expr(self, blk) -> str:
+        """C++ expression of the next block index (kHalt for HALT)."""
+        t = blk.terminator
+        if t is None:
+            return "kHalt"
+        if isinstance(t, Jump):
+            return self.target(t.target)
+        v = self.read(t.var)
+        tg = [self.target(x) for x in t.targets]
+        if len(tg) == 2:
+            # Loom's scalar dispatch: any non-zero selects the second label
+            # (bse.hpp:180-185).
+            return f"(({v}) ? {tg[1]} : {tg[0]})"
+        e = "kHalt"  # out-of-table values leave the thread where it is
+        for i in reversed(range(len(tg))):
+            e = f"(({v}) == {i} ? {tg[i]} : {e})"
+        return e
+
+    @staticmethod
+    def target(t: int) -> str:
+        return "kHalt" if t == HALT else str(t)
+
+    def goto_transfer(self, blk, indent: str) -> List[str]:
+        t = blk.terminator
+        if t is None:
+            return [indent + "goto L_HALT;"]
+        if isinstance(t, Jump):
+            return [indent + f"goto {self.label(t.target)};"]
+        v = self.read(t.var)
+        if len(t.targets) == 2:
+            return [
+                indent
+                + f"if({v}) goto {self.label(t.targets[1])}; else goto {self.label(t.targets[0])};"
+            ]
+        lines = [indent + f"switch({v}) {{"]
+        for i, tg in enumerate(t.targets):
+            lines.append(indent + f"case {i}: goto {self.label(tg)};")
+        lines.append(indent + "default: goto L_HALT;")
+        lines.append(indent + "}")
+        return lines
+
+    @staticmethod
+    def label(t: int) -> str:
+        return "L_HALT" if t == HALT else f"L_B{t}"
+
+
+def generate(k: Kernel) -> str:
+    L = Lowering(k)
+    name = k.name
+    nb = k.num_blocks
+    nin = len(k.inputs)
+    nout = len(k.outputs)
+    live_in, _ = k.liveness()
+    state = k.state_regs()
+    scol = {r: nin + nout + j for j, r in enumerate(state)}
+    counts = k.instr_counts()
+    live_bytes = [sum(L.regs[r].nbytes for r in li) for li in live_in]
+    regs = [r for r in k.regs if r.idx != L.pc]
+    if nin + nout + len(state) > 96:
+        raise ValueError(f"{name}: too many columns")
+
+    o: List[str] = []
+    w = o.append
+    w(f"// Generated by loom_b200.codegen from loom_b200/ir/{name}.lir.")
+    w(f"// Kernel IR digest {k.digest()}; regenerate instead of editing.")
+    w('#include "../engine/plain.cuh"')
+    w('#include "../engine/regroup.cuh"')
+    w('#include "../runtime_iface.h"')
+    w("")
+    w(f"namespace loom_b200 {{ namespace k_{name} {{")
+    w("")
+    w(f"__constant__ unsigned kInstrTab[{nb}] = {{{', '.join(map(str, counts))}}};")
+    w(f"__constant__ unsigned kLiveTab[{nb}] = {{{', '.join(map(str, live_bytes))}}};")
+    w("")
+    w("struct K")
+    w("{")
+    w(f"    static constexpr int kNumBlocks = {nb};")
+    w("    struct Regs")
+    w("    {")
+    for r in regs:
+        w(f"        {CTYPE[r.storage]} r{r.idx}; // {r.name}: {','.join(r.types)}")
+    if not regs:
+        w("        int unused;")
+    w("    };")
+    w("")
+    # ---- inputs / outputs
+    w("    __device__ __forceinline__ static void")
+    w("    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)")
+    w("    {")
+    for r in regs:
+        w(f"        R.r{r.idx} = 0;")
+    for i, (reg, t, vname) in enumerate(k.inputs):
+        ct = CTYPE[t]
+        w(f"        {{ // input {vname}")
+        w(f"            const {ct}* col = static_cast<const {ct}*>(c.p[{i}]);")
+        w(f"            const {ct} v = col ? col[tid] : static_cast<{ct}>(tid);")
+        w("            " + L.write(Operand(type=t, reg=reg), "v"))
+        w("        }")
+    w("    }")
+    w("")
+    w("    __device__ __forceinline__ static void")
+    w("    store_outputs(const Regs& R, const Columns& c, const unsigned long long tid)")
+    w("    {")
+    for j, (reg, t, vname) in enumerate(k.outputs):
+        ct = CTYPE[t]
+        w(f"        static_cast<{ct}*>(c.p[{nin + j}])[tid] = {L.read(Operand(type=t, reg=reg))}; // {vname}")
+    w("    }")
+    w("")
+    w("    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }")
+    w("    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }")
+    w("")
+    # ---- exec (one block)
+    w("    __device__ __forceinline__ static int")
+    w("    exec(const int b, Regs& R, Ctx& ctx)")
+    w("    {")
+    w("        (void)ctx;")
+    w("        switch(b)")
+    w("        {")
+    for blk in k.blocks:
+        w(f"        case {blk.idx}: // {blk.label}")
+        w("        {")
+        o.extend(L.body(blk.instrs, "            "))
+        w(f"            return {L.next_expr(blk)};")
+        w("        }")
+    w("        default: return kHalt;")
+    w("        }")
+    w("    }")
+    w("")
+    # ---- run (goto CFG)
+    w("    template <bool kProf>")
+    w("    __device__ __forceinline__ static void")
+    w("    run(Regs& R, Ctx& ctx)")
+    w("    {")
+    for blk in k.blocks:
+        w(f"    L_B{blk.idx}: // {blk.label}")
+        w("        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }")
+        w(f"        if constexpr(kProf) count_block(ctx, {len(blk.instrs)}u);")
+        o.extend(L.body(blk.instrs, "        "))
+        o.extend(L.goto_transfer(blk, "        "))
+    w("    L_HALT:")
+    w("        return;")
+    w("    }")
+    w("")
+    # ---- save / restore
+    for fn, const in (("save", "const "), ("restore", "")):
+        w("    __device__ __forceinline__ static void")
+        w(f"    {fn}(const int b, {const}Regs& R, const Columns& c, const unsigned slot)")
+        w("    {")
+        w("        switch(b)")
+        w("        {")
+        for blk in k.blocks:
+            li = sorted(live_in[blk.idx])
+            if not li:
+                continue
+            w(f"        case {blk.idx}:")
+            for r in li:
+                st = CTYPE[L.regs[r].storage]
+                col = f"static_cast<{st}*>(c.p[{scol[r]}])[slot]"
+                if fn == "save":
+                    w(f"            {col} = R.r{r};")
+                else:
+                    w(f"            R.r{r} = {col};")
+            w("            break;")
+        w("        default: break;")
+        w("        }")
+        w("    }")
+        w("")
+    w("};")
+    w("")
+    # ---- host side
+    w("const int kInTypes[] = {" + ", ".join(ABI_TYPE[t] for _, t, _ in k.inputs) + "};")
+    w("const int kOutTypes[] = {" + ", ".join(ABI_TYPE[t] for _, t, _ in k.outputs) + "};")
+    w("const char* const kInNames[] = {" + ", ".join(f'"{n}"' for _, _, n in k.inputs) + "};")
+    w("const char* const kOutNames[] = {" + ", ".join(f'"{n}"' for _, _, n in k.outputs) + "};")
+    w("const int kStateTypes[] = {" + ", ".join(["0"] + [ABI_TYPE[L.regs[r].storage] for r in state]) + "};")
+    w(f"const uint32_t kInstrs[] = {{{', '.join(map(str, counts))}}};")
+    w(f"const uint32_t kLive[] = {{{', '.join(map(str, live_bytes))}}};")
+    state_size = sum(r.nbytes for r in k.regs)
+    w("")
+    w("const loom_b200_kernel_info kInfo = {")
+    w(f'    "{name}", "{k.digest()}", {nin}u, {nout}u, kInTypes, kOutTypes, kInNames, kOutNames,')
+    w(f"    {nb}u, {len(k.regs)}u, {state_size}u, {len(state)}u, kInstrs, kLive}};")
+    w("")
+    w("cudaError_t launch_plain(const PlainLaunch& a)")
+    w("{")
+    w("    const unsigned long long grid = (a.n + a.block - 1) / a.block;")
+    w("    if(grid == 0) return cudaSuccess;")
+    w("    if(a.profile)")
+    w("        plain_kernel<K, true><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(")
+    w("            a.cols, a.n, a.max_steps, a.status, a.counters);")
+    w("    else")
+    w("        plain_kernel<K, false><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(")
+    w("            a.cols, a.n, a.max_steps, a.status, a.counters);")
+    w("    return cudaGetLastError();")
+    w("}")
+    w("")
+    w("cudaError_t launch_regroup(const RegroupLaunch& a)")
+    w("{")
+    w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
+    w("    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),")
+    w("                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);")
+    w("}")
+    w("")
+    w("cudaError_t regroup_occupancy(int block, int* ctas)")
+    w("{")
+    w("    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);")
+    w("}")
+    w("")
+    w(f"}} }} // namespace loom_b200::k_{name}")
+    w("")
+    w(f"extern const loom_b200::KernelEntry loom_b200_entry_{name};")
+    w(f"const loom_b200::KernelEntry loom_b200_entry_{name} = {{")
+    w(f"    &loom_b200::k_{name}::kInfo, {len(state)}, loom_b200::k_{name}::kStateTypes + 1,")
+    w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
+    w(f"    &loom_b200::k_{name}::regroup_occupancy}};")
+    return "\n".join(o) + "\n"
+
+
+def generate_registry(names: List[str]) -> str:
+    o = ["// Generated by loom_b200.codegen: the kernels compiled into libloom_b200.", ""]
+    o.append('#include "../runtime_iface.h"')
+    o.append("")
+    for n in names:
+        o.append(f"extern const loom_b200::KernelEntry loom_b200_entry_{n};")
+    o.append("")
+    o.append("namespace loom_b200 {")
+    o.append("const KernelEntry* const kRegistry[] = {")
+    for n in names:
+        o.append(f"    &loom_b200_entry_{n},")
+    o.append("};")
+    o.append(f"const int kRegistrySize = {len(names)};")
+    o.append("} // namespace loom_b200")
+    return "\n".join(o) + "\n"

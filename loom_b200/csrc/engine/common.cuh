@@ -1,0 +1,145 @@
+// Shared device-side definitions of the B200 Loom engine.
+//
+// Generated kernel code (loom_b200/csrc/gen/*.cu) includes this header; the
+// engines in plain.cuh and regroup.cuh are templates over the generated
+// kernel structs.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+
+#include "loom_b200.h"
+
+namespace loom_b200
+{
+/// Maximum number of columns (inputs + outputs + state registers) per kernel;
+/// the pointer table travels in the kernel's parameter space.
+constexpr int kMaxCols = 96;
+
+/// Block index used for "thread finished" (Loom's halt_pos, core.hpp:985).
+constexpr int kHalt = -1;
+/// Lane holds no thread.
+constexpr int kEmpty = -2;
+
+struct Columns
+{
+    void* p[kMaxCols];
+};
+
+/// Status bits written by device code (also returned through the C ABI).
+enum : unsigned
+{
+    kStatusStepLimit    = LOOM_B200_STATUS_STEP_LIMIT,
+    kStatusAssertFp     = LOOM_B200_STATUS_ASSERT_FP,
+    kStatusQueueOverrun = LOOM_B200_STATUS_QUEUE_OVERRUN,
+    kStatusBarrierTimeout = LOOM_B200_STATUS_BARRIER_TIMEOUT,
+};
+
+/// Per-thread execution context: step guard, instruction counters and the
+/// status word.
+struct Ctx
+{
+    unsigned long long steps;
+    unsigned long long max_steps;
+    unsigned long long thread_instr;
+    unsigned long long warp_instr;
+    unsigned*          status;
+
+    __device__ __forceinline__ void
+    flag(unsigned bit)
+    {
+        atomicOr(status, bit);
+    }
+};
+
+template <typename To, typename From>
+__device__ __forceinline__ To
+bitcast(const From v)
+{
+    static_assert(sizeof(To) == sizeof(From), "bitcast needs equal sizes");
+    To r;
+    memcpy(&r, &v, sizeof(To));
+    return r;
+}
+
+// C++ library semantics of the Loom op set (Loom src/vm/operators.hpp).
+// std::max / std::min: (a < b) ? b : a and (b < a) ? b : a.
+template <typename T>
+__device__ __forceinline__ T
+op_max(const T a, const T b)
+{
+    return (a < b) ? b : a;
+}
+template <typename T>
+__device__ __forceinline__ T
+op_min(const T a, const T b)
+{
+    return (b < a) ? b : a;
+}
+
+__device__ __forceinline__ float op_abs(float v) { return fabsf(v); }
+__device__ __forceinline__ double op_abs(double v) { return fabs(v); }
+__device__ __forceinline__ int op_abs(int v) { return v < 0 ? -v : v; }
+__device__ __forceinline__ long long op_abs(long long v) { return v < 0 ? -v : v; }
+
+__device__ __forceinline__ float op_round(float v) { return roundf(v); }
+__device__ __forceinline__ double op_round(double v) { return round(v); }
+__device__ __forceinline__ float op_ceil(float v) { return ceilf(v); }
+__device__ __forceinline__ double op_ceil(double v) { return ceil(v); }
+__device__ __forceinline__ float op_floor(float v) { return floorf(v); }
+__device__ __forceinline__ double op_floor(double v) { return floor(v); }
+__device__ __forceinline__ float op_trunc(float v) { return truncf(v); }
+__device__ __forceinline__ double op_trunc(double v) { return trunc(v); }
+__device__ __forceinline__ float op_sqrt(float v) { return sqrtf(v); }
+__device__ __forceinline__ double op_sqrt(double v) { return sqrt(v); }
+__device__ __forceinline__ float op_sin(float v) { return sinf(v); }
+__device__ __forceinline__ double op_sin(double v) { return sin(v); }
+__device__ __forceinline__ float op_cos(float v) { return cosf(v); }
+__device__ __forceinline__ double op_cos(double v) { return cos(v); }
+__device__ __forceinline__ float op_copysign(float a, float b) { return copysignf(a, b); }
+__device__ __forceinline__ double op_copysign(double a, double b) { return copysign(a, b); }
+__device__ __forceinline__ float op_fma(float x, float y, float z) { return fmaf(x, y, z); }
+__device__ __forceinline__ double op_fma(double x, double y, double z) { return fma(x, y, z); }
+// rsqrt is 1 / sqrt(x) with IEEE division and square root (operators.hpp:166-174).
+__device__ __forceinline__ float op_rsqrt(float v) { return 1.0f / sqrtf(v); }
+__device__ __forceinline__ double op_rsqrt(double v) { return 1.0 / sqrt(v); }
+
+/// assert_fp (operators.hpp:256-276) aborts the host process on NaN or
+/// infinity; on the device it raises a status bit and passes the value on.
+template <typename T>
+__device__ __forceinline__ T
+op_assert_fp(const T v, Ctx& ctx)
+{
+    if(!isfinite(v)) ctx.flag(kStatusAssertFp);
+    return v;
+}
+
+__device__ __forceinline__ unsigned
+lanemask_lt()
+{
+    unsigned m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+/// Block-wide sum of three counters into global memory, one atomic per warp.
+__device__ __forceinline__ void
+flush_counters(unsigned long long* dst,
+               unsigned long long a,
+               unsigned long long b,
+               unsigned long long c)
+{
+    for(int o = 16; o > 0; o >>= 1)
+    {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if((threadIdx.x & 31) == 0)
+    {
+        if(a) atomicAdd(dst + 0, a);
+        if(b) atomicAdd(dst + 1, b);
+        if(c) atomicAdd(dst + 2, c);
+    }
+}
+} // namespace loom_b200

@@ -1,0 +1,548 @@
+// C-ABI runtime of libloom_b200: kernel registry, handles, device memory and
+// launches of the plain and regrouping engines.
+//
+// The handle plays the role of Loom's backend facades (cuda::MemoryFacade /
+// StreamFacade, Loom src/vm/cuda.hpp:1029-1327): it owns the device columns
+// and the regrouping workspace (RAII on the host side of the ABI), copies
+// inputs in and outputs out, and runs the kernel to completion on the device
+// without per-round host round trips.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "runtime_iface.h"
+
+using namespace loom_b200;
+
+namespace
+{
+thread_local std::string g_last_error;
+
+int
+cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    if(e == cudaErrorMemoryAllocation) return LOOM_B200_ERR_OOM;
+    if(e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return LOOM_B200_ERR_NO_DEVICE;
+    return LOOM_B200_ERR_CUDA;
+}
+
+#define LB_CUDA(call)                                  \
+    do                                                 \
+    {                                                  \
+        const cudaError_t e_ = (call);                 \
+        if(e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while(0)
+
+size_t
+type_bytes(int t)
+{
+    switch(t)
+    {
+    case LOOM_B200_B8:
+    case LOOM_B200_I8:
+    case LOOM_B200_U8: return 1;
+    case LOOM_B200_I16:
+    case LOOM_B200_U16: return 2;
+    case LOOM_B200_I32:
+    case LOOM_B200_U32:
+    case LOOM_B200_F32: return 4;
+    default: return 8;
+    }
+}
+
+__global__ void
+regroup_reset(RegroupCtl*        ctl,
+              unsigned*          qcnt,
+              unsigned*          qhead,
+              unsigned           num_blocks,
+              unsigned long long input_cursor)
+{
+    for(unsigned i = threadIdx.x; i < 3 * num_blocks; i += blockDim.x)
+    {
+        if(i < 2 * num_blocks)
+            qcnt[i] = 0u;
+        else
+            qhead[i - 2 * num_blocks] = 0u;
+    }
+    if(threadIdx.x == 0)
+    {
+        ctl->bar_count    = 0u;
+        ctl->bar_gen      = 0u;
+        ctl->done         = 0u;
+        ctl->pad0         = 0u;
+        ctl->init_head    = 0ull;
+        ctl->input_cursor = input_cursor;
+    }
+}
+
+constexpr unsigned long long kDefaultMaxSteps    = 1ull << 40;
+constexpr unsigned long long kBarrierSpins       = 1ull << 25;
+constexpr unsigned           kDefaultPlainBlock  = 256;
+constexpr unsigned           kDefaultRegroupBlock = 256;
+constexpr unsigned           kDefaultUtr         = 16;
+constexpr unsigned           kDefaultPeriod      = 256;
+} // namespace
+
+struct loom_b200_handle
+{
+    const KernelEntry* e = nullptr;
+    loom_b200_opts     opts{};
+    uint64_t           capacity = 0;
+    int                device   = 0;
+    int                sms      = 0;
+    cudaStream_t       stream   = nullptr;
+    cudaEvent_t        ev0 = nullptr, ev1 = nullptr;
+
+    // staging columns for run_host
+    std::vector<void*> d_in, d_out;
+    // device bookkeeping
+    unsigned*           d_status   = nullptr;
+    unsigned long long* d_counters = nullptr; // 8 counters
+    // regrouping workspace, sized for `ws_cap` slots
+    uint64_t            ws_cap = 0;
+    std::vector<void*>  d_state;
+    unsigned*           d_q     = nullptr;
+    unsigned*           d_qcnt  = nullptr;
+    unsigned*           d_qhead = nullptr;
+    unsigned*           d_tid   = nullptr;
+    RegroupCtl*         d_ctl   = nullptr;
+
+    loom_b200_stats stats{};
+    unsigned        last_grid     = 0;
+    bool            pending       = false; // launched, counters not read yet
+    uint64_t        launches      = 0;
+    uint64_t        plain_threads = 0;
+};
+
+namespace
+{
+void
+free_ws(loom_b200_handle* h)
+{
+    for(void* p: h->d_state) cudaFree(p);
+    h->d_state.clear();
+    cudaFree(h->d_q);
+    cudaFree(h->d_qcnt);
+    cudaFree(h->d_qhead);
+    cudaFree(h->d_tid);
+    h->d_q = nullptr;
+    h->d_qcnt = h->d_qhead = h->d_tid = nullptr;
+    h->ws_cap = 0;
+}
+
+int
+ensure_ws(loom_b200_handle* h, uint64_t cap)
+{
+    if(cap <= h->ws_cap) return LOOM_B200_OK;
+    free_ws(h);
+    const KernelEntry& e = *h->e;
+    const uint64_t     B = e.info->num_blocks;
+    h->d_state.assign(static_cast<size_t>(e.num_state), nullptr);
+    for(int i = 0; i < e.num_state; ++i)
+        LB_CUDA(cudaMalloc(&h->d_state[i], cap * type_bytes(e.state_types[i])));
+    LB_CUDA(cudaMalloc(&h->d_q, 2 * B * cap * sizeof(unsigned)));
+    LB_CUDA(cudaMalloc(&h->d_qcnt, 2 * B * sizeof(unsigned)));
+    LB_CUDA(cudaMalloc(&h->d_qhead, B * sizeof(unsigned)));
+    LB_CUDA(cudaMalloc(&h->d_tid, cap * sizeof(unsigned)));
+    h->ws_cap = cap;
+    return LOOM_B200_OK;
+}
+
+void
+normalise(loom_b200_opts& o)
+{
+    if(o.block_size == 0 || o.block_size % 32 != 0 || o.block_size > 1024)
+        o.block_size = o.mode == LOOM_B200_REGROUP ? kDefaultRegroupBlock
+                                                   : kDefaultPlainBlock;
+    if(o.utr_lanes == 0 || o.utr_lanes > 32) o.utr_lanes = kDefaultUtr;
+    if(o.period == 0) o.period = kDefaultPeriod;
+    if(o.max_steps == 0) o.max_steps = kDefaultMaxSteps;
+}
+
+int
+finish_launch(loom_b200_handle* h)
+{
+    if(!h->pending) return h->stats.status ? LOOM_B200_ERR_DEVICE : LOOM_B200_OK;
+    LB_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    LB_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    unsigned long long c[8];
+    unsigned           status = 0;
+    LB_CUDA(cudaMemcpy(c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    LB_CUDA(cudaMemcpy(&status, h->d_status, sizeof(status), cudaMemcpyDeviceToHost));
+    loom_b200_stats& s = h->stats;
+    s.launches     = h->launches;
+    s.thread_instr = c[0];
+    s.warp_instr   = c[1];
+    s.parks        = c[2];
+    s.state_bytes  = c[3];
+    s.rounds       = c[5];
+    s.threads      = c[4] + h->plain_threads;
+    s.status       = status;
+    s.grid         = h->last_grid;
+    s.ms           = ms;
+    h->pending     = false;
+    return status ? LOOM_B200_ERR_DEVICE : LOOM_B200_OK;
+}
+
+int
+launch(loom_b200_handle* h,
+       const void* const* in,
+       void* const*       out,
+       uint64_t           n,
+       cudaStream_t       stream)
+{
+    const KernelEntry&           e    = *h->e;
+    const loom_b200_kernel_info& info = *e.info;
+    if(n == 0) return LOOM_B200_OK;
+    if(n >= (1ull << 32))
+    {
+        g_last_error = "at most 2^32 - 1 threads per launch";
+        return LOOM_B200_ERR_INVALID;
+    }
+    Columns cols{};
+    int     c = 0;
+    for(uint32_t i = 0; i < info.num_inputs; ++i)
+        cols.p[c++] = const_cast<void*>(in[i]);
+    for(uint32_t i = 0; i < info.num_outputs; ++i)
+    {
+        if(out[i] == nullptr)
+        {
+            g_last_error = "output column is NULL";
+            return LOOM_B200_ERR_INVALID;
+        }
+        cols.p[c++] = out[i];
+    }
+    const loom_b200_opts& o = h->opts;
+    if(o.mode == LOOM_B200_REGROUP)
+    {
+        // the workspace is reallocated only between launches
+        const uint64_t pop = o.population ? std::min<uint64_t>(o.population, n) : n;
+        const uint64_t cap = o.no_refill ? n : pop;
+        if(cap > h->ws_cap)
+        {
+            LB_CUDA(cudaStreamSynchronize(stream));
+            const int rc = ensure_ws(h, cap);
+            if(rc) return rc;
+        }
+    }
+    LB_CUDA(cudaEventRecord(h->ev0, stream));
+    if(o.mode == LOOM_B200_REGROUP)
+    {
+        const uint64_t pop = o.population ? std::min<uint64_t>(o.population, n) : n;
+        const uint64_t cap = o.no_refill ? n : pop;
+        for(int i = 0; i < e.num_state; ++i) cols.p[c++] = h->d_state[i];
+        int ctas = 0;
+        LB_CUDA(e.regroup_occupancy(static_cast<int>(o.block_size), &ctas));
+        if(ctas <= 0)
+        {
+            g_last_error = "regroup kernel does not fit on an SM at this block size";
+            return LOOM_B200_ERR_INVALID;
+        }
+        if(o.ctas_per_sm) ctas = std::min<int>(ctas, static_cast<int>(o.ctas_per_sm));
+        RegroupLaunch L{};
+        L.params.cols          = cols;
+        L.params.q             = h->d_q;
+        L.params.qcnt          = h->d_qcnt;
+        L.params.qhead         = h->d_qhead;
+        L.params.tidcol        = h->d_tid;
+        L.params.ctl           = h->d_ctl;
+        L.params.status        = h->d_status;
+        L.params.counters      = h->d_counters;
+        L.params.n             = n;
+        L.params.max_rounds    = o.max_steps;
+        L.params.barrier_spins = o.barrier_spins ? o.barrier_spins : kBarrierSpins;
+        L.params.phantoms      = o.fault_phantom_ctas;
+        L.params.cap           = static_cast<unsigned>(cap);
+        L.params.utr           = o.utr_lanes;
+        L.params.period        = o.period;
+        L.params.refill        = o.no_refill ? 0u : 1u;
+        L.grid                 = static_cast<unsigned>(ctas * h->sms);
+        L.block                = o.block_size;
+        L.stream               = stream;
+        regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl,
+                                             h->d_qcnt,
+                                             h->d_qhead,
+                                             info.num_blocks,
+                                             std::min<uint64_t>(n, cap));
+        LB_CUDA(cudaGetLastError());
+        LB_CUDA(e.regroup(L));
+        h->last_grid = L.grid;
+    }
+    else
+    {
+        PlainLaunch L{};
+        L.cols      = cols;
+        L.n         = n;
+        L.max_steps = o.max_steps;
+        L.status    = h->d_status;
+        L.counters  = h->d_counters;
+        L.block     = o.block_size;
+        L.profile   = o.profile != 0;
+        L.stream    = stream;
+        LB_CUDA(e.plain(L));
+        h->last_grid = static_cast<unsigned>((n + o.block_size - 1) / o.block_size);
+        h->plain_threads += n;
+    }
+    LB_CUDA(cudaEventRecord(h->ev1, stream));
+    h->pending = true;
+    h->launches += 1;
+    return LOOM_B200_OK;
+}
+} // namespace
+
+extern "C" {
+
+int
+loom_b200_version(void)
+{
+    return LOOM_B200_ABI_VERSION;
+}
+
+const char*
+loom_b200_error_string(int code)
+{
+    switch(code)
+    {
+    case LOOM_B200_OK: return "ok";
+    case LOOM_B200_ERR_INVALID:
+        return g_last_error.empty() ? "invalid argument" : g_last_error.c_str();
+    case LOOM_B200_ERR_NOT_FOUND: return "kernel not compiled into libloom_b200";
+    case LOOM_B200_ERR_CUDA:
+    case LOOM_B200_ERR_OOM:
+    case LOOM_B200_ERR_NO_DEVICE:
+        return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+    case LOOM_B200_ERR_DEVICE: return "device status word set (see stats.status)";
+    case LOOM_B200_ERR_BUDGET: return "request exceeds the device memory budget";
+    case LOOM_B200_ERR_CANCELLED: return "request cancelled";
+    case LOOM_B200_ERR_TIMEOUT: return "watchdog expired";
+    default: return "unknown error";
+    }
+}
+
+int
+loom_b200_kernel_count(void)
+{
+    return kRegistrySize;
+}
+
+int
+loom_b200_kernel_get(int index, const loom_b200_kernel_info** info)
+{
+    if(!info || index < 0 || index >= kRegistrySize) return LOOM_B200_ERR_INVALID;
+    *info = kRegistry[index]->info;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_kernel_find(const char* name, const loom_b200_kernel_info** info)
+{
+    if(!name || !info) return LOOM_B200_ERR_INVALID;
+    for(int i = 0; i < kRegistrySize; ++i)
+        if(std::strcmp(kRegistry[i]->info->name, name) == 0)
+        {
+            *info = kRegistry[i]->info;
+            return LOOM_B200_OK;
+        }
+    return LOOM_B200_ERR_NOT_FOUND;
+}
+
+int
+loom_b200_create(const char*           kernel,
+                 uint64_t              capacity,
+                 const loom_b200_opts* opts,
+                 loom_b200_handle**    out)
+{
+    if(!kernel || !out) return LOOM_B200_ERR_INVALID;
+    *out = nullptr;
+    const KernelEntry* e = nullptr;
+    for(int i = 0; i < kRegistrySize; ++i)
+        if(std::strcmp(kRegistry[i]->info->name, kernel) == 0) e = kRegistry[i];
+    if(!e) return LOOM_B200_ERR_NOT_FOUND;
+    int ndev = 0;
+    const cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if(ce != cudaSuccess || ndev == 0)
+    {
+        g_last_error = ce != cudaSuccess ? cudaGetErrorString(ce) : "no CUDA device";
+        return LOOM_B200_ERR_NO_DEVICE;
+    }
+    auto* h = new(std::nothrow) loom_b200_handle();
+    if(!h) return LOOM_B200_ERR_OOM;
+    h->e        = e;
+    h->capacity = capacity;
+    if(opts) h->opts = *opts;
+    normalise(h->opts);
+    auto fail = [&](int rc)
+    {
+        loom_b200_destroy(h);
+        return rc;
+    };
+    if(cudaGetDevice(&h->device) != cudaSuccess) return fail(LOOM_B200_ERR_CUDA);
+    if(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device) !=
+       cudaSuccess)
+        return fail(LOOM_B200_ERR_CUDA);
+    if(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
+        return fail(LOOM_B200_ERR_CUDA);
+    if(cudaMalloc(&h->d_status, sizeof(unsigned)) != cudaSuccess ||
+       cudaMalloc(&h->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+       cudaMalloc(&h->d_ctl, sizeof(RegroupCtl)) != cudaSuccess)
+        return fail(LOOM_B200_ERR_OOM);
+    if(cudaMemset(h->d_counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+       cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess)
+        return fail(LOOM_B200_ERR_CUDA);
+    const loom_b200_kernel_info& info = *e->info;
+    h->d_in.assign(info.num_inputs, nullptr);
+    h->d_out.assign(info.num_outputs, nullptr);
+    if(capacity)
+    {
+        for(uint32_t i = 0; i < info.num_inputs; ++i)
+            if(cudaMalloc(&h->d_in[i], capacity * type_bytes(info.input_types[i])) !=
+               cudaSuccess)
+                return fail(LOOM_B200_ERR_OOM);
+        for(uint32_t i = 0; i < info.num_outputs; ++i)
+            if(cudaMalloc(&h->d_out[i], capacity * type_bytes(info.output_types[i])) !=
+               cudaSuccess)
+                return fail(LOOM_B200_ERR_OOM);
+    }
+    *out = h;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_destroy(loom_b200_handle* h)
+{
+    if(!h) return LOOM_B200_OK;
+    if(h->stream) cudaStreamSynchronize(h->stream);
+    free_ws(h);
+    for(void* p: h->d_in) cudaFree(p);
+    for(void* p: h->d_out) cudaFree(p);
+    cudaFree(h->d_status);
+    cudaFree(h->d_counters);
+    cudaFree(h->d_ctl);
+    if(h->ev0) cudaEventDestroy(h->ev0);
+    if(h->ev1) cudaEventDestroy(h->ev1);
+    if(h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_set_opts(loom_b200_handle* h, const loom_b200_opts* opts)
+{
+    if(!h || !opts) return LOOM_B200_ERR_INVALID;
+    if(h->pending)
+    {
+        const int rc = finish_launch(h);
+        if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
+    }
+    h->opts = *opts;
+    normalise(h->opts);
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_get_opts(const loom_b200_handle* h, loom_b200_opts* opts)
+{
+    if(!h || !opts) return LOOM_B200_ERR_INVALID;
+    *opts = h->opts;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_run_host(loom_b200_handle*  h,
+                   const void* const* inputs,
+                   void* const*       outputs,
+                   uint64_t           n)
+{
+    if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
+        return LOOM_B200_ERR_INVALID;
+    if(n > h->capacity)
+    {
+        g_last_error = "n exceeds the handle's capacity";
+        return LOOM_B200_ERR_INVALID;
+    }
+    if(n == 0) return LOOM_B200_OK;
+    const loom_b200_kernel_info& info = *h->e->info;
+    std::vector<const void*>     din(info.num_inputs);
+    for(uint32_t i = 0; i < info.num_inputs; ++i)
+    {
+        if(inputs[i] == nullptr)
+            din[i] = nullptr; // iota
+        else
+        {
+            LB_CUDA(cudaMemcpyAsync(h->d_in[i],
+                                    inputs[i],
+                                    n * type_bytes(info.input_types[i]),
+                                    cudaMemcpyHostToDevice,
+                                    h->stream));
+            din[i] = h->d_in[i];
+        }
+    }
+    int rc = launch(h, din.data(), h->d_out.data(), n, h->stream);
+    if(rc) return rc;
+    for(uint32_t i = 0; i < info.num_outputs; ++i)
+        LB_CUDA(cudaMemcpyAsync(outputs[i],
+                                h->d_out[i],
+                                n * type_bytes(info.output_types[i]),
+                                cudaMemcpyDeviceToHost,
+                                h->stream));
+    LB_CUDA(cudaStreamSynchronize(h->stream));
+    return finish_launch(h);
+}
+
+int
+loom_b200_run_device(loom_b200_handle*  h,
+                     const void* const* inputs,
+                     void* const*       outputs,
+                     uint64_t           n,
+                     void*              stream)
+{
+    if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
+        return LOOM_B200_ERR_INVALID;
+    return launch(h,
+                  inputs,
+                  outputs,
+                  n,
+                  stream ? static_cast<cudaStream_t>(stream) : h->stream);
+}
+
+int
+loom_b200_sync(loom_b200_handle* h)
+{
+    if(!h) return LOOM_B200_ERR_INVALID;
+    return finish_launch(h);
+}
+
+int
+loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats)
+{
+    if(!h || !stats) return LOOM_B200_ERR_INVALID;
+    const int rc = finish_launch(h);
+    if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
+    *stats = h->stats;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_reset_stats(loom_b200_handle* h)
+{
+    if(!h) return LOOM_B200_ERR_INVALID;
+    const int rc = finish_launch(h);
+    if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
+    LB_CUDA(cudaMemset(h->d_counters, 0, 8 * sizeof(unsigned long long)));
+    LB_CUDA(cudaMemset(h->d_status, 0, sizeof(unsigned)));
+    h->stats         = loom_b200_stats{};
+    h->launches      = 0;
+    h->plain_threads = 0;
+    return LOOM_B200_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,45 @@
+// Interface between the hand-written runtime (runtime.cu) and the generated
+// per-kernel translation units (gen/*.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "engine/regroup.cuh"
+#include "loom_b200.h"
+
+namespace loom_b200
+{
+struct PlainLaunch
+{
+    Columns             cols;
+    unsigned long long  n;
+    unsigned long long  max_steps;
+    unsigned*           status;
+    unsigned long long* counters;
+    unsigned            block;
+    bool                profile;
+    cudaStream_t        stream;
+};
+
+struct RegroupLaunch
+{
+    RegroupParams params;
+    unsigned      grid;
+    unsigned      block;
+    cudaStream_t  stream;
+};
+
+/// One compiled kernel: its descriptor and the launchers of both engines.
+struct KernelEntry
+{
+    const loom_b200_kernel_info* info;
+    int                          num_state;   // state columns
+    const int*                   state_types; // storage type per state column
+    cudaError_t (*plain)(const PlainLaunch&);
+    cudaError_t (*regroup)(const RegroupLaunch&);
+    cudaError_t (*regroup_occupancy)(int block, int* ctas_per_sm);
+};
+
+extern const KernelEntry* const kRegistry[];
+extern const int                kRegistrySize;
+} // namespace loom_b200

@@ -1,0 +1,170 @@
+"""Parity of both B200 engines with Loom's scalar backend (needs a GPU).
+
+Every kernel of the registry runs through the C ABI in plain and regrouping
+form on the golden inputs and must reproduce Loom bse's outputs bit for bit
+(tests/golden/, made by tests/golden/make_golden.py).  Large cases check
+size-independent properties: plain == regroup on every thread, a seeded
+sample against the C oracle, known answers, and the total VM-instruction
+count equal to the oracle's (each executed block counted once per thread).
+"""
+
+import numpy as np
+import pytest
+
+from loom_b200 import api
+from loom_b200.codegen import ir
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+KERNELS = ir.available()
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint8)
+
+
+def _as_list(x):
+    return list(x) if isinstance(x, tuple) else [x]
+
+
+def _check(name, got, want):
+    for g, w in zip(got, want):
+        assert np.array_equal(_bits(g), _bits(w)), f"{name}: {int((g != w).sum())} threads differ"
+
+
+@pytest.mark.parametrize("mode", ["plain", "regroup"])
+@pytest.mark.parametrize("name", KERNELS)
+def test_engine_matches_loom_bse(name, mode, golden):
+    ins, outs = golden(name)
+    with api.Function(name, len(ins[0]), mode) as f:
+        got = _as_list(f(*ins))
+        s = f.stats(raise_on_device_error=True)
+    _check(name, got, outs)
+    assert s["threads"] == len(ins[0])
+
+
+REGROUP_VARIANTS = [
+    dict(utr_lanes=1, period=1),
+    dict(utr_lanes=32, period=3),
+    dict(utr_lanes=16, period=7, block_size=64),
+    dict(utr_lanes=8, period=1000, block_size=1024),
+    dict(population=100),
+    dict(population=1000, utr_lanes=24),
+    dict(refill=False, period=5),
+    dict(ctas_per_sm=1, population=37),
+]
+
+
+@pytest.mark.parametrize("variant", REGROUP_VARIANTS, ids=lambda v: ",".join(f"{k}={x}" for k, x in v.items()))
+@pytest.mark.parametrize("name", ["fib_u64", "collatz_u64", "fac_u64", "jmp4_u64", "union_cmov_f32", "slt_inv_u32"])
+def test_regroup_options_keep_results(name, variant, golden):
+    ins, outs = golden(name)
+    with api.Function(name, len(ins[0]), "regroup", **variant) as f:
+        got = _as_list(f(*ins))
+        s = f.stats(raise_on_device_error=True)
+    _check(name, got, outs)
+    assert s["threads"] == len(ins[0])
+
+
+def test_plain_block_sizes(golden):
+    ins, outs = golden("collatz_u64")
+    for bs in (32, 128, 512, 1024):
+        with api.Function("collatz_u64", len(ins[0]), "plain", block_size=bs) as f:
+            _check("collatz_u64", _as_list(f(*ins)), outs)
+
+
+@pytest.mark.parametrize("mode", ["plain", "regroup"])
+def test_instruction_count_equals_oracle(mode, golden):
+    ins, outs = golden("collatz_u64")
+    (_,), counts = O.Interp("collatz_u64").run(ins, count_instr=True)
+    with api.Function("collatz_u64", len(ins[0]), mode, profile=True) as f:
+        f(*ins)
+        s = f.stats(raise_on_device_error=True)
+    assert s["thread_instr"] == int(counts.sum())
+    assert 0.0 < s["lane_efficiency"] <= 1.0
+
+
+def test_fib_config0_full_size():
+    """2^20 threads, n uniform in [0, 93]: bit-exact against the numpy
+    restatement of Loom's val_fib (programs.hpp:353-368)."""
+    n = O.uniform_int(11, 1 << 20, 0, 93)
+    want = O.val_fib(n)
+    for mode in ("plain", "regroup"):
+        with api.Function("fib_u64", len(n), mode) as f:
+            got = f(n)
+            f.stats(raise_on_device_error=True)
+        assert np.array_equal(got, want), mode
+
+
+def test_collatz_large_plain_equals_regroup_and_oracle_sample():
+    """2^22 threads: both engines agree on every thread; a seeded sample
+    matches the C oracle; known stopping times hold."""
+    n = O.uniform_int(12, 1 << 22, 1, (1 << 32) - 1)
+    n[:4] = [27, 97, 837799, 1]
+    with api.Function("collatz_u64", len(n), "plain") as f:
+        a = f(n)
+    with api.Function("collatz_u64", len(n), "regroup", population=1 << 18) as f:
+        b = f(n)
+        s = f.stats(raise_on_device_error=True)
+    assert np.array_equal(a, b)
+    assert a[:4].tolist() == [111, 118, 524, 0]
+    idx = O.uniform_int(13, 4096, 0, len(n) - 1).astype(np.int64)
+    (want,) = O.Interp("collatz_u64").run([n[idx]])
+    assert np.array_equal(a[idx], want)
+    assert s["threads"] == len(n)
+
+
+def test_iota_input_column():
+    """A NULL input column feeds the thread index (no input traffic)."""
+    with api.Function("collatz_u64", 5000, "regroup") as f:
+        got = f(None, n=5000)
+    assert np.array_equal(got, O.val_collatz(np.arange(5000, dtype=np.uint64)))
+
+
+@pytest.mark.parametrize("mode", ["plain", "regroup"])
+def test_step_guard_ends_a_runaway_thread(mode):
+    """fib(2^64 - 1) never halts; the step guard ends it with a status bit
+    instead of hanging the GPU, the other threads finish, and the handle
+    stays usable."""
+    n = np.arange(64, dtype=np.uint64)
+    n[5] = np.uint64(2**64 - 1)
+    with api.Function("fib_u64", len(n), mode, max_steps=2000, period=16) as f:
+        with pytest.raises(api.LoomError) as e:
+            f(n)
+        assert e.value.code == api.ERR_DEVICE
+        assert f.stats()["status"] & api.STATUS_STEP_LIMIT
+        good = np.delete(np.arange(64), 5)
+        f.reset_stats()
+        m = n.copy()
+        m[5] = 7
+        got = f(m)
+        assert np.array_equal(got, O.val_fib(m))
+
+
+def test_barrier_wait_is_bounded():
+    """Fault injection: the grid barrier waits for CTAs that do not exist;
+    its bounded wait runs out, the status word says so, and the next launch
+    on the same handle is correct."""
+    n = O.uniform_int(3, 4096, 0, 93)
+    with api.Function("fib_u64", len(n), "regroup", fault_phantom_ctas=1, barrier_spins=20000) as f:
+        with pytest.raises(api.LoomError):
+            f(n)
+        assert f.stats()["status"] & api.STATUS_BARRIER_TIMEOUT
+        f.set_opts("regroup")
+        f.reset_stats()
+        assert np.array_equal(f(n), O.val_fib(n))
+
+
+def test_run_device_with_torch_columns():
+    import torch
+
+    n = O.uniform_int(21, 100000, 1, 1 << 20)
+    d_in = torch.from_numpy(n.view(np.int64)).cuda()
+    d_out = torch.empty(len(n), dtype=torch.int32, device="cuda")
+    with api.Function("collatz_u64", 0, "regroup") as f:
+        f.run_device([d_in], [d_out], len(n), stream=torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        f.sync()
+    got = d_out.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, O.val_collatz(n))

@@ -1,0 +1,97 @@
+"""The oracle pinned against Loom's own scalar backend (CPU only).
+
+tests/golden/*.npz hold outputs of vm::bse::function<K> compiled from the Loom
+headers (tests/golden/make_golden.py); the C restatement of bse must
+reproduce every one of them bit for bit, and the numpy restatements of Loom's
+validators (src/tests/programs.hpp:290-389) must agree with both.
+"""
+
+import numpy as np
+import pytest
+
+from loom_b200.codegen import ir
+from oracle import oracle as O
+
+KERNELS = ir.available()
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint8)
+
+
+@pytest.mark.parametrize("name", KERNELS)
+def test_interp_matches_golden(name, golden):
+    ins, outs = golden(name)
+    got = O.Interp(name).run(ins)
+    assert len(got) == len(outs)
+    for g, o in zip(got, outs):
+        assert np.array_equal(_bits(g), _bits(o)), name
+
+
+def test_golden_fixture_for_every_kernel():
+    import pathlib
+
+    d = pathlib.Path(__file__).parent / "golden"
+    assert {p.stem for p in d.glob("*.npz")} == set(KERNELS)
+
+
+def test_val_fib_matches_golden(golden):
+    (n,), (c,) = golden("fib_u64")
+    assert np.array_equal(O.val_fib(n), c)
+    # Loom README.md:113-128 example values
+    assert int(O.val_fib(np.array([90], dtype=np.uint64))[0]) == 2880067194370816120
+
+
+def test_val_collatz_matches_golden(golden):
+    (n,), (s,) = golden("collatz_u64")
+    assert np.array_equal(O.val_collatz(n), s)
+    known = {1: 0, 2: 1, 3: 7, 6: 8, 7: 16, 27: 111, 97: 118, 837799: 524}
+    for k, v in known.items():
+        assert int(O.val_collatz(np.array([k], dtype=np.uint64))[0]) == v
+
+
+def test_val_fac_and_jmp4(golden):
+    (a,), (r,) = golden("fac_u64")
+    assert np.array_equal(O.val_fac(a), r)
+    (i,), (j,) = golden("jmp4_u64")
+    assert np.array_equal(O.val_jmp4(i), j)
+
+
+def test_interp_out_of_table_parmjump_halts():
+    # jmp4: values outside the 4-entry table leave the thread unchanged,
+    # like bse's switch without a matching case (bse.hpp:192-198)
+    i = np.array([0, 1, 2, 3, 4, 9, 200], dtype=np.uint32)
+    (o,) = O.Interp("jmp4_f32").run([i])
+    assert o.tolist() == [1, 3, 7, 11, 4, 9, 200]
+
+
+def test_interp_step_limit():
+    # fib of 2^64 - 1 loops while i <= n, i.e. forever: the guard must end it
+    with pytest.raises(RuntimeError):
+        O.Interp("fib_u64").run([np.array([2**64 - 1], dtype=np.uint64)], max_steps=1000)
+
+
+def test_interp_instruction_counts():
+    # fib(n) for n >= 2: START (3) + work (4) + (n - 1) loop iterations (6)
+    n = np.array([0, 1, 2, 10], dtype=np.uint64)
+    (_,), cnt = O.Interp("fib_u64").run([n], count_instr=True)
+    assert cnt.tolist() == [3, 3, 3 + 4 + 6, 3 + 4 + 6 * 9]
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="Loom bse runner not built here")
+def test_interp_matches_loom_bse_fresh_inputs():
+    import kernel_domains as D
+
+    for name in ["fib_u64", "collatz_u64", "arithmetic_f32", "union_cmov_f64", "slt_inv_u32"]:
+        k = ir.load(name)
+        ins = D.inputs_for(name, 3000, 99, [t for _, t, _ in k.inputs])
+        a = O.Interp(name).run(ins)
+        b = O.ref_run(name, ins, 3000, threads=2)
+        for x, y in zip(a, b):
+            assert np.array_equal(_bits(x), _bits(y)), name
+
+
+def test_splitmix_stream_is_fixed():
+    # SplitMix64 reference values for seed 0 (Steele et al. 2014)
+    z = O.splitmix64(0, 3)
+    assert z.tolist() == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F]
