@@ -93,10 +93,17 @@ typedef struct loom_b200_opts
                              largest same-PC group has >= utr_lanes lanes
                              (the GPU form of Loom's UTR, simd.hpp:3273-3292) */
     uint32_t period;      /* regroup: max block steps per tile per round */
+    uint32_t burst;       /* regroup: blocks a lane runs between two votes */
+    uint32_t spread_lanes; /* regroup: when the majority block holds at least
+                              this many lanes, every live lane runs the
+                              burst (33 = majority lanes only) */
+    uint32_t catchup;     /* regroup: blocks a lane behind the majority block
+                             may run to reach it before a burst
+                             (0 = default, 0xffffffff = none) */
     uint64_t population;  /* regroup: resident thread slots; 0 = all inputs */
     uint64_t max_steps;   /* per-thread block-step guard; 0 = 2^40 */
-    uint32_t profile;     /* plain: collect lane-efficiency counters */
-    uint32_t no_refill;   /* regroup: do not refill halted lanes in registers */
+    uint32_t profile;     /* collect lane-efficiency counters (slower) */
+    uint32_t no_prefetch; /* regroup: do not prefetch each lane's next input */
     uint32_t ctas_per_sm; /* regroup: resident CTAs per SM; 0 = occupancy max */
     uint32_t fault_phantom_ctas; /* fault injection for tests: the grid barrier
                                     also waits for this many CTAs that do not
@@ -151,8 +158,9 @@ int loom_b200_run_host(loom_b200_handle*  h,
                        void* const*       outputs,
                        uint64_t           n);
 
-/* Device columns in and out, enqueued on `stream` (a cudaStream_t, NULL =
- * the handle's own stream); returns without synchronising. */
+/* Device columns in and out, enqueued on `stream` (a cudaStream_t; NULL is
+ * the CUDA default stream, as everywhere in CUDA); returns without
+ * synchronising. */
 int loom_b200_run_device(loom_b200_handle*  h,
                          const void* const* inputs,
                          void* const*       outputs,

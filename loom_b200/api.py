@@ -88,10 +88,13 @@ class Opts(ctypes.Structure):
         ("block_size", ctypes.c_uint32),
         ("utr_lanes", ctypes.c_uint32),
         ("period", ctypes.c_uint32),
+        ("burst", ctypes.c_uint32),
+        ("spread_lanes", ctypes.c_uint32),
+        ("catchup", ctypes.c_uint32),
         ("population", ctypes.c_uint64),
         ("max_steps", ctypes.c_uint64),
         ("profile", ctypes.c_uint32),
-        ("no_refill", ctypes.c_uint32),
+        ("no_prefetch", ctypes.c_uint32),
         ("ctas_per_sm", ctypes.c_uint32),
         ("fault_phantom_ctas", ctypes.c_uint32),
         ("barrier_spins", ctypes.c_uint64),
@@ -215,10 +218,13 @@ def make_opts(
     block_size: int = 0,
     utr_lanes: int = 0,
     period: int = 0,
+    burst: int = 0,
+    spread_lanes: int = 0,
+    catchup: int = 0,
     population: int = 0,
     max_steps: int = 0,
     profile: bool = False,
-    refill: bool = True,
+    prefetch: bool = True,
     ctas_per_sm: int = 0,
     fault_phantom_ctas: int = 0,
     barrier_spins: int = 0,
@@ -230,10 +236,13 @@ def make_opts(
         block_size=block_size,
         utr_lanes=utr_lanes,
         period=period,
+        burst=burst,
+        spread_lanes=spread_lanes,
+        catchup=catchup,
         population=population,
         max_steps=max_steps,
         profile=1 if profile else 0,
-        no_refill=0 if refill else 1,
+        no_prefetch=0 if prefetch else 1,
         ctas_per_sm=ctas_per_sm,
         fault_phantom_ctas=fault_phantom_ctas,
         barrier_spins=barrier_spins,
@@ -301,7 +310,7 @@ class Function:
 
     def run_device(self, inputs: Sequence, outputs: Sequence, n: int, stream=None) -> None:
         """Device columns in and out; asynchronous on `stream` (cudaStream_t
-        handle or torch.cuda.Stream; None = the handle's own stream)."""
+        handle or torch.cuda.Stream; None = the CUDA default stream)."""
         pin = (ctypes.c_void_p * max(1, len(inputs)))(*[_ptr(a) for a in inputs])
         pout = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
         s = getattr(stream, "cuda_stream", stream)

@@ -6,11 +6,13 @@ struct ``K`` with
 * ``Regs``            the Loom register file as scalars (kept in CUDA
                       registers); Union registers (Loom src/common/union.hpp)
                       are stored as unsigned integers and bit-cast per view;
-* ``run<kProf>``      the whole program as a goto CFG (plain engine);
-* ``exec(b)``         one basic block, returning the next block (regrouping
-                      engine);
-* ``save/restore(b)`` the live-in registers of block b to/from the SoA state
-                      file;
+* ``run_burst<kProf>`` the whole program as a goto CFG that can be entered at
+                      any block and stops after a budget of blocks: the
+                      plain engine runs it from block 0 with the step guard
+                      as budget, the regrouping engine runs bursts of a few
+                      blocks between warp votes;
+* ``save/restore(b)`` the live-in registers of block b to/from the queue of
+                      block b (an SoA segment per block and round parity);
 * ``load_inputs`` / ``store_outputs`` the input/output columns;
 
 plus the host-side descriptor and launchers.  Op semantics follow Loom
@@ -264,12 +266,27 @@ def generate(k: Kernel) -> str:
     nout = len(k.outputs)
     live_in, _ = k.liveness()
     state = k.state_regs()
-    scol = {r: nin + nout + j for j, r in enumerate(state)}
     counts = k.instr_counts()
     live_bytes = [sum(L.regs[r].nbytes for r in li) for li in live_in]
     regs = [r for r in k.regs if r.idx != L.pc]
-    if nin + nout + len(state) > 96:
+    if nin + nout > 96:
         raise ValueError(f"{name}: too many columns")
+    # queue segments: per block, live-in columns by decreasing size, then the
+    # u32 input index; each segment padded to 8 bytes per entry
+    layout = []
+    row_total = 0
+    for b in range(nb):
+        cols = sorted(live_in[b], key=lambda r: (-L.regs[r].nbytes, r))
+        off = row_total
+        placed = []
+        for r in cols:
+            placed.append((r, off))
+            off += L.regs[r].nbytes
+        tid_off = off
+        off += 4
+        off = (off + 7) // 8 * 8
+        layout.append({"cols": placed, "tid": tid_off})
+        row_total = off
 
     o: List[str] = []
     w = o.append
@@ -296,18 +313,42 @@ def generate(k: Kernel) -> str:
     w("    };")
     w("")
     # ---- inputs / outputs
+    w("    struct In")
+    w("    {")
+    for i, (reg, t, vname) in enumerate(k.inputs):
+        w(f"        {CTYPE[t]} v{i}; // {vname}")
+    if not k.inputs:
+        w("        int unused;")
+    w("    };")
+    w("")
+    w("    // Reads the input columns of thread `tid` (a NULL column is iota).")
     w("    __device__ __forceinline__ static void")
-    w("    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)")
+    w("    load_in(In& in, const Columns& c, const unsigned long long tid)")
+    w("    {")
+    for i, (reg, t, vname) in enumerate(k.inputs):
+        ct = CTYPE[t]
+        w(f"        {{ const {ct}* col = static_cast<const {ct}*>(c.p[{i}]);")
+        w(f"          in.v{i} = col ? col[tid] : static_cast<{ct}>(tid); }}")
+    w("        (void)in; (void)c; (void)tid;")
+    w("    }")
+    w("")
+    w("    // Loom's set_inputs: input variables written, every other register zero.")
+    w("    __device__ __forceinline__ static void")
+    w("    start(Regs& R, const In& in)")
     w("    {")
     for r in regs:
         w(f"        R.r{r.idx} = 0;")
     for i, (reg, t, vname) in enumerate(k.inputs):
-        ct = CTYPE[t]
-        w(f"        {{ // input {vname}")
-        w(f"            const {ct}* col = static_cast<const {ct}*>(c.p[{i}]);")
-        w(f"            const {ct} v = col ? col[tid] : static_cast<{ct}>(tid);")
-        w("            " + L.write(Operand(type=t, reg=reg), "v"))
-        w("        }")
+        w("        " + L.write(Operand(type=t, reg=reg), f"in.v{i}"))
+    w("        (void)in;")
+    w("    }")
+    w("")
+    w("    __device__ __forceinline__ static void")
+    w("    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)")
+    w("    {")
+    w("        In in;")
+    w("        load_in(in, c, tid);")
+    w("        start(R, in);")
     w("    }")
     w("")
     w("    __device__ __forceinline__ static void")
@@ -321,59 +362,66 @@ def generate(k: Kernel) -> str:
     w("    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }")
     w("    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }")
     w("")
-    # ---- exec (one block)
+    # ---- run_burst (goto CFG entered at any block, bounded by a budget)
+    w("    // Runs the lane's own path from block `entry` for at most `budget`")
+    w("    // blocks (with kStop: also stopping on arrival at block `stop`);")
+    w("    // returns the block it stopped at, or kHalt.")
+    w("    template <bool kProf, bool kStop = false>")
     w("    __device__ __forceinline__ static int")
-    w("    exec(const int b, Regs& R, Ctx& ctx)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)")
     w("    {")
     w("        (void)ctx;")
-    w("        switch(b)")
+    w("        (void)stop;")
+    w("        switch(entry)")
     w("        {")
     for blk in k.blocks:
-        w(f"        case {blk.idx}: // {blk.label}")
-        w("        {")
-        o.extend(L.body(blk.instrs, "            "))
-        w(f"            return {L.next_expr(blk)};")
-        w("        }")
+        w(f"        case {blk.idx}: goto L_B{blk.idx};")
     w("        default: return kHalt;")
     w("        }")
-    w("    }")
-    w("")
-    # ---- run (goto CFG)
-    w("    template <bool kProf>")
-    w("    __device__ __forceinline__ static void")
-    w("    run(Regs& R, Ctx& ctx)")
-    w("    {")
     for blk in k.blocks:
         w(f"    L_B{blk.idx}: // {blk.label}")
-        w("        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }")
+        w(f"        if(budget == 0u || (kStop && stop == {blk.idx})) return {blk.idx};")
+        w("        --budget;")
         w(f"        if constexpr(kProf) count_block(ctx, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
         o.extend(L.goto_transfer(blk, "        "))
     w("    L_HALT:")
-    w("        return;")
+    w("        return kHalt;")
     w("    }")
     w("")
-    # ---- save / restore
-    for fn, const in (("save", "const "), ("restore", "")):
-        w("    __device__ __forceinline__ static void")
-        w(f"    {fn}(const int b, {const}Regs& R, const Columns& c, const unsigned slot)")
+    # ---- save / restore: queue (parity, block) holds the block's live-in
+    # registers and the input index, one SoA column each
+    w(f"    static constexpr unsigned long long kRowBytes = {row_total}ull;")
+    for fn in ("save", "restore"):
+        w("    __device__ __forceinline__ static " + ("void" if fn == "save" else "unsigned"))
+        if fn == "save":
+            w("    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,")
+            w("         const unsigned idx, const unsigned tid)")
+        else:
+            w("    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,")
+            w("            const unsigned idx)")
         w("    {")
+        q = "" if fn == "save" else "const "
+        w(f"        {q}char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;")
         w("        switch(b)")
         w("        {")
         for blk in k.blocks:
-            li = sorted(live_in[blk.idx])
-            if not li:
-                continue
-            w(f"        case {blk.idx}:")
-            for r in li:
-                st = CTYPE[L.regs[r].storage]
-                col = f"static_cast<{st}*>(c.p[{scol[r]}])[slot]"
+            b = blk.idx
+            w(f"        case {b}:")
+            for r, off in layout[b]["cols"]:
+                stt = CTYPE[L.regs[r].storage]
+                col = f"reinterpret_cast<{q}{stt}*>(base + {off}ull * cap)[idx]"
                 if fn == "save":
                     w(f"            {col} = R.r{r};")
                 else:
                     w(f"            R.r{r} = {col};")
-            w("            break;")
-        w("        default: break;")
+            tcol = f"reinterpret_cast<{q}unsigned*>(base + {layout[b]['tid']}ull * cap)[idx]"
+            if fn == "save":
+                w(f"            {tcol} = tid;")
+                w("            return;")
+            else:
+                w(f"            return {tcol};")
+        w("        default: " + ("return;" if fn == "save" else "return 0xffffffffu;"))
         w("        }")
         w("    }")
         w("")
@@ -384,7 +432,6 @@ def generate(k: Kernel) -> str:
     w("const int kOutTypes[] = {" + ", ".join(ABI_TYPE[t] for _, t, _ in k.outputs) + "};")
     w("const char* const kInNames[] = {" + ", ".join(f'"{n}"' for _, _, n in k.inputs) + "};")
     w("const char* const kOutNames[] = {" + ", ".join(f'"{n}"' for _, _, n in k.outputs) + "};")
-    w("const int kStateTypes[] = {" + ", ".join(["0"] + [ABI_TYPE[L.regs[r].storage] for r in state]) + "};")
     w(f"const uint32_t kInstrs[] = {{{', '.join(map(str, counts))}}};")
     w(f"const uint32_t kLive[] = {{{', '.join(map(str, live_bytes))}}};")
     state_size = sum(r.nbytes for r in k.regs)
@@ -409,20 +456,22 @@ def generate(k: Kernel) -> str:
     w("cudaError_t launch_regroup(const RegroupLaunch& a)")
     w("{")
     w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
-    w("    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),")
-    w("                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);")
+    w("    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)")
+    w("                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);")
+    w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
     w("}")
     w("")
-    w("cudaError_t regroup_occupancy(int block, int* ctas)")
+    w("cudaError_t regroup_occupancy(int block, bool profile, int* ctas)")
     w("{")
-    w("    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);")
+    w("    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)")
+    w("                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);")
     w("}")
     w("")
     w(f"}} }} // namespace loom_b200::k_{name}")
     w("")
     w(f"extern const loom_b200::KernelEntry loom_b200_entry_{name};")
     w(f"const loom_b200::KernelEntry loom_b200_entry_{name} = {{")
-    w(f"    &loom_b200::k_{name}::kInfo, {len(state)}, loom_b200::k_{name}::kStateTypes + 1,")
+    w(f"    &loom_b200::k_{name}::kInfo, loom_b200::k_{name}::K::kRowBytes,")
     w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
     w(f"    &loom_b200::k_{name}::regroup_occupancy}};")
     return "\n".join(o) + "\n"

@@ -35,12 +35,9 @@ enum : unsigned
     kStatusBarrierTimeout = LOOM_B200_STATUS_BARRIER_TIMEOUT,
 };
 
-/// Per-thread execution context: step guard, instruction counters and the
-/// status word.
+/// Per-thread execution context: instruction counters and the status word.
 struct Ctx
 {
-    unsigned long long steps;
-    unsigned long long max_steps;
     unsigned long long thread_instr;
     unsigned long long warp_instr;
     unsigned*          status;
@@ -120,6 +117,18 @@ lanemask_lt()
     unsigned m;
     asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+/// Counting hook at every block entry of K::run_burst<true>: the lowest
+/// active lane adds the block's instruction count once for the warp, every
+/// lane adds it for itself (lane efficiency = thread / (32 * warp)).
+__device__ __forceinline__ void
+count_block(Ctx& ctx, const unsigned n_instr)
+{
+    const unsigned active = __activemask();
+    if((threadIdx.x & 31) == static_cast<unsigned>(__ffs(active) - 1))
+        ctx.warp_instr += n_instr;
+    ctx.thread_instr += n_instr;
 }
 
 /// Block-wide sum of three counters into global memory, one atomic per warp.

@@ -1,6 +1,6 @@
 // Plain drop-in engine: one CUDA thread per Loom thread, in input order.
 //
-// The generated K::run<> lowers the kernel's basic blocks to a goto CFG
+// The generated K::run_burst<> lowers the kernel's basic blocks to a goto CFG
 // inside one function, so divergence and reconvergence are the hardware's
 // (Blackwell independent thread scheduling).  This replaces Loom's test-only
 // CUDA backend (src/vm/cuda.hpp:1329-1579), which launched one kernel per
@@ -25,25 +25,22 @@ plain_kernel(const Columns                  cols,
 {
     const unsigned long long tid =
         static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    Ctx ctx{0ull, max_steps, 0ull, 0ull, status};
+    Ctx ctx{0ull, 0ull, status};
     if(tid < n)
     {
         typename K::Regs R;
         K::load_inputs(R, cols, tid);
-        K::template run<kProf>(R, ctx);
+        // the block budget is the step guard: a thread that has not halted
+        // when it runs out is stopped and flagged
+        const unsigned budget = max_steps < 0xffffffffull
+                                    ? static_cast<unsigned>(max_steps)
+                                    : 0xffffffffu;
+        if(K::template run_burst<kProf>(0, R, ctx, budget) != kHalt)
+            ctx.flag(kStatusStepLimit);
         K::store_outputs(R, cols, tid);
     }
     if constexpr(kProf)
         flush_counters(counters, ctx.thread_instr, ctx.warp_instr, 0ull);
 }
 
-/// Counting hook called at every block entry of K::run<true>.
-__device__ __forceinline__ void
-count_block(Ctx& ctx, const unsigned n_instr)
-{
-    const unsigned active = __activemask();
-    if((threadIdx.x & 31) == static_cast<unsigned>(__ffs(active) - 1))
-        ctx.warp_instr += n_instr;
-    ctx.thread_instr += n_instr;
-}
 } // namespace loom_b200

@@ -7,22 +7,32 @@
 // every row by PC (2669-2745) and exchanges halted rows for new inputs
 // (bve.hpp:1208-1229).  The same method, laid out for Blackwell:
 //
-//  * state file: one SoA column per register that is live at some block
-//    entry, indexed by slot; a parked thread stores only the live-in set of
-//    the block it waits at;
-//  * per-basic-block work queues of slot ids, double-buffered by round
-//    (q[round & 1][block][...]); warps pop 32-entry tiles, so every tile
-//    starts with all lanes at one PC;
-//  * in registers, a warp keeps executing the block that the largest
-//    same-PC lane group stands at (__match_any_sync + __reduce_max_sync)
-//    while that group has >= utr lanes and fewer than `period` steps ran;
-//  * a halted lane writes its outputs and takes the next input in place
-//    (warp-aggregated atomicAdd on the input cursor): the exchange step;
-//  * at the end of a tile, lanes are grouped by PC (__match_any_sync), one
-//    atomicAdd per group reserves queue space, lanes write their slot ids at
-//    base + rank and their live registers to the state file;
+//  * per-basic-block work queues that carry the thread state itself: queue
+//    (parity, b) is an SoA segment holding, for each waiting thread, the
+//    registers live at the entry of block b plus its input index.  Parking a
+//    lane group appends contiguous entries (one atomicAdd per group, lanes
+//    at base + rank); a tile is 32 consecutive entries, so restores are
+//    coalesced loads and every tile starts with all lanes at one PC.  The
+//    queues are double-buffered by round parity; the counting sort of the
+//    hybrid backend becomes these warp-aggregated appends;
+//  * in registers, a warp keeps running the block that the largest same-PC
+//    lane group stands at while that group has >= utr lanes and fewer than
+//    `period` block steps ran.  A step is a burst of up to `burst` blocks
+//    along each lane's own path (hardware reconvergence inside the burst),
+//    so the vote costs one ballot per burst; only when the majority block
+//    loses its quorum does the warp vote again with __match_any_sync and
+//    __reduce_max_sync.  Lanes behind the majority block may first run up to
+//    `catchup` blocks to reach it;
+//  * exchange: a halted lane writes its outputs and continues with a new
+//    input that it prefetched into registers earlier (one warp-aggregated
+//    atomicAdd on the input cursor per claim), so the input load latency is
+//    hidden behind the burst;
+//  * admission: the input cursor runs against a per-round admission limit
+//    that keeps the threads in flight (in lanes or parked) within the
+//    population, which bounds every queue;
 //  * rounds are separated by a grid barrier whose wait is bounded; the last
-//    CTA to arrive resets the queue counters and decides termination.
+//    CTA to arrive resets the queue counters, computes the next admission
+//    limit and decides termination.
 // Pure kernels make any execution order valid, so regrouping never changes
 // a thread's result (Loom README.md:103-107).
 #pragma once
@@ -37,17 +47,16 @@ struct RegroupCtl
     unsigned           bar_gen;
     unsigned           done;
     unsigned           pad0;
-    unsigned long long init_head;    // round-0 admission cursor
-    unsigned long long input_cursor; // next input for in-place exchange
+    unsigned long long cursor;    // next input index to admit
+    unsigned long long admit_end; // inputs below this index may enter this round
 };
 
 struct RegroupParams
 {
-    Columns             cols;
-    unsigned*           q;      // [2][num_blocks][cap] slot ids
-    unsigned*           qcnt;   // [2][num_blocks]
-    unsigned*           qhead;  // [num_blocks] pop cursors of the current round
-    unsigned*           tidcol; // [cap] input index of the thread in a slot
+    Columns             cols;     // inputs then outputs
+    char*               state;    // queues with their state: [2][K::kRowBytes * cap]
+    unsigned*           qcnt;     // [2][num_blocks] entries per queue
+    unsigned*           qhead;    // [num_blocks] pop cursors of the current round
     RegroupCtl*         ctl;
     unsigned*           status;
     // accumulated over launches: 0 thread_instr, 1 warp_instr, 2 parks,
@@ -56,10 +65,13 @@ struct RegroupParams
     unsigned long long  n;
     unsigned long long  max_rounds;
     unsigned long long  barrier_spins;
-    unsigned            cap;
-    unsigned            utr;
-    unsigned            period;
-    unsigned            refill;
+    unsigned            cap;      // population: entries per queue, multiple of 32
+    unsigned            utr;      // majority quorum, lanes
+    unsigned            period;   // block steps per tile per round
+    unsigned            burst;    // blocks a lane runs between two votes
+    unsigned            spread;   // majority size from which all live lanes run
+    unsigned            catchup;  // blocks a lane behind the majority may run to reach it
+    unsigned            prefetch; // prefetch the next input of every lane
     unsigned            phantoms; // fault injection: CTAs the barrier waits for in vain
 };
 
@@ -76,8 +88,11 @@ ld_volatile64(const unsigned long long* p)
 }
 
 /// Grid barrier with a bounded wait.  The last CTA to arrive runs `last`
-/// before releasing the others.  Returns false when the wait ran out (the
-/// status word then carries kStatusBarrierTimeout and ctl->done is set).
+/// before releasing the others.  Returns whether the CTA should run another
+/// round: false when the launch is done or when the wait ran out (the status
+/// word then carries kStatusBarrierTimeout and ctl->done is set).  The value
+/// is decided by thread 0 and shared, so every thread of the CTA leaves the
+/// round loop together.
 template <typename F>
 __device__ bool
 grid_barrier(RegroupCtl*        ctl,
@@ -90,7 +105,7 @@ grid_barrier(RegroupCtl*        ctl,
     __syncthreads();
     if(threadIdx.x == 0)
     {
-        ok = 1;
+        int            go  = 1;
         const unsigned gen = ld_volatile(&ctl->bar_gen);
         __threadfence();
         const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
@@ -106,23 +121,43 @@ grid_barrier(RegroupCtl*        ctl,
             unsigned long long i = 0;
             while(ld_volatile(&ctl->bar_gen) == gen)
             {
-                __nanosleep(200);
+                __nanosleep(100);
                 if(++i > spins)
                 {
                     atomicOr(status, kStatusBarrierTimeout);
                     *reinterpret_cast<volatile unsigned*>(&ctl->done) = 1u;
-                    ok = 0;
+                    go = 0;
                     break;
                 }
             }
             __threadfence();
         }
+        if(ld_volatile(&ctl->done) != 0u) go = 0;
+        ok = go;
     }
     __syncthreads();
     return ok != 0;
 }
 
-template <typename K>
+/// Claims input indices for the lanes in `need` with one atomicAdd for the
+/// warp.  Returns this lane's index, or ~0 when the lane got none; `dry`
+/// turns true once the round's admission limit is reached.
+__device__ __forceinline__ unsigned long long
+claim_inputs(const unsigned need, RegroupCtl* ctl, unsigned long long admit_end, bool& dry)
+{
+    constexpr unsigned FULL   = 0xffffffffu;
+    const unsigned     lane   = threadIdx.x & 31u;
+    const int          leader = __ffs(need) - 1;
+    unsigned long long base   = 0;
+    if(static_cast<int>(lane) == leader)
+        base = atomicAdd(&ctl->cursor, static_cast<unsigned long long>(__popc(need)));
+    base = __shfl_sync(FULL, base, leader);
+    if(base + __popc(need) >= admit_end) dry = true;
+    const unsigned long long t = base + __popc(need & lanemask_lt());
+    return ((need >> lane) & 1u) && t < admit_end ? t : ~0ull;
+}
+
+template <typename K, bool kProf>
 __global__ void
 regroup_kernel(const RegroupParams p)
 {
@@ -131,108 +166,113 @@ regroup_kernel(const RegroupParams p)
 
     const unsigned lane  = threadIdx.x & 31u;
     const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned long long n_init =
-        p.n < static_cast<unsigned long long>(p.cap) ? p.n : p.cap;
 
-    Ctx ctx{0ull, ~0ull, 0ull, 0ull, p.status};
+    Ctx ctx{0ull, 0ull, p.status};
     unsigned long long parks = 0, sbytes = 0, finished = 0;
     typename K::Regs   R;
+    typename K::In     pf; // prefetched next input of this lane
+    unsigned long long pf_tid = ~0ull;
 
     for(unsigned round = 0;; ++round)
     {
-        const unsigned cur = round & 1u, nxt = cur ^ 1u;
-        unsigned       bsel = gwarp % B;
+        const unsigned           cur = round & 1u, nxt = cur ^ 1u;
+        const unsigned long long admit_end = ld_volatile64(&p.ctl->admit_end);
+        unsigned                 bsel = gwarp % B;
+        bool                     dry  = false; // no more admissions this round
 
         for(;;)
         {
             // ------------------------------------------------ take a tile
-            int                tb = kEmpty;
-            unsigned           tk = 0;
-            unsigned long long toff = 0;
+            // parked threads first (work conserving), then fresh inputs
+            int      tb = kEmpty;
+            unsigned tk = 0, toff = 0;
             if(lane == 0)
             {
-                if(round == 0 && ld_volatile64(&p.ctl->init_head) < n_init)
+                for(int i = 0; i < B; ++i)
                 {
-                    const unsigned long long off =
-                        atomicAdd(&p.ctl->init_head, 32ull);
-                    if(off < n_init)
+                    const unsigned b = (bsel + i) % B;
+                    unsigned cnt     = ld_volatile(&p.qcnt[cur * B + b]);
+                    if(cnt > p.cap) cnt = p.cap; // an overrun was flagged
+                    if(ld_volatile(&p.qhead[b]) >= cnt) continue;
+                    const unsigned off = atomicAdd(&p.qhead[b], 32u);
+                    if(off < cnt)
                     {
-                        tb   = kHalt; // marks a fresh-input tile
+                        tb   = static_cast<int>(b);
                         toff = off;
-                        tk   = static_cast<unsigned>(
-                            n_init - off < 32ull ? n_init - off : 32ull);
+                        tk   = cnt - off < 32u ? cnt - off : 32u;
+                        bsel = b;
+                        break;
                     }
                 }
-                if(tb == kEmpty)
-                    for(int i = 0; i < B; ++i)
-                    {
-                        const unsigned b   = (bsel + i) % B;
-                        const unsigned cnt = ld_volatile(&p.qcnt[cur * B + b]);
-                        if(ld_volatile(&p.qhead[b]) >= cnt) continue;
-                        const unsigned off = atomicAdd(&p.qhead[b], 32u);
-                        if(off < cnt)
-                        {
-                            tb   = static_cast<int>(b);
-                            toff = off;
-                            tk   = cnt - off < 32u ? cnt - off : 32u;
-                            bsel = b;
-                            break;
-                        }
-                    }
             }
             tb   = __shfl_sync(FULL, tb, 0);
             tk   = __shfl_sync(FULL, tk, 0);
             toff = __shfl_sync(FULL, toff, 0);
-            if(tb == kEmpty) break;
 
-            int                pc   = kEmpty;
-            unsigned           slot = 0;
-            unsigned long long tid  = 0;
-            if(lane < tk)
+            int                pc  = kEmpty;
+            unsigned long long tid = 0;
+            if(tb >= 0)
             {
-                if(tb == kHalt)
+                if(lane < tk)
                 {
-                    slot = static_cast<unsigned>(toff) + lane;
-                    tid  = toff + lane;
-                    K::load_inputs(R, p.cols, tid);
-                    pc = 0;
+                    tid = K::restore(tb, R, p.state, p.cap, cur, toff + lane);
+                    if(tid < p.n)
+                    {
+                        pc = tb;
+                        sbytes += K::live_bytes(tb) + 4u;
+                    }
+                    else
+                        ctx.flag(kStatusQueueOverrun);
                 }
-                else
+            }
+            else
+            {
+                if(dry) break;
+                const unsigned long long t = claim_inputs(FULL, p.ctl, admit_end, dry);
+                if(__ballot_sync(FULL, t != ~0ull) == 0u) break;
+                if(t != ~0ull)
                 {
-                    const unsigned long long qi =
-                        (static_cast<unsigned long long>(cur) * B + tb) * p.cap +
-                        toff + lane;
-                    slot = p.q[qi];
-                    tid  = p.tidcol[slot];
-                    K::restore(tb, R, p.cols, slot);
-                    sbytes += K::live_bytes(tb) + 8u;
-                    pc = tb;
+                    typename K::In in;
+                    K::load_in(in, p.cols, t);
+                    K::start(R, in);
+                    tid = t;
+                    pc  = 0;
                 }
+                tb = 0;
+                tk = 32u;
             }
 
             // ------------------------------------------------ run
-            for(unsigned step = 0;; ++step)
+            int      m     = tb;
+            unsigned mc    = tk;
+            unsigned steps = 0;
+            for(;;)
             {
-                const unsigned live = __ballot_sync(FULL, pc >= 0);
-                if(live == 0u) break;
-                const unsigned peers = __match_any_sync(FULL, pc);
-                const unsigned key =
-                    pc >= 0 ? ((static_cast<unsigned>(__popc(peers)) << 16) |
-                               static_cast<unsigned>(pc))
-                            : 0u;
-                const unsigned best = __reduce_max_sync(FULL, key);
-                const int      m    = static_cast<int>(best & 0xffffu);
-                const unsigned mc   = best >> 16;
-                if(step > 0 && (mc < p.utr || step >= p.period)) break;
-
-                const unsigned ni = K::instr(m);
-                if(lane == 0) ctx.warp_instr += ni;
-                if(pc == m)
+                // prefetch the next input of every lane that has none
+                if(p.prefetch && !dry)
                 {
-                    ctx.thread_instr += ni;
-                    pc = K::exec(m, R, ctx);
+                    const unsigned need = __ballot_sync(FULL, pf_tid == ~0ull);
+                    if(need)
+                    {
+                        const unsigned long long t = claim_inputs(need, p.ctl, admit_end, dry);
+                        if(t != ~0ull)
+                        {
+                            pf_tid = t;
+                            K::load_in(pf, p.cols, t);
+                        }
+                    }
                 }
+                // catch-up: lanes behind the majority block (for instance
+                // lanes that just started at block 0) run toward it, so the
+                // burst starts with the warp converged at m
+                if(p.catchup && pc >= 0 && pc != m)
+                    pc = K::template run_burst<kProf, true>(pc, R, ctx, p.catchup, m);
+                if(pc >= 0 && (mc >= p.spread || pc == m))
+                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst);
+                steps += p.burst;
 
+                // exchange: halted lanes write their outputs and continue
+                // with a prefetched input, or claim one now
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
                 {
@@ -240,77 +280,115 @@ regroup_kernel(const RegroupParams p)
                     {
                         K::store_outputs(R, p.cols, tid);
                         ++finished;
-                    }
-                    if(p.refill)
-                    {
-                        const int          leader = __ffs(hm) - 1;
-                        unsigned long long base   = 0;
-                        if(static_cast<int>(lane) == leader)
-                            base = atomicAdd(&p.ctl->input_cursor,
-                                             static_cast<unsigned long long>(
-                                                 __popc(hm)));
-                        base = __shfl_sync(FULL, base, leader);
-                        if(pc == kHalt)
+                        pc = kEmpty;
+                        if(pf_tid != ~0ull)
                         {
-                            const unsigned long long t =
-                                base + __popc(hm & lanemask_lt());
-                            if(t < p.n)
-                            {
-                                tid = t;
-                                K::load_inputs(R, p.cols, t);
-                                pc = 0;
-                            }
-                            else
-                                pc = kEmpty;
+                            K::start(R, pf);
+                            tid    = pf_tid;
+                            pf_tid = ~0ull;
+                            pc     = 0;
                         }
                     }
-                    else if(pc == kHalt)
-                        pc = kEmpty;
+                    if(!dry)
+                    {
+                        const unsigned need = __ballot_sync(FULL, pc == kEmpty);
+                        if(need)
+                        {
+                            const unsigned long long t =
+                                claim_inputs(need, p.ctl, admit_end, dry);
+                            if(t != ~0ull)
+                            {
+                                typename K::In in;
+                                K::load_in(in, p.cols, t);
+                                K::start(R, in);
+                                tid = t;
+                                pc  = 0;
+                            }
+                        }
+                    }
                 }
+
+                if(steps >= p.period) break;
+                const unsigned cm = __popc(__ballot_sync(FULL, pc == m));
+                if(cm >= p.utr)
+                {
+                    mc = cm;
+                    continue;
+                }
+                const unsigned peers = __match_any_sync(FULL, pc);
+                const unsigned key =
+                    pc >= 0 ? ((static_cast<unsigned>(__popc(peers)) << 16) |
+                               static_cast<unsigned>(pc))
+                            : 0u;
+                const unsigned best = __reduce_max_sync(FULL, key);
+                if(best == 0u) break; // no live lane left
+                m  = static_cast<int>(best & 0xffffu);
+                mc = best >> 16;
+                if(mc < p.utr) break;
             }
 
             // ------------------------------------------------ park
-            const unsigned live = __ballot_sync(FULL, pc >= 0);
-            if(pc >= 0)
+            // live threads wait in the queue of their block; a prefetched
+            // input that never started waits in the queue of block 0
+            for(int pass = 0; pass < 2; ++pass)
             {
-                const unsigned peers  = __match_any_sync(live, pc);
-                const int      leader = __ffs(peers) - 1;
-                unsigned       base   = 0;
-                if(static_cast<int>(lane) == leader)
-                    base = atomicAdd(&p.qcnt[nxt * B + pc],
-                                     static_cast<unsigned>(__popc(peers)));
-                base = __shfl_sync(peers, base, leader);
-                const unsigned idx = base + __popc(peers & lanemask_lt());
-                if(idx < p.cap && slot < p.cap)
+                if(pass == 1)
                 {
-                    p.q[(static_cast<unsigned long long>(nxt) * B + pc) * p.cap +
-                        idx]       = slot;
-                    p.tidcol[slot] = static_cast<unsigned>(tid);
-                    K::save(pc, R, p.cols, slot);
-                    sbytes += K::live_bytes(pc) + 8u;
-                    ++parks;
+                    if(__ballot_sync(FULL, pf_tid != ~0ull) == 0u) break;
+                    pc = kEmpty;
+                    if(pf_tid != ~0ull)
+                    {
+                        K::start(R, pf);
+                        tid    = pf_tid;
+                        pf_tid = ~0ull;
+                        pc     = 0;
+                    }
                 }
-                else
-                    ctx.flag(kStatusQueueOverrun);
+                const unsigned live = __ballot_sync(FULL, pc >= 0);
+                if(pc >= 0)
+                {
+                    const unsigned peers  = __match_any_sync(live, pc);
+                    const int      leader = __ffs(peers) - 1;
+                    unsigned       base   = 0;
+                    if(static_cast<int>(lane) == leader)
+                        base = atomicAdd(&p.qcnt[nxt * B + pc],
+                                         static_cast<unsigned>(__popc(peers)));
+                    base = __shfl_sync(peers, base, leader);
+                    const unsigned idx = base + __popc(peers & lanemask_lt());
+                    if(idx < p.cap)
+                    {
+                        K::save(pc, R, p.state, p.cap, nxt, idx, static_cast<unsigned>(tid));
+                        sbytes += K::live_bytes(pc) + 4u;
+                        ++parks;
+                    }
+                    else
+                        ctx.flag(kStatusQueueOverrun);
+                }
             }
         }
 
         // ---------------------------------------------------- round end
-        const bool ok = grid_barrier(
+        const bool more = grid_barrier(
             p.ctl,
             p.status,
             p.barrier_spins,
             p.phantoms,
             [&]()
             {
-                unsigned long long total = 0;
+                unsigned long long parked = 0;
                 for(int b = 0; b < B; ++b)
                 {
-                    total += ld_volatile(&p.qcnt[nxt * B + b]);
+                    parked += ld_volatile(&p.qcnt[nxt * B + b]);
                     p.qcnt[cur * B + b] = 0u;
                     p.qhead[b]          = 0u;
                 }
-                unsigned done = total == 0ull ? 1u : 0u;
+                // claims beyond the limit were refused: give them back
+                unsigned long long c = ld_volatile64(&p.ctl->cursor);
+                if(c > admit_end) c = admit_end;
+                const unsigned long long room = parked < p.cap ? p.cap - parked : 0ull;
+                p.ctl->cursor    = c;
+                p.ctl->admit_end = c + room < p.n ? c + room : p.n;
+                unsigned done    = parked == 0ull && c >= p.n ? 1u : 0u;
                 if(!done && round + 1ull >= p.max_rounds)
                 {
                     atomicOr(p.status, kStatusStepLimit);
@@ -319,7 +397,7 @@ regroup_kernel(const RegroupParams p)
                 *reinterpret_cast<volatile unsigned*>(&p.ctl->done) = done;
                 if(done) atomicAdd(p.counters + 5, round + 1ull);
             });
-        if(!ok || ld_volatile(&p.ctl->done) != 0u) break;
+        if(!more) break;
     }
 
     flush_counters(p.counters, ctx.thread_instr, ctx.warp_instr, parks);

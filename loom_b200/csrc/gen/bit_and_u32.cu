@@ -18,21 +18,40 @@ struct K
         unsigned int r1; // b: u32
     };
 
+    struct In
+    {
+        unsigned int v0; // a
+        unsigned int v1; // b
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
     __device__ __forceinline__ static void
-    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        { const unsigned int* col = static_cast<const unsigned int*>(c.p[0]);
+          in.v0 = col ? col[tid] : static_cast<unsigned int>(tid); }
+        { const unsigned int* col = static_cast<const unsigned int*>(c.p[1]);
+          in.v1 = col ? col[tid] : static_cast<unsigned int>(tid); }
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
     {
         R.r0 = 0;
         R.r1 = 0;
-        { // input a
-            const unsigned int* col = static_cast<const unsigned int*>(c.p[0]);
-            const unsigned int v = col ? col[tid] : static_cast<unsigned int>(tid);
-            R.r0 = static_cast<unsigned int>(v);
-        }
-        { // input b
-            const unsigned int* col = static_cast<const unsigned int*>(c.p[1]);
-            const unsigned int v = col ? col[tid] : static_cast<unsigned int>(tid);
-            R.r1 = static_cast<unsigned int>(v);
-        }
+        R.r0 = static_cast<unsigned int>(in.v0);
+        R.r1 = static_cast<unsigned int>(in.v1);
+        (void)in;
+    }
+
+    __device__ __forceinline__ static void
+    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    {
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
     }
 
     __device__ __forceinline__ static void
@@ -44,57 +63,59 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
 
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // blocks (with kStop: also stopping on arrival at block `stop`);
+    // returns the block it stopped at, or kHalt.
+    template <bool kProf, bool kStop = false>
     __device__ __forceinline__ static int
-    exec(const int b, Regs& R, Ctx& ctx)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
     {
         (void)ctx;
-        switch(b)
+        (void)stop;
+        switch(entry)
         {
-        case 0: // START
-        {
-            R.r0 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r0) & static_cast<unsigned int>(R.r1)));
-            return kHalt;
-        }
+        case 0: goto L_B0;
         default: return kHalt;
         }
-    }
-
-    template <bool kProf>
-    __device__ __forceinline__ static void
-    run(Regs& R, Ctx& ctx)
-    {
     L_B0: // START
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 0)) return 0;
+        --budget;
         if constexpr(kProf) count_block(ctx, 1u);
         R.r0 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r0) & static_cast<unsigned int>(R.r1)));
         goto L_HALT;
     L_HALT:
-        return;
+        return kHalt;
     }
 
+    static constexpr unsigned long long kRowBytes = 16ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, const Columns& c, const unsigned slot)
+    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
     {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            static_cast<unsigned int*>(c.p[3])[slot] = R.r0;
-            static_cast<unsigned int*>(c.p[4])[slot] = R.r1;
-            break;
-        default: break;
+            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r0;
+            reinterpret_cast<unsigned int*>(base + 4ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+            return;
+        default: return;
         }
     }
 
-    __device__ __forceinline__ static void
-    restore(const int b, Regs& R, const Columns& c, const unsigned slot)
+    __device__ __forceinline__ static unsigned
+    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
     {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            R.r0 = static_cast<unsigned int*>(c.p[3])[slot];
-            R.r1 = static_cast<unsigned int*>(c.p[4])[slot];
-            break;
-        default: break;
+            R.r0 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
+            R.r1 = reinterpret_cast<const unsigned int*>(base + 4ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        default: return 0xffffffffu;
         }
     }
 
@@ -104,7 +125,6 @@ const int kInTypes[] = {LOOM_B200_U32, LOOM_B200_U32};
 const int kOutTypes[] = {LOOM_B200_U32};
 const char* const kInNames[] = {"a", "b"};
 const char* const kOutNames[] = {"a"};
-const int kStateTypes[] = {0, LOOM_B200_U32, LOOM_B200_U32};
 const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {8};
 
@@ -128,19 +148,21 @@ cudaError_t launch_plain(const PlainLaunch& a)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),
-                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
 }
 
 } } // namespace loom_b200::k_bit_and_u32
 
 extern const loom_b200::KernelEntry loom_b200_entry_bit_and_u32;
 const loom_b200::KernelEntry loom_b200_entry_bit_and_u32 = {
-    &loom_b200::k_bit_and_u32::kInfo, 2, loom_b200::k_bit_and_u32::kStateTypes + 1,
+    &loom_b200::k_bit_and_u32::kInfo, loom_b200::k_bit_and_u32::K::kRowBytes,
     &loom_b200::k_bit_and_u32::launch_plain, &loom_b200::k_bit_and_u32::launch_regroup,
     &loom_b200::k_bit_and_u32::regroup_occupancy};

@@ -17,15 +17,35 @@ struct K
         unsigned char r0; // a: u8
     };
 
+    struct In
+    {
+        unsigned char v0; // a
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
+    __device__ __forceinline__ static void
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        { const unsigned char* col = static_cast<const unsigned char*>(c.p[0]);
+          in.v0 = col ? col[tid] : static_cast<unsigned char>(tid); }
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
+    {
+        R.r0 = 0;
+        R.r0 = static_cast<unsigned char>(in.v0);
+        (void)in;
+    }
+
     __device__ __forceinline__ static void
     load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
     {
-        R.r0 = 0;
-        { // input a
-            const unsigned char* col = static_cast<const unsigned char*>(c.p[0]);
-            const unsigned char v = col ? col[tid] : static_cast<unsigned char>(tid);
-            R.r0 = static_cast<unsigned char>(v);
-        }
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
     }
 
     __device__ __forceinline__ static void
@@ -37,55 +57,57 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
 
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // blocks (with kStop: also stopping on arrival at block `stop`);
+    // returns the block it stopped at, or kHalt.
+    template <bool kProf, bool kStop = false>
     __device__ __forceinline__ static int
-    exec(const int b, Regs& R, Ctx& ctx)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
     {
         (void)ctx;
-        switch(b)
+        (void)stop;
+        switch(entry)
         {
-        case 0: // START
-        {
-            R.r0 = static_cast<unsigned char>(static_cast<unsigned char>(~static_cast<unsigned char>(R.r0)));
-            return kHalt;
-        }
+        case 0: goto L_B0;
         default: return kHalt;
         }
-    }
-
-    template <bool kProf>
-    __device__ __forceinline__ static void
-    run(Regs& R, Ctx& ctx)
-    {
     L_B0: // START
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 0)) return 0;
+        --budget;
         if constexpr(kProf) count_block(ctx, 1u);
         R.r0 = static_cast<unsigned char>(static_cast<unsigned char>(~static_cast<unsigned char>(R.r0)));
         goto L_HALT;
     L_HALT:
-        return;
+        return kHalt;
     }
 
+    static constexpr unsigned long long kRowBytes = 8ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, const Columns& c, const unsigned slot)
+    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
     {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            static_cast<unsigned char*>(c.p[2])[slot] = R.r0;
-            break;
-        default: break;
+            reinterpret_cast<unsigned char*>(base + 0ull * cap)[idx] = R.r0;
+            reinterpret_cast<unsigned*>(base + 1ull * cap)[idx] = tid;
+            return;
+        default: return;
         }
     }
 
-    __device__ __forceinline__ static void
-    restore(const int b, Regs& R, const Columns& c, const unsigned slot)
+    __device__ __forceinline__ static unsigned
+    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
     {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            R.r0 = static_cast<unsigned char*>(c.p[2])[slot];
-            break;
-        default: break;
+            R.r0 = reinterpret_cast<const unsigned char*>(base + 0ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 1ull * cap)[idx];
+        default: return 0xffffffffu;
         }
     }
 
@@ -95,7 +117,6 @@ const int kInTypes[] = {LOOM_B200_U8};
 const int kOutTypes[] = {LOOM_B200_U8};
 const char* const kInNames[] = {"a"};
 const char* const kOutNames[] = {"a"};
-const int kStateTypes[] = {0, LOOM_B200_U8};
 const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {1};
 
@@ -119,19 +140,21 @@ cudaError_t launch_plain(const PlainLaunch& a)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),
-                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
 }
 
 } } // namespace loom_b200::k_bit_not_u8
 
 extern const loom_b200::KernelEntry loom_b200_entry_bit_not_u8;
 const loom_b200::KernelEntry loom_b200_entry_bit_not_u8 = {
-    &loom_b200::k_bit_not_u8::kInfo, 1, loom_b200::k_bit_not_u8::kStateTypes + 1,
+    &loom_b200::k_bit_not_u8::kInfo, loom_b200::k_bit_not_u8::K::kRowBytes,
     &loom_b200::k_bit_not_u8::launch_plain, &loom_b200::k_bit_not_u8::launch_regroup,
     &loom_b200::k_bit_not_u8::regroup_occupancy};

@@ -19,17 +19,37 @@ struct K
         unsigned long long r3; // c: u64
     };
 
+    struct In
+    {
+        unsigned long long v0; // a
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
     __device__ __forceinline__ static void
-    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        { const unsigned long long* col = static_cast<const unsigned long long*>(c.p[0]);
+          in.v0 = col ? col[tid] : static_cast<unsigned long long>(tid); }
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
     {
         R.r1 = 0;
         R.r2 = 0;
         R.r3 = 0;
-        { // input a
-            const unsigned long long* col = static_cast<const unsigned long long*>(c.p[0]);
-            const unsigned long long v = col ? col[tid] : static_cast<unsigned long long>(tid);
-            R.r1 = static_cast<unsigned long long>(v);
-        }
+        R.r1 = static_cast<unsigned long long>(in.v0);
+        (void)in;
+    }
+
+    __device__ __forceinline__ static void
+    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    {
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
     }
 
     __device__ __forceinline__ static void
@@ -41,95 +61,90 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
 
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // blocks (with kStop: also stopping on arrival at block `stop`);
+    // returns the block it stopped at, or kHalt.
+    template <bool kProf, bool kStop = false>
     __device__ __forceinline__ static int
-    exec(const int b, Regs& R, Ctx& ctx)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
     {
         (void)ctx;
-        switch(b)
+        (void)stop;
+        switch(entry)
         {
-        case 0: // START
-        {
-            R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
-            R.r1 = static_cast<unsigned long long>(((R.r2) ? (((unsigned long long)0x1ull)) : (R.r1)));
-            return ((R.r2) ? kHalt : 1);
-        }
-        case 1: // cinit
-        {
-            R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
-            return 2;
-        }
-        case 2: // loop
-        {
-            R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
-            R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r3) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
-            R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r3) == static_cast<unsigned long long>(((unsigned long long)0x0ull))));
-            return ((R.r2) ? kHalt : 2);
-        }
+        case 0: goto L_B0;
+        case 1: goto L_B1;
+        case 2: goto L_B2;
         default: return kHalt;
         }
-    }
-
-    template <bool kProf>
-    __device__ __forceinline__ static void
-    run(Regs& R, Ctx& ctx)
-    {
     L_B0: // START
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 0)) return 0;
+        --budget;
         if constexpr(kProf) count_block(ctx, 3u);
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r1 = static_cast<unsigned long long>(((R.r2) ? (((unsigned long long)0x1ull)) : (R.r1)));
         if(R.r2) goto L_HALT; else goto L_B1;
     L_B1: // cinit
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 1)) return 1;
+        --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         goto L_B2;
     L_B2: // loop
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 2)) return 2;
+        --budget;
         if constexpr(kProf) count_block(ctx, 4u);
         R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r3) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r3) == static_cast<unsigned long long>(((unsigned long long)0x0ull))));
         if(R.r2) goto L_HALT; else goto L_B2;
     L_HALT:
-        return;
+        return kHalt;
     }
 
+    static constexpr unsigned long long kRowBytes = 56ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, const Columns& c, const unsigned slot)
+    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
     {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            static_cast<unsigned long long*>(c.p[2])[slot] = R.r1;
-            break;
+            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+            return;
         case 1:
-            static_cast<unsigned long long*>(c.p[2])[slot] = R.r1;
-            break;
+            reinterpret_cast<unsigned long long*>(base + 16ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+            return;
         case 2:
-            static_cast<unsigned long long*>(c.p[2])[slot] = R.r1;
-            static_cast<unsigned long long*>(c.p[3])[slot] = R.r3;
-            break;
-        default: break;
+            reinterpret_cast<unsigned long long*>(base + 32ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned long long*>(base + 40ull * cap)[idx] = R.r3;
+            reinterpret_cast<unsigned*>(base + 48ull * cap)[idx] = tid;
+            return;
+        default: return;
         }
     }
 
-    __device__ __forceinline__ static void
-    restore(const int b, Regs& R, const Columns& c, const unsigned slot)
+    __device__ __forceinline__ static unsigned
+    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
     {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            R.r1 = static_cast<unsigned long long*>(c.p[2])[slot];
-            break;
+            R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
         case 1:
-            R.r1 = static_cast<unsigned long long*>(c.p[2])[slot];
-            break;
+            R.r1 = reinterpret_cast<const unsigned long long*>(base + 16ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
         case 2:
-            R.r1 = static_cast<unsigned long long*>(c.p[2])[slot];
-            R.r3 = static_cast<unsigned long long*>(c.p[3])[slot];
-            break;
-        default: break;
+            R.r1 = reinterpret_cast<const unsigned long long*>(base + 32ull * cap)[idx];
+            R.r3 = reinterpret_cast<const unsigned long long*>(base + 40ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 48ull * cap)[idx];
+        default: return 0xffffffffu;
         }
     }
 
@@ -139,7 +154,6 @@ const int kInTypes[] = {LOOM_B200_U64};
 const int kOutTypes[] = {LOOM_B200_U64};
 const char* const kInNames[] = {"a"};
 const char* const kOutNames[] = {"a"};
-const int kStateTypes[] = {0, LOOM_B200_U64, LOOM_B200_U64};
 const uint32_t kInstrs[] = {3, 2, 4};
 const uint32_t kLive[] = {8, 8, 16};
 
@@ -163,19 +177,21 @@ cudaError_t launch_plain(const PlainLaunch& a)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),
-                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
 }
 
 } } // namespace loom_b200::k_fac_u64
 
 extern const loom_b200::KernelEntry loom_b200_entry_fac_u64;
 const loom_b200::KernelEntry loom_b200_entry_fac_u64 = {
-    &loom_b200::k_fac_u64::kInfo, 2, loom_b200::k_fac_u64::kStateTypes + 1,
+    &loom_b200::k_fac_u64::kInfo, loom_b200::k_fac_u64::K::kRowBytes,
     &loom_b200::k_fac_u64::launch_plain, &loom_b200::k_fac_u64::launch_regroup,
     &loom_b200::k_fac_u64::regroup_occupancy};

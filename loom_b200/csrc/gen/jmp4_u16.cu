@@ -17,15 +17,35 @@ struct K
         unsigned short r1; // i: u16
     };
 
+    struct In
+    {
+        unsigned short v0; // i
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
+    __device__ __forceinline__ static void
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        { const unsigned short* col = static_cast<const unsigned short*>(c.p[0]);
+          in.v0 = col ? col[tid] : static_cast<unsigned short>(tid); }
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
+    {
+        R.r1 = 0;
+        R.r1 = static_cast<unsigned short>(in.v0);
+        (void)in;
+    }
+
     __device__ __forceinline__ static void
     load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
     {
-        R.r1 = 0;
-        { // input i
-            const unsigned short* col = static_cast<const unsigned short*>(c.p[0]);
-            const unsigned short v = col ? col[tid] : static_cast<unsigned short>(tid);
-            R.r1 = static_cast<unsigned short>(v);
-        }
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
     }
 
     __device__ __forceinline__ static void
@@ -37,46 +57,27 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
 
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // blocks (with kStop: also stopping on arrival at block `stop`);
+    // returns the block it stopped at, or kHalt.
+    template <bool kProf, bool kStop = false>
     __device__ __forceinline__ static int
-    exec(const int b, Regs& R, Ctx& ctx)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
     {
         (void)ctx;
-        switch(b)
+        (void)stop;
+        switch(entry)
         {
-        case 0: // START
-        {
-            return ((R.r1) == 0 ? 1 : ((R.r1) == 1 ? 2 : ((R.r1) == 2 ? 3 : ((R.r1) == 3 ? 4 : kHalt))));
-        }
-        case 1: // l0
-        {
-            R.r1 = static_cast<unsigned short>(((unsigned short)0x1ull));
-            return kHalt;
-        }
-        case 2: // l1
-        {
-            R.r1 = static_cast<unsigned short>(((unsigned short)0x3ull));
-            return kHalt;
-        }
-        case 3: // l2
-        {
-            R.r1 = static_cast<unsigned short>(((unsigned short)0x7ull));
-            return kHalt;
-        }
-        case 4: // l3
-        {
-            R.r1 = static_cast<unsigned short>(((unsigned short)0xbull));
-            return kHalt;
-        }
+        case 0: goto L_B0;
+        case 1: goto L_B1;
+        case 2: goto L_B2;
+        case 3: goto L_B3;
+        case 4: goto L_B4;
         default: return kHalt;
         }
-    }
-
-    template <bool kProf>
-    __device__ __forceinline__ static void
-    run(Regs& R, Ctx& ctx)
-    {
     L_B0: // START
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 0)) return 0;
+        --budget;
         if constexpr(kProf) count_block(ctx, 1u);
         switch(R.r1) {
         case 0: goto L_B1;
@@ -86,50 +87,80 @@ struct K
         default: goto L_HALT;
         }
     L_B1: // l0
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 1)) return 1;
+        --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x1ull));
         goto L_HALT;
     L_B2: // l1
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 2)) return 2;
+        --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x3ull));
         goto L_HALT;
     L_B3: // l2
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 3)) return 3;
+        --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x7ull));
         goto L_HALT;
     L_B4: // l3
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 4)) return 4;
+        --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0xbull));
         goto L_HALT;
     L_HALT:
-        return;
+        return kHalt;
     }
 
+    static constexpr unsigned long long kRowBytes = 40ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, const Columns& c, const unsigned slot)
+    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
     {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            static_cast<unsigned short*>(c.p[2])[slot] = R.r1;
-            break;
-        default: break;
+            reinterpret_cast<unsigned short*>(base + 0ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned*>(base + 2ull * cap)[idx] = tid;
+            return;
+        case 1:
+            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+            return;
+        case 2:
+            reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
+            return;
+        case 3:
+            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+            return;
+        case 4:
+            reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = tid;
+            return;
+        default: return;
         }
     }
 
-    __device__ __forceinline__ static void
-    restore(const int b, Regs& R, const Columns& c, const unsigned slot)
+    __device__ __forceinline__ static unsigned
+    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
     {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            R.r1 = static_cast<unsigned short*>(c.p[2])[slot];
-            break;
-        default: break;
+            R.r1 = reinterpret_cast<const unsigned short*>(base + 0ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 2ull * cap)[idx];
+        case 1:
+            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        case 2:
+            return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+        case 3:
+            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        case 4:
+            return reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+        default: return 0xffffffffu;
         }
     }
 
@@ -139,7 +170,6 @@ const int kInTypes[] = {LOOM_B200_U16};
 const int kOutTypes[] = {LOOM_B200_U16};
 const char* const kInNames[] = {"i"};
 const char* const kOutNames[] = {"i"};
-const int kStateTypes[] = {0, LOOM_B200_U16};
 const uint32_t kInstrs[] = {1, 2, 2, 2, 2};
 const uint32_t kLive[] = {2, 0, 0, 0, 0};
 
@@ -163,19 +193,21 @@ cudaError_t launch_plain(const PlainLaunch& a)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),
-                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
 }
 
 } } // namespace loom_b200::k_jmp4_u16
 
 extern const loom_b200::KernelEntry loom_b200_entry_jmp4_u16;
 const loom_b200::KernelEntry loom_b200_entry_jmp4_u16 = {
-    &loom_b200::k_jmp4_u16::kInfo, 1, loom_b200::k_jmp4_u16::kStateTypes + 1,
+    &loom_b200::k_jmp4_u16::kInfo, loom_b200::k_jmp4_u16::K::kRowBytes,
     &loom_b200::k_jmp4_u16::launch_plain, &loom_b200::k_jmp4_u16::launch_regroup,
     &loom_b200::k_jmp4_u16::regroup_occupancy};

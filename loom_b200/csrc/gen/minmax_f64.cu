@@ -21,24 +21,43 @@ struct K
         double r4; // n: f64
     };
 
+    struct In
+    {
+        double v0; // a
+        double v1; // b
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
     __device__ __forceinline__ static void
-    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        { const double* col = static_cast<const double*>(c.p[0]);
+          in.v0 = col ? col[tid] : static_cast<double>(tid); }
+        { const double* col = static_cast<const double*>(c.p[1]);
+          in.v1 = col ? col[tid] : static_cast<double>(tid); }
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
     {
         R.r0 = 0;
         R.r1 = 0;
         R.r2 = 0;
         R.r3 = 0;
         R.r4 = 0;
-        { // input a
-            const double* col = static_cast<const double*>(c.p[0]);
-            const double v = col ? col[tid] : static_cast<double>(tid);
-            R.r0 = static_cast<double>(v);
-        }
-        { // input b
-            const double* col = static_cast<const double*>(c.p[1]);
-            const double v = col ? col[tid] : static_cast<double>(tid);
-            R.r1 = static_cast<double>(v);
-        }
+        R.r0 = static_cast<double>(in.v0);
+        R.r1 = static_cast<double>(in.v1);
+        (void)in;
+    }
+
+    __device__ __forceinline__ static void
+    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    {
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
     }
 
     __device__ __forceinline__ static void
@@ -50,61 +69,61 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
 
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // blocks (with kStop: also stopping on arrival at block `stop`);
+    // returns the block it stopped at, or kHalt.
+    template <bool kProf, bool kStop = false>
     __device__ __forceinline__ static int
-    exec(const int b, Regs& R, Ctx& ctx)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
     {
         (void)ctx;
-        switch(b)
+        (void)stop;
+        switch(entry)
         {
-        case 0: // START
-        {
-            R.r3 = static_cast<double>(op_max<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
-            R.r4 = static_cast<double>(op_min<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
-            R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<double>(R.r3) > static_cast<double>(R.r4)));
-            return kHalt;
-        }
+        case 0: goto L_B0;
         default: return kHalt;
         }
-    }
-
-    template <bool kProf>
-    __device__ __forceinline__ static void
-    run(Regs& R, Ctx& ctx)
-    {
     L_B0: // START
-        if(++ctx.steps > ctx.max_steps) { ctx.flag(kStatusStepLimit); return; }
+        if(budget == 0u || (kStop && stop == 0)) return 0;
+        --budget;
         if constexpr(kProf) count_block(ctx, 3u);
         R.r3 = static_cast<double>(op_max<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
         R.r4 = static_cast<double>(op_min<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<double>(R.r3) > static_cast<double>(R.r4)));
         goto L_HALT;
     L_HALT:
-        return;
+        return kHalt;
     }
 
+    static constexpr unsigned long long kRowBytes = 24ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, const Columns& c, const unsigned slot)
+    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
     {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            static_cast<double*>(c.p[3])[slot] = R.r0;
-            static_cast<double*>(c.p[4])[slot] = R.r1;
-            break;
-        default: break;
+            reinterpret_cast<double*>(base + 0ull * cap)[idx] = R.r0;
+            reinterpret_cast<double*>(base + 8ull * cap)[idx] = R.r1;
+            reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
+            return;
+        default: return;
         }
     }
 
-    __device__ __forceinline__ static void
-    restore(const int b, Regs& R, const Columns& c, const unsigned slot)
+    __device__ __forceinline__ static unsigned
+    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
     {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
         switch(b)
         {
         case 0:
-            R.r0 = static_cast<double*>(c.p[3])[slot];
-            R.r1 = static_cast<double*>(c.p[4])[slot];
-            break;
-        default: break;
+            R.r0 = reinterpret_cast<const double*>(base + 0ull * cap)[idx];
+            R.r1 = reinterpret_cast<const double*>(base + 8ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+        default: return 0xffffffffu;
         }
     }
 
@@ -114,7 +133,6 @@ const int kInTypes[] = {LOOM_B200_F64, LOOM_B200_F64};
 const int kOutTypes[] = {LOOM_B200_U64};
 const char* const kInNames[] = {"a", "b"};
 const char* const kOutNames[] = {"r"};
-const int kStateTypes[] = {0, LOOM_B200_F64, LOOM_B200_F64};
 const uint32_t kInstrs[] = {3};
 const uint32_t kLive[] = {16};
 
@@ -138,19 +156,21 @@ cudaError_t launch_plain(const PlainLaunch& a)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(&regroup_kernel<K>),
-                                       dim3(a.grid), dim3(a.block), args, 0, a.stream);
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K>, block, 0);
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
 }
 
 } } // namespace loom_b200::k_minmax_f64
 
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f64;
 const loom_b200::KernelEntry loom_b200_entry_minmax_f64 = {
-    &loom_b200::k_minmax_f64::kInfo, 2, loom_b200::k_minmax_f64::kStateTypes + 1,
+    &loom_b200::k_minmax_f64::kInfo, loom_b200::k_minmax_f64::K::kRowBytes,
     &loom_b200::k_minmax_f64::launch_plain, &loom_b200::k_minmax_f64::launch_regroup,
     &loom_b200::k_minmax_f64::regroup_occupancy};

@@ -62,7 +62,7 @@ regroup_reset(RegroupCtl*        ctl,
               unsigned*          qcnt,
               unsigned*          qhead,
               unsigned           num_blocks,
-              unsigned long long input_cursor)
+              unsigned long long admit_end)
 {
     for(unsigned i = threadIdx.x; i < 3 * num_blocks; i += blockDim.x)
     {
@@ -73,12 +73,12 @@ regroup_reset(RegroupCtl*        ctl,
     }
     if(threadIdx.x == 0)
     {
-        ctl->bar_count    = 0u;
-        ctl->bar_gen      = 0u;
-        ctl->done         = 0u;
-        ctl->pad0         = 0u;
-        ctl->init_head    = 0ull;
-        ctl->input_cursor = input_cursor;
+        ctl->bar_count = 0u;
+        ctl->bar_gen   = 0u;
+        ctl->done      = 0u;
+        ctl->pad0      = 0u;
+        ctl->cursor    = 0ull;
+        ctl->admit_end = admit_end;
     }
 }
 
@@ -87,7 +87,11 @@ constexpr unsigned long long kBarrierSpins       = 1ull << 25;
 constexpr unsigned           kDefaultPlainBlock  = 256;
 constexpr unsigned           kDefaultRegroupBlock = 256;
 constexpr unsigned           kDefaultUtr         = 16;
-constexpr unsigned           kDefaultPeriod      = 256;
+constexpr unsigned           kDefaultPeriod      = 1024;
+constexpr unsigned           kDefaultBurst       = 32;
+constexpr unsigned           kDefaultSpread      = 33;
+constexpr unsigned           kDefaultCatchup     = 4;
+constexpr unsigned           kNoCatchup          = 0xffffffffu;
 } // namespace
 
 struct loom_b200_handle
@@ -105,13 +109,12 @@ struct loom_b200_handle
     // device bookkeeping
     unsigned*           d_status   = nullptr;
     unsigned long long* d_counters = nullptr; // 8 counters
-    // regrouping workspace, sized for `ws_cap` slots
-    uint64_t            ws_cap = 0;
-    std::vector<void*>  d_state;
-    unsigned*           d_q     = nullptr;
+    // regrouping workspace: the queues with their state, sized for `ws_cap`
+    // entries per queue
+    uint64_t            ws_cap  = 0;
+    char*               d_state = nullptr;
     unsigned*           d_qcnt  = nullptr;
     unsigned*           d_qhead = nullptr;
-    unsigned*           d_tid   = nullptr;
     RegroupCtl*         d_ctl   = nullptr;
 
     loom_b200_stats stats{};
@@ -126,15 +129,19 @@ namespace
 void
 free_ws(loom_b200_handle* h)
 {
-    for(void* p: h->d_state) cudaFree(p);
-    h->d_state.clear();
-    cudaFree(h->d_q);
+    cudaFree(h->d_state);
     cudaFree(h->d_qcnt);
     cudaFree(h->d_qhead);
-    cudaFree(h->d_tid);
-    h->d_q = nullptr;
-    h->d_qcnt = h->d_qhead = h->d_tid = nullptr;
+    h->d_state = nullptr;
+    h->d_qcnt = h->d_qhead = nullptr;
     h->ws_cap = 0;
+}
+
+/// Population rounded up to whole tiles (keeps every queue column aligned).
+uint64_t
+round_cap(uint64_t cap)
+{
+    return (cap + 31) / 32 * 32;
 }
 
 int
@@ -144,13 +151,9 @@ ensure_ws(loom_b200_handle* h, uint64_t cap)
     free_ws(h);
     const KernelEntry& e = *h->e;
     const uint64_t     B = e.info->num_blocks;
-    h->d_state.assign(static_cast<size_t>(e.num_state), nullptr);
-    for(int i = 0; i < e.num_state; ++i)
-        LB_CUDA(cudaMalloc(&h->d_state[i], cap * type_bytes(e.state_types[i])));
-    LB_CUDA(cudaMalloc(&h->d_q, 2 * B * cap * sizeof(unsigned)));
+    LB_CUDA(cudaMalloc(&h->d_state, 2 * e.row_bytes * cap));
     LB_CUDA(cudaMalloc(&h->d_qcnt, 2 * B * sizeof(unsigned)));
     LB_CUDA(cudaMalloc(&h->d_qhead, B * sizeof(unsigned)));
-    LB_CUDA(cudaMalloc(&h->d_tid, cap * sizeof(unsigned)));
     h->ws_cap = cap;
     return LOOM_B200_OK;
 }
@@ -163,6 +166,9 @@ normalise(loom_b200_opts& o)
                                                    : kDefaultPlainBlock;
     if(o.utr_lanes == 0 || o.utr_lanes > 32) o.utr_lanes = kDefaultUtr;
     if(o.period == 0) o.period = kDefaultPeriod;
+    if(o.burst == 0) o.burst = kDefaultBurst;
+    if(o.spread_lanes == 0) o.spread_lanes = kDefaultSpread;
+    if(o.catchup == 0) o.catchup = kDefaultCatchup;
     if(o.max_steps == 0) o.max_steps = kDefaultMaxSteps;
 }
 
@@ -224,8 +230,8 @@ launch(loom_b200_handle* h,
     if(o.mode == LOOM_B200_REGROUP)
     {
         // the workspace is reallocated only between launches
-        const uint64_t pop = o.population ? std::min<uint64_t>(o.population, n) : n;
-        const uint64_t cap = o.no_refill ? n : pop;
+        const uint64_t cap =
+            round_cap(o.population ? std::min<uint64_t>(o.population, n) : n);
         if(cap > h->ws_cap)
         {
             LB_CUDA(cudaStreamSynchronize(stream));
@@ -236,11 +242,10 @@ launch(loom_b200_handle* h,
     LB_CUDA(cudaEventRecord(h->ev0, stream));
     if(o.mode == LOOM_B200_REGROUP)
     {
-        const uint64_t pop = o.population ? std::min<uint64_t>(o.population, n) : n;
-        const uint64_t cap = o.no_refill ? n : pop;
-        for(int i = 0; i < e.num_state; ++i) cols.p[c++] = h->d_state[i];
+        const uint64_t cap =
+            round_cap(o.population ? std::min<uint64_t>(o.population, n) : n);
         int ctas = 0;
-        LB_CUDA(e.regroup_occupancy(static_cast<int>(o.block_size), &ctas));
+        LB_CUDA(e.regroup_occupancy(static_cast<int>(o.block_size), o.profile != 0, &ctas));
         if(ctas <= 0)
         {
             g_last_error = "regroup kernel does not fit on an SM at this block size";
@@ -249,10 +254,9 @@ launch(loom_b200_handle* h,
         if(o.ctas_per_sm) ctas = std::min<int>(ctas, static_cast<int>(o.ctas_per_sm));
         RegroupLaunch L{};
         L.params.cols          = cols;
-        L.params.q             = h->d_q;
+        L.params.state         = h->d_state;
         L.params.qcnt          = h->d_qcnt;
         L.params.qhead         = h->d_qhead;
-        L.params.tidcol        = h->d_tid;
         L.params.ctl           = h->d_ctl;
         L.params.status        = h->d_status;
         L.params.counters      = h->d_counters;
@@ -263,9 +267,13 @@ launch(loom_b200_handle* h,
         L.params.cap           = static_cast<unsigned>(cap);
         L.params.utr           = o.utr_lanes;
         L.params.period        = o.period;
-        L.params.refill        = o.no_refill ? 0u : 1u;
+        L.params.burst         = o.burst;
+        L.params.spread        = o.spread_lanes;
+        L.params.catchup       = o.catchup == kNoCatchup ? 0u : o.catchup;
+        L.params.prefetch      = o.no_prefetch ? 0u : 1u;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = o.block_size;
+        L.profile              = o.profile != 0;
         L.stream               = stream;
         regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl,
                                              h->d_qcnt,
@@ -507,11 +515,7 @@ loom_b200_run_device(loom_b200_handle*  h,
 {
     if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
         return LOOM_B200_ERR_INVALID;
-    return launch(h,
-                  inputs,
-                  outputs,
-                  n,
-                  stream ? static_cast<cudaStream_t>(stream) : h->stream);
+    return launch(h, inputs, outputs, n, static_cast<cudaStream_t>(stream));
 }
 
 int

@@ -26,6 +26,7 @@ struct RegroupLaunch
     RegroupParams params;
     unsigned      grid;
     unsigned      block;
+    bool          profile;
     cudaStream_t  stream;
 };
 
@@ -33,11 +34,10 @@ struct RegroupLaunch
 struct KernelEntry
 {
     const loom_b200_kernel_info* info;
-    int                          num_state;   // state columns
-    const int*                   state_types; // storage type per state column
+    unsigned long long           row_bytes; // queue bytes per entry, summed over blocks
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
-    cudaError_t (*regroup_occupancy)(int block, int* ctas_per_sm);
+    cudaError_t (*regroup_occupancy)(int block, bool profile, int* ctas_per_sm);
 };
 
 extern const KernelEntry* const kRegistry[];

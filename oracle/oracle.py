@@ -226,8 +226,7 @@ def val_collatz(n: np.ndarray) -> np.ndarray:
             odd = (xl & np.uint64(1)).astype(bool)
             x[live] = np.where(odd, xl * np.uint64(3) + np.uint64(1), xl >> np.uint64(1))
             steps[live] += np.uint32(1)
-            live = x != 1
-            live &= True
+            live = x > 1
     return steps
 
 

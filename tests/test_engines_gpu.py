@@ -51,7 +51,9 @@ REGROUP_VARIANTS = [
     dict(utr_lanes=8, period=1000, block_size=1024),
     dict(population=100),
     dict(population=1000, utr_lanes=24),
-    dict(refill=False, period=5),
+    dict(prefetch=False, period=5),
+    dict(burst=1, catchup=0xFFFFFFFF, spread_lanes=33),
+    dict(burst=64, spread_lanes=1, utr_lanes=1),
     dict(ctas_per_sm=1, population=37),
 ]
 
