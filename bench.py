@@ -1,20 +1,26 @@
 """Benchmark: Loom kernels on one B200, regrouped vs plain.
 
-Workload (default): the Collatz stopping-time kernel on 2^24 threads,
-n uniform in [1, 2^32) from SplitMix64 (seed 1), u64 arithmetic, u32 output.
-A step is one launch of the regrouping engine over all 2^24 threads with the
-inputs resident in HBM (128 MiB in + 64 MiB out per step, larger than the
-126 MB L2, so no flush is needed between steps).  `value` is Loom threads
-completed per second (Msamples/s) of the regrouping engine; the plain engine
-is timed the same way beside it.  `e2e` is the same metric through the
-public API with pinned host buffers (H2D of the inputs and D2H of the outputs
-inside the timed region).
+Default workload (`--workload pt`): the FP32 sphere path tracer
+(loom_b200/kernels/sphere_pt.hpp) rendering the Cornell box of spheres at
+1024x768 with 64 samples per pixel: 50,331,648 Loom threads, one per
+pixel-sample.  A step is one launch of the regrouping engine over all of
+them.  The per-thread inputs (instance, sample index) are generated on the
+device (no input traffic); the scene is a 304-byte table; the outputs are
+three f32 columns (604 MB per step, larger than the 126 MB L2, so no flush
+is needed between steps).  `value` is Loom threads completed per second
+(Msamples/s) of the regrouping engine; the plain engine is timed the same
+way beside it.  `e2e` is the same metric through the public API with host
+buffers: the table copied in and the three output columns copied back to
+pinned host memory inside the timed region.
+
+Other workloads: `--workload collatz` (2^24 threads, n ~ U[1, 2^32)),
+`--workload fib` (2^20 threads, n ~ U{0..93}).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload collatz|fib]
+                    [--workload pt|collatz|fib]
 
 Under torchrun each rank runs the full workload on its own GPU (weak
-scaling, no data-path collective; Loom threads are independent), times with
+scaling, no data-path collective: Loom threads are independent), times with
 CUDA events and reports the max over ranks.
 """
 
@@ -22,7 +28,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import pathlib
 import statistics
@@ -35,34 +40,154 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
-WORKLOADS = {
-    "collatz": dict(
-        kernel="collatz_u64",
-        n=1 << 24,
-        desc="Collatz stopping time, 2^24 threads, n ~ U[1, 2^32) (SplitMix64 seed 1), u64 -> steps:u32",
-        lo=1,
-        hi=(1 << 32) - 1,
-        in_bytes=8,
-        out_bytes=4,
-        dtype="u64",
-    ),
-    "fib": dict(
-        kernel="fib_u64",
-        n=1 << 20,
-        desc="Fibonacci (Loom README IR), 2^20 threads, n ~ U{0..93} (SplitMix64 seed 1), u64",
-        lo=0,
-        hi=93,
-        in_bytes=8,
-        out_bytes=8,
-        dtype="u64",
-    ),
+# Regrouping options per workload, from the sweeps kept in profiles/
+TUNED = {
+    "sphere_pt_f32": dict(burst=4, utr_lanes=8, population=1 << 21, block_size=256, period=4096),
+    "collatz_u64": dict(burst=64, utr_lanes=16, block_size=512, period=65536, prefetch=False),
+    "fib_u64": dict(burst=64, utr_lanes=16, block_size=512, period=1024, prefetch=False),
 }
 
 
-def make_inputs(w):
-    from oracle import oracle as O
+# ---------------------------------------------------------------- workloads
+class Workload:
+    kernel = ""
+    desc = ""
+    dtype = ""
 
-    return O.uniform_int(1, w["n"], w["lo"], w["hi"])
+    def prepare(self, torch, device: bool = True):
+        raise NotImplementedError
+
+
+class PathTracing(Workload):
+    kernel = "sphere_pt_f32"
+    dtype = "f32"
+
+    def __init__(self, width=1024, height=768, spp=64):
+        from loom_b200 import scenes as S
+
+        self.S = S
+        self.req = S.cornell_request(width, height, spp, seed=1)
+        self.table, self.starts = S.pack([self.req])
+        self.n = self.req.threads
+        self.desc = (
+            f"sphere path tracer, Cornell box of 9 spheres (walls r=1e5, mirror, glass IOR 1.5, light), "
+            f"{width}x{height} x {spp} spp = {self.n} threads, FP32, RR from depth 5, max depth 16"
+        )
+        self.in_bytes = 0
+        self.out_bytes = 12
+
+    def inputs(self, api):
+        return [api.Broadcast(0, "u32"), api.Iota()]
+
+    def device_buffers(self, torch):
+        self.d_table = torch.from_numpy(self.table.view(np.int32)).cuda()
+        self.d_out = [torch.empty(self.n, dtype=torch.float32, device="cuda") for _ in range(3)]
+
+    def launch(self, f, api, stream):
+        f.launch_device(self.inputs(api), self.d_out, self.n, table=self.d_table, stream=stream)
+
+    def check(self, api):
+        """Bit-exact parity of a seeded sample against the C oracle."""
+        from oracle import oracle as O
+
+        got = [o.cpu().numpy() for o in self.d_out]
+        idx = np.sort(O.uniform_int(5, 256, 0, self.n - 1).astype(np.int64))
+        ins = O.expand_inputs(["instance", "local_iota"], self.n, self.starts, ["u32", "u32"])
+        want = O.Interp(self.kernel).run([a[idx] for a in ins], table=self.table)
+        return all(np.array_equal(g[idx].view(np.uint32), w.view(np.uint32)) for g, w in zip(got, want)), idx
+
+    def e2e(self, api, torch, steps, warmup, dist):
+        h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
+        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+
+        def step():
+            L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, None, self.table)
+            api.check(api.lib().loom_b200_launch_host(fe._h, api.ctypes.byref(L)))
+
+        for _ in range(warmup):
+            step()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        dt = time.perf_counter() - t0
+        got = [h.numpy() for h in h_out]
+        ok = all(np.array_equal(g, d.cpu().numpy()) for g, d in zip(got, self.d_out))
+        fe.close()
+        return dt, ok, self.table.nbytes, 3 * 4 * self.n
+
+    def cpu_inputs(self):
+        from oracle import oracle as O
+
+        return O.expand_inputs(["instance", "local_iota"], self.n, self.starts, ["u32", "u32"]), self.table
+
+
+class IntegerLoop(Workload):
+    def __init__(self, kernel, n, lo, hi, out_bytes, desc):
+        self.kernel = kernel
+        self.n = n
+        self.lo, self.hi = lo, hi
+        self.desc = desc
+        self.dtype = "u64"
+        self.in_bytes = 8
+        self.out_bytes = out_bytes
+        from oracle import oracle as O
+
+        self.x = O.uniform_int(1, n, lo, hi)
+
+    def device_buffers(self, torch):
+        self.d_in = torch.from_numpy(self.x.view(np.int64)).cuda()
+        dt = torch.int32 if self.out_bytes == 4 else torch.int64
+        self.d_out = torch.empty(self.n, dtype=dt, device="cuda")
+
+    def launch(self, f, api, stream):
+        f.run_device([self.d_in], [self.d_out], self.n, stream=stream)
+
+    def check(self, api):
+        from oracle import oracle as O
+
+        got = self.d_out.cpu().numpy().view(np.uint32 if self.out_bytes == 4 else np.uint64)
+        idx = O.uniform_int(5, 4096, 0, self.n - 1).astype(np.int64)
+        (want,) = O.Interp(self.kernel).run([self.x[idx]])
+        return bool(np.array_equal(got[idx], want)), idx
+
+    def e2e(self, api, torch, steps, warmup, dist):
+        h_in = torch.from_numpy(self.x.view(np.int64)).pin_memory()
+        h_out = torch.empty(self.n, dtype=self.d_out.dtype).pin_memory()
+        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+        for _ in range(warmup):
+            fe.run_host_ptrs([h_in], [h_out], self.n)
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fe.run_host_ptrs([h_in], [h_out], self.n)
+        dt = time.perf_counter() - t0
+        ok = bool(np.array_equal(h_out.numpy(), self.d_out.cpu().numpy()))
+        fe.close()
+        return dt, ok, self.n * self.in_bytes, self.n * self.out_bytes
+
+    def cpu_inputs(self):
+        return [self.x], None
+
+
+def make_workload(name):
+    if name == "pt":
+        return PathTracing()
+    if name == "pt_small":  # the profiling case: same scene at 256x192
+        return PathTracing(256, 192, 64)
+    if name == "collatz":
+        return IntegerLoop(
+            "collatz_u64", 1 << 24, 1, (1 << 32) - 1, 4,
+            "Collatz stopping time, 2^24 threads, n ~ U[1, 2^32) (SplitMix64 seed 1), u64 -> steps:u32",
+        )
+    if name == "fib":
+        return IntegerLoop(
+            "fib_u64", 1 << 20, 0, 93, 8,
+            "Fibonacci (Loom README IR), 2^20 threads, n ~ U{0..93} (SplitMix64 seed 1), u64",
+        )
+    raise ValueError(name)
 
 
 # ---------------------------------------------------------------- clocks
@@ -135,47 +260,56 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU arm
-def cpu_reference(w, x, target_s: float = 4.0):
-    """Loom's bse (oracle/_ref) on all host cores over a bounded sample;
-    falls back to the C restatement (single thread) where bse was not
-    built.  Returns (Msamples/s, info)."""
+def cpu_reference(w, target_s: float = 4.0):
+    """Loom's bse (oracle/_ref) on all host cores over a bounded sample of
+    the workload's threads; falls back to the C restatement (one thread)
+    where bse was not built.  Returns (Msamples/s, info)."""
     from oracle import oracle as O
 
     cores = os.cpu_count() or 1
-    name = w["kernel"]
+    ins, table = w.cpu_inputs()
+    # a seeded random subset of the workload's threads (cost per thread
+    # varies across the image; a prefix would not be representative)
+    perm = np.random.default_rng(7).permutation(w.n)
+    ins = [np.ascontiguousarray(a[perm]) for a in ins]
     if O.ref_available():
         kind = "reference"
 
         def run(m):
-            O.ref_run(name, [x[:m]], m, threads=cores)
+            O.ref_run(w.kernel, [a[:m] for a in ins], m, threads=cores, table=table)
 
         used = cores
     else:
         kind = "port"
-        it = O.Interp(name)
+        it = O.Interp(w.kernel)
 
         def run(m):
-            it.run([x[:m]])
+            it.run([a[:m] for a in ins], table=table)
 
         used = 1
-    m = 1 << 14
+    m = 1 << 12
     while True:
         t0 = time.perf_counter()
         run(m)
         dt = time.perf_counter() - t0
-        if dt > target_s / 8 or m >= len(x):
+        if dt > target_s / 8 or m >= w.n:
             break
-        m = min(len(x), m * 4)
-    m = min(len(x), max(m, int(m * target_s / max(dt, 1e-9))))
+        m = min(w.n, m * 4)
+    m = min(w.n, max(m, int(m * target_s / max(dt, 1e-9))))
     t0 = time.perf_counter()
     run(m)
     dt = time.perf_counter() - t0
     cpu = _cpu_model()
+    how = (
+        "Loom bse (vm::bse::function), g++ -O2 -mfma, one std::thread per core"
+        if kind == "reference"
+        else "C restatement of bse, one thread"
+    )
     return m / dt / 1e6, {
         "unit": "Msamples/s",
         "cores": used,
         "kind": kind,
-        "sample": f"first {m} threads of the workload ({cpu}; {'Loom bse, g++ -O2 -mfma, std::thread per core' if kind == 'reference' else 'C restatement of bse, 1 thread'})",
+        "sample": f"{m} threads drawn at random (seed 7) from the workload's {w.n}, on {cpu}; {how}",
         "seconds": round(dt, 3),
     }
 
@@ -218,35 +352,35 @@ def time_steps(fn, steps: int, warmup: int, torch, dist=None):
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="collatz", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "collatz", "fib"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
-    w = WORKLOADS[args.workload]
     warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    w = make_workload(args.workload)
     config = {
-        "workload": w["desc"],
-        "kernel": w["kernel"],
-        "threads_per_gpu": w["n"],
-        "l2": "inputs larger than L2 (no flush)" if w["n"] * w["in_bytes"] > 126e6 else "L2 flushed between steps",
+        "workload": w.desc,
+        "kernel": w.kernel,
+        "threads_per_gpu": w.n,
+        "l2": "outputs larger than L2 (no flush)",
         "parallelism": f"replicas{world}" if world > 1 else "single",
+        "regroup_options": TUNED[w.kernel],
     }
+    metric = "Msamples/s (Loom threads completed per second), regrouped engine; plain engine and SIMT lane efficiency beside it"
 
     if args.impl == "reference":
         if rank != 0:
             return
-        x = make_inputs(w)
-        vals = []
-        info = None
+        vals, info = [], None
         for i in range(warmup + args.steps):
-            v, info = cpu_reference(w, x, target_s=2.0)
+            v, info = cpu_reference(w, target_s=2.0)
             if i >= warmup:
                 vals.append(v)
         value = statistics.median(vals)
@@ -254,7 +388,7 @@ def main() -> None:
             json.dumps(
                 {
                     "impl": "reference",
-                    "metric": "Msamples/s (Loom threads completed per second)",
+                    "metric": metric,
                     "value": round(value, 3),
                     "unit": "Msamples/s",
                     "n_gpus": args.gpus,
@@ -263,7 +397,7 @@ def main() -> None:
                     "higher_is_better": True,
                     "scaling": "weak",
                     "vs_baseline": None,
-                    "dtype": w["dtype"],
+                    "dtype": w.dtype,
                     "data": "synthetic",
                     "config": config,
                     "cpu_baseline": dict(info, value=round(value, 3)),
@@ -289,66 +423,41 @@ def main() -> None:
 
     from loom_b200 import api
 
-    n = w["n"]
-    x = make_inputs(w)
-    d_in = torch.from_numpy(x.view(np.int64)).cuda()
-    out_dt = torch.int32 if w["out_bytes"] == 4 else torch.int64
-    d_out = torch.empty(n, dtype=out_dt, device="cuda")
     # a dedicated stream: the library launches on it and the CUDA events of
     # time_steps are recorded on it (torch's current stream)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
+    w.device_buffers(torch)
 
     res = {}
     for mode in ("plain", "regroup"):
-        f = api.Function(w["kernel"], 0, mode)
-        step = lambda: f.run_device([d_in], [d_out], n, stream=stream)  # noqa: E731
-        ms = time_steps(step, args.steps, warmup, torch, dist)
+        opts = TUNED[w.kernel] if mode == "regroup" else {}
+        f = api.Function(w.kernel, 0, mode, **opts)
+        ms = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
         f.sync()
         f.reset_stats()
-        # one counted launch for lane efficiency (plain needs its profiling variant)
-        if mode == "plain":
-            f.set_opts("plain", profile=True)
-        f.run_device([d_in], [d_out], n, stream=stream)
+        f.set_opts(mode, profile=True, **opts)  # one counted launch for lane efficiency
+        w.launch(f, api, stream)
         torch.cuda.synchronize()
         st = f.stats(raise_on_device_error=True)
+        f.set_opts(mode, **opts)
+        f.reset_stats()
         res[mode] = dict(ms=ms, stats=st, fn=f)
+    plain_out_ok, _ = w.check(api)
 
-    # clocks: sample during a second timed pass of the headline engine
+    # the headline: the regrouping engine, clocks sampled during the timed region
     f = res["regroup"]["fn"]
-    f.set_opts("regroup")
-    f.reset_stats()
     with ClockSampler(local) as clk:
-        ms_r = time_steps(lambda: f.run_device([d_in], [d_out], n, stream=stream), args.steps, warmup, torch, dist)
+        ms_r = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
     st_r = f.stats(raise_on_device_error=True)
-    kern_ms = st_r["ms"]  # last launch, device time of the megakernel stream span
+    kern_ms = st_r["ms"]
+    parity_ok, idx = w.check(api)
 
-    # parity of this run
-    got = d_out.cpu().numpy().view(np.uint32 if w["out_bytes"] == 4 else np.uint64)
-    from oracle import oracle as O
-
-    idx = O.uniform_int(5, 4096, 0, n - 1).astype(np.int64)
-    (want,) = O.Interp(w["kernel"]).run([x[idx]])
-    parity_ok = bool(np.array_equal(got[idx], want))
-
-    # e2e through the public API with pinned host buffers
-    h_in = torch.from_numpy(x.view(np.int64)).pin_memory()
-    h_out = torch.empty(n, dtype=out_dt).pin_memory()
-    fe = api.Function(w["kernel"], n, "regroup")
-    e2e_step = lambda: fe.run_host_ptrs([h_in], [h_out], n)  # noqa: E731
-    for _ in range(warmup):
-        e2e_step()
-    if dist is not None:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    e2e_s = time.perf_counter() - t0
+    e2e_s, e2e_ok, h2d, d2h = w.e2e(api, torch, args.steps, warmup, dist)
     if dist is not None:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_ok = bool(np.array_equal(h_out.numpy().view(got.dtype)[idx], want))
 
     if rank != 0:
         if dist is not None:
@@ -363,22 +472,33 @@ def main() -> None:
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
 
     ms_step = ms_r / args.steps
-    value = world * n / (ms_step / 1e3) / 1e6
+    value = world * w.n / (ms_step / 1e3) / 1e6
     plain_ms = res["plain"]["ms"] / args.steps
-    plain_value = world * n / (plain_ms / 1e3) / 1e6
+    plain_value = world * w.n / (plain_ms / 1e3) / 1e6
     sr = res["regroup"]["stats"]
     sp = res["plain"]["stats"]
-    # algorithmic bytes of one megakernel launch: inputs + outputs + state file
-    algo_bytes = n * (w["in_bytes"] + w["out_bytes"]) + sr["state_bytes"] / max(1, sr["launches"])
+    # algorithmic bytes of one megakernel launch: inputs, outputs, table and
+    # the queue state the engine moved (saves + restores, counted in-kernel)
+    state_per_launch = st_r["state_bytes"] / max(1, st_r["launches"])
+    algo_bytes = w.n * (w.in_bytes + w.out_bytes) + state_per_launch
     achieved = algo_bytes / (kern_ms / 1e3) / 1e9
+
+    # DRAM traffic of the dominant kernel from an ncu capture (per thread,
+    # scaled to this launch), see profiles/roofline_traffic.json
+    traffic = None
+    tf = ROOT / "profiles" / "roofline_traffic.json"
+    if tf.exists():
+        t = json.loads(tf.read_text()).get(w.kernel)
+        if t:
+            traffic = int(t["dram_bytes_per_thread"] * w.n)
 
     cpu = None
     if not args.no_cpu:
-        v, info = cpu_reference(w, x)
+        v, info = cpu_reference(w)
         cpu = dict(info, value=round(v, 3))
 
     line = {
-        "metric": "Msamples/s (Loom threads completed per second), regrouped engine; plain engine and SIMT lane efficiency beside it",
+        "metric": metric,
         "value": round(value, 3),
         "unit": "Msamples/s",
         "n_gpus": world,
@@ -388,40 +508,46 @@ def main() -> None:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": w["dtype"],
+        "dtype": w.dtype,
         "data": "synthetic",
         "config": config,
         "plain": {
             "value": round(plain_value, 3),
             "ms_per_step": round(plain_ms, 4),
             "lane_efficiency": round(sp["lane_efficiency"], 4),
-            "kernel_ms_profiled": round(sp["ms"], 4),
         },
         "regroup": {
             "kernel_ms": round(kern_ms, 4),
             "lane_efficiency": round(sr["lane_efficiency"], 4),
-            "rounds": sr["rounds"],
-            "parks_per_thread": round(sr["parks"] / n, 4),
-            "state_bytes_per_launch": int(sr["state_bytes"]),
+            "rounds": int(st_r["rounds"] / max(1, st_r["launches"])),
+            "parks_per_thread": round(st_r["parks"] / max(1, st_r["launches"]) / w.n, 4),
+            "state_bytes_per_launch": int(state_per_launch),
         },
         "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
-        "parity": {"sample_threads": len(idx), "device_ok": parity_ok, "e2e_ok": e2e_ok},
+        "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",
+        "parity": {
+            "sample_threads": int(len(idx)),
+            "regroup_device_ok": bool(parity_ok),
+            "plain_device_ok": bool(plain_out_ok),
+            "e2e_ok": bool(e2e_ok),
+        },
         "roofline": {
             "bound": "hbm",
             "achieved": round(achieved, 2),
             "peak": hbm_peak,
             "unit": "GB/s",
             "frac": round(achieved / hbm_peak, 5),
-            "traffic": None,
+            "traffic": traffic,
+            "algorithmic_bytes": int(algo_bytes),
             "peak_source": peak_src,
-            "note": "algorithmic bytes = inputs + outputs + state-file saves/restores; the engines are SIMT-issue-bound, see profiles/",
+            "note": "algorithmic bytes = outputs + inputs + queue-state saves/restores of the regrouping megakernel; the engine is SIMT issue/latency bound, not HBM bound (profiles/)",
         },
         "cpu_baseline": cpu,
         "e2e": {
-            "value": round(world * n * args.steps / e2e_s / 1e6, 3),
+            "value": round(world * w.n * args.steps / e2e_s / 1e6, 3),
             "unit": "Msamples/s",
-            "h2d_bytes_per_step": n * w["in_bytes"],
-            "d2h_bytes_per_step": n * w["out_bytes"],
+            "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h),
         },
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
@@ -429,7 +555,6 @@ def main() -> None:
     print(json.dumps(line))
     for r in res.values():
         r["fn"].close()
-    fe.close()
     if dist is not None:
         dist.destroy_process_group()
 

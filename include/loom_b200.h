@@ -97,9 +97,9 @@ typedef struct loom_b200_opts
     uint32_t spread_lanes; /* regroup: when the majority block holds at least
                               this many lanes, every live lane runs the
                               burst (33 = majority lanes only) */
-    uint32_t catchup;     /* regroup: blocks a lane behind the majority block
-                             may run to reach it before a burst
-                             (0 = default, 0xffffffff = none) */
+    uint32_t no_refill;   /* regroup: halted lanes without a prefetched input
+                             wait for the next vote instead of claiming one */
+    uint32_t pad0;
     uint64_t population;  /* regroup: resident thread slots; 0 = all inputs */
     uint64_t max_steps;   /* per-thread block-step guard; 0 = 2^40 */
     uint32_t profile;     /* collect lane-efficiency counters (slower) */
@@ -127,6 +127,39 @@ typedef struct loom_b200_stats
     uint32_t grid;         /* CTAs of the last launch */
     double   ms;           /* device time of the last launch (CUDA events) */
 } loom_b200_stats;
+
+/* Input column forms (loom_b200_input.form). */
+#define LOOM_B200_IN_ARRAY 0u      /* ptr[tid] */
+#define LOOM_B200_IN_IOTA 1u       /* the thread index tid */
+#define LOOM_B200_IN_BROADCAST 2u  /* `value` (its low bytes) for every thread */
+#define LOOM_B200_IN_LOCAL_IOTA 3u /* tid minus the first thread of its instance */
+#define LOOM_B200_IN_INSTANCE 4u   /* index of the thread's instance */
+
+typedef struct loom_b200_input
+{
+    const void* ptr;  /* LOOM_B200_IN_ARRAY: the column */
+    uint32_t    form; /* LOOM_B200_IN_* */
+    uint32_t    pad;
+    uint64_t    value; /* LOOM_B200_IN_BROADCAST: the bit pattern */
+} loom_b200_input;
+
+/* One launch over n threads that may belong to several instances of the
+ * kernel (render requests, input batches): instance i owns threads
+ * [instance_starts[i], instance_starts[i + 1]).  Threads of different
+ * instances that stand at the same basic block share warps.  `table` is the
+ * read-only table of 32-bit words that the tab op reads (a Loom extension,
+ * loom_b200/frontend/b200_ops.hpp). */
+typedef struct loom_b200_launch
+{
+    const loom_b200_input* inputs;          /* one per kernel input */
+    void* const*           outputs;         /* one per kernel output */
+    uint64_t               n;
+    const uint64_t*        instance_starts; /* num_instances + 1 offsets, or NULL */
+    uint32_t               num_instances;
+    uint32_t               pad;
+    const uint32_t*        table;           /* or NULL */
+    uint64_t               table_words;
+} loom_b200_launch;
 
 typedef struct loom_b200_handle loom_b200_handle;
 
@@ -166,6 +199,16 @@ int loom_b200_run_device(loom_b200_handle*  h,
                          void* const*       outputs,
                          uint64_t           n,
                          void*              stream);
+
+/* General launch on device memory: every pointer of `L` (array inputs,
+ * outputs, instance_starts, table) is a device pointer; asynchronous on
+ * `stream`. */
+int loom_b200_launch_device(loom_b200_handle* h, const loom_b200_launch* L, void* stream);
+
+/* General launch on host memory: array inputs, outputs, instance_starts and
+ * the table are host arrays; the call copies them in, runs the kernel,
+ * copies the outputs back and returns after they arrived. */
+int loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L);
 
 int loom_b200_sync(loom_b200_handle* h);
 int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);

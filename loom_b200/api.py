@@ -20,7 +20,13 @@ from typing import Dict, List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
-LIB_PATH = pathlib.Path(__file__).resolve().parent / "libloom_b200.so"
+import os
+
+# LOOM_B200_LIB selects another build of the library (e.g. one with more
+# kernels compiled in); default: the in-tree build
+LIB_PATH = pathlib.Path(
+    os.environ.get("LOOM_B200_LIB", pathlib.Path(__file__).resolve().parent / "libloom_b200.so")
+)
 
 PLAIN = 0
 REGROUP = 1
@@ -35,6 +41,12 @@ ERR_BUDGET = -6
 ERR_NO_DEVICE = -7
 ERR_CANCELLED = -8
 ERR_TIMEOUT = -9
+
+IN_ARRAY = 0
+IN_IOTA = 1
+IN_BROADCAST = 2
+IN_LOCAL_IOTA = 3
+IN_INSTANCE = 4
 
 STATUS_STEP_LIMIT = 1
 STATUS_ASSERT_FP = 2
@@ -90,7 +102,8 @@ class Opts(ctypes.Structure):
         ("period", ctypes.c_uint32),
         ("burst", ctypes.c_uint32),
         ("spread_lanes", ctypes.c_uint32),
-        ("catchup", ctypes.c_uint32),
+        ("no_refill", ctypes.c_uint32),
+        ("pad0", ctypes.c_uint32),
         ("population", ctypes.c_uint64),
         ("max_steps", ctypes.c_uint64),
         ("profile", ctypes.c_uint32),
@@ -116,6 +129,54 @@ class StatsC(ctypes.Structure):
     ]
 
 
+class InputC(ctypes.Structure):
+    _fields_ = [
+        ("ptr", ctypes.c_void_p),
+        ("form", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("value", ctypes.c_uint64),
+    ]
+
+
+class LaunchC(ctypes.Structure):
+    _fields_ = [
+        ("inputs", ctypes.POINTER(InputC)),
+        ("outputs", ctypes.POINTER(ctypes.c_void_p)),
+        ("n", ctypes.c_uint64),
+        ("instance_starts", ctypes.c_void_p),
+        ("num_instances", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("table", ctypes.c_void_p),
+        ("table_words", ctypes.c_uint64),
+    ]
+
+
+class Iota:
+    """Input column = thread index."""
+
+
+class LocalIota:
+    """Input column = thread index within its instance."""
+
+
+class Instance:
+    """Input column = index of the thread's instance."""
+
+
+class Broadcast:
+    """Input column = one value for every thread."""
+
+    def __init__(self, value, type_name: str):
+        self.value = value
+        self.type_name = type_name
+
+    def bits(self) -> int:
+        a = np.array([self.value], dtype=NP_TYPE[self.type_name])
+        b = np.zeros(8, dtype=np.uint8)
+        b[: a.itemsize] = a.view(np.uint8)
+        return int(b.view(np.uint64)[0])
+
+
 _lib = None
 
 # every symbol include/loom_b200.h declares
@@ -131,6 +192,8 @@ EXPORTS = [
     "loom_b200_get_opts",
     "loom_b200_run_host",
     "loom_b200_run_device",
+    "loom_b200_launch_device",
+    "loom_b200_launch_host",
     "loom_b200_sync",
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
@@ -161,6 +224,8 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_get_opts.argtypes = [vp, ctypes.POINTER(Opts)]
     L.loom_b200_run_host.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint64]
     L.loom_b200_run_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint64, vp]
+    L.loom_b200_launch_device.argtypes = [vp, ctypes.POINTER(LaunchC), vp]
+    L.loom_b200_launch_host.argtypes = [vp, ctypes.POINTER(LaunchC)]
     L.loom_b200_sync.argtypes = [vp]
     L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
     L.loom_b200_reset_stats.argtypes = [vp]
@@ -220,7 +285,7 @@ def make_opts(
     period: int = 0,
     burst: int = 0,
     spread_lanes: int = 0,
-    catchup: int = 0,
+    refill: bool = True,
     population: int = 0,
     max_steps: int = 0,
     profile: bool = False,
@@ -238,7 +303,8 @@ def make_opts(
         period=period,
         burst=burst,
         spread_lanes=spread_lanes,
-        catchup=catchup,
+        no_refill=0 if refill else 1,
+        pad0=0,
         population=population,
         max_steps=max_steps,
         profile=1 if profile else 0,
@@ -315,6 +381,56 @@ class Function:
         pout = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
         s = getattr(stream, "cuda_stream", stream)
         check(lib().loom_b200_run_device(self._h, pin, pout, n, s))
+
+    def _launch_struct(self, inputs, outputs, n, instance_starts, table):
+        ins = (InputC * max(1, len(inputs)))()
+        keep = []
+        for i, (a, (_, t)) in enumerate(zip(inputs, self.info.inputs)):
+            if a is None or a is Iota or isinstance(a, Iota):
+                ins[i] = InputC(None, IN_IOTA, 0, 0)
+            elif a is LocalIota or isinstance(a, LocalIota):
+                ins[i] = InputC(None, IN_LOCAL_IOTA, 0, 0)
+            elif a is Instance or isinstance(a, Instance):
+                ins[i] = InputC(None, IN_INSTANCE, 0, 0)
+            elif isinstance(a, Broadcast):
+                ins[i] = InputC(None, IN_BROADCAST, 0, a.bits())
+            else:
+                if isinstance(a, np.ndarray):
+                    a = np.ascontiguousarray(a, dtype=NP_TYPE[t])
+                    keep.append(a)
+                ins[i] = InputC(_ptr(a), IN_ARRAY, 0, 0)
+        outs = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
+        L = LaunchC()
+        L.inputs = ins
+        L.outputs = outs
+        L.n = n
+        L.instance_starts = _ptr(instance_starts)
+        L.num_instances = 0 if instance_starts is None else len(instance_starts) - 1
+        L.table = _ptr(table)
+        L.table_words = 0 if table is None else len(table)
+        keep += [ins, outs, instance_starts, table]
+        return L, keep
+
+    def launch_host(self, inputs, n: int, instance_starts=None, table=None):
+        """General blocking launch on host arrays; inputs may be arrays or
+        Iota / LocalIota / Instance / Broadcast.  Returns output arrays."""
+        outs = [np.empty(n, dtype=NP_TYPE[t]) for _, t in self.info.outputs]
+        if instance_starts is not None:
+            instance_starts = np.ascontiguousarray(instance_starts, dtype=np.uint64)
+        if table is not None:
+            table = np.ascontiguousarray(table, dtype=np.uint32)
+        L, keep = self._launch_struct(inputs, outs, n, instance_starts, table)
+        check(lib().loom_b200_launch_host(self._h, ctypes.byref(L)))
+        del keep
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def launch_device(self, inputs, outputs, n: int, instance_starts=None, table=None, stream=None):
+        """General asynchronous launch; every array is device memory (torch
+        tensors or raw pointers)."""
+        L, keep = self._launch_struct(inputs, outputs, n, instance_starts, table)
+        s = getattr(stream, "cuda_stream", stream)
+        check(lib().loom_b200_launch_device(self._h, ctypes.byref(L), s))
+        del keep
 
     def sync(self) -> None:
         check(lib().loom_b200_sync(self._h))

@@ -151,6 +151,9 @@ class Lowering:
             return f"op_fma({a[0]}, {a[1]}, {z})"
         if op == "assert_fp":
             return f"op_assert_fp({a[0]}, ctx)"
+        if op == "tab":
+            (t,) = ot
+            return f"table_load<{CTYPE[t]}>(*ctx.cols, static_cast<unsigned>({a[0]}))"
         if op == "sct":
             t, _ = ot
             consts = [literal(c) for c in ins.consts]
@@ -271,12 +274,18 @@ def generate(k: Kernel) -> str:
     regs = [r for r in k.regs if r.idx != L.pc]
     if nin + nout > 96:
         raise ValueError(f"{name}: too many columns")
-    # queue segments: per block, live-in columns by decreasing size, then the
+    # work queues: one per block plus one per context of each dispatch block
+    queues = k.queues()
+    qlive = k.queue_liveness()
+    disp = k.dispatch_blocks()
+    nq = len(queues)
+    qbytes = [sum(L.regs[r].nbytes for r in li) for li in qlive]
+    # queue segments: per queue, live-in columns by decreasing size, then the
     # u32 input index; each segment padded to 8 bytes per entry
     layout = []
     row_total = 0
-    for b in range(nb):
-        cols = sorted(live_in[b], key=lambda r: (-L.regs[r].nbytes, r))
+    for q in range(nq):
+        cols = sorted(qlive[q], key=lambda r: (-L.regs[r].nbytes, r))
         off = row_total
         placed = []
         for r in cols:
@@ -299,11 +308,13 @@ def generate(k: Kernel) -> str:
     w(f"namespace loom_b200 {{ namespace k_{name} {{")
     w("")
     w(f"__constant__ unsigned kInstrTab[{nb}] = {{{', '.join(map(str, counts))}}};")
-    w(f"__constant__ unsigned kLiveTab[{nb}] = {{{', '.join(map(str, live_bytes))}}};")
+    w(f"__constant__ unsigned kLiveTab[{nq}] = {{{', '.join(map(str, qbytes))}}};")
+    w(f"__constant__ int kQueueBlock[{nq}] = {{{', '.join(str(b) for b, _ in queues)}}};")
     w("")
     w("struct K")
     w("{")
     w(f"    static constexpr int kNumBlocks = {nb};")
+    w(f"    static constexpr int kNumQueues = {nq};")
     w("    struct Regs")
     w("    {")
     for r in regs:
@@ -326,9 +337,7 @@ def generate(k: Kernel) -> str:
     w("    load_in(In& in, const Columns& c, const unsigned long long tid)")
     w("    {")
     for i, (reg, t, vname) in enumerate(k.inputs):
-        ct = CTYPE[t]
-        w(f"        {{ const {ct}* col = static_cast<const {ct}*>(c.p[{i}]);")
-        w(f"          in.v{i} = col ? col[tid] : static_cast<{ct}>(tid); }}")
+        w(f"        in.v{i} = load_input<{CTYPE[t]}>(c, {i}, tid);")
     w("        (void)in; (void)c; (void)tid;")
     w("    }")
     w("")
@@ -360,18 +369,57 @@ def generate(k: Kernel) -> str:
     w("    }")
     w("")
     w("    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }")
-    w("    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }")
+    w("    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }")
+    w("    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }")
+    w("")
+    per_block = [[qi for qi, (b, _) in enumerate(queues) if b == blk] for blk in range(nb)]
+    maxq = max(len(x) for x in per_block)
+    w(f"    static constexpr int kMaxQueuesPerBlock = {maxq};")
+    w("    // j-th queue holding threads that stand at block b (-1: none).")
+    w("    __device__ __forceinline__ static int")
+    w("    queue_list(const int b, const int j)")
+    w("    {")
+    multi = [(blk, ql) for blk, ql in enumerate(per_block) if len(ql) > 1]
+    for blk, ql in multi:
+        w(f"        if(b == {blk})")
+        w("        {")
+        w("            switch(j)")
+        w("            {")
+        for j, qi in enumerate(ql):
+            w(f"            case {j}: return {qi};")
+        w("            default: return -1;")
+        w("            }")
+        w("        }")
+    w("        return j == 0 ? b : -1;")
+    w("    }")
+    w("")
+    w("    // Queue a thread standing at block pc waits in: the block's own queue,")
+    w("    // or for a dispatch block the queue of the context its register selects.")
+    w("    __device__ __forceinline__ static int")
+    w("    queue_of(const int pc, const Regs& R)")
+    w("    {")
+    w("        (void)R;")
+    for d, (v, ctx) in sorted(disp.items()):
+        w(f"        if(pc == {d})")
+        w("        {")
+        w(f"            switch(static_cast<unsigned long long>(R.r{v}))")
+        w("            {")
+        for kk in ctx:
+            w(f"            case {kk}ull: return {queues.index((d, kk))};")
+        w("            default: break;")
+        w("            }")
+        w("        }")
+    w("        return pc;")
+    w("    }")
     w("")
     # ---- run_burst (goto CFG entered at any block, bounded by a budget)
     w("    // Runs the lane's own path from block `entry` for at most `budget`")
-    w("    // blocks (with kStop: also stopping on arrival at block `stop`);")
-    w("    // returns the block it stopped at, or kHalt.")
-    w("    template <bool kProf, bool kStop = false>")
+    w("    // blocks; returns the block it stopped at, or kHalt.")
+    w("    template <bool kProf>")
     w("    __device__ __forceinline__ static int")
-    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)")
     w("    {")
     w("        (void)ctx;")
-    w("        (void)stop;")
     w("        switch(entry)")
     w("        {")
     for blk in k.blocks:
@@ -380,7 +428,7 @@ def generate(k: Kernel) -> str:
     w("        }")
     for blk in k.blocks:
         w(f"    L_B{blk.idx}: // {blk.label}")
-        w(f"        if(budget == 0u || (kStop && stop == {blk.idx})) return {blk.idx};")
+        w(f"        if(budget == 0u) return {blk.idx};")
         w("        --budget;")
         w(f"        if constexpr(kProf) count_block(ctx, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
@@ -395,27 +443,29 @@ def generate(k: Kernel) -> str:
     for fn in ("save", "restore"):
         w("    __device__ __forceinline__ static " + ("void" if fn == "save" else "unsigned"))
         if fn == "save":
-            w("    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,")
+            w("    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,")
             w("         const unsigned idx, const unsigned tid)")
         else:
-            w("    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,")
+            w("    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,")
             w("            const unsigned idx)")
         w("    {")
         q = "" if fn == "save" else "const "
         w(f"        {q}char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;")
-        w("        switch(b)")
+        w("        switch(q)")
         w("        {")
-        for blk in k.blocks:
-            b = blk.idx
-            w(f"        case {b}:")
-            for r, off in layout[b]["cols"]:
+        for qi, (b, kk) in enumerate(queues):
+            w(f"        case {qi}: // {k.blocks[b].label}" + ("" if kk is None else f", context {kk}"))
+            if fn == "restore" and kk is not None:
+                v = disp[b][0]
+                w(f"            R.r{v} = static_cast<{CTYPE[L.regs[v].storage]}>({kk});")
+            for r, off in layout[qi]["cols"]:
                 stt = CTYPE[L.regs[r].storage]
                 col = f"reinterpret_cast<{q}{stt}*>(base + {off}ull * cap)[idx]"
                 if fn == "save":
                     w(f"            {col} = R.r{r};")
                 else:
                     w(f"            R.r{r} = {col};")
-            tcol = f"reinterpret_cast<{q}unsigned*>(base + {layout[b]['tid']}ull * cap)[idx]"
+            tcol = f"reinterpret_cast<{q}unsigned*>(base + {layout[qi]['tid']}ull * cap)[idx]"
             if fn == "save":
                 w(f"            {tcol} = tid;")
                 w("            return;")
@@ -471,7 +521,7 @@ def generate(k: Kernel) -> str:
     w("")
     w(f"extern const loom_b200::KernelEntry loom_b200_entry_{name};")
     w(f"const loom_b200::KernelEntry loom_b200_entry_{name} = {{")
-    w(f"    &loom_b200::k_{name}::kInfo, loom_b200::k_{name}::K::kRowBytes,")
+    w(f"    &loom_b200::k_{name}::kInfo, loom_b200::k_{name}::K::kRowBytes, {nq},")
     w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
     w(f"    &loom_b200::k_{name}::regroup_occupancy}};")
     return "\n".join(o) + "\n"

@@ -227,6 +227,138 @@ class Kernel:
                     changed = True
         return live_in, live_out
 
+    # ------------------------------------------------------------ dispatch
+    def predecessors(self) -> List[List[int]]:
+        preds: List[List[int]] = [[] for _ in self.blocks]
+        for b in self.blocks:
+            for t in b.successors():
+                if t != HALT and b.idx not in preds[t]:
+                    preds[t].append(b.idx)
+        return preds
+
+    def dispatch_blocks(self) -> Dict[int, Tuple[int, Dict[int, int]]]:
+        """Blocks used as subroutines: block D ends with a ParmJump on a
+        register v that D does not write, and every predecessor of D last
+        writes v with a literal k before reaching D (Loom kernels call shared
+        code this way, e.g. the RNG block of src/smallpt/vm/pt.hpp:889-914).
+        Returns {D: (v, {k: target})}; the target of each context is known
+        statically, which makes liveness context sensitive."""
+        out: Dict[int, Tuple[int, Dict[int, int]]] = {}
+        preds = self.predecessors()
+        for b in self.blocks:
+            t = b.terminator
+            if not isinstance(t, ParmJump) or t.var.is_literal or b.idx == 0:
+                continue
+            v = t.var.reg
+            if any(v in ins.writes() for ins in b.instrs):
+                continue
+            ctx: Dict[int, int] = {}
+            ok = bool(preds[b.idx])
+            for p in preds[b.idx]:
+                last = None
+                for ins in self.blocks[p].instrs:
+                    if v in ins.writes():
+                        last = ins
+                if not (
+                    isinstance(last, Compute)
+                    and last.op == "mov"
+                    and last.args[0].is_literal
+                    and last.dst.reg == v
+                ):
+                    ok = False
+                    break
+                k = int(last.args[0].value())
+                if not 0 <= k < len(t.targets) or self.blocks[p].successors() != [b.idx]:
+                    ok = False
+                    break
+                ctx[k] = t.targets[k]
+            if ok:
+                out[b.idx] = (v, dict(sorted(ctx.items())))
+        return out
+
+    def queues(self) -> List[Tuple[int, Optional[int]]]:
+        """Work queues of the regrouping engine: one per block (context k =
+        None, the block's own live set) followed by one per context of every
+        dispatch block."""
+        q: List[Tuple[int, Optional[int]]] = [(b.idx, None) for b in self.blocks]
+        for d, (_, ctx) in sorted(self.dispatch_blocks().items()):
+            for k in ctx:
+                q.append((d, k))
+        return q
+
+    def queue_liveness(self) -> List[Set[int]]:
+        """Registers a thread parked in each queue must carry.
+
+        Liveness runs on the CFG in which every dispatch block D is split
+        into one copy per context k that jumps straight to its target, and
+        each predecessor flows into the copy of the context it selects.  A
+        queue (D, k) holds D's copy for context k without the dispatch
+        register (restored as the constant k); queue (b, None) holds the live
+        set of b on the split CFG (for D itself: the union over contexts)."""
+        disp = self.dispatch_blocks()
+        pc = self.pc_reg()
+        nodes: List[Tuple[int, Optional[int]]] = self.queues()
+        index = {n: i for i, n in enumerate(nodes)}
+        use: List[Set[int]] = []
+        defs: List[Set[int]] = []
+        for b, _ in nodes:
+            u: Set[int] = set()
+            d: Set[int] = set()
+            for ins in self.blocks[b].instrs:
+                for r in ins.reads():
+                    if r not in d:
+                        u.add(r)
+                for r in ins.writes():
+                    d.add(r)
+            u.discard(pc)
+            d.discard(pc)
+            use.append(u)
+            defs.append(d)
+
+        def succs(node) -> List[Tuple[int, Optional[int]]]:
+            b, k = node
+            if b in disp and k is not None:
+                return [(disp[b][1][k], None)] if disp[b][1][k] != HALT else [(HALT, None)]
+            out = []
+            for t in self.blocks[b].successors():
+                if t != HALT and t in disp and b != t:
+                    v = disp[t][0]
+                    last = None
+                    for ins in self.blocks[b].instrs:
+                        if v in ins.writes():
+                            last = ins
+                    k2 = int(last.args[0].value())
+                    out.append((t, k2))
+                else:
+                    out.append((t, None))
+            return out
+
+        halt_use = {r for r, _, _ in self.outputs}
+        live = [set() for _ in nodes]
+        changed = True
+        while changed:
+            changed = False
+            for i in reversed(range(len(nodes))):
+                out: Set[int] = set()
+                for s in succs(nodes[i]):
+                    out |= halt_use if s[0] == HALT else live[index[s]]
+                new = use[i] | (out - defs[i])
+                if new != live[i]:
+                    live[i] = new
+                    changed = True
+        # a context queue does not store its dispatch register
+        for i, (b, k) in enumerate(nodes):
+            if k is not None:
+                live[i] = live[i] - {disp[b][0]}
+        # the plain queue of a dispatch block: union over its contexts plus
+        # the dispatch register (fallback for values outside the contexts)
+        for d, (v, ctx) in disp.items():
+            u: Set[int] = set()
+            for k in ctx:
+                u |= live[index[(d, k)]]
+            live[index[(d, None)]] = u | {v}
+        return live
+
     def state_regs(self) -> List[int]:
         """Registers that are live at the entry of some block: the columns of
         the regrouping engine's state file."""

@@ -12,18 +12,29 @@
 
 namespace loom_b200
 {
-/// Maximum number of columns (inputs + outputs + state registers) per kernel;
-/// the pointer table travels in the kernel's parameter space.
-constexpr int kMaxCols = 96;
+/// Maximum number of columns (inputs + outputs) per kernel; the pointer
+/// table travels in the kernel's parameter space.
+constexpr int kMaxCols = 64;
+/// Maximum number of input columns.
+constexpr int kMaxIn = 16;
 
 /// Block index used for "thread finished" (Loom's halt_pos, core.hpp:985).
 constexpr int kHalt = -1;
 /// Lane holds no thread.
 constexpr int kEmpty = -2;
 
+/// Input and output columns of a launch, plus what the input forms and the
+/// table op read.  Input i is read according to form[i]
+/// (LOOM_B200_IN_*): an array, the thread index, a broadcast value, the
+/// thread index within its instance, or the instance index.
 struct Columns
 {
-    void* p[kMaxCols];
+    void*                     p[kMaxCols];
+    unsigned                  form[kMaxIn];
+    unsigned long long        value[kMaxIn];
+    const unsigned long long* inst_start; // num_inst + 1 thread offsets
+    unsigned                  num_inst;
+    const unsigned*           table;      // words read by the tab op
 };
 
 /// Status bits written by device code (also returned through the C ABI).
@@ -35,12 +46,16 @@ enum : unsigned
     kStatusBarrierTimeout = LOOM_B200_STATUS_BARRIER_TIMEOUT,
 };
 
-/// Per-thread execution context: instruction counters and the status word.
+struct Columns;
+
+/// Per-thread execution context: instruction counters, the status word and
+/// the launch's columns (for the table op).
 struct Ctx
 {
     unsigned long long thread_instr;
     unsigned long long warp_instr;
     unsigned*          status;
+    const Columns*     cols;
 
     __device__ __forceinline__ void
     flag(unsigned bit)
@@ -129,6 +144,53 @@ count_block(Ctx& ctx, const unsigned n_instr)
     if((threadIdx.x & 31) == static_cast<unsigned>(__ffs(active) - 1))
         ctx.warp_instr += n_instr;
     ctx.thread_instr += n_instr;
+}
+
+/// Instance of thread `tid`: the last i with inst_start[i] <= tid.
+__device__ __forceinline__ unsigned
+find_instance(const Columns& c, const unsigned long long tid)
+{
+    unsigned lo = 0, hi = c.num_inst; // inst_start[lo] <= tid < inst_start[hi]
+    while(hi - lo > 1)
+    {
+        const unsigned mid = (lo + hi) >> 1;
+        if(c.inst_start[mid] <= tid)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+/// Input i of thread `tid` as T.
+template <typename T>
+__device__ __forceinline__ T
+load_input(const Columns& c, const int i, const unsigned long long tid)
+{
+    switch(c.form[i])
+    {
+    case LOOM_B200_IN_ARRAY: return static_cast<const T*>(c.p[i])[tid];
+    case LOOM_B200_IN_BROADCAST:
+    {
+        T v;
+        memcpy(&v, &c.value[i], sizeof(T));
+        return v;
+    }
+    case LOOM_B200_IN_LOCAL_IOTA:
+        return static_cast<T>(c.num_inst ? tid - c.inst_start[find_instance(c, tid)] : tid);
+    case LOOM_B200_IN_INSTANCE:
+        return static_cast<T>(c.num_inst ? find_instance(c, tid) : 0u);
+    default: return static_cast<T>(tid);
+    }
+}
+
+/// The tab op (a Loom extension): word `idx` of the launch's table as T,
+/// through the read-only data path.
+template <typename T>
+__device__ __forceinline__ T
+table_load(const Columns& c, const unsigned idx)
+{
+    return bitcast<T>(__ldg(c.table + idx));
 }
 
 /// Block-wide sum of three counters into global memory, one atomic per warp.

@@ -25,7 +25,7 @@ plain_kernel(const Columns                  cols,
 {
     const unsigned long long tid =
         static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    Ctx ctx{0ull, 0ull, status};
+    Ctx ctx{0ull, 0ull, status, &cols};
     if(tid < n)
     {
         typename K::Regs R;

@@ -21,8 +21,7 @@
 //    along each lane's own path (hardware reconvergence inside the burst),
 //    so the vote costs one ballot per burst; only when the majority block
 //    loses its quorum does the warp vote again with __match_any_sync and
-//    __reduce_max_sync.  Lanes behind the majority block may first run up to
-//    `catchup` blocks to reach it;
+//    __reduce_max_sync;
 //  * exchange: a halted lane writes its outputs and continues with a new
 //    input that it prefetched into registers earlier (one warp-aggregated
 //    atomicAdd on the input cursor per claim), so the input load latency is
@@ -70,8 +69,8 @@ struct RegroupParams
     unsigned            period;   // block steps per tile per round
     unsigned            burst;    // blocks a lane runs between two votes
     unsigned            spread;   // majority size from which all live lanes run
-    unsigned            catchup;  // blocks a lane behind the majority may run to reach it
     unsigned            prefetch; // prefetch the next input of every lane
+    unsigned            refill;   // halted lanes claim new inputs at once
     unsigned            phantoms; // fault injection: CTAs the barrier waits for in vain
 };
 
@@ -161,29 +160,23 @@ template <typename K, bool kProf>
 __global__ void
 regroup_kernel(const RegroupParams p)
 {
-    constexpr int      B    = K::kNumBlocks;
+    constexpr int      B    = K::kNumQueues;
     constexpr unsigned FULL = 0xffffffffu;
-
     const unsigned lane  = threadIdx.x & 31u;
     const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-
-    Ctx ctx{0ull, 0ull, p.status};
+    Ctx ctx{0ull, 0ull, p.status, &p.cols};
     unsigned long long parks = 0, sbytes = 0, finished = 0;
     typename K::Regs   R;
-    typename K::In     pf; // prefetched next input of this lane
+    typename K::In     pf;
     unsigned long long pf_tid = ~0ull;
-
     for(unsigned round = 0;; ++round)
     {
         const unsigned           cur = round & 1u, nxt = cur ^ 1u;
         const unsigned long long admit_end = ld_volatile64(&p.ctl->admit_end);
         unsigned                 bsel = gwarp % B;
-        bool                     dry  = false; // no more admissions this round
-
+        bool                     dry  = false;
         for(;;)
         {
-            // ------------------------------------------------ take a tile
-            // parked threads first (work conserving), then fresh inputs
             int      tb = kEmpty;
             unsigned tk = 0, toff = 0;
             if(lane == 0)
@@ -192,7 +185,7 @@ regroup_kernel(const RegroupParams p)
                 {
                     const unsigned b = (bsel + i) % B;
                     unsigned cnt     = ld_volatile(&p.qcnt[cur * B + b]);
-                    if(cnt > p.cap) cnt = p.cap; // an overrun was flagged
+                    if(cnt > p.cap) cnt = p.cap;
                     if(ld_volatile(&p.qhead[b]) >= cnt) continue;
                     const unsigned off = atomicAdd(&p.qhead[b], 32u);
                     if(off < cnt)
@@ -208,7 +201,6 @@ regroup_kernel(const RegroupParams p)
             tb   = __shfl_sync(FULL, tb, 0);
             tk   = __shfl_sync(FULL, tk, 0);
             toff = __shfl_sync(FULL, toff, 0);
-
             int                pc  = kEmpty;
             unsigned long long tid = 0;
             if(tb >= 0)
@@ -216,63 +208,36 @@ regroup_kernel(const RegroupParams p)
                 if(lane < tk)
                 {
                     tid = K::restore(tb, R, p.state, p.cap, cur, toff + lane);
-                    if(tid < p.n)
-                    {
-                        pc = tb;
-                        sbytes += K::live_bytes(tb) + 4u;
-                    }
-                    else
-                        ctx.flag(kStatusQueueOverrun);
+                    if(tid < p.n) { pc = K::block_of(tb); sbytes += K::live_bytes(tb) + 4u; }
+                    else ctx.flag(kStatusQueueOverrun);
                 }
+                tb = K::block_of(tb);
             }
             else
             {
                 if(dry) break;
                 const unsigned long long t = claim_inputs(FULL, p.ctl, admit_end, dry);
                 if(__ballot_sync(FULL, t != ~0ull) == 0u) break;
-                if(t != ~0ull)
-                {
-                    typename K::In in;
-                    K::load_in(in, p.cols, t);
-                    K::start(R, in);
-                    tid = t;
-                    pc  = 0;
-                }
-                tb = 0;
-                tk = 32u;
+                if(t != ~0ull) { typename K::In in; K::load_in(in, p.cols, t); K::start(R, in); tid = t; pc = 0; }
+                tb = 0; tk = 32u;
             }
-
-            // ------------------------------------------------ run
             int      m     = tb;
             unsigned mc    = tk;
             unsigned steps = 0;
             for(;;)
             {
-                // prefetch the next input of every lane that has none
                 if(p.prefetch && !dry)
                 {
                     const unsigned need = __ballot_sync(FULL, pf_tid == ~0ull);
                     if(need)
                     {
                         const unsigned long long t = claim_inputs(need, p.ctl, admit_end, dry);
-                        if(t != ~0ull)
-                        {
-                            pf_tid = t;
-                            K::load_in(pf, p.cols, t);
-                        }
+                        if(t != ~0ull) { pf_tid = t; K::load_in(pf, p.cols, t); }
                     }
                 }
-                // catch-up: lanes behind the majority block (for instance
-                // lanes that just started at block 0) run toward it, so the
-                // burst starts with the warp converged at m
-                if(p.catchup && pc >= 0 && pc != m)
-                    pc = K::template run_burst<kProf, true>(pc, R, ctx, p.catchup, m);
                 if(pc >= 0 && (mc >= p.spread || pc == m))
                     pc = K::template run_burst<kProf>(pc, R, ctx, p.burst);
                 steps += p.burst;
-
-                // exchange: halted lanes write their outputs and continue
-                // with a prefetched input, or claim one now
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
                 {
@@ -281,88 +246,55 @@ regroup_kernel(const RegroupParams p)
                         K::store_outputs(R, p.cols, tid);
                         ++finished;
                         pc = kEmpty;
-                        if(pf_tid != ~0ull)
-                        {
-                            K::start(R, pf);
-                            tid    = pf_tid;
-                            pf_tid = ~0ull;
-                            pc     = 0;
-                        }
+                        if(pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
                     }
-                    if(!dry)
+                    if(!dry && p.refill)
                     {
                         const unsigned need = __ballot_sync(FULL, pc == kEmpty);
                         if(need)
                         {
-                            const unsigned long long t =
-                                claim_inputs(need, p.ctl, admit_end, dry);
-                            if(t != ~0ull)
-                            {
-                                typename K::In in;
-                                K::load_in(in, p.cols, t);
-                                K::start(R, in);
-                                tid = t;
-                                pc  = 0;
-                            }
+                            const unsigned long long t = claim_inputs(need, p.ctl, admit_end, dry);
+                            if(t != ~0ull) { typename K::In in; K::load_in(in, p.cols, t); K::start(R, in); tid = t; pc = 0; }
                         }
                     }
                 }
-
                 if(steps >= p.period) break;
                 const unsigned cm = __popc(__ballot_sync(FULL, pc == m));
-                if(cm >= p.utr)
-                {
-                    mc = cm;
-                    continue;
-                }
+                if(cm >= p.utr) { mc = cm; continue; }
                 const unsigned peers = __match_any_sync(FULL, pc);
-                const unsigned key =
-                    pc >= 0 ? ((static_cast<unsigned>(__popc(peers)) << 16) |
-                               static_cast<unsigned>(pc))
-                            : 0u;
+                const unsigned key = pc >= 0 ? ((static_cast<unsigned>(__popc(peers)) << 16) | static_cast<unsigned>(pc)) : 0u;
                 const unsigned best = __reduce_max_sync(FULL, key);
-                if(best == 0u) break; // no live lane left
+                if(best == 0u) break;
                 m  = static_cast<int>(best & 0xffffu);
                 mc = best >> 16;
                 if(mc < p.utr) break;
             }
-
-            // ------------------------------------------------ park
-            // live threads wait in the queue of their block; a prefetched
-            // input that never started waits in the queue of block 0
             for(int pass = 0; pass < 2; ++pass)
             {
                 if(pass == 1)
                 {
                     if(__ballot_sync(FULL, pf_tid != ~0ull) == 0u) break;
                     pc = kEmpty;
-                    if(pf_tid != ~0ull)
-                    {
-                        K::start(R, pf);
-                        tid    = pf_tid;
-                        pf_tid = ~0ull;
-                        pc     = 0;
-                    }
+                    if(pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
                 }
                 const unsigned live = __ballot_sync(FULL, pc >= 0);
                 if(pc >= 0)
                 {
-                    const unsigned peers  = __match_any_sync(live, pc);
+                    const int      q      = K::queue_of(pc, R);
+                    const unsigned peers  = __match_any_sync(live, q);
                     const int      leader = __ffs(peers) - 1;
                     unsigned       base   = 0;
                     if(static_cast<int>(lane) == leader)
-                        base = atomicAdd(&p.qcnt[nxt * B + pc],
-                                         static_cast<unsigned>(__popc(peers)));
+                        base = atomicAdd(&p.qcnt[nxt * B + q], static_cast<unsigned>(__popc(peers)));
                     base = __shfl_sync(peers, base, leader);
                     const unsigned idx = base + __popc(peers & lanemask_lt());
                     if(idx < p.cap)
                     {
-                        K::save(pc, R, p.state, p.cap, nxt, idx, static_cast<unsigned>(tid));
-                        sbytes += K::live_bytes(pc) + 4u;
+                        K::save(q, R, p.state, p.cap, nxt, idx, static_cast<unsigned>(tid));
+                        sbytes += K::live_bytes(q) + 4u;
                         ++parks;
                     }
-                    else
-                        ctx.flag(kStatusQueueOverrun);
+                    else ctx.flag(kStatusQueueOverrun);
                 }
             }
         }

@@ -8,10 +8,12 @@ namespace loom_b200 { namespace k_bool_or_u64 {
 
 __constant__ unsigned kInstrTab[1] = {2};
 __constant__ unsigned kLiveTab[1] = {16};
+__constant__ int kQueueBlock[1] = {0};
 
 struct K
 {
     static constexpr int kNumBlocks = 1;
+    static constexpr int kNumQueues = 1;
     struct Regs
     {
         unsigned long long r0; // a: u64
@@ -28,10 +30,8 @@ struct K
     __device__ __forceinline__ static void
     load_in(In& in, const Columns& c, const unsigned long long tid)
     {
-        { const unsigned long long* col = static_cast<const unsigned long long*>(c.p[0]);
-          in.v0 = col ? col[tid] : static_cast<unsigned long long>(tid); }
-        { const unsigned long long* col = static_cast<const unsigned long long*>(c.p[1]);
-          in.v1 = col ? col[tid] : static_cast<unsigned long long>(tid); }
+        in.v0 = load_input<unsigned long long>(c, 0, tid);
+        in.v1 = load_input<unsigned long long>(c, 1, tid);
         (void)in; (void)c; (void)tid;
     }
 
@@ -61,24 +61,40 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
-    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
+    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
+    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+
+    static constexpr int kMaxQueuesPerBlock = 1;
+    // j-th queue holding threads that stand at block b (-1: none).
+    __device__ __forceinline__ static int
+    queue_list(const int b, const int j)
+    {
+        return j == 0 ? b : -1;
+    }
+
+    // Queue a thread standing at block pc waits in: the block's own queue,
+    // or for a dispatch block the queue of the context its register selects.
+    __device__ __forceinline__ static int
+    queue_of(const int pc, const Regs& R)
+    {
+        (void)R;
+        return pc;
+    }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks (with kStop: also stopping on arrival at block `stop`);
-    // returns the block it stopped at, or kHalt.
-    template <bool kProf, bool kStop = false>
+    // blocks; returns the block it stopped at, or kHalt.
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop;
         switch(entry)
         {
         case 0: goto L_B0;
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u || (kStop && stop == 0)) return 0;
+        if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r0 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r0) || static_cast<unsigned long long>(R.r1)));
@@ -90,13 +106,13 @@ struct K
 
     static constexpr unsigned long long kRowBytes = 24ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,
          const unsigned idx, const unsigned tid)
     {
         char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r0;
             reinterpret_cast<unsigned long long*>(base + 8ull * cap)[idx] = R.r1;
             reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
@@ -106,13 +122,13 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned
-    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,
             const unsigned idx)
     {
         const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             R.r0 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
             R.r1 = reinterpret_cast<const unsigned long long*>(base + 8ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
@@ -164,6 +180,6 @@ cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 
 extern const loom_b200::KernelEntry loom_b200_entry_bool_or_u64;
 const loom_b200::KernelEntry loom_b200_entry_bool_or_u64 = {
-    &loom_b200::k_bool_or_u64::kInfo, loom_b200::k_bool_or_u64::K::kRowBytes,
+    &loom_b200::k_bool_or_u64::kInfo, loom_b200::k_bool_or_u64::K::kRowBytes, 1,
     &loom_b200::k_bool_or_u64::launch_plain, &loom_b200::k_bool_or_u64::launch_regroup,
     &loom_b200::k_bool_or_u64::regroup_occupancy};

@@ -8,10 +8,12 @@ namespace loom_b200 { namespace k_fac_u64 {
 
 __constant__ unsigned kInstrTab[3] = {3, 2, 4};
 __constant__ unsigned kLiveTab[3] = {8, 8, 16};
+__constant__ int kQueueBlock[3] = {0, 1, 2};
 
 struct K
 {
     static constexpr int kNumBlocks = 3;
+    static constexpr int kNumQueues = 3;
     struct Regs
     {
         unsigned long long r1; // a: u64
@@ -28,8 +30,7 @@ struct K
     __device__ __forceinline__ static void
     load_in(In& in, const Columns& c, const unsigned long long tid)
     {
-        { const unsigned long long* col = static_cast<const unsigned long long*>(c.p[0]);
-          in.v0 = col ? col[tid] : static_cast<unsigned long long>(tid); }
+        in.v0 = load_input<unsigned long long>(c, 0, tid);
         (void)in; (void)c; (void)tid;
     }
 
@@ -59,17 +60,33 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
-    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
+    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
+    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+
+    static constexpr int kMaxQueuesPerBlock = 1;
+    // j-th queue holding threads that stand at block b (-1: none).
+    __device__ __forceinline__ static int
+    queue_list(const int b, const int j)
+    {
+        return j == 0 ? b : -1;
+    }
+
+    // Queue a thread standing at block pc waits in: the block's own queue,
+    // or for a dispatch block the queue of the context its register selects.
+    __device__ __forceinline__ static int
+    queue_of(const int pc, const Regs& R)
+    {
+        (void)R;
+        return pc;
+    }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks (with kStop: also stopping on arrival at block `stop`);
-    // returns the block it stopped at, or kHalt.
-    template <bool kProf, bool kStop = false>
+    // blocks; returns the block it stopped at, or kHalt.
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -78,20 +95,20 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u || (kStop && stop == 0)) return 0;
+        if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 3u);
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r1 = static_cast<unsigned long long>(((R.r2) ? (((unsigned long long)0x1ull)) : (R.r1)));
         if(R.r2) goto L_HALT; else goto L_B1;
     L_B1: // cinit
-        if(budget == 0u || (kStop && stop == 1)) return 1;
+        if(budget == 0u) return 1;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         goto L_B2;
     L_B2: // loop
-        if(budget == 0u || (kStop && stop == 2)) return 2;
+        if(budget == 0u) return 2;
         --budget;
         if constexpr(kProf) count_block(ctx, 4u);
         R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
@@ -104,21 +121,21 @@ struct K
 
     static constexpr unsigned long long kRowBytes = 56ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,
          const unsigned idx, const unsigned tid)
     {
         char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
             reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
             return;
-        case 1:
+        case 1: // cinit
             reinterpret_cast<unsigned long long*>(base + 16ull * cap)[idx] = R.r1;
             reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
             return;
-        case 2:
+        case 2: // loop
             reinterpret_cast<unsigned long long*>(base + 32ull * cap)[idx] = R.r1;
             reinterpret_cast<unsigned long long*>(base + 40ull * cap)[idx] = R.r3;
             reinterpret_cast<unsigned*>(base + 48ull * cap)[idx] = tid;
@@ -128,19 +145,19 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned
-    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,
             const unsigned idx)
     {
         const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
-        case 1:
+        case 1: // cinit
             R.r1 = reinterpret_cast<const unsigned long long*>(base + 16ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
-        case 2:
+        case 2: // loop
             R.r1 = reinterpret_cast<const unsigned long long*>(base + 32ull * cap)[idx];
             R.r3 = reinterpret_cast<const unsigned long long*>(base + 40ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 48ull * cap)[idx];
@@ -192,6 +209,6 @@ cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 
 extern const loom_b200::KernelEntry loom_b200_entry_fac_u64;
 const loom_b200::KernelEntry loom_b200_entry_fac_u64 = {
-    &loom_b200::k_fac_u64::kInfo, loom_b200::k_fac_u64::K::kRowBytes,
+    &loom_b200::k_fac_u64::kInfo, loom_b200::k_fac_u64::K::kRowBytes, 3,
     &loom_b200::k_fac_u64::launch_plain, &loom_b200::k_fac_u64::launch_regroup,
     &loom_b200::k_fac_u64::regroup_occupancy};

@@ -8,10 +8,12 @@ namespace loom_b200 { namespace k_jmp4_u64 {
 
 __constant__ unsigned kInstrTab[5] = {1, 2, 2, 2, 2};
 __constant__ unsigned kLiveTab[5] = {8, 0, 0, 0, 0};
+__constant__ int kQueueBlock[5] = {0, 1, 2, 3, 4};
 
 struct K
 {
     static constexpr int kNumBlocks = 5;
+    static constexpr int kNumQueues = 5;
     struct Regs
     {
         unsigned long long r1; // i: u64
@@ -26,8 +28,7 @@ struct K
     __device__ __forceinline__ static void
     load_in(In& in, const Columns& c, const unsigned long long tid)
     {
-        { const unsigned long long* col = static_cast<const unsigned long long*>(c.p[0]);
-          in.v0 = col ? col[tid] : static_cast<unsigned long long>(tid); }
+        in.v0 = load_input<unsigned long long>(c, 0, tid);
         (void)in; (void)c; (void)tid;
     }
 
@@ -55,17 +56,33 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
-    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
+    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
+    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+
+    static constexpr int kMaxQueuesPerBlock = 1;
+    // j-th queue holding threads that stand at block b (-1: none).
+    __device__ __forceinline__ static int
+    queue_list(const int b, const int j)
+    {
+        return j == 0 ? b : -1;
+    }
+
+    // Queue a thread standing at block pc waits in: the block's own queue,
+    // or for a dispatch block the queue of the context its register selects.
+    __device__ __forceinline__ static int
+    queue_of(const int pc, const Regs& R)
+    {
+        (void)R;
+        return pc;
+    }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks (with kStop: also stopping on arrival at block `stop`);
-    // returns the block it stopped at, or kHalt.
-    template <bool kProf, bool kStop = false>
+    // blocks; returns the block it stopped at, or kHalt.
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -76,7 +93,7 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u || (kStop && stop == 0)) return 0;
+        if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 1u);
         switch(R.r1) {
@@ -87,25 +104,25 @@ struct K
         default: goto L_HALT;
         }
     L_B1: // l0
-        if(budget == 0u || (kStop && stop == 1)) return 1;
+        if(budget == 0u) return 1;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned long long>(((unsigned long long)0x1ull));
         goto L_HALT;
     L_B2: // l1
-        if(budget == 0u || (kStop && stop == 2)) return 2;
+        if(budget == 0u) return 2;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned long long>(((unsigned long long)0x3ull));
         goto L_HALT;
     L_B3: // l2
-        if(budget == 0u || (kStop && stop == 3)) return 3;
+        if(budget == 0u) return 3;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned long long>(((unsigned long long)0x7ull));
         goto L_HALT;
     L_B4: // l3
-        if(budget == 0u || (kStop && stop == 4)) return 4;
+        if(budget == 0u) return 4;
         --budget;
         if constexpr(kProf) count_block(ctx, 2u);
         R.r1 = static_cast<unsigned long long>(((unsigned long long)0xbull));
@@ -116,26 +133,26 @@ struct K
 
     static constexpr unsigned long long kRowBytes = 48ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,
          const unsigned idx, const unsigned tid)
     {
         char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
             reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
             return;
-        case 1:
+        case 1: // l0
             reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
             return;
-        case 2:
+        case 2: // l1
             reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
             return;
-        case 3:
+        case 3: // l2
             reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = tid;
             return;
-        case 4:
+        case 4: // l3
             reinterpret_cast<unsigned*>(base + 40ull * cap)[idx] = tid;
             return;
         default: return;
@@ -143,22 +160,22 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned
-    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,
             const unsigned idx)
     {
         const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
-        case 1:
+        case 1: // l0
             return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
-        case 2:
+        case 2: // l1
             return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
-        case 3:
+        case 3: // l2
             return reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
-        case 4:
+        case 4: // l3
             return reinterpret_cast<const unsigned*>(base + 40ull * cap)[idx];
         default: return 0xffffffffu;
         }
@@ -208,6 +225,6 @@ cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 
 extern const loom_b200::KernelEntry loom_b200_entry_jmp4_u64;
 const loom_b200::KernelEntry loom_b200_entry_jmp4_u64 = {
-    &loom_b200::k_jmp4_u64::kInfo, loom_b200::k_jmp4_u64::K::kRowBytes,
+    &loom_b200::k_jmp4_u64::kInfo, loom_b200::k_jmp4_u64::K::kRowBytes, 5,
     &loom_b200::k_jmp4_u64::launch_plain, &loom_b200::k_jmp4_u64::launch_regroup,
     &loom_b200::k_jmp4_u64::regroup_occupancy};

@@ -38,6 +38,7 @@ extern const loom_b200::KernelEntry loom_b200_entry_rsqrt_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_sct_inv_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_sin_cos_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_slt_inv_u32;
+extern const loom_b200::KernelEntry loom_b200_entry_sphere_pt_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_sqrt_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_trunc_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_union_cmov_f32;
@@ -83,6 +84,7 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_sct_inv_u32,
     &loom_b200_entry_sin_cos_f32,
     &loom_b200_entry_slt_inv_u32,
+    &loom_b200_entry_sphere_pt_f32,
     &loom_b200_entry_sqrt_f32,
     &loom_b200_entry_trunc_f32,
     &loom_b200_entry_union_cmov_f32,
@@ -90,5 +92,5 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 42;
+const int kRegistrySize = 43;
 } // namespace loom_b200

@@ -8,10 +8,12 @@ namespace loom_b200 { namespace k_trunc_f32 {
 
 __constant__ unsigned kInstrTab[1] = {4};
 __constant__ unsigned kLiveTab[1] = {4};
+__constant__ int kQueueBlock[1] = {0};
 
 struct K
 {
     static constexpr int kNumBlocks = 1;
+    static constexpr int kNumQueues = 1;
     struct Regs
     {
         unsigned int r0; // x: u32,f32
@@ -27,8 +29,7 @@ struct K
     __device__ __forceinline__ static void
     load_in(In& in, const Columns& c, const unsigned long long tid)
     {
-        { const float* col = static_cast<const float*>(c.p[0]);
-          in.v0 = col ? col[tid] : static_cast<float>(tid); }
+        in.v0 = load_input<float>(c, 0, tid);
         (void)in; (void)c; (void)tid;
     }
 
@@ -57,24 +58,40 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
-    __device__ __forceinline__ static unsigned live_bytes(const int b) { return kLiveTab[b]; }
+    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
+    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+
+    static constexpr int kMaxQueuesPerBlock = 1;
+    // j-th queue holding threads that stand at block b (-1: none).
+    __device__ __forceinline__ static int
+    queue_list(const int b, const int j)
+    {
+        return j == 0 ? b : -1;
+    }
+
+    // Queue a thread standing at block pc waits in: the block's own queue,
+    // or for a dispatch block the queue of the context its register selects.
+    __device__ __forceinline__ static int
+    queue_of(const int pc, const Regs& R)
+    {
+        (void)R;
+        return pc;
+    }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks (with kStop: also stopping on arrival at block `stop`);
-    // returns the block it stopped at, or kHalt.
-    template <bool kProf, bool kStop = false>
+    // blocks; returns the block it stopped at, or kHalt.
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const int stop = kEmpty)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop;
         switch(entry)
         {
         case 0: goto L_B0;
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u || (kStop && stop == 0)) return 0;
+        if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 4u);
         R.r1 = static_cast<float>(op_trunc(static_cast<float>(bitcast<float>(R.r0))));
@@ -88,13 +105,13 @@ struct K
 
     static constexpr unsigned long long kRowBytes = 8ull;
     __device__ __forceinline__ static void
-    save(const int b, const Regs& R, char* st, const unsigned cap, const unsigned par,
+    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,
          const unsigned idx, const unsigned tid)
     {
         char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r0;
             reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
             return;
@@ -103,13 +120,13 @@ struct K
     }
 
     __device__ __forceinline__ static unsigned
-    restore(const int b, Regs& R, const char* st, const unsigned cap, const unsigned par,
+    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,
             const unsigned idx)
     {
         const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
-        switch(b)
+        switch(q)
         {
-        case 0:
+        case 0: // START
             R.r0 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
             return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
         default: return 0xffffffffu;
@@ -160,6 +177,6 @@ cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
 
 extern const loom_b200::KernelEntry loom_b200_entry_trunc_f32;
 const loom_b200::KernelEntry loom_b200_entry_trunc_f32 = {
-    &loom_b200::k_trunc_f32::kInfo, loom_b200::k_trunc_f32::K::kRowBytes,
+    &loom_b200::k_trunc_f32::kInfo, loom_b200::k_trunc_f32::K::kRowBytes, 1,
     &loom_b200::k_trunc_f32::launch_plain, &loom_b200::k_trunc_f32::launch_regroup,
     &loom_b200::k_trunc_f32::regroup_occupancy};

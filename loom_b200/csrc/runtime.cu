@@ -84,14 +84,13 @@ regroup_reset(RegroupCtl*        ctl,
 
 constexpr unsigned long long kDefaultMaxSteps    = 1ull << 40;
 constexpr unsigned long long kBarrierSpins       = 1ull << 25;
+constexpr unsigned long long kDefaultStateBudget = 8ull << 30; // queue state bytes
 constexpr unsigned           kDefaultPlainBlock  = 256;
 constexpr unsigned           kDefaultRegroupBlock = 256;
 constexpr unsigned           kDefaultUtr         = 16;
 constexpr unsigned           kDefaultPeriod      = 1024;
 constexpr unsigned           kDefaultBurst       = 32;
 constexpr unsigned           kDefaultSpread      = 33;
-constexpr unsigned           kDefaultCatchup     = 4;
-constexpr unsigned           kNoCatchup          = 0xffffffffu;
 } // namespace
 
 struct loom_b200_handle
@@ -116,6 +115,12 @@ struct loom_b200_handle
     unsigned*           d_qcnt  = nullptr;
     unsigned*           d_qhead = nullptr;
     RegroupCtl*         d_ctl   = nullptr;
+
+    // device copies of instance starts and table for launch_host
+    void*  d_starts     = nullptr;
+    size_t starts_bytes = 0;
+    void*  d_table      = nullptr;
+    size_t table_bytes  = 0;
 
     loom_b200_stats stats{};
     unsigned        last_grid     = 0;
@@ -144,17 +149,41 @@ round_cap(uint64_t cap)
     return (cap + 31) / 32 * 32;
 }
 
+/// Threads in flight of a regrouping launch: the requested population, or
+/// as many as the queue state of kDefaultStateBudget bytes holds.
+uint64_t
+population(const loom_b200_handle* h, uint64_t n)
+{
+    uint64_t p = h->opts.population ? h->opts.population : n;
+    const uint64_t fit = kDefaultStateBudget / (2 * h->e->row_bytes) / 32 * 32;
+    if(!h->opts.population && fit && p > fit) p = fit;
+    return round_cap(std::min<uint64_t>(p, n));
+}
+
 int
 ensure_ws(loom_b200_handle* h, uint64_t cap)
 {
     if(cap <= h->ws_cap) return LOOM_B200_OK;
     free_ws(h);
     const KernelEntry& e = *h->e;
-    const uint64_t     B = e.info->num_blocks;
+    const uint64_t     B = e.num_queues;
     LB_CUDA(cudaMalloc(&h->d_state, 2 * e.row_bytes * cap));
     LB_CUDA(cudaMalloc(&h->d_qcnt, 2 * B * sizeof(unsigned)));
     LB_CUDA(cudaMalloc(&h->d_qhead, B * sizeof(unsigned)));
     h->ws_cap = cap;
+    return LOOM_B200_OK;
+}
+
+/// Grows a device buffer to at least `bytes` (contents are not kept).
+int
+grow(void** p, size_t* have, size_t bytes)
+{
+    if(bytes <= *have) return LOOM_B200_OK;
+    cudaFree(*p);
+    *p    = nullptr;
+    *have = 0;
+    LB_CUDA(cudaMalloc(p, bytes));
+    *have = bytes;
     return LOOM_B200_OK;
 }
 
@@ -168,7 +197,6 @@ normalise(loom_b200_opts& o)
     if(o.period == 0) o.period = kDefaultPeriod;
     if(o.burst == 0) o.burst = kDefaultBurst;
     if(o.spread_lanes == 0) o.spread_lanes = kDefaultSpread;
-    if(o.catchup == 0) o.catchup = kDefaultCatchup;
     if(o.max_steps == 0) o.max_steps = kDefaultMaxSteps;
 }
 
@@ -198,40 +226,57 @@ finish_launch(loom_b200_handle* h)
     return status ? LOOM_B200_ERR_DEVICE : LOOM_B200_OK;
 }
 
+/// Launch with every pointer of `L` on the device.
 int
-launch(loom_b200_handle* h,
-       const void* const* in,
-       void* const*       out,
-       uint64_t           n,
-       cudaStream_t       stream)
+launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
 {
     const KernelEntry&           e    = *h->e;
     const loom_b200_kernel_info& info = *e.info;
+    const uint64_t               n    = L.n;
     if(n == 0) return LOOM_B200_OK;
     if(n >= (1ull << 32))
     {
         g_last_error = "at most 2^32 - 1 threads per launch";
         return LOOM_B200_ERR_INVALID;
     }
+    if(info.num_inputs > static_cast<uint32_t>(kMaxIn) ||
+       info.num_inputs + info.num_outputs > static_cast<uint32_t>(kMaxCols))
+    {
+        g_last_error = "too many columns";
+        return LOOM_B200_ERR_INVALID;
+    }
     Columns cols{};
     int     c = 0;
     for(uint32_t i = 0; i < info.num_inputs; ++i)
-        cols.p[c++] = const_cast<void*>(in[i]);
+    {
+        const loom_b200_input& in = L.inputs[i];
+        if(in.form > LOOM_B200_IN_INSTANCE ||
+           (in.form == LOOM_B200_IN_ARRAY && in.ptr == nullptr))
+        {
+            g_last_error = "bad input column";
+            return LOOM_B200_ERR_INVALID;
+        }
+        cols.form[i]  = in.form;
+        cols.value[i] = in.value;
+        cols.p[c++]   = const_cast<void*>(in.ptr);
+    }
     for(uint32_t i = 0; i < info.num_outputs; ++i)
     {
-        if(out[i] == nullptr)
+        if(L.outputs[i] == nullptr)
         {
             g_last_error = "output column is NULL";
             return LOOM_B200_ERR_INVALID;
         }
-        cols.p[c++] = out[i];
+        cols.p[c++] = L.outputs[i];
     }
+    cols.inst_start = reinterpret_cast<const unsigned long long*>(L.instance_starts);
+    cols.num_inst   = L.instance_starts ? L.num_instances : 0u;
+    cols.table      = L.table;
     const loom_b200_opts& o = h->opts;
     if(o.mode == LOOM_B200_REGROUP)
     {
         // the workspace is reallocated only between launches
-        const uint64_t cap =
-            round_cap(o.population ? std::min<uint64_t>(o.population, n) : n);
+        const uint64_t cap = population(h, n);
         if(cap > h->ws_cap)
         {
             LB_CUDA(cudaStreamSynchronize(stream));
@@ -242,13 +287,19 @@ launch(loom_b200_handle* h,
     LB_CUDA(cudaEventRecord(h->ev0, stream));
     if(o.mode == LOOM_B200_REGROUP)
     {
-        const uint64_t cap =
-            round_cap(o.population ? std::min<uint64_t>(o.population, n) : n);
-        int ctas = 0;
-        LB_CUDA(e.regroup_occupancy(static_cast<int>(o.block_size), o.profile != 0, &ctas));
+        const uint64_t cap = population(h, n);
+        // the largest CTA size up to the requested one that fits on an SM
+        unsigned block = o.block_size;
+        int      ctas  = 0;
+        for(;;)
+        {
+            LB_CUDA(e.regroup_occupancy(static_cast<int>(block), o.profile != 0, &ctas));
+            if(ctas > 0 || block <= 32) break;
+            block /= 2;
+        }
         if(ctas <= 0)
         {
-            g_last_error = "regroup kernel does not fit on an SM at this block size";
+            g_last_error = "regroup kernel does not fit on an SM";
             return LOOM_B200_ERR_INVALID;
         }
         if(o.ctas_per_sm) ctas = std::min<int>(ctas, static_cast<int>(o.ctas_per_sm));
@@ -269,16 +320,16 @@ launch(loom_b200_handle* h,
         L.params.period        = o.period;
         L.params.burst         = o.burst;
         L.params.spread        = o.spread_lanes;
-        L.params.catchup       = o.catchup == kNoCatchup ? 0u : o.catchup;
+        L.params.refill        = o.no_refill ? 0u : 1u;
         L.params.prefetch      = o.no_prefetch ? 0u : 1u;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
-        L.block                = o.block_size;
+        L.block                = block;
         L.profile              = o.profile != 0;
         L.stream               = stream;
         regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl,
                                              h->d_qcnt,
                                              h->d_qhead,
-                                             info.num_blocks,
+                                             e.num_queues,
                                              std::min<uint64_t>(n, cap));
         LB_CUDA(cudaGetLastError());
         LB_CUDA(e.regroup(L));
@@ -434,6 +485,8 @@ loom_b200_destroy(loom_b200_handle* h)
     for(void* p: h->d_out) cudaFree(p);
     cudaFree(h->d_status);
     cudaFree(h->d_counters);
+    cudaFree(h->d_starts);
+    cudaFree(h->d_table);
     cudaFree(h->d_ctl);
     if(h->ev0) cudaEventDestroy(h->ev0);
     if(h->ev1) cudaEventDestroy(h->ev1);
@@ -465,13 +518,19 @@ loom_b200_get_opts(const loom_b200_handle* h, loom_b200_opts* opts)
 }
 
 int
-loom_b200_run_host(loom_b200_handle*  h,
-                   const void* const* inputs,
-                   void* const*       outputs,
-                   uint64_t           n)
+loom_b200_launch_device(loom_b200_handle* h, const loom_b200_launch* L, void* stream)
 {
-    if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
+    if(!h || !L || (!L->inputs && h->e->info->num_inputs) || !L->outputs)
         return LOOM_B200_ERR_INVALID;
+    return launch(h, *L, static_cast<cudaStream_t>(stream));
+}
+
+int
+loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L)
+{
+    if(!h || !L || (!L->inputs && h->e->info->num_inputs) || !L->outputs)
+        return LOOM_B200_ERR_INVALID;
+    const uint64_t n = L->n;
     if(n > h->capacity)
     {
         g_last_error = "n exceeds the handle's capacity";
@@ -479,31 +538,69 @@ loom_b200_run_host(loom_b200_handle*  h,
     }
     if(n == 0) return LOOM_B200_OK;
     const loom_b200_kernel_info& info = *h->e->info;
-    std::vector<const void*>     din(info.num_inputs);
+    std::vector<loom_b200_input> din(L->inputs, L->inputs + info.num_inputs);
     for(uint32_t i = 0; i < info.num_inputs; ++i)
-    {
-        if(inputs[i] == nullptr)
-            din[i] = nullptr; // iota
-        else
+        if(din[i].form == LOOM_B200_IN_ARRAY && din[i].ptr)
         {
             LB_CUDA(cudaMemcpyAsync(h->d_in[i],
-                                    inputs[i],
+                                    din[i].ptr,
                                     n * type_bytes(info.input_types[i]),
                                     cudaMemcpyHostToDevice,
                                     h->stream));
-            din[i] = h->d_in[i];
+            din[i].ptr = h->d_in[i];
         }
+    loom_b200_launch D = *L;
+    D.inputs           = din.data();
+    D.outputs          = h->d_out.data();
+    if(L->instance_starts)
+    {
+        const size_t bytes = (static_cast<size_t>(L->num_instances) + 1) * sizeof(uint64_t);
+        int rc = grow(&h->d_starts, &h->starts_bytes, bytes);
+        if(rc) return rc;
+        LB_CUDA(cudaMemcpyAsync(h->d_starts, L->instance_starts, bytes,
+                                cudaMemcpyHostToDevice, h->stream));
+        D.instance_starts = static_cast<const uint64_t*>(h->d_starts);
     }
-    int rc = launch(h, din.data(), h->d_out.data(), n, h->stream);
+    if(L->table)
+    {
+        const size_t bytes = L->table_words * sizeof(uint32_t);
+        int rc = grow(&h->d_table, &h->table_bytes, bytes);
+        if(rc) return rc;
+        LB_CUDA(cudaMemcpyAsync(h->d_table, L->table, bytes, cudaMemcpyHostToDevice,
+                                h->stream));
+        D.table = static_cast<const uint32_t*>(h->d_table);
+    }
+    int rc = launch(h, D, h->stream);
     if(rc) return rc;
     for(uint32_t i = 0; i < info.num_outputs; ++i)
-        LB_CUDA(cudaMemcpyAsync(outputs[i],
+        LB_CUDA(cudaMemcpyAsync(L->outputs[i],
                                 h->d_out[i],
                                 n * type_bytes(info.output_types[i]),
                                 cudaMemcpyDeviceToHost,
                                 h->stream));
     LB_CUDA(cudaStreamSynchronize(h->stream));
     return finish_launch(h);
+}
+
+int
+loom_b200_run_host(loom_b200_handle*  h,
+                   const void* const* inputs,
+                   void* const*       outputs,
+                   uint64_t           n)
+{
+    if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
+        return LOOM_B200_ERR_INVALID;
+    std::vector<loom_b200_input> in(h->e->info->num_inputs);
+    for(size_t i = 0; i < in.size(); ++i)
+        in[i] = loom_b200_input{inputs[i],
+                                inputs[i] ? LOOM_B200_IN_ARRAY : LOOM_B200_IN_IOTA,
+                                0u,
+                                0ull};
+    loom_b200_launch L{};
+    L.inputs  = in.data();
+    L.outputs = outputs;
+    L.n       = n;
+    return loom_b200_launch_host(h, &L);
 }
 
 int
@@ -515,7 +612,17 @@ loom_b200_run_device(loom_b200_handle*  h,
 {
     if(!h || (!inputs && h->e->info->num_inputs) || !outputs)
         return LOOM_B200_ERR_INVALID;
-    return launch(h, inputs, outputs, n, static_cast<cudaStream_t>(stream));
+    std::vector<loom_b200_input> in(h->e->info->num_inputs);
+    for(size_t i = 0; i < in.size(); ++i)
+        in[i] = loom_b200_input{inputs[i],
+                                inputs[i] ? LOOM_B200_IN_ARRAY : LOOM_B200_IN_IOTA,
+                                0u,
+                                0ull};
+    loom_b200_launch L{};
+    L.inputs  = in.data();
+    L.outputs = outputs;
+    L.n       = n;
+    return launch(h, L, static_cast<cudaStream_t>(stream));
 }
 
 int

@@ -34,7 +34,8 @@ struct RegroupLaunch
 struct KernelEntry
 {
     const loom_b200_kernel_info* info;
-    unsigned long long           row_bytes; // queue bytes per entry, summed over blocks
+    unsigned long long           row_bytes;  // queue bytes per entry, summed over queues
+    unsigned                     num_queues; // work queues of the regrouping engine
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
     cudaError_t (*regroup_occupancy)(int block, bool profile, int* ctas_per_sm);

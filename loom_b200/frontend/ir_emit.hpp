@@ -38,6 +38,8 @@
 #include <vm/core.hpp>
 #include <vm/operators.hpp>
 
+#include "b200_ops.hpp"
+
 #include <cstdint>
 #include <cstring>
 #include <sstream>
@@ -289,6 +291,23 @@ struct op_info<loom::vm::ops::pacc<T, I, Acc, Cmp>>
         return std::string(tname_v<T>) + "," + std::string(tname_v<I>) + "," +
                std::string(fname<Acc>::value) + "," +
                std::string(fname<Cmp>::value);
+    }
+    static std::string
+    consts()
+    {
+        return {};
+    }
+};
+
+/// Table lookup extension (b200_ops.hpp): dst <- word idx of the table as T.
+template <typename T>
+struct op_info<loom::vm::b200::ops::tab<T>>
+{
+    static constexpr std::string_view name = "tab";
+    static std::string
+    optype()
+    {
+        return std::string(tname_v<T>);
     }
     static std::string
     consts()

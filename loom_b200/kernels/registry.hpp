@@ -14,6 +14,7 @@
 #include <tests/programs.hpp>
 
 #include "collatz.hpp"
+#include "sphere_pt.hpp"
 
 #include <cstdint>
 
@@ -35,6 +36,7 @@ using std::uint8_t;
     X(fib_u64,            fib_test<std::uint64_t>)                             \
     X(fib_u32,            fib_test<std::uint32_t>)                             \
     X(collatz_u64,        loom::vm::b200::kernels::collatz<std::uint64_t>)     \
+    X(sphere_pt_f32,      loom::vm::b200::kernels::sphere_pt<float>)           \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

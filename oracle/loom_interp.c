@@ -27,7 +27,8 @@
  *   void* li_load(const char* ir_text)               parse; NULL on error
  *   const char* li_error(void)
  *   int   li_run(void* k, const void* const* in, void* const* out,
- *                uint64_t n, uint64_t max_steps, uint64_t* instr_counts)
+ *                uint64_t n, uint64_t max_steps, uint64_t* instr_counts,
+ *                const uint32_t* table)      table: words of the tab op
  *   void  li_free(void* k)
  */
 #define _POSIX_C_SOURCE 200809L
@@ -111,6 +112,7 @@ enum
     OP_SCT,
     OP_SLT,
     OP_PACC,
+    OP_TAB,
     OP_COUNT
 };
 
@@ -120,7 +122,7 @@ static const char* const OPNAMES[] = {
     "le",    "land", "lor",   "lnot", "band",      "bor",   "bxor", "bnot",
     "shl",   "shr",  "abs",   "rsqrt", "max",      "min",   "round", "ceil",
     "floor", "trunc", "sin",  "cos",  "sqrt",      "copysign", "sct", "slt",
-    "pacc"};
+    "pacc",  "tab"};
 
 /* typed value */
 typedef struct
@@ -730,9 +732,9 @@ fp_binop(int op, val a, val b)
     return r;
 }
 
-/* one Compute statement */
+/* one Compute statement; `table` is the word table of the tab extension */
 static int
-compute(const kernel* k, uint64_t* R, const instr* in)
+compute(const kernel* k, uint64_t* R, const instr* in, const uint32_t* table)
 {
     val a[8];
     int na = in->nargs < 8 ? in->nargs : 8;
@@ -834,6 +836,13 @@ compute(const kernel* k, uint64_t* R, const instr* in)
         r = convert(a[1 + ix], t);
         break;
     }
+    case OP_TAB:
+    {
+        /* word idx of the table, read as the op's type (a 32-bit type) */
+        uint64_t idx = convert(a[0], T_U32).v.u;
+        r = from_bits(t, table ? table[idx] : 0u);
+        break;
+    }
     case OP_PACC:
     {
         int it = in->ot[1];
@@ -858,7 +867,8 @@ li_run(void*              kp,
        void* const*       out,
        uint64_t           n,
        uint64_t           max_steps,
-       uint64_t*          instr_counts)
+       uint64_t*          instr_counts,
+       const uint32_t*    table)
 {
     const kernel* k      = kp;
     uint64_t*     R      = calloc(k->nregs + 1, sizeof(uint64_t));
@@ -893,7 +903,7 @@ li_run(void*              kp,
                 const instr* ins = &b->ins[i];
                 ++icount;
                 if(ins->kind == 0)
-                    compute(k, R, ins);
+                    compute(k, R, ins, table);
                 else if(ins->kind == 1)
                     next = ins->targets[0];
                 else

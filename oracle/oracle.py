@@ -91,6 +91,7 @@ def _lib():
             ctypes.c_uint64,
             ctypes.c_uint64,
             ctypes.c_void_p,
+            ctypes.c_void_p,
         ]
         lib.li_free.argtypes = [ctypes.c_void_p]
         _interp_lib = lib
@@ -131,9 +132,10 @@ class Interp:
         n: Optional[int] = None,
         max_steps: int = 1 << 40,
         count_instr: bool = False,
+        table: Optional[np.ndarray] = None,
     ):
         """Returns a list of output arrays (and per-thread instruction counts
-        when ``count_instr``)."""
+        when ``count_instr``).  `table` holds the words of the tab op."""
         if n is None:
             n = len(next(a for a in inputs if a is not None))
         ins = [
@@ -146,8 +148,15 @@ class Interp:
         )
         pout = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
         counts = np.zeros(n, dtype=np.uint64) if count_instr else None
+        tab = None if table is None else np.ascontiguousarray(table, dtype=np.uint32)
         rc = _lib().li_run(
-            self._k, pin, pout, n, max_steps, None if counts is None else counts.ctypes.data
+            self._k,
+            pin,
+            pout,
+            n,
+            max_steps,
+            None if counts is None else counts.ctypes.data,
+            None if tab is None else tab.ctypes.data,
         )
         if rc != 0:
             raise RuntimeError(f"{self.name}: a thread exceeded max_steps")
@@ -162,8 +171,15 @@ def ref_available() -> bool:
     return REF_SO.exists()
 
 
-def ref_run(name: str, inputs: Sequence[Optional[np.ndarray]], n: int, threads: int = 1):
-    """Run Loom's own bse (oracle/_ref/libloomref.so) on threads [0, n)."""
+def ref_run(
+    name: str,
+    inputs: Sequence[Optional[np.ndarray]],
+    n: int,
+    threads: int = 1,
+    table: Optional[np.ndarray] = None,
+):
+    """Run Loom's own bse (oracle/_ref/libloomref.so) on threads [0, n);
+    `table` is bound for the tab op."""
     global _ref_lib
     if _ref_lib is None:
         if not REF_SO.exists():
@@ -176,6 +192,7 @@ def ref_run(name: str, inputs: Sequence[Optional[np.ndarray]], n: int, threads: 
             ctypes.POINTER(ctypes.c_void_p),
             ctypes.c_uint64,
             ctypes.c_int,
+            ctypes.c_void_p,
         ]
         _ref_lib = lib
     text = (IR_DIR / f"{name}.lir").read_text()
@@ -189,7 +206,10 @@ def ref_run(name: str, inputs: Sequence[Optional[np.ndarray]], n: int, threads: 
         *[None if a is None else a.ctypes.data for a in ins]
     )
     pout = (ctypes.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
-    rc = _ref_lib.loom_ref_run(name.encode(), pin, pout, n, threads)
+    tab = None if table is None else np.ascontiguousarray(table, dtype=np.uint32)
+    rc = _ref_lib.loom_ref_run(
+        name.encode(), pin, pout, n, threads, None if tab is None else tab.ctypes.data
+    )
     if rc != 0:
         raise KeyError(f"{name} not in the reference runner")
     return outs
@@ -272,3 +292,33 @@ def uniform_int(seed: int, n: int, lo: int, hi: int) -> np.ndarray:
     hi_bits = (z >> np.uint64(32)) * np.uint64(span)
     lo_bits = ((z & np.uint64(0xFFFFFFFF)) * np.uint64(span)) >> np.uint64(32)
     return ((hi_bits + lo_bits) >> np.uint64(32)) + np.uint64(lo)
+
+
+def expand_inputs(forms, n: int, instance_starts=None, types=None):
+    """Materialises input columns given as arrays or the engine's input forms
+    ("iota", "local_iota", "instance", ("broadcast", value)) so the CPU
+    checkers see exactly what the device threads read."""
+    starts = None if instance_starts is None else np.asarray(instance_starts, dtype=np.uint64)
+    tid = np.arange(n, dtype=np.uint64)
+    inst = (
+        np.zeros(n, dtype=np.uint64)
+        if starts is None
+        else (np.searchsorted(starts, tid, side="right") - 1).astype(np.uint64)
+    )
+    out = []
+    for j, f in enumerate(forms):
+        t = NP_TYPE[types[j]] if types else np.uint32
+        if isinstance(f, np.ndarray):
+            out.append(f)
+        elif f == "iota" or f is None:
+            out.append(tid.astype(t))
+        elif f == "local_iota":
+            base = np.zeros(n, dtype=np.uint64) if starts is None else starts[inst.astype(np.int64)]
+            out.append((tid - base).astype(t))
+        elif f == "instance":
+            out.append(inst.astype(t))
+        elif isinstance(f, tuple) and f[0] == "broadcast":
+            out.append(np.full(n, f[1], dtype=t))
+        else:
+            raise ValueError(f"unknown input form {f!r}")
+    return out

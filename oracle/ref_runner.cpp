@@ -8,7 +8,8 @@
 //
 // C ABI:
 //   int loom_ref_run(const char* kernel, const void* const* inputs,
-//                    void* const* outputs, uint64_t n, int threads)
+//                    void* const* outputs, uint64_t n, int threads,
+//                    const uint32_t* table)
 // runs bse on threads [0, n) split into `threads` contiguous slices (one
 // std::thread each, as Loom's demo spreads pixels over cores,
 // src/smallpt/vm/vm.cpp:66-70).  A NULL input column means "iota".
@@ -50,13 +51,15 @@ input(const void* const* in, std::uint64_t t)
 
 template <typename K, std::size_t... I, std::size_t... O>
 void
-run_slice(const void* const* in,
-          void* const*       out,
-          std::uint64_t      b,
-          std::uint64_t      e,
+run_slice(const void* const*   in,
+          void* const*         out,
+          std::uint64_t        b,
+          std::uint64_t        e,
+          const std::uint32_t* table,
           std::index_sequence<I...>,
           std::index_sequence<O...>)
 {
+    loom::vm::b200::bind_table(table); // the tab extension of this thread
     loom::vm::bse::function<K> f;
     for(std::uint64_t t = b; t < e; ++t)
     {
@@ -70,7 +73,11 @@ run_slice(const void* const* in,
 
 template <typename K>
 void
-run_kernel(const void* const* in, void* const* out, std::uint64_t n, int threads)
+run_kernel(const void* const*   in,
+           void* const*         out,
+           std::uint64_t        n,
+           int                  threads,
+           const std::uint32_t* table)
 {
     constexpr std::size_t ni = loom::typelist::length<typename K::input_vars>;
     constexpr std::size_t no = loom::typelist::length<typename K::output_vars>;
@@ -90,6 +97,7 @@ run_kernel(const void* const* in, void* const* out, std::uint64_t n, int threads
                              out,
                              b,
                              e,
+                             table,
                              std::make_index_sequence<ni>{},
                              std::make_index_sequence<no>{});
             });
@@ -99,17 +107,18 @@ run_kernel(const void* const* in, void* const* out, std::uint64_t n, int threads
 } // namespace
 
 extern "C" int
-loom_ref_run(const char*        kernel,
-             const void* const* inputs,
-             void* const*       outputs,
-             std::uint64_t      n,
-             int                threads)
+loom_ref_run(const char*          kernel,
+             const void* const*   inputs,
+             void* const*         outputs,
+             std::uint64_t        n,
+             int                  threads,
+             const std::uint32_t* table)
 {
-#define LOOM_REF_CASE(NAME, ...)                                  \
-    if(std::strcmp(kernel, #NAME) == 0)                           \
-    {                                                             \
-        run_kernel<__VA_ARGS__>(inputs, outputs, n, threads);     \
-        return 0;                                                 \
+#define LOOM_REF_CASE(NAME, ...)                                         \
+    if(std::strcmp(kernel, #NAME) == 0)                                  \
+    {                                                                    \
+        run_kernel<__VA_ARGS__>(inputs, outputs, n, threads, table);     \
+        return 0;                                                        \
     }
     LOOM_B200_KERNELS(LOOM_REF_CASE)
 #undef LOOM_REF_CASE

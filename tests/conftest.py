@@ -25,6 +25,18 @@ def cuda_available() -> bool:
 
 
 @pytest.fixture(scope="session")
+def golden_extra():
+    """Table and instance offsets of a golden fixture (None when absent)."""
+    import numpy as np
+
+    def load(name):
+        z = np.load(ROOT / "tests" / "golden" / f"{name}.npz")
+        return {k: z[k] for k in ("table", "starts") if k in z.files}
+
+    return load
+
+
+@pytest.fixture(scope="session")
 def golden():
     """Loads tests/golden/<kernel>.npz as (inputs, outputs)."""
     import numpy as np

@@ -44,7 +44,36 @@ def _ir_io(name: str):
     return ins, outs
 
 
+def make_pt(name: str) -> pathlib.Path:
+    """Path tracer fixtures: a small Cornell-box render and a batch of three
+    random-scene requests in one launch, with their table and instance
+    offsets."""
+    import numpy as np
+
+    from loom_b200 import scenes as S
+
+    rng = np.random.default_rng(SEED)
+    reqs = [S.cornell_request(32, 24, 4, seed=11)]
+    for k in range(3):
+        r = S.random_request(rng, seed=100 + k)
+        r.width, r.height, r.spp = 16, 16, 4
+        reqs.append(r)
+    table, starts = S.pack(reqs)
+    n = int(starts[-1])
+    ins = O.expand_inputs(["instance", "local_iota"], n, starts, ["u32", "u32"])
+    outs = O.ref_run(name, ins, n, threads=4, table=table)
+    arrays = {f"in{i}": a for i, a in enumerate(ins)}
+    arrays.update({f"out{j}": a for j, a in enumerate(outs)})
+    arrays["table"] = table
+    arrays["starts"] = starts
+    path = HERE / f"{name}.npz"
+    np.savez_compressed(path, **arrays)
+    return path
+
+
 def make(name: str) -> pathlib.Path:
+    if name.startswith("sphere_pt"):
+        return make_pt(name)
     ins_t, _ = _ir_io(name)
     n = SIZES.get(name, DEFAULT_N)
     ins = D.inputs_for(name, n, SEED, ins_t)

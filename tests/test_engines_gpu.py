@@ -35,13 +35,47 @@ def _check(name, got, want):
 
 @pytest.mark.parametrize("mode", ["plain", "regroup"])
 @pytest.mark.parametrize("name", KERNELS)
-def test_engine_matches_loom_bse(name, mode, golden):
+def test_engine_matches_loom_bse(name, mode, golden, golden_extra):
     ins, outs = golden(name)
-    with api.Function(name, len(ins[0]), mode) as f:
-        got = _as_list(f(*ins))
+    extra = golden_extra(name)
+    n = len(ins[0])
+    with api.Function(name, n, mode) as f:
+        if "table" in extra:
+            got = _as_list(f.launch_host(ins, n, table=extra["table"]))
+        else:
+            got = _as_list(f(*ins))
         s = f.stats(raise_on_device_error=True)
     _check(name, got, outs)
-    assert s["threads"] == len(ins[0])
+    assert s["threads"] == n
+
+
+@pytest.mark.parametrize("mode", ["plain", "regroup"])
+def test_path_tracer_instance_forms(mode, golden, golden_extra):
+    """The batched path-tracing fixture (a Cornell render and three random
+    scenes in one launch) with (instance, sample) computed on the device
+    from the instance offsets instead of input arrays."""
+    name = "sphere_pt_f32"
+    ins, outs = golden(name)
+    extra = golden_extra(name)
+    n = len(ins[0])
+    with api.Function(name, n, mode) as f:
+        got = _as_list(
+            f.launch_host(
+                [api.Instance(), api.LocalIota()],
+                n,
+                instance_starts=extra["starts"],
+                table=extra["table"],
+            )
+        )
+        f.stats(raise_on_device_error=True)
+    _check(name, got, outs)
+
+
+def test_broadcast_input_form(golden):
+    ins, outs = golden("collatz_u64")
+    with api.Function("collatz_u64", 64, "regroup") as f:
+        got = f.launch_host([api.Broadcast(27, "u64")], 64)
+    assert (got == 111).all()
 
 
 REGROUP_VARIANTS = [
@@ -52,18 +86,25 @@ REGROUP_VARIANTS = [
     dict(population=100),
     dict(population=1000, utr_lanes=24),
     dict(prefetch=False, period=5),
-    dict(burst=1, catchup=0xFFFFFFFF, spread_lanes=33),
+    dict(burst=1, refill=False, spread_lanes=33),
     dict(burst=64, spread_lanes=1, utr_lanes=1),
     dict(ctas_per_sm=1, population=37),
+    dict(burst=1, utr_lanes=4, population=64),
 ]
 
 
 @pytest.mark.parametrize("variant", REGROUP_VARIANTS, ids=lambda v: ",".join(f"{k}={x}" for k, x in v.items()))
-@pytest.mark.parametrize("name", ["fib_u64", "collatz_u64", "fac_u64", "jmp4_u64", "union_cmov_f32", "slt_inv_u32"])
-def test_regroup_options_keep_results(name, variant, golden):
+@pytest.mark.parametrize(
+    "name", ["fib_u64", "collatz_u64", "fac_u64", "jmp4_u64", "union_cmov_f32", "slt_inv_u32", "sphere_pt_f32"]
+)
+def test_regroup_options_keep_results(name, variant, golden, golden_extra):
     ins, outs = golden(name)
+    extra = golden_extra(name)
     with api.Function(name, len(ins[0]), "regroup", **variant) as f:
-        got = _as_list(f(*ins))
+        if "table" in extra:
+            got = _as_list(f.launch_host(ins, len(ins[0]), table=extra["table"]))
+        else:
+            got = _as_list(f(*ins))
         s = f.stats(raise_on_device_error=True)
     _check(name, got, outs)
     assert s["threads"] == len(ins[0])
