@@ -65,7 +65,7 @@ enum loom_b200_type
 typedef struct loom_b200_kernel_info
 {
     const char*        name;          /* registry name, e.g. "fib_u64" */
-    const char*        ir_digest;     /* sha256 prefix of the kernel's text IR */
+    const char*        ir_digest;     /* structural digest of the text IR (16 hex) */
     uint32_t           num_inputs;
     uint32_t           num_outputs;
     const int*         input_types;   /* enum loom_b200_type */
@@ -169,6 +169,10 @@ const char* loom_b200_error_string(int code);
 int         loom_b200_kernel_count(void);
 int         loom_b200_kernel_get(int index, const loom_b200_kernel_info** info);
 int         loom_b200_kernel_find(const char* name, const loom_b200_kernel_info** info);
+/* Finds a compiled kernel by the structural digest of its IR (16 hex
+ * digits, loom_b200/frontend/ir_emit.hpp: structural_digest): how the C++
+ * front end binds a Loom kernel type to its compiled code. */
+int         loom_b200_kernel_find_digest(const char* digest, const loom_b200_kernel_info** info);
 
 /* ------------------------------------------------------------ function
  * Replaces vm::cuda::function<K>(n)(inputs...) (Loom src/vm/cuda.hpp:

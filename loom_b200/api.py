@@ -186,6 +186,7 @@ EXPORTS = [
     "loom_b200_kernel_count",
     "loom_b200_kernel_get",
     "loom_b200_kernel_find",
+    "loom_b200_kernel_find_digest",
     "loom_b200_create",
     "loom_b200_destroy",
     "loom_b200_set_opts",
@@ -218,6 +219,7 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_kernel_count.restype = ctypes.c_int
     L.loom_b200_kernel_get.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
     L.loom_b200_kernel_find.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
+    L.loom_b200_kernel_find_digest.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
     L.loom_b200_create.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(Opts), ctypes.POINTER(vp)]
     L.loom_b200_destroy.argtypes = [vp]
     L.loom_b200_set_opts.argtypes = [vp, ctypes.POINTER(Opts)]

@@ -178,7 +178,7 @@ class Kernel:
         return None
 
     def digest(self) -> str:
-        return hashlib.sha256(self.text.encode()).hexdigest()[:16]
+        return structural_digest(self.text)
 
     def instr_counts(self) -> List[int]:
         return [len(b.instrs) for b in self.blocks]
@@ -367,6 +367,20 @@ class Kernel:
         for li in live_in:
             s |= li
         return sorted(s)
+
+
+def structural_digest(text: str) -> str:
+    """FNV-1a (64-bit) of the IR without its `kernel <name>` line, as 16 hex
+    digits: two kernel types with the same program get the same digest
+    whatever they are called (the C++ front end computes the same value)."""
+    h = 0xCBF29CE484222325
+    for ln in text.splitlines(keepends=True):
+        if ln.startswith("kernel "):
+            continue
+        for byte in ln.encode():
+            h ^= byte
+            h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return f"{h:016x}"
 
 
 # ---------------------------------------------------------------- parsing

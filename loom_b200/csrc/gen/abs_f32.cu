@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/abs_f32.lir.
-// Kernel IR digest 6678ab5136a149ef; regenerate instead of editing.
+// Kernel IR digest b8f9f3e71f3dd087; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -139,7 +139,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "abs_f32", "6678ab5136a149ef", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "abs_f32", "b8f9f3e71f3dd087", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 4u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

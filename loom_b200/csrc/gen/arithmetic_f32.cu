@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/arithmetic_f32.lir.
-// Kernel IR digest 7f0175ddfc4a3081; regenerate instead of editing.
+// Kernel IR digest 227cde21b6ec745c; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -161,7 +161,7 @@ const uint32_t kInstrs[] = {8};
 const uint32_t kLive[] = {12};
 
 const loom_b200_kernel_info kInfo = {
-    "arithmetic_f32", "7f0175ddfc4a3081", 3u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "arithmetic_f32", "227cde21b6ec745c", 3u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 4u, 16u, 3u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/arithmetic_f64.lir.
-// Kernel IR digest 69afbd9d697bba4a; regenerate instead of editing.
+// Kernel IR digest 4932865793b0f1f5; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -161,7 +161,7 @@ const uint32_t kInstrs[] = {8};
 const uint32_t kLive[] = {24};
 
 const loom_b200_kernel_info kInfo = {
-    "arithmetic_f64", "69afbd9d697bba4a", 3u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "arithmetic_f64", "4932865793b0f1f5", 3u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 4u, 32u, 3u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bit_and_u32.lir.
-// Kernel IR digest 7cd157cc624a6a15; regenerate instead of editing.
+// Kernel IR digest 9d0c304ca08325e7; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "bit_and_u32", "7cd157cc624a6a15", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bit_and_u32", "9d0c304ca08325e7", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

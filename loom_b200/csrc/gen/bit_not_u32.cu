@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bit_not_u32.lir.
-// Kernel IR digest 29fbc0dbc6ab9c88; regenerate instead of editing.
+// Kernel IR digest 32c0b16cfd4ac9d0; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "bit_not_u32", "29fbc0dbc6ab9c88", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bit_not_u32", "32c0b16cfd4ac9d0", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 4u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bit_not_u8.lir.
-// Kernel IR digest 8f8bb2fe1b43cd02; regenerate instead of editing.
+// Kernel IR digest ed1172c51caee85e; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {1};
 
 const loom_b200_kernel_info kInfo = {
-    "bit_not_u8", "8f8bb2fe1b43cd02", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bit_not_u8", "ed1172c51caee85e", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 1u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

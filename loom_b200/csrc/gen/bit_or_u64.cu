@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bit_or_u64.lir.
-// Kernel IR digest 882681fe8e0dfa04; regenerate instead of editing.
+// Kernel IR digest d764855eafbf747f; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {16};
 
 const loom_b200_kernel_info kInfo = {
-    "bit_or_u64", "882681fe8e0dfa04", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bit_or_u64", "d764855eafbf747f", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bit_xor_u16.lir.
-// Kernel IR digest 5da17235c234c9aa; regenerate instead of editing.
+// Kernel IR digest 76ca05cfe2d39503; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "bit_xor_u16", "5da17235c234c9aa", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bit_xor_u16", "76ca05cfe2d39503", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 4u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

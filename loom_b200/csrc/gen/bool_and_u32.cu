@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bool_and_u32.lir.
-// Kernel IR digest 7e841cddab8ecc10; regenerate instead of editing.
+// Kernel IR digest 3877edb5323e72d7; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -146,7 +146,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "bool_and_u32", "7e841cddab8ecc10", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bool_and_u32", "3877edb5323e72d7", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

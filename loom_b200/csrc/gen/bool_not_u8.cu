@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bool_not_u8.lir.
-// Kernel IR digest 0e4b2e6e6d7d7aa0; regenerate instead of editing.
+// Kernel IR digest 8595b2d0cdb804ca; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -139,7 +139,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {1};
 
 const loom_b200_kernel_info kInfo = {
-    "bool_not_u8", "0e4b2e6e6d7d7aa0", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bool_not_u8", "8595b2d0cdb804ca", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 1u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

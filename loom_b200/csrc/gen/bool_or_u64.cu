@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/bool_or_u64.lir.
-// Kernel IR digest de3775e3db5d49f2; regenerate instead of editing.
+// Kernel IR digest ba7db244ac54fe19; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -146,7 +146,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {16};
 
 const loom_b200_kernel_info kInfo = {
-    "bool_or_u64", "de3775e3db5d49f2", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "bool_or_u64", "ba7db244ac54fe19", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/ceilfloor_f32.lir.
-// Kernel IR digest 44b1a0e6dba880da; regenerate instead of editing.
+// Kernel IR digest 342b9fa6529f61be; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -142,7 +142,7 @@ const uint32_t kInstrs[] = {3};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "ceilfloor_f32", "44b1a0e6dba880da", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "ceilfloor_f32", "342b9fa6529f61be", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

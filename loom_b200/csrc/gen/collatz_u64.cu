@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/collatz_u64.lir.
-// Kernel IR digest 4d4fd74f333fab47; regenerate instead of editing.
+// Kernel IR digest 1d3a9b27bd054717; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -171,7 +171,7 @@ const uint32_t kInstrs[] = {3, 8};
 const uint32_t kLive[] = {8, 12};
 
 const loom_b200_kernel_info kInfo = {
-    "collatz_u64", "4d4fd74f333fab47", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "collatz_u64", "1d3a9b27bd054717", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     2u, 7u, 52u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

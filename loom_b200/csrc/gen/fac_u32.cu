@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/fac_u32.lir.
-// Kernel IR digest 2d253d4c9cb61748; regenerate instead of editing.
+// Kernel IR digest 65a54b87b1c17409; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -175,7 +175,7 @@ const uint32_t kInstrs[] = {3, 2, 4};
 const uint32_t kLive[] = {4, 4, 8};
 
 const loom_b200_kernel_info kInfo = {
-    "fac_u32", "2d253d4c9cb61748", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "fac_u32", "65a54b87b1c17409", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 4u, 16u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

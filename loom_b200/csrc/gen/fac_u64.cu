@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/fac_u64.lir.
-// Kernel IR digest a649e9040b0c2ffa; regenerate instead of editing.
+// Kernel IR digest 6ae155bc014b7b7e; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -175,7 +175,7 @@ const uint32_t kInstrs[] = {3, 2, 4};
 const uint32_t kLive[] = {8, 8, 16};
 
 const loom_b200_kernel_info kInfo = {
-    "fac_u64", "a649e9040b0c2ffa", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "fac_u64", "6ae155bc014b7b7e", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 4u, 32u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/fib_u32.lir.
-// Kernel IR digest b58369e636389a54; regenerate instead of editing.
+// Kernel IR digest 4878b52b2b7bd460; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -189,7 +189,7 @@ const uint32_t kInstrs[] = {3, 4, 6};
 const uint32_t kLive[] = {4, 4, 16};
 
 const loom_b200_kernel_info kInfo = {
-    "fib_u32", "b58369e636389a54", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "fib_u32", "4878b52b2b7bd460", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 7u, 28u, 4u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

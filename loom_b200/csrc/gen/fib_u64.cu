@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/fib_u64.lir.
-// Kernel IR digest bb1806e2e217b1f7; regenerate instead of editing.
+// Kernel IR digest b3270907704ae138; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -189,7 +189,7 @@ const uint32_t kInstrs[] = {3, 4, 6};
 const uint32_t kLive[] = {8, 8, 32};
 
 const loom_b200_kernel_info kInfo = {
-    "fib_u64", "bb1806e2e217b1f7", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "fib_u64", "b3270907704ae138", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 7u, 56u, 4u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

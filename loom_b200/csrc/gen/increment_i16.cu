@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/increment_i16.lir.
-// Kernel IR digest 47acaf53616a6272; regenerate instead of editing.
+// Kernel IR digest 017b81187c11eef8; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {2};
 
 const loom_b200_kernel_info kInfo = {
-    "increment_i16", "47acaf53616a6272", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "increment_i16", "017b81187c11eef8", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 2u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/increment_i32.lir.
-// Kernel IR digest 9011c975a7b242bd; regenerate instead of editing.
+// Kernel IR digest 8fce5d89a7ace4d6; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "increment_i32", "9011c975a7b242bd", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "increment_i32", "8fce5d89a7ace4d6", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 4u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/increment_u64.lir.
-// Kernel IR digest 01b36c54976f08ea; regenerate instead of editing.
+// Kernel IR digest 5b5ab17c9e3bc116; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "increment_u64", "01b36c54976f08ea", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "increment_u64", "5b5ab17c9e3bc116", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/increment_u8.lir.
-// Kernel IR digest d231cc5b05a28c5f; regenerate instead of editing.
+// Kernel IR digest 8d528a8476d61cbb; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -138,7 +138,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {1};
 
 const loom_b200_kernel_info kInfo = {
-    "increment_u8", "d231cc5b05a28c5f", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "increment_u8", "8d528a8476d61cbb", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 1u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/jmp4_f32.lir.
-// Kernel IR digest ba086766363ef9c9; regenerate instead of editing.
+// Kernel IR digest 17430c478d6ba619; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -191,7 +191,7 @@ const uint32_t kInstrs[] = {1, 2, 2, 2, 2};
 const uint32_t kLive[] = {4, 0, 0, 0, 0};
 
 const loom_b200_kernel_info kInfo = {
-    "jmp4_f32", "ba086766363ef9c9", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "jmp4_f32", "17430c478d6ba619", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     5u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

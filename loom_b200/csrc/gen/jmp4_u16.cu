@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/jmp4_u16.lir.
-// Kernel IR digest 60352a890be18ac3; regenerate instead of editing.
+// Kernel IR digest 32b4dc4a191cac25; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -191,7 +191,7 @@ const uint32_t kInstrs[] = {1, 2, 2, 2, 2};
 const uint32_t kLive[] = {2, 0, 0, 0, 0};
 
 const loom_b200_kernel_info kInfo = {
-    "jmp4_u16", "60352a890be18ac3", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "jmp4_u16", "32b4dc4a191cac25", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     5u, 2u, 4u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/jmp4_u64.lir.
-// Kernel IR digest a6b0e2b9c3659406; regenerate instead of editing.
+// Kernel IR digest 6908d41f2ca4fd33; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -191,7 +191,7 @@ const uint32_t kInstrs[] = {1, 2, 2, 2, 2};
 const uint32_t kLive[] = {8, 0, 0, 0, 0};
 
 const loom_b200_kernel_info kInfo = {
-    "jmp4_u64", "a6b0e2b9c3659406", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "jmp4_u64", "6908d41f2ca4fd33", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     5u, 2u, 16u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

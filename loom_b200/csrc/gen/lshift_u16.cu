@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/lshift_u16.lir.
-// Kernel IR digest ae20da1d8bb81b44; regenerate instead of editing.
+// Kernel IR digest 2f91f9a7a6b09aa9; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "lshift_u16", "ae20da1d8bb81b44", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "lshift_u16", "2f91f9a7a6b09aa9", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 4u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

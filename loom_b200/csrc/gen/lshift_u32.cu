@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/lshift_u32.lir.
-// Kernel IR digest dabc96684c218d4e; regenerate instead of editing.
+// Kernel IR digest a3e81060ee432851; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "lshift_u32", "dabc96684c218d4e", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "lshift_u32", "a3e81060ee432851", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/lshift_u64.lir.
-// Kernel IR digest c6a6fddaf36b9bde; regenerate instead of editing.
+// Kernel IR digest 60e41cb0162bd745; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {16};
 
 const loom_b200_kernel_info kInfo = {
-    "lshift_u64", "c6a6fddaf36b9bde", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "lshift_u64", "60e41cb0162bd745", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

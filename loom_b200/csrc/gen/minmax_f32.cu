@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/minmax_f32.lir.
-// Kernel IR digest 71302e45c213a19e; regenerate instead of editing.
+// Kernel IR digest a5ab18eb1110ed37; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -153,7 +153,7 @@ const uint32_t kInstrs[] = {3};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "minmax_f32", "71302e45c213a19e", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "minmax_f32", "a5ab18eb1110ed37", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 5u, 20u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

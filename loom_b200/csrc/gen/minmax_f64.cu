@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/minmax_f64.lir.
-// Kernel IR digest 7b49318e5ff56457; regenerate instead of editing.
+// Kernel IR digest 27fcd9355d465bbc; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -153,7 +153,7 @@ const uint32_t kInstrs[] = {3};
 const uint32_t kLive[] = {16};
 
 const loom_b200_kernel_info kInfo = {
-    "minmax_f64", "7b49318e5ff56457", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "minmax_f64", "27fcd9355d465bbc", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 5u, 40u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/rshift_u16.lir.
-// Kernel IR digest 89c718dba79550fe; regenerate instead of editing.
+// Kernel IR digest 09697ab7c643153f; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "rshift_u16", "89c718dba79550fe", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "rshift_u16", "09697ab7c643153f", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 4u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/rshift_u64.lir.
-// Kernel IR digest 015fa7247a79c1db; regenerate instead of editing.
+// Kernel IR digest 5b3d545f1aa30a9b; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {1};
 const uint32_t kLive[] = {16};
 
 const loom_b200_kernel_info kInfo = {
-    "rshift_u64", "015fa7247a79c1db", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "rshift_u64", "5b3d545f1aa30a9b", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 2u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/rsqrt_f32.lir.
-// Kernel IR digest 51b91aad49267870; regenerate instead of editing.
+// Kernel IR digest 1b4f87f6c3b5ebba; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -145,7 +145,7 @@ const uint32_t kInstrs[] = {6};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "rsqrt_f32", "51b91aad49267870", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "rsqrt_f32", "1b4f87f6c3b5ebba", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

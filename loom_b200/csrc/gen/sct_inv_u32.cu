@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/sct_inv_u32.lir.
-// Kernel IR digest f7f901a8b0ea2bb5; regenerate instead of editing.
+// Kernel IR digest 9f3afb7c761fec65; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -142,7 +142,7 @@ const uint32_t kInstrs[] = {3};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "sct_inv_u32", "f7f901a8b0ea2bb5", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "sct_inv_u32", "9f3afb7c761fec65", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

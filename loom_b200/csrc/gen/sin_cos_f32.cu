@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/sin_cos_f32.lir.
-// Kernel IR digest 5f27598684ec4cd4; regenerate instead of editing.
+// Kernel IR digest 914e172005128d9b; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -147,7 +147,7 @@ const uint32_t kInstrs[] = {8};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "sin_cos_f32", "5f27598684ec4cd4", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "sin_cos_f32", "914e172005128d9b", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/slt_inv_u32.lir.
-// Kernel IR digest a39f4d5b8f98b7f4; regenerate instead of editing.
+// Kernel IR digest 4406be6c24fa7cce; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -154,7 +154,7 @@ const uint32_t kInstrs[] = {7};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "slt_inv_u32", "a39f4d5b8f98b7f4", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "slt_inv_u32", "4406be6c24fa7cce", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 6u, 24u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/sphere_pt_f32.lir.
-// Kernel IR digest 212cbadb212691aa; regenerate instead of editing.
+// Kernel IR digest 144eab9a4253b9da; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -2655,7 +2655,7 @@ const uint32_t kInstrs[] = {32, 63, 5, 38, 2, 28, 4, 3, 2, 2, 4, 4, 18, 5, 26, 2
 const uint32_t kLive[] = {164, 132, 176, 192, 184, 184, 36, 216, 216, 216, 192, 192, 188, 188, 192, 216, 224, 176, 220, 208, 192, 188, 164, 220};
 
 const loom_b200_kernel_info kInfo = {
-    "sphere_pt_f32", "212cbadb212691aa", 2u, 3u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "sphere_pt_f32", "144eab9a4253b9da", 2u, 3u, kInTypes, kOutTypes, kInNames, kOutNames,
     24u, 134u, 536u, 71u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

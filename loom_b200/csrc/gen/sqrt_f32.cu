@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/sqrt_f32.lir.
-// Kernel IR digest a188f807ee8cd48b; regenerate instead of editing.
+// Kernel IR digest dc159108ec322c7b; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -144,7 +144,7 @@ const uint32_t kInstrs[] = {5};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "sqrt_f32", "a188f807ee8cd48b", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "sqrt_f32", "dc159108ec322c7b", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

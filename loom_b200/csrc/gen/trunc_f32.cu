@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/trunc_f32.lir.
-// Kernel IR digest 1ae64e616ed1c4e8; regenerate instead of editing.
+// Kernel IR digest 724f5bc005faca49; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -143,7 +143,7 @@ const uint32_t kInstrs[] = {4};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "trunc_f32", "1ae64e616ed1c4e8", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "trunc_f32", "724f5bc005faca49", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/union_cmov_f32.lir.
-// Kernel IR digest 2a8ca2b8398d459d; regenerate instead of editing.
+// Kernel IR digest 8b9f96f35e3d727e; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -141,7 +141,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "union_cmov_f32", "2a8ca2b8398d459d", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "union_cmov_f32", "8b9f96f35e3d727e", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/union_cmov_f64.lir.
-// Kernel IR digest 236dccde9d04baef; regenerate instead of editing.
+// Kernel IR digest 2f16efd86241f4d9; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -141,7 +141,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {8};
 
 const loom_b200_kernel_info kInfo = {
-    "union_cmov_f64", "236dccde9d04baef", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "union_cmov_f64", "2f16efd86241f4d9", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

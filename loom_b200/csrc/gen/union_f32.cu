@@ -1,5 +1,5 @@
 // Generated by loom_b200.codegen from loom_b200/ir/union_f32.lir.
-// Kernel IR digest 3c99e81949745f96; regenerate instead of editing.
+// Kernel IR digest bb103b6f74ec74c5; regenerate instead of editing.
 #include "../engine/plain.cuh"
 #include "../engine/regroup.cuh"
 #include "../runtime_iface.h"
@@ -141,7 +141,7 @@ const uint32_t kInstrs[] = {2};
 const uint32_t kLive[] = {4};
 
 const loom_b200_kernel_info kInfo = {
-    "union_f32", "3c99e81949745f96", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
+    "union_f32", "bb103b6f74ec74c5", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -414,6 +414,19 @@ loom_b200_kernel_find(const char* name, const loom_b200_kernel_info** info)
 }
 
 int
+loom_b200_kernel_find_digest(const char* digest, const loom_b200_kernel_info** info)
+{
+    if(!digest || !info) return LOOM_B200_ERR_INVALID;
+    for(int i = 0; i < kRegistrySize; ++i)
+        if(std::strcmp(kRegistry[i]->info->ir_digest, digest) == 0)
+        {
+            *info = kRegistry[i]->info;
+            return LOOM_B200_OK;
+        }
+    return LOOM_B200_ERR_NOT_FOUND;
+}
+
+int
 loom_b200_create(const char*           kernel,
                  uint64_t              capacity,
                  const loom_b200_opts* opts,

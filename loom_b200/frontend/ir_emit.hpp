@@ -41,6 +41,7 @@
 #include "b200_ops.hpp"
 
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <sstream>
 #include <string>
@@ -469,5 +470,38 @@ std::string
 emit(std::string_view name)
 {
     return emitter<K>::emit(name);
+}
+
+/// @brief FNV-1a (64-bit) of the IR text without its `kernel` line, as 16
+/// hex digits: identifies the program independently of its registry name.
+inline std::string
+structural_digest(std::string_view text)
+{
+    std::uint64_t h = 0xcbf29ce484222325ull;
+    std::size_t   pos = 0;
+    while(pos < text.size())
+    {
+        std::size_t end = text.find('\n', pos);
+        end             = end == std::string_view::npos ? text.size() : end + 1;
+        const std::string_view ln = text.substr(pos, end - pos);
+        if(ln.substr(0, 7) != "kernel ")
+            for(const unsigned char c: ln)
+            {
+                h ^= c;
+                h *= 0x100000001b3ull;
+            }
+        pos = end;
+    }
+    char buf[17];
+    std::snprintf(buf, sizeof buf, "%016llx", static_cast<unsigned long long>(h));
+    return buf;
+}
+
+/// @brief Structural digest of kernel @p K.
+template <Kernel K>
+std::string
+digest()
+{
+    return structural_digest(emit<K>(""));
 }
 } // namespace loom::vm::b200::ir

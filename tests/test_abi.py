@@ -46,6 +46,25 @@ def test_registry_matches_ir():
         assert info.state_size == sum(r.nbytes for r in k.regs)
 
 
+def test_find_by_structural_digest():
+    """The C++ front end binds a kernel type by the digest of its IR: every
+    compiled kernel is found under its own digest, and digests are unique."""
+    import ctypes
+
+    L = api.lib()
+    digests = {}
+    for n in api.kernels():
+        d = ir.load(n).digest()
+        assert re.fullmatch(r"[0-9a-f]{16}", d), d
+        assert d not in digests, (n, digests.get(d))
+        digests[d] = n
+        p = ctypes.POINTER(api.KernelInfoC)()
+        assert L.loom_b200_kernel_find_digest(d.encode(), ctypes.byref(p)) == 0
+        assert p.contents.name.decode() == n
+    p = ctypes.POINTER(api.KernelInfoC)()
+    assert L.loom_b200_kernel_find_digest(b"0000000000000000", ctypes.byref(p)) == api.ERR_NOT_FOUND
+
+
 def test_unknown_kernel_is_not_found():
     with pytest.raises(api.LoomError) as e:
         api.info("no_such_kernel")
