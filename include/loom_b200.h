@@ -218,6 +218,43 @@ int loom_b200_sync(loom_b200_handle* h);
 int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);
 int loom_b200_reset_stats(loom_b200_handle* h);
 
+/* ------------------------------------------------------------ no allocation
+ * No counterpart in the reference: Loom's backends allocate their device
+ * memory themselves.
+ *
+ * Runs `kernel` on the regrouping engine like loom_b200_launch_device, but
+ * allocates nothing: no cudaMalloc, no cudaFree, no handle.  It is for
+ * callers that must not allocate device memory at the point of the call,
+ * for instance a plugin inside a host whose caching allocator or memory pool
+ * already holds the free memory (cudaMalloc would fail there), or code that
+ * must not stall on cudaMalloc's implicit device synchronisation.  The
+ * caller passes device pointers for every input, output, instance offset
+ * and table of `L`; the engine's queues and control words live in a fixed
+ * device array of LOOM_B200_STATIC_SCRATCH_BYTES that each GPU which loads
+ * this library holds until the process exits.
+ *
+ * Limits: at most 2^32 - 1 threads; the threads in flight (`population` of
+ * `opts`, or, when that is 0, as many as the array holds) need 2 x row
+ * bytes of queue state each (a few tens of bytes for small kernels, 2832 for
+ * sphere_pt_f32), and a population the array cannot hold is refused with
+ * LOOM_B200_ERR_BUDGET.  `opts` may be NULL (defaults of loom_b200_create);
+ * its mode, profile and fault_phantom_ctas fields are ignored.
+ *
+ * The first call on a device looks up the array's device address (and so
+ * loads it onto that device): make that first call before any stream
+ * capture.  Every call shares the array and clears what must start at zero;
+ * calls whose launches overlap on the GPU (other streams, other host
+ * threads) race on it.  The call returns after the launch finished on
+ * `stream` (NULL: the CUDA default stream); *status_out (may be NULL)
+ * receives the device status bits, and a non-zero status returns
+ * LOOM_B200_ERR_DEVICE. */
+#define LOOM_B200_STATIC_SCRATCH_BYTES (64ull << 20)
+int loom_b200_launch_static(const char*             kernel,
+                            const loom_b200_launch* L,
+                            const loom_b200_opts*   opts,
+                            void*                   stream,
+                            uint32_t*               status_out);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -198,6 +198,7 @@ EXPORTS = [
     "loom_b200_sync",
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
+    "loom_b200_launch_static",
 ]
 
 
@@ -231,6 +232,13 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_sync.argtypes = [vp]
     L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
     L.loom_b200_reset_stats.argtypes = [vp]
+    L.loom_b200_launch_static.argtypes = [
+        ctypes.c_char_p,
+        ctypes.POINTER(LaunchC),
+        ctypes.POINTER(Opts),
+        vp,
+        ctypes.POINTER(ctypes.c_uint32),
+    ]
     _lib = L
     return L
 
