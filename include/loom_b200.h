@@ -218,6 +218,83 @@ int loom_b200_sync(loom_b200_handle* h);
 int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);
 int loom_b200_reset_stats(loom_b200_handle* h);
 
+/* ------------------------------------------------------------ serving
+ * Continuous batching of requests on the regrouping engine.  Replaces the
+ * exchange loop of Loom's streams (StreamFacade::exchange, Loom
+ * src/vm/bve.hpp:1208-1270; tests/stream_wrapper.hpp:33-80) and the worker
+ * pool that feeds them (mp::Shop, src/vm/mp.hpp:316-385) for whole
+ * requests: a request (an instance of n threads) is admitted in arrival
+ * order as soon as its thread state fits (a request slot, n entries of the
+ * column rings, its table body in the arena), joins the threads already in
+ * flight in the running megakernel, and its outputs come back when its last
+ * thread finished.  The device runs slices of `slice_rounds` regroup rounds;
+ * between slices the parked threads stay resident in the device queues.
+ * A server is driven by one host thread; every call is synchronous on the
+ * server's stream. */
+typedef struct loom_b200_server loom_b200_server;
+
+typedef struct loom_b200_server_cfg
+{
+    uint64_t        ring_threads; /* entries of each column ring: a power of
+                                     two in [32, 2^31]; bounds the threads of
+                                     the requests in flight */
+    uint64_t        table_words;  /* words of the table arena for request bodies */
+    uint32_t        header_words; /* table words per request header (0: none);
+                                     the header of the request in slot i sits
+                                     at word i * header_words, and the
+                                     INSTANCE input form gives i */
+    int32_t         reloc_word;   /* header word holding an offset into the
+                                     request's body; the server adds the
+                                     body's table position (-1: none) */
+    uint32_t        max_requests; /* request slots (in flight at once) */
+    uint32_t        slice_rounds; /* regroup rounds per slice (0: 4) */
+    const uint32_t* forms;        /* one LOOM_B200_IN_* per kernel input
+                                     (ARRAY, IOTA, LOCAL_IOTA, INSTANCE);
+                                     NULL: every input an ARRAY */
+} loom_b200_server_cfg;
+
+typedef struct loom_b200_request
+{
+    uint64_t           n;          /* threads (<= ring_threads) */
+    const void* const* inputs;     /* host arrays of the ARRAY-form inputs */
+    void* const*       outputs;    /* host arrays that receive the outputs */
+    const uint32_t*    header;     /* header_words words (copied at submit) */
+    const uint32_t*    body;       /* body_words words, or NULL */
+    uint64_t           body_words;
+} loom_b200_request;
+
+typedef struct loom_b200_server_stats
+{
+    uint64_t submitted, admitted, completed;
+    uint64_t threads;      /* threads of the completed requests */
+    uint64_t slices;       /* megakernel launches */
+    uint64_t rounds;       /* regroup rounds over all slices */
+    uint64_t queued;       /* submitted, not admitted */
+    uint64_t in_flight;    /* admitted, not completed */
+    uint64_t unreported;   /* completed, ticket not returned by step yet */
+    uint64_t device_bytes; /* device memory the server holds */
+    uint64_t thread_instr, warp_instr; /* with opts.profile: lane efficiency */
+    uint32_t status;       /* OR of LOOM_B200_STATUS_* */
+    uint32_t pad;
+} loom_b200_server_stats;
+
+/* `opts`: engine options (population = resident threads; 0: 2^21);
+ * `stream`: a cudaStream_t (NULL: the CUDA default stream). */
+int loom_b200_server_create(const char*                 kernel,
+                            const loom_b200_opts*       opts,
+                            const loom_b200_server_cfg* cfg,
+                            void*                       stream,
+                            loom_b200_server**          out);
+int loom_b200_server_destroy(loom_b200_server* s);
+/* Queues a request; its host arrays must stay valid until its ticket comes
+ * back from loom_b200_server_step.  LOOM_B200_ERR_BUDGET: larger than the
+ * ring or the arena. */
+int loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_t* ticket);
+/* Admits what fits, runs one slice, copies out the requests that finished
+ * and returns up to max_done of their tickets (the rest on later calls). */
+int loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, uint32_t* n_done);
+int loom_b200_server_get_stats(const loom_b200_server* s, loom_b200_server_stats* st);
+
 /* ------------------------------------------------------------ no allocation
  * No counterpart in the reference: Loom's backends allocate their device
  * memory themselves.

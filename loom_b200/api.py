@@ -151,6 +151,49 @@ class LaunchC(ctypes.Structure):
     ]
 
 
+class ServerCfgC(ctypes.Structure):
+    _fields_ = [
+        ("ring_threads", ctypes.c_uint64),
+        ("table_words", ctypes.c_uint64),
+        ("header_words", ctypes.c_uint32),
+        ("reloc_word", ctypes.c_int32),
+        ("max_requests", ctypes.c_uint32),
+        ("slice_rounds", ctypes.c_uint32),
+        ("forms", ctypes.POINTER(ctypes.c_uint32)),
+    ]
+
+
+class RequestC(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint64),
+        ("inputs", ctypes.POINTER(ctypes.c_void_p)),
+        ("outputs", ctypes.POINTER(ctypes.c_void_p)),
+        ("header", ctypes.POINTER(ctypes.c_uint32)),
+        ("body", ctypes.POINTER(ctypes.c_uint32)),
+        ("body_words", ctypes.c_uint64),
+    ]
+
+
+class ServerStatsC(ctypes.Structure):
+    _fields_ = [
+        (f, ctypes.c_uint64)
+        for f in (
+            "submitted",
+            "admitted",
+            "completed",
+            "threads",
+            "slices",
+            "rounds",
+            "queued",
+            "in_flight",
+            "unreported",
+            "device_bytes",
+            "thread_instr",
+            "warp_instr",
+        )
+    ] + [("status", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
 class Iota:
     """Input column = thread index."""
 
@@ -199,6 +242,11 @@ EXPORTS = [
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
     "loom_b200_launch_static",
+    "loom_b200_server_create",
+    "loom_b200_server_destroy",
+    "loom_b200_server_submit",
+    "loom_b200_server_step",
+    "loom_b200_server_get_stats",
 ]
 
 
@@ -232,6 +280,22 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_sync.argtypes = [vp]
     L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
     L.loom_b200_reset_stats.argtypes = [vp]
+    L.loom_b200_server_create.argtypes = [
+        ctypes.c_char_p,
+        ctypes.POINTER(Opts),
+        ctypes.POINTER(ServerCfgC),
+        vp,
+        ctypes.POINTER(vp),
+    ]
+    L.loom_b200_server_destroy.argtypes = [vp]
+    L.loom_b200_server_submit.argtypes = [vp, ctypes.POINTER(RequestC), ctypes.POINTER(ctypes.c_uint64)]
+    L.loom_b200_server_step.argtypes = [
+        vp,
+        ctypes.POINTER(ctypes.c_uint64),
+        ctypes.c_uint32,
+        ctypes.POINTER(ctypes.c_uint32),
+    ]
+    L.loom_b200_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStatsC)]
     L.loom_b200_launch_static.argtypes = [
         ctypes.c_char_p,
         ctypes.POINTER(LaunchC),
@@ -463,6 +527,115 @@ class Function:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             lib().loom_b200_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Server:
+    """Continuous batching of requests of one kernel (loom_b200_server_*).
+
+    ``forms`` gives the form of each kernel input (array inputs come with
+    every request; IOTA / LOCAL_IOTA / INSTANCE are computed on the device).
+    A request may carry a table header (``header_words`` words, the
+    INSTANCE form gives its slot) and a body whose table position the server
+    adds to header word ``reloc_word``.
+    """
+
+    FORM = {"array": IN_ARRAY, "iota": IN_IOTA, "local_iota": IN_LOCAL_IOTA, "instance": IN_INSTANCE}
+
+    def __init__(
+        self,
+        kernel: str,
+        ring_threads: int,
+        max_requests: int = 1024,
+        slice_rounds: int = 4,
+        forms: Optional[Sequence[str]] = None,
+        header_words: int = 0,
+        reloc_word: int = -1,
+        table_words: int = 0,
+        stream=None,
+        **opts,
+    ):
+        self.info = info(kernel)
+        self._h = ctypes.c_void_p()
+        fs = [self.FORM[f] for f in forms] if forms else [IN_ARRAY] * len(self.info.inputs)
+        self._forms = (ctypes.c_uint32 * max(1, len(fs)))(*fs)
+        self.forms = fs
+        cfg = ServerCfgC(ring_threads, table_words, header_words, reloc_word, max_requests, slice_rounds, self._forms)
+        o = make_opts("regroup", **opts)
+        s = getattr(stream, "cuda_stream", stream)
+        check(lib().loom_b200_server_create(kernel.encode(), ctypes.byref(o), ctypes.byref(cfg), s, ctypes.byref(self._h)))
+        self.header_words = header_words
+        self._live: Dict[int, tuple] = {}
+        self._done = (ctypes.c_uint64 * max(1, max_requests))()
+        self._max = max(1, max_requests)
+
+    def submit(self, n: int, inputs: Sequence = (), outputs: Optional[Sequence] = None, header=None, body=None) -> int:
+        """Queues a request of n threads; returns its ticket.  Array inputs
+        and outputs are host arrays (numpy or pinned torch tensors) that
+        stay referenced until the request completes; outputs default to new
+        numpy arrays, returned by ``result``."""
+        if outputs is None:
+            outputs = [np.empty(n, dtype=NP_TYPE[t]) for _, t in self.info.outputs]
+        ins = []
+        it = iter(inputs)
+        for f, (_, t) in zip(self.forms, self.info.inputs):
+            if f == IN_ARRAY:
+                a = next(it)
+                if isinstance(a, np.ndarray):
+                    a = np.ascontiguousarray(a, dtype=NP_TYPE[t])
+                ins.append(a)
+            else:
+                ins.append(None)
+        pin = (ctypes.c_void_p * max(1, len(ins)))(*[_ptr(a) for a in ins])
+        pout = (ctypes.c_void_p * len(outputs))(*[_ptr(o) for o in outputs])
+        hdr = None if header is None else np.ascontiguousarray(header, dtype=np.uint32)
+        bod = None if body is None else np.ascontiguousarray(body, dtype=np.uint32)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        r = RequestC(
+            n,
+            pin,
+            pout,
+            None if hdr is None else hdr.ctypes.data_as(u32p),
+            None if bod is None else bod.ctypes.data_as(u32p),
+            0 if bod is None else len(bod),
+        )
+        t = ctypes.c_uint64()
+        check(lib().loom_b200_server_submit(self._h, ctypes.byref(r), ctypes.byref(t)))
+        self._live[t.value] = (ins, outputs, hdr, bod, pin, pout)
+        return t.value
+
+    def step(self) -> List[int]:
+        """Admits, runs one slice, returns the tickets that completed."""
+        k = ctypes.c_uint32()
+        check(lib().loom_b200_server_step(self._h, self._done, self._max, ctypes.byref(k)))
+        return [self._done[i] for i in range(k.value)]
+
+    def result(self, ticket: int):
+        """Outputs of a completed request (and forgets it)."""
+        outs = self._live.pop(ticket)[1]
+        return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def stats(self) -> Dict[str, int]:
+        st = ServerStatsC()
+        check(lib().loom_b200_server_get_stats(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStatsC._fields_ if f != "pad"}
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib().loom_b200_server_destroy(h)
             self._h = None
 
     def __del__(self):

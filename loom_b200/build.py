@@ -140,7 +140,7 @@ def _headers() -> List[pathlib.Path]:
 
 def compile_all(jobs: Optional[int] = None, verbose: bool = False) -> pathlib.Path:
     OBJ.mkdir(parents=True, exist_ok=True)
-    srcs = [CSRC / "runtime.cu", CSRC / "static_scratch.cu", *sorted(GEN.glob("*.cu"))]
+    srcs = [CSRC / "runtime.cu", CSRC / "server.cu", CSRC / "static_scratch.cu", *sorted(GEN.glob("*.cu"))]
     hdr_mtime = max(h.stat().st_mtime for h in _headers())
     cc = nvcc()
 

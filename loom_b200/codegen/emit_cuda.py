@@ -365,7 +365,7 @@ def generate(k: Kernel) -> str:
     w("    {")
     for j, (reg, t, vname) in enumerate(k.outputs):
         ct = CTYPE[t]
-        w(f"        static_cast<{ct}*>(c.p[{nin + j}])[tid] = {L.read(Operand(type=t, reg=reg))}; // {vname}")
+        w(f"        static_cast<{ct}*>(c.p[{nin + j}])[col_index(c, tid)] = {L.read(Operand(type=t, reg=reg))}; // {vname}")
     w("    }")
     w("")
     w("    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }")

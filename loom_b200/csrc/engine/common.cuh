@@ -35,7 +35,21 @@ struct Columns
     const unsigned long long* inst_start; // num_inst + 1 thread offsets
     unsigned                  num_inst;
     const unsigned*           table;      // words read by the tab op
+    // Serving: array columns are rings indexed by tid & ring_mask (0: by
+    // tid); the instance form reads inst_id[i] (NULL: i); every thread id in
+    // flight lies in [tid_base, tid_base + 2^32), so the 32-bit ids kept in
+    // the queue state name one thread each.
+    unsigned long long        ring_mask;
+    unsigned long long        tid_base;
+    const unsigned*           inst_id;
 };
+
+/// Position of thread `tid` in the array columns.
+__device__ __forceinline__ unsigned long long
+col_index(const Columns& c, const unsigned long long tid)
+{
+    return c.ring_mask ? (tid & c.ring_mask) : tid;
+}
 
 /// Status bits written by device code (also returned through the C ABI).
 enum : unsigned
@@ -162,6 +176,16 @@ find_instance(const Columns& c, const unsigned long long tid)
     return lo;
 }
 
+/// Instance id of thread `tid`: its position among the instances, or the
+/// id that inst_id gives that position.
+__device__ __forceinline__ unsigned
+instance_id(const Columns& c, const unsigned long long tid)
+{
+    if(!c.num_inst) return 0u;
+    const unsigned i = find_instance(c, tid);
+    return c.inst_id ? c.inst_id[i] : i;
+}
+
 /// Input i of thread `tid` as T.
 template <typename T>
 __device__ __forceinline__ T
@@ -169,7 +193,7 @@ load_input(const Columns& c, const int i, const unsigned long long tid)
 {
     switch(c.form[i])
     {
-    case LOOM_B200_IN_ARRAY: return static_cast<const T*>(c.p[i])[tid];
+    case LOOM_B200_IN_ARRAY: return static_cast<const T*>(c.p[i])[col_index(c, tid)];
     case LOOM_B200_IN_BROADCAST:
     {
         T v;
@@ -178,8 +202,7 @@ load_input(const Columns& c, const int i, const unsigned long long tid)
     }
     case LOOM_B200_IN_LOCAL_IOTA:
         return static_cast<T>(c.num_inst ? tid - c.inst_start[find_instance(c, tid)] : tid);
-    case LOOM_B200_IN_INSTANCE:
-        return static_cast<T>(c.num_inst ? find_instance(c, tid) : 0u);
+    case LOOM_B200_IN_INSTANCE: return static_cast<T>(instance_id(c, tid));
     default: return static_cast<T>(tid);
     }
 }

@@ -46,8 +46,9 @@ struct RegroupCtl
     unsigned           bar_gen;
     unsigned           done;
     unsigned           pad0;
-    unsigned long long cursor;    // next input index to admit
-    unsigned long long admit_end; // inputs below this index may enter this round
+    unsigned long long cursor;     // next input index to admit
+    unsigned long long admit_end;  // inputs below this index may enter this round
+    unsigned long long next_round; // round number the next launch continues with
 };
 
 struct RegroupParams
@@ -72,6 +73,13 @@ struct RegroupParams
     unsigned            prefetch; // prefetch the next input of every lane
     unsigned            refill;   // halted lanes claim new inputs at once
     unsigned            phantoms; // fault injection: CTAs the barrier waits for in vain
+    // Serving: a launch may run a slice of `slice_rounds` rounds (0: until
+    // done) starting at round `round0`, whose parity selects the queues it
+    // resumes from; a finished thread adds one to inst_done[its instance id]
+    // (NULL: no per-instance counts).
+    unsigned            round0;
+    unsigned            slice_rounds;
+    unsigned*           inst_done;
 };
 
 __device__ __forceinline__ unsigned
@@ -169,7 +177,7 @@ regroup_kernel(const RegroupParams p)
     typename K::Regs   R;
     typename K::In     pf;
     unsigned long long pf_tid = ~0ull;
-    for(unsigned round = 0;; ++round)
+    for(unsigned round = p.round0;; ++round)
     {
         const unsigned           cur = round & 1u, nxt = cur ^ 1u;
         const unsigned long long admit_end = ld_volatile64(&p.ctl->admit_end);
@@ -207,7 +215,9 @@ regroup_kernel(const RegroupParams p)
             {
                 if(lane < tk)
                 {
-                    tid = K::restore(tb, R, p.state, p.cap, cur, toff + lane);
+                    // the queue keeps the low 32 bits of the thread id
+                    const unsigned t32 = K::restore(tb, R, p.state, p.cap, cur, toff + lane);
+                    tid = p.cols.tid_base + static_cast<unsigned>(t32 - static_cast<unsigned>(p.cols.tid_base));
                     if(tid < p.n) { pc = K::block_of(tb); sbytes += K::live_bytes(tb) + 4u; }
                     else ctx.flag(kStatusQueueOverrun);
                 }
@@ -245,6 +255,14 @@ regroup_kernel(const RegroupParams p)
                     {
                         K::store_outputs(R, p.cols, tid);
                         ++finished;
+                        if(p.inst_done)
+                        {
+                            // one atomic per instance among the halting lanes
+                            const unsigned id    = instance_id(p.cols, tid);
+                            const unsigned peers = __match_any_sync(hm, id);
+                            if(static_cast<int>(lane) == __ffs(peers) - 1)
+                                atomicAdd(p.inst_done + id, static_cast<unsigned>(__popc(peers)));
+                        }
                         pc = kEmpty;
                         if(pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
                     }
@@ -321,13 +339,17 @@ regroup_kernel(const RegroupParams p)
                 p.ctl->cursor    = c;
                 p.ctl->admit_end = c + room < p.n ? c + room : p.n;
                 unsigned done    = parked == 0ull && c >= p.n ? 1u : 0u;
-                if(!done && round + 1ull >= p.max_rounds)
+                const unsigned long long ran = round + 1ull - p.round0;
+                if(!done && p.slice_rounds && ran >= p.slice_rounds)
+                    done = 1u; // end of the slice: the parked threads wait for the next one
+                else if(!done && ran >= p.max_rounds)
                 {
                     atomicOr(p.status, kStatusStepLimit);
                     done = 1u;
                 }
+                p.ctl->next_round = round + 1ull;
                 *reinterpret_cast<volatile unsigned*>(&p.ctl->done) = done;
-                if(done) atomicAdd(p.counters + 5, round + 1ull);
+                if(done) atomicAdd(p.counters + 5, ran);
             });
         if(!more) break;
     }

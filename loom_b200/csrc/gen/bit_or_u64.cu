@@ -57,7 +57,7 @@ struct K
     __device__ __forceinline__ static void
     store_outputs(const Regs& R, const Columns& c, const unsigned long long tid)
     {
-        static_cast<unsigned long long*>(c.p[2])[tid] = R.r0; // a
+        static_cast<unsigned long long*>(c.p[2])[col_index(c, tid)] = R.r0; // a
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }

@@ -319,9 +319,9 @@ struct K
     __device__ __forceinline__ static void
     store_outputs(const Regs& R, const Columns& c, const unsigned long long tid)
     {
-        static_cast<float*>(c.p[2])[tid] = R.r3; // L0
-        static_cast<float*>(c.p[3])[tid] = R.r4; // L1
-        static_cast<float*>(c.p[4])[tid] = R.r5; // L2
+        static_cast<float*>(c.p[2])[col_index(c, tid)] = R.r3; // L0
+        static_cast<float*>(c.p[3])[col_index(c, tid)] = R.r4; // L1
+        static_cast<float*>(c.p[4])[col_index(c, tid)] = R.r5; // L2
     }
 
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }

@@ -130,6 +130,17 @@ def pack(requests: Sequence[Request]) -> Tuple[np.ndarray, np.ndarray]:
     return words, starts
 
 
+def request_words(r: Request) -> Tuple[np.ndarray, np.ndarray]:
+    """One request as a server request: its 16-word header with the first
+    sphere word (header word 4) relative to the start of its body, and the
+    body (its sphere records).  The server adds the body's table position to
+    word 4 when it admits the request."""
+    words, _ = pack([r])
+    header = words[:HEADER_WORDS].copy()
+    header[4] = 0
+    return header, words[HEADER_WORDS:].copy()
+
+
 def pixel_average(rgb: Sequence[np.ndarray], spp: int) -> np.ndarray:
     """Per-pixel mean of the per-sample radiance, summed in sample order
     (deterministic); returns (pixels, 3) float32."""

@@ -97,3 +97,23 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(api.LoomError) as e:
         api.Function("fib_u64", 16)
     assert e.value.code in (api.ERR_NO_DEVICE, api.ERR_CUDA)
+
+
+def test_server_create_without_device_fails_cleanly():
+    from conftest import cuda_available
+
+    if cuda_available():
+        pytest.skip("a device is visible")
+    with pytest.raises(api.LoomError) as e:
+        api.Server("collatz_u64", ring_threads=1 << 10)
+    assert e.value.code in (api.ERR_NO_DEVICE, api.ERR_CUDA)
+
+
+def test_server_rejects_bad_configuration():
+    """Checked before any device call: ring size not a power of two, no
+    request slots, a relocated word outside the header."""
+    for kw in (dict(ring_threads=1000), dict(ring_threads=1 << 10, max_requests=0),
+               dict(ring_threads=1 << 10, header_words=4, reloc_word=4)):
+        with pytest.raises(api.LoomError) as e:
+            api.Server("collatz_u64", **kw)
+        assert e.value.code == api.ERR_INVALID, kw
