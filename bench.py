@@ -13,21 +13,34 @@ way beside it.  `e2e` is the same metric through the public API with host
 buffers: the table copied in and the three output columns copied back to
 pinned host memory inside the timed region.
 
-Other workloads: `--workload collatz` (2^24 threads, n ~ U[1, 2^32)),
-`--workload fib` (2^20 threads, n ~ U{0..93}).
+Other workloads:
+  batch    256 render requests of uneven size, each with its own random
+           scene, in one launch (about 473 M threads)
+  collatz  2^24 threads, n ~ U[1, 2^32)
+  fib      2^20 threads, n ~ U{0..93}
+  serve    the serving loop: Poisson arrivals of a request mix (60 % render
+           requests as in `batch`, 20 % Collatz batches of 2^16-2^22 inputs,
+           20 % Fibonacci batches of 2^16-2^20 inputs) at 25/50/75/100 % of
+           the measured capacity; throughput and p50/p99 latency of the
+           continuous-batching servers beside a plain-engine FIFO queue.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pt|collatz|fib]
+                    [--workload pt|pt_small|batch|collatz|fib|serve]
 
 Under torchrun each rank runs the full workload on its own GPU (weak
 scaling, no data-path collective: Loom threads are independent), times with
 CUDA events and reports the max over ranks.
+
+The CPU leg (skipped with --no-cpu) times Loom's own scalar backend on the
+host cores and is also the parity check: the reference's outputs for a
+seeded sample of threads are compared bit for bit with both engines'.
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import pathlib
 import statistics
@@ -40,12 +53,14 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
-# Regrouping options per workload, from the sweeps kept in profiles/
+# Regrouping options per kernel, from the sweeps summarised in profiles/
 TUNED = {
     "sphere_pt_f32": dict(burst=4, utr_lanes=8, population=1 << 21, block_size=256, period=4096),
     "collatz_u64": dict(burst=64, utr_lanes=16, block_size=512, period=65536, prefetch=False),
     "fib_u64": dict(burst=64, utr_lanes=16, block_size=512, period=1024, prefetch=False),
 }
+
+CHECK_THREADS = 1 << 14  # threads compared with the reference
 
 
 # ---------------------------------------------------------------- workloads
@@ -53,9 +68,21 @@ class Workload:
     kernel = ""
     desc = ""
     dtype = ""
+    n = 0
+    in_bytes = 0
+    out_bytes = 0
 
-    def prepare(self, torch, device: bool = True):
-        raise NotImplementedError
+    def check_tids(self) -> np.ndarray:
+        """A seeded sample of thread ids for the parity check."""
+        rng = np.random.default_rng(5)
+        return np.unique(rng.integers(0, self.n, size=min(CHECK_THREADS, self.n)))
+
+    def outputs_at(self, tids):
+        """Device outputs of threads `tids` (host arrays, one per output)."""
+        import torch
+
+        ix = torch.from_numpy(np.ascontiguousarray(tids, dtype=np.int64)).cuda()
+        return [o[ix].cpu().numpy() for o in self.d_out]
 
 
 class PathTracing(Workload):
@@ -65,7 +92,6 @@ class PathTracing(Workload):
     def __init__(self, width=1024, height=768, spp=64):
         from loom_b200 import scenes as S
 
-        self.S = S
         self.req = S.cornell_request(width, height, spp, seed=1)
         self.table, self.starts = S.pack([self.req])
         self.n = self.req.threads
@@ -86,15 +112,9 @@ class PathTracing(Workload):
     def launch(self, f, api, stream):
         f.launch_device(self.inputs(api), self.d_out, self.n, table=self.d_table, stream=stream)
 
-    def check(self, api):
-        """Bit-exact parity of a seeded sample against the C oracle."""
-        from oracle import oracle as O
-
-        got = [o.cpu().numpy() for o in self.d_out]
-        idx = np.sort(O.uniform_int(5, 256, 0, self.n - 1).astype(np.int64))
-        ins = O.expand_inputs(["instance", "local_iota"], self.n, self.starts, ["u32", "u32"])
-        want = O.Interp(self.kernel).run([a[idx] for a in ins], table=self.table)
-        return all(np.array_equal(g[idx].view(np.uint32), w.view(np.uint32)) for g, w in zip(got, want)), idx
+    def ref_inputs(self, tids):
+        tids = np.asarray(tids, dtype=np.uint64)
+        return [np.zeros(len(tids), dtype=np.uint32), tids.astype(np.uint32)], self.table
 
     def e2e(self, api, torch, steps, warmup, dist):
         h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
@@ -112,49 +132,102 @@ class PathTracing(Workload):
         for _ in range(steps):
             step()
         dt = time.perf_counter() - t0
-        got = [h.numpy() for h in h_out]
-        ok = all(np.array_equal(g, d.cpu().numpy()) for g, d in zip(got, self.d_out))
+        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_out, self.d_out))
         fe.close()
         return dt, ok, self.table.nbytes, 3 * 4 * self.n
 
-    def cpu_inputs(self):
-        from oracle import oracle as O
 
-        return O.expand_inputs(["instance", "local_iota"], self.n, self.starts, ["u32", "u32"]), self.table
+class BatchedPathTracing(PathTracing):
+    """Many render requests of uneven size in one launch: each request has
+    its own resolution, sample count and random scene (loom_b200.scenes
+    .random_request); threads of all requests share the megakernel and are
+    mapped to (request, sample) on the device from the instance offsets."""
+
+    def __init__(self, count=256, seed=3):
+        from loom_b200 import scenes as S
+
+        rng = np.random.default_rng(seed)
+        self.reqs = [S.random_request(rng, seed=i + 1) for i in range(count)]
+        self.table, self.starts = S.pack(self.reqs)
+        self.n = int(self.starts[-1])
+        self.desc = (
+            f"{count} batched render requests (seed {seed}): resolution from {{64,128,256,512}}^2, spp from "
+            f"{{1,4,16,64}}, 8-64 random spheres each (60/20/20 diffuse/mirror/glass, 1-4 emitters), "
+            f"{self.n} threads in one launch, FP32"
+        )
+        self.in_bytes = 0
+        self.out_bytes = 12
+
+    def inputs(self, api):
+        return [api.Instance(), api.LocalIota()]
+
+    def device_buffers(self, torch):
+        super().device_buffers(torch)
+        self.d_starts = torch.from_numpy(self.starts.view(np.int64)).cuda()
+
+    def launch(self, f, api, stream):
+        f.launch_device(
+            self.inputs(api), self.d_out, self.n, instance_starts=self.d_starts, table=self.d_table, stream=stream
+        )
+
+    def check_tids(self):
+        """4 random threads of every request."""
+        rng = np.random.default_rng(5)
+        lo, hi = self.starts[:-1].astype(np.int64), self.starts[1:].astype(np.int64)
+        return np.unique(np.concatenate([rng.integers(a, b, size=4) for a, b in zip(lo, hi)]))
+
+    def ref_inputs(self, tids):
+        tids = np.asarray(tids, dtype=np.uint64)
+        inst = (np.searchsorted(self.starts, tids, side="right") - 1).astype(np.int64)
+        return [inst.astype(np.uint32), (tids - self.starts[inst]).astype(np.uint32)], self.table
+
+    def e2e(self, api, torch, steps, warmup, dist):
+        h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
+        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+
+        def step():
+            L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, self.starts, self.table)
+            api.check(api.lib().loom_b200_launch_host(fe._h, api.ctypes.byref(L)))
+
+        for _ in range(warmup):
+            step()
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            step()
+        dt = time.perf_counter() - t0
+        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_out, self.d_out))
+        fe.close()
+        return dt, ok, self.table.nbytes + self.starts.nbytes, 3 * 4 * self.n
 
 
 class IntegerLoop(Workload):
     def __init__(self, kernel, n, lo, hi, out_bytes, desc):
+        from loom_b200 import inputs as I
+
         self.kernel = kernel
         self.n = n
-        self.lo, self.hi = lo, hi
         self.desc = desc
         self.dtype = "u64"
         self.in_bytes = 8
         self.out_bytes = out_bytes
-        from oracle import oracle as O
-
-        self.x = O.uniform_int(1, n, lo, hi)
+        self.x = I.uniform_int(1, n, lo, hi)
 
     def device_buffers(self, torch):
         self.d_in = torch.from_numpy(self.x.view(np.int64)).cuda()
         dt = torch.int32 if self.out_bytes == 4 else torch.int64
-        self.d_out = torch.empty(self.n, dtype=dt, device="cuda")
+        self.d_out = [torch.empty(self.n, dtype=dt, device="cuda")]
 
     def launch(self, f, api, stream):
-        f.run_device([self.d_in], [self.d_out], self.n, stream=stream)
+        f.run_device([self.d_in], self.d_out, self.n, stream=stream)
 
-    def check(self, api):
-        from oracle import oracle as O
-
-        got = self.d_out.cpu().numpy().view(np.uint32 if self.out_bytes == 4 else np.uint64)
-        idx = O.uniform_int(5, 4096, 0, self.n - 1).astype(np.int64)
-        (want,) = O.Interp(self.kernel).run([self.x[idx]])
-        return bool(np.array_equal(got[idx], want)), idx
+    def ref_inputs(self, tids):
+        return [self.x[np.asarray(tids, dtype=np.int64)]], None
 
     def e2e(self, api, torch, steps, warmup, dist):
         h_in = torch.from_numpy(self.x.view(np.int64)).pin_memory()
-        h_out = torch.empty(self.n, dtype=self.d_out.dtype).pin_memory()
+        h_out = torch.empty(self.n, dtype=self.d_out[0].dtype).pin_memory()
         fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
         for _ in range(warmup):
             fe.run_host_ptrs([h_in], [h_out], self.n)
@@ -164,12 +237,9 @@ class IntegerLoop(Workload):
         for _ in range(steps):
             fe.run_host_ptrs([h_in], [h_out], self.n)
         dt = time.perf_counter() - t0
-        ok = bool(np.array_equal(h_out.numpy(), self.d_out.cpu().numpy()))
+        ok = bool(torch.equal(h_out, self.d_out[0].cpu()))
         fe.close()
         return dt, ok, self.n * self.in_bytes, self.n * self.out_bytes
-
-    def cpu_inputs(self):
-        return [self.x], None
 
 
 def make_workload(name):
@@ -177,6 +247,8 @@ def make_workload(name):
         return PathTracing()
     if name == "pt_small":  # the profiling case: same scene at 256x192
         return PathTracing(256, 192, 64)
+    if name == "batch":
+        return BatchedPathTracing()
     if name == "collatz":
         return IntegerLoop(
             "collatz_u64", 1 << 24, 1, (1 << 32) - 1, 4,
@@ -259,61 +331,7 @@ class ClockSampler:
         }
 
 
-# ---------------------------------------------------------------- CPU arm
-def cpu_reference(w, target_s: float = 4.0):
-    """Loom's bse (oracle/_ref) on all host cores over a bounded sample of
-    the workload's threads; falls back to the C restatement (one thread)
-    where bse was not built.  Returns (Msamples/s, info)."""
-    from oracle import oracle as O
-
-    cores = os.cpu_count() or 1
-    ins, table = w.cpu_inputs()
-    # a seeded random subset of the workload's threads (cost per thread
-    # varies across the image; a prefix would not be representative)
-    perm = np.random.default_rng(7).permutation(w.n)
-    ins = [np.ascontiguousarray(a[perm]) for a in ins]
-    if O.ref_available():
-        kind = "reference"
-
-        def run(m):
-            O.ref_run(w.kernel, [a[:m] for a in ins], m, threads=cores, table=table)
-
-        used = cores
-    else:
-        kind = "port"
-        it = O.Interp(w.kernel)
-
-        def run(m):
-            it.run([a[:m] for a in ins], table=table)
-
-        used = 1
-    m = 1 << 12
-    while True:
-        t0 = time.perf_counter()
-        run(m)
-        dt = time.perf_counter() - t0
-        if dt > target_s / 8 or m >= w.n:
-            break
-        m = min(w.n, m * 4)
-    m = min(w.n, max(m, int(m * target_s / max(dt, 1e-9))))
-    t0 = time.perf_counter()
-    run(m)
-    dt = time.perf_counter() - t0
-    cpu = _cpu_model()
-    how = (
-        "Loom bse (vm::bse::function), g++ -O2 -mfma, one std::thread per core"
-        if kind == "reference"
-        else "C restatement of bse, one thread"
-    )
-    return m / dt / 1e6, {
-        "unit": "Msamples/s",
-        "cores": used,
-        "kind": kind,
-        "sample": f"{m} threads drawn at random (seed 7) from the workload's {w.n}, on {cpu}; {how}",
-        "seconds": round(dt, 3),
-    }
-
-
+# ---------------------------------------------------------------- CPU leg
 def _cpu_model() -> str:
     try:
         for ln in open("/proc/cpuinfo"):
@@ -322,6 +340,73 @@ def _cpu_model() -> str:
     except Exception:
         pass
     return "unknown CPU"
+
+
+def _reference_runner():
+    """Loom's bse (oracle/_ref) on all host cores, else the C restatement on
+    one core: returns (run(kernel, inputs, table) -> outputs, kind, cores)."""
+    from oracle import oracle as O
+
+    cores = os.cpu_count() or 1
+    if O.ref_available():
+
+        def run(kernel, ins, table):
+            return O.ref_run(kernel, ins, len(ins[0]), threads=cores, table=table)
+
+        return run, "reference", cores
+
+    def run(kernel, ins, table):
+        return O.Interp(kernel).run(ins, table=table)
+
+    return run, "port", 1
+
+
+def cpu_reference(w, check_tids=None, target_s: float = 2.0):
+    """Times the reference on a bounded random sample of the workload's
+    threads (about `target_s` seconds of CPU work), and, with `check_tids`,
+    returns the reference's outputs of those threads for the parity check.
+    Returns (Msamples/s, info, outputs or None)."""
+    run, kind, cores = _reference_runner()
+    rng = np.random.default_rng(7)
+    pool = rng.integers(0, w.n, size=min(w.n, 1 << 26))
+    m = 1 << 12
+    while True:
+        ins, table = w.ref_inputs(pool[:m])
+        t0 = time.perf_counter()
+        run(w.kernel, ins, table)
+        dt = time.perf_counter() - t0
+        if dt > target_s / 8 or m >= len(pool):
+            break
+        m = min(len(pool), m * 4)
+    m = min(len(pool), max(m, int(m * target_s / max(dt, 1e-9))))
+    ins, table = w.ref_inputs(pool[:m])
+    t0 = time.perf_counter()
+    run(w.kernel, ins, table)
+    dt = time.perf_counter() - t0
+    how = (
+        "Loom bse (vm::bse::function), g++ -O2 -mfma, one std::thread per core"
+        if kind == "reference"
+        else "C restatement of bse, one thread"
+    )
+    info = {
+        "unit": "Msamples/s",
+        "cores": cores,
+        "kind": kind,
+        "sample": f"{m} threads drawn at random (seed 7) from the workload's {w.n}, on {_cpu_model()}; {how}",
+        "seconds": round(dt, 3),
+    }
+    want = None
+    if check_tids is not None:
+        ins, table = w.ref_inputs(check_tids)
+        want = run(w.kernel, ins, table)
+    return m / dt / 1e6, info, want
+
+
+def same_bits(got, want) -> bool:
+    return all(
+        np.array_equal(np.ascontiguousarray(g).view(np.uint8), np.ascontiguousarray(w).view(np.uint8))
+        for g, w in zip(got, want)
+    )
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -349,14 +434,330 @@ def time_steps(fn, steps: int, warmup: int, torch, dist=None):
     return ms
 
 
+def base_line(args, warmup, world, w_desc, kernel, dtype, metric, extra=None):
+    line = {
+        "metric": metric,
+        "unit": "Msamples/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": dtype,
+        "data": "synthetic",
+        "config": {
+            "workload": w_desc,
+            "kernel": kernel,
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+        },
+    }
+    if extra:
+        line["config"].update(extra)
+    return line
+
+
+METRIC = (
+    "Msamples/s (Loom threads completed per second), regrouped engine; plain engine and SIMT lane "
+    "efficiency beside it"
+)
+
+
+# ---------------------------------------------------------------- serving
+SERVE_KERNELS = {"pt": "sphere_pt_f32", "collatz": "collatz_u64", "fib": "fib_u64"}
+SERVE_POOL = {"collatz": (1 << 23, 1, (1 << 32) - 1), "fib": (1 << 21, 0, 93)}
+SERVE_BUDGET = 100 << 30  # device bytes for thread state, columns and tables
+
+
+class ServeMix:
+    """Seeded request stream: 60 % render requests drawn as in the batched
+    workload, 20 % Collatz batches of 2^16-2^22 inputs, 20 % Fibonacci
+    batches of 2^16-2^20 inputs (sizes log-uniform over the powers of two;
+    inputs are slices of a seeded pool of each kind)."""
+
+    def __init__(self, seed: int):
+        self.rng = np.random.default_rng(seed)
+        self.seed = seed
+        self.k = 0
+
+    def draw(self, count: int):
+        from loom_b200 import scenes as S
+
+        out = []
+        for _ in range(count):
+            self.k += 1
+            u = self.rng.uniform()
+            if u < 0.6:
+                r = S.random_request(self.rng, seed=self.seed * 100003 + self.k)
+                h, b = S.request_words(r)
+                out.append(("pt", r.threads, dict(header=h, body=b), r))
+            else:
+                kind = "collatz" if u < 0.8 else "fib"
+                lo, hi = (16, 22) if kind == "collatz" else (16, 20)
+                n = 1 << int(self.rng.integers(lo, hi + 1))
+                off = int(self.rng.integers(0, SERVE_POOL[kind][0] - n + 1))
+                out.append((kind, n, off, None))
+        return out
+
+
+class PinnedPool:
+    """Pinned host buffers by power-of-two size class, reused across
+    requests (outputs of requests in flight)."""
+
+    def __init__(self, torch):
+        self.torch = torch
+        self.free = {}
+
+    def get(self, nbytes: int):
+        c = 1 << max(12, math.ceil(math.log2(max(1, nbytes))))
+        lst = self.free.setdefault(c, [])
+        return lst.pop() if lst else self.torch.empty(c, dtype=self.torch.uint8).pin_memory()
+
+    def put(self, t):
+        self.free.setdefault(t.numel(), []).append(t)
+
+
+class RegroupService:
+    """The continuous-batching servers of the three kernels (loom_b200.serving)."""
+
+    def __init__(self, api, torch, stream, pool, inputs, profile=False):
+        from loom_b200 import scenes as S
+        from loom_b200 import serving
+
+        self.api, self.pool, self.inputs = api, pool, inputs
+        st = stream
+        mk = dict(stream=st, profile=profile)
+        self.p = serving.Pool(
+            {
+                "pt": api.Server(
+                    "sphere_pt_f32", ring_threads=1 << 26, max_requests=512, slice_rounds=4,
+                    forms=["instance", "local_iota"], header_words=S.HEADER_WORDS, reloc_word=4,
+                    table_words=1 << 20, **TUNED["sphere_pt_f32"], **mk,
+                ),
+                "collatz": api.Server(
+                    "collatz_u64", ring_threads=1 << 25, max_requests=512, slice_rounds=2,
+                    population=1 << 22, **TUNED["collatz_u64"], **mk,
+                ),
+                "fib": api.Server(
+                    "fib_u64", ring_threads=1 << 23, max_requests=512, slice_rounds=2,
+                    population=1 << 21, **TUNED["fib_u64"], **mk,
+                ),
+            }
+        )
+        self.bufs = {}
+
+    def device_bytes(self):
+        return sum(s["device_bytes"] for s in self.p.stats().values())
+
+    def submit(self, req):
+        kind, n, a, _ = req
+        info = self.p.servers[kind].info
+        ob = [np.dtype(api_np(self.api, t)).itemsize for _, t in info.outputs]
+        buf = self.pool.get(n * sum(ob))
+        outs, off = [], buf.data_ptr()
+        for b in ob:
+            outs.append(off)
+            off += n * b
+        if kind == "pt":
+            key = self.p.submit(kind, n, outputs=outs, **a)
+        else:
+            key = self.p.submit(kind, n, inputs=[self.inputs[kind][a : a + n]], outputs=outs)
+        self.bufs[key] = buf
+        return key
+
+    def busy(self):
+        return self.p.busy()
+
+    def step(self):
+        done = self.p.step()
+        for key in done:
+            self.p.result(*key)
+            self.pool.put(self.bufs.pop(key))
+        return done
+
+    def lane_efficiency(self):
+        ti = sum(s["thread_instr"] for s in self.p.stats().values())
+        wi = sum(s["warp_instr"] for s in self.p.stats().values())
+        return ti / (32.0 * wi) if wi else None
+
+    def close(self):
+        self.p.close()
+
+
+def api_np(api, t):
+    return api.NP_TYPE[t]
+
+
+class PlainQueue:
+    """The baseline: a FIFO queue per kernel; each step launches every
+    waiting request of a kernel in one plain-engine launch (host columns in
+    and out), and a request that arrives meanwhile waits for the next."""
+
+    CAPACITY = {"pt": 1 << 27, "collatz": 1 << 25, "fib": 1 << 23}  # threads per launch
+
+    def __init__(self, api, torch, stream, pool, inputs, profile=False):
+        self.api, self.inputs = api, inputs
+        self.f = {
+            k: api.Function(v, self.CAPACITY[k], "plain", profile=profile) for k, v in SERVE_KERNELS.items()
+        }
+        self.wait = {k: [] for k in SERVE_KERNELS}
+        self.t = 0
+
+    def submit(self, req):
+        self.t += 1
+        self.wait[req[0]].append((self.t, req))
+        return (req[0], self.t)
+
+    def busy(self):
+        return any(self.wait.values())
+
+    def step(self):
+        from loom_b200 import scenes as S
+
+        api = self.api
+        done = []
+        for kind, lst in self.wait.items():
+            if not lst:
+                continue
+            k, total = 0, 0
+            while k < len(lst) and total + lst[k][1][1] <= self.CAPACITY[kind]:
+                total += lst[k][1][1]
+                k += 1
+            batch, self.wait[kind] = lst[:k], lst[k:]
+            if kind == "pt":
+                table, starts = S.pack([r[3] for _, r in batch])
+                n = int(starts[-1])
+                self.f[kind].launch_host([api.Instance(), api.LocalIota()], n, instance_starts=starts, table=table)
+            else:
+                x = np.concatenate([self.inputs[kind][r[2] : r[2] + r[1]].numpy().view(np.uint64) for _, r in batch])
+                self.f[kind](x)
+            done += [(kind, t) for t, _ in batch]
+        return done
+
+    def device_bytes(self):
+        return None
+
+    def lane_efficiency(self):
+        ti = wi = 0
+        for f in self.f.values():
+            s = f.stats()
+            ti += s["thread_instr"]
+            wi += s["warp_instr"]
+        return ti / (32.0 * wi) if wi else None
+
+    def close(self):
+        for f in self.f.values():
+            f.close()
+
+
+def run_requests(svc, reqs, arrivals):
+    """Feeds `reqs` at `arrivals` (seconds from start) and steps `svc` until
+    every request completed.  Returns (latencies, makespan, threads)."""
+    t0 = time.perf_counter()
+    i, lat, inflight = 0, [], {}
+    last = 0.0
+    while i < len(reqs) or inflight:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and arrivals[i] <= now:
+            inflight[svc.submit(reqs[i])] = arrivals[i]
+            i += 1
+        if inflight:
+            for key in svc.step():
+                last = time.perf_counter() - t0
+                lat.append(last - inflight.pop(key))
+        elif i < len(reqs):
+            time.sleep(max(0.0, min(arrivals[i] - now, 0.002)))
+    threads = sum(r[1] for r in reqs)
+    return np.asarray(lat), last, threads
+
+
+def serve_main(args, warmup, world, rank, local):
+    import torch
+
+    if world > 1:
+        torch.cuda.set_device(local)
+    from loom_b200 import api
+    from loom_b200 import inputs as I
+
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    pool = PinnedPool(torch)
+    inputs = {
+        k: torch.from_numpy(I.uniform_int(20 + j, n, lo, hi).view(np.int64)).pin_memory()
+        for j, (k, (n, lo, hi)) in enumerate(SERVE_POOL.items())
+    }
+    mix = ServeMix(seed=17 + rank)
+    loads = (0.25, 0.5, 0.75, 1.0)
+    out = {}
+    with ClockSampler(local) as clk:
+        for name, cls in (("regroup", RegroupService), ("plain", PlainQueue)):
+            svc = cls(api, torch, stream, pool, inputs)
+            # warm-up and capacity: a closed batch (every request at t = 0)
+            run_requests(svc, mix.draw(24), np.zeros(24))
+            cal = mix.draw(160)
+            lat, span, threads = run_requests(svc, cal, np.zeros(len(cal)))
+            cap = threads / span
+            mean_threads = threads / len(cal)
+            res = {"capacity_msamples_s": round(cap / 1e6, 3), "device_bytes": svc.device_bytes(), "loads": []}
+            for L in loads:
+                rate = L * cap / mean_threads  # requests per second
+                count = max(8, int(rate * args.serve_seconds))
+                reqs = mix.draw(count)
+                arr = np.cumsum(mix.rng.exponential(1.0 / rate, size=count))
+                lat, span, threads = run_requests(svc, reqs, arr)
+                res["loads"].append(
+                    {
+                        "offered_load": L,
+                        "requests": count,
+                        "msamples_s": round(threads / span / 1e6, 3),
+                        "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+                        "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+                        "mean_ms": round(float(lat.mean()) * 1e3, 2),
+                    }
+                )
+            svc.close()
+            # lane efficiency of the same mix in a counted (slower) run
+            svc = cls(api, torch, stream, pool, inputs, profile=True)
+            reqs = mix.draw(48)
+            run_requests(svc, reqs, np.zeros(len(reqs)))
+            le = svc.lane_efficiency()
+            res["lane_efficiency"] = None if le is None else round(le, 4)
+            svc.close()
+            out[name] = res
+
+    full = out["regroup"]["loads"][-1]
+    line = base_line(
+        args, warmup, world,
+        "serving: Poisson arrivals at 25/50/75/100 % of measured capacity; mix 60 % render requests "
+        "(batched-workload distribution), 20 % Collatz batches 2^16-2^22, 20 % Fibonacci batches 2^16-2^20",
+        "sphere_pt_f32+collatz_u64+fib_u64", "mixed", "Msamples/s at 100 % offered load, p50/p99 latency",
+        {"budget_bytes": SERVE_BUDGET, "seconds_per_load": args.serve_seconds},
+    )
+    line.update(
+        {
+            "value": full["msamples_s"],
+            "p50_ms": full["p50_ms"],
+            "p99_ms": full["p99_ms"],
+            "fraction_of_capacity": round(full["msamples_s"] / out["regroup"]["capacity_msamples_s"], 4),
+            "regroup": out["regroup"],
+            "plain": out["plain"],
+            "gpu_launches": None,
+            "clocks": clk.summary(),
+        }
+    )
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "collatz", "fib"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "serve"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -364,47 +765,31 @@ def main() -> None:
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.workload == "serve":
+        serve_main(args, warmup, world, rank, local)
+        return
+
     w = make_workload(args.workload)
-    config = {
-        "workload": w.desc,
-        "kernel": w.kernel,
+    extra = {
         "threads_per_gpu": w.n,
         "l2": "outputs larger than L2 (no flush)",
-        "parallelism": f"replicas{world}" if world > 1 else "single",
         "regroup_options": TUNED[w.kernel],
     }
-    metric = "Msamples/s (Loom threads completed per second), regrouped engine; plain engine and SIMT lane efficiency beside it"
 
     if args.impl == "reference":
         if rank != 0:
             return
         vals, info = [], None
         for i in range(warmup + args.steps):
-            v, info = cpu_reference(w, target_s=2.0)
+            v, info, _ = cpu_reference(w, target_s=2.0)
             if i >= warmup:
                 vals.append(v)
         value = statistics.median(vals)
-        print(
-            json.dumps(
-                {
-                    "impl": "reference",
-                    "metric": metric,
-                    "value": round(value, 3),
-                    "unit": "Msamples/s",
-                    "n_gpus": args.gpus,
-                    "steps": args.steps,
-                    "warmup": warmup,
-                    "higher_is_better": True,
-                    "scaling": "weak",
-                    "vs_baseline": None,
-                    "dtype": w.dtype,
-                    "data": "synthetic",
-                    "config": config,
-                    "cpu_baseline": dict(info, value=round(value, 3)),
-                    "e2e": {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                }
-            )
-        )
+        line = base_line(args, warmup, args.gpus, w.desc, w.kernel, w.dtype, METRIC, extra)
+        line = {"impl": "reference", **line, "value": round(value, 3)}
+        line["cpu_baseline"] = dict(info, value=round(value, 3))
+        line["e2e"] = {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+        print(json.dumps(line))
         return
 
     import torch
@@ -428,6 +813,7 @@ def main() -> None:
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     w.device_buffers(torch)
+    tids = w.check_tids()
 
     res = {}
     for mode in ("plain", "regroup"):
@@ -442,8 +828,7 @@ def main() -> None:
         st = f.stats(raise_on_device_error=True)
         f.set_opts(mode, **opts)
         f.reset_stats()
-        res[mode] = dict(ms=ms, stats=st, fn=f)
-    plain_out_ok, _ = w.check(api)
+        res[mode] = dict(ms=ms, stats=st, fn=f, out=w.outputs_at(tids))
 
     # the headline: the regrouping engine, clocks sampled during the timed region
     f = res["regroup"]["fn"]
@@ -451,7 +836,7 @@ def main() -> None:
         ms_r = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
     st_r = f.stats(raise_on_device_error=True)
     kern_ms = st_r["ms"]
-    parity_ok, idx = w.check(api)
+    out_r = w.outputs_at(tids)
 
     e2e_s, e2e_ok, h2d, d2h = w.e2e(api, torch, args.steps, warmup, dist)
     if dist is not None:
@@ -492,66 +877,59 @@ def main() -> None:
         if t:
             traffic = int(t["dram_bytes_per_thread"] * w.n)
 
-    cpu = None
+    cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
+    plain_regroup_same = same_bits(res["plain"]["out"], out_r)
+    parity["plain_equals_regroup"] = bool(plain_regroup_same)
+    parity["e2e_equals_device"] = bool(e2e_ok)
     if not args.no_cpu:
-        v, info = cpu_reference(w)
+        v, info, want = cpu_reference(w, check_tids=tids)
         cpu = dict(info, value=round(v, 3))
+        parity["checked_against"] = info["kind"]
+        parity["regroup_ok"] = bool(same_bits(out_r, want))
+        parity["plain_ok"] = bool(same_bits(res["plain"]["out"], want))
 
-    line = {
-        "metric": metric,
-        "value": round(value, 3),
-        "unit": "Msamples/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": warmup,
-        "ms_per_step": round(ms_step, 4),
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": w.dtype,
-        "data": "synthetic",
-        "config": config,
-        "plain": {
-            "value": round(plain_value, 3),
-            "ms_per_step": round(plain_ms, 4),
-            "lane_efficiency": round(sp["lane_efficiency"], 4),
-        },
-        "regroup": {
-            "kernel_ms": round(kern_ms, 4),
-            "lane_efficiency": round(sr["lane_efficiency"], 4),
-            "rounds": int(st_r["rounds"] / max(1, st_r["launches"])),
-            "parks_per_thread": round(st_r["parks"] / max(1, st_r["launches"]) / w.n, 4),
-            "state_bytes_per_launch": int(state_per_launch),
-        },
-        "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
-        "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",
-        "parity": {
-            "sample_threads": int(len(idx)),
-            "regroup_device_ok": bool(parity_ok),
-            "plain_device_ok": bool(plain_out_ok),
-            "e2e_ok": bool(e2e_ok),
-        },
-        "roofline": {
-            "bound": "hbm",
-            "achieved": round(achieved, 2),
-            "peak": hbm_peak,
-            "unit": "GB/s",
-            "frac": round(achieved / hbm_peak, 5),
-            "traffic": traffic,
-            "algorithmic_bytes": int(algo_bytes),
-            "peak_source": peak_src,
-            "note": "algorithmic bytes = outputs + inputs + queue-state saves/restores of the regrouping megakernel; the engine is SIMT issue/latency bound, not HBM bound (profiles/)",
-        },
-        "cpu_baseline": cpu,
-        "e2e": {
-            "value": round(world * w.n * args.steps / e2e_s / 1e6, 3),
-            "unit": "Msamples/s",
-            "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h),
-        },
-        "gpu_launches": 2 * args.steps,
-        "clocks": clk.summary(),
-    }
+    line = base_line(args, warmup, world, w.desc, w.kernel, w.dtype, METRIC, extra)
+    line.update(
+        {
+            "value": round(value, 3),
+            "ms_per_step": round(ms_step, 4),
+            "plain": {
+                "value": round(plain_value, 3),
+                "ms_per_step": round(plain_ms, 4),
+                "lane_efficiency": round(sp["lane_efficiency"], 4),
+            },
+            "regroup": {
+                "kernel_ms": round(kern_ms, 4),
+                "lane_efficiency": round(sr["lane_efficiency"], 4),
+                "rounds": int(st_r["rounds"] / max(1, st_r["launches"])),
+                "parks_per_thread": round(st_r["parks"] / max(1, st_r["launches"]) / w.n, 4),
+                "state_bytes_per_launch": int(state_per_launch),
+            },
+            "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
+            "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",
+            "parity": parity,
+            "roofline": {
+                "bound": "hbm",
+                "achieved": round(achieved, 2),
+                "peak": hbm_peak,
+                "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 5),
+                "traffic": traffic,
+                "algorithmic_bytes": int(algo_bytes),
+                "peak_source": peak_src,
+                "note": "algorithmic bytes = outputs + inputs + queue-state saves/restores of the regrouping megakernel; the engine is SIMT issue/latency bound, not HBM bound (profiles/)",
+            },
+            "cpu_baseline": cpu,
+            "e2e": {
+                "value": round(world * w.n * args.steps / e2e_s / 1e6, 3),
+                "unit": "Msamples/s",
+                "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+            },
+            "gpu_launches": 2 * args.steps,
+            "clocks": clk.summary(),
+        }
+    )
     print(json.dumps(line))
     for r in res.values():
         r["fn"].close()

@@ -95,3 +95,12 @@ def test_splitmix_stream_is_fixed():
     # SplitMix64 reference values for seed 0 (Steele et al. 2014)
     z = O.splitmix64(0, 3)
     assert z.tolist() == [0xE220A8397B1DCDAF, 0x6E789E6AA1B965F4, 0x06C45D188009454F]
+
+
+def test_workload_inputs_match_the_oracle_stream():
+    """The bench's input generator (loom_b200.inputs) and the oracle's give
+    the same arrays, so both sides of every parity check read equal inputs."""
+    from loom_b200 import inputs as I
+
+    for seed, n, lo, hi in ((1, 1000, 1, (1 << 32) - 1), (5, 777, 0, 93), (9, 100, 3, (1 << 63) + 5)):
+        assert np.array_equal(I.uniform_int(seed, n, lo, hi), O.uniform_int(seed, n, lo, hi))
