@@ -749,6 +749,44 @@ def serve_main(args, warmup, world, rank, local):
         print(json.dumps(line))
 
 
+def tune_main(args) -> None:
+    """Coordinate search over the regrouping options (loom_b200.autotune) on
+    this workload; writes the best point and the fastest points to a JSON
+    file (merged into loom_b200/tuning.json by the maintainer)."""
+    import torch
+
+    from loom_b200 import api
+    from loom_b200 import autotune as T
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    w = make_workload(args.workload)
+    w.device_buffers(torch)
+    f = api.Function(w.kernel, 0, "regroup")
+    space = dict(T.SPACE)
+    if w.kernel == "sphere_pt_f32":  # 2 x 2832 queue bytes per thread in flight
+        space["population"] = [p for p in space["population"] if p <= 1 << 22]
+
+    def make_launch(opts):
+        f.set_opts("regroup", **opts)
+        return lambda: w.launch(f, api, stream)
+
+    def validate():
+        f.stats(raise_on_device_error=True)
+        f.reset_stats()
+
+    seed = dict(T.DEFAULT, **TUNED[w.kernel])
+    res = T.tune(make_launch, w.n, seed=seed, space=space, budget_s=args.tune_budget,
+                 log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate)
+    res["workload"] = args.workload
+    res["kernel"] = w.kernel
+    res["device"] = torch.cuda.get_device_name(0)
+    pathlib.Path(args.tune).write_text(json.dumps(res, indent=1) + "\n")
+    print(json.dumps({k: res[k] for k in ("kernel", "workload", "best", "ms", "msamples_s")}))
+    f.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -758,6 +796,8 @@ def main() -> None:
     ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
+    ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")
+    ap.add_argument("--tune-budget", type=float, default=300.0, help="seconds of tuning")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -767,6 +807,9 @@ def main() -> None:
 
     if args.workload == "serve":
         serve_main(args, warmup, world, rank, local)
+        return
+    if args.tune:
+        tune_main(args)
         return
 
     w = make_workload(args.workload)

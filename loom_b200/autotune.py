@@ -1,0 +1,141 @@
+"""Autotuner of the regrouping engine's launch options.
+
+The options that decide how well a kernel regroups depend on the kernel and
+on its inputs: how many lanes must agree before a warp keeps running
+(`utr_lanes`), how long a lane runs between votes (`burst`), when every live
+lane runs along (`spread_lanes`), how many block steps a tile gets per round
+(`period`), the threads in flight (`population`, which sizes every work
+queue), the CTA size, the CTAs per SM (the register budget a thread can
+use: fewer CTAs leave more registers per thread) and input prefetching.
+
+`tune` runs a coordinate search: starting from a seed point it tries every
+value of one option with the others fixed, keeps the fastest, moves to the
+next option, and repeats the sweep until a pass brings less than 1 %.
+Every point is timed on the device with CUDA events on the launching
+stream (median of `reps` launches after one warm-up launch).  Results are
+kept in `tuning.json` beside this module, per kernel and workload, and read
+back by `tuned`.
+"""
+
+from __future__ import annotations
+
+import json
+import pathlib
+import statistics
+import time
+from typing import Callable, Dict, List, Optional
+
+HERE = pathlib.Path(__file__).resolve().parent
+TUNING_FILE = HERE / "tuning.json"
+
+SPACE: Dict[str, List] = {
+    "burst": [1, 2, 4, 8, 16, 32, 64],
+    "utr_lanes": [1, 4, 8, 12, 16, 20, 24],
+    "spread_lanes": [1, 8, 16, 24, 33],
+    "period": [256, 1024, 4096, 16384, 65536],
+    "block_size": [128, 256, 512],
+    "population": [1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23],
+    "ctas_per_sm": [0, 1, 2, 4],
+    "prefetch": [True, False],
+}
+
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True)
+
+
+def time_launch(fn: Callable[[], None], reps: int = 2) -> float:
+    """Median device milliseconds of `fn` (launches on torch's current
+    stream), after one warm-up call."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def tune(
+    make_launch: Callable[[Dict], Callable[[], None]],
+    n_threads: int,
+    seed: Optional[Dict] = None,
+    space: Optional[Dict[str, List]] = None,
+    passes: int = 2,
+    reps: int = 2,
+    budget_s: float = 600.0,
+    log: Optional[Callable[[str], None]] = None,
+    validate: Optional[Callable[[], None]] = None,
+) -> Dict:
+    """Coordinate search.  `make_launch(opts)` returns a no-argument callable
+    that launches the workload once with those options; `validate()`, called
+    after each timed point, raises when the launches set a device status.
+    Returns {"best": opts, "ms": t, "points": [...]}."""
+    space = dict(SPACE if space is None else space)
+    cur = dict(DEFAULT if seed is None else seed)
+    for k in space:
+        cur.setdefault(k, space[k][0])
+    cache: Dict[str, float] = {}
+    points = []
+    t_start = time.perf_counter()
+
+    def measure(opts: Dict) -> float:
+        key = json.dumps(opts, sort_keys=True)
+        if key not in cache:
+            if opts.get("population") and opts["population"] < 32:
+                cache[key] = float("inf")
+            else:
+                ms = time_launch(make_launch(opts), reps)
+                if validate:
+                    validate()
+                cache[key] = ms
+                points.append({"opts": dict(opts), "ms": round(ms, 4), "msamples_s": round(n_threads / ms / 1e3, 3)})
+                if log:
+                    log(f"{ms:9.3f} ms  {opts}")
+        return cache[key]
+
+    best = measure(cur)
+    for _ in range(passes):
+        start = best
+        for k, values in space.items():
+            for v in values:
+                if time.perf_counter() - t_start > budget_s:
+                    break
+                cand = dict(cur)
+                cand[k] = v
+                ms = measure(cand)
+                if ms < best:
+                    best, cur = ms, cand
+        if best > 0.99 * start:
+            break
+    return {"best": cur, "ms": round(best, 4), "msamples_s": round(n_threads / best / 1e3, 3), "points": points}
+
+
+def load() -> Dict:
+    return json.loads(TUNING_FILE.read_text()) if TUNING_FILE.exists() else {}
+
+
+def tuned(kernel: str, workload: str = "default") -> Optional[Dict]:
+    """The options stored for (kernel, workload), falling back to the
+    kernel's default entry; None when the kernel was never tuned."""
+    t = load().get(kernel, {})
+    e = t.get(workload) or t.get("default")
+    return None if e is None else dict(e["best"])
+
+
+def store(kernel: str, workload: str, result: Dict, device: str = "", keep_points: int = 12) -> None:
+    data = load()
+    entry = {
+        "best": result["best"],
+        "ms": result["ms"],
+        "msamples_s": result["msamples_s"],
+        "device": device,
+        "points": sorted(result["points"], key=lambda p: p["ms"])[:keep_points],
+    }
+    data.setdefault(kernel, {})[workload] = entry
+    TUNING_FILE.write_text(json.dumps(data, indent=1, sort_keys=True) + "\n")
