@@ -53,12 +53,22 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
-# Regrouping options per kernel, from the sweeps summarised in profiles/
-TUNED = {
+# Regrouping options: the autotuner's results (loom_b200/tuning.json, made
+# by `bench.py --tune`), per kernel and workload; these are the seeds used
+# where a kernel was never tuned.
+FALLBACK = {
     "sphere_pt_f32": dict(burst=4, utr_lanes=8, population=1 << 21, block_size=256, period=4096),
     "collatz_u64": dict(burst=64, utr_lanes=16, block_size=512, period=65536, prefetch=False),
     "fib_u64": dict(burst=64, utr_lanes=16, block_size=512, period=1024, prefetch=False),
 }
+
+
+def regroup_opts(kernel: str, key: str = "default") -> dict:
+    from loom_b200 import autotune as T
+
+    t = T.tuned(kernel, key)
+    return dict(t) if t else dict(FALLBACK[kernel])
+
 
 CHECK_THREADS = 1 << 14  # threads compared with the reference
 
@@ -66,6 +76,7 @@ CHECK_THREADS = 1 << 14  # threads compared with the reference
 # ---------------------------------------------------------------- workloads
 class Workload:
     kernel = ""
+    tune_key = "default"
     desc = ""
     dtype = ""
     n = 0
@@ -88,6 +99,7 @@ class Workload:
 class PathTracing(Workload):
     kernel = "sphere_pt_f32"
     dtype = "f32"
+    tune_key = "pt"
 
     def __init__(self, width=1024, height=768, spp=64):
         from loom_b200 import scenes as S
@@ -118,7 +130,7 @@ class PathTracing(Workload):
 
     def e2e(self, api, torch, steps, warmup, dist):
         h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
-        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+        fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
 
         def step():
             L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, None, self.table)
@@ -138,6 +150,7 @@ class PathTracing(Workload):
 
 
 class BatchedPathTracing(PathTracing):
+    tune_key = "batch"
     """Many render requests of uneven size in one launch: each request has
     its own resolution, sample count and random scene (loom_b200.scenes
     .random_request); threads of all requests share the megakernel and are
@@ -183,7 +196,7 @@ class BatchedPathTracing(PathTracing):
 
     def e2e(self, api, torch, steps, warmup, dist):
         h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
-        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+        fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
 
         def step():
             L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, self.starts, self.table)
@@ -228,7 +241,7 @@ class IntegerLoop(Workload):
     def e2e(self, api, torch, steps, warmup, dist):
         h_in = torch.from_numpy(self.x.view(np.int64)).pin_memory()
         h_out = torch.empty(self.n, dtype=self.d_out[0].dtype).pin_memory()
-        fe = api.Function(self.kernel, self.n, "regroup", **TUNED[self.kernel])
+        fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
         for _ in range(warmup):
             fe.run_host_ptrs([h_in], [h_out], self.n)
         if dist is not None:
@@ -516,6 +529,18 @@ class PinnedPool:
     def put(self, t):
         self.free.setdefault(t.numel(), []).append(t)
 
+    def reserve(self, sizes):
+        """Allocates ahead (outside a timed region) what requests of these
+        byte sizes would take at once."""
+        need = {}
+        for nbytes in sizes:
+            c = 1 << max(12, math.ceil(math.log2(max(1, nbytes))))
+            need[c] = need.get(c, 0) + 1
+        for c, k in need.items():
+            lst = self.free.setdefault(c, [])
+            while len(lst) < k:
+                lst.append(self.torch.empty(c, dtype=self.torch.uint8).pin_memory())
+
 
 class RegroupService:
     """The continuous-batching servers of the three kernels (loom_b200.serving)."""
@@ -532,15 +557,15 @@ class RegroupService:
                 "pt": api.Server(
                     "sphere_pt_f32", ring_threads=1 << 26, max_requests=512, slice_rounds=4,
                     forms=["instance", "local_iota"], header_words=S.HEADER_WORDS, reloc_word=4,
-                    table_words=1 << 20, **TUNED["sphere_pt_f32"], **mk,
+                    table_words=1 << 20, **regroup_opts("sphere_pt_f32", "batch"), **mk,
                 ),
                 "collatz": api.Server(
                     "collatz_u64", ring_threads=1 << 25, max_requests=512, slice_rounds=2,
-                    population=1 << 22, **TUNED["collatz_u64"], **mk,
+                    **{**regroup_opts("collatz_u64"), "population": 1 << 22}, **mk,
                 ),
                 "fib": api.Server(
                     "fib_u64", ring_threads=1 << 23, max_requests=512, slice_rounds=2,
-                    population=1 << 21, **TUNED["fib_u64"], **mk,
+                    **{**regroup_opts("fib_u64"), "population": 1 << 21}, **mk,
                 ),
             }
         )
@@ -597,6 +622,7 @@ class PlainQueue:
 
     def __init__(self, api, torch, stream, pool, inputs, profile=False):
         self.api, self.inputs = api, inputs
+        self.pool = None
         self.f = {
             k: api.Function(v, self.CAPACITY[k], "plain", profile=profile) for k, v in SERVE_KERNELS.items()
         }
@@ -650,9 +676,14 @@ class PlainQueue:
             f.close()
 
 
+OUT_BYTES = {"pt": 12, "collatz": 4, "fib": 8}
+
+
 def run_requests(svc, reqs, arrivals):
     """Feeds `reqs` at `arrivals` (seconds from start) and steps `svc` until
     every request completed.  Returns (latencies, makespan, threads)."""
+    if getattr(svc, "pool", None) is not None:
+        svc.pool.reserve([r[1] * OUT_BYTES[r[0]] for r in reqs])
     t0 = time.perf_counter()
     i, lat, inflight = 0, [], {}
     last = 0.0
@@ -764,6 +795,7 @@ def tune_main(args) -> None:
     w = make_workload(args.workload)
     w.device_buffers(torch)
     f = api.Function(w.kernel, 0, "regroup")
+    w.opts = regroup_opts(w.kernel, w.tune_key)
     space = dict(T.SPACE)
     if w.kernel == "sphere_pt_f32":  # 2 x 2832 queue bytes per thread in flight
         space["population"] = [p for p in space["population"] if p <= 1 << 22]
@@ -776,7 +808,7 @@ def tune_main(args) -> None:
         f.stats(raise_on_device_error=True)
         f.reset_stats()
 
-    seed = dict(T.DEFAULT, **TUNED[w.kernel])
+    seed = dict(T.DEFAULT, **regroup_opts(w.kernel, w.tune_key))
     res = T.tune(make_launch, w.n, seed=seed, space=space, budget_s=args.tune_budget,
                  log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate)
     res["workload"] = args.workload
@@ -813,10 +845,12 @@ def main() -> None:
         return
 
     w = make_workload(args.workload)
+    w.opts = regroup_opts(w.kernel, w.tune_key)
     extra = {
         "threads_per_gpu": w.n,
         "l2": "outputs larger than L2 (no flush)",
-        "regroup_options": TUNED[w.kernel],
+        "regroup_options": w.opts,
+        "regroup_options_from": "loom_b200/tuning.json (bench.py --tune, coordinate search)",
     }
 
     if args.impl == "reference":
@@ -860,7 +894,7 @@ def main() -> None:
 
     res = {}
     for mode in ("plain", "regroup"):
-        opts = TUNED[w.kernel] if mode == "regroup" else {}
+        opts = dict(w.opts, graph=True) if mode == "regroup" else {}
         f = api.Function(w.kernel, 0, mode, **opts)
         ms = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
         f.sync()
@@ -916,8 +950,8 @@ def main() -> None:
     traffic = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
-        t = json.loads(tf.read_text()).get(w.kernel)
-        if t:
+        t = json.loads(tf.read_text()).get(w.tune_key)
+        if t and t.get("kernel") == w.kernel:
             traffic = int(t["dram_bytes_per_thread"] * w.n)
 
     cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
@@ -947,6 +981,7 @@ def main() -> None:
                 "rounds": int(st_r["rounds"] / max(1, st_r["launches"])),
                 "parks_per_thread": round(st_r["parks"] / max(1, st_r["launches"]) / w.n, 4),
                 "state_bytes_per_launch": int(state_per_launch),
+                "graph_launches": int(st_r.get("graph_launches", 0)),
             },
             "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
             "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",

@@ -99,7 +99,10 @@ typedef struct loom_b200_opts
                               burst (33 = majority lanes only) */
     uint32_t no_refill;   /* regroup: halted lanes without a prefetched input
                              wait for the next vote instead of claiming one */
-    uint32_t pad0;
+    uint32_t graph;       /* regroup: capture the launch sequence (queue reset
+                             + engine kernel) into a CUDA graph on first use
+                             and replay it while the launch arguments stay
+                             the same */
     uint64_t population;  /* regroup: resident thread slots; 0 = all inputs */
     uint64_t max_steps;   /* per-thread block-step guard; 0 = 2^40 */
     uint32_t profile;     /* collect lane-efficiency counters (slower) */
@@ -126,6 +129,8 @@ typedef struct loom_b200_stats
     uint32_t status;       /* OR of LOOM_B200_STATUS_* */
     uint32_t grid;         /* CTAs of the last launch */
     double   ms;           /* device time of the last launch (CUDA events) */
+    uint64_t graph_captures; /* CUDA graphs captured (opts.graph) */
+    uint64_t graph_launches; /* launches replayed from a graph */
 } loom_b200_stats;
 
 /* Input column forms (loom_b200_input.form). */
@@ -315,7 +320,7 @@ int loom_b200_server_get_stats(const loom_b200_server* s, loom_b200_server_stats
  * bytes of queue state each (a few tens of bytes for small kernels, 2832 for
  * sphere_pt_f32), and a population the array cannot hold is refused with
  * LOOM_B200_ERR_BUDGET.  `opts` may be NULL (defaults of loom_b200_create);
- * its mode, profile and fault_phantom_ctas fields are ignored.
+ * its mode, profile, graph and fault_phantom_ctas fields are ignored.
  *
  * The first call on a device looks up the array's device address (and so
  * loads it onto that device): make that first call before any stream

@@ -103,7 +103,7 @@ class Opts(ctypes.Structure):
         ("burst", ctypes.c_uint32),
         ("spread_lanes", ctypes.c_uint32),
         ("no_refill", ctypes.c_uint32),
-        ("pad0", ctypes.c_uint32),
+        ("graph", ctypes.c_uint32),
         ("population", ctypes.c_uint64),
         ("max_steps", ctypes.c_uint64),
         ("profile", ctypes.c_uint32),
@@ -126,6 +126,8 @@ class StatsC(ctypes.Structure):
         ("status", ctypes.c_uint32),
         ("grid", ctypes.c_uint32),
         ("ms", ctypes.c_double),
+        ("graph_captures", ctypes.c_uint64),
+        ("graph_launches", ctypes.c_uint64),
     ]
 
 
@@ -367,6 +369,7 @@ def make_opts(
     ctas_per_sm: int = 0,
     fault_phantom_ctas: int = 0,
     barrier_spins: int = 0,
+    graph: bool = False,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -378,7 +381,7 @@ def make_opts(
         burst=burst,
         spread_lanes=spread_lanes,
         no_refill=0 if refill else 1,
-        pad0=0,
+        graph=1 if graph else 0,
         population=population,
         max_steps=max_steps,
         profile=1 if profile else 0,

@@ -122,6 +122,13 @@ struct loom_b200_handle
     void*  d_table      = nullptr;
     size_t table_bytes  = 0;
 
+    // CUDA graph of the regrouping launch sequence (opts.graph)
+    cudaStream_t    cap_stream   = nullptr;
+    cudaGraphExec_t graph_exec   = nullptr;
+    RegroupLaunch   graph_key{};
+    uint64_t        graph_admit  = 0;
+    bool            graph_broken = false; // capture refused: launch directly
+
     loom_b200_stats stats{};
     unsigned        last_grid     = 0;
     bool            pending       = false; // launched, counters not read yet
@@ -226,6 +233,59 @@ finish_launch(loom_b200_handle* h)
     return status ? LOOM_B200_ERR_DEVICE : LOOM_B200_OK;
 }
 
+/// The regrouping launch sequence (queue reset, engine kernel) as a CUDA
+/// graph: captured on first use, replayed while the launch arguments stay
+/// the same, re-captured when they change.  Where capture is refused the
+/// handle falls back to direct launches for good.
+int
+launch_graph(loom_b200_handle* h, const RegroupLaunch& L, uint64_t admit, cudaStream_t stream)
+{
+    const bool same = h->graph_exec && h->graph_admit == admit && h->graph_key.grid == L.grid &&
+                      h->graph_key.block == L.block && h->graph_key.profile == L.profile &&
+                      std::memcmp(&h->graph_key.params, &L.params, sizeof(RegroupParams)) == 0;
+    if(!same)
+    {
+        if(h->graph_exec)
+        {
+            cudaGraphExecDestroy(h->graph_exec);
+            h->graph_exec = nullptr;
+        }
+        if(!h->cap_stream && cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+        {
+            h->graph_broken = true;
+            return LOOM_B200_ERR_CUDA;
+        }
+        RegroupLaunch C = L;
+        C.stream        = h->cap_stream;
+        cudaGraph_t g   = nullptr;
+        cudaError_t err = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal);
+        if(err == cudaSuccess)
+        {
+            regroup_reset<<<1, 256, 0, h->cap_stream>>>(h->d_ctl, h->d_qcnt, h->d_qhead,
+                                                        h->e->num_queues, admit);
+            cudaError_t e1 = cudaGetLastError();
+            cudaError_t e2 = h->e->regroup(C);
+            cudaError_t e3 = cudaStreamEndCapture(h->cap_stream, &g);
+            err            = e1 != cudaSuccess ? e1 : e2 != cudaSuccess ? e2 : e3;
+        }
+        if(err == cudaSuccess) err = cudaGraphInstantiate(&h->graph_exec, g, 0);
+        if(g) cudaGraphDestroy(g);
+        if(err != cudaSuccess)
+        {
+            cudaGetLastError(); // the refusal is not an error of the launch
+            h->graph_exec   = nullptr;
+            h->graph_broken = true;
+            return LOOM_B200_ERR_CUDA;
+        }
+        h->graph_key   = L;
+        h->graph_admit = admit;
+        h->stats.graph_captures += 1;
+    }
+    LB_CUDA(cudaGraphLaunch(h->graph_exec, stream));
+    h->stats.graph_launches += 1;
+    return LOOM_B200_OK;
+}
+
 /// Launch with every pointer of `L` on the device.
 int
 launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
@@ -326,13 +386,13 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         L.block                = block;
         L.profile              = o.profile != 0;
         L.stream               = stream;
-        regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl,
-                                             h->d_qcnt,
-                                             h->d_qhead,
-                                             e.num_queues,
-                                             std::min<uint64_t>(n, cap));
-        LB_CUDA(cudaGetLastError());
-        LB_CUDA(e.regroup(L));
+        const uint64_t admit = std::min<uint64_t>(n, cap);
+        if(!(o.graph && !h->graph_broken && launch_graph(h, L, admit, stream) == LOOM_B200_OK))
+        {
+            regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl, h->d_qcnt, h->d_qhead, e.num_queues, admit);
+            LB_CUDA(cudaGetLastError());
+            LB_CUDA(e.regroup(L));
+        }
         h->last_grid = L.grid;
     }
     else
@@ -503,6 +563,8 @@ loom_b200_destroy(loom_b200_handle* h)
     cudaFree(h->d_ctl);
     if(h->ev0) cudaEventDestroy(h->ev0);
     if(h->ev1) cudaEventDestroy(h->ev1);
+    if(h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+    if(h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if(h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LOOM_B200_OK;

@@ -211,3 +211,26 @@ def test_run_device_with_torch_columns():
         f.sync()
     got = d_out.cpu().numpy().view(np.uint32)
     assert np.array_equal(got, O.val_collatz(n))
+
+
+def test_graph_replay_equals_direct_launch():
+    """opts.graph: the regrouping launch sequence is captured once and
+    replayed while the arguments stay the same; new arguments re-capture."""
+    import torch
+
+    x = O.uniform_int(31, 50000, 1, 1 << 32)
+    d_x = torch.from_numpy(x.view(np.int64)).cuda()
+    outs = [torch.empty(len(x), dtype=torch.int32, device="cuda") for _ in range(2)]
+    with api.Function("collatz_u64", 0, "regroup", graph=True) as f:
+        for _ in range(3):
+            f.run_device([d_x], [outs[0]], len(x))
+            f.sync()
+        s = f.stats(raise_on_device_error=True)
+        assert (s["graph_captures"], s["graph_launches"]) == (1, 3)
+        f.run_device([d_x], [outs[1]], len(x))  # another output column: new graph
+        f.sync()
+        s = f.stats(raise_on_device_error=True)
+        assert (s["graph_captures"], s["graph_launches"]) == (2, 4)
+    want = O.val_collatz(x)
+    for o in outs:
+        assert np.array_equal(o.cpu().numpy().view(np.uint32), want)
