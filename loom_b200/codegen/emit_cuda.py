@@ -342,11 +342,16 @@ def generate(k: Kernel) -> str:
     w("    }")
     w("")
     w("    // Loom's set_inputs: input variables written, every other register zero.")
+    w("    // Only registers live at START are written: the others are written")
+    w("    // before they are read on every path.")
     w("    __device__ __forceinline__ static void")
     w("    start(Regs& R, const In& in)")
     w("    {")
+    live0 = k.liveness()[0][0] if k.blocks else set()
+    in_regs = {reg for reg, _, _ in k.inputs}
     for r in regs:
-        w(f"        R.r{r.idx} = 0;")
+        if r.idx in live0 and r.idx not in in_regs:
+            w(f"        R.r{r.idx} = 0;")
     for i, (reg, t, vname) in enumerate(k.inputs):
         w("        " + L.write(Operand(type=t, reg=reg), f"in.v{i}"))
     w("        (void)in;")

@@ -40,13 +40,11 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
+    // Only registers live at START are written: the others are written
+    // before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
-        R.r0 = 0;
-        R.r1 = 0;
-        R.r2 = 0;
-        R.r3 = 0;
         R.r0 = bitcast<unsigned long long>(static_cast<double>(in.v0));
         R.r1 = static_cast<double>(in.v1);
         R.r2 = static_cast<double>(in.v2);

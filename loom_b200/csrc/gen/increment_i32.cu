@@ -33,10 +33,11 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
+    // Only registers live at START are written: the others are written
+    // before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
-        R.r0 = 0;
         R.r0 = static_cast<int>(in.v0);
         (void)in;
     }

@@ -167,54 +167,17 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
+    // Only registers live at START are written: the others are written
+    // before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
-        R.r1 = 0;
-        R.r2 = 0;
         R.r3 = 0;
         R.r4 = 0;
         R.r5 = 0;
-        R.r6 = 0;
-        R.r7 = 0;
-        R.r8 = 0;
-        R.r9 = 0;
-        R.r10 = 0;
-        R.r11 = 0;
-        R.r12 = 0;
-        R.r13 = 0;
-        R.r14 = 0;
-        R.r15 = 0;
-        R.r16 = 0;
-        R.r17 = 0;
-        R.r18 = 0;
-        R.r19 = 0;
-        R.r20 = 0;
-        R.r21 = 0;
-        R.r22 = 0;
-        R.r23 = 0;
-        R.r24 = 0;
-        R.r25 = 0;
-        R.r26 = 0;
-        R.r27 = 0;
-        R.r28 = 0;
-        R.r29 = 0;
-        R.r30 = 0;
-        R.r31 = 0;
-        R.r32 = 0;
-        R.r33 = 0;
-        R.r34 = 0;
-        R.r35 = 0;
-        R.r36 = 0;
-        R.r37 = 0;
-        R.r38 = 0;
-        R.r39 = 0;
-        R.r40 = 0;
-        R.r41 = 0;
         R.r42 = 0;
         R.r43 = 0;
         R.r44 = 0;
-        R.r45 = 0;
         R.r46 = 0;
         R.r47 = 0;
         R.r48 = 0;
@@ -222,29 +185,6 @@ struct K
         R.r50 = 0;
         R.r51 = 0;
         R.r52 = 0;
-        R.r53 = 0;
-        R.r54 = 0;
-        R.r55 = 0;
-        R.r56 = 0;
-        R.r57 = 0;
-        R.r58 = 0;
-        R.r59 = 0;
-        R.r60 = 0;
-        R.r61 = 0;
-        R.r62 = 0;
-        R.r63 = 0;
-        R.r64 = 0;
-        R.r65 = 0;
-        R.r66 = 0;
-        R.r67 = 0;
-        R.r68 = 0;
-        R.r69 = 0;
-        R.r70 = 0;
-        R.r71 = 0;
-        R.r72 = 0;
-        R.r73 = 0;
-        R.r74 = 0;
-        R.r75 = 0;
         R.r76 = 0;
         R.r77 = 0;
         R.r78 = 0;
@@ -255,54 +195,22 @@ struct K
         R.r83 = 0;
         R.r84 = 0;
         R.r85 = 0;
-        R.r86 = 0;
         R.r87 = 0;
-        R.r88 = 0;
-        R.r89 = 0;
-        R.r90 = 0;
-        R.r91 = 0;
         R.r92 = 0;
         R.r93 = 0;
         R.r94 = 0;
-        R.r95 = 0;
-        R.r96 = 0;
-        R.r97 = 0;
-        R.r98 = 0;
-        R.r99 = 0;
         R.r100 = 0;
         R.r101 = 0;
         R.r102 = 0;
         R.r103 = 0;
         R.r104 = 0;
         R.r105 = 0;
-        R.r106 = 0;
-        R.r107 = 0;
-        R.r108 = 0;
-        R.r109 = 0;
-        R.r110 = 0;
-        R.r111 = 0;
-        R.r112 = 0;
-        R.r113 = 0;
-        R.r114 = 0;
-        R.r115 = 0;
-        R.r116 = 0;
         R.r117 = 0;
         R.r118 = 0;
         R.r119 = 0;
-        R.r120 = 0;
-        R.r121 = 0;
-        R.r122 = 0;
-        R.r123 = 0;
-        R.r124 = 0;
-        R.r125 = 0;
-        R.r126 = 0;
         R.r127 = 0;
         R.r128 = 0;
         R.r129 = 0;
-        R.r130 = 0;
-        R.r131 = 0;
-        R.r132 = 0;
-        R.r133 = 0;
         R.r1 = static_cast<unsigned int>(in.v0);
         R.r2 = static_cast<unsigned int>(in.v1);
         (void)in;
