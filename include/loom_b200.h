@@ -222,6 +222,16 @@ int loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L);
 int loom_b200_sync(loom_b200_handle* h);
 int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);
 int loom_b200_reset_stats(loom_b200_handle* h);
+/* Per basic block, over the profiled launches (opts.profile) since the last
+ * reset: VM instructions executed summed over threads, and issued summed
+ * over warp steps (lane efficiency of block b = thread_instr[b] / (32 *
+ * warp_instr[b])).  num_blocks must equal the kernel's.  Replaces reading
+ * Loom's per-instruction debug trace (src/vm/dbg.hpp:920-1143) for the
+ * question of where lanes go idle. */
+int loom_b200_get_block_stats(loom_b200_handle* h,
+                              uint64_t*         thread_instr,
+                              uint64_t*         warp_instr,
+                              uint32_t          num_blocks);
 
 /* ------------------------------------------------------------ serving
  * Continuous batching of requests on the regrouping engine.  Replaces the

@@ -243,6 +243,7 @@ EXPORTS = [
     "loom_b200_sync",
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
+    "loom_b200_get_block_stats",
     "loom_b200_launch_static",
     "loom_b200_server_create",
     "loom_b200_server_destroy",
@@ -282,6 +283,12 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_sync.argtypes = [vp]
     L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
     L.loom_b200_reset_stats.argtypes = [vp]
+    L.loom_b200_get_block_stats.argtypes = [
+        vp,
+        ctypes.POINTER(ctypes.c_uint64),
+        ctypes.POINTER(ctypes.c_uint64),
+        ctypes.c_uint32,
+    ]
     L.loom_b200_server_create.argtypes = [
         ctypes.c_char_p,
         ctypes.POINTER(Opts),
@@ -525,6 +532,23 @@ class Function:
 
     def reset_stats(self) -> None:
         check(lib().loom_b200_reset_stats(self._h))
+
+    def block_stats(self) -> List[Dict[str, float]]:
+        """Per basic block over the profiled launches since the last reset:
+        VM instructions (thread and warp sums) and lane efficiency."""
+        nb = self.info.num_blocks
+        ti = (ctypes.c_uint64 * nb)()
+        wi = (ctypes.c_uint64 * nb)()
+        check(lib().loom_b200_get_block_stats(self._h, ti, wi, nb))
+        return [
+            {
+                "block": b,
+                "thread_instr": ti[b],
+                "warp_instr": wi[b],
+                "lane_efficiency": ti[b] / (32.0 * wi[b]) if wi[b] else float("nan"),
+            }
+            for b in range(nb)
+        ]
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -435,7 +435,7 @@ def generate(k: Kernel) -> str:
         w(f"    L_B{blk.idx}: // {blk.label}")
         w(f"        if(budget == 0u) return {blk.idx};")
         w("        --budget;")
-        w(f"        if constexpr(kProf) count_block(ctx, {len(blk.instrs)}u);")
+        w(f"        if constexpr(kProf) count_block(ctx, {blk.idx}, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
         o.extend(L.goto_transfer(blk, "        "))
     w("    L_HALT:")

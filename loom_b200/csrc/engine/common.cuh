@@ -70,6 +70,7 @@ struct Ctx
     unsigned long long warp_instr;
     unsigned*          status;
     const Columns*     cols;
+    unsigned long long* blk; // profiled launches: per-block counters in shared memory
 
     __device__ __forceinline__ void
     flag(unsigned bit)
@@ -151,13 +152,39 @@ lanemask_lt()
 /// Counting hook at every block entry of K::run_burst<true>: the lowest
 /// active lane adds the block's instruction count once for the warp, every
 /// lane adds it for itself (lane efficiency = thread / (32 * warp)).
+/// With a per-block array (profiled launches), the lowest lane also adds
+/// the block's thread and warp instructions to entry 2b and 2b + 1 there.
 __device__ __forceinline__ void
-count_block(Ctx& ctx, const unsigned n_instr)
+count_block(Ctx& ctx, const int b, const unsigned n_instr)
 {
     const unsigned active = __activemask();
     if((threadIdx.x & 31) == static_cast<unsigned>(__ffs(active) - 1))
+    {
         ctx.warp_instr += n_instr;
+        if(ctx.blk)
+        {
+            atomicAdd(ctx.blk + 2 * b, static_cast<unsigned long long>(__popc(active)) * n_instr);
+            atomicAdd(ctx.blk + 2 * b + 1, static_cast<unsigned long long>(n_instr));
+        }
+    }
     ctx.thread_instr += n_instr;
+}
+
+/// Shared per-block counters of a profiled launch: cleared at kernel start,
+/// added into dst[0 .. 2 * nb) at the end (every thread of the CTA calls both).
+__device__ __forceinline__ void
+block_counters_clear(unsigned long long* s, const int nb)
+{
+    for(int i = threadIdx.x; i < 2 * nb; i += blockDim.x) s[i] = 0ull;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void
+block_counters_flush(const unsigned long long* s, const int nb, unsigned long long* dst)
+{
+    __syncthreads();
+    for(int i = threadIdx.x; i < 2 * nb; i += blockDim.x)
+        if(s[i]) atomicAdd(dst + i, s[i]);
 }
 
 /// Instance of thread `tid`: the last i with inst_start[i] <= tid.

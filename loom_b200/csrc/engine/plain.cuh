@@ -25,7 +25,9 @@ plain_kernel(const Columns                  cols,
 {
     const unsigned long long tid =
         static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    Ctx ctx{0ull, 0ull, status, &cols};
+    __shared__ unsigned long long s_blk[2 * (kProf ? K::kNumBlocks : 1)];
+    Ctx ctx{0ull, 0ull, status, &cols, kProf ? s_blk : nullptr};
+    if constexpr(kProf) block_counters_clear(s_blk, K::kNumBlocks);
     if(tid < n)
     {
         typename K::Regs R;
@@ -40,7 +42,10 @@ plain_kernel(const Columns                  cols,
         K::store_outputs(R, cols, tid);
     }
     if constexpr(kProf)
+    {
         flush_counters(counters, ctx.thread_instr, ctx.warp_instr, 0ull);
+        block_counters_flush(s_blk, K::kNumBlocks, counters + 8);
+    }
 }
 
 } // namespace loom_b200

@@ -60,7 +60,8 @@ struct RegroupParams
     RegroupCtl*         ctl;
     unsigned*           status;
     // accumulated over launches: 0 thread_instr, 1 warp_instr, 2 parks,
-    // 3 state bytes, 4 threads finished, 5 rounds
+    // 3 state bytes, 4 threads finished, 5 rounds; profiled launches also
+    // add thread / warp instructions of block b to 8 + 2b / 9 + 2b
     unsigned long long* counters;
     unsigned long long  n;
     unsigned long long  max_rounds;
@@ -172,7 +173,9 @@ regroup_kernel(const RegroupParams p)
     constexpr unsigned FULL = 0xffffffffu;
     const unsigned lane  = threadIdx.x & 31u;
     const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    Ctx ctx{0ull, 0ull, p.status, &p.cols};
+    __shared__ unsigned long long s_blk[2 * (kProf ? K::kNumBlocks : 1)];
+    Ctx ctx{0ull, 0ull, p.status, &p.cols, kProf ? s_blk : nullptr};
+    if constexpr(kProf) block_counters_clear(s_blk, K::kNumBlocks);
     unsigned long long parks = 0, sbytes = 0, finished = 0;
     typename K::Regs   R;
     typename K::In     pf;
@@ -356,5 +359,6 @@ regroup_kernel(const RegroupParams p)
 
     flush_counters(p.counters, ctx.thread_instr, ctx.warp_instr, parks);
     flush_counters(p.counters + 3, sbytes, finished, 0ull);
+    if constexpr(kProf) block_counters_flush(s_blk, K::kNumBlocks, p.counters + 8);
 }
 } // namespace loom_b200

@@ -92,7 +92,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r0 = bitcast<unsigned int>(static_cast<float>(op_abs(static_cast<float>(bitcast<float>(R.r0)))));
         R.r0 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r0)) >= static_cast<float>((0x0.0p+0f))));
         goto L_HALT;

@@ -92,7 +92,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r0 = static_cast<unsigned char>(static_cast<bool>(!static_cast<unsigned char>(R.r0)));
         R.r0 = static_cast<unsigned char>(op_min<unsigned char>(static_cast<unsigned char>(R.r0), static_cast<unsigned char>(((unsigned char)0x1ull))));
         goto L_HALT;

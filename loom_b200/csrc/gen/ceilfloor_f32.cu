@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r1 = bitcast<unsigned int>(static_cast<float>(op_ceil(static_cast<float>(R.r0))));
         R.r0 = static_cast<float>(op_floor(static_cast<float>(R.r0)));
         R.r1 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r1)) >= static_cast<float>(R.r0)));

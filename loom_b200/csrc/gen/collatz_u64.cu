@@ -98,14 +98,14 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r2 = static_cast<unsigned int>(((unsigned int)0x0ull));
         R.r3 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         if(R.r3) goto L_HALT; else goto L_B1;
     L_B1: // loop
         if(budget == 0u) return 1;
         --budget;
-        if constexpr(kProf) count_block(ctx, 8u);
+        if constexpr(kProf) count_block(ctx, 1, 8u);
         R.r4 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) & static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r5 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) >> static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r6 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(((unsigned long long)0x3ull))));

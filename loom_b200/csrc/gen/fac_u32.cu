@@ -96,20 +96,20 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r2 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r1) <= static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r1 = static_cast<unsigned int>(((R.r2) ? (((unsigned int)0x1ull)) : (R.r1)));
         if(R.r2) goto L_HALT; else goto L_B1;
     L_B1: // cinit
         if(budget == 0u) return 1;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 1, 2u);
         R.r3 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r1) - static_cast<unsigned int>(((unsigned int)0x1ull))));
         goto L_B2;
     L_B2: // loop
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 2, 4u);
         R.r1 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r1) * static_cast<unsigned int>(R.r3)));
         R.r3 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r3) - static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r2 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r3) == static_cast<unsigned int>(((unsigned int)0x0ull))));

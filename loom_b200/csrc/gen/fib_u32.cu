@@ -99,14 +99,14 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r3 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r1) <= static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r2 = static_cast<unsigned int>(((R.r3) ? (R.r1) : (((unsigned int)0x1ull))));
         if(R.r3) goto L_HALT; else goto L_B1;
     L_B1: // work
         if(budget == 0u) return 1;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 1, 4u);
         R.r4 = static_cast<unsigned int>(((unsigned int)0x0ull));
         R.r2 = static_cast<unsigned int>(((unsigned int)0x1ull));
         R.r5 = static_cast<unsigned int>(((unsigned int)0x2ull));
@@ -114,7 +114,7 @@ struct K
     L_B2: // loop
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kProf) count_block(ctx, 6u);
+        if constexpr(kProf) count_block(ctx, 2, 6u);
         R.r6 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r4) + static_cast<unsigned int>(R.r2)));
         R.r4 = static_cast<unsigned int>(R.r2);
         R.r2 = static_cast<unsigned int>(R.r6);

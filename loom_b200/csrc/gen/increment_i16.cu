@@ -92,7 +92,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 1u);
+        if constexpr(kProf) count_block(ctx, 0, 1u);
         R.r0 = static_cast<short>(static_cast<short>(static_cast<short>(R.r0) + static_cast<short>(((short)0x1ull))));
         goto L_HALT;
     L_HALT:

@@ -96,7 +96,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 1u);
+        if constexpr(kProf) count_block(ctx, 0, 1u);
         switch(R.r1) {
         case 0: goto L_B1;
         case 1: goto L_B2;
@@ -107,25 +107,25 @@ struct K
     L_B1: // l0
         if(budget == 0u) return 1;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 1, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x1ull));
         goto L_HALT;
     L_B2: // l1
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 2, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x3ull));
         goto L_HALT;
     L_B3: // l2
         if(budget == 0u) return 3;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 3, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x7ull));
         goto L_HALT;
     L_B4: // l3
         if(budget == 0u) return 4;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 4, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0xbull));
         goto L_HALT;
     L_HALT:

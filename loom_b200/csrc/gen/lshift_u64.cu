@@ -96,7 +96,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 1u);
+        if constexpr(kProf) count_block(ctx, 0, 1u);
         R.r0 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r0) << static_cast<unsigned long long>(R.r1)));
         goto L_HALT;
     L_HALT:

@@ -99,7 +99,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r3 = static_cast<double>(op_max<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
         R.r4 = static_cast<double>(op_min<double>(static_cast<double>(R.r0), static_cast<double>(R.r1)));
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<double>(R.r3) > static_cast<double>(R.r4)));

@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 6u);
+        if constexpr(kProf) count_block(ctx, 0, 6u);
         R.r1 = static_cast<float>(op_rsqrt(static_cast<float>(bitcast<float>(R.r0))));
         R.r0 = bitcast<unsigned int>(static_cast<float>(op_sqrt(static_cast<float>(bitcast<float>(R.r0)))));
         R.r0 = bitcast<unsigned int>(static_cast<float>(static_cast<float>(static_cast<float>((0x1.0000000000000p+0f)) / static_cast<float>(bitcast<float>(R.r0)))));

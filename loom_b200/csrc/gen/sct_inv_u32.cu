@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r1 = static_cast<unsigned int>(static_cast<unsigned int>(((R.r0) == 0 ? ((unsigned int)0x0ull) : ((R.r0) == 1 ? ((unsigned int)0xaull) : ((R.r0) == 2 ? ((unsigned int)0x14ull) : ((unsigned int)0x1eull))))));
         R.r0 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r0) * static_cast<unsigned int>(((unsigned int)0xaull))));
         R.r1 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r0) == static_cast<unsigned int>(R.r1)));

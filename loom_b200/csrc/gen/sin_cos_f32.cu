@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 8u);
+        if constexpr(kProf) count_block(ctx, 0, 8u);
         R.r1 = static_cast<float>(op_sin(static_cast<float>(bitcast<float>(R.r0))));
         R.r0 = bitcast<unsigned int>(static_cast<float>(op_cos(static_cast<float>(bitcast<float>(R.r0)))));
         R.r1 = static_cast<float>(static_cast<float>(static_cast<float>(R.r1) * static_cast<float>(R.r1)));

@@ -97,7 +97,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 7u);
+        if constexpr(kProf) count_block(ctx, 0, 7u);
         R.r2 = static_cast<unsigned int>(((unsigned int)0x0ull));
         R.r3 = static_cast<unsigned int>(((unsigned int)0xaull));
         R.r4 = static_cast<unsigned int>(((unsigned int)0x14ull));

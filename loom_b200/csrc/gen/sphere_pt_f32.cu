@@ -314,7 +314,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 32u);
+        if constexpr(kProf) count_block(ctx, 0, 32u);
         R.r6 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r1) * static_cast<unsigned int>(((unsigned int)0x10ull))));
         R.r7 = static_cast<unsigned int>(table_load<unsigned int>(*ctx.cols, static_cast<unsigned>(R.r6)));
         R.r8 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r6) + static_cast<unsigned int>(((unsigned int)0x1ull))));
@@ -350,7 +350,7 @@ struct K
     L_B1: // prim
         if(budget == 0u) return 1;
         --budget;
-        if constexpr(kProf) count_block(ctx, 63u);
+        if constexpr(kProf) count_block(ctx, 1, 63u);
         R.r27 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r20) & static_cast<unsigned int>(((unsigned int)0x3ull))));
         R.r28 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r27) & static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r29 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r27) >> static_cast<unsigned int>(((unsigned int)0x1ull))));
@@ -417,7 +417,7 @@ struct K
     L_B2: // bounce
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kProf) count_block(ctx, 5u);
+        if constexpr(kProf) count_block(ctx, 2, 5u);
         R.r53 = static_cast<float>((0x1.93e5960000000p+99f));
         R.r54 = static_cast<unsigned int>(R.r13);
         R.r55 = static_cast<unsigned int>(((unsigned int)0x0ull));
@@ -426,7 +426,7 @@ struct K
     L_B3: // isect
         if(budget == 0u) return 3;
         --budget;
-        if constexpr(kProf) count_block(ctx, 38u);
+        if constexpr(kProf) count_block(ctx, 3, 38u);
         R.r57 = static_cast<float>(table_load<float>(*ctx.cols, static_cast<unsigned>(R.r56)));
         R.r8 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r58 = static_cast<float>(table_load<float>(*ctx.cols, static_cast<unsigned>(R.r8)));
@@ -468,13 +468,13 @@ struct K
     L_B4: // shade
         if(budget == 0u) return 4;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 4, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r54) >= static_cast<unsigned int>(R.r13)));
         if(R.r33) goto L_HALT; else goto L_B5;
     L_B5: // hitp
         if(budget == 0u) return 5;
         --budget;
-        if constexpr(kProf) count_block(ctx, 28u);
+        if constexpr(kProf) count_block(ctx, 5, 28u);
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r54) * static_cast<unsigned int>(((unsigned int)0x8ull))));
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(R.r12)));
         R.r57 = static_cast<float>(table_load<float>(*ctx.cols, static_cast<unsigned>(R.r56)));
@@ -506,7 +506,7 @@ struct K
     L_B6: // emit
         if(budget == 0u) return 6;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 6, 4u);
         R.r3 = static_cast<float>(op_fma(R.r49, R.r76, R.r3));
         R.r4 = static_cast<float>(op_fma(R.r50, R.r77, R.r4));
         R.r5 = static_cast<float>(op_fma(R.r51, R.r78, R.r5));
@@ -514,26 +514,26 @@ struct K
     L_B7: // surf
         if(budget == 0u) return 7;
         --budget;
-        if constexpr(kProf) count_block(ctx, 3u);
+        if constexpr(kProf) count_block(ctx, 7, 3u);
         R.r52 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r52) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r52) >= static_cast<unsigned int>(((unsigned int)0x10ull))));
         if(R.r33) goto L_HALT; else goto L_B8;
     L_B8: // rrchk
         if(budget == 0u) return 8;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 8, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r52) >= static_cast<unsigned int>(((unsigned int)0x5ull))));
         if(R.r33) goto L_B9; else goto L_B12;
     L_B9: // rr_roll
         if(budget == 0u) return 9;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 9, 2u);
         R.r26 = static_cast<unsigned int>(((unsigned int)0x1ull));
         goto L_B23;
     L_B10: // rr
         if(budget == 0u) return 10;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 10, 4u);
         R.r86 = static_cast<float>(op_max<float>(static_cast<float>(R.r76), static_cast<float>(R.r77)));
         R.r86 = static_cast<float>(op_max<float>(static_cast<float>(R.r86), static_cast<float>(R.r78)));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r130)) < static_cast<float>(R.r86)));
@@ -541,7 +541,7 @@ struct K
     L_B11: // rr_keep
         if(budget == 0u) return 11;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 11, 4u);
         R.r76 = static_cast<float>(static_cast<float>(static_cast<float>(R.r76) / static_cast<float>(R.r86)));
         R.r77 = static_cast<float>(static_cast<float>(static_cast<float>(R.r77) / static_cast<float>(R.r86)));
         R.r78 = static_cast<float>(static_cast<float>(static_cast<float>(R.r78) / static_cast<float>(R.r86)));
@@ -549,7 +549,7 @@ struct K
     L_B12: // scatter
         if(budget == 0u) return 12;
         --budget;
-        if constexpr(kProf) count_block(ctx, 18u);
+        if constexpr(kProf) count_block(ctx, 12, 18u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r76)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r77)));
         R.r51 = static_cast<float>(static_cast<float>(static_cast<float>(R.r51) * static_cast<float>(R.r78)));
@@ -576,7 +576,7 @@ struct K
     L_B13: // mirror
         if(budget == 0u) return 13;
         --budget;
-        if constexpr(kProf) count_block(ctx, 5u);
+        if constexpr(kProf) count_block(ctx, 13, 5u);
         R.r95 = static_cast<float>(static_cast<float>(static_cast<float>(R.r87) * static_cast<float>((-0x1.0000000000000p+1f))));
         R.r42 = static_cast<float>(op_fma(R.r95, R.r83, R.r42));
         R.r43 = static_cast<float>(op_fma(R.r95, R.r84, R.r43));
@@ -585,7 +585,7 @@ struct K
     L_B14: // diffuse
         if(budget == 0u) return 14;
         --budget;
-        if constexpr(kProf) count_block(ctx, 26u);
+        if constexpr(kProf) count_block(ctx, 14, 26u);
         R.r96 = static_cast<float>(op_abs(static_cast<float>(R.r92)));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(R.r96) > static_cast<float>((0x1.99999a0000000p-4f))));
         R.r97 = static_cast<float>(((R.r33) ? ((0x0.0p+0f)) : ((0x1.0000000000000p+0f))));
@@ -615,13 +615,13 @@ struct K
     L_B15: // disk_roll
         if(budget == 0u) return 15;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 15, 2u);
         R.r26 = static_cast<unsigned int>(((unsigned int)0x2ull));
         goto L_B23;
     L_B16: // disk
         if(budget == 0u) return 16;
         --budget;
-        if constexpr(kProf) count_block(ctx, 8u);
+        if constexpr(kProf) count_block(ctx, 16, 8u);
         R.r106 = static_cast<float>(static_cast<float>(static_cast<float>(bitcast<float>(R.r130)) * static_cast<float>((0x1.0000000000000p+1f))));
         R.r106 = static_cast<float>(static_cast<float>(static_cast<float>(R.r106) - static_cast<float>((0x1.0000000000000p+0f))));
         R.r107 = static_cast<float>(static_cast<float>(static_cast<float>(bitcast<float>(R.r131)) * static_cast<float>((0x1.0000000000000p+1f))));
@@ -633,7 +633,7 @@ struct K
     L_B17: // disk_ok
         if(budget == 0u) return 17;
         --budget;
-        if constexpr(kProf) count_block(ctx, 20u);
+        if constexpr(kProf) count_block(ctx, 17, 20u);
         R.r109 = static_cast<float>(static_cast<float>(static_cast<float>((0x1.0000000000000p+0f)) - static_cast<float>(R.r108)));
         R.r109 = static_cast<float>(op_sqrt(static_cast<float>(R.r109)));
         R.r42 = static_cast<float>(static_cast<float>(static_cast<float>(R.r100) * static_cast<float>(R.r106)));
@@ -657,7 +657,7 @@ struct K
     L_B18: // glass
         if(budget == 0u) return 18;
         --budget;
-        if constexpr(kProf) count_block(ctx, 13u);
+        if constexpr(kProf) count_block(ctx, 18, 13u);
         R.r110 = static_cast<float>(static_cast<float>(static_cast<float>((0x1.0000000000000p+0f)) / static_cast<float>((0x1.8000000000000p+0f))));
         R.r111 = static_cast<float>(((R.r88) ? (R.r110) : ((0x1.8000000000000p+0f))));
         R.r112 = static_cast<float>((0x0.0p+0f));
@@ -674,7 +674,7 @@ struct K
     L_B19: // refr
         if(budget == 0u) return 19;
         --budget;
-        if constexpr(kProf) count_block(ctx, 40u);
+        if constexpr(kProf) count_block(ctx, 19, 40u);
         R.r115 = static_cast<float>(op_sqrt(static_cast<float>(R.r113)));
         R.r115 = static_cast<float>(op_fma(R.r112, R.r111, R.r115));
         R.r116 = static_cast<float>(static_cast<float>(-static_cast<float>(R.r115)));
@@ -718,13 +718,13 @@ struct K
     L_B20: // fres
         if(budget == 0u) return 20;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 20, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r130)) < static_cast<float>(R.r127)));
         if(R.r33) goto L_B21; else goto L_B22;
     L_B21: // take_refl
         if(budget == 0u) return 21;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 21, 4u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r128)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r128)));
         R.r51 = static_cast<float>(static_cast<float>(static_cast<float>(R.r51) * static_cast<float>(R.r128)));
@@ -732,7 +732,7 @@ struct K
     L_B22: // take_refr
         if(budget == 0u) return 22;
         --budget;
-        if constexpr(kProf) count_block(ctx, 7u);
+        if constexpr(kProf) count_block(ctx, 22, 7u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r129)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r129)));
         R.r51 = static_cast<float>(static_cast<float>(static_cast<float>(R.r51) * static_cast<float>(R.r129)));
@@ -743,7 +743,7 @@ struct K
     L_B23: // roll
         if(budget == 0u) return 23;
         --budget;
-        if constexpr(kProf) count_block(ctx, 292u);
+        if constexpr(kProf) count_block(ctx, 23, 292u);
         R.r130 = static_cast<unsigned int>(R.r24);
         R.r131 = static_cast<unsigned int>(R.r25);
         R.r130 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r130) + static_cast<unsigned int>(R.r11)));

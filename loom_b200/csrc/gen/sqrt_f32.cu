@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 5u);
+        if constexpr(kProf) count_block(ctx, 0, 5u);
         R.r1 = static_cast<float>(static_cast<float>(static_cast<float>(bitcast<float>(R.r0)) * static_cast<float>(bitcast<float>(R.r0))));
         R.r1 = static_cast<float>(op_sqrt(static_cast<float>(R.r1)));
         R.r0 = bitcast<unsigned int>(static_cast<float>(static_cast<float>(static_cast<float>(R.r1) - static_cast<float>(bitcast<float>(R.r0)))));

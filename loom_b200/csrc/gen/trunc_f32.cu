@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 4u);
+        if constexpr(kProf) count_block(ctx, 0, 4u);
         R.r1 = static_cast<float>(op_trunc(static_cast<float>(bitcast<float>(R.r0))));
         R.r1 = static_cast<float>(op_abs(static_cast<float>(R.r1)));
         R.r0 = bitcast<unsigned int>(static_cast<float>(op_abs(static_cast<float>(bitcast<float>(R.r0)))));

@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r1 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r0)) < static_cast<float>((0x1.0000000000000p-1f))));
         R.r0 = static_cast<unsigned int>(((R.r1) ? (((unsigned int)0xc8ull)) : (((unsigned int)0x64ull))));
         goto L_HALT;

@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r1 = static_cast<unsigned long long>(static_cast<bool>(static_cast<double>(bitcast<double>(R.r0)) < static_cast<double>((0x1.0000000000000p-1))));
         R.r0 = static_cast<unsigned long long>(((R.r1) ? (((unsigned long long)0xc8ull)) : (((unsigned long long)0x64ull))));
         goto L_HALT;

@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r1 = bitcast<unsigned int>(static_cast<float>(R.r0));
         R.r1 = static_cast<unsigned int>(bitcast<float>(R.r1));
         goto L_HALT;

@@ -93,7 +93,7 @@ struct K
     L_B0: // START
         if(budget == 0u) return 0;
         --budget;
-        if constexpr(kProf) count_block(ctx, 2u);
+        if constexpr(kProf) count_block(ctx, 0, 2u);
         R.r1 = bitcast<unsigned long long>(static_cast<double>(R.r0));
         R.r1 = static_cast<unsigned long long>(bitcast<double>(R.r1));
         goto L_HALT;

@@ -82,6 +82,13 @@ regroup_reset(RegroupCtl*        ctl,
     }
 }
 
+/// Launch counters: 8 totals, then thread and warp instructions per block.
+size_t
+counter_bytes(const KernelEntry& e)
+{
+    return (8 + 2 * static_cast<size_t>(e.info->num_blocks)) * sizeof(unsigned long long);
+}
+
 constexpr unsigned long long kDefaultMaxSteps    = 1ull << 40;
 constexpr unsigned long long kBarrierSpins       = 1ull << 25;
 constexpr unsigned long long kDefaultStateBudget = 8ull << 30; // queue state bytes
@@ -107,7 +114,7 @@ struct loom_b200_handle
     std::vector<void*> d_in, d_out;
     // device bookkeeping
     unsigned*           d_status   = nullptr;
-    unsigned long long* d_counters = nullptr; // 8 counters
+    unsigned long long* d_counters = nullptr; // 8 counters, then 2 per block (profiled launches)
     // regrouping workspace: the queues with their state, sized for `ws_cap`
     // entries per queue
     uint64_t            ws_cap  = 0;
@@ -524,10 +531,10 @@ loom_b200_create(const char*           kernel,
        cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess)
         return fail(LOOM_B200_ERR_CUDA);
     if(cudaMalloc(&h->d_status, sizeof(unsigned)) != cudaSuccess ||
-       cudaMalloc(&h->d_counters, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+       cudaMalloc(&h->d_counters, counter_bytes(*e)) != cudaSuccess ||
        cudaMalloc(&h->d_ctl, sizeof(RegroupCtl)) != cudaSuccess)
         return fail(LOOM_B200_ERR_OOM);
-    if(cudaMemset(h->d_counters, 0, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+    if(cudaMemset(h->d_counters, 0, counter_bytes(*e)) != cudaSuccess ||
        cudaMemset(h->d_status, 0, sizeof(unsigned)) != cudaSuccess)
         return fail(LOOM_B200_ERR_CUDA);
     const loom_b200_kernel_info& info = *e->info;
@@ -718,12 +725,33 @@ loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats)
 }
 
 int
+loom_b200_get_block_stats(loom_b200_handle* h,
+                          uint64_t*         thread_instr,
+                          uint64_t*         warp_instr,
+                          uint32_t          num_blocks)
+{
+    if(!h || !thread_instr || !warp_instr || num_blocks != h->e->info->num_blocks)
+        return LOOM_B200_ERR_INVALID;
+    const int rc = finish_launch(h);
+    if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
+    std::vector<unsigned long long> c(2 * static_cast<size_t>(num_blocks));
+    LB_CUDA(cudaMemcpy(c.data(), h->d_counters + 8, c.size() * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost));
+    for(uint32_t b = 0; b < num_blocks; ++b)
+    {
+        thread_instr[b] = c[2 * b];
+        warp_instr[b]   = c[2 * b + 1];
+    }
+    return LOOM_B200_OK;
+}
+
+int
 loom_b200_reset_stats(loom_b200_handle* h)
 {
     if(!h) return LOOM_B200_ERR_INVALID;
     const int rc = finish_launch(h);
     if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
-    LB_CUDA(cudaMemset(h->d_counters, 0, 8 * sizeof(unsigned long long)));
+    LB_CUDA(cudaMemset(h->d_counters, 0, counter_bytes(*h->e)));
     LB_CUDA(cudaMemset(h->d_status, 0, sizeof(unsigned)));
     h->stats         = loom_b200_stats{};
     h->launches      = 0;

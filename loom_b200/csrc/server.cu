@@ -433,7 +433,8 @@ loom_b200_server_create(const char*                 kernel,
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_qhead), B * sizeof(unsigned));
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_ctl), sizeof(RegroupCtl));
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_status), sizeof(unsigned));
-    rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_counters), 8 * sizeof(unsigned long long));
+    const size_t cbytes = (8 + 2 * static_cast<size_t>(info.num_blocks)) * sizeof(unsigned long long);
+    rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_counters), cbytes);
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_done), mr * sizeof(unsigned));
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_starts), (mr + 1) * sizeof(unsigned long long));
     rc = rc ? rc : dalloc(s, reinterpret_cast<void**>(&s->d_ids), mr * sizeof(unsigned));
@@ -451,7 +452,7 @@ loom_b200_server_create(const char*                 kernel,
         serve_reset<<<1, 256, 0, s->stream>>>(s->d_ctl, s->d_qcnt, s->d_qhead, e->num_queues);
         if(cudaGetLastError() != cudaSuccess ||
            cudaMemsetAsync(s->d_status, 0, sizeof(unsigned), s->stream) != cudaSuccess ||
-           cudaMemsetAsync(s->d_counters, 0, 8 * sizeof(unsigned long long), s->stream) != cudaSuccess ||
+           cudaMemsetAsync(s->d_counters, 0, cbytes, s->stream) != cudaSuccess ||
            cudaStreamSynchronize(s->stream) != cudaSuccess)
             rc = LOOM_B200_ERR_CUDA;
     }

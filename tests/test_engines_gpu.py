@@ -234,3 +234,19 @@ def test_graph_replay_equals_direct_launch():
     want = O.val_collatz(x)
     for o in outs:
         assert np.array_equal(o.cpu().numpy().view(np.uint32), want)
+
+
+@pytest.mark.parametrize("mode", ["plain", "regroup"])
+def test_block_stats_add_up(mode, golden):
+    """Per-block counters of a profiled launch sum to the launch totals, and
+    every thread executes exactly the oracle's instruction count."""
+    ins, _ = golden("fib_u64")
+    with api.Function("fib_u64", len(ins[0]), mode, profile=True) as f:
+        f(*ins)
+        s = f.stats(raise_on_device_error=True)
+        blocks = f.block_stats()
+    assert sum(b["thread_instr"] for b in blocks) == s["thread_instr"]
+    assert sum(b["warp_instr"] for b in blocks) == s["warp_instr"]
+    _, cnt = O.Interp("fib_u64").run(ins, count_instr=True)
+    assert s["thread_instr"] == int(cnt.sum())
+    assert all(b["warp_instr"] * 32 >= b["thread_instr"] for b in blocks)
