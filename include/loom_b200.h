@@ -113,6 +113,10 @@ typedef struct loom_b200_opts
                                     exist, so its bounded wait must run out */
     uint64_t barrier_spins; /* regroup: polls before a barrier wait gives up
                                (0 = default, about 7 s) */
+    uint32_t cost_model;  /* regroup: per-block quorum from a cost model (a
+                             long block runs only with enough lanes, else its
+                             lanes park and come back as full warps) */
+    uint32_t pad1;
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

@@ -111,6 +111,8 @@ class Opts(ctypes.Structure):
         ("ctas_per_sm", ctypes.c_uint32),
         ("fault_phantom_ctas", ctypes.c_uint32),
         ("barrier_spins", ctypes.c_uint64),
+        ("cost_model", ctypes.c_uint32),
+        ("pad1", ctypes.c_uint32),
     ]
 
 
@@ -377,6 +379,7 @@ def make_opts(
     fault_phantom_ctas: int = 0,
     barrier_spins: int = 0,
     graph: bool = False,
+    cost_model: bool = False,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -396,6 +399,7 @@ def make_opts(
         ctas_per_sm=ctas_per_sm,
         fault_phantom_ctas=fault_phantom_ctas,
         barrier_spins=barrier_spins,
+        cost_model=1 if cost_model else 0,
     )
 
 

@@ -37,9 +37,10 @@ SPACE: Dict[str, List] = {
     "population": [1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23],
     "ctas_per_sm": [0, 1, 2, 4],
     "prefetch": [True, False],
+    "cost_model": [False, True],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:

@@ -310,6 +310,17 @@ def generate(k: Kernel) -> str:
     w(f"__constant__ unsigned kInstrTab[{nb}] = {{{', '.join(map(str, counts))}}};")
     w(f"__constant__ unsigned kLiveTab[{nq}] = {{{', '.join(map(str, qbytes))}}};")
     w(f"__constant__ int kQueueBlock[{nq}] = {{{', '.join(str(b) for b, _ in queues)}}};")
+    # Regrouping cost model: a group of g lanes at block b either runs it
+    # now (I_b warp instructions) or parks (C_b column stores now, C_b loads
+    # per restored tile of 32, then I_b at full width); parking is cheaper
+    # while g < 32 (I_b - C_b) / (I_b + C_b), which is the block's quorum.
+    quorum = []
+    for b in range(nb):
+        cols = max((len(qlive[q]) for q, (qb, _) in enumerate(queues) if qb == b), default=0) + 1
+        ib = counts[b]
+        quorum.append(min(28, max(0, math.ceil(32 * (ib - cols) / (ib + cols)))) if ib > cols else 0)
+    heavy = {b for b in range(nb) if quorum[b] > 0}
+    w(f"__constant__ unsigned kQuorumTab[{nb}] = {{{', '.join(map(str, quorum))}}};")
     w("")
     w("struct K")
     w("{")
@@ -342,12 +353,12 @@ def generate(k: Kernel) -> str:
     w("    }")
     w("")
     w("    // Loom's set_inputs: input variables written, every other register zero.")
-    w("    // Only registers live at START are written: the others are written")
-    w("    // before they are read on every path.")
+    w("    // Only registers live at START (those its queue carries) are written:")
+    w("    // the others are written before they are read on every path.")
     w("    __device__ __forceinline__ static void")
     w("    start(Regs& R, const In& in)")
     w("    {")
-    live0 = k.liveness()[0][0] if k.blocks else set()
+    live0 = qlive[queues.index((0, None))] if k.blocks else set()
     in_regs = {reg for reg, _, _ in k.inputs}
     for r in regs:
         if r.idx in live0 and r.idx not in in_regs:
@@ -376,6 +387,7 @@ def generate(k: Kernel) -> str:
     w("    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }")
     w("    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }")
     w("    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }")
+    w("    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }")
     w("")
     per_block = [[qi for qi, (b, _) in enumerate(queues) if b == blk] for blk in range(nb)]
     maxq = max(len(x) for x in per_block)
@@ -419,12 +431,17 @@ def generate(k: Kernel) -> str:
     w("")
     # ---- run_burst (goto CFG entered at any block, bounded by a budget)
     w("    // Runs the lane's own path from block `entry` for at most `budget`")
-    w("    // blocks; returns the block it stopped at, or kHalt.")
+    w("    // blocks; returns the block it stopped at, or kHalt.  With")
+    w("    // `stop_heavy`, a block whose quorum is above zero is entered only as")
+    w("    // the first block of the burst, when the warp's vote chose it.")
     w("    template <bool kProf>")
     w("    __device__ __forceinline__ static int")
-    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)")
     w("    {")
     w("        (void)ctx;")
+    w("        (void)stop_heavy;")
+    w("        const unsigned first = budget;")
+    w("        (void)first;")
     w("        switch(entry)")
     w("        {")
     for blk in k.blocks:
@@ -433,11 +450,19 @@ def generate(k: Kernel) -> str:
     w("        }")
     for blk in k.blocks:
         w(f"    L_B{blk.idx}: // {blk.label}")
+        transfer = L.goto_transfer(blk, "        ")
+        if blk.idx in heavy:
+            # a lane that loops on the block keeps going; one that comes
+            # from another block waits for the warp's vote
+            w(f"        if(stop_heavy && budget != first) return {blk.idx};")
+            w(f"    L_B{blk.idx}_again:")
+            own = f"goto L_B{blk.idx};"
+            transfer = [t.replace(own, f"goto L_B{blk.idx}_again;") for t in transfer]
         w(f"        if(budget == 0u) return {blk.idx};")
         w("        --budget;")
         w(f"        if constexpr(kProf) count_block(ctx, {blk.idx}, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
-        o.extend(L.goto_transfer(blk, "        "))
+        o.extend(transfer)
     w("    L_HALT:")
     w("        return kHalt;")
     w("    }")

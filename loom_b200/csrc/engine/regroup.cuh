@@ -81,6 +81,9 @@ struct RegroupParams
     unsigned            round0;
     unsigned            slice_rounds;
     unsigned*           inst_done;
+    // Cost model: a block's quorum is the larger of utr and K::quorum(b),
+    // and blocks with a quorum are entered only at the start of a burst.
+    unsigned            cost_model;
 };
 
 __device__ __forceinline__ unsigned
@@ -180,6 +183,13 @@ regroup_kernel(const RegroupParams p)
     typename K::Regs   R;
     typename K::In     pf;
     unsigned long long pf_tid = ~0ull;
+    const bool         cost_on = p.cost_model != 0u;
+    // lanes a group at block b needs to keep running
+    auto need = [&](const int b) -> unsigned
+    {
+        const unsigned q = cost_on ? K::quorum(b) : 0u;
+        return q > p.utr ? q : p.utr;
+    };
     for(unsigned round = p.round0;; ++round)
     {
         const unsigned           cur = round & 1u, nxt = cur ^ 1u;
@@ -249,7 +259,7 @@ regroup_kernel(const RegroupParams p)
                     }
                 }
                 if(pc >= 0 && (mc >= p.spread || pc == m))
-                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst);
+                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
                 steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
@@ -281,14 +291,15 @@ regroup_kernel(const RegroupParams p)
                 }
                 if(steps >= p.period) break;
                 const unsigned cm = __popc(__ballot_sync(FULL, pc == m));
-                if(cm >= p.utr) { mc = cm; continue; }
+                if(cm >= need(m)) { mc = cm; continue; }
+                // the largest group that meets its block's quorum, if any
                 const unsigned peers = __match_any_sync(FULL, pc);
-                const unsigned key = pc >= 0 ? ((static_cast<unsigned>(__popc(peers)) << 16) | static_cast<unsigned>(pc)) : 0u;
-                const unsigned best = __reduce_max_sync(FULL, key);
+                const unsigned gs    = static_cast<unsigned>(__popc(peers));
+                const unsigned key   = pc >= 0 && gs >= need(pc) ? ((gs << 16) | static_cast<unsigned>(pc)) : 0u;
+                const unsigned best  = __reduce_max_sync(FULL, key);
                 if(best == 0u) break;
                 m  = static_cast<int>(best & 0xffffu);
                 mc = best >> 16;
-                if(mc < p.utr) break;
             }
             for(int pass = 0; pass < 2; ++pass)
             {

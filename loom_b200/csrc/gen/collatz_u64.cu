@@ -9,6 +9,7 @@ namespace loom_b200 { namespace k_collatz_u64 {
 __constant__ unsigned kInstrTab[2] = {3, 8};
 __constant__ unsigned kLiveTab[2] = {8, 12};
 __constant__ int kQueueBlock[2] = {0, 1};
+__constant__ unsigned kQuorumTab[2] = {7, 15};
 
 struct K
 {
@@ -38,8 +39,8 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
-    // Only registers live at START are written: the others are written
-    // before they are read on every path.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
@@ -64,6 +65,7 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -83,12 +85,17 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.
+    // blocks; returns the block it stopped at, or kHalt.  With
+    // `stop_heavy`, a block whose quorum is above zero is entered only as
+    // the first block of the burst, when the warp's vote chose it.
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
+        const unsigned first = budget;
+        (void)first;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -96,6 +103,8 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
+        if(stop_heavy && budget != first) return 0;
+    L_B0_again:
         if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 0, 3u);
@@ -103,6 +112,8 @@ struct K
         R.r3 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         if(R.r3) goto L_HALT; else goto L_B1;
     L_B1: // loop
+        if(stop_heavy && budget != first) return 1;
+    L_B1_again:
         if(budget == 0u) return 1;
         --budget;
         if constexpr(kProf) count_block(ctx, 1, 8u);
@@ -113,7 +124,7 @@ struct K
         R.r1 = static_cast<unsigned long long>(((R.r4) ? (R.r6) : (R.r5)));
         R.r2 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r2) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r3 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) != static_cast<unsigned long long>(((unsigned long long)0x1ull))));
-        if(R.r3) goto L_B1; else goto L_HALT;
+        if(R.r3) goto L_B1_again; else goto L_HALT;
     L_HALT:
         return kHalt;
     }

@@ -9,6 +9,7 @@ namespace loom_b200 { namespace k_fac_u64 {
 __constant__ unsigned kInstrTab[3] = {3, 2, 4};
 __constant__ unsigned kLiveTab[3] = {8, 8, 16};
 __constant__ int kQueueBlock[3] = {0, 1, 2};
+__constant__ unsigned kQuorumTab[3] = {7, 0, 5};
 
 struct K
 {
@@ -35,8 +36,8 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
-    // Only registers live at START are written: the others are written
-    // before they are read on every path.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
@@ -61,6 +62,7 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -80,12 +82,17 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.
+    // blocks; returns the block it stopped at, or kHalt.  With
+    // `stop_heavy`, a block whose quorum is above zero is entered only as
+    // the first block of the burst, when the warp's vote chose it.
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
+        const unsigned first = budget;
+        (void)first;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -94,6 +101,8 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
+        if(stop_heavy && budget != first) return 0;
+    L_B0_again:
         if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 0, 3u);
@@ -107,13 +116,15 @@ struct K
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         goto L_B2;
     L_B2: // loop
+        if(stop_heavy && budget != first) return 2;
+    L_B2_again:
         if(budget == 0u) return 2;
         --budget;
         if constexpr(kProf) count_block(ctx, 2, 4u);
         R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r3) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r3) == static_cast<unsigned long long>(((unsigned long long)0x0ull))));
-        if(R.r2) goto L_HALT; else goto L_B2;
+        if(R.r2) goto L_HALT; else goto L_B2_again;
     L_HALT:
         return kHalt;
     }

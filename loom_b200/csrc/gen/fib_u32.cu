@@ -9,6 +9,7 @@ namespace loom_b200 { namespace k_fib_u32 {
 __constant__ unsigned kInstrTab[3] = {3, 4, 6};
 __constant__ unsigned kLiveTab[3] = {4, 4, 16};
 __constant__ int kQueueBlock[3] = {0, 1, 2};
+__constant__ unsigned kQuorumTab[3] = {7, 11, 3};
 
 struct K
 {
@@ -38,8 +39,8 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
-    // Only registers live at START are written: the others are written
-    // before they are read on every path.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
@@ -64,6 +65,7 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -83,12 +85,17 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.
+    // blocks; returns the block it stopped at, or kHalt.  With
+    // `stop_heavy`, a block whose quorum is above zero is entered only as
+    // the first block of the burst, when the warp's vote chose it.
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
+        const unsigned first = budget;
+        (void)first;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -97,6 +104,8 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
+        if(stop_heavy && budget != first) return 0;
+    L_B0_again:
         if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 0, 3u);
@@ -104,6 +113,8 @@ struct K
         R.r2 = static_cast<unsigned int>(((R.r3) ? (R.r1) : (((unsigned int)0x1ull))));
         if(R.r3) goto L_HALT; else goto L_B1;
     L_B1: // work
+        if(stop_heavy && budget != first) return 1;
+    L_B1_again:
         if(budget == 0u) return 1;
         --budget;
         if constexpr(kProf) count_block(ctx, 1, 4u);
@@ -112,6 +123,8 @@ struct K
         R.r5 = static_cast<unsigned int>(((unsigned int)0x2ull));
         goto L_B2;
     L_B2: // loop
+        if(stop_heavy && budget != first) return 2;
+    L_B2_again:
         if(budget == 0u) return 2;
         --budget;
         if constexpr(kProf) count_block(ctx, 2, 6u);
@@ -120,7 +133,7 @@ struct K
         R.r2 = static_cast<unsigned int>(R.r6);
         R.r5 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r5) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r3 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r5) <= static_cast<unsigned int>(R.r1)));
-        if(R.r3) goto L_B2; else goto L_HALT;
+        if(R.r3) goto L_B2_again; else goto L_HALT;
     L_HALT:
         return kHalt;
     }

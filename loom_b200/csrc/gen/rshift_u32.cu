@@ -9,6 +9,7 @@ namespace loom_b200 { namespace k_rshift_u32 {
 __constant__ unsigned kInstrTab[1] = {1};
 __constant__ unsigned kLiveTab[1] = {8};
 __constant__ int kQueueBlock[1] = {0};
+__constant__ unsigned kQuorumTab[1] = {0};
 
 struct K
 {
@@ -36,8 +37,8 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
-    // Only registers live at START are written: the others are written
-    // before they are read on every path.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
@@ -63,6 +64,7 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -82,12 +84,17 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.
+    // blocks; returns the block it stopped at, or kHalt.  With
+    // `stop_heavy`, a block whose quorum is above zero is entered only as
+    // the first block of the burst, when the warp's vote chose it.
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
+        const unsigned first = budget;
+        (void)first;
         switch(entry)
         {
         case 0: goto L_B0;

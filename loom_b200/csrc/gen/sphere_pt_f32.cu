@@ -9,6 +9,7 @@ namespace loom_b200 { namespace k_sphere_pt_f32 {
 __constant__ unsigned kInstrTab[24] = {32, 63, 5, 38, 2, 28, 4, 3, 2, 2, 4, 4, 18, 5, 26, 2, 8, 20, 13, 40, 2, 4, 7, 292};
 __constant__ unsigned kLiveTab[28] = {8, 68, 76, 92, 84, 84, 36, 104, 104, 104, 108, 108, 104, 92, 76, 100, 108, 112, 108, 108, 120, 96, 80, 220, 60, 104, 100, 116};
 __constant__ int kQueueBlock[28] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 23, 23, 23, 23};
+__constant__ unsigned kQuorumTab[24] = {27, 18, 0, 8, 0, 4, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 6, 0, 0, 0, 22};
 
 struct K
 {
@@ -167,50 +168,11 @@ struct K
     }
 
     // Loom's set_inputs: input variables written, every other register zero.
-    // Only registers live at START are written: the others are written
-    // before they are read on every path.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
     __device__ __forceinline__ static void
     start(Regs& R, const In& in)
     {
-        R.r3 = 0;
-        R.r4 = 0;
-        R.r5 = 0;
-        R.r42 = 0;
-        R.r43 = 0;
-        R.r44 = 0;
-        R.r46 = 0;
-        R.r47 = 0;
-        R.r48 = 0;
-        R.r49 = 0;
-        R.r50 = 0;
-        R.r51 = 0;
-        R.r52 = 0;
-        R.r76 = 0;
-        R.r77 = 0;
-        R.r78 = 0;
-        R.r79 = 0;
-        R.r80 = 0;
-        R.r81 = 0;
-        R.r82 = 0;
-        R.r83 = 0;
-        R.r84 = 0;
-        R.r85 = 0;
-        R.r87 = 0;
-        R.r92 = 0;
-        R.r93 = 0;
-        R.r94 = 0;
-        R.r100 = 0;
-        R.r101 = 0;
-        R.r102 = 0;
-        R.r103 = 0;
-        R.r104 = 0;
-        R.r105 = 0;
-        R.r117 = 0;
-        R.r118 = 0;
-        R.r119 = 0;
-        R.r127 = 0;
-        R.r128 = 0;
-        R.r129 = 0;
         R.r1 = static_cast<unsigned int>(in.v0);
         R.r2 = static_cast<unsigned int>(in.v1);
         (void)in;
@@ -235,6 +197,7 @@ struct K
     __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 5;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -277,12 +240,17 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.
+    // blocks; returns the block it stopped at, or kHalt.  With
+    // `stop_heavy`, a block whose quorum is above zero is entered only as
+    // the first block of the burst, when the warp's vote chose it.
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
+        const unsigned first = budget;
+        (void)first;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -312,6 +280,8 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
+        if(stop_heavy && budget != first) return 0;
+    L_B0_again:
         if(budget == 0u) return 0;
         --budget;
         if constexpr(kProf) count_block(ctx, 0, 32u);
@@ -348,6 +318,8 @@ struct K
         R.r26 = static_cast<unsigned int>(((unsigned int)0x0ull));
         goto L_B23;
     L_B1: // prim
+        if(stop_heavy && budget != first) return 1;
+    L_B1_again:
         if(budget == 0u) return 1;
         --budget;
         if constexpr(kProf) count_block(ctx, 1, 63u);
@@ -424,6 +396,8 @@ struct K
         R.r56 = static_cast<unsigned int>(R.r12);
         goto L_B3;
     L_B3: // isect
+        if(stop_heavy && budget != first) return 3;
+    L_B3_again:
         if(budget == 0u) return 3;
         --budget;
         if constexpr(kProf) count_block(ctx, 3, 38u);
@@ -464,7 +438,7 @@ struct K
         R.r55 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r55) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(((unsigned int)0x8ull))));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r55) < static_cast<unsigned int>(R.r13)));
-        if(R.r33) goto L_B3; else goto L_B4;
+        if(R.r33) goto L_B3_again; else goto L_B4;
     L_B4: // shade
         if(budget == 0u) return 4;
         --budget;
@@ -472,6 +446,8 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r54) >= static_cast<unsigned int>(R.r13)));
         if(R.r33) goto L_HALT; else goto L_B5;
     L_B5: // hitp
+        if(stop_heavy && budget != first) return 5;
+    L_B5_again:
         if(budget == 0u) return 5;
         --budget;
         if constexpr(kProf) count_block(ctx, 5, 28u);
@@ -583,6 +559,8 @@ struct K
         R.r44 = static_cast<float>(op_fma(R.r95, R.r85, R.r44));
         goto L_B2;
     L_B14: // diffuse
+        if(stop_heavy && budget != first) return 14;
+    L_B14_again:
         if(budget == 0u) return 14;
         --budget;
         if constexpr(kProf) count_block(ctx, 14, 26u);
@@ -672,6 +650,8 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(R.r113) < static_cast<float>((0x0.0p+0f))));
         if(R.r33) goto L_B13; else goto L_B19;
     L_B19: // refr
+        if(stop_heavy && budget != first) return 19;
+    L_B19_again:
         if(budget == 0u) return 19;
         --budget;
         if constexpr(kProf) count_block(ctx, 19, 40u);
@@ -741,6 +721,8 @@ struct K
         R.r44 = static_cast<float>(R.r119);
         goto L_B2;
     L_B23: // roll
+        if(stop_heavy && budget != first) return 23;
+    L_B23_again:
         if(budget == 0u) return 23;
         --budget;
         if constexpr(kProf) count_block(ctx, 23, 292u);

@@ -90,6 +90,9 @@ REGROUP_VARIANTS = [
     dict(burst=64, spread_lanes=1, utr_lanes=1),
     dict(ctas_per_sm=1, population=37),
     dict(burst=1, utr_lanes=4, population=64),
+    dict(cost_model=True),
+    dict(cost_model=True, burst=16, utr_lanes=24, population=512),
+    dict(cost_model=True, burst=1, utr_lanes=1, period=2),
 ]
 
 
