@@ -423,6 +423,19 @@ def same_bits(got, want) -> bool:
 
 
 # ---------------------------------------------------------------- GPU arm
+def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
+    """The largest `x` over the ranks of the process group (every rank gets
+    it); `x` itself without one.  NCCL groups reduce a CUDA tensor, gloo
+    groups a CPU tensor."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def time_steps(fn, steps: int, warmup: int, torch, dist=None):
     for _ in range(warmup):
         fn()
@@ -439,9 +452,7 @@ def time_steps(fn, steps: int, warmup: int, torch, dist=None):
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         dist.barrier()
     torch.cuda.synchronize()
     return ms
@@ -916,10 +927,7 @@ def main() -> None:
     out_r = w.outputs_at(tids)
 
     e2e_s, e2e_ok, h2d, d2h = w.e2e(api, torch, args.steps, warmup, dist)
-    if dist is not None:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
 
     if rank != 0:
         if dist is not None:

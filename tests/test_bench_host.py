@@ -1,0 +1,91 @@
+"""Host-side logic of bench.py, on CPU: the max-over-ranks reduction of the
+multi-GPU run (two gloo ranks), the serving request mix and the option
+lookup.  No GPU; the GPU arms are exercised on a B200."""
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import bench
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        # each rank's step time; every rank must see the slowest
+        got = bench.max_over_ranks(10.0 + 3.5 * rank, dist, device="cpu")
+        dist.barrier()
+        q.put((rank, got))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_with_two_gloo_ranks():
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs)
+    res = dict(q.get(timeout=5) for _ in procs)
+    assert res == {0: 13.5, 1: 13.5}
+
+
+def test_max_over_ranks_single_process():
+    assert bench.max_over_ranks(7.25) == 7.25
+
+
+def test_serving_mix_is_seeded_and_follows_its_distribution():
+    a = bench.ServeMix(17).draw(400)
+    b = bench.ServeMix(17).draw(400)
+    assert [(r[0], r[1]) for r in a] == [(r[0], r[1]) for r in b]
+    kinds = [r[0] for r in a]
+    assert 0.5 < kinds.count("pt") / len(kinds) < 0.7
+    for kind, n, extra, _ in a:
+        if kind == "collatz":
+            assert 1 << 16 <= n <= 1 << 22 and n & (n - 1) == 0
+            assert 0 <= extra <= bench.SERVE_POOL["collatz"][0] - n
+        elif kind == "fib":
+            assert 1 << 16 <= n <= 1 << 20
+        else:
+            assert n == extra["header"][0] * extra["header"][1] * (1 << extra["header"][2])
+
+
+def test_regroup_options_come_from_the_tuning_file():
+    from loom_b200 import autotune as T
+
+    for kernel in bench.FALLBACK:
+        o = bench.regroup_opts(kernel)
+        assert o, kernel
+        t = T.tuned(kernel)
+        if t is not None:
+            assert o == t
+
+
+def test_reference_runner_without_gpu():
+    """The CPU leg runs and checks on any machine: reference outputs of a
+    few Collatz threads equal the known stopping times."""
+    run, kind, cores = bench._reference_runner()
+    x = np.array([1, 2, 3, 6, 7, 27], dtype=np.uint64)
+    (steps,) = run("collatz_u64", [x], None)
+    assert list(steps) == [0, 1, 7, 8, 16, 111]
+    assert kind in ("reference", "port") and cores >= 1
