@@ -819,7 +819,11 @@ def tune_main(args) -> None:
         f.stats(raise_on_device_error=True)
         f.reset_stats()
 
-    seed = dict(T.DEFAULT, **regroup_opts(w.kernel, w.tune_key))
+    seed = [
+        dict(T.DEFAULT, **regroup_opts(w.kernel, w.tune_key)),
+        dict(T.DEFAULT, cost_model=True, utr_lanes=4, burst=32),
+        dict(T.DEFAULT),
+    ]
     res = T.tune(make_launch, w.n, seed=seed, space=space, budget_s=args.tune_budget,
                  log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate)
     res["workload"] = args.workload

@@ -10,7 +10,9 @@ use: fewer CTAs leave more registers per thread) and input prefetching.
 
 `tune` runs a coordinate search: starting from a seed point it tries every
 value of one option with the others fixed, keeps the fastest, moves to the
-next option, and repeats the sweep until a pass brings less than 1 %.
+next option, and repeats the sweep until a pass brings less than 1 %.  With
+several seeds (the stored point, the defaults with and without the cost
+model) it searches from each and keeps the fastest point found.
 Every point is timed on the device with CUDA events on the launching
 stream (median of `reps` launches after one warm-up launch).  Results are
 kept in `tuning.json` beside this module, per kernel and workload, and read
@@ -65,7 +67,7 @@ def time_launch(fn: Callable[[], None], reps: int = 2) -> float:
 def tune(
     make_launch: Callable[[Dict], Callable[[], None]],
     n_threads: int,
-    seed: Optional[Dict] = None,
+    seed=None,
     space: Optional[Dict[str, List]] = None,
     passes: int = 2,
     reps: int = 2,
@@ -78,9 +80,7 @@ def tune(
     after each timed point, raises when the launches set a device status.
     Returns {"best": opts, "ms": t, "points": [...]}."""
     space = dict(SPACE if space is None else space)
-    cur = dict(DEFAULT if seed is None else seed)
-    for k in space:
-        cur.setdefault(k, space[k][0])
+    seeds = [DEFAULT] if seed is None else (list(seed) if isinstance(seed, (list, tuple)) else [seed])
     cache: Dict[str, float] = {}
     points = []
     t_start = time.perf_counter()
@@ -100,21 +100,33 @@ def tune(
                     log(f"{ms:9.3f} ms  {opts}")
         return cache[key]
 
-    best = measure(cur)
-    for _ in range(passes):
-        start = best
-        for k, values in space.items():
-            for v in values:
-                if time.perf_counter() - t_start > budget_s:
-                    break
-                cand = dict(cur)
-                cand[k] = v
-                ms = measure(cand)
-                if ms < best:
-                    best, cur = ms, cand
-        if best > 0.99 * start:
-            break
-    return {"best": cur, "ms": round(best, 4), "msamples_s": round(n_threads / best / 1e3, 3), "points": points}
+    overall, overall_ms = None, float("inf")
+    for sd in seeds:
+        cur = dict(sd)
+        for k in space:
+            cur.setdefault(k, DEFAULT.get(k, space[k][0]))
+        best = measure(cur)
+        for _ in range(passes):
+            start = best
+            for k, values in space.items():
+                for v in values:
+                    if time.perf_counter() - t_start > budget_s:
+                        break
+                    cand = dict(cur)
+                    cand[k] = v
+                    ms = measure(cand)
+                    if ms < best:
+                        best, cur = ms, cand
+            if best > 0.99 * start:
+                break
+        if best < overall_ms:
+            overall, overall_ms = cur, best
+    return {
+        "best": overall,
+        "ms": round(overall_ms, 4),
+        "msamples_s": round(n_threads / overall_ms / 1e3, 3),
+        "points": points,
+    }
 
 
 def load() -> Dict:
