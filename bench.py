@@ -18,6 +18,9 @@ Other workloads:
            scene, in one launch (about 473 M threads)
   collatz  2^24 threads, n ~ U[1, 2^32)
   fib      2^20 threads, n ~ U{0..93}
+  loom_pt, loom_pt2
+           Loom's own path tracers (pt_const, pt2_const) at the 40x40
+           configurations of its published CPU results
   serve    the serving loop: Poisson arrivals of a request mix (60 % render
            requests as in `batch`, 20 % Collatz batches of 2^16-2^22 inputs,
            20 % Fibonacci batches of 2^16-2^20 inputs) at 25/50/75/100 % of
@@ -25,7 +28,7 @@ Other workloads:
            continuous-batching servers beside a plain-engine FIFO queue.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pt|pt_small|batch|collatz|fib|serve]
+                    [--workload pt|pt_small|batch|collatz|fib|loom_pt|loom_pt2|serve]
 
 Under torchrun each rank runs the full workload on its own GPU (weak
 scaling, no data-path collective: Loom threads are independent), times with
@@ -60,6 +63,8 @@ FALLBACK = {
     "sphere_pt_f32": dict(burst=4, utr_lanes=8, population=1 << 21, block_size=256, period=4096),
     "collatz_u64": dict(burst=64, utr_lanes=16, block_size=512, period=65536, prefetch=False),
     "fib_u64": dict(burst=64, utr_lanes=16, block_size=512, period=1024, prefetch=False),
+    "pt_const_40": dict(cost_model=True, utr_lanes=4, burst=32, block_size=128),
+    "pt2_const_40": dict(cost_model=True, utr_lanes=4, burst=32, block_size=128),
 }
 
 
@@ -150,11 +155,12 @@ class PathTracing(Workload):
 
 
 class BatchedPathTracing(PathTracing):
-    tune_key = "batch"
     """Many render requests of uneven size in one launch: each request has
     its own resolution, sample count and random scene (loom_b200.scenes
     .random_request); threads of all requests share the megakernel and are
     mapped to (request, sample) on the device from the instance offsets."""
+
+    tune_key = "batch"
 
     def __init__(self, count=256, seed=3):
         from loom_b200 import scenes as S
@@ -255,7 +261,60 @@ class IntegerLoop(Workload):
         return dt, ok, self.n * self.in_bytes, self.n * self.out_bytes
 
 
+class LoomPathTracer(Workload):
+    """Loom's own path tracers (src/smallpt/vm/pt.hpp) at the 40x40
+    configurations of its published results: one Loom thread per pixel,
+    adaptive sampling up to 64 samples (blur 1, depth 2, threshold 1e-4 for
+    pt_const, 1e-3 for pt2_const).  A step renders the image once."""
+
+    dtype = "f32"
+
+    def __init__(self, kernel, threshold):
+        self.kernel = kernel
+        self.tune_key = "default"
+        x, y = np.meshgrid(np.arange(40, dtype=np.uint32), np.arange(40, dtype=np.uint32))
+        self.pixels = ((x << 16) | y).reshape(-1)
+        self.n = len(self.pixels)
+        self.desc = (
+            f"Loom's {kernel.rsplit('_', 1)[0]} (src/smallpt/vm/pt.hpp), 40x40 pixels, up to 64 adaptive samples, "
+            f"blur 1, threshold {threshold}, depth 2: one thread per pixel, {self.n} threads per step"
+        )
+        self.in_bytes = 4
+        self.out_bytes = 20
+
+    def device_buffers(self, torch):
+        self.d_in = torch.from_numpy(self.pixels.view(np.int32)).cuda()
+        self.d_out = [torch.empty(self.n, dtype=torch.float32, device="cuda") for _ in range(3)]
+        self.d_out += [torch.empty(self.n, dtype=torch.int32, device="cuda") for _ in range(2)]
+
+    def launch(self, f, api, stream):
+        f.run_device([self.d_in], self.d_out, self.n, stream=stream)
+
+    def ref_inputs(self, tids):
+        return [self.pixels[np.asarray(tids, dtype=np.int64)]], None
+
+    def e2e(self, api, torch, steps, warmup, dist):
+        h_in = torch.from_numpy(self.pixels.view(np.int32)).pin_memory()
+        h_out = [torch.empty(self.n, dtype=o.dtype).pin_memory() for o in self.d_out]
+        fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
+        for _ in range(warmup):
+            fe.run_host_ptrs([h_in], h_out, self.n)
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            fe.run_host_ptrs([h_in], h_out, self.n)
+        dt = time.perf_counter() - t0
+        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_out, self.d_out))
+        fe.close()
+        return dt, ok, self.n * self.in_bytes, self.n * self.out_bytes
+
+
 def make_workload(name):
+    if name == "loom_pt":
+        return LoomPathTracer("pt_const_40", "1e-4")
+    if name == "loom_pt2":
+        return LoomPathTracer("pt2_const_40", "1e-3")
     if name == "pt":
         return PathTracing()
     if name == "pt_small":  # the profiling case: same scene at 256x192
@@ -840,7 +899,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "serve"])
+    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")

@@ -3,8 +3,8 @@ nvcc compilation for sm_100a.
 
 Steps
   1. extract  (only where the Loom headers are available, LOOM_REF_DIR or the
-              default location): compile loom_b200/frontend/extract_main.cpp
-              with g++ and rewrite loom_b200/ir/*.lir from the kernel types;
+              default location): one small g++ program per registry kernel
+              prints its IR; loom_b200/ir/*.lir are rewritten where changed;
   2. generate loom_b200/csrc/gen/<kernel>.cu for every .lir file;
   3. compile  every .cu with nvcc -gencode arch=compute_100a,code=sm_100a and
               link loom_b200/libloom_b200.so.
@@ -17,6 +17,7 @@ from __future__ import annotations
 import concurrent.futures as cf
 import os
 import pathlib
+import re
 import shutil
 import subprocess
 import sys
@@ -73,39 +74,85 @@ def run(cmd: List[str], **kw) -> None:
 
 
 # ---------------------------------------------------------------- 1. extract
-def extract(ref: pathlib.Path, names: Optional[List[str]] = None) -> None:
-    """Rebuild the text IR of the registry kernels from their Loom types."""
-    exe = ROOT / "_build" / "loom_extract"
-    exe.parent.mkdir(parents=True, exist_ok=True)
-    srcs = [PKG / "frontend" / "extract_main.cpp", PKG / "frontend" / "ir_emit.hpp"]
-    srcs += list((PKG / "kernels").glob("*.hpp"))
-    if not exe.exists() or max(s.stat().st_mtime for s in srcs) > exe.stat().st_mtime:
-        run(
-            [
-                "g++",
-                "-std=c++20",
-                "-O1",
-                "-fno-exceptions",
-                "-w",
-                "-ftemplate-depth=4096",
-                "-fconstexpr-depth=4096",
-                "-fconstexpr-ops-limit=1000000000",
-                f"-I{ref / 'src'}",
-                f"-I{ref / 'ext' / 'include'}",
-                f"-I{PKG / 'frontend' / 'shim'}",
-                str(srcs[0]),
-                "-o",
-                str(exe),
-            ]
-        )
+# Deep template limits: Loom's larger kernels (its own path tracers) nest
+# type lists thousands deep.
+TEMPLATE_FLAGS = [
+    "-ftemplate-depth=16384",
+    "-fconstexpr-depth=16384",
+    "-fconstexpr-ops-limit=4000000000",
+]
+
+
+def registry_kernels() -> List[tuple]:
+    """(name, C++ type) of every X(name, type) line of the registry."""
+    out = []
+    for ln in (PKG / "kernels" / "registry.hpp").read_text().splitlines():
+        m = re.match(r"\s*X\((\w+),\s*(.*?)\)\s*\\?\s*$", ln)
+        if m:
+            out.append((m.group(1), m.group(2).strip()))
+    return out
+
+
+def _write_if_changed(p: pathlib.Path, text: str) -> None:
+    if not p.exists() or p.read_text() != text:
+        p.write_text(text)
+
+
+def extract(ref: pathlib.Path, names: Optional[List[str]] = None, jobs: Optional[int] = None) -> None:
+    """Rebuild the text IR of the registry kernels from their Loom types: one
+    small program per kernel (compiled in parallel, without optimisation, as
+    it runs once) prints the kernel's IR."""
+    work = ROOT / "_build" / "extract"
+    work.mkdir(parents=True, exist_ok=True)
+    deps = [PKG / "frontend" / "ir_emit.hpp", PKG / "frontend" / "b200_ops.hpp"]
+    deps += list((PKG / "kernels").glob("*.hpp"))
+    dep_mtime = max(d.stat().st_mtime for d in deps)
     IR_DIR.mkdir(exist_ok=True)
-    tmp = ROOT / "_build" / "ir_tmp"
-    tmp.mkdir(parents=True, exist_ok=True)
-    run([str(exe), str(tmp), *(names or [])])
-    for f in tmp.glob("*.lir"):
-        dst = IR_DIR / f.name
-        if not dst.exists() or dst.read_text() != f.read_text():
-            shutil.copyfile(f, dst)
+    todo = [(n, t) for n, t in registry_kernels() if not names or n in names]
+
+    def one(item) -> None:
+        name, ty = item
+        src = work / f"{name}.cpp"
+        exe = work / name
+        _write_if_changed(
+            src,
+            "// IR extractor of one registry kernel (generated by loom_b200/build.py).\n"
+            '#include "ir_emit.hpp"\n'
+            '#include "registry.hpp"\n'
+            "#include <fstream>\n"
+            "int main(int argc, char* argv[])\n{\n"
+            "    if(argc < 2) return 2;\n"
+            "    std::ofstream f(argv[1]);\n"
+            f'    f << loom::vm::b200::ir::emit<{ty}>("{name}");\n'
+            "    return f ? 0 : 1;\n}\n",
+        )
+        if not exe.exists() or max(dep_mtime, src.stat().st_mtime) > exe.stat().st_mtime:
+            run(
+                [
+                    "g++",
+                    "-std=c++20",
+                    "-O0",
+                    "-fno-exceptions",
+                    "-w",
+                    *TEMPLATE_FLAGS,
+                    f"-I{PKG / 'frontend'}",
+                    f"-I{PKG / 'kernels'}",
+                    f"-I{ref / 'src'}",
+                    f"-I{ref / 'ext' / 'include'}",
+                    f"-I{PKG / 'frontend' / 'shim'}",
+                    str(src),
+                    "-o",
+                    str(exe),
+                ]
+            )
+        tmp = work / f"{name}.lir"
+        run([str(exe), str(tmp)])
+        dst = IR_DIR / f"{name}.lir"
+        if not dst.exists() or dst.read_text() != tmp.read_text():
+            shutil.copyfile(tmp, dst)
+
+    with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        list(ex.map(one, todo))
 
 
 # ---------------------------------------------------------------- 2. generate
@@ -123,11 +170,6 @@ def generate() -> List[str]:
         if stale.stem not in names and stale.stem != "registry":
             stale.unlink()
     return names
-
-
-def _write_if_changed(p: pathlib.Path, text: str) -> None:
-    if not p.exists() or p.read_text() != text:
-        p.write_text(text)
 
 
 # ---------------------------------------------------------------- 3. compile

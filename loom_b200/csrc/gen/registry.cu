@@ -31,6 +31,8 @@ extern const loom_b200::KernelEntry loom_b200_entry_lshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_lshift_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f64;
+extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_40;
+extern const loom_b200::KernelEntry loom_b200_entry_pt_const_40;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u16;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u64;
@@ -77,6 +79,8 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_lshift_u64,
     &loom_b200_entry_minmax_f32,
     &loom_b200_entry_minmax_f64,
+    &loom_b200_entry_pt2_const_40,
+    &loom_b200_entry_pt_const_40,
     &loom_b200_entry_rshift_u16,
     &loom_b200_entry_rshift_u32,
     &loom_b200_entry_rshift_u64,
@@ -92,5 +96,5 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 43;
+const int kRegistrySize = 45;
 } // namespace loom_b200

@@ -8,9 +8,12 @@
 ///
 /// The reference's own test programs (Loom src/tests/programs.hpp) are
 /// included unchanged: they are the kernels Loom's backends are tested on
-/// (src/tests/vm.cpp:266-328, src/tests/vm.cu:76-86).
+/// (src/tests/vm.cpp:266-328, src/tests/vm.cu:76-86); so are its path-tracing
+/// kernels (src/smallpt/vm/pt.hpp), at the configurations of its published
+/// benchmarks (src/benchmarks/pt.cpp:30-35).
 #pragma once
 
+#include <smallpt/vm/pt.hpp>
 #include <tests/programs.hpp>
 
 #include "collatz.hpp"
@@ -37,6 +40,11 @@ using std::uint8_t;
     X(fib_u32,            fib_test<std::uint32_t>)                             \
     X(collatz_u64,        loom::vm::b200::kernels::collatz<std::uint64_t>)     \
     X(sphere_pt_f32,      loom::vm::b200::kernels::sphere_pt<float>)           \
+    /* Loom's own path tracers (src/smallpt/vm/pt.hpp:1259-1729) at the  */    \
+    /* 40x40 configurations of its published benchmark results: 64      */    \
+    /* samples, blur 1, depth 2, threshold 1e-4 (v1) and 1e-3 (v2)       */    \
+    X(pt_const_40,        loom::vm::pt_const<float, loom::vm::constants<CS(40), CS(0.0001), CS(64), CS(1), CS(2)>>) \
+    X(pt2_const_40,       loom::vm::pt2_const<float, loom::vm::constants<CS(40), CS(0.001), CS(64), CS(1), CS(2)>>) \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

@@ -71,9 +71,26 @@ def make_pt(name: str) -> pathlib.Path:
     return path
 
 
+def loom_pt_pixels(width: int = 40, height: int = 40):
+    """Every pixel of a Loom path-tracer render, encoded as Loom's demo does
+    (x << 16 | y, src/smallpt/vm/enc.hpp:30-34), in row order."""
+    import numpy as np
+
+    x, y = np.meshgrid(np.arange(width, dtype=np.uint32), np.arange(height, dtype=np.uint32))
+    return ((x << 16) | y).reshape(-1)
+
+
 def make(name: str) -> pathlib.Path:
     if name.startswith("sphere_pt"):
         return make_pt(name)
+    if name.startswith(("pt_const", "pt2_const")):
+        ins = [loom_pt_pixels()]
+        outs = O.ref_run(name, ins, len(ins[0]), threads=8)
+        arrays = {"in0": ins[0]}
+        arrays.update({f"out{j}": a for j, a in enumerate(outs)})
+        path = HERE / f"{name}.npz"
+        np.savez_compressed(path, **arrays)
+        return path
     ins_t, _ = _ir_io(name)
     n = SIZES.get(name, DEFAULT_N)
     ins = D.inputs_for(name, n, SEED, ins_t)
@@ -95,8 +112,10 @@ def main() -> None:
         raise SystemExit("Loom headers not found: set LOOM_REF_DIR")
     from loom_b200.codegen import ir
 
+    wanted = sys.argv[1:]
     for name in ir.available():
-        print(make(name))
+        if not wanted or name in wanted:
+            print(make(name))
 
 
 if __name__ == "__main__":

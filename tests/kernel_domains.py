@@ -57,6 +57,10 @@ def inputs_for(name: str, n: int, seed: int, input_types: List[str]) -> List[np.
             a = np.where(a == info.max, info.max - 1, a).astype(dt)
         elif name.startswith(("jmp4", "sct_inv", "slt_inv")):
             a = _ints(s, n, 0, 3, dt)
+        elif name.startswith(("pt_const", "pt2_const")):
+            # pixels of the 40x40 render, encoded x << 16 | y as Loom's demo does
+            xy = _ints(s, n, 0, 40 * 40 - 1, np.uint32)
+            a = (((xy % 40) << 16) | (xy // 40)).astype(dt)
         elif name.startswith(("lshift", "rshift")):
             a = _ints(s, n, 2, 10, dt)
         elif name.startswith("bool"):

@@ -98,7 +98,7 @@ REGROUP_VARIANTS = [
 
 @pytest.mark.parametrize("variant", REGROUP_VARIANTS, ids=lambda v: ",".join(f"{k}={x}" for k, x in v.items()))
 @pytest.mark.parametrize(
-    "name", ["fib_u64", "collatz_u64", "fac_u64", "jmp4_u64", "union_cmov_f32", "slt_inv_u32", "sphere_pt_f32"]
+    "name", ["fib_u64", "collatz_u64", "fac_u64", "jmp4_u64", "union_cmov_f32", "slt_inv_u32", "sphere_pt_f32", "pt_const_40"]
 )
 def test_regroup_options_keep_results(name, variant, golden, golden_extra):
     ins, outs = golden(name)

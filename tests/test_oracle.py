@@ -19,9 +19,18 @@ def _bits(a):
     return np.ascontiguousarray(a).view(np.uint8)
 
 
+# Loom's own path tracers run up to 64 adaptive samples per pixel: the C
+# restatement checks a seeded subset of their 1600 pixels to stay fast.
+SUBSET = {"pt_const_40": 160, "pt2_const_40": 160}
+
+
 @pytest.mark.parametrize("name", KERNELS)
 def test_interp_matches_golden(name, golden, golden_extra):
     ins, outs = golden(name)
+    if name in SUBSET:
+        idx = np.sort(O.uniform_int(3, SUBSET[name], 0, len(ins[0]) - 1).astype(np.int64))
+        ins = [a[idx] for a in ins]
+        outs = [a[idx] for a in outs]
     got = O.Interp(name).run(ins, table=golden_extra(name).get("table"))
     assert len(got) == len(outs)
     for g, o in zip(got, outs):
