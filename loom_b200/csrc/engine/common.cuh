@@ -119,9 +119,13 @@ __device__ __forceinline__ float op_trunc(float v) { return truncf(v); }
 __device__ __forceinline__ double op_trunc(double v) { return trunc(v); }
 __device__ __forceinline__ float op_sqrt(float v) { return sqrtf(v); }
 __device__ __forceinline__ double op_sqrt(double v) { return sqrt(v); }
-__device__ __forceinline__ float op_sin(float v) { return sinf(v); }
+// Float sin and cos are evaluated in double and rounded once to float: the
+// result is the correctly rounded value except within a hair of a rounding
+// boundary, which is what the host's libm (the scalar backend's std::sin,
+// operators.hpp:314-325) returns for all but a few arguments.
+__device__ __forceinline__ float op_sin(float v) { return static_cast<float>(sin(static_cast<double>(v))); }
 __device__ __forceinline__ double op_sin(double v) { return sin(v); }
-__device__ __forceinline__ float op_cos(float v) { return cosf(v); }
+__device__ __forceinline__ float op_cos(float v) { return static_cast<float>(cos(static_cast<double>(v))); }
 __device__ __forceinline__ double op_cos(double v) { return cos(v); }
 __device__ __forceinline__ float op_copysign(float a, float b) { return copysignf(a, b); }
 __device__ __forceinline__ double op_copysign(double a, double b) { return copysign(a, b); }

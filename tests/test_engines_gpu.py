@@ -28,8 +28,22 @@ def _as_list(x):
     return list(x) if isinstance(x, tuple) else [x]
 
 
+# Bit-exact everywhere except where a kernel's float results go through the
+# host libm's sinf/cosf, which the device matches to within an ulp (it
+# evaluates them in double and rounds once): Loom's pt2_const_40 calls them
+# on every bounce.  There every float output is held within ULP_TOLERANCE
+# units in the last place of the scalar backend's value, and integer outputs
+# (ray counts, pixel ids) stay exact.
+ULP_TOLERANCE = {"pt2_const_40": 4}
+
+
 def _check(name, got, want):
     for g, w in zip(got, want):
+        if name in ULP_TOLERANCE and np.asarray(w).dtype.kind == "f":
+            g, w = np.asarray(g), np.asarray(w)
+            ulps = np.abs(g.astype(np.float64) - w.astype(np.float64)) / np.spacing(np.abs(w)).astype(np.float64)
+            assert float(ulps.max()) <= ULP_TOLERANCE[name], f"{name}: {float(ulps.max())} ulp apart"
+            continue
         assert np.array_equal(_bits(g), _bits(w)), f"{name}: {int((g != w).sum())} threads differ"
 
 
@@ -253,3 +267,16 @@ def test_block_stats_add_up(mode, golden):
     _, cnt = O.Interp("fib_u64").run(ins, count_instr=True)
     assert s["thread_instr"] == int(cnt.sum())
     assert all(b["warp_instr"] * 32 >= b["thread_instr"] for b in blocks)
+
+
+def test_loom_pt2_engines_agree_bit_for_bit(golden):
+    """Where the scalar backend is matched within ULP_TOLERANCE (libm sin and
+    cos), the two engines still agree with each other exactly."""
+    ins, _ = golden("pt2_const_40")
+    got = {}
+    for mode in ("plain", "regroup"):
+        with api.Function("pt2_const_40", len(ins[0]), mode) as f:
+            got[mode] = _as_list(f(*ins))
+            f.stats(raise_on_device_error=True)
+    for a, b in zip(got["plain"], got["regroup"]):
+        assert np.array_equal(_bits(a), _bits(b))
