@@ -21,6 +21,8 @@ Other workloads:
   loom_pt, loom_pt2
            Loom's own path tracers (pt_const, pt2_const) at the 40x40
            configurations of its published CPU results
+  loom_pt_512, loom_pt2_512
+           the same programs at 512x512 pixels (262,144 threads)
   serve    the serving loop: Poisson arrivals of a request mix (60 % render
            requests as in `batch`, 20 % Collatz batches of 2^16-2^22 inputs,
            20 % Fibonacci batches of 2^16-2^20 inputs) at 25/50/75/100 % of
@@ -28,7 +30,7 @@ Other workloads:
            continuous-batching servers beside a plain-engine FIFO queue.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pt|pt_small|batch|collatz|fib|loom_pt|loom_pt2|serve]
+                    [--workload pt|pt_small|batch|collatz|fib|loom_pt|loom_pt2|loom_pt_512|loom_pt2_512|serve]
 
 Under torchrun each rank runs the full workload on its own GPU (weak
 scaling, no data-path collective: Loom threads are independent), times with
@@ -65,6 +67,8 @@ FALLBACK = {
     "fib_u64": dict(burst=64, utr_lanes=16, block_size=512, period=1024, prefetch=False),
     "pt_const_40": dict(cost_model=True, utr_lanes=4, burst=32, block_size=128),
     "pt2_const_40": dict(cost_model=True, utr_lanes=4, burst=32, block_size=128),
+    "pt_const_512": dict(cost_model=True, utr_lanes=4, burst=32, block_size=256),
+    "pt2_const_512": dict(cost_model=True, utr_lanes=4, burst=32, block_size=256),
 }
 
 
@@ -269,15 +273,15 @@ class LoomPathTracer(Workload):
 
     dtype = "f32"
 
-    def __init__(self, kernel, threshold):
+    def __init__(self, kernel, threshold, side=40):
         self.kernel = kernel
         self.tune_key = "default"
-        x, y = np.meshgrid(np.arange(40, dtype=np.uint32), np.arange(40, dtype=np.uint32))
+        x, y = np.meshgrid(np.arange(side, dtype=np.uint32), np.arange(side, dtype=np.uint32))
         self.pixels = ((x << 16) | y).reshape(-1)
         self.n = len(self.pixels)
         self.desc = (
-            f"Loom's {kernel.rsplit('_', 1)[0]} (src/smallpt/vm/pt.hpp), 40x40 pixels, up to 64 adaptive samples, "
-            f"blur 1, threshold {threshold}, depth 2: one thread per pixel, {self.n} threads per step"
+            f"Loom's {kernel.rsplit('_', 1)[0]} (src/smallpt/vm/pt.hpp), {side}x{side} pixels, up to 64 adaptive "
+            f"samples, blur 1, threshold {threshold}, depth 2: one thread per pixel, {self.n} threads per step"
         )
         self.in_bytes = 4
         self.out_bytes = 20
@@ -315,6 +319,10 @@ def make_workload(name):
         return LoomPathTracer("pt_const_40", "1e-4")
     if name == "loom_pt2":
         return LoomPathTracer("pt2_const_40", "1e-3")
+    if name == "loom_pt_512":
+        return LoomPathTracer("pt_const_512", "1e-4", 512)
+    if name == "loom_pt2_512":
+        return LoomPathTracer("pt2_const_512", "1e-3", 512)
     if name == "pt":
         return PathTracing()
     if name == "pt_small":  # the profiling case: same scene at 256x192
@@ -477,7 +485,7 @@ def cpu_reference(w, check_tids=None, target_s: float = 2.0):
 # Float outputs that pass through the host libm's sinf/cosf (Loom's
 # pt2_const) are held within this many ulp of the reference; everything else
 # is compared bit for bit.
-ULP_TOLERANCE = {"pt2_const_40": 4}
+ULP_TOLERANCE = {"pt2_const_40": 4, "pt2_const_512": 4}
 
 
 def same_bits(got, want, kernel: str = "") -> bool:
@@ -893,6 +901,9 @@ def tune_main(args) -> None:
         dict(T.DEFAULT, **regroup_opts(w.kernel, w.tune_key)),
         dict(T.DEFAULT, cost_model=True, utr_lanes=4, burst=32),
         dict(T.DEFAULT),
+        # no parking: every live lane runs every burst (latency-bound runs
+        # of few long threads)
+        dict(T.DEFAULT, utr_lanes=1, spread_lanes=1, burst=64, period=1 << 20),
     ]
     res = T.tune(make_launch, w.n, seed=seed, space=space, budget_s=args.tune_budget,
                  log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate)
@@ -910,7 +921,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "serve"])
+    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")

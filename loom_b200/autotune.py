@@ -34,7 +34,7 @@ SPACE: Dict[str, List] = {
     "burst": [1, 2, 4, 8, 16, 32, 64],
     "utr_lanes": [1, 4, 8, 12, 16, 20, 24],
     "spread_lanes": [1, 8, 16, 24, 33],
-    "period": [256, 1024, 4096, 16384, 65536],
+    "period": [256, 1024, 4096, 16384, 65536, 1 << 20],
     "block_size": [128, 256, 512],
     "population": [1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23],
     "ctas_per_sm": [0, 1, 2, 4],

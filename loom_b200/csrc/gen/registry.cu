@@ -32,7 +32,9 @@ extern const loom_b200::KernelEntry loom_b200_entry_lshift_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f64;
 extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_40;
+extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_512;
 extern const loom_b200::KernelEntry loom_b200_entry_pt_const_40;
+extern const loom_b200::KernelEntry loom_b200_entry_pt_const_512;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u16;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u64;
@@ -80,7 +82,9 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_minmax_f32,
     &loom_b200_entry_minmax_f64,
     &loom_b200_entry_pt2_const_40,
+    &loom_b200_entry_pt2_const_512,
     &loom_b200_entry_pt_const_40,
+    &loom_b200_entry_pt_const_512,
     &loom_b200_entry_rshift_u16,
     &loom_b200_entry_rshift_u32,
     &loom_b200_entry_rshift_u64,
@@ -96,5 +100,5 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 45;
+const int kRegistrySize = 47;
 } // namespace loom_b200

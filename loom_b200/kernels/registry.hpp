@@ -45,6 +45,9 @@ using std::uint8_t;
     /* samples, blur 1, depth 2, threshold 1e-4 (v1) and 1e-3 (v2)       */    \
     X(pt_const_40,        loom::vm::pt_const<float, loom::vm::constants<CS(40), CS(0.0001), CS(64), CS(1), CS(2)>>) \
     X(pt2_const_40,       loom::vm::pt2_const<float, loom::vm::constants<CS(40), CS(0.001), CS(64), CS(1), CS(2)>>) \
+    /* the same programs at 512x512 pixels, enough threads to fill a GPU */    \
+    X(pt_const_512,       loom::vm::pt_const<float, loom::vm::constants<CS(512), CS(0.0001), CS(64), CS(1), CS(2)>>) \
+    X(pt2_const_512,      loom::vm::pt2_const<float, loom::vm::constants<CS(512), CS(0.001), CS(64), CS(1), CS(2)>>) \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

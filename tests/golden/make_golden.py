@@ -84,7 +84,10 @@ def make(name: str) -> pathlib.Path:
     if name.startswith("sphere_pt"):
         return make_pt(name)
     if name.startswith(("pt_const", "pt2_const")):
-        ins = [loom_pt_pixels()]
+        side = int(name.rsplit("_", 1)[1])
+        ins = [loom_pt_pixels(side, side)]
+        if len(ins[0]) > 4096:  # a seeded subset of the larger renders
+            ins = D.inputs_for(name, 4096, SEED, ["u32"])
         outs = O.ref_run(name, ins, len(ins[0]), threads=8)
         arrays = {"in0": ins[0]}
         arrays.update({f"out{j}": a for j, a in enumerate(outs)})

@@ -58,9 +58,11 @@ def inputs_for(name: str, n: int, seed: int, input_types: List[str]) -> List[np.
         elif name.startswith(("jmp4", "sct_inv", "slt_inv")):
             a = _ints(s, n, 0, 3, dt)
         elif name.startswith(("pt_const", "pt2_const")):
-            # pixels of the 40x40 render, encoded x << 16 | y as Loom's demo does
-            xy = _ints(s, n, 0, 40 * 40 - 1, np.uint32)
-            a = (((xy % 40) << 16) | (xy // 40)).astype(dt)
+            # pixels of the square render (side in the name), encoded
+            # x << 16 | y as Loom's demo does
+            side = int(name.rsplit("_", 1)[1])
+            xy = _ints(s, n, 0, side * side - 1, np.uint32)
+            a = (((xy % side) << 16) | (xy // side)).astype(dt)
         elif name.startswith(("lshift", "rshift")):
             a = _ints(s, n, 2, 10, dt)
         elif name.startswith("bool"):

@@ -34,7 +34,7 @@ def _as_list(x):
 # on every bounce.  There every float output is held within ULP_TOLERANCE
 # units in the last place of the scalar backend's value, and integer outputs
 # (ray counts, pixel ids) stay exact.
-ULP_TOLERANCE = {"pt2_const_40": 4}
+ULP_TOLERANCE = {"pt2_const_40": 4, "pt2_const_512": 4}
 
 
 def _check(name, got, want):
