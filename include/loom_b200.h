@@ -116,7 +116,12 @@ typedef struct loom_b200_opts
     uint32_t cost_model;  /* regroup: per-block quorum from a cost model (a
                              long block runs only with enough lanes, else its
                              lanes park and come back as full warps) */
-    uint32_t pad1;
+    uint32_t schedule;    /* regroup: 0 runs the largest same-block group
+                             (Loom's majority rule); 1 runs the group at the
+                             block earliest in program order, so lagging lanes
+                             catch up and merge; 2 steps one block at a time
+                             in that order without votes or parking (a
+                             reconvergence stack in software, plus refill) */
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

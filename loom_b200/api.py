@@ -112,7 +112,7 @@ class Opts(ctypes.Structure):
         ("fault_phantom_ctas", ctypes.c_uint32),
         ("barrier_spins", ctypes.c_uint64),
         ("cost_model", ctypes.c_uint32),
-        ("pad1", ctypes.c_uint32),
+        ("schedule", ctypes.c_uint32),
     ]
 
 
@@ -380,6 +380,7 @@ def make_opts(
     barrier_spins: int = 0,
     graph: bool = False,
     cost_model: bool = False,
+    schedule: int = 0,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -400,6 +401,7 @@ def make_opts(
         fault_phantom_ctas=fault_phantom_ctas,
         barrier_spins=barrier_spins,
         cost_model=1 if cost_model else 0,
+        schedule=int(schedule),
     )
 
 

@@ -40,9 +40,10 @@ SPACE: Dict[str, List] = {
     "ctas_per_sm": [0, 1, 2, 4],
     "prefetch": [True, False],
     "cost_model": [False, True],
+    "schedule": [0, 1, 2],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:

@@ -321,6 +321,7 @@ def generate(k: Kernel) -> str:
         quorum.append(min(28, max(0, math.ceil(32 * (ib - cols) / (ib + cols)))) if ib > cols else 0)
     heavy = {b for b in range(nb) if quorum[b] > 0}
     w(f"__constant__ unsigned kQuorumTab[{nb}] = {{{', '.join(map(str, quorum))}}};")
+    w(f"__constant__ unsigned kRankTab[{nb}] = {{{', '.join(map(str, k.rpo_ranks()))}}};")
     w("")
     w("struct K")
     w("{")
@@ -388,6 +389,7 @@ def generate(k: Kernel) -> str:
     w("    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }")
     w("    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }")
     w("    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }")
+    w("    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }")
     w("")
     per_block = [[qi for qi, (b, _) in enumerate(queues) if b == blk] for blk in range(nb)]
     maxq = max(len(x) for x in per_block)

@@ -359,6 +359,30 @@ class Kernel:
             live[index[(d, None)]] = u | {v}
         return live
 
+    def rpo_ranks(self) -> List[int]:
+        """Rank of every block in reverse post-order of a depth-first walk
+        from START (loop headers before their bodies, a join after both of
+        its branches); unreachable blocks come last."""
+        seen = [False] * self.num_blocks
+        post: List[int] = []
+        stack = [(0, iter(self.blocks[0].successors()))] if self.blocks else []
+        if self.blocks:
+            seen[0] = True
+        while stack:
+            b, it = stack[-1]
+            nxt = next((t for t in it if t != HALT and not seen[t]), None)
+            if nxt is None:
+                post.append(b)
+                stack.pop()
+            else:
+                seen[nxt] = True
+                stack.append((nxt, iter(self.blocks[nxt].successors())))
+        order = list(reversed(post)) + [b for b in range(self.num_blocks) if not seen[b]]
+        rank = [0] * self.num_blocks
+        for r, b in enumerate(order):
+            rank[b] = r
+        return rank
+
     def state_regs(self) -> List[int]:
         """Registers that are live at the entry of some block: the columns of
         the regrouping engine's state file."""

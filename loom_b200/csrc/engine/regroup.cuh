@@ -84,6 +84,12 @@ struct RegroupParams
     // Cost model: a block's quorum is the larger of utr and K::quorum(b),
     // and blocks with a quorum are entered only at the start of a burst.
     unsigned            cost_model;
+    // Warp schedule: 0 runs the largest group that meets its quorum; 1 runs
+    // the group at the block earliest in reverse post-order, so lanes that
+    // lag catch up with the others and merge at join blocks and loop heads;
+    // 2 steps one block at a time in that order with no vote and no quorum
+    // (lanes park only when the period ends).
+    unsigned            schedule;
 };
 
 __device__ __forceinline__ unsigned
@@ -179,6 +185,10 @@ regroup_kernel(const RegroupParams p)
     __shared__ unsigned long long s_blk[2 * (kProf ? K::kNumBlocks : 1)];
     Ctx ctx{0ull, 0ull, p.status, &p.cols, kProf ? s_blk : nullptr};
     if constexpr(kProf) block_counters_clear(s_blk, K::kNumBlocks);
+    // block ranks in reverse post-order, for the schedules that order groups
+    __shared__ unsigned s_rank[K::kNumBlocks];
+    for(int i = threadIdx.x; i < K::kNumBlocks; i += blockDim.x) s_rank[i] = K::rank(i);
+    __syncthreads();
     unsigned long long parks = 0, sbytes = 0, finished = 0;
     typename K::Regs   R;
     typename K::In     pf;
@@ -258,7 +268,21 @@ regroup_kernel(const RegroupParams p)
                         if(t != ~0ull) { pf_tid = t; K::load_in(pf, p.cols, t); }
                     }
                 }
-                if(pc >= 0 && (mc >= p.spread || pc == m))
+                if(p.schedule == 2u)
+                {
+                    // one block at a time, always the block earliest in
+                    // reverse post-order among the warp's lanes: lanes that
+                    // lag run until they reach the others (MinPC stepping,
+                    // the order a reconvergence stack keeps)
+                    for(unsigned i = 0; i < p.burst; ++i)
+                    {
+                        const unsigned rk = pc >= 0 ? s_rank[pc] : 0xffffffffu;
+                        const unsigned lo = __reduce_min_sync(FULL, rk);
+                        if(lo == 0xffffffffu) break;
+                        if(rk == lo) pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false);
+                    }
+                }
+                else if(pc >= 0 && (mc >= p.spread || pc == m))
                     pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
                 steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
@@ -290,16 +314,26 @@ regroup_kernel(const RegroupParams p)
                     }
                 }
                 if(steps >= p.period) break;
+                if(p.schedule == 2u)
+                {
+                    // no quorum: the warp keeps its lanes until the period
+                    // ends or none is left
+                    if(__ballot_sync(FULL, pc >= 0) == 0u) break;
+                    continue;
+                }
                 const unsigned cm = __popc(__ballot_sync(FULL, pc == m));
-                if(cm >= need(m)) { mc = cm; continue; }
-                // the largest group that meets its block's quorum, if any
+                if(!p.schedule && cm >= need(m)) { mc = cm; continue; }
+                // the group to run next among those that meet their block's
+                // quorum: the largest, or the one earliest in program order
                 const unsigned peers = __match_any_sync(FULL, pc);
                 const unsigned gs    = static_cast<unsigned>(__popc(peers));
-                const unsigned key   = pc >= 0 && gs >= need(pc) ? ((gs << 16) | static_cast<unsigned>(pc)) : 0u;
+                const bool     elig  = pc >= 0 && gs >= need(pc);
+                const unsigned prio  = p.schedule ? 0xffffu - K::rank(pc) : gs;
+                const unsigned key   = elig ? ((prio << 16) | static_cast<unsigned>(pc)) : 0u;
                 const unsigned best  = __reduce_max_sync(FULL, key);
                 if(best == 0u) break;
                 m  = static_cast<int>(best & 0xffffu);
-                mc = best >> 16;
+                mc = p.schedule ? static_cast<unsigned>(__popc(__ballot_sync(FULL, pc == m))) : best >> 16;
             }
             for(int pass = 0; pass < 2; ++pass)
             {

@@ -10,6 +10,7 @@ __constant__ unsigned kInstrTab[2] = {3, 8};
 __constant__ unsigned kLiveTab[2] = {8, 12};
 __constant__ int kQueueBlock[2] = {0, 1};
 __constant__ unsigned kQuorumTab[2] = {7, 15};
+__constant__ unsigned kRankTab[2] = {0, 1};
 
 struct K
 {
@@ -66,6 +67,7 @@ struct K
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
+    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).

@@ -10,6 +10,7 @@ __constant__ unsigned kInstrTab[3] = {3, 4, 6};
 __constant__ unsigned kLiveTab[3] = {8, 8, 32};
 __constant__ int kQueueBlock[3] = {0, 1, 2};
 __constant__ unsigned kQuorumTab[3] = {7, 11, 3};
+__constant__ unsigned kRankTab[3] = {0, 1, 2};
 
 struct K
 {
@@ -66,6 +67,7 @@ struct K
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
+    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).

@@ -10,6 +10,7 @@ __constant__ unsigned kInstrTab[24] = {32, 63, 5, 38, 2, 28, 4, 3, 2, 2, 4, 4, 1
 __constant__ unsigned kLiveTab[28] = {8, 68, 76, 92, 84, 84, 36, 104, 104, 104, 108, 108, 104, 92, 76, 100, 108, 112, 108, 108, 120, 96, 80, 220, 60, 104, 100, 116};
 __constant__ int kQueueBlock[28] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23, 23, 23, 23, 23};
 __constant__ unsigned kQuorumTab[24] = {27, 18, 0, 8, 0, 4, 0, 0, 0, 0, 0, 0, 0, 0, 5, 0, 0, 0, 0, 6, 0, 0, 0, 22};
+__constant__ unsigned kRankTab[24] = {0, 9, 10, 11, 12, 13, 14, 15, 16, 17, 7, 8, 18, 21, 22, 23, 5, 6, 19, 20, 2, 3, 4, 1};
 
 struct K
 {
@@ -198,6 +199,7 @@ struct K
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
+    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 5;
     // j-th queue holding threads that stand at block b (-1: none).

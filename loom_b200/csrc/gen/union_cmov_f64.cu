@@ -10,6 +10,7 @@ __constant__ unsigned kInstrTab[1] = {2};
 __constant__ unsigned kLiveTab[1] = {8};
 __constant__ int kQueueBlock[1] = {0};
 __constant__ unsigned kQuorumTab[1] = {0};
+__constant__ unsigned kRankTab[1] = {0};
 
 struct K
 {
@@ -62,6 +63,7 @@ struct K
     __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
+    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).

@@ -390,6 +390,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         L.params.refill        = o.no_refill ? 0u : 1u;
         L.params.prefetch      = o.no_prefetch ? 0u : 1u;
         L.params.cost_model    = o.cost_model;
+        L.params.schedule      = o.schedule;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
         L.profile              = o.profile != 0;

@@ -569,6 +569,7 @@ run_slice(loom_b200_server* s)
     L.params.refill        = o.no_refill ? 0u : 1u;
     L.params.prefetch      = o.no_prefetch ? 0u : 1u;
     L.params.cost_model    = o.cost_model;
+    L.params.schedule      = o.schedule;
     L.params.round0        = static_cast<unsigned>(s->next_round);
     L.params.slice_rounds  = s->cfg.slice_rounds;
     L.params.inst_done     = s->d_done;

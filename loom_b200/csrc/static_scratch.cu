@@ -232,6 +232,7 @@ loom_b200_launch_static(const char*             kernel,
     R.params.refill        = o.no_refill ? 0u : 1u;
     R.params.prefetch      = o.no_prefetch ? 0u : 1u;
     R.params.cost_model    = o.cost_model;
+    R.params.schedule      = o.schedule;
     R.grid                 = static_cast<unsigned>(ctas * slot.sms);
     R.block                = block;
     R.profile              = false;

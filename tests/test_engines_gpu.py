@@ -107,6 +107,11 @@ REGROUP_VARIANTS = [
     dict(cost_model=True),
     dict(cost_model=True, burst=16, utr_lanes=24, population=512),
     dict(cost_model=True, burst=1, utr_lanes=1, period=2),
+    dict(schedule=1),
+    dict(schedule=1, utr_lanes=1, spread_lanes=1, burst=64),
+    dict(schedule=1, cost_model=True, burst=8, population=300),
+    dict(schedule=2, burst=16),
+    dict(schedule=2, burst=3, period=7, population=100),
 ]
 
 
