@@ -432,18 +432,26 @@ def generate(k: Kernel) -> str:
     w("    }")
     w("")
     # ---- run_burst (goto CFG entered at any block, bounded by a budget)
+    # the budget is counted at loop headers only (targets of edges that go
+    # back in reverse post-order): every cycle passes one, and the blocks in
+    # between have no early exit, so a diverged warp reconverges at their
+    # post-dominators as in straight CUDA
+    rank = k.rpo_ranks()
+    headers = {t for b in k.blocks for t in b.successors() if t != HALT and rank[t] <= rank[b.idx]}
     w("    // Runs the lane's own path from block `entry` for at most `budget`")
-    w("    // blocks; returns the block it stopped at, or kHalt.  With")
-    w("    // `stop_heavy`, a block whose quorum is above zero is entered only as")
-    w("    // the first block of the burst, when the warp's vote chose it.")
-    w("    template <bool kProf>")
+    w("    // loop iterations (visits of a loop header); returns the block it")
+    w("    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is")
+    w("    // above zero is entered only as the first block of the burst, when")
+    w("    // the warp's vote chose it.")
+    w("    // kStopHeavy is a template parameter so that the form without the")
+    w("    // stops has no early exits at all between loop headers.")
+    w("    template <bool kProf, bool kStopHeavy = false>")
     w("    __device__ __forceinline__ static int")
-    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)")
     w("    {")
     w("        (void)ctx;")
-    w("        (void)stop_heavy;")
-    w("        const unsigned first = budget;")
-    w("        (void)first;")
+    w("        bool fresh = true; // no block run yet in this burst")
+    w("        (void)fresh;")
     w("        switch(entry)")
     w("        {")
     for blk in k.blocks:
@@ -456,12 +464,15 @@ def generate(k: Kernel) -> str:
         if blk.idx in heavy:
             # a lane that loops on the block keeps going; one that comes
             # from another block waits for the warp's vote
-            w(f"        if(stop_heavy && budget != first) return {blk.idx};")
+            w(f"        if constexpr(kStopHeavy) {{ if(!fresh) return {blk.idx}; }}")
             w(f"    L_B{blk.idx}_again:")
             own = f"goto L_B{blk.idx};"
             transfer = [t.replace(own, f"goto L_B{blk.idx}_again;") for t in transfer]
-        w(f"        if(budget == 0u) return {blk.idx};")
-        w("        --budget;")
+        if blk.idx in headers:
+            w(f"        if(budget == 0u) return {blk.idx};")
+            w("        --budget;")
+        if heavy:
+            w("        if constexpr(kStopHeavy) fresh = false;")
         w(f"        if constexpr(kProf) count_block(ctx, {blk.idx}, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
         o.extend(transfer)

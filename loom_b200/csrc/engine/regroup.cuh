@@ -279,11 +279,12 @@ regroup_kernel(const RegroupParams p)
                         const unsigned rk = pc >= 0 ? s_rank[pc] : 0xffffffffu;
                         const unsigned lo = __reduce_min_sync(FULL, rk);
                         if(lo == 0xffffffffu) break;
-                        if(rk == lo) pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false);
+                        if(rk == lo) pc = K::template run_burst<kProf>(pc, R, ctx, 1u);
                     }
                 }
                 else if(pc >= 0 && (mc >= p.spread || pc == m))
-                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
+                    pc = cost_on ? K::template run_burst<kProf, true>(pc, R, ctx, p.burst)
+                                 : K::template run_burst<kProf, false>(pc, R, ctx, p.burst);
                 steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)

@@ -82,25 +82,25 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.  With
-    // `stop_heavy`, a block whose quorum is above zero is entered only as
-    // the first block of the burst, when the warp's vote chose it.
-    template <bool kProf>
+    // loop iterations (visits of a loop header); returns the block it
+    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
+    // above zero is entered only as the first block of the burst, when
+    // the warp's vote chose it.
+    // kStopHeavy is a template parameter so that the form without the
+    // stops has no early exits at all between loop headers.
+    template <bool kProf, bool kStopHeavy = false>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop_heavy;
-        const unsigned first = budget;
-        (void)first;
+        bool fresh = true; // no block run yet in this burst
+        (void)fresh;
         switch(entry)
         {
         case 0: goto L_B0;
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u) return 0;
-        --budget;
         if constexpr(kProf) count_block(ctx, 0, 1u);
         R.r0 = static_cast<int>(static_cast<int>(static_cast<int>(R.r0) + static_cast<int>(((int)0x1ull))));
         goto L_HALT;

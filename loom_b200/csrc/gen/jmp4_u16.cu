@@ -82,17 +82,19 @@ struct K
     }
 
     // Runs the lane's own path from block `entry` for at most `budget`
-    // blocks; returns the block it stopped at, or kHalt.  With
-    // `stop_heavy`, a block whose quorum is above zero is entered only as
-    // the first block of the burst, when the warp's vote chose it.
-    template <bool kProf>
+    // loop iterations (visits of a loop header); returns the block it
+    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
+    // above zero is entered only as the first block of the burst, when
+    // the warp's vote chose it.
+    // kStopHeavy is a template parameter so that the form without the
+    // stops has no early exits at all between loop headers.
+    template <bool kProf, bool kStopHeavy = false>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
     {
         (void)ctx;
-        (void)stop_heavy;
-        const unsigned first = budget;
-        (void)first;
+        bool fresh = true; // no block run yet in this burst
+        (void)fresh;
         switch(entry)
         {
         case 0: goto L_B0;
@@ -103,8 +105,7 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if(budget == 0u) return 0;
-        --budget;
+        if constexpr(kStopHeavy) fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 1u);
         switch(R.r1) {
         case 0: goto L_B1;
@@ -114,34 +115,30 @@ struct K
         default: goto L_HALT;
         }
     L_B1: // l0
-        if(stop_heavy && budget != first) return 1;
+        if constexpr(kStopHeavy) { if(!fresh) return 1; }
     L_B1_again:
-        if(budget == 0u) return 1;
-        --budget;
+        if constexpr(kStopHeavy) fresh = false;
         if constexpr(kProf) count_block(ctx, 1, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x1ull));
         goto L_HALT;
     L_B2: // l1
-        if(stop_heavy && budget != first) return 2;
+        if constexpr(kStopHeavy) { if(!fresh) return 2; }
     L_B2_again:
-        if(budget == 0u) return 2;
-        --budget;
+        if constexpr(kStopHeavy) fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x3ull));
         goto L_HALT;
     L_B3: // l2
-        if(stop_heavy && budget != first) return 3;
+        if constexpr(kStopHeavy) { if(!fresh) return 3; }
     L_B3_again:
-        if(budget == 0u) return 3;
-        --budget;
+        if constexpr(kStopHeavy) fresh = false;
         if constexpr(kProf) count_block(ctx, 3, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0x7ull));
         goto L_HALT;
     L_B4: // l3
-        if(stop_heavy && budget != first) return 4;
+        if constexpr(kStopHeavy) { if(!fresh) return 4; }
     L_B4_again:
-        if(budget == 0u) return 4;
-        --budget;
+        if constexpr(kStopHeavy) fresh = false;
         if constexpr(kProf) count_block(ctx, 4, 2u);
         R.r1 = static_cast<unsigned short>(((unsigned short)0xbull));
         goto L_HALT;
