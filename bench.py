@@ -15,7 +15,7 @@ pinned host memory inside the timed region.
 
 Other workloads:
   batch    256 render requests of uneven size, each with its own random
-           scene, in one launch (about 473 M threads)
+           scene, in one launch (392.8 M threads)
   collatz  2^24 threads, n ~ U[1, 2^32)
   fib      2^20 threads, n ~ U{0..93}
   loom_pt, loom_pt2

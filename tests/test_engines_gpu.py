@@ -285,3 +285,19 @@ def test_loom_pt2_engines_agree_bit_for_bit(golden):
             f.stats(raise_on_device_error=True)
     for a, b in zip(got["plain"], got["regroup"]):
         assert np.array_equal(_bits(a), _bits(b))
+
+
+def test_headless_render_writes_a_png(tmp_path):
+    """The render command traces a small Cornell image on the device and
+    writes it as a PNG; both engines give the same pixels."""
+    from loom_b200 import render as Rd
+    from loom_b200 import scenes as S
+
+    req = S.cornell_request(32, 24, 4, seed=3)
+    a = Rd.render(req, "regroup")
+    b = Rd.render(req, "plain")
+    assert a.shape == (32 * 24, 3) and np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert float(a.mean()) > 0.0
+    out = tmp_path / "c.png"
+    Rd.main(["--out", str(out), "--width", "32", "--height", "24", "--spp", "4"])
+    assert out.read_bytes()[:8] == b"\x89PNG\r\n\x1a\n"
