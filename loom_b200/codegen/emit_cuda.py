@@ -443,13 +443,12 @@ def generate(k: Kernel) -> str:
     w("    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is")
     w("    // above zero is entered only as the first block of the burst, when")
     w("    // the warp's vote chose it.")
-    w("    // kStopHeavy is a template parameter so that the form without the")
-    w("    // stops has no early exits at all between loop headers.")
-    w("    template <bool kProf, bool kStopHeavy = false>")
+    w("    template <bool kProf>")
     w("    __device__ __forceinline__ static int")
-    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)")
     w("    {")
     w("        (void)ctx;")
+    w("        (void)stop_heavy;")
     w("        bool fresh = true; // no block run yet in this burst")
     w("        (void)fresh;")
     w("        switch(entry)")
@@ -464,7 +463,7 @@ def generate(k: Kernel) -> str:
         if blk.idx in heavy:
             # a lane that loops on the block keeps going; one that comes
             # from another block waits for the warp's vote
-            w(f"        if constexpr(kStopHeavy) {{ if(!fresh) return {blk.idx}; }}")
+            w(f"        if(stop_heavy && !fresh) return {blk.idx};")
             w(f"    L_B{blk.idx}_again:")
             own = f"goto L_B{blk.idx};"
             transfer = [t.replace(own, f"goto L_B{blk.idx}_again;") for t in transfer]
@@ -472,7 +471,7 @@ def generate(k: Kernel) -> str:
             w(f"        if(budget == 0u) return {blk.idx};")
             w("        --budget;")
         if heavy:
-            w("        if constexpr(kStopHeavy) fresh = false;")
+            w("        fresh = false;")
         w(f"        if constexpr(kProf) count_block(ctx, {blk.idx}, {len(blk.instrs)}u);")
         o.extend(L.body(blk.instrs, "        "))
         o.extend(transfer)

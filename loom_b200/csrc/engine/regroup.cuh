@@ -283,8 +283,7 @@ regroup_kernel(const RegroupParams p)
                     }
                 }
                 else if(pc >= 0 && (mc >= p.spread || pc == m))
-                    pc = cost_on ? K::template run_burst<kProf, true>(pc, R, ctx, p.burst)
-                                 : K::template run_burst<kProf, false>(pc, R, ctx, p.burst);
+                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
                 steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)

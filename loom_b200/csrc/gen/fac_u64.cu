@@ -88,13 +88,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -105,24 +104,24 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if constexpr(kStopHeavy) { if(!fresh) return 0; }
+        if(stop_heavy && !fresh) return 0;
     L_B0_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r1) <= static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r1 = static_cast<unsigned long long>(((R.r2) ? (((unsigned long long)0x1ull)) : (R.r1)));
         if(R.r2) goto L_HALT; else goto L_B1;
     L_B1: // cinit
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 1, 2u);
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         goto L_B2;
     L_B2: // loop
-        if constexpr(kStopHeavy) { if(!fresh) return 2; }
+        if(stop_heavy && !fresh) return 2;
     L_B2_again:
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 4u);
         R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r3) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));

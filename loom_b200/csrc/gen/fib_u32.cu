@@ -91,13 +91,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -108,28 +107,28 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if constexpr(kStopHeavy) { if(!fresh) return 0; }
+        if(stop_heavy && !fresh) return 0;
     L_B0_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r3 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r1) <= static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r2 = static_cast<unsigned int>(((R.r3) ? (R.r1) : (((unsigned int)0x1ull))));
         if(R.r3) goto L_HALT; else goto L_B1;
     L_B1: // work
-        if constexpr(kStopHeavy) { if(!fresh) return 1; }
+        if(stop_heavy && !fresh) return 1;
     L_B1_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 1, 4u);
         R.r4 = static_cast<unsigned int>(((unsigned int)0x0ull));
         R.r2 = static_cast<unsigned int>(((unsigned int)0x1ull));
         R.r5 = static_cast<unsigned int>(((unsigned int)0x2ull));
         goto L_B2;
     L_B2: // loop
-        if constexpr(kStopHeavy) { if(!fresh) return 2; }
+        if(stop_heavy && !fresh) return 2;
     L_B2_again:
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 6u);
         R.r6 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r4) + static_cast<unsigned int>(R.r2)));
         R.r4 = static_cast<unsigned int>(R.r2);

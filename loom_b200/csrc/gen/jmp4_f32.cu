@@ -86,13 +86,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -105,7 +104,7 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 1u);
         switch(R.r1) {
         case 0: goto L_B1;
@@ -115,30 +114,30 @@ struct K
         default: goto L_HALT;
         }
     L_B1: // l0
-        if constexpr(kStopHeavy) { if(!fresh) return 1; }
+        if(stop_heavy && !fresh) return 1;
     L_B1_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 1, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x1ull));
         goto L_HALT;
     L_B2: // l1
-        if constexpr(kStopHeavy) { if(!fresh) return 2; }
+        if(stop_heavy && !fresh) return 2;
     L_B2_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x3ull));
         goto L_HALT;
     L_B3: // l2
-        if constexpr(kStopHeavy) { if(!fresh) return 3; }
+        if(stop_heavy && !fresh) return 3;
     L_B3_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 3, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0x7ull));
         goto L_HALT;
     L_B4: // l3
-        if constexpr(kStopHeavy) { if(!fresh) return 4; }
+        if(stop_heavy && !fresh) return 4;
     L_B4_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 4, 2u);
         R.r1 = static_cast<unsigned int>(((unsigned int)0xbull));
         goto L_HALT;

@@ -93,13 +93,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)

@@ -87,13 +87,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -102,9 +101,9 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if constexpr(kStopHeavy) { if(!fresh) return 0; }
+        if(stop_heavy && !fresh) return 0;
     L_B0_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 3u);
         R.r1 = static_cast<unsigned int>(static_cast<unsigned int>(((R.r0) == 0 ? ((unsigned int)0x0ull) : ((R.r0) == 1 ? ((unsigned int)0xaull) : ((R.r0) == 2 ? ((unsigned int)0x14ull) : ((unsigned int)0x1eull))))));
         R.r0 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r0) * static_cast<unsigned int>(((unsigned int)0xaull))));

@@ -246,13 +246,12 @@ struct K
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
     // the warp's vote chose it.
-    // kStopHeavy is a template parameter so that the form without the
-    // stops has no early exits at all between loop headers.
-    template <bool kProf, bool kStopHeavy = false>
+    template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
     {
         (void)ctx;
+        (void)stop_heavy;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -284,9 +283,9 @@ struct K
         default: return kHalt;
         }
     L_B0: // START
-        if constexpr(kStopHeavy) { if(!fresh) return 0; }
+        if(stop_heavy && !fresh) return 0;
     L_B0_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 0, 32u);
         R.r6 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r1) * static_cast<unsigned int>(((unsigned int)0x10ull))));
         R.r7 = static_cast<unsigned int>(table_load<unsigned int>(*ctx.cols, static_cast<unsigned>(R.r6)));
@@ -321,9 +320,9 @@ struct K
         R.r26 = static_cast<unsigned int>(((unsigned int)0x0ull));
         goto L_B23;
     L_B1: // prim
-        if constexpr(kStopHeavy) { if(!fresh) return 1; }
+        if(stop_heavy && !fresh) return 1;
     L_B1_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 1, 63u);
         R.r27 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r20) & static_cast<unsigned int>(((unsigned int)0x3ull))));
         R.r28 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r27) & static_cast<unsigned int>(((unsigned int)0x1ull))));
@@ -391,7 +390,7 @@ struct K
     L_B2: // bounce
         if(budget == 0u) return 2;
         --budget;
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 5u);
         R.r53 = static_cast<float>((0x1.93e5960000000p+99f));
         R.r54 = static_cast<unsigned int>(R.r13);
@@ -399,11 +398,11 @@ struct K
         R.r56 = static_cast<unsigned int>(R.r12);
         goto L_B3;
     L_B3: // isect
-        if constexpr(kStopHeavy) { if(!fresh) return 3; }
+        if(stop_heavy && !fresh) return 3;
     L_B3_again:
         if(budget == 0u) return 3;
         --budget;
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 3, 38u);
         R.r57 = static_cast<float>(table_load<float>(*ctx.cols, static_cast<unsigned>(R.r56)));
         R.r8 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(((unsigned int)0x1ull))));
@@ -444,14 +443,14 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r55) < static_cast<unsigned int>(R.r13)));
         if(R.r33) goto L_B3_again; else goto L_B4;
     L_B4: // shade
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 4, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r54) >= static_cast<unsigned int>(R.r13)));
         if(R.r33) goto L_HALT; else goto L_B5;
     L_B5: // hitp
-        if constexpr(kStopHeavy) { if(!fresh) return 5; }
+        if(stop_heavy && !fresh) return 5;
     L_B5_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 5, 28u);
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r54) * static_cast<unsigned int>(((unsigned int)0x8ull))));
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(R.r12)));
@@ -482,44 +481,44 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r79) == static_cast<unsigned int>(((unsigned int)0x3ull))));
         if(R.r33) goto L_B6; else goto L_B7;
     L_B6: // emit
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 6, 4u);
         R.r3 = static_cast<float>(op_fma(R.r49, R.r76, R.r3));
         R.r4 = static_cast<float>(op_fma(R.r50, R.r77, R.r4));
         R.r5 = static_cast<float>(op_fma(R.r51, R.r78, R.r5));
         goto L_HALT;
     L_B7: // surf
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 7, 3u);
         R.r52 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r52) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r52) >= static_cast<unsigned int>(((unsigned int)0x10ull))));
         if(R.r33) goto L_HALT; else goto L_B8;
     L_B8: // rrchk
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 8, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r52) >= static_cast<unsigned int>(((unsigned int)0x5ull))));
         if(R.r33) goto L_B9; else goto L_B12;
     L_B9: // rr_roll
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 9, 2u);
         R.r26 = static_cast<unsigned int>(((unsigned int)0x1ull));
         goto L_B23;
     L_B10: // rr
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 10, 4u);
         R.r86 = static_cast<float>(op_max<float>(static_cast<float>(R.r76), static_cast<float>(R.r77)));
         R.r86 = static_cast<float>(op_max<float>(static_cast<float>(R.r86), static_cast<float>(R.r78)));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r130)) < static_cast<float>(R.r86)));
         if(R.r33) goto L_B11; else goto L_HALT;
     L_B11: // rr_keep
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 11, 4u);
         R.r76 = static_cast<float>(static_cast<float>(static_cast<float>(R.r76) / static_cast<float>(R.r86)));
         R.r77 = static_cast<float>(static_cast<float>(static_cast<float>(R.r77) / static_cast<float>(R.r86)));
         R.r78 = static_cast<float>(static_cast<float>(static_cast<float>(R.r78) / static_cast<float>(R.r86)));
         goto L_B12;
     L_B12: // scatter
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 12, 18u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r76)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r77)));
@@ -545,7 +544,7 @@ struct K
         default: goto L_HALT;
         }
     L_B13: // mirror
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 13, 5u);
         R.r95 = static_cast<float>(static_cast<float>(static_cast<float>(R.r87) * static_cast<float>((-0x1.0000000000000p+1f))));
         R.r42 = static_cast<float>(op_fma(R.r95, R.r83, R.r42));
@@ -553,9 +552,9 @@ struct K
         R.r44 = static_cast<float>(op_fma(R.r95, R.r85, R.r44));
         goto L_B2;
     L_B14: // diffuse
-        if constexpr(kStopHeavy) { if(!fresh) return 14; }
+        if(stop_heavy && !fresh) return 14;
     L_B14_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 14, 26u);
         R.r96 = static_cast<float>(op_abs(static_cast<float>(R.r92)));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(R.r96) > static_cast<float>((0x1.99999a0000000p-4f))));
@@ -584,12 +583,12 @@ struct K
         R.r105 = static_cast<float>(op_fma(R.r92, R.r101, (-(R.r45))));
         goto L_B15;
     L_B15: // disk_roll
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 15, 2u);
         R.r26 = static_cast<unsigned int>(((unsigned int)0x2ull));
         goto L_B23;
     L_B16: // disk
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 16, 8u);
         R.r106 = static_cast<float>(static_cast<float>(static_cast<float>(bitcast<float>(R.r130)) * static_cast<float>((0x1.0000000000000p+1f))));
         R.r106 = static_cast<float>(static_cast<float>(static_cast<float>(R.r106) - static_cast<float>((0x1.0000000000000p+0f))));
@@ -600,7 +599,7 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(R.r108) < static_cast<float>((0x1.0000000000000p+0f))));
         if(R.r33) goto L_B17; else goto L_B15;
     L_B17: // disk_ok
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 17, 20u);
         R.r109 = static_cast<float>(static_cast<float>(static_cast<float>((0x1.0000000000000p+0f)) - static_cast<float>(R.r108)));
         R.r109 = static_cast<float>(op_sqrt(static_cast<float>(R.r109)));
@@ -623,7 +622,7 @@ struct K
         R.r44 = static_cast<float>(static_cast<float>(static_cast<float>(R.r44) * static_cast<float>(R.r45)));
         goto L_B2;
     L_B18: // glass
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 18, 13u);
         R.r110 = static_cast<float>(static_cast<float>(static_cast<float>((0x1.0000000000000p+0f)) / static_cast<float>((0x1.8000000000000p+0f))));
         R.r111 = static_cast<float>(((R.r88) ? (R.r110) : ((0x1.8000000000000p+0f))));
@@ -639,9 +638,9 @@ struct K
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(R.r113) < static_cast<float>((0x0.0p+0f))));
         if(R.r33) goto L_B13; else goto L_B19;
     L_B19: // refr
-        if constexpr(kStopHeavy) { if(!fresh) return 19; }
+        if(stop_heavy && !fresh) return 19;
     L_B19_again:
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 19, 40u);
         R.r115 = static_cast<float>(op_sqrt(static_cast<float>(R.r113)));
         R.r115 = static_cast<float>(op_fma(R.r112, R.r111, R.r115));
@@ -684,19 +683,19 @@ struct K
         R.r26 = static_cast<unsigned int>(((unsigned int)0x3ull));
         goto L_B23;
     L_B20: // fres
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 20, 2u);
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<float>(bitcast<float>(R.r130)) < static_cast<float>(R.r127)));
         if(R.r33) goto L_B21; else goto L_B22;
     L_B21: // take_refl
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 21, 4u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r128)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r128)));
         R.r51 = static_cast<float>(static_cast<float>(static_cast<float>(R.r51) * static_cast<float>(R.r128)));
         goto L_B13;
     L_B22: // take_refr
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 22, 7u);
         R.r49 = static_cast<float>(static_cast<float>(static_cast<float>(R.r49) * static_cast<float>(R.r129)));
         R.r50 = static_cast<float>(static_cast<float>(static_cast<float>(R.r50) * static_cast<float>(R.r129)));
@@ -706,11 +705,11 @@ struct K
         R.r44 = static_cast<float>(R.r119);
         goto L_B2;
     L_B23: // roll
-        if constexpr(kStopHeavy) { if(!fresh) return 23; }
+        if(stop_heavy && !fresh) return 23;
     L_B23_again:
         if(budget == 0u) return 23;
         --budget;
-        if constexpr(kStopHeavy) fresh = false;
+        fresh = false;
         if constexpr(kProf) count_block(ctx, 23, 292u);
         R.r130 = static_cast<unsigned int>(R.r24);
         R.r131 = static_cast<unsigned int>(R.r25);
