@@ -4,7 +4,8 @@ nvcc compilation for sm_100a.
 Steps
   1. extract  (only where the Loom headers are available, LOOM_REF_DIR or the
               default location): one small g++ program per registry kernel
-              prints its IR; loom_b200/ir/*.lir are rewritten where changed;
+              prints its IR; loom_b200/ir/*.lir are written for kernels that
+              have none, for all with --reextract (after a kernel changed);
   2. generate loom_b200/csrc/gen/<kernel>.cu for every .lir file;
   3. compile  every .cu with nvcc -gencode arch=compute_100a,code=sm_100a and
               link loom_b200/libloom_b200.so.
@@ -202,13 +203,17 @@ def compile_all(jobs: Optional[int] = None, verbose: bool = False) -> pathlib.Pa
     return LIB
 
 
-def build(extract_ir: bool = True, verbose: bool = False) -> pathlib.Path:
+def build(extract_ir: bool = True, verbose: bool = False, reextract: bool = False) -> pathlib.Path:
+    """Extract the IR of registry kernels that have none yet (all of them
+    with `reextract`, after a kernel's source changed), generate, compile."""
     ref = default_ref_dir() if extract_ir else None
     if ref is not None:
-        extract(ref)
+        names = None if reextract else [n for n, _ in registry_kernels() if not (IR_DIR / f"{n}.lir").exists()]
+        if names is None or names:
+            extract(ref, names)
     generate()
     return compile_all(verbose=verbose)
 
 
 if __name__ == "__main__":
-    print(build(verbose=True))
+    print(build(verbose=True, reextract="--reextract" in sys.argv))
