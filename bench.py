@@ -357,7 +357,12 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # LOOM_B200_CLOCKS_DIR keeps the raw samples; by default they go to a
+        # temporary directory and only the summary reaches the bench line
+        import tempfile
+
+        d = os.environ.get("LOOM_B200_CLOCKS_DIR") or tempfile.mkdtemp(prefix="loom_b200_clocks_")
+        self.path = pathlib.Path(d) / f"clocks_rank{index}.csv"
 
     def __enter__(self):
         try:
