@@ -1018,6 +1018,29 @@ def main() -> None:
     kern_ms = st_r["ms"]
     out_r = w.outputs_at(tids)
 
+    # the other tuned form of the same workload, when there is one: Loom's
+    # majority rule with the cost model (the highest lane efficiency)
+    alt = None
+    from loom_b200 import autotune as T
+
+    alt_opts = T.tuned(w.kernel, w.tune_key + "_majority") if w.tune_key != "default" else None
+    if alt_opts:
+        fa = api.Function(w.kernel, 0, "regroup", **dict(alt_opts, graph=True))
+        ms_a = time_steps(lambda: w.launch(fa, api, stream), args.steps, warmup, torch, dist) / args.steps
+        fa.set_opts("regroup", profile=True, **alt_opts)
+        w.launch(fa, api, stream)
+        torch.cuda.synchronize()
+        sa = fa.stats(raise_on_device_error=True)
+        alt = {
+            "options": alt_opts,
+            "value": round(world * w.n / (ms_a / 1e3) / 1e6, 3),
+            "ms_per_step": round(ms_a, 4),
+            "lane_efficiency": round(sa["lane_efficiency"], 4),
+            "speedup_vs_plain": None,
+            "same_outputs": bool(same_bits(w.outputs_at(tids), out_r)),
+        }
+        fa.close()
+
     e2e_s, e2e_ok, h2d, d2h = w.e2e(api, torch, args.steps, warmup, dist)
     e2e_s = max_over_ranks(e2e_s, dist)
 
@@ -1086,6 +1109,9 @@ def main() -> None:
                 "graph_launches": int(st_r.get("graph_launches", 0)),
             },
             "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
+            "regroup_majority_cost_model": (
+                dict(alt, speedup_vs_plain=round(plain_ms / alt["ms_per_step"], 4)) if alt else None
+            ),
             "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",
             "parity": parity,
             "roofline": {
