@@ -1074,7 +1074,7 @@ def main() -> None:
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
         t = json.loads(tf.read_text()).get(w.tune_key)
-        if t and t.get("kernel") == w.kernel:
+        if t and t.get("kernel") == w.kernel and t.get("dram_bytes_per_thread"):
             traffic = int(t["dram_bytes_per_thread"] * w.n)
 
     cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
