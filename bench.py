@@ -1071,11 +1071,28 @@ def main() -> None:
     # DRAM traffic of the dominant kernel from an ncu capture (per thread,
     # scaled to this launch), see profiles/roofline_traffic.json
     traffic = None
+    issue = None
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
         t = json.loads(tf.read_text()).get(w.tune_key)
         if t and t.get("kernel") == w.kernel and t.get("dram_bytes_per_thread"):
             traffic = int(t["dram_bytes_per_thread"] * w.n)
+        # the engine's own bound: warp instructions issued per second against
+        # one per cycle on each of the 148 x 4 SM sub-partitions, at the SM
+        # clock sampled during the timed region; SASS warp instructions per
+        # thread come from an ncu capture of the same tuned options
+        if t and t.get("kernel") == w.kernel and t.get("sass_options") == w.opts:
+            mhz = clk.summary().get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+            inst = t["sass_warp_inst_per_thread"] * w.n
+            got = inst / (kern_ms / 1e3) / 1e9
+            top = 148 * 4 * mhz / 1e3
+            issue = {
+                "achieved": round(got, 1),
+                "peak": round(top, 1),
+                "unit": "G warp instructions/s",
+                "frac": round(got / top, 4),
+                "sass_warp_inst_per_thread": t["sass_warp_inst_per_thread"],
+            }
 
     cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
     plain_regroup_same = same_bits(res["plain"]["out"], out_r)
@@ -1125,6 +1142,7 @@ def main() -> None:
                 "peak_source": peak_src,
                 "note": "algorithmic bytes = outputs + inputs + queue-state saves/restores of the regrouping megakernel; the engine is SIMT issue/latency bound, not HBM bound (profiles/)",
             },
+            "issue_roofline": issue,
             "cpu_baseline": cpu,
             "e2e": {
                 "value": round(world * w.n * args.steps / e2e_s / 1e6, 3),
