@@ -174,8 +174,11 @@ claim_inputs(const unsigned need, RegroupCtl* ctl, unsigned long long admit_end,
     return ((need >> lane) & 1u) && t < admit_end ? t : ~0ull;
 }
 
+/// The megakernel.  `__maxnreg__` holds it to the kernel's register cap
+/// (`K::kRegroupMaxRegs`) so that enough warps stay resident to hide the
+/// latency of the lanes it keeps running.
 template <typename K, bool kProf>
-__global__ void
+__global__ void __maxnreg__(K::kRegroupMaxRegs)
 regroup_kernel(const RegroupParams p)
 {
     constexpr int      B    = K::kNumQueues;

@@ -16,6 +16,7 @@ struct K
 {
     static constexpr int kNumBlocks = 3;
     static constexpr int kNumQueues = 3;
+    static constexpr int kRegroupMaxRegs = 64;
     struct Regs
     {
         unsigned int r1; // n: u32

@@ -16,6 +16,7 @@ struct K
 {
     static constexpr int kNumBlocks = 1;
     static constexpr int kNumQueues = 1;
+    static constexpr int kRegroupMaxRegs = 64;
     struct Regs
     {
         unsigned char r0; // val: u8
