@@ -23,6 +23,9 @@ Other workloads:
            configurations of its published CPU results
   loom_pt_512, loom_pt2_512
            the same programs at 512x512 pixels (262,144 threads)
+  loom_primary, loom_primary_b20
+           Loom's primary-ray tracer (primary_const) at its benchmark's
+           configuration: 256x256 pixels, 64 samples, blur 1 or 20
   serve    the serving loop: Poisson arrivals of a request mix (60 % render
            requests as in `batch`, 20 % Collatz batches of 2^16-2^22 inputs,
            20 % Fibonacci batches of 2^16-2^20 inputs) at 25/50/75/100 % of
@@ -30,7 +33,8 @@ Other workloads:
            continuous-batching servers beside a plain-engine FIFO queue.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pt|pt_small|batch|collatz|fib|loom_pt|loom_pt2|loom_pt_512|loom_pt2_512|serve]
+                    [--workload pt|pt_small|batch|collatz|fib|loom_pt|loom_pt2|loom_pt_512|loom_pt2_512|
+                                loom_primary|loom_primary_b20|serve]
 
 Under torchrun each rank runs the full workload on its own GPU (weak
 scaling, no data-path collective: Loom threads are independent), times with
@@ -71,6 +75,8 @@ FALLBACK = {
     # the fastest regrouping form measured (the plain engine is faster still)
     "pt_const_512": dict(schedule=2, burst=64, period=1 << 20, prefetch=False, utr_lanes=1),
     "pt2_const_512": dict(schedule=2, burst=64, period=1 << 20, prefetch=False, utr_lanes=1),
+    "primary_const_256": dict(schedule=2, burst=64, period=1 << 20, prefetch=False, utr_lanes=1),
+    "primary_const_b20_256": dict(schedule=2, burst=64, period=1 << 20, prefetch=False, utr_lanes=1),
 }
 
 
@@ -275,16 +281,22 @@ class LoomPathTracer(Workload):
 
     dtype = "f32"
 
-    def __init__(self, kernel, threshold, side=40):
+    def __init__(self, kernel, threshold, side=40, blur=1):
         self.kernel = kernel
         self.tune_key = "default"
         x, y = np.meshgrid(np.arange(side, dtype=np.uint32), np.arange(side, dtype=np.uint32))
         self.pixels = ((x << 16) | y).reshape(-1)
         self.n = len(self.pixels)
-        self.desc = (
-            f"Loom's {kernel.rsplit('_', 1)[0]} (src/smallpt/vm/pt.hpp), {side}x{side} pixels, up to 64 adaptive "
-            f"samples, blur 1, threshold {threshold}, depth 2: one thread per pixel, {self.n} threads per step"
-        )
+        if threshold is None:  # primary rays: a fixed sample count, no bounces
+            self.desc = (
+                f"Loom's primary_const (src/smallpt/vm/pt.hpp), {side}x{side} pixels, 64 primary-ray samples "
+                f"per pixel, blur {blur}: one thread per pixel, {self.n} threads per step"
+            )
+        else:
+            self.desc = (
+                f"Loom's {kernel.rsplit('_', 1)[0]} (src/smallpt/vm/pt.hpp), {side}x{side} pixels, up to 64 adaptive "
+                f"samples, blur {blur}, threshold {threshold}, depth 2: one thread per pixel, {self.n} threads per step"
+            )
         self.in_bytes = 4
         self.out_bytes = 20
 
@@ -325,6 +337,10 @@ def make_workload(name):
         return LoomPathTracer("pt_const_512", "1e-4", 512)
     if name == "loom_pt2_512":
         return LoomPathTracer("pt2_const_512", "1e-3", 512)
+    if name == "loom_primary":
+        return LoomPathTracer("primary_const_256", None, 256)
+    if name == "loom_primary_b20":
+        return LoomPathTracer("primary_const_b20_256", None, 256, blur=20)
     if name == "pt":
         return PathTracing()
     if name == "pt_small":  # the profiling case: same scene at 256x192
@@ -928,7 +944,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "serve"])
+    ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "loom_primary", "loom_primary_b20", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")

@@ -31,6 +31,8 @@ extern const loom_b200::KernelEntry loom_b200_entry_lshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_lshift_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f64;
+extern const loom_b200::KernelEntry loom_b200_entry_primary_const_256;
+extern const loom_b200::KernelEntry loom_b200_entry_primary_const_b20_256;
 extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_40;
 extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_512;
 extern const loom_b200::KernelEntry loom_b200_entry_pt_const_40;
@@ -81,6 +83,8 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_lshift_u64,
     &loom_b200_entry_minmax_f32,
     &loom_b200_entry_minmax_f64,
+    &loom_b200_entry_primary_const_256,
+    &loom_b200_entry_primary_const_b20_256,
     &loom_b200_entry_pt2_const_40,
     &loom_b200_entry_pt2_const_512,
     &loom_b200_entry_pt_const_40,
@@ -100,5 +104,5 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 47;
+const int kRegistrySize = 49;
 } // namespace loom_b200

@@ -48,6 +48,11 @@ using std::uint8_t;
     /* the same programs at 512x512 pixels, enough threads to fill a GPU */    \
     X(pt_const_512,       loom::vm::pt_const<float, loom::vm::constants<CS(512), CS(0.0001), CS(64), CS(1), CS(2)>>) \
     X(pt2_const_512,      loom::vm::pt2_const<float, loom::vm::constants<CS(512), CS(0.001), CS(64), CS(1), CS(2)>>) \
+    /* Loom's primary-ray tracer (pt.hpp:1369-1420) at the configuration */    \
+    /* of its benchmark (src/benchmarks/primary.cpp:33): 256x256 pixels, */    \
+    /* 64 samples per pixel, blur 1 and 20 (CMakeLists.txt:420)          */    \
+    X(primary_const_256,  loom::vm::primary_const<float, loom::vm::constants<CS(256), CS(0.1), CS(64), CS(1)>>) \
+    X(primary_const_b20_256, loom::vm::primary_const<float, loom::vm::constants<CS(256), CS(0.1), CS(64), CS(20)>>) \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

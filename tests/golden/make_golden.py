@@ -83,7 +83,7 @@ def loom_pt_pixels(width: int = 40, height: int = 40):
 def make(name: str) -> pathlib.Path:
     if name.startswith("sphere_pt"):
         return make_pt(name)
-    if name.startswith(("pt_const", "pt2_const")):
+    if name.startswith(("pt_const", "pt2_const", "primary_const")):
         side = int(name.rsplit("_", 1)[1])
         ins = [loom_pt_pixels(side, side)]
         if len(ins[0]) > 4096:  # a seeded subset of the larger renders

@@ -57,7 +57,7 @@ def inputs_for(name: str, n: int, seed: int, input_types: List[str]) -> List[np.
             a = np.where(a == info.max, info.max - 1, a).astype(dt)
         elif name.startswith(("jmp4", "sct_inv", "slt_inv")):
             a = _ints(s, n, 0, 3, dt)
-        elif name.startswith(("pt_const", "pt2_const")):
+        elif name.startswith(("pt_const", "pt2_const", "primary_const")):
             # pixels of the square render (side in the name), encoded
             # x << 16 | y as Loom's demo does
             side = int(name.rsplit("_", 1)[1])

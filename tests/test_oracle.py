@@ -21,7 +21,8 @@ def _bits(a):
 
 # Loom's own path tracers run up to 64 adaptive samples per pixel: the C
 # restatement checks a seeded subset of their 1600 pixels to stay fast.
-SUBSET = {"pt_const_40": 160, "pt2_const_40": 160, "pt_const_512": 160, "pt2_const_512": 160}
+SUBSET = {"pt_const_40": 160, "pt2_const_40": 160, "pt_const_512": 160, "pt2_const_512": 160,
+          "primary_const_256": 160, "primary_const_b20_256": 160}
 
 
 @pytest.mark.parametrize("name", KERNELS)
