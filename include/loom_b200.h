@@ -242,6 +242,57 @@ int loom_b200_get_block_stats(loom_b200_handle* h,
                               uint64_t*         warp_instr,
                               uint32_t          num_blocks);
 
+/* ------------------------------------------------------------ state inspection
+ * The regrouping engine's work queues read back after a launch: at which
+ * Loom block each parked thread waits and the registers it carries there.
+ * This takes the place of Loom's inspector (src/vm/dbg.hpp:918-933
+ * print_state, 1143 inspect), which steps one thread on the CPU and prints
+ * its PC label and registers: here the rows are every thread the engine
+ * parked.  Threads stay parked when a launch ends before they finish, i.e.
+ * when opts.max_steps (for the regrouping engine: rounds of the megakernel)
+ * runs out; the launch then reports LOOM_B200_STATUS_STEP_LIMIT and its
+ * queues keep their rows until the handle's next launch.  After a launch
+ * that finished every thread the queues are empty. */
+
+/* One work queue: the block it holds threads for and their live registers.
+ * A block ending in a dispatch on a register the callers set (a subroutine
+ * such as Loom's RNG block) has one more queue per caller: `context` is the
+ * value the caller set, restored without being stored (-1 for a block's own
+ * queue). */
+typedef struct loom_b200_queue_layout
+{
+    uint32_t           block;    /* Loom block index (0 = START) */
+    int32_t            context;  /* dispatch context, or -1 */
+    uint32_t           num_cols; /* live registers saved per parked thread */
+    const uint32_t*    regs;     /* register index of each column (IR order, PC = 0) */
+    const int*         types;    /* enum loom_b200_type of each column */
+    const char* const* names;    /* register name of each column */
+} loom_b200_queue_layout;
+
+/* The queues of a compiled kernel (static; no GPU needed). */
+int loom_b200_kernel_queues(const char*                    kernel,
+                            uint32_t*                      num_queues,
+                            const loom_b200_queue_layout** queues);
+
+/* Threads parked in each queue at the end of the handle's last launch
+ * (waits for it; zero for the plain engine).  Writes min(max_queues, the
+ * kernel's queues) counts and the kernel's queue count. */
+int loom_b200_parked_counts(loom_b200_handle* h,
+                            uint32_t*         counts,
+                            uint32_t          max_queues,
+                            uint32_t*         num_queues);
+
+/* Copies up to max_rows parked rows of one queue to host memory: column c
+ * into cols[c] (num_cols arrays of the column's type; NULL skips a column,
+ * or all when cols is NULL) and the low 32 bits of each row's thread index
+ * into tids (may be NULL).  *rows receives the rows copied. */
+int loom_b200_parked_dump(loom_b200_handle* h,
+                          uint32_t          queue,
+                          void* const*      cols,
+                          uint32_t*         tids,
+                          uint64_t          max_rows,
+                          uint64_t*         rows);
+
 /* ------------------------------------------------------------ serving
  * Continuous batching of requests on the regrouping engine.  Replaces the
  * exchange loop of Loom's streams (StreamFacade::exchange, Loom

@@ -246,6 +246,9 @@ EXPORTS = [
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
     "loom_b200_get_block_stats",
+    "loom_b200_kernel_queues",
+    "loom_b200_parked_counts",
+    "loom_b200_parked_dump",
     "loom_b200_launch_static",
     "loom_b200_server_create",
     "loom_b200_server_destroy",
@@ -290,6 +293,25 @@ def lib() -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_uint64),
         ctypes.POINTER(ctypes.c_uint64),
         ctypes.c_uint32,
+    ]
+    L.loom_b200_kernel_queues.argtypes = [
+        ctypes.c_char_p,
+        ctypes.POINTER(ctypes.c_uint32),
+        ctypes.POINTER(ctypes.POINTER(QueueLayoutC)),
+    ]
+    L.loom_b200_parked_counts.argtypes = [
+        vp,
+        ctypes.POINTER(ctypes.c_uint32),
+        ctypes.c_uint32,
+        ctypes.POINTER(ctypes.c_uint32),
+    ]
+    L.loom_b200_parked_dump.argtypes = [
+        vp,
+        ctypes.c_uint32,
+        ctypes.POINTER(vp),
+        ctypes.POINTER(ctypes.c_uint32),
+        ctypes.c_uint64,
+        ctypes.POINTER(ctypes.c_uint64),
     ]
     L.loom_b200_server_create.argtypes = [
         ctypes.c_char_p,
@@ -354,6 +376,32 @@ def kernels() -> List[str]:
         p = ctypes.POINTER(KernelInfoC)()
         check(L.loom_b200_kernel_get(i, ctypes.byref(p)))
         out.append(p.contents.name.decode())
+    return out
+
+
+class QueueLayoutC(ctypes.Structure):
+    _fields_ = [
+        ("block", ctypes.c_uint32),
+        ("context", ctypes.c_int32),
+        ("num_cols", ctypes.c_uint32),
+        ("regs", ctypes.POINTER(ctypes.c_uint32)),
+        ("types", ctypes.POINTER(ctypes.c_int)),
+        ("names", ctypes.POINTER(ctypes.c_char_p)),
+    ]
+
+
+def queues(kernel: str) -> List[Dict]:
+    """The regrouping engine's work queues of `kernel` (static tables of the
+    library): block, dispatch context (-1: the block's own queue) and the
+    registers a parked thread carries, as (index, name, type)."""
+    nq = ctypes.c_uint32()
+    p = ctypes.POINTER(QueueLayoutC)()
+    check(lib().loom_b200_kernel_queues(kernel.encode(), ctypes.byref(nq), ctypes.byref(p)))
+    out = []
+    for q in range(nq.value):
+        c = p[q]
+        cols = [(c.regs[i], c.names[i].decode(), TYPE_NAMES[c.types[i]]) for i in range(c.num_cols)]
+        out.append({"queue": q, "block": c.block, "context": c.context, "cols": cols})
     return out
 
 
@@ -555,6 +603,39 @@ class Function:
             }
             for b in range(nb)
         ]
+
+    def parked(self, max_rows: int = 1 << 20) -> List[Dict]:
+        """The threads the last regrouping launch left parked (see
+        `loom_b200_parked_dump`): per non-empty queue its block, context,
+        row count, thread ids (low 32 bits) and one array per live
+        register, by register name."""
+        qs = queues(self.kernel)
+        counts = (ctypes.c_uint32 * max(1, len(qs)))()
+        nq = ctypes.c_uint32()
+        check(lib().loom_b200_parked_counts(self._h, counts, len(qs), ctypes.byref(nq)))
+        out = []
+        for q in qs:
+            n = min(int(counts[q["queue"]]), max_rows)
+            if n == 0:
+                continue
+            arrs = [np.empty(n, dtype=NP_TYPE[t]) for _, _, t in q["cols"]]
+            ptrs = (ctypes.c_void_p * max(1, len(arrs)))(*[a.ctypes.data for a in arrs])
+            tids = np.empty(n, dtype=np.uint32)
+            got = ctypes.c_uint64()
+            check(
+                lib().loom_b200_parked_dump(
+                    self._h,
+                    q["queue"],
+                    ptrs,
+                    tids.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                    n,
+                    ctypes.byref(got),
+                )
+            )
+            k = int(got.value)
+            regs = {name: a[:k] for (_, name, _), a in zip(q["cols"], arrs)}
+            out.append(dict(queue=q["queue"], block=q["block"], context=q["context"], rows=k, tid=tids[:k], regs=regs))
+        return out
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -543,6 +543,32 @@ def generate(k: Kernel) -> str:
     w(f'    "{name}", "{k.digest()}", {nin}u, {nout}u, kInTypes, kOutTypes, kInNames, kOutNames,')
     w(f"    {nb}u, {len(k.regs)}u, {state_size}u, {len(state)}u, kInstrs, kLive}};")
     w("")
+    # queue layouts for state inspection: the block (and dispatch context)
+    # of each queue, its columns in save order and where they lie in a row
+    assert all(rg.idx == i for i, rg in enumerate(k.regs)), "registers out of order"
+    assert all(qk is None or -(2**31) <= qk < 2**31 for _, qk in queues), "dispatch context out of range"
+    for qi, (qb, qk) in enumerate(queues):
+        cols = layout[qi]["cols"]
+        if cols:
+            w(f"const uint32_t kQRegs{qi}[] = {{{', '.join(f'{r}u' for r, _ in cols)}}};")
+            w(f"const int kQTypes{qi}[] = {{{', '.join(ABI_TYPE[L.regs[r].storage] for r, _ in cols)}}};")
+            names = ", ".join('"' + k.regs[r].name + '"' for r, _ in cols)
+            w(f"const char* const kQNames{qi}[] = {{{names}}};")
+            w(f"const unsigned long long kQOffs{qi}[] = {{{', '.join(f'{off}ull' for _, off in cols)}}};")
+    w("const loom_b200_queue_layout kQueues[] = {")
+    for qi, (qb, qk) in enumerate(queues):
+        cols = layout[qi]["cols"]
+        if cols:
+            w(f"    {{{qb}u, {-1 if qk is None else qk}, {len(cols)}u, kQRegs{qi}, kQTypes{qi}, kQNames{qi}}},")
+        else:
+            w(f"    {{{qb}u, {-1 if qk is None else qk}, 0u, nullptr, nullptr, nullptr}},")
+    w("};")
+    w("const QueueSegment kSegments[] = {")
+    for qi in range(nq):
+        offs = f"kQOffs{qi}" if layout[qi]["cols"] else "nullptr"
+        w(f"    {{{offs}, {layout[qi]['tid']}ull}},")
+    w("};")
+    w("")
     w("cudaError_t launch_plain(const PlainLaunch& a)")
     w("{")
     w("    const unsigned long long grid = (a.n + a.block - 1) / a.block;")
@@ -576,7 +602,8 @@ def generate(k: Kernel) -> str:
     w(f"const loom_b200::KernelEntry loom_b200_entry_{name} = {{")
     w(f"    &loom_b200::k_{name}::kInfo, loom_b200::k_{name}::K::kRowBytes, {nq},")
     w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
-    w(f"    &loom_b200::k_{name}::regroup_occupancy}};")
+    w(f"    &loom_b200::k_{name}::regroup_occupancy,")
+    w(f"    loom_b200::k_{name}::kQueues, loom_b200::k_{name}::kSegments}};")
     return "\n".join(o) + "\n"
 
 

@@ -152,6 +152,17 @@ const loom_b200_kernel_info kInfo = {
     "abs_f32", "b8f9f3e71f3dd087", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 4u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_U32};
+const char* const kQNames0[] = {"x"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 4ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -185,4 +196,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_abs_f32;
 const loom_b200::KernelEntry loom_b200_entry_abs_f32 = {
     &loom_b200::k_abs_f32::kInfo, loom_b200::k_abs_f32::K::kRowBytes, 1,
     &loom_b200::k_abs_f32::launch_plain, &loom_b200::k_abs_f32::launch_regroup,
-    &loom_b200::k_abs_f32::regroup_occupancy};
+    &loom_b200::k_abs_f32::regroup_occupancy,
+    loom_b200::k_abs_f32::kQueues, loom_b200::k_abs_f32::kSegments};

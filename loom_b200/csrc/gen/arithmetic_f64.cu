@@ -174,6 +174,17 @@ const loom_b200_kernel_info kInfo = {
     "arithmetic_f64", "4932865793b0f1f5", 3u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 4u, 32u, 3u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u, 1u, 2u};
+const int kQTypes0[] = {LOOM_B200_U64, LOOM_B200_F64, LOOM_B200_F64};
+const char* const kQNames0[] = {"a", "b", "c"};
+const unsigned long long kQOffs0[] = {0ull, 8ull, 16ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 3u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 24ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -207,4 +218,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_arithmetic_f64;
 const loom_b200::KernelEntry loom_b200_entry_arithmetic_f64 = {
     &loom_b200::k_arithmetic_f64::kInfo, loom_b200::k_arithmetic_f64::K::kRowBytes, 1,
     &loom_b200::k_arithmetic_f64::launch_plain, &loom_b200::k_arithmetic_f64::launch_regroup,
-    &loom_b200::k_arithmetic_f64::regroup_occupancy};
+    &loom_b200::k_arithmetic_f64::regroup_occupancy,
+    loom_b200::k_arithmetic_f64::kQueues, loom_b200::k_arithmetic_f64::kSegments};

@@ -157,6 +157,17 @@ const loom_b200_kernel_info kInfo = {
     "bit_xor_u16", "76ca05cfe2d39503", 2u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 4u, 2u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u, 1u};
+const int kQTypes0[] = {LOOM_B200_U16, LOOM_B200_U16};
+const char* const kQNames0[] = {"a", "b"};
+const unsigned long long kQOffs0[] = {0ull, 2ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 4ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -190,4 +201,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_bit_xor_u16;
 const loom_b200::KernelEntry loom_b200_entry_bit_xor_u16 = {
     &loom_b200::k_bit_xor_u16::kInfo, loom_b200::k_bit_xor_u16::K::kRowBytes, 1,
     &loom_b200::k_bit_xor_u16::launch_plain, &loom_b200::k_bit_xor_u16::launch_regroup,
-    &loom_b200::k_bit_xor_u16::regroup_occupancy};
+    &loom_b200::k_bit_xor_u16::regroup_occupancy,
+    loom_b200::k_bit_xor_u16::kQueues, loom_b200::k_bit_xor_u16::kSegments};

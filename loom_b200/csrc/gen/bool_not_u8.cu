@@ -152,6 +152,17 @@ const loom_b200_kernel_info kInfo = {
     "bool_not_u8", "8595b2d0cdb804ca", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 1u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_U8};
+const char* const kQNames0[] = {"a"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 1ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -185,4 +196,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_bool_not_u8;
 const loom_b200::KernelEntry loom_b200_entry_bool_not_u8 = {
     &loom_b200::k_bool_not_u8::kInfo, loom_b200::k_bool_not_u8::K::kRowBytes, 1,
     &loom_b200::k_bool_not_u8::launch_plain, &loom_b200::k_bool_not_u8::launch_regroup,
-    &loom_b200::k_bool_not_u8::regroup_occupancy};
+    &loom_b200::k_bool_not_u8::regroup_occupancy,
+    loom_b200::k_bool_not_u8::kQueues, loom_b200::k_bool_not_u8::kSegments};

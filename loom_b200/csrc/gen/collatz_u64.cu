@@ -185,6 +185,23 @@ const loom_b200_kernel_info kInfo = {
     "collatz_u64", "1d3a9b27bd054717", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     2u, 7u, 52u, 2u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {1u};
+const int kQTypes0[] = {LOOM_B200_U64};
+const char* const kQNames0[] = {"n"};
+const unsigned long long kQOffs0[] = {0ull};
+const uint32_t kQRegs1[] = {1u, 2u};
+const int kQTypes1[] = {LOOM_B200_U64, LOOM_B200_U32};
+const char* const kQNames1[] = {"n", "steps"};
+const unsigned long long kQOffs1[] = {16ull, 24ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+    {1u, -1, 2u, kQRegs1, kQTypes1, kQNames1},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 8ull},
+    {kQOffs1, 28ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -218,4 +235,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_collatz_u64;
 const loom_b200::KernelEntry loom_b200_entry_collatz_u64 = {
     &loom_b200::k_collatz_u64::kInfo, loom_b200::k_collatz_u64::K::kRowBytes, 2,
     &loom_b200::k_collatz_u64::launch_plain, &loom_b200::k_collatz_u64::launch_regroup,
-    &loom_b200::k_collatz_u64::regroup_occupancy};
+    &loom_b200::k_collatz_u64::regroup_occupancy,
+    loom_b200::k_collatz_u64::kQueues, loom_b200::k_collatz_u64::kSegments};

@@ -191,6 +191,29 @@ const loom_b200_kernel_info kInfo = {
     "fac_u64", "6ae155bc014b7b7e", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 4u, 32u, 2u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {1u};
+const int kQTypes0[] = {LOOM_B200_U64};
+const char* const kQNames0[] = {"a"};
+const unsigned long long kQOffs0[] = {0ull};
+const uint32_t kQRegs1[] = {1u};
+const int kQTypes1[] = {LOOM_B200_U64};
+const char* const kQNames1[] = {"a"};
+const unsigned long long kQOffs1[] = {16ull};
+const uint32_t kQRegs2[] = {1u, 3u};
+const int kQTypes2[] = {LOOM_B200_U64, LOOM_B200_U64};
+const char* const kQNames2[] = {"a", "c"};
+const unsigned long long kQOffs2[] = {32ull, 40ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+    {1u, -1, 1u, kQRegs1, kQTypes1, kQNames1},
+    {2u, -1, 2u, kQRegs2, kQTypes2, kQNames2},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 8ull},
+    {kQOffs1, 24ull},
+    {kQOffs2, 48ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -224,4 +247,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_fac_u64;
 const loom_b200::KernelEntry loom_b200_entry_fac_u64 = {
     &loom_b200::k_fac_u64::kInfo, loom_b200::k_fac_u64::K::kRowBytes, 3,
     &loom_b200::k_fac_u64::launch_plain, &loom_b200::k_fac_u64::launch_regroup,
-    &loom_b200::k_fac_u64::regroup_occupancy};
+    &loom_b200::k_fac_u64::regroup_occupancy,
+    loom_b200::k_fac_u64::kQueues, loom_b200::k_fac_u64::kSegments};

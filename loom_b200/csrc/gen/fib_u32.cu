@@ -204,6 +204,29 @@ const loom_b200_kernel_info kInfo = {
     "fib_u32", "4878b52b2b7bd460", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     3u, 7u, 28u, 4u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {1u};
+const int kQTypes0[] = {LOOM_B200_U32};
+const char* const kQNames0[] = {"n"};
+const unsigned long long kQOffs0[] = {0ull};
+const uint32_t kQRegs1[] = {1u};
+const int kQTypes1[] = {LOOM_B200_U32};
+const char* const kQNames1[] = {"n"};
+const unsigned long long kQOffs1[] = {8ull};
+const uint32_t kQRegs2[] = {1u, 2u, 4u, 5u};
+const int kQTypes2[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames2[] = {"n", "c", "p", "i"};
+const unsigned long long kQOffs2[] = {16ull, 20ull, 24ull, 28ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+    {1u, -1, 1u, kQRegs1, kQTypes1, kQNames1},
+    {2u, -1, 4u, kQRegs2, kQTypes2, kQNames2},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 4ull},
+    {kQOffs1, 12ull},
+    {kQOffs2, 32ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -237,4 +260,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_fib_u32;
 const loom_b200::KernelEntry loom_b200_entry_fib_u32 = {
     &loom_b200::k_fib_u32::kInfo, loom_b200::k_fib_u32::K::kRowBytes, 3,
     &loom_b200::k_fib_u32::launch_plain, &loom_b200::k_fib_u32::launch_regroup,
-    &loom_b200::k_fib_u32::regroup_occupancy};
+    &loom_b200::k_fib_u32::regroup_occupancy,
+    loom_b200::k_fib_u32::kQueues, loom_b200::k_fib_u32::kSegments};

@@ -151,6 +151,17 @@ const loom_b200_kernel_info kInfo = {
     "increment_i16", "017b81187c11eef8", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 1u, 2u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_I16};
+const char* const kQNames0[] = {"val"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 2ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -184,4 +195,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_increment_i16;
 const loom_b200::KernelEntry loom_b200_entry_increment_i16 = {
     &loom_b200::k_increment_i16::kInfo, loom_b200::k_increment_i16::K::kRowBytes, 1,
     &loom_b200::k_increment_i16::launch_plain, &loom_b200::k_increment_i16::launch_regroup,
-    &loom_b200::k_increment_i16::regroup_occupancy};
+    &loom_b200::k_increment_i16::regroup_occupancy,
+    loom_b200::k_increment_i16::kQueues, loom_b200::k_increment_i16::kSegments};

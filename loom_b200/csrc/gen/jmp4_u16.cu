@@ -209,6 +209,25 @@ const loom_b200_kernel_info kInfo = {
     "jmp4_u16", "32b4dc4a191cac25", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     5u, 2u, 4u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {1u};
+const int kQTypes0[] = {LOOM_B200_U16};
+const char* const kQNames0[] = {"i"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+    {1u, -1, 0u, nullptr, nullptr, nullptr},
+    {2u, -1, 0u, nullptr, nullptr, nullptr},
+    {3u, -1, 0u, nullptr, nullptr, nullptr},
+    {4u, -1, 0u, nullptr, nullptr, nullptr},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 2ull},
+    {nullptr, 8ull},
+    {nullptr, 16ull},
+    {nullptr, 24ull},
+    {nullptr, 32ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -242,4 +261,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_jmp4_u16;
 const loom_b200::KernelEntry loom_b200_entry_jmp4_u16 = {
     &loom_b200::k_jmp4_u16::kInfo, loom_b200::k_jmp4_u16::K::kRowBytes, 5,
     &loom_b200::k_jmp4_u16::launch_plain, &loom_b200::k_jmp4_u16::launch_regroup,
-    &loom_b200::k_jmp4_u16::regroup_occupancy};
+    &loom_b200::k_jmp4_u16::regroup_occupancy,
+    loom_b200::k_jmp4_u16::kQueues, loom_b200::k_jmp4_u16::kSegments};

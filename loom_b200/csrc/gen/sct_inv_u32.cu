@@ -157,6 +157,17 @@ const loom_b200_kernel_info kInfo = {
     "sct_inv_u32", "9f3afb7c761fec65", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_U32};
+const char* const kQNames0[] = {"i"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 4ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -190,4 +201,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_sct_inv_u32;
 const loom_b200::KernelEntry loom_b200_entry_sct_inv_u32 = {
     &loom_b200::k_sct_inv_u32::kInfo, loom_b200::k_sct_inv_u32::K::kRowBytes, 1,
     &loom_b200::k_sct_inv_u32::launch_plain, &loom_b200::k_sct_inv_u32::launch_regroup,
-    &loom_b200::k_sct_inv_u32::regroup_occupancy};
+    &loom_b200::k_sct_inv_u32::regroup_occupancy,
+    loom_b200::k_sct_inv_u32::kQueues, loom_b200::k_sct_inv_u32::kSegments};

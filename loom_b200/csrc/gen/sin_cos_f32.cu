@@ -162,6 +162,17 @@ const loom_b200_kernel_info kInfo = {
     "sin_cos_f32", "914e172005128d9b", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 8u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_U32};
+const char* const kQNames0[] = {"x"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 4ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -195,4 +206,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_sin_cos_f32;
 const loom_b200::KernelEntry loom_b200_entry_sin_cos_f32 = {
     &loom_b200::k_sin_cos_f32::kInfo, loom_b200::k_sin_cos_f32::K::kRowBytes, 1,
     &loom_b200::k_sin_cos_f32::launch_plain, &loom_b200::k_sin_cos_f32::launch_regroup,
-    &loom_b200::k_sin_cos_f32::regroup_occupancy};
+    &loom_b200::k_sin_cos_f32::regroup_occupancy,
+    loom_b200::k_sin_cos_f32::kQueues, loom_b200::k_sin_cos_f32::kSegments};

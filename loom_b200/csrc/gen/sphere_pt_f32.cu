@@ -2534,6 +2534,179 @@ const loom_b200_kernel_info kInfo = {
     "sphere_pt_f32", "144eab9a4253b9da", 2u, 3u, kInTypes, kOutTypes, kInNames, kOutNames,
     24u, 134u, 536u, 71u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {1u, 2u};
+const int kQTypes0[] = {LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames0[] = {"inst", "sid"};
+const unsigned long long kQOffs0[] = {0ull, 4ull};
+const uint32_t kQRegs1[] = {7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u, 130u, 131u};
+const int kQTypes1[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames1[] = {"w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1", "u0", "u1"};
+const unsigned long long kQOffs1[] = {16ull, 20ull, 24ull, 28ull, 32ull, 36ull, 40ull, 44ull, 48ull, 52ull, 56ull, 60ull, 64ull, 68ull, 72ull, 76ull, 80ull};
+const uint32_t kQRegs2[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u};
+const int kQTypes2[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
+const char* const kQNames2[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth"};
+const unsigned long long kQOffs2[] = {88ull, 92ull, 96ull, 100ull, 104ull, 108ull, 112ull, 116ull, 120ull, 124ull, 128ull, 132ull, 136ull, 140ull, 144ull, 148ull, 152ull, 156ull, 160ull};
+const uint32_t kQRegs3[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u, 55u, 56u};
+const int kQTypes3[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames3[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid", "i", "sp"};
+const unsigned long long kQOffs3[] = {168ull, 172ull, 176ull, 180ull, 184ull, 188ull, 192ull, 196ull, 200ull, 204ull, 208ull, 212ull, 216ull, 220ull, 224ull, 228ull, 232ull, 236ull, 240ull, 244ull, 248ull, 252ull, 256ull};
+const uint32_t kQRegs4[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u};
+const int kQTypes4[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
+const char* const kQNames4[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid"};
+const unsigned long long kQOffs4[] = {264ull, 268ull, 272ull, 276ull, 280ull, 284ull, 288ull, 292ull, 296ull, 300ull, 304ull, 308ull, 312ull, 316ull, 320ull, 324ull, 328ull, 332ull, 336ull, 340ull, 344ull};
+const uint32_t kQRegs5[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u};
+const int kQTypes5[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
+const char* const kQNames5[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid"};
+const unsigned long long kQOffs5[] = {352ull, 356ull, 360ull, 364ull, 368ull, 372ull, 376ull, 380ull, 384ull, 388ull, 392ull, 396ull, 400ull, 404ull, 408ull, 412ull, 416ull, 420ull, 424ull, 428ull, 432ull};
+const uint32_t kQRegs6[] = {3u, 4u, 5u, 49u, 50u, 51u, 76u, 77u, 78u};
+const int kQTypes6[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames6[] = {"L0", "L1", "L2", "T0", "T1", "T2", "cr", "cg", "cb"};
+const unsigned long long kQOffs6[] = {440ull, 444ull, 448ull, 452ull, 456ull, 460ull, 464ull, 468ull, 472ull};
+const uint32_t kQRegs7[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
+const int kQTypes7[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames7[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
+const unsigned long long kQOffs7[] = {480ull, 484ull, 488ull, 492ull, 496ull, 500ull, 504ull, 508ull, 512ull, 516ull, 520ull, 524ull, 528ull, 532ull, 536ull, 540ull, 544ull, 548ull, 552ull, 556ull, 560ull, 564ull, 568ull, 572ull, 576ull, 580ull};
+const uint32_t kQRegs8[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
+const int kQTypes8[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames8[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
+const unsigned long long kQOffs8[] = {592ull, 596ull, 600ull, 604ull, 608ull, 612ull, 616ull, 620ull, 624ull, 628ull, 632ull, 636ull, 640ull, 644ull, 648ull, 652ull, 656ull, 660ull, 664ull, 668ull, 672ull, 676ull, 680ull, 684ull, 688ull, 692ull};
+const uint32_t kQRegs9[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
+const int kQTypes9[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames9[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
+const unsigned long long kQOffs9[] = {704ull, 708ull, 712ull, 716ull, 720ull, 724ull, 728ull, 732ull, 736ull, 740ull, 744ull, 748ull, 752ull, 756ull, 760ull, 764ull, 768ull, 772ull, 776ull, 780ull, 784ull, 788ull, 792ull, 796ull, 800ull, 804ull};
+const uint32_t kQRegs10[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 130u};
+const int kQTypes10[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
+const char* const kQNames10[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "u0"};
+const unsigned long long kQOffs10[] = {816ull, 820ull, 824ull, 828ull, 832ull, 836ull, 840ull, 844ull, 848ull, 852ull, 856ull, 860ull, 864ull, 868ull, 872ull, 876ull, 880ull, 884ull, 888ull, 892ull, 896ull, 900ull, 904ull, 908ull, 912ull, 916ull, 920ull};
+const uint32_t kQRegs11[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 86u};
+const int kQTypes11[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames11[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "p"};
+const unsigned long long kQOffs11[] = {928ull, 932ull, 936ull, 940ull, 944ull, 948ull, 952ull, 956ull, 960ull, 964ull, 968ull, 972ull, 976ull, 980ull, 984ull, 988ull, 992ull, 996ull, 1000ull, 1004ull, 1008ull, 1012ull, 1016ull, 1020ull, 1024ull, 1028ull, 1032ull};
+const uint32_t kQRegs12[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
+const int kQTypes12[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames12[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
+const unsigned long long kQOffs12[] = {1040ull, 1044ull, 1048ull, 1052ull, 1056ull, 1060ull, 1064ull, 1068ull, 1072ull, 1076ull, 1080ull, 1084ull, 1088ull, 1092ull, 1096ull, 1100ull, 1104ull, 1108ull, 1112ull, 1116ull, 1120ull, 1124ull, 1128ull, 1132ull, 1136ull, 1140ull};
+const uint32_t kQRegs13[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u};
+const int kQTypes13[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames13[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn"};
+const unsigned long long kQOffs13[] = {1152ull, 1156ull, 1160ull, 1164ull, 1168ull, 1172ull, 1176ull, 1180ull, 1184ull, 1188ull, 1192ull, 1196ull, 1200ull, 1204ull, 1208ull, 1212ull, 1216ull, 1220ull, 1224ull, 1228ull, 1232ull, 1236ull, 1240ull};
+const uint32_t kQRegs14[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u};
+const int kQTypes14[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames14[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2"};
+const unsigned long long kQOffs14[] = {1248ull, 1252ull, 1256ull, 1260ull, 1264ull, 1268ull, 1272ull, 1276ull, 1280ull, 1284ull, 1288ull, 1292ull, 1296ull, 1300ull, 1304ull, 1308ull, 1312ull, 1316ull, 1320ull};
+const uint32_t kQRegs15[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u};
+const int kQTypes15[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames15[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2"};
+const unsigned long long kQOffs15[] = {1328ull, 1332ull, 1336ull, 1340ull, 1344ull, 1348ull, 1352ull, 1356ull, 1360ull, 1364ull, 1368ull, 1372ull, 1376ull, 1380ull, 1384ull, 1388ull, 1392ull, 1396ull, 1400ull, 1404ull, 1408ull, 1412ull, 1416ull, 1420ull, 1424ull};
+const uint32_t kQRegs16[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 130u, 131u};
+const int kQTypes16[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames16[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "u0", "u1"};
+const unsigned long long kQOffs16[] = {1432ull, 1436ull, 1440ull, 1444ull, 1448ull, 1452ull, 1456ull, 1460ull, 1464ull, 1468ull, 1472ull, 1476ull, 1480ull, 1484ull, 1488ull, 1492ull, 1496ull, 1500ull, 1504ull, 1508ull, 1512ull, 1516ull, 1520ull, 1524ull, 1528ull, 1532ull, 1536ull};
+const uint32_t kQRegs17[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 106u, 107u, 108u};
+const int kQTypes17[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames17[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "dx", "dy", "rr2"};
+const unsigned long long kQOffs17[] = {1544ull, 1548ull, 1552ull, 1556ull, 1560ull, 1564ull, 1568ull, 1572ull, 1576ull, 1580ull, 1584ull, 1588ull, 1592ull, 1596ull, 1600ull, 1604ull, 1608ull, 1612ull, 1616ull, 1620ull, 1624ull, 1628ull, 1632ull, 1636ull, 1640ull, 1644ull, 1648ull, 1652ull};
+const uint32_t kQRegs18[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 88u, 92u, 93u, 94u};
+const int kQTypes18[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames18[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "into", "nl0", "nl1", "nl2"};
+const unsigned long long kQOffs18[] = {1664ull, 1668ull, 1672ull, 1676ull, 1680ull, 1684ull, 1688ull, 1692ull, 1696ull, 1700ull, 1704ull, 1708ull, 1712ull, 1716ull, 1720ull, 1724ull, 1728ull, 1732ull, 1736ull, 1740ull, 1744ull, 1748ull, 1752ull, 1756ull, 1760ull, 1764ull, 1768ull};
+const uint32_t kQRegs19[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 88u, 111u, 112u, 113u};
+const int kQTypes19[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames19[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "into", "nnt", "ddn", "c2"};
+const unsigned long long kQOffs19[] = {1776ull, 1780ull, 1784ull, 1788ull, 1792ull, 1796ull, 1800ull, 1804ull, 1808ull, 1812ull, 1816ull, 1820ull, 1824ull, 1828ull, 1832ull, 1836ull, 1840ull, 1844ull, 1848ull, 1852ull, 1856ull, 1860ull, 1864ull, 1868ull, 1872ull, 1876ull, 1880ull};
+const uint32_t kQRegs20[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 117u, 118u, 119u, 127u, 128u, 129u, 130u};
+const int kQTypes20[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
+const char* const kQNames20[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "td0", "td1", "td2", "pp", "rp", "tp", "u0"};
+const unsigned long long kQOffs20[] = {1888ull, 1892ull, 1896ull, 1900ull, 1904ull, 1908ull, 1912ull, 1916ull, 1920ull, 1924ull, 1928ull, 1932ull, 1936ull, 1940ull, 1944ull, 1948ull, 1952ull, 1956ull, 1960ull, 1964ull, 1968ull, 1972ull, 1976ull, 1980ull, 1984ull, 1988ull, 1992ull, 1996ull, 2000ull, 2004ull};
+const uint32_t kQRegs21[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 128u};
+const int kQTypes21[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames21[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "rp"};
+const unsigned long long kQOffs21[] = {2016ull, 2020ull, 2024ull, 2028ull, 2032ull, 2036ull, 2040ull, 2044ull, 2048ull, 2052ull, 2056ull, 2060ull, 2064ull, 2068ull, 2072ull, 2076ull, 2080ull, 2084ull, 2088ull, 2092ull, 2096ull, 2100ull, 2104ull, 2108ull};
+const uint32_t kQRegs22[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 117u, 118u, 119u, 129u};
+const int kQTypes22[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames22[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "td0", "td1", "td2", "tp"};
+const unsigned long long kQOffs22[] = {2120ull, 2124ull, 2128ull, 2132ull, 2136ull, 2140ull, 2144ull, 2148ull, 2152ull, 2156ull, 2160ull, 2164ull, 2168ull, 2172ull, 2176ull, 2180ull, 2184ull, 2188ull, 2192ull, 2196ull};
+const uint32_t kQRegs23[] = {3u, 4u, 5u, 7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 87u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 117u, 118u, 119u, 127u, 128u, 129u};
+const int kQTypes23[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames23[] = {"L0", "L1", "L2", "w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1", "rpt", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "dn", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "td0", "td1", "td2", "pp", "rp", "tp"};
+const unsigned long long kQOffs23[] = {2208ull, 2212ull, 2216ull, 2220ull, 2224ull, 2228ull, 2232ull, 2236ull, 2240ull, 2244ull, 2248ull, 2252ull, 2256ull, 2260ull, 2264ull, 2268ull, 2272ull, 2276ull, 2280ull, 2284ull, 2288ull, 2292ull, 2296ull, 2300ull, 2304ull, 2308ull, 2312ull, 2316ull, 2320ull, 2324ull, 2328ull, 2332ull, 2336ull, 2340ull, 2344ull, 2348ull, 2352ull, 2356ull, 2360ull, 2364ull, 2368ull, 2372ull, 2376ull, 2380ull, 2384ull, 2388ull, 2392ull, 2396ull, 2400ull, 2404ull, 2408ull, 2412ull, 2416ull, 2420ull, 2424ull};
+const uint32_t kQRegs24[] = {7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u};
+const int kQTypes24[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
+const char* const kQNames24[] = {"w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1"};
+const unsigned long long kQOffs24[] = {2432ull, 2436ull, 2440ull, 2444ull, 2448ull, 2452ull, 2456ull, 2460ull, 2464ull, 2468ull, 2472ull, 2476ull, 2480ull, 2484ull, 2488ull};
+const uint32_t kQRegs25[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
+const int kQTypes25[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames25[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
+const unsigned long long kQOffs25[] = {2496ull, 2500ull, 2504ull, 2508ull, 2512ull, 2516ull, 2520ull, 2524ull, 2528ull, 2532ull, 2536ull, 2540ull, 2544ull, 2548ull, 2552ull, 2556ull, 2560ull, 2564ull, 2568ull, 2572ull, 2576ull, 2580ull, 2584ull, 2588ull, 2592ull, 2596ull};
+const uint32_t kQRegs26[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u};
+const int kQTypes26[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames26[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2"};
+const unsigned long long kQOffs26[] = {2608ull, 2612ull, 2616ull, 2620ull, 2624ull, 2628ull, 2632ull, 2636ull, 2640ull, 2644ull, 2648ull, 2652ull, 2656ull, 2660ull, 2664ull, 2668ull, 2672ull, 2676ull, 2680ull, 2684ull, 2688ull, 2692ull, 2696ull, 2700ull, 2704ull};
+const uint32_t kQRegs27[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 117u, 118u, 119u, 127u, 128u, 129u};
+const int kQTypes27[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames27[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "td0", "td1", "td2", "pp", "rp", "tp"};
+const unsigned long long kQOffs27[] = {2712ull, 2716ull, 2720ull, 2724ull, 2728ull, 2732ull, 2736ull, 2740ull, 2744ull, 2748ull, 2752ull, 2756ull, 2760ull, 2764ull, 2768ull, 2772ull, 2776ull, 2780ull, 2784ull, 2788ull, 2792ull, 2796ull, 2800ull, 2804ull, 2808ull, 2812ull, 2816ull, 2820ull, 2824ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
+    {1u, -1, 17u, kQRegs1, kQTypes1, kQNames1},
+    {2u, -1, 19u, kQRegs2, kQTypes2, kQNames2},
+    {3u, -1, 23u, kQRegs3, kQTypes3, kQNames3},
+    {4u, -1, 21u, kQRegs4, kQTypes4, kQNames4},
+    {5u, -1, 21u, kQRegs5, kQTypes5, kQNames5},
+    {6u, -1, 9u, kQRegs6, kQTypes6, kQNames6},
+    {7u, -1, 26u, kQRegs7, kQTypes7, kQNames7},
+    {8u, -1, 26u, kQRegs8, kQTypes8, kQNames8},
+    {9u, -1, 26u, kQRegs9, kQTypes9, kQNames9},
+    {10u, -1, 27u, kQRegs10, kQTypes10, kQNames10},
+    {11u, -1, 27u, kQRegs11, kQTypes11, kQNames11},
+    {12u, -1, 26u, kQRegs12, kQTypes12, kQNames12},
+    {13u, -1, 23u, kQRegs13, kQTypes13, kQNames13},
+    {14u, -1, 19u, kQRegs14, kQTypes14, kQNames14},
+    {15u, -1, 25u, kQRegs15, kQTypes15, kQNames15},
+    {16u, -1, 27u, kQRegs16, kQTypes16, kQNames16},
+    {17u, -1, 28u, kQRegs17, kQTypes17, kQNames17},
+    {18u, -1, 27u, kQRegs18, kQTypes18, kQNames18},
+    {19u, -1, 27u, kQRegs19, kQTypes19, kQNames19},
+    {20u, -1, 30u, kQRegs20, kQTypes20, kQNames20},
+    {21u, -1, 24u, kQRegs21, kQTypes21, kQNames21},
+    {22u, -1, 20u, kQRegs22, kQTypes22, kQNames22},
+    {23u, -1, 55u, kQRegs23, kQTypes23, kQNames23},
+    {23u, 0, 15u, kQRegs24, kQTypes24, kQNames24},
+    {23u, 1, 26u, kQRegs25, kQTypes25, kQNames25},
+    {23u, 2, 25u, kQRegs26, kQTypes26, kQNames26},
+    {23u, 3, 29u, kQRegs27, kQTypes27, kQNames27},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 8ull},
+    {kQOffs1, 84ull},
+    {kQOffs2, 164ull},
+    {kQOffs3, 260ull},
+    {kQOffs4, 348ull},
+    {kQOffs5, 436ull},
+    {kQOffs6, 476ull},
+    {kQOffs7, 584ull},
+    {kQOffs8, 696ull},
+    {kQOffs9, 808ull},
+    {kQOffs10, 924ull},
+    {kQOffs11, 1036ull},
+    {kQOffs12, 1144ull},
+    {kQOffs13, 1244ull},
+    {kQOffs14, 1324ull},
+    {kQOffs15, 1428ull},
+    {kQOffs16, 1540ull},
+    {kQOffs17, 1656ull},
+    {kQOffs18, 1772ull},
+    {kQOffs19, 1884ull},
+    {kQOffs20, 2008ull},
+    {kQOffs21, 2112ull},
+    {kQOffs22, 2200ull},
+    {kQOffs23, 2428ull},
+    {kQOffs24, 2492ull},
+    {kQOffs25, 2600ull},
+    {kQOffs26, 2708ull},
+    {kQOffs27, 2828ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -2567,4 +2740,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_sphere_pt_f32;
 const loom_b200::KernelEntry loom_b200_entry_sphere_pt_f32 = {
     &loom_b200::k_sphere_pt_f32::kInfo, loom_b200::k_sphere_pt_f32::K::kRowBytes, 28,
     &loom_b200::k_sphere_pt_f32::launch_plain, &loom_b200::k_sphere_pt_f32::launch_regroup,
-    &loom_b200::k_sphere_pt_f32::regroup_occupancy};
+    &loom_b200::k_sphere_pt_f32::regroup_occupancy,
+    loom_b200::k_sphere_pt_f32::kQueues, loom_b200::k_sphere_pt_f32::kSegments};

@@ -153,6 +153,17 @@ const loom_b200_kernel_info kInfo = {
     "union_f64", "3e8da7eca4ff6655", 1u, 1u, kInTypes, kOutTypes, kInNames, kOutNames,
     1u, 2u, 16u, 1u, kInstrs, kLive};
 
+const uint32_t kQRegs0[] = {0u};
+const int kQTypes0[] = {LOOM_B200_F64};
+const char* const kQNames0[] = {"i"};
+const unsigned long long kQOffs0[] = {0ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 8ull},
+};
+
 cudaError_t launch_plain(const PlainLaunch& a)
 {
     const unsigned long long grid = (a.n + a.block - 1) / a.block;
@@ -186,4 +197,5 @@ extern const loom_b200::KernelEntry loom_b200_entry_union_f64;
 const loom_b200::KernelEntry loom_b200_entry_union_f64 = {
     &loom_b200::k_union_f64::kInfo, loom_b200::k_union_f64::K::kRowBytes, 1,
     &loom_b200::k_union_f64::launch_plain, &loom_b200::k_union_f64::launch_regroup,
-    &loom_b200::k_union_f64::regroup_occupancy};
+    &loom_b200::k_union_f64::regroup_occupancy,
+    loom_b200::k_union_f64::kQueues, loom_b200::k_union_f64::kSegments};

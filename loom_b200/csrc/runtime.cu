@@ -138,6 +138,7 @@ struct loom_b200_handle
 
     loom_b200_stats stats{};
     unsigned        last_grid     = 0;
+    uint64_t        last_cap      = 0; // queue capacity of the last launch (0: plain)
     bool            pending       = false; // launched, counters not read yet
     uint64_t        launches      = 0;
     uint64_t        plain_threads = 0;
@@ -403,9 +404,11 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
             LB_CUDA(e.regroup(L));
         }
         h->last_grid = L.grid;
+        h->last_cap  = cap;
     }
     else
     {
+        h->last_cap = 0;
         PlainLaunch L{};
         L.cols      = cols;
         L.n         = n;
@@ -744,6 +747,90 @@ loom_b200_get_block_stats(loom_b200_handle* h,
         thread_instr[b] = c[2 * b];
         warp_instr[b]   = c[2 * b + 1];
     }
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_kernel_queues(const char* kernel, uint32_t* num_queues, const loom_b200_queue_layout** queues)
+{
+    if(!kernel || !num_queues || !queues) return LOOM_B200_ERR_INVALID;
+    for(int i = 0; i < kRegistrySize; ++i)
+        if(std::strcmp(kRegistry[i]->info->name, kernel) == 0)
+        {
+            *num_queues = kRegistry[i]->num_queues;
+            *queues     = kRegistry[i]->queues;
+            return LOOM_B200_OK;
+        }
+    g_last_error = "kernel not compiled into libloom_b200";
+    return LOOM_B200_ERR_NOT_FOUND;
+}
+
+namespace
+{
+/// Parked rows per queue after the handle's last launch, and the parity of
+/// the state half that holds them: the megakernel parks a round's leftovers
+/// in the half of the next round, whose number it leaves in the control
+/// block; the counts of that half survive the launch.
+int
+parked_state(loom_b200_handle* h, std::vector<unsigned>& counts, unsigned& parity)
+{
+    const int rc = finish_launch(h);
+    if(rc != LOOM_B200_OK && rc != LOOM_B200_ERR_DEVICE) return rc;
+    const unsigned B = h->e->num_queues;
+    counts.assign(B, 0u);
+    parity = 0;
+    if(h->last_cap == 0 || !h->d_qcnt) return LOOM_B200_OK;
+    RegroupCtl ctl{};
+    LB_CUDA(cudaMemcpy(&ctl, h->d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost));
+    parity = static_cast<unsigned>(ctl.next_round & 1ull);
+    LB_CUDA(cudaMemcpy(counts.data(), h->d_qcnt + parity * B, B * sizeof(unsigned), cudaMemcpyDeviceToHost));
+    for(unsigned& c : counts)
+        if(c > h->last_cap) c = static_cast<unsigned>(h->last_cap); // rows past capacity were never written
+    return LOOM_B200_OK;
+}
+} // namespace
+
+int
+loom_b200_parked_counts(loom_b200_handle* h, uint32_t* counts, uint32_t max_queues, uint32_t* num_queues)
+{
+    if(!h || (!counts && max_queues)) return LOOM_B200_ERR_INVALID;
+    std::vector<unsigned> c;
+    unsigned              parity = 0;
+    const int             rc     = parked_state(h, c, parity);
+    if(rc) return rc;
+    for(uint32_t q = 0; q < max_queues && q < c.size(); ++q) counts[q] = c[q];
+    if(num_queues) *num_queues = static_cast<uint32_t>(c.size());
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_parked_dump(loom_b200_handle* h,
+                      uint32_t          queue,
+                      void* const*      cols,
+                      uint32_t*         tids,
+                      uint64_t          max_rows,
+                      uint64_t*         rows)
+{
+    if(!h || !rows || queue >= h->e->num_queues) return LOOM_B200_ERR_INVALID;
+    *rows = 0;
+    std::vector<unsigned> c;
+    unsigned              parity = 0;
+    const int             rc     = parked_state(h, c, parity);
+    if(rc) return rc;
+    const uint64_t n = std::min<uint64_t>(c[queue], max_rows);
+    if(n == 0) return LOOM_B200_OK;
+    const loom_b200_queue_layout& ql   = h->e->queues[queue];
+    const QueueSegment&           seg  = h->e->segments[queue];
+    const uint64_t                cap  = h->last_cap;
+    const char*                   half = h->d_state + parity * h->e->row_bytes * cap;
+    for(uint32_t k = 0; cols && k < ql.num_cols; ++k)
+    {
+        if(!cols[k]) continue;
+        const size_t width = type_bytes(ql.types[k]);
+        LB_CUDA(cudaMemcpy(cols[k], half + seg.col_off[k] * cap, n * width, cudaMemcpyDeviceToHost));
+    }
+    if(tids) LB_CUDA(cudaMemcpy(tids, half + seg.tid_off * cap, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    *rows = n;
     return LOOM_B200_OK;
 }
 

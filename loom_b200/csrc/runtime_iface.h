@@ -30,6 +30,16 @@ struct RegroupLaunch
     cudaStream_t  stream;
 };
 
+/// Where one queue's columns lie in a row of the regrouping state: column c
+/// of queue q holds `cap` values from byte `col_off[c] * cap` of the state
+/// half of the round's parity, the thread ids (low 32 bits) from
+/// `tid_off * cap`.
+struct QueueSegment
+{
+    const unsigned long long* col_off;
+    unsigned long long        tid_off;
+};
+
 /// One compiled kernel: its descriptor and the launchers of both engines.
 struct KernelEntry
 {
@@ -39,6 +49,8 @@ struct KernelEntry
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
     cudaError_t (*regroup_occupancy)(int block, bool profile, int* ctas_per_sm);
+    const loom_b200_queue_layout* queues;   // num_queues entries
+    const QueueSegment*           segments; // num_queues entries
 };
 
 extern const KernelEntry* const kRegistry[];
