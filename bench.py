@@ -524,6 +524,35 @@ def same_bits(got, want, kernel: str = "") -> bool:
 
 
 # ---------------------------------------------------------------- GPU arm
+def ncu_rooflines(w, kern_ms: float, sm_mhz: float, path: pathlib.Path = None):
+    """Figures of the dominant kernel that come from an ncu capture
+    (profiles/roofline_traffic.json, per thread, scaled to this launch):
+    DRAM traffic per launch, and the issue roofline — SASS warp instructions
+    per second against one per cycle on each of the 148 x 4 SM
+    sub-partitions at `sm_mhz`.  The issue figure is given only when the
+    capture was taken with the same regrouping options.  Returns (traffic
+    bytes or None, issue dict or None)."""
+    tf = path or ROOT / "profiles" / "roofline_traffic.json"
+    if not tf.exists():
+        return None, None
+    t = json.loads(tf.read_text()).get(w.tune_key)
+    if not t or t.get("kernel") != w.kernel:
+        return None, None
+    traffic = int(t["dram_bytes_per_thread"] * w.n) if t.get("dram_bytes_per_thread") else None
+    issue = None
+    if t.get("sass_options") == w.opts and t.get("sass_warp_inst_per_thread") and kern_ms > 0:
+        got = t["sass_warp_inst_per_thread"] * w.n / (kern_ms / 1e3) / 1e9
+        top = 148 * 4 * sm_mhz / 1e3
+        issue = {
+            "achieved": round(got, 1),
+            "peak": round(top, 1),
+            "unit": "G warp instructions/s",
+            "frac": round(got / top, 4),
+            "sass_warp_inst_per_thread": t["sass_warp_inst_per_thread"],
+        }
+    return traffic, issue
+
+
 def max_over_ranks(x: float, dist=None, device: str = "cuda") -> float:
     """The largest `x` over the ranks of the process group (every rank gets
     it); `x` itself without one.  NCCL groups reduce a CUDA tensor, gloo
@@ -983,6 +1012,8 @@ def main() -> None:
         value = statistics.median(vals)
         line = base_line(args, warmup, args.gpus, w.desc, w.kernel, w.dtype, METRIC, extra)
         line = {"impl": "reference", **line, "value": round(value, 3)}
+        # the whole workload at the sampled rate
+        line["ms_per_step"] = round(w.n / (value * 1e6) * 1e3, 4)
         line["cpu_baseline"] = dict(info, value=round(value, 3))
         line["e2e"] = {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
         print(json.dumps(line))
@@ -1084,31 +1115,9 @@ def main() -> None:
     algo_bytes = w.n * (w.in_bytes + w.out_bytes) + state_per_launch
     achieved = algo_bytes / (kern_ms / 1e3) / 1e9
 
-    # DRAM traffic of the dominant kernel from an ncu capture (per thread,
-    # scaled to this launch), see profiles/roofline_traffic.json
-    traffic = None
-    issue = None
-    tf = ROOT / "profiles" / "roofline_traffic.json"
-    if tf.exists():
-        t = json.loads(tf.read_text()).get(w.tune_key)
-        if t and t.get("kernel") == w.kernel and t.get("dram_bytes_per_thread"):
-            traffic = int(t["dram_bytes_per_thread"] * w.n)
-        # the engine's own bound: warp instructions issued per second against
-        # one per cycle on each of the 148 x 4 SM sub-partitions, at the SM
-        # clock sampled during the timed region; SASS warp instructions per
-        # thread come from an ncu capture of the same tuned options
-        if t and t.get("kernel") == w.kernel and t.get("sass_options") == w.opts:
-            mhz = clk.summary().get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
-            inst = t["sass_warp_inst_per_thread"] * w.n
-            got = inst / (kern_ms / 1e3) / 1e9
-            top = 148 * 4 * mhz / 1e3
-            issue = {
-                "achieved": round(got, 1),
-                "peak": round(top, 1),
-                "unit": "G warp instructions/s",
-                "frac": round(got / top, 4),
-                "sass_warp_inst_per_thread": t["sass_warp_inst_per_thread"],
-            }
+    traffic, issue = ncu_rooflines(
+        w, kern_ms, clk.summary().get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    )
 
     cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
     plain_regroup_same = same_bits(res["plain"]["out"], out_r)

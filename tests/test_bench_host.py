@@ -89,3 +89,33 @@ def test_reference_runner_without_gpu():
     (steps,) = run("collatz_u64", [x], None)
     assert list(steps) == [0, 1, 7, 8, 16, 111]
     assert kind in ("reference", "port") and cores >= 1
+
+
+def test_issue_roofline_of_the_committed_capture():
+    """The headline bench line's issue roofline: the committed capture's
+    SASS warp instructions per path, scaled to the full launch, over the
+    kernel time, against 148 SMs x 4 schedulers at the sampled clock; only
+    for the options the capture was taken with."""
+    w = bench.make_workload("pt")
+    w.opts = bench.regroup_opts(w.kernel, w.tune_key)
+    traffic, issue = bench.ncu_rooflines(w, 41.47, 1965.0)
+    assert issue is not None
+    per = issue["sass_warp_inst_per_thread"]
+    want = per * w.n / 41.47e-3 / 1e9
+    assert issue["achieved"] == pytest.approx(want, rel=1e-3)
+    assert issue["peak"] == pytest.approx(148 * 4 * 1.965, abs=0.05)
+    assert 0 < issue["frac"] < 1
+    # another option set: no issue figure from a capture of different code
+    w.opts = dict(w.opts, schedule=0)
+    assert bench.ncu_rooflines(w, 41.47, 1965.0)[1] is None
+
+
+def test_rooflines_without_a_capture(tmp_path):
+    w = bench.make_workload("collatz")
+    w.opts = bench.regroup_opts(w.kernel, w.tune_key)
+    assert bench.ncu_rooflines(w, 3.6, 1965.0) == (None, None)
+    assert bench.ncu_rooflines(w, 3.6, 1965.0, path=tmp_path / "none.json") == (None, None)
+    f = tmp_path / "t.json"
+    f.write_text('{"default": {"kernel": "collatz_u64", "dram_bytes_per_thread": 12.5}}')
+    traffic, issue = bench.ncu_rooflines(w, 3.6, 1965.0, path=f)
+    assert traffic == int(12.5 * w.n) and issue is None
