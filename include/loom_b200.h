@@ -104,7 +104,9 @@ typedef struct loom_b200_opts
                              and replay it while the launch arguments stay
                              the same */
     uint64_t population;  /* regroup: resident thread slots; 0 = all inputs */
-    uint64_t max_steps;   /* per-thread block-step guard; 0 = 2^40 */
+    uint64_t max_steps;   /* plain: per-thread block-step guard; regroup:
+                             rounds of the megakernel (a tile runs at most
+                             `period` block steps per round); 0 = 2^40 */
     uint32_t profile;     /* collect lane-efficiency counters (slower) */
     uint32_t no_prefetch; /* regroup: do not prefetch each lane's next input */
     uint32_t ctas_per_sm; /* regroup: resident CTAs per SM; 0 = occupancy max */
@@ -362,13 +364,29 @@ int loom_b200_server_create(const char*                 kernel,
                             loom_b200_server**          out);
 int loom_b200_server_destroy(loom_b200_server* s);
 /* Queues a request; its host arrays must stay valid until its ticket comes
- * back from loom_b200_server_step.  LOOM_B200_ERR_BUDGET: larger than the
- * ring or the arena. */
+ * back from loom_b200_server_step (or from loom_b200_server_failed).
+ * LOOM_B200_ERR_BUDGET: larger than the ring or the arena. */
 int loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_t* ticket);
 /* Admits what fits, runs one slice, copies out the requests that finished
  * and returns up to max_done of their tickets (the rest on later calls). */
 int loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, uint32_t* n_done);
 int loom_b200_server_get_stats(const loom_b200_server* s, loom_b200_server_stats* st);
+/* Cancels a request (no counterpart in Loom, whose streams have no request
+ * boundary).  A queued request leaves the queue at once.  The threads of a
+ * request in flight cannot be taken back from the device: they run to their
+ * end, and the request is dropped then (its outputs are not written and its
+ * ticket never comes back from loom_b200_server_step).  Either way the
+ * ticket comes back once from loom_b200_server_failed with
+ * LOOM_B200_ERR_CANCELLED, after which its host arrays are no longer used.
+ * LOOM_B200_ERR_INVALID: the ticket is not pending or was cancelled already. */
+int loom_b200_server_cancel(loom_b200_server* s, uint64_t ticket);
+/* Host-side watchdog: at each loom_b200_server_step, a request submitted
+ * more than timeout_us microseconds earlier and not completed is cancelled
+ * as above, with LOOM_B200_ERR_TIMEOUT (0, the default: off). */
+int loom_b200_server_set_timeout(loom_b200_server* s, uint64_t timeout_us);
+/* Hands out up to max tickets of cancelled or timed-out requests, oldest
+ * first, with their LOOM_B200_ERR_* code (either array may be NULL). */
+int loom_b200_server_failed(loom_b200_server* s, uint64_t* tickets, int32_t* codes, uint32_t max, uint32_t* n);
 
 /* ------------------------------------------------------------ no allocation
  * No counterpart in the reference: Loom's backends allocate their device

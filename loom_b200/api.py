@@ -255,6 +255,9 @@ EXPORTS = [
     "loom_b200_server_submit",
     "loom_b200_server_step",
     "loom_b200_server_get_stats",
+    "loom_b200_server_cancel",
+    "loom_b200_server_set_timeout",
+    "loom_b200_server_failed",
 ]
 
 
@@ -329,6 +332,15 @@ def lib() -> ctypes.CDLL:
         ctypes.POINTER(ctypes.c_uint32),
     ]
     L.loom_b200_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStatsC)]
+    L.loom_b200_server_cancel.argtypes = [vp, ctypes.c_uint64]
+    L.loom_b200_server_set_timeout.argtypes = [vp, ctypes.c_uint64]
+    L.loom_b200_server_failed.argtypes = [
+        vp,
+        ctypes.POINTER(ctypes.c_uint64),
+        ctypes.POINTER(ctypes.c_int32),
+        ctypes.c_uint32,
+        ctypes.POINTER(ctypes.c_uint32),
+    ]
     L.loom_b200_launch_static.argtypes = [
         ctypes.c_char_p,
         ctypes.POINTER(LaunchC),
@@ -740,6 +752,32 @@ class Server:
         """Outputs of a completed request (and forgets it)."""
         outs = self._live.pop(ticket)[1]
         return outs[0] if len(outs) == 1 else tuple(outs)
+
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a request (``loom_b200_server_cancel``): a queued one at
+        once, one in flight when its threads have finished.  False when the
+        ticket is not pending."""
+        return lib().loom_b200_server_cancel(self._h, ticket) == OK
+
+    def set_timeout(self, seconds: float) -> None:
+        """Host-side watchdog: requests not completed `seconds` after their
+        submission are cancelled with ERR_TIMEOUT (0: off)."""
+        check(lib().loom_b200_server_set_timeout(self._h, int(round(seconds * 1e6))))
+
+    def failed(self) -> List[tuple]:
+        """(ticket, code) of the requests cancelled or timed out since the
+        last call; their arrays are released."""
+        out = []
+        t = (ctypes.c_uint64 * 64)()
+        c = (ctypes.c_int32 * 64)()
+        k = ctypes.c_uint32()
+        while True:
+            check(lib().loom_b200_server_failed(self._h, t, c, 64, ctypes.byref(k)))
+            for i in range(k.value):
+                out.append((t[i], c[i]))
+                self._live.pop(t[i], None)
+            if k.value < 64:
+                return out
 
     def stats(self) -> Dict[str, int]:
         st = ServerStatsC()

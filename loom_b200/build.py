@@ -177,6 +177,7 @@ def generate() -> List[str]:
 def _headers() -> List[pathlib.Path]:
     return list((CSRC / "engine").glob("*.cuh")) + [
         CSRC / "runtime_iface.h",
+        CSRC / "request_book.hpp",
         INCLUDE / "loom_b200.h",
     ]
 

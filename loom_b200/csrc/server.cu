@@ -18,7 +18,10 @@
 //    flight, and they share warps whenever they stand at the same block;
 //  * after each slice the per-instance completion counters come back; a
 //    request whose threads all finished has its outputs copied to the host
-//    and frees its slot, ring range and table space.
+//    and frees its slot, ring range and table space;
+//  * the caller can cancel a request, and a host-side watchdog cancels the
+//    requests older than a timeout (request_book.hpp); a cancelled request
+//    in flight is dropped once its threads have finished.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,6 +32,7 @@
 #include <new>
 #include <vector>
 
+#include "request_book.hpp"
 #include "runtime_iface.h"
 
 using namespace loom_b200;
@@ -117,6 +121,8 @@ struct Request
     std::vector<uint32_t> header;
     const uint32_t*       body       = nullptr;
     uint64_t              body_words = 0;
+    SteadyClock::time_point born{}; // submission time, for the watchdog
+    int                     fail = 0; // LOOM_B200_ERR_* once cancelled
     // in flight
     uint32_t slot     = 0;
     uint64_t vstart   = 0;
@@ -223,6 +229,8 @@ struct loom_b200_server
     std::vector<unsigned long long> h_starts;
     std::vector<unsigned>   h_ids;
     std::deque<uint64_t>    done_q; // completed tickets not handed out yet
+    std::deque<Failure>     failed_q; // cancelled tickets not handed out yet
+    uint64_t                timeout_us = 0; // watchdog (0: off)
     uint64_t                vnext      = 0;
     uint64_t                next_round = 0;
     uint64_t                ticket     = 0;
@@ -492,6 +500,7 @@ loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_
     Request q;
     q.ticket = ++s->ticket;
     q.n      = r->n;
+    q.born   = SteadyClock::now();
     q.inputs.assign(info.num_inputs, nullptr);
     for(uint32_t i = 0; i < info.num_inputs; ++i)
         if(s->forms[i] == LOOM_B200_IN_ARRAY)
@@ -610,6 +619,15 @@ run_slice(loom_b200_server* s)
             keep.push_back(std::move(r));
             continue;
         }
+        if(r.fail)
+        {
+            // cancelled in flight: its threads have finished, so its slot,
+            // ring range and arena words are free; nothing is copied out
+            s->arena.release(r.arena_at, r.body_words);
+            s->free_slots.push_back(r.slot);
+            s->failed_q.push_back({r.ticket, r.fail});
+            continue;
+        }
         const uint64_t pos = r.vstart & s->mask;
         for(uint32_t j = 0; j < info.num_outputs; ++j)
         {
@@ -635,6 +653,8 @@ loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, ui
 {
     if(!s) return LOOM_B200_ERR_INVALID;
     if(n_done) *n_done = 0;
+    expire_requests(s->queued, s->flight, SteadyClock::now(), s->timeout_us, LOOM_B200_ERR_TIMEOUT,
+                    s->failed_q);
     const int rc = run_slice(s);
     uint32_t  k  = 0;
     while(done && k < max_done && !s->done_q.empty())
@@ -644,6 +664,31 @@ loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, ui
     }
     if(n_done) *n_done = k;
     return rc;
+}
+
+int
+loom_b200_server_cancel(loom_b200_server* s, uint64_t ticket)
+{
+    if(!s) return LOOM_B200_ERR_INVALID;
+    return cancel_request(s->queued, s->flight, ticket, LOOM_B200_ERR_CANCELLED, s->failed_q)
+               ? LOOM_B200_OK
+               : LOOM_B200_ERR_INVALID;
+}
+
+int
+loom_b200_server_set_timeout(loom_b200_server* s, uint64_t timeout_us)
+{
+    if(!s) return LOOM_B200_ERR_INVALID;
+    s->timeout_us = timeout_us;
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_server_failed(loom_b200_server* s, uint64_t* tickets, int32_t* codes, uint32_t max, uint32_t* n)
+{
+    if(!s || !n) return LOOM_B200_ERR_INVALID;
+    *n = drain_failures(s->failed_q, tickets, codes, max);
+    return LOOM_B200_OK;
 }
 
 int

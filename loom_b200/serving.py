@@ -4,7 +4,9 @@
 Each ``step`` gives every server that has work one slice of its
 regrouping megakernel; a request admitted by a server joins the threads of
 that server's requests in flight.  Completions come back as
-``(kind, ticket)`` pairs; ``result`` hands out the outputs.
+``(kind, ticket)`` pairs; ``result`` hands out the outputs.  Requests
+cancelled by ``cancel`` or by a server's watchdog (``timeout``) come back
+from ``failures`` as ``(kind, ticket, code)``.
 """
 
 from __future__ import annotations
@@ -15,9 +17,13 @@ from . import api
 
 
 class Pool:
-    def __init__(self, servers: Dict[str, api.Server]):
+    def __init__(self, servers: Dict[str, api.Server], timeout: float = 0.0):
         self.servers = dict(servers)
         self._work = {k: 0 for k in self.servers}  # submitted, not completed
+        self._failed: List[Tuple[str, int, int]] = []
+        if timeout:
+            for srv in self.servers.values():
+                srv.set_timeout(timeout)
 
     def submit(self, kind: str, n: int, **request) -> Tuple[str, int]:
         t = self.servers[kind].submit(n, **request)
@@ -34,7 +40,24 @@ class Pool:
                 for t in srv.step():
                     done.append((k, t))
                     self._work[k] -= 1
+                self._collect(k, srv)
         return done
+
+    def cancel(self, kind: str, ticket: int) -> bool:
+        ok = self.servers[kind].cancel(ticket)
+        self._collect(kind, self.servers[kind])
+        return ok
+
+    def failures(self) -> List[Tuple[str, int, int]]:
+        """(kind, ticket, code) of the requests that ended without
+        completing since the last call."""
+        out, self._failed = self._failed, []
+        return out
+
+    def _collect(self, kind: str, srv: api.Server) -> None:
+        for t, code in srv.failed():
+            self._failed.append((kind, t, code))
+            self._work[kind] -= 1
 
     def result(self, kind: str, ticket: int):
         return self.servers[kind].result(ticket)
