@@ -1,8 +1,8 @@
 """Oracle: CPU restatements of Loom's scalar semantics.
 
 TEST AND BASELINE INFRASTRUCTURE ONLY.  tests/, __graft_entry__.smoke() and
-bench.py's cpu_baseline leg use this module as the checker; the product
-(loom_b200) never imports it.
+bench.py's cpu_baseline leg use this module to check results against; the
+product (loom_b200) never imports it.
 
 Three layers, each pinned against the next:
   * ``Interp``  — oracle/loom_interp.c, a plain-C restatement of vm::bse
@@ -297,7 +297,7 @@ def uniform_int(seed: int, n: int, lo: int, hi: int) -> np.ndarray:
 def expand_inputs(forms, n: int, instance_starts=None, types=None):
     """Materialises input columns given as arrays or the engine's input forms
     ("iota", "local_iota", "instance", ("broadcast", value)) so the CPU
-    checkers see exactly what the device threads read."""
+    references see exactly what the device threads read."""
     starts = None if instance_starts is None else np.asarray(instance_starts, dtype=np.uint64)
     tid = np.arange(n, dtype=np.uint64)
     inst = (

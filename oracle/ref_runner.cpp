@@ -3,8 +3,9 @@
 //
 // TEST AND BASELINE INFRASTRUCTURE ONLY.  Compiled from the Loom headers
 // where they lie (oracle/build_ref.py); the resulting oracle/_ref/
-// libloomref.so is the checker for golden fixtures and the timed CPU
-// reference arm of bench.py.  Nothing in the product links it.
+// libloomref.so writes the golden fixtures, checks results in the tests and
+// is the timed CPU reference arm of bench.py.  Nothing in the product links
+// it.
 //
 // C ABI:
 //   int loom_ref_run(const char* kernel, const void* const* inputs,
