@@ -13,6 +13,8 @@ extern const loom_b200::KernelEntry loom_b200_entry_bit_xor_u16;
 extern const loom_b200::KernelEntry loom_b200_entry_bool_and_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_bool_not_u8;
 extern const loom_b200::KernelEntry loom_b200_entry_bool_or_u64;
+extern const loom_b200::KernelEntry loom_b200_entry_bump_u32;
+extern const loom_b200::KernelEntry loom_b200_entry_canonical_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_ceilfloor_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_collatz_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_fac_u32;
@@ -37,6 +39,7 @@ extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_40;
 extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_512;
 extern const loom_b200::KernelEntry loom_b200_entry_pt_const_40;
 extern const loom_b200::KernelEntry loom_b200_entry_pt_const_512;
+extern const loom_b200::KernelEntry loom_b200_entry_rotl32_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u16;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_rshift_u64;
@@ -46,6 +49,7 @@ extern const loom_b200::KernelEntry loom_b200_entry_sin_cos_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_slt_inv_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_sphere_pt_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_sqrt_f32;
+extern const loom_b200::KernelEntry loom_b200_entry_threefry_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_trunc_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_union_cmov_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_union_cmov_f64;
@@ -65,6 +69,8 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_bool_and_u32,
     &loom_b200_entry_bool_not_u8,
     &loom_b200_entry_bool_or_u64,
+    &loom_b200_entry_bump_u32,
+    &loom_b200_entry_canonical_f32,
     &loom_b200_entry_ceilfloor_f32,
     &loom_b200_entry_collatz_u64,
     &loom_b200_entry_fac_u32,
@@ -89,6 +95,7 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_pt2_const_512,
     &loom_b200_entry_pt_const_40,
     &loom_b200_entry_pt_const_512,
+    &loom_b200_entry_rotl32_u32,
     &loom_b200_entry_rshift_u16,
     &loom_b200_entry_rshift_u32,
     &loom_b200_entry_rshift_u64,
@@ -98,11 +105,12 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_slt_inv_u32,
     &loom_b200_entry_sphere_pt_f32,
     &loom_b200_entry_sqrt_f32,
+    &loom_b200_entry_threefry_u32,
     &loom_b200_entry_trunc_f32,
     &loom_b200_entry_union_cmov_f32,
     &loom_b200_entry_union_cmov_f64,
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 49;
+const int kRegistrySize = 53;
 } // namespace loom_b200

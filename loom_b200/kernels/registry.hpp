@@ -17,6 +17,7 @@
 #include <tests/programs.hpp>
 
 #include "collatz.hpp"
+#include "rng_tests.hpp"
 #include "sphere_pt.hpp"
 
 #include <cstdint>
@@ -53,6 +54,11 @@ using std::uint8_t;
     /* 64 samples per pixel, blur 1 and 20 (CMakeLists.txt:420)          */    \
     X(primary_const_256,  loom::vm::primary_const<float, loom::vm::constants<CS(256), CS(0.1), CS(64), CS(1)>>) \
     X(primary_const_b20_256, loom::vm::primary_const<float, loom::vm::constants<CS(256), CS(0.1), CS(64), CS(20)>>) \
+    /* the path tracers' RNG macros, one kernel each (rng_tests.hpp)   */    \
+    X(rotl32_u32,         loom::vm::b200::kernels::rotl32_k)                   \
+    X(threefry_u32,       loom::vm::b200::kernels::threefry_k)                 \
+    X(canonical_f32,      loom::vm::b200::kernels::canonical_k<float>)         \
+    X(bump_u32,           loom::vm::b200::kernels::bump_k)                     \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

@@ -63,6 +63,10 @@ def inputs_for(name: str, n: int, seed: int, input_types: List[str]) -> List[np.
             side = int(name.rsplit("_", 1)[1])
             xy = _ints(s, n, 0, side * side - 1, np.uint32)
             a = (((xy % side) << 16) | (xy // side)).astype(dt)
+        elif name.startswith("rotl32") and j == 1:
+            # rotation counts as Loom's RNG test draws them
+            # (src/tests/vm_smallpt.cpp:353)
+            a = _ints(s, n, 0, 31, dt)
         elif name.startswith(("lshift", "rshift")):
             a = _ints(s, n, 2, 10, dt)
         elif name.startswith("bool"):

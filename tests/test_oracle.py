@@ -6,6 +6,8 @@ reproduce every one of them bit for bit, and the numpy restatements of Loom's
 validators (src/tests/programs.hpp:290-389) must agree with both.
 """
 
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -39,10 +41,9 @@ def test_interp_matches_golden(name, golden, golden_extra):
 
 
 def test_golden_fixture_for_every_kernel():
-    import pathlib
-
     d = pathlib.Path(__file__).parent / "golden"
-    assert {p.stem for p in d.glob("*.npz")} == set(KERNELS)
+    # rng_kat.npz holds known answers beside the RNG kernels' fixtures
+    assert {p.stem for p in d.glob("*.npz")} - {"rng_kat"} == set(KERNELS)
 
 
 def test_val_fib_matches_golden(golden):
@@ -114,3 +115,22 @@ def test_workload_inputs_match_the_oracle_stream():
 
     for seed, n, lo, hi in ((1, 1000, 1, (1 << 32) - 1), (5, 777, 0, 93), (9, 100, 3, (1 << 63) + 5)):
         assert np.array_equal(I.uniform_int(seed, n, lo, hi), O.uniform_int(seed, n, lo, hi))
+
+
+RNG_KERNELS = {"rotl32_u32": 1, "threefry_u32": 2, "canonical_f32": 1, "bump_u32": 2}
+
+
+@pytest.mark.parametrize("name", sorted(RNG_KERNELS))
+def test_rng_macros_match_loom_cpp_functions(name, golden):
+    """The RNG macros of the path tracers (one kernel each) give the known
+    answers of Loom's plain C++ functions (src/common/random.hpp: rotl32,
+    threefry2x32r32<0xdead, 0xbeef>, gen_canonical, bump_ctr) on the
+    fixture's inputs, in Loom's scalar backend (the golden outputs) and in
+    the C restatement; tests/golden/make_rng_kat.py wrote the answers."""
+    kat = np.load(pathlib.Path(__file__).resolve().parent / "golden" / "rng_kat.npz")
+    ins, outs = golden(name)
+    got = O.Interp(name).run(ins)
+    for j in range(RNG_KERNELS[name]):
+        want = kat[f"{name}_out{j}"]
+        assert np.array_equal(np.ascontiguousarray(outs[j]).view(np.uint32), want), f"{name} golden out{j}"
+        assert np.array_equal(np.ascontiguousarray(got[j]).view(np.uint32), want), f"{name} interp out{j}"
