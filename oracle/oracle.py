@@ -268,6 +268,48 @@ def val_jmp4(i: np.ndarray) -> np.ndarray:
     return np.array([table.get(int(v), int(v)) for v in i], dtype=i.dtype)
 
 
+def val_inc(i: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:292-297: i + 1 in the integer type."""
+    i = np.asarray(i)
+    with np.errstate(over="ignore"):
+        return (i + i.dtype.type(1)).astype(i.dtype)
+
+
+def _uint_of(a: np.ndarray):
+    return np.dtype(f"u{np.asarray(a).dtype.itemsize}")
+
+
+def val_union1(i: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:307-313: the value converted to the
+    unsigned integer of the float's size (truncation toward zero)."""
+    i = np.asarray(i)
+    return np.trunc(i).astype(_uint_of(i))
+
+
+def val_union2(i: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:315-322: 200 below 0.5, else 100."""
+    i = np.asarray(i)
+    return np.where(i < i.dtype.type(0.5), 200, 100).astype(_uint_of(i))
+
+
+def val_lshift(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:339-344: a << b, kept to the type."""
+    a = np.asarray(a)
+    return np.left_shift(a, np.asarray(b).astype(a.dtype)).astype(a.dtype)
+
+
+def val_rshift(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:346-351: a >> b."""
+    a = np.asarray(a)
+    return np.right_shift(a, np.asarray(b).astype(a.dtype)).astype(a.dtype)
+
+
+def val_bit_not(v: np.ndarray) -> np.ndarray:
+    """Loom src/tests/programs.hpp:373-378: ~v."""
+    v = np.asarray(v)
+    return np.invert(v).astype(v.dtype)
+
+
 # ---------------------------------------------------------------- inputs
 def splitmix64(seed: int, n: int) -> np.ndarray:
     """SplitMix64 stream (Steele, Lea, Flood 2014), the documented PRNG of all

@@ -68,6 +68,41 @@ def test_val_fac_and_jmp4(golden):
     assert np.array_equal(O.val_jmp4(i), j)
 
 
+def _logical(f):
+    return lambda *a: f(*[np.asarray(x) != 0 for x in a]).astype(np.asarray(a[0]).dtype)
+
+
+# the validator of each Loom test program, as Loom's test pairs them
+# (src/tests/vm.cpp:277-327: val_* of programs.hpp:290-389 and std functors)
+VALIDATORS = {
+    "increment": O.val_inc,
+    "union_cmov": O.val_union2,
+    "union": O.val_union1,
+    "bit_and": np.bitwise_and,
+    "bit_or": np.bitwise_or,
+    "bit_xor": np.bitwise_xor,
+    "bit_not": O.val_bit_not,
+    "bool_and": _logical(np.logical_and),
+    "bool_or": _logical(np.logical_or),
+    "bool_not": _logical(np.logical_not),
+    "lshift": O.val_lshift,
+    "rshift": O.val_rshift,
+}
+
+
+@pytest.mark.parametrize(
+    "name", [k for k in KERNELS if any(k.startswith(p + "_") for p in VALIDATORS)]
+)
+def test_loom_validators_match_golden(name, golden):
+    """Loom's own validators agree with bse's outputs in every fixture of
+    the test programs they cover."""
+    prefix = next(p for p in VALIDATORS if name.startswith(p + "_"))
+    ins, (out,) = golden(name)
+    want = VALIDATORS[prefix](*ins)
+    assert want.dtype == out.dtype, (want.dtype, out.dtype)
+    assert np.array_equal(want, out), name
+
+
 def test_interp_out_of_table_parmjump_halts():
     # jmp4: values outside the 4-entry table leave the thread unchanged,
     # like bse's switch without a matching case (bse.hpp:192-198)
