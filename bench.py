@@ -616,6 +616,74 @@ METRIC = (
     "efficiency beside it"
 )
 
+# Loom's benchmarks append one CSV row per run (date, repo hash, compiler,
+# fast-math, CPU model, SIMD ISA, benchmark id, seconds;
+# src/benchmarks/bm.hpp:103-139); `--csv PATH` appends the same kind of row,
+# extended with the GPU figures of the bench line.
+CSV_FIELDS = [
+    "date", "repo_hash", "compiler", "device", "impl", "workload", "kernel", "n_gpus", "ms_per_step",
+    "msamples_s", "plain_msamples_s", "lane_efficiency", "state_gbs", "issue_frac", "p50_ms", "p99_ms",
+]
+
+
+def csv_row(line: dict, device: str = "", compiler: str = "", repo_hash: str = "") -> dict:
+    """The CSV row of a bench line (missing figures left empty)."""
+    import datetime
+
+    rg = line.get("regroup") or {}
+    roof = line.get("roofline") or {}
+    issue = line.get("issue_roofline") or {}
+    cfg = line.get("config") or {}
+    return {
+        "date": datetime.datetime.now(datetime.timezone.utc).strftime("%Y-%m-%dT%H:%M:%SZ"),
+        "repo_hash": repo_hash,
+        "compiler": compiler,
+        "device": device,
+        "impl": line.get("impl", "b200"),
+        "workload": cfg.get("workload", ""),
+        "kernel": cfg.get("kernel", ""),
+        "n_gpus": line.get("n_gpus", ""),
+        "ms_per_step": line.get("ms_per_step", ""),
+        "msamples_s": line.get("value", ""),
+        "plain_msamples_s": (line.get("plain") or {}).get("value", ""),
+        "lane_efficiency": rg.get("lane_efficiency", ""),
+        "state_gbs": roof.get("achieved", ""),
+        "issue_frac": issue.get("frac", ""),
+        "p50_ms": line.get("p50_ms", ""),
+        "p99_ms": line.get("p99_ms", ""),
+    }
+
+
+def append_csv(path: str, line: dict) -> None:
+    """Appends the row of `line` to the CSV file at `path` (header first
+    when the file is new)."""
+    import csv
+    import subprocess
+
+    def out(cmd):
+        try:
+            return subprocess.run(cmd, capture_output=True, text=True, timeout=10, cwd=ROOT).stdout.strip()
+        except Exception:
+            return ""
+
+    device = ""
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            device = torch.cuda.get_device_name(0)
+    except Exception:
+        pass
+    nv = out(["nvcc", "--version"]).splitlines()
+    row = csv_row(line, device, nv[-1] if nv else "", out(["git", "rev-parse", "--short", "HEAD"]))
+    f = pathlib.Path(path)
+    new = not f.exists() or f.stat().st_size == 0
+    with open(f, "a", newline="") as fh:
+        w = csv.DictWriter(fh, fieldnames=CSV_FIELDS)
+        if new:
+            w.writeheader()
+        w.writerow(row)
+
 
 # ---------------------------------------------------------------- serving
 SERVE_KERNELS = {"pt": "sphere_pt_f32", "collatz": "collatz_u64", "fib": "fib_u64"}
@@ -919,6 +987,8 @@ def serve_main(args, warmup, world, rank, local):
     )
     if rank == 0:
         print(json.dumps(line))
+        if args.csv:
+            append_csv(args.csv, line)
 
 
 def tune_main(args) -> None:
@@ -978,6 +1048,7 @@ def main() -> None:
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")
     ap.add_argument("--tune-budget", type=float, default=300.0, help="seconds of tuning")
+    ap.add_argument("--csv", metavar="PATH", help="append a CSV row of the result to PATH")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
 
@@ -1017,6 +1088,8 @@ def main() -> None:
         line["cpu_baseline"] = dict(info, value=round(value, 3))
         line["e2e"] = {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
         print(json.dumps(line))
+        if args.csv:
+            append_csv(args.csv, line)
         return
 
     import torch
@@ -1180,6 +1253,8 @@ def main() -> None:
         }
     )
     print(json.dumps(line))
+    if args.csv:
+        append_csv(args.csv, line)
     for r in res.values():
         r["fn"].close()
     if dist is not None:

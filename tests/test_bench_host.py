@@ -119,3 +119,29 @@ def test_rooflines_without_a_capture(tmp_path):
     f.write_text('{"default": {"kernel": "collatz_u64", "dram_bytes_per_thread": 12.5}}')
     traffic, issue = bench.ncu_rooflines(w, 3.6, 1965.0, path=f)
     assert traffic == int(12.5 * w.n) and issue is None
+
+
+def test_csv_rows_of_bench_lines(tmp_path):
+    """`--csv` appends one row per run, as Loom's benchmarks do
+    (src/benchmarks/bm.hpp:103-139), with the GPU figures of the line."""
+    import csv
+
+    line = {
+        "value": 1213.0, "ms_per_step": 41.49, "n_gpus": 1,
+        "plain": {"value": 346.9}, "regroup": {"lane_efficiency": 0.4156},
+        "roofline": {"achieved": 14.6}, "issue_roofline": {"frac": 0.7356},
+        "config": {"workload": "sphere path tracer", "kernel": "sphere_pt_f32"},
+    }
+    serve = {"value": 1406.2, "p50_ms": 27.4, "p99_ms": 104.2, "n_gpus": 1, "regroup": {"lane_efficiency": 0.85},
+             "config": {"workload": "serving", "kernel": "sphere_pt_f32+collatz_u64+fib_u64"}}
+    ref = {"impl": "reference", "value": 9.0, "ms_per_step": 5580.0, "n_gpus": 1, "config": {"workload": "w", "kernel": "k"}}
+    f = tmp_path / "runs.csv"
+    for ln in (line, serve, ref):
+        bench.append_csv(str(f), ln)
+    rows = list(csv.DictReader(open(f)))
+    assert [r["impl"] for r in rows] == ["b200", "b200", "reference"]
+    assert list(rows[0]) == bench.CSV_FIELDS
+    assert float(rows[0]["msamples_s"]) == 1213.0 and float(rows[0]["issue_frac"]) == 0.7356
+    assert float(rows[0]["plain_msamples_s"]) == 346.9 and float(rows[0]["state_gbs"]) == 14.6
+    assert float(rows[1]["p99_ms"]) == 104.2 and rows[1]["issue_frac"] == ""
+    assert rows[2]["lane_efficiency"] == "" and rows[0]["date"].endswith("Z")
