@@ -436,13 +436,19 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU leg
 def _cpu_model() -> str:
+    """CPU model and widest x86 vector ISA of the host (Loom reports both
+    beside its CPU timings: src/benchmarks/bm.hpp:39-69, simd.hpp:66-77)."""
+    model, flags = "unknown CPU", set()
     try:
         for ln in open("/proc/cpuinfo"):
-            if ln.startswith("model name"):
-                return ln.split(":", 1)[1].strip()
+            if ln.startswith("model name") and model == "unknown CPU":
+                model = ln.split(":", 1)[1].strip()
+            elif ln.startswith("flags") and not flags:
+                flags = set(ln.split(":", 1)[1].split())
     except Exception:
         pass
-    return "unknown CPU"
+    isa = next((name for flag, name in (("avx512f", "AVX-512"), ("avx2", "AVX2"), ("avx", "AVX")) if flag in flags), "")
+    return f"{model} ({isa})" if isa else model
 
 
 def _reference_runner():
