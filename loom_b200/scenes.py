@@ -154,13 +154,43 @@ def pixel_average(rgb: Sequence[np.ndarray], spp: int) -> np.ndarray:
     return np.stack(out, axis=1)
 
 
+def _to_8bit(img: np.ndarray, width: int, height: int) -> np.ndarray:
+    px = np.clip(img.reshape(height, width, 3), 0.0, 1.0) ** (1.0 / 2.2)
+    return (px * 255.0 + 0.5).astype(np.uint8)
+
+
+def to_ppm(img: np.ndarray, width: int, height: int, path: str) -> None:
+    """Writes a (height*width, 3) linear image as a binary 8-bit PPM (P6),
+    the format of Loom's demo output (src/smallpt/common/io.hpp:36-48), with
+    the same tone curve as `to_png`."""
+    data = _to_8bit(img, width, height)
+    with open(path, "wb") as fh:
+        fh.write(f"P6\n{width} {height}\n255\n".encode())
+        fh.write(data.tobytes())
+
+
+def to_pfm(img: np.ndarray, width: int, height: int, path: str) -> None:
+    """Writes a (height*width, 3) linear image as a little-endian colour PFM
+    (float32 radiance, unclamped; rows stored bottom to top as the format
+    defines)."""
+    data = np.ascontiguousarray(np.asarray(img, dtype="<f4").reshape(height, width, 3)[::-1])
+    with open(path, "wb") as fh:
+        fh.write(f"PF\n{width} {height}\n-1.0\n".encode())
+        fh.write(data.tobytes())
+
+
+def write_image(img: np.ndarray, width: int, height: int, path: str) -> None:
+    """PNG, PPM or PFM by the file's suffix."""
+    suffix = str(path).rsplit(".", 1)[-1].lower()
+    {"png": to_png, "ppm": to_ppm, "pfm": to_pfm}[suffix](img, width, height, path)
+
+
 def to_png(img: np.ndarray, width: int, height: int, path: str) -> None:
     """Writes a (height*width, 3) linear image as an 8-bit sRGB-ish PNG."""
     import struct
     import zlib
 
-    px = np.clip(img.reshape(height, width, 3), 0.0, 1.0) ** (1.0 / 2.2)
-    data = (px * 255.0 + 0.5).astype(np.uint8)
+    data = _to_8bit(img, width, height)
     raw = b"".join(b"\x00" + data[y].tobytes() for y in range(height))
 
     def chunk(tag: bytes, body: bytes) -> bytes:
