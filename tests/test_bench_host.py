@@ -145,3 +145,27 @@ def test_csv_rows_of_bench_lines(tmp_path):
     assert float(rows[0]["plain_msamples_s"]) == 346.9 and float(rows[0]["state_gbs"]) == 14.6
     assert float(rows[1]["p99_ms"]) == 104.2 and rows[1]["issue_frac"] == ""
     assert rows[2]["lane_efficiency"] == "" and rows[0]["date"].endswith("Z")
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    """The reference arm launched as the multi-GPU bench is launched (two
+    ranks under torch.distributed.run): rank 0 times Loom's CPU backend and
+    prints the only line; the other rank exits 0 without work."""
+    import json
+    import subprocess
+    import sys
+
+    root = bench.ROOT
+    cmd = [
+        sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+        "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+        str(root / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3",
+        "--workload", "collatz",
+    ]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] in ("reference", "port")
