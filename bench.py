@@ -391,11 +391,18 @@ class ClockSampler:
                     f"--query-gpu={self.FIELDS}",
                     "--format=csv,noheader,nounits",
                     "-lms",
-                    "200",
+                    "50",
                 ],
                 stdout=self.f,
                 stderr=subprocess.DEVNULL,
             )
+            # the timed region starts once the first sample is in (nvidia-smi
+            # takes a moment to come up), at most two seconds from now
+            t_end = time.monotonic() + 2.0
+            while time.monotonic() < t_end and self.proc.poll() is None:
+                if self.path.stat().st_size > 0:
+                    break
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
@@ -1046,7 +1053,7 @@ def tune_main(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "loom_primary", "loom_primary_b20", "serve"])
