@@ -1,0 +1,240 @@
+// Generated by loom_b200.codegen from loom_b200/ir/cross_f32.lir.
+// Kernel IR digest 8849fa3651fb3de1; regenerate instead of editing.
+#include "../engine/plain.cuh"
+#include "../engine/regroup.cuh"
+#include "../runtime_iface.h"
+
+namespace loom_b200 { namespace k_cross_f32 {
+
+__constant__ unsigned kInstrTab[1] = {6};
+__constant__ unsigned kLiveTab[1] = {24};
+__constant__ int kQueueBlock[1] = {0};
+__constant__ unsigned kQuorumTab[1] = {0};
+__constant__ unsigned kRankTab[1] = {0};
+
+struct K
+{
+    static constexpr int kNumBlocks = 1;
+    static constexpr int kNumQueues = 1;
+    static constexpr int kRegroupMaxRegs = 64;
+    struct Regs
+    {
+        float r0; // x0: f32
+        float r1; // x1: f32
+        float r2; // x2: f32
+        float r3; // y0: f32
+        float r4; // y1: f32
+        float r5; // y2: f32
+        float r6; // z0: f32
+        float r7; // z1: f32
+        float r8; // z2: f32
+        float r9; // t1: f32
+    };
+
+    struct In
+    {
+        float v0; // x0
+        float v1; // x1
+        float v2; // x2
+        float v3; // y0
+        float v4; // y1
+        float v5; // y2
+    };
+
+    // Reads the input columns of thread `tid` (a NULL column is iota).
+    __device__ __forceinline__ static void
+    load_in(In& in, const Columns& c, const unsigned long long tid)
+    {
+        in.v0 = load_input<float>(c, 0, tid);
+        in.v1 = load_input<float>(c, 1, tid);
+        in.v2 = load_input<float>(c, 2, tid);
+        in.v3 = load_input<float>(c, 3, tid);
+        in.v4 = load_input<float>(c, 4, tid);
+        in.v5 = load_input<float>(c, 5, tid);
+        (void)in; (void)c; (void)tid;
+    }
+
+    // Loom's set_inputs: input variables written, every other register zero.
+    // Only registers live at START (those its queue carries) are written:
+    // the others are written before they are read on every path.
+    __device__ __forceinline__ static void
+    start(Regs& R, const In& in)
+    {
+        R.r0 = static_cast<float>(in.v0);
+        R.r1 = static_cast<float>(in.v1);
+        R.r2 = static_cast<float>(in.v2);
+        R.r3 = static_cast<float>(in.v3);
+        R.r4 = static_cast<float>(in.v4);
+        R.r5 = static_cast<float>(in.v5);
+        (void)in;
+    }
+
+    __device__ __forceinline__ static void
+    load_inputs(Regs& R, const Columns& c, const unsigned long long tid)
+    {
+        In in;
+        load_in(in, c, tid);
+        start(R, in);
+    }
+
+    __device__ __forceinline__ static void
+    store_outputs(const Regs& R, const Columns& c, const unsigned long long tid)
+    {
+        static_cast<float*>(c.p[6])[col_index(c, tid)] = R.r6; // z0
+        static_cast<float*>(c.p[7])[col_index(c, tid)] = R.r7; // z1
+        static_cast<float*>(c.p[8])[col_index(c, tid)] = R.r8; // z2
+    }
+
+    __device__ __forceinline__ static unsigned instr(const int b) { return kInstrTab[b]; }
+    __device__ __forceinline__ static unsigned live_bytes(const int q) { return kLiveTab[q]; }
+    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
+    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
+    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
+
+    static constexpr int kMaxQueuesPerBlock = 1;
+    // j-th queue holding threads that stand at block b (-1: none).
+    __device__ __forceinline__ static int
+    queue_list(const int b, const int j)
+    {
+        return j == 0 ? b : -1;
+    }
+
+    // Queue a thread standing at block pc waits in: the block's own queue,
+    // or for a dispatch block the queue of the context its register selects.
+    __device__ __forceinline__ static int
+    queue_of(const int pc, const Regs& R)
+    {
+        (void)R;
+        return pc;
+    }
+
+    // Runs the lane's own path from block `entry` for at most `budget`
+    // loop iterations (visits of a loop header); returns the block it
+    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
+    // above zero is entered only as the first block of the burst, when
+    // the warp's vote chose it.
+    template <bool kProf>
+    __device__ __forceinline__ static int
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    {
+        (void)ctx;
+        (void)stop_heavy;
+        bool fresh = true; // no block run yet in this burst
+        (void)fresh;
+        switch(entry)
+        {
+        case 0: goto L_B0;
+        default: return kHalt;
+        }
+    L_B0: // START
+        if constexpr(kProf) count_block(ctx, 0, 6u);
+        R.r9 = static_cast<float>(static_cast<float>(static_cast<float>(R.r2) * static_cast<float>(R.r4)));
+        R.r6 = static_cast<float>(op_fma(R.r1, R.r5, (-(R.r9))));
+        R.r9 = static_cast<float>(static_cast<float>(static_cast<float>(R.r0) * static_cast<float>(R.r5)));
+        R.r7 = static_cast<float>(op_fma(R.r2, R.r3, (-(R.r9))));
+        R.r9 = static_cast<float>(static_cast<float>(static_cast<float>(R.r1) * static_cast<float>(R.r3)));
+        R.r8 = static_cast<float>(op_fma(R.r0, R.r4, (-(R.r9))));
+        goto L_HALT;
+    L_HALT:
+        return kHalt;
+    }
+
+    static constexpr unsigned long long kRowBytes = 32ull;
+    __device__ __forceinline__ static void
+    save(const int q, const Regs& R, char* st, const unsigned cap, const unsigned par,
+         const unsigned idx, const unsigned tid)
+    {
+        char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
+        switch(q)
+        {
+        case 0: // START
+            reinterpret_cast<float*>(base + 0ull * cap)[idx] = R.r0;
+            reinterpret_cast<float*>(base + 4ull * cap)[idx] = R.r1;
+            reinterpret_cast<float*>(base + 8ull * cap)[idx] = R.r2;
+            reinterpret_cast<float*>(base + 12ull * cap)[idx] = R.r3;
+            reinterpret_cast<float*>(base + 16ull * cap)[idx] = R.r4;
+            reinterpret_cast<float*>(base + 20ull * cap)[idx] = R.r5;
+            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+            return;
+        default: return;
+        }
+    }
+
+    __device__ __forceinline__ static unsigned
+    restore(const int q, Regs& R, const char* st, const unsigned cap, const unsigned par,
+            const unsigned idx)
+    {
+        const char* base = st + static_cast<unsigned long long>(par) * kRowBytes * cap;
+        switch(q)
+        {
+        case 0: // START
+            R.r0 = reinterpret_cast<const float*>(base + 0ull * cap)[idx];
+            R.r1 = reinterpret_cast<const float*>(base + 4ull * cap)[idx];
+            R.r2 = reinterpret_cast<const float*>(base + 8ull * cap)[idx];
+            R.r3 = reinterpret_cast<const float*>(base + 12ull * cap)[idx];
+            R.r4 = reinterpret_cast<const float*>(base + 16ull * cap)[idx];
+            R.r5 = reinterpret_cast<const float*>(base + 20ull * cap)[idx];
+            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        default: return 0xffffffffu;
+        }
+    }
+
+};
+
+const int kInTypes[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const int kOutTypes[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kInNames[] = {"x0", "x1", "x2", "y0", "y1", "y2"};
+const char* const kOutNames[] = {"z0", "z1", "z2"};
+const uint32_t kInstrs[] = {6};
+const uint32_t kLive[] = {24};
+
+const loom_b200_kernel_info kInfo = {
+    "cross_f32", "8849fa3651fb3de1", 6u, 3u, kInTypes, kOutTypes, kInNames, kOutNames,
+    1u, 10u, 40u, 6u, kInstrs, kLive};
+
+const uint32_t kQRegs0[] = {0u, 1u, 2u, 3u, 4u, 5u};
+const int kQTypes0[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
+const char* const kQNames0[] = {"x0", "x1", "x2", "y0", "y1", "y2"};
+const unsigned long long kQOffs0[] = {0ull, 4ull, 8ull, 12ull, 16ull, 20ull};
+const loom_b200_queue_layout kQueues[] = {
+    {0u, -1, 6u, kQRegs0, kQTypes0, kQNames0},
+};
+const QueueSegment kSegments[] = {
+    {kQOffs0, 24ull},
+};
+
+cudaError_t launch_plain(const PlainLaunch& a)
+{
+    const unsigned long long grid = (a.n + a.block - 1) / a.block;
+    if(grid == 0) return cudaSuccess;
+    if(a.profile)
+        plain_kernel<K, true><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(
+            a.cols, a.n, a.max_steps, a.status, a.counters);
+    else
+        plain_kernel<K, false><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(
+            a.cols, a.n, a.max_steps, a.status, a.counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_regroup(const RegroupLaunch& a)
+{
+    void* args[] = {const_cast<RegroupParams*>(&a.params)};
+    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
+                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+}
+
+cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
+{
+    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
+}
+
+} } // namespace loom_b200::k_cross_f32
+
+extern const loom_b200::KernelEntry loom_b200_entry_cross_f32;
+const loom_b200::KernelEntry loom_b200_entry_cross_f32 = {
+    &loom_b200::k_cross_f32::kInfo, loom_b200::k_cross_f32::K::kRowBytes, 1,
+    &loom_b200::k_cross_f32::launch_plain, &loom_b200::k_cross_f32::launch_regroup,
+    &loom_b200::k_cross_f32::regroup_occupancy,
+    loom_b200::k_cross_f32::kQueues, loom_b200::k_cross_f32::kSegments};

@@ -17,6 +17,7 @@ extern const loom_b200::KernelEntry loom_b200_entry_bump_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_canonical_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_ceilfloor_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_collatz_u64;
+extern const loom_b200::KernelEntry loom_b200_entry_cross_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_fac_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_fac_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_fib_u32;
@@ -33,6 +34,7 @@ extern const loom_b200::KernelEntry loom_b200_entry_lshift_u32;
 extern const loom_b200::KernelEntry loom_b200_entry_lshift_u64;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_minmax_f64;
+extern const loom_b200::KernelEntry loom_b200_entry_norm_f32;
 extern const loom_b200::KernelEntry loom_b200_entry_primary_const_256;
 extern const loom_b200::KernelEntry loom_b200_entry_primary_const_b20_256;
 extern const loom_b200::KernelEntry loom_b200_entry_pt2_const_40;
@@ -73,6 +75,7 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_canonical_f32,
     &loom_b200_entry_ceilfloor_f32,
     &loom_b200_entry_collatz_u64,
+    &loom_b200_entry_cross_f32,
     &loom_b200_entry_fac_u32,
     &loom_b200_entry_fac_u64,
     &loom_b200_entry_fib_u32,
@@ -89,6 +92,7 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_lshift_u64,
     &loom_b200_entry_minmax_f32,
     &loom_b200_entry_minmax_f64,
+    &loom_b200_entry_norm_f32,
     &loom_b200_entry_primary_const_256,
     &loom_b200_entry_primary_const_b20_256,
     &loom_b200_entry_pt2_const_40,
@@ -112,5 +116,5 @@ const KernelEntry* const kRegistry[] = {
     &loom_b200_entry_union_f32,
     &loom_b200_entry_union_f64,
 };
-const int kRegistrySize = 53;
+const int kRegistrySize = 55;
 } // namespace loom_b200

@@ -17,6 +17,7 @@
 #include <tests/programs.hpp>
 
 #include "collatz.hpp"
+#include "linal_tests.hpp"
 #include "rng_tests.hpp"
 #include "sphere_pt.hpp"
 
@@ -59,6 +60,9 @@ using std::uint8_t;
     X(threefry_u32,       loom::vm::b200::kernels::threefry_k)                 \
     X(canonical_f32,      loom::vm::b200::kernels::canonical_k<float>)         \
     X(bump_u32,           loom::vm::b200::kernels::bump_k)                     \
+    /* and its vector macros (linal_tests.hpp)                         */    \
+    X(cross_f32,          loom::vm::b200::kernels::cross_k<float>)             \
+    X(norm_f32,           loom::vm::b200::kernels::norm_k<float>)              \
     /* Loom test programs (src/tests/programs.hpp) */                          \
     X(increment_i32,      increment<std::int32_t>)                             \
     X(increment_u8,       increment<std::uint8_t>)                             \

@@ -1,12 +1,16 @@
-// Loom's plain C++ random-number functions (src/common/random.hpp) over raw
-// input columns: the known answers the RNG kernels' golden outputs are
-// pinned to, as Loom's own test compares them (src/tests/vm_smallpt.cpp:
-// 349-378).  Built and run by make_rng_kat.py; not part of the product.
+// Loom's plain C++ functions behind the path tracers' VM macros, over raw
+// input columns: the random-number functions of src/common/random.hpp and
+// the vector functions of src/common/linal.hpp.  They are the known answers
+// the macro kernels' golden outputs are checked against, as Loom's own
+// tests compare them (src/tests/vm_smallpt.cpp:349-378,
+// src/tests/vm_linal.cpp:82-156).  Built and run by make_macro_kat.py; not
+// part of the product.
 //
-//   rng_kat <function> <n>  reads the kernel's input columns from stdin (n
-//   little-endian u32 each, one column after the other) and writes its
-//   output columns to stdout the same way.
+//   macro_kat <function> <n>  reads the kernel's input columns from stdin
+//   (n little-endian 32-bit words each, one column after the other) and
+//   writes its output columns to stdout the same way.
 #include <common/functional.hpp>
+#include <common/linal.hpp>
 #include <common/random.hpp>
 
 #include <array>
@@ -86,6 +90,33 @@ main(int argc, char** argv)
         }
         write_column(c0);
         write_column(c1);
+    }
+    else if(fn == "cross" || fn == "norm")
+    {
+        using Vec3f      = loom::Vector<float, 3, std::array>;
+        const int    nin = fn == "cross" ? 6 : 3;
+        std::vector<std::vector<float>> in(nin);
+        for(auto& c: in)
+        {
+            const auto w = read_column(n);
+            if(w.size() != n) return 3;
+            c.resize(n);
+            std::memcpy(c.data(), w.data(), n * sizeof(float));
+        }
+        std::vector<std::uint32_t> o[3];
+        for(auto& c: o) c.resize(n);
+        for(std::size_t i = 0; i < n; ++i)
+        {
+            const Vec3f a{in[0][i], in[1][i], in[2][i]};
+            const Vec3f r = fn == "cross" ? Vec3f(loom::cross(a, Vec3f{in[3][i], in[4][i], in[5][i]}))
+                                          : Vec3f(loom::normalize(a));
+            for(int j = 0; j < 3; ++j)
+            {
+                const float f = r[j];
+                std::memcpy(&o[j][i], &f, sizeof f);
+            }
+        }
+        for(const auto& c: o) write_column(c);
     }
     else
         return 2;

@@ -42,8 +42,8 @@ def test_interp_matches_golden(name, golden, golden_extra):
 
 def test_golden_fixture_for_every_kernel():
     d = pathlib.Path(__file__).parent / "golden"
-    # rng_kat.npz holds known answers beside the RNG kernels' fixtures
-    assert {p.stem for p in d.glob("*.npz")} - {"rng_kat"} == set(KERNELS)
+    # macro_kat.npz holds known answers beside the macro kernels' fixtures
+    assert {p.stem for p in d.glob("*.npz")} - {"macro_kat"} == set(KERNELS)
 
 
 def test_val_fib_matches_golden(golden):
@@ -153,6 +153,11 @@ def test_workload_inputs_match_the_oracle_stream():
 
 
 RNG_KERNELS = {"rotl32_u32": 1, "threefry_u32": 2, "canonical_f32": 1, "bump_u32": 2}
+LINAL_KERNELS = {"cross_f32": 3, "norm_f32": 3}
+
+
+def _kat():
+    return np.load(pathlib.Path(__file__).resolve().parent / "golden" / "macro_kat.npz")
 
 
 @pytest.mark.parametrize("name", sorted(RNG_KERNELS))
@@ -160,12 +165,53 @@ def test_rng_macros_match_loom_cpp_functions(name, golden):
     """The RNG macros of the path tracers (one kernel each) give the known
     answers of Loom's plain C++ functions (src/common/random.hpp: rotl32,
     threefry2x32r32<0xdead, 0xbeef>, gen_canonical, bump_ctr) on the
-    fixture's inputs, in Loom's scalar backend (the golden outputs) and in
-    the C restatement; tests/golden/make_rng_kat.py wrote the answers."""
-    kat = np.load(pathlib.Path(__file__).resolve().parent / "golden" / "rng_kat.npz")
+    fixture's inputs, exactly, in Loom's scalar backend (the golden outputs)
+    and in the C restatement; tests/golden/make_macro_kat.py wrote the
+    answers."""
+    kat = _kat()
     ins, outs = golden(name)
     got = O.Interp(name).run(ins)
     for j in range(RNG_KERNELS[name]):
         want = kat[f"{name}_out{j}"]
         assert np.array_equal(np.ascontiguousarray(outs[j]).view(np.uint32), want), f"{name} golden out{j}"
         assert np.array_equal(np.ascontiguousarray(got[j]).view(np.uint32), want), f"{name} interp out{j}"
+
+
+def ulp_distance(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Distance in units in the last place between float32 arrays: the
+    difference of their bit patterns mapped to a monotonic integer line
+    (negative floats mirrored below zero), the comparison of Dawson's
+    "Comparing floating point numbers"."""
+    def line(x):
+        i = np.ascontiguousarray(x, dtype=np.float32).view(np.int32).astype(np.int64)
+        return np.where(i < 0, -(i & 0x7FFFFFFF), i)
+
+    return np.abs(line(a) - line(b))
+
+
+@pytest.mark.parametrize("name", sorted(LINAL_KERNELS))
+def test_vector_macros_match_loom_cpp_functions(name, golden):
+    """The vector macros of the sphere path tracer (vec3_cross, vec3_norm)
+    against Loom's C++ cross and normalize (src/common/linal.hpp) with the
+    bound of Loom's own test: within 30 ulp for at least 99 % of the inputs
+    (src/tests/vm_linal.cpp:57, 100-156).  The two round differently (the
+    macro multiplies by a reciprocal square root), so the bound, not bit
+    equality, is the check; bse and the C restatement agree exactly."""
+    kat = _kat()
+    ins, outs = golden(name)
+    got = O.Interp(name).run(ins)
+    ok = np.ones(len(ins[0]), dtype=bool)
+    for j in range(LINAL_KERNELS[name]):
+        want = kat[f"{name}_out{j}"].view(np.float32)
+        ok &= ulp_distance(outs[j], want) <= 30
+        assert np.array_equal(np.ascontiguousarray(got[j]).view(np.uint32), np.ascontiguousarray(outs[j]).view(np.uint32))
+    assert ok.mean() >= 0.99, f"{name}: {ok.mean():.4f} within 30 ulp"
+
+
+def test_ulp_distance():
+    one = np.float32(1.0)
+    nxt = np.nextafter(one, np.float32(2.0))
+    assert ulp_distance(np.array([one]), np.array([nxt]))[0] == 1
+    assert ulp_distance(np.array([np.float32(-0.0)]), np.array([np.float32(0.0)]))[0] == 0
+    tiny = np.nextafter(np.float32(0.0), np.float32(1.0))
+    assert ulp_distance(np.array([-tiny]), np.array([tiny]))[0] == 2
