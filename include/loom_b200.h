@@ -412,7 +412,11 @@ int loom_b200_server_failed(loom_b200_server* s, uint64_t* tickets, int32_t* cod
  *
  * The first call on a device looks up the array's device address (and so
  * loads it onto that device): make that first call before any stream
- * capture.  Every call shares the array and clears what must start at zero;
+ * capture.  The address is kept for the life of the process; a process that
+ * calls cudaDeviceReset discards the array with the device's other state and
+ * must not call this entry point on that device again.  The call waits for
+ * its launch before it returns.  Every call shares the array and clears what
+ * must start at zero;
  * calls whose launches overlap on the GPU (other streams, other host
  * threads) race on it.  The call returns after the launch finished on
  * `stream` (NULL: the CUDA default stream); *status_out (may be NULL)

@@ -116,6 +116,32 @@ def test_static_path_tracer_matches_launch_device_twice(golden, golden_extra):
             assert torch.equal(g.view(torch.int32), w.view(torch.int32)), f"call {call}: outputs differ"
 
 
+@pytest.mark.gpu
+def test_static_device_status_then_clean_call():
+    """A launch that stops at its round limit reports the device status
+    (LOOM_B200_ERR_DEVICE with the STEP_LIMIT bit in *status_out); the next
+    call starts from cleared control words and equals the handle-based launch
+    bit for bit, although the shared array still holds the stopped launch's
+    parked threads."""
+    import torch
+
+    x = O.uniform_int(9, 100_000, 1, 1 << 40)
+    d_x = torch.from_numpy(x.view(np.int64)).cuda()
+    out = torch.empty(len(x), dtype=torch.int32, device="cuda")
+    opts = api.Opts()
+    opts.population = 4096  # many rounds are needed ...
+    opts.max_steps = 1  # ... and the engine may run one
+    rc, status = _static("collatz_u64", [d_x], [out], len(x), opts=opts)
+    assert rc == api.ERR_DEVICE
+    assert status & api.STATUS_STEP_LIMIT
+    want = torch.empty(len(x), dtype=torch.int32, device="cuda")
+    got = torch.full((len(x),), -1, dtype=torch.int32, device="cuda")
+    _existing("collatz_u64", [d_x], [want], len(x))
+    rc, status = _static("collatz_u64", [d_x], [got], len(x), opts=None)
+    assert (rc, status) == (api.OK, 0), f"rc {rc} status {status:#x}"
+    assert torch.equal(got, want)
+
+
 def test_static_refuses_what_the_array_cannot_hold():
     """Sizes beyond the fixed array are refused before anything runs (no GPU
     needed): a population whose queue state exceeds the array, and more
