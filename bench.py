@@ -122,11 +122,14 @@ class PathTracing(Workload):
         from loom_b200 import scenes as S
 
         self.req = S.cornell_request(width, height, spp, seed=1)
+        self.spp = spp
+        self.pixels = width * height
         self.table, self.starts = S.pack([self.req])
         self.n = self.req.threads
         self.desc = (
             f"sphere path tracer, Cornell box of 9 spheres (walls r=1e5, mirror, glass IOR 1.5, light), "
-            f"{width}x{height} x {spp} spp = {self.n} threads, FP32, RR from depth 5, max depth 16"
+            f"{width}x{height} x {spp} spp = {self.n} threads, FP32, RR from depth 5, max depth 16; "
+            f"output: the {width}x{height} RGB f32 image (per-pixel mean of its {spp} samples in sample order)"
         )
         self.in_bytes = 0
         self.out_bytes = 12
@@ -137,21 +140,48 @@ class PathTracing(Workload):
     def device_buffers(self, torch):
         self.d_table = torch.from_numpy(self.table.view(np.int32)).cuda()
         self.d_out = [torch.empty(self.n, dtype=torch.float32, device="cuda") for _ in range(3)]
+        self.d_img = [torch.empty(self.pixels, dtype=torch.float32, device="cuda") for _ in range(3)]
 
     def launch(self, f, api, stream):
+        """One step: the render (one thread per pixel-sample), then the image
+        (per-pixel means, loom_b200_group_mean)."""
         f.launch_device(self.inputs(api), self.d_out, self.n, table=self.d_table, stream=stream)
+        for o, img in zip(self.d_out, self.d_img):
+            api.group_mean(o, img, self.pixels, self.spp, stream=stream)
+
+    launches_per_step = 5  # queue reset + megakernel (or the plain kernel) + 3 group means
+
+    def check_tids(self):
+        """Every sample of 256 random pixels (16,384 threads)."""
+        rng = np.random.default_rng(5)
+        px = np.sort(rng.choice(self.pixels, size=256, replace=False))
+        return (px[:, None] * self.spp + np.arange(self.spp)[None, :]).reshape(-1)
+
+    def image_rows_ok(self, want_samples, tids):
+        """The device image at the checked pixels against the per-pixel mean
+        (in sample order) of the reference's per-sample outputs."""
+        import torch
+
+        from loom_b200 import scenes as S
+
+        px = np.asarray(tids, dtype=np.int64).reshape(-1, self.spp)[:, 0] // self.spp
+        want = S.pixel_average(want_samples, self.spp)
+        ix = torch.from_numpy(px).cuda()
+        got = np.stack([img[ix].cpu().numpy() for img in self.d_img], axis=1)
+        return bool(np.array_equal(got.view(np.uint32), want.view(np.uint32)))
 
     def ref_inputs(self, tids):
         tids = np.asarray(tids, dtype=np.uint64)
         return [np.zeros(len(tids), dtype=np.uint32), tids.astype(np.uint32)], self.table
 
     def e2e(self, api, torch, steps, warmup, dist):
-        h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
+        """The image through loom_b200_launch_host_mean: scene table in,
+        render, per-pixel means, image rows back to pinned host memory."""
+        h_img = [torch.empty(self.pixels, dtype=torch.float32).pin_memory() for _ in range(3)]
         fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
 
         def step():
-            L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, None, self.table)
-            api.check(api.lib().loom_b200_launch_host(fe._h, api.ctypes.byref(L)))
+            fe.launch_host_mean(self.inputs(api), self.n, group=self.spp, table=self.table, outputs=h_img)
 
         for _ in range(warmup):
             step()
@@ -161,9 +191,9 @@ class PathTracing(Workload):
         for _ in range(steps):
             step()
         dt = time.perf_counter() - t0
-        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_out, self.d_out))
+        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_img, self.d_img))
         fe.close()
-        return dt, ok, self.table.nbytes, 3 * 4 * self.n
+        return dt, ok, self.table.nbytes, 3 * 4 * self.pixels
 
 
 class BatchedPathTracing(PathTracing):
@@ -173,6 +203,7 @@ class BatchedPathTracing(PathTracing):
     mapped to (request, sample) on the device from the instance offsets."""
 
     tune_key = "batch"
+    launches_per_step = 2
 
     def __init__(self, count=256, seed=3):
         from loom_b200 import scenes as S
@@ -181,10 +212,12 @@ class BatchedPathTracing(PathTracing):
         self.reqs = [S.random_request(rng, seed=i + 1) for i in range(count)]
         self.table, self.starts = S.pack(self.reqs)
         self.n = int(self.starts[-1])
+        self.spp_of = np.array([r.spp for r in self.reqs], dtype=np.uint32)
+        self.pixels = int(sum(r.width * r.height for r in self.reqs))
         self.desc = (
             f"{count} batched render requests (seed {seed}): resolution from {{64,128,256,512}}^2, spp from "
             f"{{1,4,16,64}}, 8-64 random spheres each (60/20/20 diffuse/mirror/glass, 1-4 emitters), "
-            f"{self.n} threads in one launch, FP32"
+            f"{self.n} threads in one launch, FP32; end to end: each request's image (per-pixel means)"
         )
         self.in_bytes = 0
         self.out_bytes = 12
@@ -193,7 +226,8 @@ class BatchedPathTracing(PathTracing):
         return [api.Instance(), api.LocalIota()]
 
     def device_buffers(self, torch):
-        super().device_buffers(torch)
+        self.d_table = torch.from_numpy(self.table.view(np.int32)).cuda()
+        self.d_out = [torch.empty(self.n, dtype=torch.float32, device="cuda") for _ in range(3)]
         self.d_starts = torch.from_numpy(self.starts.view(np.int64)).cuda()
 
     def launch(self, f, api, stream):
@@ -207,18 +241,27 @@ class BatchedPathTracing(PathTracing):
         lo, hi = self.starts[:-1].astype(np.int64), self.starts[1:].astype(np.int64)
         return np.unique(np.concatenate([rng.integers(a, b, size=4) for a, b in zip(lo, hi)]))
 
+    def request_of(self, tids):
+        return np.searchsorted(self.starts, np.asarray(tids, dtype=np.uint64), side="right") - 1
+
+    def image_rows_ok(self, want_samples, tids):
+        return None
+
     def ref_inputs(self, tids):
         tids = np.asarray(tids, dtype=np.uint64)
         inst = (np.searchsorted(self.starts, tids, side="right") - 1).astype(np.int64)
         return [inst.astype(np.uint32), (tids - self.starts[inst]).astype(np.uint32)], self.table
 
     def e2e(self, api, torch, steps, warmup, dist):
-        h_out = [torch.empty(self.n, dtype=torch.float32).pin_memory() for _ in range(3)]
+        """Every request's image through loom_b200_launch_host_mean (per
+        request: its samples per pixel), compared with the per-pixel means
+        of the device's per-sample outputs."""
+        h_img = [torch.empty(self.pixels, dtype=torch.float32).pin_memory() for _ in range(3)]
         fe = api.Function(self.kernel, self.n, "regroup", **self.opts)
 
         def step():
-            L, keep = fe._launch_struct(self.inputs(api), h_out, self.n, self.starts, self.table)
-            api.check(api.lib().loom_b200_launch_host(fe._h, api.ctypes.byref(L)))
+            fe.launch_host_mean(self.inputs(api), self.n, instance_group=self.spp_of, instance_starts=self.starts,
+                                table=self.table, outputs=h_img)
 
         for _ in range(warmup):
             step()
@@ -228,12 +271,25 @@ class BatchedPathTracing(PathTracing):
         for _ in range(steps):
             step()
         dt = time.perf_counter() - t0
-        ok = all(torch.equal(h, d.cpu()) for h, d in zip(h_out, self.d_out))
+        # check: the images of 8 requests against the means of the device outputs
+        from loom_b200 import scenes as S
+
+        ok, row = True, 0
+        for i, r in enumerate(self.reqs):
+            rows = r.width * r.height
+            if i % 32 == 0:
+                a, b = int(self.starts[i]), int(self.starts[i + 1])
+                want = S.pixel_average([o[a:b].cpu().numpy() for o in self.d_out], r.spp)
+                got = np.stack([h[row : row + rows].numpy() for h in h_img], axis=1)
+                ok &= bool(np.array_equal(got.view(np.uint32), want.view(np.uint32)))
+            row += rows
         fe.close()
-        return dt, ok, self.table.nbytes + self.starts.nbytes, 3 * 4 * self.n
+        return dt, ok, self.table.nbytes + self.starts.nbytes, 3 * 4 * self.pixels
 
 
 class IntegerLoop(Workload):
+    launches_per_step = 2
+
     def __init__(self, kernel, n, lo, hi, out_bytes, desc):
         from loom_b200 import inputs as I
 
@@ -280,6 +336,7 @@ class LoomPathTracer(Workload):
     pt_const, 1e-3 for pt2_const).  A step renders the image once."""
 
     dtype = "f32"
+    launches_per_step = 2
 
     def __init__(self, kernel, threshold, side=40, blur=1):
         self.kernel = kernel
@@ -792,9 +849,36 @@ class RegroupService:
             }
         )
         self.bufs = {}
+        self.reqs = {}
+        self.keep_samples = False
+        self.samples = []  # (kind, reference inputs, table, outputs) of sampled threads
 
     def device_bytes(self):
         return sum(s["device_bytes"] for s in self.p.stats().values())
+
+    def _sample(self, key, req, buf):
+        """Keeps 4 threads of a completed request (their reference inputs and
+        the served outputs) for the parity check."""
+        from loom_b200 import scenes as S
+
+        kind, n, a, r = req
+        rng = np.random.default_rng(len(self.samples))
+        j = np.unique(rng.integers(0, n, size=4))
+        info = self.p.servers[kind].info
+        dts = [np.dtype(api_np(self.api, t)) for _, t in info.outputs]
+        host = buf.numpy()
+        got, off = [], 0
+        for dt in dts:
+            col = host[off : off + n * dt.itemsize].view(dt)
+            got.append(col[j].copy())
+            off += n * dt.itemsize
+        if kind == "pt":
+            table, _ = S.pack([r])
+            ins = [np.zeros(len(j), dtype=np.uint32), j.astype(np.uint32)]
+        else:
+            table = None
+            ins = [self.inputs[kind][a : a + n].numpy().view(np.uint64)[j]]
+        self.samples.append((kind, ins, table, got))
 
     def submit(self, req):
         kind, n, a, _ = req
@@ -810,6 +894,7 @@ class RegroupService:
         else:
             key = self.p.submit(kind, n, inputs=[self.inputs[kind][a : a + n]], outputs=outs)
         self.bufs[key] = buf
+        self.reqs[key] = req
         return key
 
     def busy(self):
@@ -819,7 +904,11 @@ class RegroupService:
         done = self.p.step()
         for key in done:
             self.p.result(*key)
-            self.pool.put(self.bufs.pop(key))
+            req = self.reqs.pop(key)
+            buf = self.bufs.pop(key)
+            if self.keep_samples and key[1] % 4 == 0:
+                self._sample(key, req, buf)
+            self.pool.put(buf)
         return done
 
     def lane_efficiency(self):
@@ -924,11 +1013,15 @@ def run_requests(svc, reqs, arrivals):
     return np.asarray(lat), last, threads
 
 
-def serve_main(args, warmup, world, rank, local):
+def serve_measure(seconds: float, rank: int = 0, local: int = 0, parity: bool = False):
+    """The serving loop of both services (continuous-batching regroup
+    servers, plain FIFO queue) under Poisson arrivals at 25/50/75/100 % of
+    each one's measured capacity, `seconds` of arrivals per load.  With
+    `parity`, sampled threads of some completed requests of the regroup
+    servers are kept for a check against the reference.  Returns (results
+    per service, clock summary)."""
     import torch
 
-    if world > 1:
-        torch.cuda.set_device(local)
     from loom_b200 import api
     from loom_b200 import inputs as I
 
@@ -952,9 +1045,11 @@ def serve_main(args, warmup, world, rank, local):
             cap = threads / span
             mean_threads = threads / len(cal)
             res = {"capacity_msamples_s": round(cap / 1e6, 3), "device_bytes": svc.device_bytes(), "loads": []}
+            if parity and name == "regroup":
+                svc.keep_samples = True
             for L in loads:
                 rate = L * cap / mean_threads  # requests per second
-                count = max(8, int(rate * args.serve_seconds))
+                count = max(8, int(rate * seconds))
                 reqs = mix.draw(count)
                 arr = np.cumsum(mix.rng.exponential(1.0 / rate, size=count))
                 lat, span, threads = run_requests(svc, reqs, arr)
@@ -968,6 +1063,8 @@ def serve_main(args, warmup, world, rank, local):
                         "mean_ms": round(float(lat.mean()) * 1e3, 2),
                     }
                 )
+            if parity and name == "regroup":
+                res["parity"] = serve_parity(svc, inputs)
             svc.close()
             # lane efficiency of the same mix in a counted (slower) run
             svc = cls(api, torch, stream, pool, inputs, profile=True)
@@ -977,7 +1074,28 @@ def serve_main(args, warmup, world, rank, local):
             res["lane_efficiency"] = None if le is None else round(le, 4)
             svc.close()
             out[name] = res
+    return out, clk.summary()
 
+
+def serve_parity(svc, inputs):
+    """Sampled threads of completed requests (every request whose ticket is
+    a multiple of 4, 4 threads each) against the reference."""
+    run, kind, _ = _reference_runner()
+    ok, checked, reqs = True, 0, set()
+    for kind_, want_ins, table, got in svc.samples:
+        want = run(SERVE_KERNELS[kind_], want_ins, table)
+        ok &= same_bits(got, want, SERVE_KERNELS[kind_])
+        checked += len(got[0])
+    return {"checked_against": kind, "requests_checked": len(svc.samples), "threads_checked": checked,
+            "ok": bool(ok)}
+
+
+def serve_main(args, warmup, world, rank, local):
+    import torch
+
+    if world > 1:
+        torch.cuda.set_device(local)
+    out, clocks = serve_measure(args.serve_seconds, rank, local)
     full = out["regroup"]["loads"][-1]
     line = base_line(
         args, warmup, world,
@@ -995,7 +1113,7 @@ def serve_main(args, warmup, world, rank, local):
             "regroup": out["regroup"],
             "plain": out["plain"],
             "gpu_launches": None,
-            "clocks": clk.summary(),
+            "clocks": clocks,
         }
     )
     if rank == 0:
@@ -1023,6 +1141,7 @@ def tune_main(args) -> None:
     space = dict(T.SPACE)
     if w.kernel == "sphere_pt_f32":  # 2 x 2832 queue bytes per thread in flight
         space["population"] = [p for p in space["population"] if p <= 1 << 22]
+    space["max_regs"] = api.reg_caps(w.kernel)  # the caps compiled for this kernel
 
     def make_launch(opts):
         f.set_opts("regroup", **opts)
@@ -1032,6 +1151,16 @@ def tune_main(args) -> None:
         f.stats(raise_on_device_error=True)
         f.reset_stats()
 
+    constraint = None
+    if args.tune_min_lane_eff:
+        def constraint(opts):
+            """One counted launch: VM-level lane efficiency of the point."""
+            f.set_opts("regroup", profile=True, **opts)
+            w.launch(f, api, stream)
+            le = f.stats(raise_on_device_error=True)["lane_efficiency"]
+            f.reset_stats()
+            return le >= args.tune_min_lane_eff
+
     seed = [
         dict(T.DEFAULT, **regroup_opts(w.kernel, w.tune_key)),
         dict(T.DEFAULT, cost_model=True, utr_lanes=4, burst=32),
@@ -1040,14 +1169,195 @@ def tune_main(args) -> None:
         # of few long threads)
         dict(T.DEFAULT, utr_lanes=1, spread_lanes=1, burst=64, period=1 << 20),
     ]
+    if args.tune_seed:
+        seed.insert(0, dict(T.DEFAULT, **json.loads(args.tune_seed)))
     res = T.tune(make_launch, w.n, seed=seed, space=space, budget_s=args.tune_budget,
-                 log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate)
+                 log=lambda m: print(m, file=sys.stderr, flush=True), validate=validate,
+                 constraint=constraint)
+    res["constraint"] = {"min_lane_efficiency": args.tune_min_lane_eff} if constraint else None
     res["workload"] = args.workload
     res["kernel"] = w.kernel
     res["device"] = torch.cuda.get_device_name(0)
     pathlib.Path(args.tune).write_text(json.dumps(res, indent=1) + "\n")
     print(json.dumps({k: res[k] for k in ("kernel", "workload", "best", "ms", "msamples_s")}))
     f.close()
+
+
+def measure(w, api, torch, stream, steps, warmup, dist, tids, forms, clocks_for=None):
+    """The plain engine and each regrouping form of workload `w`: CUDA-event
+    time of `steps` steps after `warmup`, one counted launch (VM-instruction
+    counters, lane efficiency) and the outputs at `tids`.  `forms` maps a
+    name to regrouping options; the form named `clocks_for` is timed again
+    with the clocks sampled.  Returns a dict per engine and form."""
+    res = {}
+    for name, mode, opts in [("plain", "plain", {})] + [(k, "regroup", o) for k, o in forms.items()]:
+        run_opts = dict(opts, graph=True) if mode == "regroup" else {}
+        f = api.Function(w.kernel, 0, mode, **run_opts)
+        clk = None
+        if name == clocks_for:
+            with ClockSampler(torch.cuda.current_device()) as c:
+                ms = time_steps(lambda: w.launch(f, api, stream), steps, warmup, torch, dist)
+            clk = c.summary()
+        else:
+            ms = time_steps(lambda: w.launch(f, api, stream), steps, warmup, torch, dist)
+        st_t = f.stats(raise_on_device_error=True)
+        out = w.outputs_at(tids)
+        extra = {}
+        if hasattr(w, "image_rows_ok"):
+            extra["image"] = [img[:].clone() for img in getattr(w, "d_img", [])]
+        dev_bytes = f.device_bytes()
+        f.reset_stats()
+        f.set_opts(mode, profile=True, **run_opts)  # one counted launch
+        w.launch(f, api, stream)
+        torch.cuda.synchronize()
+        st = f.stats(raise_on_device_error=True)
+        f.close()
+        res[name] = dict(ms=ms / steps, kernel_ms=st_t["ms"], stats=st, out=out, opts=opts, clocks=clk,
+                         device_bytes=dev_bytes, rounds=st_t["rounds"] / max(1, st_t["launches"]),
+                         parks=st_t["parks"] / max(1, st_t["launches"]),
+                         state_bytes=st_t["state_bytes"] / max(1, st_t["launches"]), **extra)
+    return res
+
+
+def regroup_forms(w):
+    """The tuned regrouping forms of a workload: the fastest (the headline
+    form) and, where tuned, Loom's majority rule with the cost model and the
+    lane-efficiency form (the fastest one measured at >= 70 % SASS lane
+    efficiency)."""
+    from loom_b200 import autotune as T
+
+    forms = {"regroup": w.opts}
+    if w.tune_key != "default":
+        for key, name in (("_majority", "majority_cost_model"), ("_lane", "lane_efficiency_form")):
+            o = T.tuned(w.kernel, w.tune_key + key)
+            if o:
+                forms[name] = o
+    return forms
+
+
+def issue_roofline(vm_instr: float, kern_ms: float, sm_mhz: float) -> dict:
+    """The SIMT issue roofline of a launch: VM instructions executed (summed
+    over Loom threads) per second against 32 lanes x 148 SMs x 4 schedulers
+    x one warp instruction per cycle at the sampled SM clock."""
+    got = vm_instr / (kern_ms / 1e3) / 1e9
+    top = 32 * 148 * 4 * sm_mhz / 1e3
+    return {"achieved": round(got, 1), "peak": round(top, 1), "unit": "G VM thread-instructions/s",
+            "frac": round(got / top, 4)}
+
+
+def workload_summary(w, res, world, cpu=None, want=None, e2e=None, tids=None):
+    """The figures of one workload: value and ms per step of the tuned
+    regrouping form, the plain engine and the other forms beside it, lane
+    efficiencies, parity against the reference on the sampled threads."""
+    rg, pl = res["regroup"], res["plain"]
+    d = {
+        "workload": w.desc,
+        "kernel": w.kernel,
+        "threads": w.n,
+        "value": round(world * w.n / (rg["ms"] / 1e3) / 1e6, 3),
+        "unit": "Msamples/s",
+        "ms_per_step": round(rg["ms"], 4),
+        "lane_efficiency": round(rg["stats"]["lane_efficiency"], 4),
+        "regroup_options": rg["opts"],
+        "device_bytes": rg["device_bytes"],
+        "plain": {
+            "value": round(world * w.n / (pl["ms"] / 1e3) / 1e6, 3),
+            "ms_per_step": round(pl["ms"], 4),
+            "lane_efficiency": round(pl["stats"]["lane_efficiency"], 4),
+        },
+        "speedup_vs_plain": round(pl["ms"] / rg["ms"], 4),
+    }
+    for name, r in res.items():
+        if name in ("plain", "regroup"):
+            continue
+        d[name] = {
+            "options": r["opts"],
+            "value": round(world * w.n / (r["ms"] / 1e3) / 1e6, 3),
+            "ms_per_step": round(r["ms"], 4),
+            "lane_efficiency": round(r["stats"]["lane_efficiency"], 4),
+            "speedup_vs_plain": round(pl["ms"] / r["ms"], 4),
+            "same_outputs": bool(same_bits(r["out"], rg["out"])),
+            "device_bytes": r["device_bytes"],
+        }
+    par = {"sample_threads": int(len(tids)), "plain_equals_regroup": bool(same_bits(pl["out"], rg["out"]))}
+    if want is not None:
+        par["checked_against"] = cpu["kind"]
+        par["regroup_ok"] = bool(same_bits(rg["out"], want, w.kernel))
+        par["plain_ok"] = bool(same_bits(pl["out"], want, w.kernel))
+        for name, r in res.items():
+            if name not in ("plain", "regroup"):
+                par[f"{name}_ok"] = bool(same_bits(r["out"], want, w.kernel))
+        if w.kernel in ULP_TOLERANCE:
+            par["float_tolerance_ulp"] = ULP_TOLERANCE[w.kernel]
+        if hasattr(w, "request_of"):
+            req = w.request_of(tids)
+            bad = set()
+            for g, x in zip(rg["out"], want):
+                diff = np.ascontiguousarray(g).view(np.uint8).reshape(len(tids), -1) != np.ascontiguousarray(
+                    x).view(np.uint8).reshape(len(tids), -1)
+                bad |= set(int(r) for r in req[diff.any(axis=1)])
+            par["requests_checked"] = int(len(np.unique(req)))
+            par["threads_per_request"] = 4
+            par["requests_failed"] = sorted(bad)
+        if rg.get("image") and hasattr(w, "image_rows_ok"):
+            w.d_img = rg["image"]
+            par["image_ok"] = w.image_rows_ok(want, tids)
+            par["image_pixels_checked"] = int(len(tids) // getattr(w, "spp", 1))
+    par["parity"] = bool(par.get("regroup_ok", par["plain_equals_regroup"]) and par["plain_equals_regroup"]
+                         and par.get("image_ok", True) is not False and not par.get("requests_failed"))
+    d["parity"] = par
+    if cpu is not None:
+        d["cpu_baseline"] = cpu
+    if e2e is not None:
+        d["e2e"] = e2e
+    return d
+
+
+def run_e2e(w, api, torch, steps, warmup, dist, world):
+    e2e_s, ok, h2d, d2h = w.e2e(api, torch, steps, warmup, dist)
+    e2e_s = max_over_ranks(e2e_s, dist)
+    return {
+        "value": round(world * w.n * steps / e2e_s / 1e6, 3),
+        "unit": "Msamples/s",
+        "h2d_bytes_per_step": int(h2d),
+        "d2h_bytes_per_step": int(d2h),
+        "equals_device": bool(ok),
+    }
+
+
+def sub_config(name, api, torch, stream, steps, warmup, dist, world, no_cpu, extra_check=None):
+    """One more configuration of the default run, measured like the
+    headline with its own (smaller) step count."""
+    w = make_workload(name)
+    w.opts = regroup_opts(w.kernel, w.tune_key)
+    w.device_buffers(torch)
+    tids = w.check_tids()
+    res = measure(w, api, torch, stream, steps, warmup, dist, tids, regroup_forms(w))
+    e2e = run_e2e(w, api, torch, steps, warmup, dist, world)
+    cpu = want = None
+    if not no_cpu:
+        v, info, want = cpu_reference(w, check_tids=tids, target_s=1.0)
+        cpu = dict(info, value=round(v, 3))
+    d = workload_summary(w, res, world, cpu, want, e2e, tids)
+    d["steps"], d["warmup"] = steps, warmup
+    if extra_check:
+        d["parity"].update(extra_check(w))
+        d["parity"]["parity"] = bool(d["parity"]["parity"] and all(
+            v for k, v in d["parity"].items() if k.endswith("_ok") and isinstance(v, bool)))
+    for attr in ("d_out", "d_in", "d_table", "d_starts", "d_img"):
+        if hasattr(w, attr):
+            delattr(w, attr)
+    torch.cuda.empty_cache()
+    return d
+
+
+def fib_full_check(w):
+    """Every one of the 2^20 Fibonacci outputs against Loom's validator
+    (val_fib, src/tests/programs.hpp:353-368)."""
+    from oracle import oracle as O
+
+    got = w.d_out[0].cpu().numpy().view(np.uint64)
+    return {"all_threads_vs_val_fib_ok": bool(np.array_equal(got, O.val_fib(w.x))), "all_threads": int(w.n)}
 
 
 def main() -> None:
@@ -1058,9 +1368,14 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "loom_primary", "loom_primary_b20", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="pt: skip the other configurations (fib, collatz, batch, serve) of the default run")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
     ap.add_argument("--tune", metavar="OUT", help="autotune the regrouping options of the workload, write JSON to OUT")
     ap.add_argument("--tune-budget", type=float, default=300.0, help="seconds of tuning")
+    ap.add_argument("--tune-min-lane-eff", type=float, default=0.0,
+                    help="tune: only points whose counted VM lane efficiency reaches this are eligible")
+    ap.add_argument("--tune-seed", default="", help="tune: JSON options of an extra seed point")
     ap.add_argument("--csv", metavar="PATH", help="append a CSV row of the result to PATH")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
@@ -1088,16 +1403,23 @@ def main() -> None:
     if args.impl == "reference":
         if rank != 0:
             return
-        vals, info = [], None
+        vals, secs, info = [], [], None
         for i in range(warmup + args.steps):
             v, info, _ = cpu_reference(w, target_s=2.0)
             if i >= warmup:
                 vals.append(v)
+                secs.append(info["seconds"])
         value = statistics.median(vals)
         line = base_line(args, warmup, args.gpus, w.desc, w.kernel, w.dtype, METRIC, extra)
         line = {"impl": "reference", **line, "value": round(value, 3)}
-        # the whole workload at the sampled rate
-        line["ms_per_step"] = round(w.n / (value * 1e6) * 1e3, 4)
+        # each step times a bounded random sample of the workload; ms_per_step
+        # is the sampled step's own time, the whole workload's projection beside it
+        line["ms_per_step"] = round(1e3 * statistics.median(secs), 4)
+        line["ms_per_step_note"] = (
+            "wall time of one step, which runs a random sample of the workload's threads (cpu_baseline.sample); "
+            "projected_ms_full_workload is the whole workload at the sampled rate"
+        )
+        line["projected_ms_full_workload"] = round(w.n / (value * 1e6) * 1e3, 4)
         line["cpu_baseline"] = dict(info, value=round(value, 3))
         line["e2e"] = {"value": round(value, 3), "unit": "Msamples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
         print(json.dumps(line))
@@ -1128,54 +1450,48 @@ def main() -> None:
     w.device_buffers(torch)
     tids = w.check_tids()
 
-    res = {}
-    for mode in ("plain", "regroup"):
-        opts = dict(w.opts, graph=True) if mode == "regroup" else {}
-        f = api.Function(w.kernel, 0, mode, **opts)
-        ms = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
-        f.sync()
-        f.reset_stats()
-        f.set_opts(mode, profile=True, **opts)  # one counted launch for lane efficiency
-        w.launch(f, api, stream)
-        torch.cuda.synchronize()
-        st = f.stats(raise_on_device_error=True)
-        f.set_opts(mode, **opts)
-        f.reset_stats()
-        res[mode] = dict(ms=ms, stats=st, fn=f, out=w.outputs_at(tids))
+    forms = regroup_forms(w)
+    res = measure(w, api, torch, stream, args.steps, warmup, dist, tids, forms, clocks_for="regroup")
+    rg = res["regroup"]
+    clocks = rg["clocks"]
+    e2e = run_e2e(w, api, torch, args.steps, warmup, dist, world)
 
-    # the headline: the regrouping engine, clocks sampled during the timed region
-    f = res["regroup"]["fn"]
-    with ClockSampler(local) as clk:
-        ms_r = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
-    st_r = f.stats(raise_on_device_error=True)
-    kern_ms = st_r["ms"]
-    out_r = w.outputs_at(tids)
+    cpu = want = None
+    if rank == 0 and not args.no_cpu:
+        v, info, want = cpu_reference(w, check_tids=tids)
+        cpu = dict(info, value=round(v, 3))
+    summary = workload_summary(w, res, world, cpu, want, e2e, tids)
 
-    # the other tuned form of the same workload, when there is one: Loom's
-    # majority rule with the cost model (the highest lane efficiency)
-    alt = None
-    from loom_b200 import autotune as T
-
-    alt_opts = T.tuned(w.kernel, w.tune_key + "_majority") if w.tune_key != "default" else None
-    if alt_opts:
-        fa = api.Function(w.kernel, 0, "regroup", **dict(alt_opts, graph=True))
-        ms_a = time_steps(lambda: w.launch(fa, api, stream), args.steps, warmup, torch, dist) / args.steps
-        fa.set_opts("regroup", profile=True, **alt_opts)
-        w.launch(fa, api, stream)
-        torch.cuda.synchronize()
-        sa = fa.stats(raise_on_device_error=True)
-        alt = {
-            "options": alt_opts,
-            "value": round(world * w.n / (ms_a / 1e3) / 1e6, 3),
-            "ms_per_step": round(ms_a, 4),
-            "lane_efficiency": round(sa["lane_efficiency"], 4),
-            "speedup_vs_plain": None,
-            "same_outputs": bool(same_bits(w.outputs_at(tids), out_r)),
+    # the other configurations of the default run, each with its parity check
+    configs = {}
+    if args.workload == "pt" and not args.no_configs:
+        for attr in ("d_out", "d_img", "d_table"):
+            if hasattr(w, attr):
+                delattr(w, attr)
+        torch.cuda.empty_cache()
+        configs["fib"] = sub_config("fib", api, torch, stream, args.steps, warmup, dist, world, args.no_cpu,
+                                    fib_full_check)
+        configs["collatz"] = sub_config("collatz", api, torch, stream, args.steps, warmup, dist, world,
+                                        args.no_cpu)
+        configs["batch"] = sub_config("batch", api, torch, stream, max(2, args.steps // 4), 3, dist, world,
+                                      args.no_cpu)
+        sv, sv_clk = serve_measure(1.0, rank, local, parity=not args.no_cpu)
+        full = sv["regroup"]["loads"][-1]
+        configs["serve"] = {
+            "workload": "serving: Poisson arrivals at 25/50/75/100 % of measured capacity (1 s per load); mix "
+                        "60 % render requests (batched-workload distribution), 20 % Collatz batches 2^16-2^22, "
+                        "20 % Fibonacci batches 2^16-2^20",
+            "value": full["msamples_s"],
+            "unit": "Msamples/s at 100 % offered load",
+            "p50_ms": full["p50_ms"],
+            "p99_ms": full["p99_ms"],
+            "fraction_of_capacity": round(full["msamples_s"] / sv["regroup"]["capacity_msamples_s"], 4),
+            "regroup": sv["regroup"],
+            "plain": sv["plain"],
+            "parity": sv["regroup"].pop("parity", None),
+            "clocks": sv_clk,
         }
-        fa.close()
-
-    e2e_s, e2e_ok, h2d, d2h = w.e2e(api, torch, args.steps, warmup, dist)
-    e2e_s = max_over_ranks(e2e_s, dist)
+        torch.cuda.set_stream(stream)
 
     if rank != 0:
         if dist is not None:
@@ -1188,88 +1504,76 @@ def main() -> None:
         peaks = json.loads(pk.read_text())
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    sm_mhz = (clocks or {}).get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
 
-    ms_step = ms_r / args.steps
-    value = world * w.n / (ms_step / 1e3) / 1e6
-    plain_ms = res["plain"]["ms"] / args.steps
-    plain_value = world * w.n / (plain_ms / 1e3) / 1e6
-    sr = res["regroup"]["stats"]
-    sp = res["plain"]["stats"]
+    kern_ms = rg["kernel_ms"]
+    vm_instr = rg["stats"]["thread_instr"]  # one counted launch: VM instructions summed over threads
+    roof = issue_roofline(vm_instr, kern_ms, sm_mhz)
+    traffic, sass = ncu_rooflines(w, kern_ms, sm_mhz)
     # algorithmic bytes of one megakernel launch: inputs, outputs, table and
     # the queue state the engine moved (saves + restores, counted in-kernel)
-    state_per_launch = st_r["state_bytes"] / max(1, st_r["launches"])
-    algo_bytes = w.n * (w.in_bytes + w.out_bytes) + state_per_launch
-    achieved = algo_bytes / (kern_ms / 1e3) / 1e9
-
-    traffic, issue = ncu_rooflines(
-        w, kern_ms, clk.summary().get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    algo_bytes = w.n * (w.in_bytes + w.out_bytes) + rg["state_bytes"]
+    hbm = algo_bytes / (kern_ms / 1e3) / 1e9
+    roof.update(
+        {
+            "bound": "simt_issue",
+            "vm_instructions_per_launch": int(vm_instr),
+            "vm_instructions_per_thread": round(vm_instr / w.n, 1),
+            "kernel_ms": round(kern_ms, 4),
+            "sm_mhz": sm_mhz,
+            "peak_source": "32 lanes x 148 SMs x 4 schedulers x 1 warp instruction per cycle at the sampled SM clock",
+            "traffic": traffic,
+            "hbm": {
+                "achieved": round(hbm, 2),
+                "peak": hbm_peak,
+                "unit": "GB/s",
+                "frac": round(hbm / hbm_peak, 5),
+                "algorithmic_bytes": int(algo_bytes),
+                "traffic": traffic,
+                "peak_source": peak_src,
+            },
+            "note": "VM instructions = Loom Compute/Jump/ParmJump executed, summed over Loom threads, counted "
+                    "in-kernel; the issue roofline in SASS warp instructions and the DRAM traffic come from the "
+                    "ncu capture named in profiles/roofline_traffic.json",
+        }
     )
-
-    cpu, parity = None, {"sample_threads": int(len(tids)), "checked_against": None}
-    plain_regroup_same = same_bits(res["plain"]["out"], out_r)
-    parity["plain_equals_regroup"] = bool(plain_regroup_same)
-    parity["e2e_equals_device"] = bool(e2e_ok)
-    if not args.no_cpu:
-        v, info, want = cpu_reference(w, check_tids=tids)
-        cpu = dict(info, value=round(v, 3))
-        parity["checked_against"] = info["kind"]
-        parity["regroup_ok"] = bool(same_bits(out_r, want, w.kernel))
-        parity["plain_ok"] = bool(same_bits(res["plain"]["out"], want, w.kernel))
-        if w.kernel in ULP_TOLERANCE:
-            parity["float_tolerance_ulp"] = ULP_TOLERANCE[w.kernel]
+    roof = {"bound": roof.pop("bound"), **roof}
 
     line = base_line(args, warmup, world, w.desc, w.kernel, w.dtype, METRIC, extra)
     line.update(
         {
-            "value": round(value, 3),
-            "ms_per_step": round(ms_step, 4),
-            "plain": {
-                "value": round(plain_value, 3),
-                "ms_per_step": round(plain_ms, 4),
-                "lane_efficiency": round(sp["lane_efficiency"], 4),
-            },
+            "value": summary["value"],
+            "ms_per_step": summary["ms_per_step"],
+            "plain": summary["plain"],
             "regroup": {
                 "kernel_ms": round(kern_ms, 4),
-                "lane_efficiency": round(sr["lane_efficiency"], 4),
-                "rounds": int(st_r["rounds"] / max(1, st_r["launches"])),
-                "parks_per_thread": round(st_r["parks"] / max(1, st_r["launches"]) / w.n, 4),
-                "state_bytes_per_launch": int(state_per_launch),
-                "graph_launches": int(st_r.get("graph_launches", 0)),
+                "lane_efficiency": summary["lane_efficiency"],
+                "rounds": int(rg["rounds"]),
+                "parks_per_thread": round(rg["parks"] / w.n, 4),
+                "state_bytes_per_launch": int(rg["state_bytes"]),
+                "device_bytes": int(rg["device_bytes"]),
             },
-            "speedup_regroup_vs_plain": round(plain_ms / ms_step, 4),
-            "regroup_majority_cost_model": (
-                dict(alt, speedup_vs_plain=round(plain_ms / alt["ms_per_step"], 4)) if alt else None
-            ),
-            "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel counters of a profiled launch",
-            "parity": parity,
-            "roofline": {
-                "bound": "hbm",
-                "achieved": round(achieved, 2),
-                "peak": hbm_peak,
-                "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 5),
-                "traffic": traffic,
-                "algorithmic_bytes": int(algo_bytes),
-                "peak_source": peak_src,
-                "note": "algorithmic bytes = outputs + inputs + queue-state saves/restores of the regrouping megakernel; the engine is SIMT issue/latency bound, not HBM bound (profiles/)",
-            },
-            "issue_roofline": issue,
+            "speedup_regroup_vs_plain": summary["speedup_vs_plain"],
+            "lane_efficiency_note": "VM instructions executed / (32 x VM instructions issued per warp), in-kernel "
+                                    "counters of a profiled launch; the SASS-level figure (ncu) in sass_issue",
+            "parity": summary["parity"],
+            "roofline": roof,
+            "sass_issue": sass,
             "cpu_baseline": cpu,
-            "e2e": {
-                "value": round(world * w.n * args.steps / e2e_s / 1e6, 3),
-                "unit": "Msamples/s",
-                "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h),
-            },
-            "gpu_launches": 2 * args.steps,
-            "clocks": clk.summary(),
+            "e2e": {k: v for k, v in e2e.items() if k != "equals_device"},
+            "gpu_launches": w.launches_per_step * args.steps,
+            "clocks": clocks,
         }
     )
+    for k in ("majority_cost_model", "lane_efficiency_form"):
+        if k in summary:
+            line[k] = summary[k]
+    line["parity"]["e2e_equals_device"] = e2e["equals_device"]
+    if configs:
+        line["configs"] = configs
     print(json.dumps(line))
     if args.csv:
         append_csv(args.csv, line)
-    for r in res.values():
-        r["fn"].close()
     if dist is not None:
         dist.destroy_process_group()
 

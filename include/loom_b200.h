@@ -81,6 +81,7 @@ typedef struct loom_b200_kernel_info
 } loom_b200_kernel_info;
 
 /* Execution form. */
+#define LOOM_B200_PERIOD_UNBOUNDED 0xffffffffu /* opts.period: no period limit */
 #define LOOM_B200_PLAIN 0u   /* one CUDA thread per Loom thread, hardware reconvergence */
 #define LOOM_B200_REGROUP 1u /* persistent megakernel, threads regrouped by PC */
 
@@ -92,7 +93,12 @@ typedef struct loom_b200_opts
     uint32_t utr_lanes;   /* regroup: keep running in registers while the
                              largest same-PC group has >= utr_lanes lanes
                              (the GPU form of Loom's UTR, simd.hpp:3273-3292) */
-    uint32_t period;      /* regroup: max block steps per tile per round */
+    uint32_t period;      /* regroup: max block steps per tile per round;
+                             LOOM_B200_PERIOD_UNBOUNDED with schedule 2: a
+                             warp never parks, so the launch runs one round,
+                             admits every input at once and needs no queue
+                             state (a few KB instead of 2 x row bytes per
+                             thread in flight) */
     uint32_t burst;       /* regroup: blocks a lane runs between two votes */
     uint32_t spread_lanes; /* regroup: when the majority block holds at least
                               this many lanes, every live lane runs the
@@ -124,6 +130,13 @@ typedef struct loom_b200_opts
                              catch up and merge; 2 steps one block at a time
                              in that order without votes or parking (a
                              reconvergence stack in software, plus refill) */
+    uint32_t host_chunks; /* launch_host: split the threads into this many
+                             ranges whose host copies overlap the kernels of
+                             the neighbouring ranges (0 = 8 ranges when the
+                             copies reach 32 MB, else 1) */
+    uint32_t max_regs;    /* regroup: registers per thread of the megakernel,
+                             one of the caps compiled for the kernel
+                             (loom_b200_kernel_reg_caps); 0 = its default */
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */
@@ -185,6 +198,10 @@ const char* loom_b200_error_string(int code);
 int         loom_b200_kernel_count(void);
 int         loom_b200_kernel_get(int index, const loom_b200_kernel_info** info);
 int         loom_b200_kernel_find(const char* name, const loom_b200_kernel_info** info);
+/* Register caps compiled for the kernel's regrouping megakernel (values for
+ * opts.max_regs), the default first: *num_caps receives their number, up to
+ * max_caps of them go to caps. */
+int         loom_b200_kernel_reg_caps(const char* kernel, uint32_t* caps, uint32_t max_caps, uint32_t* num_caps);
 /* Finds a compiled kernel by the structural digest of its IR (16 hex
  * digits, loom_b200/frontend/ir_emit.hpp: structural_digest): how the C++
  * front end binds a Loom kernel type to its compiled code. */
@@ -227,12 +244,47 @@ int loom_b200_launch_device(loom_b200_handle* h, const loom_b200_launch* L, void
 
 /* General launch on host memory: array inputs, outputs, instance_starts and
  * the table are host arrays; the call copies them in, runs the kernel,
- * copies the outputs back and returns after they arrived. */
+ * copies the outputs back and returns after they arrived.  Large copies
+ * are pipelined (opts.host_chunks): the threads run as consecutive ranges,
+ * and while range k runs, the inputs of range k + 1 go in and the outputs
+ * of range k - 1 come back (pinned host memory lets the copies overlap). */
 int loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L);
+
+/* Per-group means of float outputs: for launches whose threads are samples
+ * of one result, e.g. a render request with one thread per pixel-sample and
+ * `group` samples per pixel, which Loom's render path turns into an image
+ * (src/benchmarks/render.hpp:223-230).  Output row r is the mean of threads
+ * r * group .. r * group + group - 1, summed in thread order and divided by
+ * the group size, in the output's own float type.  With instance_group,
+ * instance i's rows cover instance_group[i] threads each and follow the rows
+ * of instance i - 1 (each instance's thread count must be a multiple of its
+ * group). */
+typedef struct loom_b200_mean
+{
+    uint32_t        group;          /* threads per row (without instance_group) */
+    uint32_t        pad;
+    const uint32_t* instance_group; /* threads per row of each instance (host), or NULL */
+} loom_b200_mean;
+
+/* loom_b200_launch_host whose outputs are the group means of `M`: every
+ * output must be f32 or f64, and the host output arrays hold one row per
+ * group.  Only the rows are copied back. */
+int loom_b200_launch_host_mean(loom_b200_handle* h, const loom_b200_launch* L, const loom_b200_mean* M);
+
+/* The same reduction of one device column of `type` (LOOM_B200_F32 or
+ * LOOM_B200_F64) with a uniform group: out[r] for r < rows from
+ * in[r * group ...]; asynchronous on `stream`. */
+int loom_b200_group_mean(uint32_t type, const void* in, void* out, uint64_t rows, uint32_t group, void* stream);
 
 int loom_b200_sync(loom_b200_handle* h);
 int loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats);
 int loom_b200_reset_stats(loom_b200_handle* h);
+/* Device memory the handle holds now: its staging columns, the regrouping
+ * engine's queues with their state, control words, counters and the copies
+ * of instance offsets and table made by launch_host.  Loom's facades size
+ * their device columns by the stream size (src/vm/cuda.hpp:86-118); this is
+ * the figure a caller budgets against. */
+int loom_b200_device_bytes(const loom_b200_handle* h, uint64_t* bytes);
 /* Per basic block, over the profiled launches (opts.profile) since the last
  * reset: VM instructions executed summed over threads, and issued summed
  * over warp steps (lane efficiency of block b = thread_instr[b] / (32 *

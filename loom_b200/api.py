@@ -52,8 +52,10 @@ STATUS_STEP_LIMIT = 1
 STATUS_ASSERT_FP = 2
 STATUS_QUEUE_OVERRUN = 4
 STATUS_BARRIER_TIMEOUT = 8
+PERIOD_UNBOUNDED = 0xFFFFFFFF  # opts.period: schedule 2 never parks
 
 TYPE_NAMES = ["b8", "i8", "u8", "i16", "u16", "i32", "u32", "i64", "u64", "f32", "f64"]
+F32, F64 = 9, 10  # enum loom_b200_type
 NP_TYPE = {
     "b8": np.uint8,
     "i8": np.int8,
@@ -113,6 +115,8 @@ class Opts(ctypes.Structure):
         ("barrier_spins", ctypes.c_uint64),
         ("cost_model", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32),
+        ("host_chunks", ctypes.c_uint32),
+        ("max_regs", ctypes.c_uint32),
     ]
 
 
@@ -152,6 +156,14 @@ class LaunchC(ctypes.Structure):
         ("pad", ctypes.c_uint32),
         ("table", ctypes.c_void_p),
         ("table_words", ctypes.c_uint64),
+    ]
+
+
+class MeanC(ctypes.Structure):
+    _fields_ = [
+        ("group", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("instance_group", ctypes.POINTER(ctypes.c_uint32)),
     ]
 
 
@@ -234,6 +246,7 @@ EXPORTS = [
     "loom_b200_kernel_get",
     "loom_b200_kernel_find",
     "loom_b200_kernel_find_digest",
+    "loom_b200_kernel_reg_caps",
     "loom_b200_create",
     "loom_b200_destroy",
     "loom_b200_set_opts",
@@ -242,9 +255,12 @@ EXPORTS = [
     "loom_b200_run_device",
     "loom_b200_launch_device",
     "loom_b200_launch_host",
+    "loom_b200_launch_host_mean",
+    "loom_b200_group_mean",
     "loom_b200_sync",
     "loom_b200_get_stats",
     "loom_b200_reset_stats",
+    "loom_b200_device_bytes",
     "loom_b200_get_block_stats",
     "loom_b200_kernel_queues",
     "loom_b200_parked_counts",
@@ -280,6 +296,12 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_kernel_get.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
     L.loom_b200_kernel_find.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
     L.loom_b200_kernel_find_digest.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.POINTER(KernelInfoC))]
+    L.loom_b200_kernel_reg_caps.argtypes = [
+        ctypes.c_char_p,
+        ctypes.POINTER(ctypes.c_uint32),
+        ctypes.c_uint32,
+        ctypes.POINTER(ctypes.c_uint32),
+    ]
     L.loom_b200_create.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(Opts), ctypes.POINTER(vp)]
     L.loom_b200_destroy.argtypes = [vp]
     L.loom_b200_set_opts.argtypes = [vp, ctypes.POINTER(Opts)]
@@ -288,9 +310,12 @@ def lib() -> ctypes.CDLL:
     L.loom_b200_run_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.c_uint64, vp]
     L.loom_b200_launch_device.argtypes = [vp, ctypes.POINTER(LaunchC), vp]
     L.loom_b200_launch_host.argtypes = [vp, ctypes.POINTER(LaunchC)]
+    L.loom_b200_launch_host_mean.argtypes = [vp, ctypes.POINTER(LaunchC), ctypes.POINTER(MeanC)]
+    L.loom_b200_group_mean.argtypes = [ctypes.c_uint32, vp, vp, ctypes.c_uint64, ctypes.c_uint32, vp]
     L.loom_b200_sync.argtypes = [vp]
     L.loom_b200_get_stats.argtypes = [vp, ctypes.POINTER(StatsC)]
     L.loom_b200_reset_stats.argtypes = [vp]
+    L.loom_b200_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     L.loom_b200_get_block_stats.argtypes = [
         vp,
         ctypes.POINTER(ctypes.c_uint64),
@@ -417,6 +442,22 @@ def queues(kernel: str) -> List[Dict]:
     return out
 
 
+def group_mean(inp, out, rows: int, group: int, stream=None) -> None:
+    """Per-group means of one device float column (loom_b200_group_mean):
+    out[r] = mean of inp[r * group : (r + 1) * group], summed in order."""
+    t = {4: F32, 8: F64}[inp.element_size()] if hasattr(inp, "element_size") else F32
+    s = getattr(stream, "cuda_stream", stream)
+    check(lib().loom_b200_group_mean(t, _ptr(inp), _ptr(out), rows, group, s))
+
+
+def reg_caps(kernel: str) -> List[int]:
+    """Register caps compiled for the kernel's megakernel, default first."""
+    caps = (ctypes.c_uint32 * 16)()
+    n = ctypes.c_uint32()
+    check(lib().loom_b200_kernel_reg_caps(kernel.encode(), caps, 16, ctypes.byref(n)))
+    return [int(caps[i]) for i in range(min(16, n.value))]
+
+
 def info(kernel: str) -> KernelInfo:
     p = ctypes.POINTER(KernelInfoC)()
     check(lib().loom_b200_kernel_find(kernel.encode(), ctypes.byref(p)))
@@ -441,6 +482,8 @@ def make_opts(
     graph: bool = False,
     cost_model: bool = False,
     schedule: int = 0,
+    host_chunks: int = 0,
+    max_regs: int = 0,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -462,6 +505,8 @@ def make_opts(
         barrier_spins=barrier_spins,
         cost_model=1 if cost_model else 0,
         schedule=int(schedule),
+        host_chunks=int(host_chunks),
+        max_regs=int(max_regs),
     )
 
 
@@ -574,6 +619,31 @@ class Function:
         del keep
         return outs[0] if len(outs) == 1 else tuple(outs)
 
+    def launch_host_mean(self, inputs, n: int, group: int = 0, instance_group=None, instance_starts=None,
+                         table=None, outputs=None):
+        """`launch_host` whose outputs are per-group means (loom_b200_launch_host_mean):
+        one row per `group` consecutive threads, or per instance_group[i]
+        threads of instance i.  `outputs` may be given (host arrays or
+        pointers of the row count); returns them."""
+        if instance_starts is not None:
+            instance_starts = np.ascontiguousarray(instance_starts, dtype=np.uint64)
+        if table is not None:
+            table = np.ascontiguousarray(table, dtype=np.uint32)
+        ig = None
+        if instance_group is not None:
+            ig = np.ascontiguousarray(instance_group, dtype=np.uint32)
+            starts = np.asarray(instance_starts, dtype=np.uint64)
+            rows = int(((starts[1:] - starts[:-1]) // ig).sum())
+        else:
+            rows = n // group if group else 0
+        if outputs is None:
+            outputs = [np.empty(rows, dtype=NP_TYPE[t]) for _, t in self.info.outputs]
+        L, keep = self._launch_struct(inputs, outputs, n, instance_starts, table)
+        M = MeanC(group, 0, None if ig is None else ig.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        check(lib().loom_b200_launch_host_mean(self._h, ctypes.byref(L), ctypes.byref(M)))
+        del keep
+        return outputs
+
     def launch_device(self, inputs, outputs, n: int, instance_starts=None, table=None, stream=None):
         """General asynchronous launch; every array is device memory (torch
         tensors or raw pointers)."""
@@ -598,6 +668,12 @@ class Function:
 
     def reset_stats(self) -> None:
         check(lib().loom_b200_reset_stats(self._h))
+
+    def device_bytes(self) -> int:
+        """Device memory the handle holds (columns, queues, control words)."""
+        b = ctypes.c_uint64()
+        check(lib().loom_b200_device_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
 
     def block_stats(self) -> List[Dict[str, float]]:
         """Per basic block over the profiled launches since the last reset:

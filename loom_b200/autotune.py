@@ -5,8 +5,10 @@ on its inputs: how many lanes must agree before a warp keeps running
 (`utr_lanes`), how long a lane runs between votes (`burst`), when every live
 lane runs along (`spread_lanes`), how many block steps a tile gets per round
 (`period`), the threads in flight (`population`, which sizes every work
-queue), the CTA size, the CTAs per SM (the register budget a thread can
-use: fewer CTAs leave more registers per thread) and input prefetching.
+queue), the CTA size, the CTAs per SM, the megakernel's register cap
+(`max_regs`, one of the caps compiled for the kernel: more registers per
+thread mean fewer spills but fewer resident warps to hide latency) and
+input prefetching.
 
 `tune` runs a coordinate search: starting from a seed point it tries every
 value of one option with the others fixed, keeps the fastest, moves to the
@@ -14,7 +16,10 @@ next option, and repeats the sweep until a pass brings less than 1 %.  With
 several seeds (the stored point, the defaults with and without the cost
 model) it searches from each and keeps the fastest point found.
 Every point is timed on the device with CUDA events on the launching
-stream (median of `reps` launches after one warm-up launch).  Results are
+stream (median of `reps` launches after one warm-up launch).  An optional
+constraint (for instance a lane efficiency of at least some fraction,
+measured by a counted launch) makes the points that miss it ineligible, so
+the search returns the fastest point that meets it.  Results are
 kept in `tuning.json` beside this module, per kernel and workload, and read
 back by `tuned`.
 """
@@ -34,16 +39,21 @@ SPACE: Dict[str, List] = {
     "burst": [1, 2, 4, 8, 16, 32, 64],
     "utr_lanes": [1, 4, 8, 12, 16, 20, 24],
     "spread_lanes": [1, 8, 16, 24, 33],
-    "period": [256, 1024, 4096, 16384, 65536, 1 << 20],
+    # 0xffffffff: no period limit (schedule 2 then never parks)
+    "period": [256, 1024, 4096, 16384, 65536, 1 << 20, 0xFFFFFFFF],
     "block_size": [128, 256, 512],
     "population": [1 << 18, 1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23],
     "ctas_per_sm": [0, 1, 2, 4],
     "prefetch": [True, False],
     "cost_model": [False, True],
     "schedule": [0, 1, 2],
+    # 0: the kernel's default cap; the others exist only for kernels large
+    # enough to reach a cap (loom_b200_kernel_reg_caps), which the caller
+    # passes as this option's values
+    "max_regs": [0],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:
@@ -75,10 +85,13 @@ def tune(
     budget_s: float = 600.0,
     log: Optional[Callable[[str], None]] = None,
     validate: Optional[Callable[[], None]] = None,
+    constraint: Optional[Callable[[Dict], bool]] = None,
 ) -> Dict:
     """Coordinate search.  `make_launch(opts)` returns a no-argument callable
     that launches the workload once with those options; `validate()`, called
-    after each timed point, raises when the launches set a device status.
+    after each timed point, raises when the launches set a device status;
+    `constraint(opts)`, called after timing, returns False for a point that
+    may not be chosen (it is recorded with "eligible": false).
     Returns {"best": opts, "ms": t, "points": [...]}."""
     space = dict(SPACE if space is None else space)
     seeds = [DEFAULT] if seed is None else (list(seed) if isinstance(seed, (list, tuple)) else [seed])
@@ -95,10 +108,14 @@ def tune(
                 ms = time_launch(make_launch(opts), reps)
                 if validate:
                     validate()
-                cache[key] = ms
-                points.append({"opts": dict(opts), "ms": round(ms, 4), "msamples_s": round(n_threads / ms / 1e3, 3)})
+                ok = constraint(opts) if constraint else True
+                cache[key] = ms if ok else float("inf")
+                pt = {"opts": dict(opts), "ms": round(ms, 4), "msamples_s": round(n_threads / ms / 1e3, 3)}
+                if not ok:
+                    pt["eligible"] = False
+                points.append(pt)
                 if log:
-                    log(f"{ms:9.3f} ms  {opts}")
+                    log(f"{ms:9.3f} ms  {opts}" + ("" if ok else "  (constraint not met)"))
         return cache[key]
 
     overall, overall_ms = None, float("inf")
@@ -122,6 +139,8 @@ def tune(
                 break
         if best < overall_ms:
             overall, overall_ms = cur, best
+    if overall is None or overall_ms == float("inf"):
+        raise RuntimeError("no point met the constraint")
     return {
         "best": overall,
         "ms": round(overall_ms, 4),
@@ -149,7 +168,7 @@ def store(kernel: str, workload: str, result: Dict, device: str = "", keep_point
         "ms": result["ms"],
         "msamples_s": result["msamples_s"],
         "device": device,
-        "points": sorted(result["points"], key=lambda p: p["ms"])[:keep_points],
+        "points": sorted(result["points"], key=lambda p: (not p.get("eligible", True), p["ms"]))[:keep_points],
     }
     data.setdefault(kernel, {})[workload] = entry
     TUNING_FILE.write_text(json.dumps(data, indent=1, sort_keys=True) + "\n")

@@ -2,8 +2,8 @@
 nvcc compilation for sm_100a.
 
 Steps
-  1. extract  (only where the Loom headers are available, LOOM_REF_DIR or the
-              default location): one small g++ program per registry kernel
+  1. extract  (only where the Loom headers are available, LOOM_REF_DIR or
+              ../reference beside this repository): one small g++ program per registry kernel
               prints its IR; loom_b200/ir/*.lir are written for kernels that
               have none, for all with --reextract (after a kernel changed);
   2. generate loom_b200/csrc/gen/<kernel>.cu for every .lir file;
@@ -54,7 +54,7 @@ NVCC_FLAGS = [
 def default_ref_dir() -> Optional[pathlib.Path]:
     env = os.environ.get("LOOM_REF_DIR")
     cands = [pathlib.Path(env)] if env else []
-    cands.append(pathlib.Path("/root/reference"))
+    cands.append(ROOT.parent / "reference")
     for c in cands:
         if (c / "src" / "vm" / "core.hpp").is_file():
             return c

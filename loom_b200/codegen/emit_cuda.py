@@ -52,6 +52,19 @@ from .ir import (
 # render requests 156.6 ms vs 180.4 ms, outputs identical.
 REGROUP_MAX_REGS = 64
 
+# Further register caps compiled for kernels large enough to reach the cap
+# (more static instructions than REG_VARIANT_MIN_INSTR): the tuner picks one
+# per workload (opts.max_regs), trading warps per SM against spills.
+REG_VARIANTS = (32, 40, 48, 56, 80, 96, 128)
+REG_VARIANT_MIN_INSTR = 300
+
+
+def reg_caps(k: Kernel) -> List[int]:
+    """Register caps of the megakernel compiled for `k`, default first."""
+    if sum(k.instr_counts()) <= REG_VARIANT_MIN_INSTR:
+        return [REGROUP_MAX_REGS]
+    return [REGROUP_MAX_REGS] + [c for c in REG_VARIANTS if c != REGROUP_MAX_REGS]
+
 CTYPE = {
     "b8": "bool",
     "i8": "signed char",
@@ -575,25 +588,43 @@ def generate(k: Kernel) -> str:
     w("    if(grid == 0) return cudaSuccess;")
     w("    if(a.profile)")
     w("        plain_kernel<K, true><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(")
-    w("            a.cols, a.n, a.max_steps, a.status, a.counters);")
+    w("            a.cols, a.first, a.n, a.max_steps, a.status, a.counters);")
     w("    else")
     w("        plain_kernel<K, false><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(")
-    w("            a.cols, a.n, a.max_steps, a.status, a.counters);")
+    w("            a.cols, a.first, a.n, a.max_steps, a.status, a.counters);")
     w("    return cudaGetLastError();")
+    w("}")
+    w("")
+    caps = reg_caps(k)
+    w(f"const unsigned kRegCaps[] = {{{', '.join(f'{c}u' for c in caps)}}};")
+    w("")
+    w("/// The megakernel at register cap `regs` (0: the default); profiled")
+    w("/// launches use the default cap.  NULL: no such cap compiled.")
+    w("const void* regroup_fn(unsigned regs, bool profile)")
+    w("{")
+    w("    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs>);")
+    w("    switch(regs)")
+    w("    {")
+    w("    case 0u:")
+    for c in caps:
+        w(f"    case {c}u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, {c}>);")
+    w("    default: return nullptr;")
+    w("    }")
     w("}")
     w("")
     w("cudaError_t launch_regroup(const RegroupLaunch& a)")
     w("{")
     w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
-    w("    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)")
-    w("                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);")
+    w("    const void* fn = regroup_fn(a.regs, a.profile);")
+    w("    if(!fn) return cudaErrorInvalidValue;")
     w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
     w("}")
     w("")
-    w("cudaError_t regroup_occupancy(int block, bool profile, int* ctas)")
+    w("cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)")
     w("{")
-    w("    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)")
-    w("                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);")
+    w("    const void* fn = regroup_fn(regs, profile);")
+    w("    if(!fn) return cudaErrorInvalidValue;")
+    w("    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);")
     w("}")
     w("")
     w(f"}} }} // namespace loom_b200::k_{name}")
@@ -603,7 +634,8 @@ def generate(k: Kernel) -> str:
     w(f"    &loom_b200::k_{name}::kInfo, loom_b200::k_{name}::K::kRowBytes, {nq},")
     w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
     w(f"    &loom_b200::k_{name}::regroup_occupancy,")
-    w(f"    loom_b200::k_{name}::kQueues, loom_b200::k_{name}::kSegments}};")
+    w(f"    loom_b200::k_{name}::kQueues, loom_b200::k_{name}::kSegments,")
+    w(f"    loom_b200::k_{name}::kRegCaps, {len(caps)}u}};")
     return "\n".join(o) + "\n"
 
 

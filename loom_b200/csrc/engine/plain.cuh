@@ -11,24 +11,28 @@
 
 namespace loom_b200
 {
-/// Launch: grid = ceil(n / blockDim.x), thread tid runs Loom thread tid.
-/// Inputs are read once, outputs written once, registers live in CUDA
-/// registers; counters[0..1] receive thread/warp VM-instruction totals when
-/// kProf is set (lane efficiency = counters[0] / (32 * counters[1])).
+/// Launch: grid = ceil(n / blockDim.x), CUDA thread i runs Loom thread
+/// first + i (Loom threads [first, first + n); inputs and outputs are
+/// indexed by the Loom thread id).  Inputs are read once, outputs written
+/// once, registers live in CUDA registers; counters[0..1] receive
+/// thread/warp VM-instruction totals when kProf is set (lane efficiency =
+/// counters[0] / (32 * counters[1])).
 template <typename K, bool kProf>
 __global__ void
 plain_kernel(const Columns                  cols,
+             const unsigned long long       first,
              const unsigned long long       n,
              const unsigned long long       max_steps,
              unsigned* __restrict__         status,
              unsigned long long* __restrict__ counters)
 {
-    const unsigned long long tid =
+    const unsigned long long i =
         static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const unsigned long long tid = first + i;
     __shared__ unsigned long long s_blk[2 * (kProf ? K::kNumBlocks : 1)];
     Ctx ctx{0ull, 0ull, status, &cols, kProf ? s_blk : nullptr};
     if constexpr(kProf) block_counters_clear(s_blk, K::kNumBlocks);
-    if(tid < n)
+    if(i < n)
     {
         typename K::Regs R;
         K::load_inputs(R, cols, tid);

@@ -68,7 +68,7 @@ struct RegroupParams
     unsigned long long  barrier_spins;
     unsigned            cap;      // population: entries per queue, multiple of 32
     unsigned            utr;      // majority quorum, lanes
-    unsigned            period;   // block steps per tile per round
+    unsigned            period;   // block steps per tile per round (LOOM_B200_PERIOD_UNBOUNDED: none)
     unsigned            burst;    // blocks a lane runs between two votes
     unsigned            spread;   // majority size from which all live lanes run
     unsigned            prefetch; // prefetch the next input of every lane
@@ -174,11 +174,11 @@ claim_inputs(const unsigned need, RegroupCtl* ctl, unsigned long long admit_end,
     return ((need >> lane) & 1u) && t < admit_end ? t : ~0ull;
 }
 
-/// The megakernel.  `__maxnreg__` holds it to the kernel's register cap
-/// (`K::kRegroupMaxRegs`) so that enough warps stay resident to hide the
-/// latency of the lanes it keeps running.
-template <typename K, bool kProf>
-__global__ void __maxnreg__(K::kRegroupMaxRegs)
+/// The megakernel.  `__maxnreg__` holds it to a register cap (`kRegs`, by
+/// default `K::kRegroupMaxRegs`) so that enough warps stay resident to hide
+/// the latency of the lanes it keeps running.
+template <typename K, bool kProf, int kRegs = K::kRegroupMaxRegs>
+__global__ void __maxnreg__(kRegs)
 regroup_kernel(const RegroupParams p)
 {
     constexpr int      B    = K::kNumQueues;
@@ -287,7 +287,7 @@ regroup_kernel(const RegroupParams p)
                 }
                 else if(pc >= 0 && (mc >= p.spread || pc == m))
                     pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
-                steps += p.burst;
+                if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
                 {
@@ -319,6 +319,10 @@ regroup_kernel(const RegroupParams p)
                 if(steps >= p.period) break;
                 if(p.schedule == 2u)
                 {
+                    // a lane left empty by a refill that found no input
+                    // takes its prefetched one, so a warp leaves the loop
+                    // with no input claimed and none parked
+                    if(pc == kEmpty && pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
                     // no quorum: the warp keeps its lanes until the period
                     // ends or none is left
                     if(__ballot_sync(FULL, pc >= 0) == 0u) break;

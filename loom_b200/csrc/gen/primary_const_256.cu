@@ -3061,25 +3061,48 @@ cudaError_t launch_plain(const PlainLaunch& a)
     if(grid == 0) return cudaSuccess;
     if(a.profile)
         plain_kernel<K, true><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(
-            a.cols, a.n, a.max_steps, a.status, a.counters);
+            a.cols, a.first, a.n, a.max_steps, a.status, a.counters);
     else
         plain_kernel<K, false><<<static_cast<unsigned>(grid), a.block, 0, a.stream>>>(
-            a.cols, a.n, a.max_steps, a.status, a.counters);
+            a.cols, a.first, a.n, a.max_steps, a.status, a.counters);
     return cudaGetLastError();
+}
+
+const unsigned kRegCaps[] = {64u, 32u, 40u, 48u, 56u, 80u, 96u, 128u};
+
+/// The megakernel at register cap `regs` (0: the default); profiled
+/// launches use the default cap.  NULL: no such cap compiled.
+const void* regroup_fn(unsigned regs, bool profile)
+{
+    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs>);
+    switch(regs)
+    {
+    case 0u:
+    case 64u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 64>);
+    case 32u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 32>);
+    case 40u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 40>);
+    case 48u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 48>);
+    case 56u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 56>);
+    case 80u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 80>);
+    case 96u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 96>);
+    case 128u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 128>);
+    default: return nullptr;
+    }
 }
 
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    const void* fn = a.profile ? reinterpret_cast<const void*>(&regroup_kernel<K, true>)
-                               : reinterpret_cast<const void*>(&regroup_kernel<K, false>);
+    const void* fn = regroup_fn(a.regs, a.profile);
+    if(!fn) return cudaErrorInvalidValue;
     return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
 {
-    return profile ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, true>, block, 0)
-                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, &regroup_kernel<K, false>, block, 0);
+    const void* fn = regroup_fn(regs, profile);
+    if(!fn) return cudaErrorInvalidValue;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
 }
 
 } } // namespace loom_b200::k_primary_const_256
@@ -3089,4 +3112,5 @@ const loom_b200::KernelEntry loom_b200_entry_primary_const_256 = {
     &loom_b200::k_primary_const_256::kInfo, loom_b200::k_primary_const_256::K::kRowBytes, 33,
     &loom_b200::k_primary_const_256::launch_plain, &loom_b200::k_primary_const_256::launch_regroup,
     &loom_b200::k_primary_const_256::regroup_occupancy,
-    loom_b200::k_primary_const_256::kQueues, loom_b200::k_primary_const_256::kSegments};
+    loom_b200::k_primary_const_256::kQueues, loom_b200::k_primary_const_256::kSegments,
+    loom_b200::k_primary_const_256::kRegCaps, 8u};

@@ -62,6 +62,7 @@ regroup_reset(RegroupCtl*        ctl,
               unsigned*          qcnt,
               unsigned*          qhead,
               unsigned           num_blocks,
+              unsigned long long first,
               unsigned long long admit_end)
 {
     for(unsigned i = threadIdx.x; i < 3 * num_blocks; i += blockDim.x)
@@ -77,9 +78,47 @@ regroup_reset(RegroupCtl*        ctl,
         ctl->bar_gen   = 0u;
         ctl->done      = 0u;
         ctl->pad0      = 0u;
-        ctl->cursor    = 0ull;
+        ctl->cursor    = first;
         ctl->admit_end = admit_end;
     }
+}
+
+/// Per-group means of a float column, summed in thread order: output row r
+/// of instance i covers threads starts[i] + (r - out_starts[i]) * group[i]
+/// and the group[i] - 1 after it; without instances every row covers
+/// `group` threads from r * group.  One CUDA thread per row.
+template <typename T>
+__global__ void
+group_mean(const T* __restrict__                  in,
+           T* __restrict__                        out,
+           const unsigned long long               rows,
+           const unsigned                         group,
+           const unsigned long long* __restrict__ starts,
+           const unsigned* __restrict__           inst_group,
+           const unsigned long long* __restrict__ out_starts,
+           const unsigned                         num_inst)
+{
+    const unsigned long long r = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if(r >= rows) return;
+    unsigned long long t0 = r * group;
+    unsigned           g  = group;
+    if(num_inst)
+    {
+        unsigned lo = 0, hi = num_inst; // out_starts[lo] <= r < out_starts[hi]
+        while(hi - lo > 1)
+        {
+            const unsigned mid = (lo + hi) >> 1;
+            if(out_starts[mid] <= r)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        g  = inst_group[lo];
+        t0 = starts[lo] + (r - out_starts[lo]) * g;
+    }
+    T acc = T(0);
+    for(unsigned j = 0; j < g; ++j) acc = acc + __ldg(in + t0 + j);
+    out[r] = acc / static_cast<T>(g);
 }
 
 /// Launch counters: 8 totals, then thread and warp instructions per block.
@@ -128,6 +167,12 @@ struct loom_b200_handle
     size_t starts_bytes = 0;
     void*  d_table      = nullptr;
     size_t table_bytes  = 0;
+    // launch_host_mean: the rows of the group means (and their offsets)
+    void*  d_rows       = nullptr;
+    size_t rows_bytes   = 0;
+    // launch_host pipeline: copy streams and one event per stage of a chunk
+    cudaStream_t             s_in = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> chunk_ev;
 
     // CUDA graph of the regrouping launch sequence (opts.graph)
     cudaStream_t    cap_stream   = nullptr;
@@ -164,11 +209,22 @@ round_cap(uint64_t cap)
     return (cap + 31) / 32 * 32;
 }
 
+/// Whether a regrouping launch never parks a thread: schedule 2 with no
+/// period limit keeps every thread in its lane until it halts.
+bool
+never_parks(const loom_b200_opts& o)
+{
+    return o.mode == LOOM_B200_REGROUP && o.schedule == 2u && o.period == LOOM_B200_PERIOD_UNBOUNDED;
+}
+
 /// Threads in flight of a regrouping launch: the requested population, or
-/// as many as the queue state of kDefaultStateBudget bytes holds.
+/// as many as the queue state of kDefaultStateBudget bytes holds.  A launch
+/// that never parks keeps its threads in registers: its queues get one tile
+/// each, which nothing writes, and it admits every input in its one round.
 uint64_t
 population(const loom_b200_handle* h, uint64_t n)
 {
+    if(never_parks(h->opts)) return 32;
     uint64_t p = h->opts.population ? h->opts.population : n;
     const uint64_t fit = kDefaultStateBudget / (2 * h->e->row_bytes) / 32 * 32;
     if(!h->opts.population && fit && p > fit) p = fit;
@@ -248,8 +304,10 @@ finish_launch(loom_b200_handle* h)
 int
 launch_graph(loom_b200_handle* h, const RegroupLaunch& L, uint64_t admit, cudaStream_t stream)
 {
+    const uint64_t first = L.params.cols.tid_base;
     const bool same = h->graph_exec && h->graph_admit == admit && h->graph_key.grid == L.grid &&
                       h->graph_key.block == L.block && h->graph_key.profile == L.profile &&
+                      h->graph_key.regs == L.regs &&
                       std::memcmp(&h->graph_key.params, &L.params, sizeof(RegroupParams)) == 0;
     if(!same)
     {
@@ -270,7 +328,7 @@ launch_graph(loom_b200_handle* h, const RegroupLaunch& L, uint64_t admit, cudaSt
         if(err == cudaSuccess)
         {
             regroup_reset<<<1, 256, 0, h->cap_stream>>>(h->d_ctl, h->d_qcnt, h->d_qhead,
-                                                        h->e->num_queues, admit);
+                                                        h->e->num_queues, first, admit);
             cudaError_t e1 = cudaGetLastError();
             cudaError_t e2 = h->e->regroup(C);
             cudaError_t e3 = cudaStreamEndCapture(h->cap_stream, &g);
@@ -294,9 +352,11 @@ launch_graph(loom_b200_handle* h, const RegroupLaunch& L, uint64_t admit, cudaSt
     return LOOM_B200_OK;
 }
 
-/// Launch with every pointer of `L` on the device.
+/// Launch with every pointer of `L` on the device: Loom threads
+/// [first, first + L.n), inputs and outputs indexed by the thread id.
+/// `graph` allows the regrouping launch to replay a CUDA graph.
 int
-launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
+launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint64_t first = 0, bool graph = true)
 {
     const KernelEntry&           e    = *h->e;
     const loom_b200_kernel_info& info = *e.info;
@@ -340,6 +400,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
     cols.inst_start = reinterpret_cast<const unsigned long long*>(L.instance_starts);
     cols.num_inst   = L.instance_starts ? L.num_instances : 0u;
     cols.table      = L.table;
+    cols.tid_base   = first; // thread ids in flight lie in [first, first + n)
     const loom_b200_opts& o = h->opts;
     if(o.mode == LOOM_B200_REGROUP)
     {
@@ -361,7 +422,13 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         int      ctas  = 0;
         for(;;)
         {
-            LB_CUDA(e.regroup_occupancy(static_cast<int>(block), o.profile != 0, &ctas));
+            const cudaError_t oe = e.regroup_occupancy(static_cast<int>(block), o.profile != 0, o.max_regs, &ctas);
+            if(oe == cudaErrorInvalidValue)
+            {
+                g_last_error = "register cap not compiled for this kernel (loom_b200_kernel_reg_caps)";
+                return LOOM_B200_ERR_INVALID;
+            }
+            LB_CUDA(oe);
             if(ctas > 0 || block <= 32) break;
             block /= 2;
         }
@@ -379,7 +446,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         L.params.ctl           = h->d_ctl;
         L.params.status        = h->d_status;
         L.params.counters      = h->d_counters;
-        L.params.n             = n;
+        L.params.n             = first + n; // end of the thread range
         L.params.max_rounds    = o.max_steps;
         L.params.barrier_spins = o.barrier_spins ? o.barrier_spins : kBarrierSpins;
         L.params.phantoms      = o.fault_phantom_ctas;
@@ -394,12 +461,13 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         L.params.schedule      = o.schedule;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
+        L.regs                 = o.max_regs;
         L.profile              = o.profile != 0;
         L.stream               = stream;
-        const uint64_t admit = std::min<uint64_t>(n, cap);
-        if(!(o.graph && !h->graph_broken && launch_graph(h, L, admit, stream) == LOOM_B200_OK))
+        const uint64_t admit = first + (never_parks(o) ? n : std::min<uint64_t>(n, cap));
+        if(!(graph && o.graph && !h->graph_broken && launch_graph(h, L, admit, stream) == LOOM_B200_OK))
         {
-            regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl, h->d_qcnt, h->d_qhead, e.num_queues, admit);
+            regroup_reset<<<1, 256, 0, stream>>>(h->d_ctl, h->d_qcnt, h->d_qhead, e.num_queues, first, admit);
             LB_CUDA(cudaGetLastError());
             LB_CUDA(e.regroup(L));
         }
@@ -411,6 +479,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream)
         h->last_cap = 0;
         PlainLaunch L{};
         L.cols      = cols;
+        L.first     = first;
         L.n         = n;
         L.max_steps = o.max_steps;
         L.status    = h->d_status;
@@ -572,7 +641,11 @@ loom_b200_destroy(loom_b200_handle* h)
     cudaFree(h->d_counters);
     cudaFree(h->d_starts);
     cudaFree(h->d_table);
+    cudaFree(h->d_rows);
     cudaFree(h->d_ctl);
+    for(cudaEvent_t ev: h->chunk_ev) cudaEventDestroy(ev);
+    if(h->s_in) cudaStreamDestroy(h->s_in);
+    if(h->s_out) cudaStreamDestroy(h->s_out);
     if(h->ev0) cudaEventDestroy(h->ev0);
     if(h->ev1) cudaEventDestroy(h->ev1);
     if(h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
@@ -612,6 +685,57 @@ loom_b200_launch_device(loom_b200_handle* h, const loom_b200_launch* L, void* st
     return launch(h, *L, static_cast<cudaStream_t>(stream));
 }
 
+namespace
+{
+/// Copies the instance offsets and the table of a host launch to the
+/// handle's device buffers on `st` and points `D` at them.
+int
+stage_tables(loom_b200_handle* h, const loom_b200_launch& L, loom_b200_launch& D, cudaStream_t st)
+{
+    if(L.instance_starts)
+    {
+        const size_t bytes = (static_cast<size_t>(L.num_instances) + 1) * sizeof(uint64_t);
+        int rc = grow(&h->d_starts, &h->starts_bytes, bytes);
+        if(rc) return rc;
+        LB_CUDA(cudaMemcpyAsync(h->d_starts, L.instance_starts, bytes, cudaMemcpyHostToDevice, st));
+        D.instance_starts = static_cast<const uint64_t*>(h->d_starts);
+    }
+    if(L.table)
+    {
+        const size_t bytes = L.table_words * sizeof(uint32_t);
+        int rc = grow(&h->d_table, &h->table_bytes, bytes);
+        if(rc) return rc;
+        LB_CUDA(cudaMemcpyAsync(h->d_table, L.table, bytes, cudaMemcpyHostToDevice, st));
+        D.table = static_cast<const uint32_t*>(h->d_table);
+    }
+    return LOOM_B200_OK;
+}
+
+/// Chunks of a host launch: 1 when the host copies are small, else enough
+/// that each chunk's copies overlap the neighbouring chunks' kernels.
+uint64_t
+host_chunks(const loom_b200_handle* h, uint64_t n, uint64_t copy_bytes)
+{
+    uint64_t c = h->opts.host_chunks ? h->opts.host_chunks : (copy_bytes >= (32ull << 20) ? 8 : 1);
+    c = std::min<uint64_t>(c, std::max<uint64_t>(1, n / 1024));
+    return std::max<uint64_t>(c, 1);
+}
+
+int
+ensure_copy_streams(loom_b200_handle* h, size_t events)
+{
+    if(!h->s_in) LB_CUDA(cudaStreamCreateWithFlags(&h->s_in, cudaStreamNonBlocking));
+    if(!h->s_out) LB_CUDA(cudaStreamCreateWithFlags(&h->s_out, cudaStreamNonBlocking));
+    while(h->chunk_ev.size() < events)
+    {
+        cudaEvent_t ev = nullptr;
+        LB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        h->chunk_ev.push_back(ev);
+    }
+    return LOOM_B200_OK;
+}
+} // namespace
+
 int
 loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L)
 {
@@ -626,45 +750,196 @@ loom_b200_launch_host(loom_b200_handle* h, const loom_b200_launch* L)
     if(n == 0) return LOOM_B200_OK;
     const loom_b200_kernel_info& info = *h->e->info;
     std::vector<loom_b200_input> din(L->inputs, L->inputs + info.num_inputs);
+    uint64_t                     per_thread = 0;
+    for(uint32_t i = 0; i < info.num_inputs; ++i)
+        if(din[i].form == LOOM_B200_IN_ARRAY && din[i].ptr) per_thread += type_bytes(info.input_types[i]);
+    for(uint32_t j = 0; j < info.num_outputs; ++j) per_thread += type_bytes(info.output_types[j]);
+    const uint64_t chunks = host_chunks(h, n, n * per_thread);
+
+    // Pipeline of `chunks` ranges of threads: the inputs of range k go in on
+    // s_in, its kernel runs on the handle's stream once they arrived, its
+    // outputs come back on s_out once it finished, so range k's copies
+    // overlap the kernels of ranges k - 1 and k + 1.  One range is the plain
+    // sequence copy in, launch, copy out.
+    if(chunks > 1)
+    {
+        const int rc = ensure_copy_streams(h, 2 * chunks + 1);
+        if(rc) return rc;
+    }
+    cudaStream_t s_in  = chunks > 1 ? h->s_in : h->stream;
+    cudaStream_t s_out = chunks > 1 ? h->s_out : h->stream;
+    loom_b200_launch D = *L;
+    for(uint32_t i = 0; i < info.num_inputs; ++i)
+        if(din[i].form == LOOM_B200_IN_ARRAY && din[i].ptr) din[i].ptr = h->d_in[i];
+    D.inputs  = din.data();
+    D.outputs = h->d_out.data();
+    if(int rc = stage_tables(h, *L, D, s_in)) return rc;
+    const uint64_t step = (n + chunks - 1) / chunks;
+    for(uint64_t k = 0; k < chunks; ++k)
+    {
+        const uint64_t a = k * step, b = std::min<uint64_t>(n, a + step);
+        if(a >= b) break;
+        for(uint32_t i = 0; i < info.num_inputs; ++i)
+            if(L->inputs[i].form == LOOM_B200_IN_ARRAY && L->inputs[i].ptr)
+            {
+                const size_t eb = type_bytes(info.input_types[i]);
+                LB_CUDA(cudaMemcpyAsync(static_cast<char*>(h->d_in[i]) + a * eb,
+                                        static_cast<const char*>(L->inputs[i].ptr) + a * eb,
+                                        (b - a) * eb, cudaMemcpyHostToDevice, s_in));
+            }
+        if(chunks > 1)
+        {
+            LB_CUDA(cudaEventRecord(h->chunk_ev[2 * k], s_in));
+            LB_CUDA(cudaStreamWaitEvent(h->stream, h->chunk_ev[2 * k], 0));
+        }
+        loom_b200_launch C = D;
+        C.n                = b - a;
+        if(int rc = launch(h, C, h->stream, a, chunks == 1)) return rc;
+        if(chunks > 1)
+        {
+            LB_CUDA(cudaEventRecord(h->chunk_ev[2 * k + 1], h->stream));
+            LB_CUDA(cudaStreamWaitEvent(s_out, h->chunk_ev[2 * k + 1], 0));
+        }
+        for(uint32_t j = 0; j < info.num_outputs; ++j)
+        {
+            const size_t eb = type_bytes(info.output_types[j]);
+            LB_CUDA(cudaMemcpyAsync(static_cast<char*>(L->outputs[j]) + a * eb,
+                                    static_cast<const char*>(h->d_out[j]) + a * eb, (b - a) * eb,
+                                    cudaMemcpyDeviceToHost, s_out));
+        }
+    }
+    LB_CUDA(cudaStreamSynchronize(s_out));
+    LB_CUDA(cudaStreamSynchronize(h->stream));
+    return finish_launch(h);
+}
+
+int
+loom_b200_group_mean(uint32_t type, const void* in, void* out, uint64_t rows, uint32_t group, void* stream)
+{
+    if(!in || !out || group == 0 || (type != LOOM_B200_F32 && type != LOOM_B200_F64))
+        return LOOM_B200_ERR_INVALID;
+    if(rows == 0) return LOOM_B200_OK;
+    const unsigned blocks = static_cast<unsigned>((rows + 255) / 256);
+    auto           st     = static_cast<cudaStream_t>(stream);
+    if(type == LOOM_B200_F32)
+        group_mean<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(in), static_cast<float*>(out), rows,
+                                                  group, nullptr, nullptr, nullptr, 0u);
+    else
+        group_mean<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(in), static_cast<double*>(out),
+                                                   rows, group, nullptr, nullptr, nullptr, 0u);
+    LB_CUDA(cudaGetLastError());
+    return LOOM_B200_OK;
+}
+
+int
+loom_b200_launch_host_mean(loom_b200_handle* h, const loom_b200_launch* L, const loom_b200_mean* M)
+{
+    if(!h || !L || !M || (!L->inputs && h->e->info->num_inputs) || !L->outputs)
+        return LOOM_B200_ERR_INVALID;
+    const uint64_t               n    = L->n;
+    const loom_b200_kernel_info& info = *h->e->info;
+    if(n > h->capacity)
+    {
+        g_last_error = "n exceeds the handle's capacity";
+        return LOOM_B200_ERR_INVALID;
+    }
+    for(uint32_t j = 0; j < info.num_outputs; ++j)
+        if(info.output_types[j] != LOOM_B200_F32 && info.output_types[j] != LOOM_B200_F64)
+        {
+            g_last_error = "group means need float outputs";
+            return LOOM_B200_ERR_INVALID;
+        }
+    // output rows: per instance its threads / its group, in instance order
+    std::vector<unsigned long long> out_starts;
+    uint64_t                        rows = 0;
+    if(M->instance_group)
+    {
+        if(!L->instance_starts || L->num_instances == 0)
+        {
+            g_last_error = "instance_group needs instance_starts";
+            return LOOM_B200_ERR_INVALID;
+        }
+        out_starts.resize(L->num_instances + 1);
+        for(uint32_t i = 0; i < L->num_instances; ++i)
+        {
+            const uint64_t t = L->instance_starts[i + 1] - L->instance_starts[i];
+            const uint32_t g = M->instance_group[i];
+            if(g == 0 || t % g != 0)
+            {
+                g_last_error = "an instance's threads are not a multiple of its group";
+                return LOOM_B200_ERR_INVALID;
+            }
+            out_starts[i] = rows;
+            rows += t / g;
+        }
+        out_starts[L->num_instances] = rows;
+        if(L->instance_starts[L->num_instances] != n)
+        {
+            g_last_error = "instance_starts must end at n";
+            return LOOM_B200_ERR_INVALID;
+        }
+    }
+    else
+    {
+        if(M->group == 0 || n % M->group != 0)
+        {
+            g_last_error = "n is not a multiple of the group";
+            return LOOM_B200_ERR_INVALID;
+        }
+        rows = n / M->group;
+    }
+    if(n == 0) return LOOM_B200_OK;
+
+    std::vector<loom_b200_input> din(L->inputs, L->inputs + info.num_inputs);
     for(uint32_t i = 0; i < info.num_inputs; ++i)
         if(din[i].form == LOOM_B200_IN_ARRAY && din[i].ptr)
         {
-            LB_CUDA(cudaMemcpyAsync(h->d_in[i],
-                                    din[i].ptr,
-                                    n * type_bytes(info.input_types[i]),
-                                    cudaMemcpyHostToDevice,
-                                    h->stream));
+            LB_CUDA(cudaMemcpyAsync(h->d_in[i], din[i].ptr, n * type_bytes(info.input_types[i]),
+                                    cudaMemcpyHostToDevice, h->stream));
             din[i].ptr = h->d_in[i];
         }
     loom_b200_launch D = *L;
     D.inputs           = din.data();
     D.outputs          = h->d_out.data();
-    if(L->instance_starts)
+    if(int rc = stage_tables(h, *L, D, h->stream)) return rc;
+    if(int rc = launch(h, D, h->stream)) return rc;
+
+    // the reduction: row buffers, and for instances the row offsets and
+    // group sizes, all in one device buffer
+    size_t row_bytes = 0;
+    for(uint32_t j = 0; j < info.num_outputs; ++j) row_bytes += rows * type_bytes(info.output_types[j]);
+    const size_t meta = M->instance_group ? (out_starts.size() * 8 + L->num_instances * 4) : 0;
+    if(int rc = grow(&h->d_rows, &h->rows_bytes, (row_bytes + 255) / 256 * 256 + meta)) return rc;
+    char*                     base = static_cast<char*>(h->d_rows);
+    const unsigned long long* d_os = nullptr;
+    const unsigned*           d_g  = nullptr;
+    if(meta)
     {
-        const size_t bytes = (static_cast<size_t>(L->num_instances) + 1) * sizeof(uint64_t);
-        int rc = grow(&h->d_starts, &h->starts_bytes, bytes);
-        if(rc) return rc;
-        LB_CUDA(cudaMemcpyAsync(h->d_starts, L->instance_starts, bytes,
+        char* m = base + (row_bytes + 255) / 256 * 256;
+        LB_CUDA(cudaMemcpyAsync(m, out_starts.data(), out_starts.size() * 8, cudaMemcpyHostToDevice, h->stream));
+        LB_CUDA(cudaMemcpyAsync(m + out_starts.size() * 8, M->instance_group, L->num_instances * 4,
                                 cudaMemcpyHostToDevice, h->stream));
-        D.instance_starts = static_cast<const uint64_t*>(h->d_starts);
+        d_os = reinterpret_cast<const unsigned long long*>(m);
+        d_g  = reinterpret_cast<const unsigned*>(m + out_starts.size() * 8);
     }
-    if(L->table)
+    const auto*    d_st   = static_cast<const unsigned long long*>(h->d_starts);
+    const unsigned blocks = static_cast<unsigned>((rows + 255) / 256);
+    size_t         off    = 0;
+    for(uint32_t j = 0; j < info.num_outputs; ++j)
     {
-        const size_t bytes = L->table_words * sizeof(uint32_t);
-        int rc = grow(&h->d_table, &h->table_bytes, bytes);
-        if(rc) return rc;
-        LB_CUDA(cudaMemcpyAsync(h->d_table, L->table, bytes, cudaMemcpyHostToDevice,
-                                h->stream));
-        D.table = static_cast<const uint32_t*>(h->d_table);
+        const size_t eb = type_bytes(info.output_types[j]);
+        if(info.output_types[j] == LOOM_B200_F32)
+            group_mean<float><<<blocks, 256, 0, h->stream>>>(
+                static_cast<const float*>(h->d_out[j]), reinterpret_cast<float*>(base + off), rows, M->group,
+                d_os ? d_st : nullptr, d_g, d_os, d_os ? L->num_instances : 0u);
+        else
+            group_mean<double><<<blocks, 256, 0, h->stream>>>(
+                static_cast<const double*>(h->d_out[j]), reinterpret_cast<double*>(base + off), rows, M->group,
+                d_os ? d_st : nullptr, d_g, d_os, d_os ? L->num_instances : 0u);
+        LB_CUDA(cudaGetLastError());
+        LB_CUDA(cudaMemcpyAsync(L->outputs[j], base + off, rows * eb, cudaMemcpyDeviceToHost, h->stream));
+        off += rows * eb;
     }
-    int rc = launch(h, D, h->stream);
-    if(rc) return rc;
-    for(uint32_t i = 0; i < info.num_outputs; ++i)
-        LB_CUDA(cudaMemcpyAsync(L->outputs[i],
-                                h->d_out[i],
-                                n * type_bytes(info.output_types[i]),
-                                cudaMemcpyDeviceToHost,
-                                h->stream));
     LB_CUDA(cudaStreamSynchronize(h->stream));
     return finish_launch(h);
 }
@@ -730,6 +1005,24 @@ loom_b200_get_stats(loom_b200_handle* h, loom_b200_stats* stats)
 }
 
 int
+loom_b200_device_bytes(const loom_b200_handle* h, uint64_t* bytes)
+{
+    if(!h || !bytes) return LOOM_B200_ERR_INVALID;
+    const loom_b200_kernel_info& info = *h->e->info;
+    uint64_t b = 0;
+    if(h->capacity)
+    {
+        for(uint32_t i = 0; i < info.num_inputs; ++i) b += h->capacity * type_bytes(info.input_types[i]);
+        for(uint32_t i = 0; i < info.num_outputs; ++i) b += h->capacity * type_bytes(info.output_types[i]);
+    }
+    b += sizeof(unsigned) + counter_bytes(*h->e) + sizeof(RegroupCtl);
+    if(h->ws_cap) b += 2 * h->e->row_bytes * h->ws_cap + 3ull * h->e->num_queues * sizeof(unsigned);
+    b += h->starts_bytes + h->table_bytes + h->rows_bytes;
+    *bytes = b;
+    return LOOM_B200_OK;
+}
+
+int
 loom_b200_get_block_stats(loom_b200_handle* h,
                           uint64_t*         thread_instr,
                           uint64_t*         warp_instr,
@@ -748,6 +1041,21 @@ loom_b200_get_block_stats(loom_b200_handle* h,
         warp_instr[b]   = c[2 * b + 1];
     }
     return LOOM_B200_OK;
+}
+
+int
+loom_b200_kernel_reg_caps(const char* kernel, uint32_t* caps, uint32_t max_caps, uint32_t* num_caps)
+{
+    if(!kernel || !num_caps || (!caps && max_caps)) return LOOM_B200_ERR_INVALID;
+    for(int i = 0; i < kRegistrySize; ++i)
+        if(std::strcmp(kRegistry[i]->info->name, kernel) == 0)
+        {
+            const KernelEntry& e = *kRegistry[i];
+            for(uint32_t c = 0; c < max_caps && c < e.num_reg_caps; ++c) caps[c] = e.reg_caps[c];
+            *num_caps = e.num_reg_caps;
+            return LOOM_B200_OK;
+        }
+    return LOOM_B200_ERR_NOT_FOUND;
 }
 
 int

@@ -12,6 +12,7 @@ namespace loom_b200
 struct PlainLaunch
 {
     Columns             cols;
+    unsigned long long  first; // Loom threads [first, first + n)
     unsigned long long  n;
     unsigned long long  max_steps;
     unsigned*           status;
@@ -26,6 +27,7 @@ struct RegroupLaunch
     RegroupParams params;
     unsigned      grid;
     unsigned      block;
+    unsigned      regs; // register cap of the megakernel (0: the kernel's default)
     bool          profile;
     cudaStream_t  stream;
 };
@@ -48,9 +50,11 @@ struct KernelEntry
     unsigned                     num_queues; // work queues of the regrouping engine
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
-    cudaError_t (*regroup_occupancy)(int block, bool profile, int* ctas_per_sm);
+    cudaError_t (*regroup_occupancy)(int block, bool profile, unsigned regs, int* ctas_per_sm);
     const loom_b200_queue_layout* queues;   // num_queues entries
     const QueueSegment*           segments; // num_queues entries
+    const unsigned*               reg_caps; // compiled register caps, default first
+    unsigned                      num_reg_caps;
 };
 
 extern const KernelEntry* const kRegistry[];

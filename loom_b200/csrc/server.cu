@@ -416,7 +416,7 @@ loom_b200_server_create(const char*                 kernel,
     int      ctas  = 0;
     for(;;)
     {
-        if(e->regroup_occupancy(static_cast<int>(block), o.profile != 0, &ctas) != cudaSuccess)
+        if(e->regroup_occupancy(static_cast<int>(block), o.profile != 0, o.max_regs, &ctas) != cudaSuccess)
         {
             delete s;
             return LOOM_B200_ERR_CUDA;
@@ -584,6 +584,7 @@ run_slice(loom_b200_server* s)
     L.params.inst_done     = s->d_done;
     L.grid                 = s->grid;
     L.block                = s->block;
+    L.regs                 = o.max_regs;
     L.profile              = o.profile != 0;
     L.stream               = s->stream;
     serve_resume<<<1, 32, 0, s->stream>>>(s->d_ctl, s->d_qcnt, s->d_qhead, s->e->num_queues,

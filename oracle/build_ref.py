@@ -1,7 +1,7 @@
 """Recipe: compile Loom's scalar backend (bse) into oracle/_ref/libloomref.so.
 
 TEST AND BASELINE INFRASTRUCTURE ONLY.  Reads the Loom headers where they
-lie (LOOM_REF_DIR, default /root/reference) and writes only into
+lie (LOOM_REF_DIR, default ../reference beside this repository) and writes only into
 oracle/_ref/ (per-kernel sources and objects in oracle/_ref/obj/).  g++ builds bse with -std=c++20 -fno-exceptions once Loom's
 fast_float include is satisfied by a small forwarding shim
 (loom_b200/frontend/shim); -ffp-contract=off keeps every Loom instruction a
@@ -25,7 +25,7 @@ OUT = HERE / "_ref" / "libloomref.so"
 
 def ref_dir() -> pathlib.Path | None:
     env = os.environ.get("LOOM_REF_DIR")
-    for c in ([pathlib.Path(env)] if env else []) + [pathlib.Path("/root/reference")]:
+    for c in ([pathlib.Path(env)] if env else []) + [ROOT.parent / "reference"]:
         if (c / "src" / "vm" / "bse.hpp").is_file():
             return c
     return None
@@ -33,7 +33,12 @@ def ref_dir() -> pathlib.Path | None:
 
 FLAGS = [
     "-std=c++20",
-    "-O2",
+    "-O3",
+    # the x86-64 level of both host CPUs here (AVX-512 F/BW/CD/DQ/VL), tuned
+    # for the build machine: the library is built once and runs on the GPU
+    # machine's host too, so it must not use extensions only one of them has
+    "-march=x86-64-v4",
+    "-mtune=native",
     "-fno-exceptions",
     "-ffp-contract=off",
     "-fno-fast-math",
@@ -69,6 +74,11 @@ def build(force: bool = False, jobs: int | None = None) -> pathlib.Path | None:
     obj_dir.mkdir(parents=True, exist_ok=True)
     deps = [HERE / "ref_kernel.hpp", *(ROOT / "loom_b200" / "kernels").glob("*.hpp")]
     dep_mtime = max(d.stat().st_mtime for d in deps)
+    # a change of compiler flags rebuilds every object
+    stamp = obj_dir / "flags.txt"
+    if not stamp.exists() or stamp.read_text() != " ".join(FLAGS):
+        force = True
+        stamp.write_text(" ".join(FLAGS))
     inc = [
         f"-I{ref / 'src'}",
         f"-I{ref / 'ext' / 'include'}",

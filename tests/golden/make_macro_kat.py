@@ -39,7 +39,7 @@ KERNELS = {
 
 
 def ref_dir() -> pathlib.Path:
-    for c in (os.environ.get("LOOM_REF_DIR"), "/root/reference"):
+    for c in (os.environ.get("LOOM_REF_DIR"), str(pathlib.Path(__file__).resolve().parents[3] / "reference")):
         if c and (pathlib.Path(c) / "src" / "common" / "random.hpp").is_file():
             return pathlib.Path(c)
     raise SystemExit("Loom headers not found: set LOOM_REF_DIR")

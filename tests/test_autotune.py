@@ -68,3 +68,32 @@ def test_store_and_lookup(tmp_path, monkeypatch):
     entry = json.loads(f.read_text())["k"]["pt"]
     assert len(entry["points"]) == 12 and entry["points"][0]["ms"] == -9.0  # fastest first
     assert entry["device"] == "B200"
+
+
+def test_constraint_keeps_the_fastest_eligible_point(fake_timing):
+    """A constraint (e.g. a minimum lane efficiency) rules points out: the
+    search returns the fastest point that meets it, and records the others
+    as ineligible."""
+    # the optimum (burst 4) is ruled out: the best eligible point is one step away
+    res = T.tune(_make_launch, 1000, seed=dict(burst=1, utr_lanes=8, block_size=256), space=SPACE,
+                 constraint=lambda o: o["burst"] != 4)
+    assert res["best"]["burst"] in (2, 8) and res["ms"] == pytest.approx(11.0)
+    assert any(p.get("eligible") is False and p["opts"]["burst"] == 4 for p in res["points"])
+    with pytest.raises(RuntimeError):
+        T.tune(_make_launch, 1000, seed=dict(BEST), space=SPACE, constraint=lambda o: False)
+
+
+def test_register_cap_is_a_tuned_option(fake_timing):
+    """max_regs is searched like any other option over the caps the caller
+    passes (the kernel's compiled caps)."""
+    space = dict(SPACE, max_regs=[0, 48, 96])
+
+    def cost(opts):
+        return _cost(opts) + {0: 1.0, 48: 0.0, 96: 2.0}[opts["max_regs"]]
+
+    import loom_b200.autotune as TT
+
+    TT.time_launch = lambda fn, reps=2: cost(fn.opts)
+    res = T.tune(_make_launch, 1000, seed=dict(BEST, max_regs=0), space=space)
+    assert res["best"]["max_regs"] == 48
+    assert "max_regs" in T.DEFAULT and T.SPACE["max_regs"] == [0]

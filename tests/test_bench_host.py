@@ -96,8 +96,11 @@ def test_issue_roofline_of_the_committed_capture():
     SASS warp instructions per path, scaled to the full launch, over the
     kernel time, against 148 SMs x 4 schedulers at the sampled clock; only
     for the options the capture was taken with."""
+    import json
+
     w = bench.make_workload("pt")
-    w.opts = bench.regroup_opts(w.kernel, w.tune_key)
+    cap = json.loads((bench.ROOT / "profiles" / "roofline_traffic.json").read_text())["pt"]
+    w.opts = dict(cap["sass_options"])
     traffic, issue = bench.ncu_rooflines(w, 41.47, 1965.0)
     assert issue is not None
     per = issue["sass_warp_inst_per_thread"]
@@ -108,6 +111,16 @@ def test_issue_roofline_of_the_committed_capture():
     # another option set: no issue figure from a capture of different code
     w.opts = dict(w.opts, schedule=0)
     assert bench.ncu_rooflines(w, 41.47, 1965.0)[1] is None
+
+
+def test_vm_issue_roofline():
+    """The headline roofline: VM instructions executed (summed over Loom
+    threads) per second against 32 lanes x 148 SMs x 4 schedulers x one
+    warp instruction per cycle at the sampled clock."""
+    r = bench.issue_roofline(6382 * 50331648, 41.44, 1965.0)
+    assert r["peak"] == pytest.approx(32 * 148 * 4 * 1.965, rel=1e-4)
+    assert r["achieved"] == pytest.approx(6382 * 50331648 / 41.44e-3 / 1e9, rel=1e-4)
+    assert r["frac"] == pytest.approx(0.208, abs=0.002)
 
 
 def test_rooflines_without_a_capture(tmp_path):

@@ -112,6 +112,9 @@ REGROUP_VARIANTS = [
     dict(schedule=1, cost_model=True, burst=8, population=300),
     dict(schedule=2, burst=16),
     dict(schedule=2, burst=3, period=7, population=100),
+    # no period limit: schedule 2 never parks, one round, no queue state
+    dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, prefetch=False),
+    dict(schedule=2, burst=1, period=api.PERIOD_UNBOUNDED, prefetch=True, block_size=64),
 ]
 
 
