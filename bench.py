@@ -557,7 +557,7 @@ def cpu_reference(w, check_tids=None, target_s: float = 2.0):
     run(w.kernel, ins, table)
     dt = time.perf_counter() - t0
     how = (
-        "Loom bse (vm::bse::function), g++ -O2 -mfma, one std::thread per core"
+        "Loom bse (vm::bse::function), g++ -O3 -march=x86-64-v4 -mfma -ffp-contract=off, one std::thread per core"
         if kind == "reference"
         else "C restatement of bse, one thread"
     )
@@ -829,24 +829,32 @@ class RegroupService:
         from loom_b200 import serving
 
         self.api, self.pool, self.inputs = api, pool, inputs
-        st = stream
-        mk = dict(stream=st, profile=profile)
+        # one stream per server, one device-memory budget for all
+        self.streams = {k: torch.cuda.Stream() for k in SERVE_KERNELS}
+        self.budget = api.Budget(SERVE_BUDGET)
+        mk = dict(profile=profile, budget=self.budget)
+        # collatz and fib servers run 256-thread CTAs, so that one CTA of each
+        # fits on an SM beside one 512-thread CTA of the path tracer (64 + 40
+        # + 48 registers per thread: 54 K of the SM's 64 K registers)
         self.p = serving.Pool(
             {
                 "pt": api.Server(
                     "sphere_pt_f32", ring_threads=1 << 26, max_requests=512, slice_rounds=4,
                     forms=["instance", "local_iota"], header_words=S.HEADER_WORDS, reloc_word=4,
-                    table_words=1 << 20, **regroup_opts("sphere_pt_f32", "batch"), **mk,
+                    table_words=1 << 20, **regroup_opts("sphere_pt_f32", "batch"), stream=self.streams["pt"], **mk,
                 ),
                 "collatz": api.Server(
                     "collatz_u64", ring_threads=1 << 25, max_requests=512, slice_rounds=2,
-                    **{**regroup_opts("collatz_u64"), "population": 1 << 22}, **mk,
+                    **{**regroup_opts("collatz_u64"), "population": 1 << 22, "block_size": 256, "ctas_per_sm": 0},
+                    stream=self.streams["collatz"], **mk,
                 ),
                 "fib": api.Server(
                     "fib_u64", ring_threads=1 << 23, max_requests=512, slice_rounds=2,
-                    **{**regroup_opts("fib_u64"), "population": 1 << 21}, **mk,
+                    **{**regroup_opts("fib_u64"), "population": 1 << 21, "block_size": 256, "ctas_per_sm": 0},
+                    stream=self.streams["fib"], **mk,
                 ),
-            }
+            },
+            shared_ctas={"pt": 1, "collatz": 1, "fib": 1},
         )
         self.bufs = {}
         self.reqs = {}
@@ -915,6 +923,13 @@ class RegroupService:
         ti = sum(s["thread_instr"] for s in self.p.stats().values())
         wi = sum(s["warp_instr"] for s in self.p.stats().values())
         return ti / (32.0 * wi) if wi else None
+
+    def busy_ms(self):
+        """Device time of every server's slices so far, summed over servers."""
+        return sum(s["busy_ms"] for s in self.p.stats().values())
+
+    def budget_waits(self):
+        return sum(s["budget_waits"] for s in self.p.stats().values())
 
     def close(self):
         self.p.close()
@@ -1052,19 +1067,29 @@ def serve_measure(seconds: float, rank: int = 0, local: int = 0, parity: bool = 
                 count = max(8, int(rate * seconds))
                 reqs = mix.draw(count)
                 arr = np.cumsum(mix.rng.exponential(1.0 / rate, size=count))
+                busy0 = svc.busy_ms() if hasattr(svc, "busy_ms") else None
                 lat, span, threads = run_requests(svc, reqs, arr)
-                res["loads"].append(
-                    {
-                        "offered_load": L,
-                        "requests": count,
-                        "msamples_s": round(threads / span / 1e6, 3),
-                        "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
-                        "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
-                        "mean_ms": round(float(lat.mean()) * 1e3, 2),
-                    }
-                )
+                row = {
+                    "offered_load": L,
+                    "requests": count,
+                    "msamples_s": round(threads / span / 1e6, 3),
+                    "p50_ms": round(float(np.percentile(lat, 50)) * 1e3, 2),
+                    "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
+                    "mean_ms": round(float(lat.mean()) * 1e3, 2),
+                }
+                if busy0 is not None:
+                    # device time of all servers' slices over the wall time:
+                    # above 1 when slices of different kernels ran together
+                    row["servers_busy_ms"] = round(svc.busy_ms() - busy0, 1)
+                    row["wall_ms"] = round(span * 1e3, 1)
+                    row["overlap"] = round((svc.busy_ms() - busy0) / (span * 1e3), 3)
+                res["loads"].append(row)
             if parity and name == "regroup":
                 res["parity"] = serve_parity(svc, inputs)
+            if hasattr(svc, "budget_waits"):
+                res["budget"] = {"limit_bytes": svc.budget.limit, "requests_that_waited": svc.budget_waits(),
+                                 "admission": "n x (state_size + column bytes per thread) + table bytes, "
+                                              "shared by the three servers, arrival order"}
             svc.close()
             # lane efficiency of the same mix in a counted (slower) run
             svc = cls(api, torch, stream, pool, inputs, profile=True)
@@ -1368,6 +1393,9 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="pt", choices=["pt", "pt_small", "batch", "collatz", "fib", "loom_pt", "loom_pt2", "loom_pt_512", "loom_pt2_512", "loom_primary", "loom_primary_b20", "serve"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU leg (timing and parity)")
+    ap.add_argument("--only", metavar="FORM", default="",
+                    help="time one engine or form alone (plain, regroup, majority_cost_model, "
+                         "lane_efficiency_form): no counted launch, no end-to-end leg, no CPU leg (for profilers)")
     ap.add_argument("--no-configs", action="store_true",
                     help="pt: skip the other configurations (fib, collatz, batch, serve) of the default run")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
@@ -1451,6 +1479,19 @@ def main() -> None:
     tids = w.check_tids()
 
     forms = regroup_forms(w)
+    if args.only:
+        # one engine or form, W + K launches and nothing else: the launch
+        # sequence a profiler's -s/-c counts refer to
+        opts = {} if args.only == "plain" else forms[args.only]
+        f = api.Function(w.kernel, 0, "plain" if args.only == "plain" else "regroup", **opts)
+        ms = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
+        st = f.stats(raise_on_device_error=True)
+        f.close()
+        if rank == 0:
+            print(json.dumps({"workload": w.desc, "form": args.only, "options": opts,
+                              "ms_per_step": round(ms / args.steps, 4), "kernel_ms": round(st["ms"], 4),
+                              "value": round(world * w.n / (ms / args.steps / 1e3) / 1e6, 3)}))
+        return
     res = measure(w, api, torch, stream, args.steps, warmup, dist, tids, forms, clocks_for="regroup")
     rg = res["regroup"]
     clocks = rg["clocks"]

@@ -362,6 +362,21 @@ int loom_b200_parked_dump(loom_b200_handle* h,
  * server's stream. */
 typedef struct loom_b200_server loom_b200_server;
 
+/* A device-memory budget for the thread state of admitted requests, shared
+ * by the servers that point to it (drive them from one host thread).  A
+ * request holds n x (state_size + its column bytes per thread) plus its
+ * header and body bytes from admission until it completes or is dropped:
+ * Loom's per-thread state is K::state_size (src/vm/core.hpp:1026-1030), and
+ * its streams bound the rows in flight by the stream size
+ * (src/vm/simd.hpp:2803-2903).  A request that does not fit waits in the
+ * queue (arrival order); one larger than the whole limit is refused at
+ * submit with LOOM_B200_ERR_BUDGET. */
+typedef struct loom_b200_budget
+{
+    uint64_t limit; /* bytes */
+    uint64_t used;  /* bytes held by admitted requests (maintained by the servers) */
+} loom_b200_budget;
+
 typedef struct loom_b200_server_cfg
 {
     uint64_t        ring_threads; /* entries of each column ring: a power of
@@ -380,6 +395,7 @@ typedef struct loom_b200_server_cfg
     const uint32_t* forms;        /* one LOOM_B200_IN_* per kernel input
                                      (ARRAY, IOTA, LOCAL_IOTA, INSTANCE);
                                      NULL: every input an ARRAY */
+    loom_b200_budget* budget;     /* shared thread-state budget, or NULL */
 } loom_b200_server_cfg;
 
 typedef struct loom_b200_request
@@ -405,6 +421,9 @@ typedef struct loom_b200_server_stats
     uint64_t thread_instr, warp_instr; /* with opts.profile: lane efficiency */
     uint32_t status;       /* OR of LOOM_B200_STATUS_* */
     uint32_t pad;
+    uint64_t budget_waits; /* requests that waited for the budget at least once */
+    uint64_t held_bytes;   /* budget bytes held by this server's requests in flight */
+    double   busy_ms;      /* device time of the slices (CUDA events on the server's stream) */
 } loom_b200_server_stats;
 
 /* `opts`: engine options (population = resident threads; 0: 2^21);
@@ -420,8 +439,18 @@ int loom_b200_server_destroy(loom_b200_server* s);
  * LOOM_B200_ERR_BUDGET: larger than the ring or the arena. */
 int loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_t* ticket);
 /* Admits what fits, runs one slice, copies out the requests that finished
- * and returns up to max_done of their tickets (the rest on later calls). */
+ * and returns up to max_done of their tickets (the rest on later calls).
+ * After loom_b200_server_launch it completes the slice that call started. */
 int loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, uint32_t* n_done);
+/* Admits what fits and starts the next slice without waiting for it, with
+ * ctas_per_sm CTAs per SM (0: the server's own launch shape), so that the
+ * slices of several servers (each on its own stream) run on the GPU at the
+ * same time; the next loom_b200_server_step completes it.  Servers whose
+ * slices overlap must fit on the SMs together (registers, threads, shared
+ * memory of one CTA each per SM), since each slice is a cooperative launch
+ * whose CTAs are resident together.  Nothing is launched when no request is
+ * in flight or admissible. */
+int loom_b200_server_launch(loom_b200_server* s, uint32_t ctas_per_sm);
 int loom_b200_server_get_stats(const loom_b200_server* s, loom_b200_server_stats* st);
 /* Cancels a request (no counterpart in Loom, whose streams have no request
  * boundary).  A queued request leaves the queue at once.  The threads of a

@@ -167,6 +167,26 @@ class MeanC(ctypes.Structure):
     ]
 
 
+class BudgetC(ctypes.Structure):
+    _fields_ = [("limit", ctypes.c_uint64), ("used", ctypes.c_uint64)]
+
+
+class Budget:
+    """A device-memory budget for the thread state of admitted requests
+    (loom_b200_budget), shared by the servers created with it."""
+
+    def __init__(self, limit_bytes: int):
+        self.c = BudgetC(int(limit_bytes), 0)
+
+    @property
+    def limit(self) -> int:
+        return int(self.c.limit)
+
+    @property
+    def used(self) -> int:
+        return int(self.c.used)
+
+
 class ServerCfgC(ctypes.Structure):
     _fields_ = [
         ("ring_threads", ctypes.c_uint64),
@@ -176,6 +196,7 @@ class ServerCfgC(ctypes.Structure):
         ("max_requests", ctypes.c_uint32),
         ("slice_rounds", ctypes.c_uint32),
         ("forms", ctypes.POINTER(ctypes.c_uint32)),
+        ("budget", ctypes.POINTER(BudgetC)),
     ]
 
 
@@ -207,7 +228,13 @@ class ServerStatsC(ctypes.Structure):
             "thread_instr",
             "warp_instr",
         )
-    ] + [("status", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+    ] + [
+        ("status", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("budget_waits", ctypes.c_uint64),
+        ("held_bytes", ctypes.c_uint64),
+        ("busy_ms", ctypes.c_double),
+    ]
 
 
 class Iota:
@@ -270,6 +297,7 @@ EXPORTS = [
     "loom_b200_server_destroy",
     "loom_b200_server_submit",
     "loom_b200_server_step",
+    "loom_b200_server_launch",
     "loom_b200_server_get_stats",
     "loom_b200_server_cancel",
     "loom_b200_server_set_timeout",
@@ -350,6 +378,7 @@ def lib() -> ctypes.CDLL:
     ]
     L.loom_b200_server_destroy.argtypes = [vp]
     L.loom_b200_server_submit.argtypes = [vp, ctypes.POINTER(RequestC), ctypes.POINTER(ctypes.c_uint64)]
+    L.loom_b200_server_launch.argtypes = [vp, ctypes.c_uint32]
     L.loom_b200_server_step.argtypes = [
         vp,
         ctypes.POINTER(ctypes.c_uint64),
@@ -767,6 +796,7 @@ class Server:
         reloc_word: int = -1,
         table_words: int = 0,
         stream=None,
+        budget: Optional[Budget] = None,
         **opts,
     ):
         self.info = info(kernel)
@@ -774,7 +804,9 @@ class Server:
         fs = [self.FORM[f] for f in forms] if forms else [IN_ARRAY] * len(self.info.inputs)
         self._forms = (ctypes.c_uint32 * max(1, len(fs)))(*fs)
         self.forms = fs
-        cfg = ServerCfgC(ring_threads, table_words, header_words, reloc_word, max_requests, slice_rounds, self._forms)
+        self.budget = budget  # kept alive while the server points to it
+        cfg = ServerCfgC(ring_threads, table_words, header_words, reloc_word, max_requests, slice_rounds, self._forms,
+                         None if budget is None else ctypes.pointer(budget.c))
         o = make_opts("regroup", **opts)
         s = getattr(stream, "cuda_stream", stream)
         check(lib().loom_b200_server_create(kernel.encode(), ctypes.byref(o), ctypes.byref(cfg), s, ctypes.byref(self._h)))
@@ -818,8 +850,14 @@ class Server:
         self._live[t.value] = (ins, outputs, hdr, bod, pin, pout)
         return t.value
 
+    def launch(self, ctas_per_sm: int = 0) -> None:
+        """Admits and starts the next slice without waiting for it
+        (loom_b200_server_launch); the next ``step`` completes it."""
+        check(lib().loom_b200_server_launch(self._h, int(ctas_per_sm)))
+
     def step(self) -> List[int]:
-        """Admits, runs one slice, returns the tickets that completed."""
+        """Admits, runs one slice (or completes the one ``launch`` started),
+        returns the tickets that completed."""
         k = ctypes.c_uint32()
         check(lib().loom_b200_server_step(self._h, self._done, self._max, ctypes.byref(k)))
         return [self._done[i] for i in range(k.value)]

@@ -1,5 +1,6 @@
-// Host bookkeeping of the serving loop's failed requests (no CUDA): requests
-// the caller cancels and requests a host-side watchdog expires.
+// Host bookkeeping of the serving loop (no CUDA): requests the caller
+// cancels, requests a host-side watchdog expires, and the device-memory
+// budget that admitted requests hold.
 //
 // Loom has neither (its streams have no request boundary,
 // src/vm/bve.hpp:1208-1270).  The server's threads cannot be taken back
@@ -86,6 +87,34 @@ expire_requests(std::deque<Req>&        queued,
             ++k;
         }
     return k;
+}
+
+/// Device bytes a request holds while admitted: per thread its state and
+/// its column entries (`per_thread`), plus its table words.
+inline uint64_t
+request_bytes(uint64_t n, uint64_t per_thread, uint64_t table_words)
+{
+    return n * per_thread + 4 * table_words;
+}
+
+/// Takes `bytes` from a budget (`limit`, `used`) when they fit; a NULL
+/// budget always fits.
+template <typename Budget>
+bool
+budget_take(Budget* b, uint64_t bytes)
+{
+    if(!b) return true;
+    if(bytes > b->limit || b->used > b->limit - bytes) return false;
+    b->used += bytes;
+    return true;
+}
+
+/// Gives `bytes` back to a budget (NULL: nothing to do).
+template <typename Budget>
+void
+budget_give(Budget* b, uint64_t bytes)
+{
+    if(b) b->used -= bytes < b->used ? bytes : b->used;
 }
 
 /// Hands out up to `max` failures, oldest first; returns how many.

@@ -123,6 +123,8 @@ struct Request
     uint64_t              body_words = 0;
     SteadyClock::time_point born{}; // submission time, for the watchdog
     int                     fail = 0; // LOOM_B200_ERR_* once cancelled
+    uint64_t                bytes  = 0;     // budget bytes while admitted
+    bool                    waited = false; // has waited for the budget
     // in flight
     uint32_t slot     = 0;
     uint64_t vstart   = 0;
@@ -220,12 +222,19 @@ struct loom_b200_server
     std::vector<void*>  d_cols;               // one ring per input (array form) and output
     uint64_t            device_bytes = 0;
 
-    // host side
+    // host side; the results of a slice come back into pinned memory, so
+    // that starting a slice does not wait for it
     std::deque<Request>     queued;
     std::vector<Request>    flight; // in virtual-start order
     std::vector<uint32_t>   free_slots;
     Arena                   arena;
-    std::vector<unsigned>   h_done;
+    unsigned*               h_done     = nullptr; // pinned, max_requests
+    RegroupCtl*             h_ctl      = nullptr; // pinned
+    unsigned*               h_status   = nullptr; // pinned
+    unsigned long long*     h_counters = nullptr; // pinned, 8
+    cudaEvent_t             ev_a = nullptr, ev_k = nullptr, ev_b = nullptr;
+    bool                    launched   = false; // a slice runs, not harvested yet
+    uint64_t                per_thread = 0;     // budget bytes per thread of a request
     std::vector<unsigned long long> h_starts;
     std::vector<unsigned>   h_ids;
     std::deque<uint64_t>    done_q; // completed tickets not handed out yet
@@ -255,6 +264,13 @@ dalloc(loom_b200_server* s, void** p, size_t bytes)
 void
 free_all(loom_b200_server* s)
 {
+    cudaFreeHost(s->h_done);
+    cudaFreeHost(s->h_ctl);
+    cudaFreeHost(s->h_status);
+    cudaFreeHost(s->h_counters);
+    if(s->ev_a) cudaEventDestroy(s->ev_a);
+    if(s->ev_k) cudaEventDestroy(s->ev_k);
+    if(s->ev_b) cudaEventDestroy(s->ev_b);
     cudaFree(s->d_state);
     cudaFree(s->d_qcnt);
     cudaFree(s->d_qhead);
@@ -310,8 +326,21 @@ admit(loom_b200_server* s)
     {
         Request& r = s->queued.front();
         if(s->vnext + r.n > tid_base(s) + ring) break; // ring full until older requests finish
+        if(!budget_take(s->cfg.budget, r.bytes))
+        {
+            // the budget is held by requests in flight (of this server or
+            // of others sharing the budget): wait, in arrival order
+            if(!r.waited) s->st.budget_waits += 1;
+            r.waited = true;
+            break;
+        }
         uint64_t at = 0;
-        if(!s->arena.alloc(r.body_words, &at)) break;
+        if(!s->arena.alloc(r.body_words, &at))
+        {
+            budget_give(s->cfg.budget, r.bytes);
+            break;
+        }
+        s->st.held_bytes += r.bytes;
         r.slot     = s->free_slots.back();
         r.vstart   = s->vnext;
         r.arena_at = at;
@@ -345,6 +374,7 @@ admit(loom_b200_server* s)
                                     cudaMemcpyHostToDevice,
                                     s->stream));
         SV_CUDA(cudaMemsetAsync(s->d_done + r.slot, 0, sizeof(unsigned), s->stream));
+        s->h_done[r.slot] = 0u;
         s->vnext += r.n;
         s->st.admitted += 1;
         s->flight.push_back(std::move(r));
@@ -470,9 +500,30 @@ loom_b200_server_create(const char*                 kernel,
         delete s;
         return rc;
     }
+    if(!rc &&
+       (cudaMallocHost(reinterpret_cast<void**>(&s->h_done), mr * sizeof(unsigned)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&s->h_ctl), sizeof(RegroupCtl)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&s->h_status), sizeof(unsigned)) != cudaSuccess ||
+        cudaMallocHost(reinterpret_cast<void**>(&s->h_counters), 8 * sizeof(unsigned long long)) != cudaSuccess))
+        rc = LOOM_B200_ERR_OOM;
+    if(!rc && (cudaEventCreate(&s->ev_a) != cudaSuccess || cudaEventCreate(&s->ev_k) != cudaSuccess ||
+               cudaEventCreateWithFlags(&s->ev_b, cudaEventDisableTiming) != cudaSuccess))
+        rc = LOOM_B200_ERR_CUDA;
+    if(rc)
+    {
+        free_all(s);
+        delete s;
+        return rc;
+    }
+    std::memset(s->h_done, 0, mr * sizeof(unsigned));
+    // budget bytes per thread: the thread state (K::state_size) and the
+    // thread's entries in the column rings
+    s->per_thread = info.state_size;
+    for(uint32_t i = 0; i < info.num_inputs; ++i)
+        if(s->forms[i] == LOOM_B200_IN_ARRAY) s->per_thread += tbytes(info.input_types[i]);
+    for(uint32_t j = 0; j < info.num_outputs; ++j) s->per_thread += tbytes(info.output_types[j]);
     s->arena.init(cfg->table_words);
     for(uint32_t i = 0; i < mr; ++i) s->free_slots.push_back(static_cast<uint32_t>(mr - 1 - i));
-    s->h_done.assign(mr, 0u);
     s->st.device_bytes = s->device_bytes;
     *out               = s;
     return LOOM_B200_OK;
@@ -483,6 +534,7 @@ loom_b200_server_destroy(loom_b200_server* s)
 {
     if(!s) return LOOM_B200_OK;
     cudaStreamSynchronize(s->stream);
+    for(const Request& r: s->flight) budget_give(s->cfg.budget, r.bytes);
     free_all(s);
     delete s;
     return LOOM_B200_OK;
@@ -514,6 +566,8 @@ loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_
     if(s->cfg.header_words) q.header.assign(r->header, r->header + s->cfg.header_words);
     q.body       = r->body;
     q.body_words = r->body ? r->body_words : 0;
+    q.bytes      = request_bytes(q.n, s->per_thread, s->cfg.header_words + q.body_words);
+    if(s->cfg.budget && q.bytes > s->cfg.budget->limit) return LOOM_B200_ERR_BUDGET;
     if(ticket) *ticket = q.ticket;
     s->queued.push_back(std::move(q));
     s->st.submitted += 1;
@@ -522,13 +576,18 @@ loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uint64_
 
 namespace
 {
+/// Admits what fits and starts a slice on the server's stream (with
+/// `ctas_per_sm` CTAs per SM, 0: the server's own shape) without waiting:
+/// the completion counters, control block, status and counters come back
+/// into pinned host memory behind it.  Nothing starts when no request is in
+/// flight.
 int
-run_slice(loom_b200_server* s)
+slice_launch(loom_b200_server* s, unsigned ctas_per_sm)
 {
+    if(s->launched) return LOOM_B200_OK;
     if(int rc = admit(s)) return rc;
     if(s->flight.empty()) return LOOM_B200_OK;
     const loom_b200_kernel_info& info = *s->e->info;
-    const uint64_t               ring = s->mask + 1;
 
     // instance table of this slice: requests in flight, in thread order
     const size_t m = s->flight.size();
@@ -583,34 +642,59 @@ run_slice(loom_b200_server* s)
     L.params.slice_rounds  = s->cfg.slice_rounds;
     L.params.inst_done     = s->d_done;
     L.grid                 = s->grid;
-    L.block                = s->block;
-    L.regs                 = o.max_regs;
-    L.profile              = o.profile != 0;
-    L.stream               = s->stream;
+    if(ctas_per_sm)
+    {
+        // never more CTAs per SM than fit (cooperative launches need every
+        // CTA resident at once)
+        int fit = 0;
+        SV_CUDA(s->e->regroup_occupancy(static_cast<int>(s->block), o.profile != 0, o.max_regs, &fit));
+        const unsigned c = std::min<unsigned>(ctas_per_sm, static_cast<unsigned>(std::max(fit, 1)));
+        L.grid           = c * static_cast<unsigned>(s->sms);
+    }
+    L.block   = s->block;
+    L.regs    = o.max_regs;
+    L.profile = o.profile != 0;
+    L.stream  = s->stream;
+    SV_CUDA(cudaEventRecord(s->ev_a, s->stream));
     serve_resume<<<1, 32, 0, s->stream>>>(s->d_ctl, s->d_qcnt, s->d_qhead, s->e->num_queues,
                                           static_cast<unsigned>(s->next_round), s->vnext, s->cap);
     SV_CUDA(cudaGetLastError());
     SV_CUDA(s->e->regroup(L));
-
-    RegroupCtl         ctl{};
-    unsigned           status = 0;
-    unsigned long long cnt[8] = {};
-    SV_CUDA(cudaMemcpyAsync(s->h_done.data(), s->d_done, s->h_done.size() * sizeof(unsigned),
+    SV_CUDA(cudaEventRecord(s->ev_k, s->stream));
+    SV_CUDA(cudaMemcpyAsync(s->h_done, s->d_done, s->cfg.max_requests * sizeof(unsigned),
                             cudaMemcpyDeviceToHost, s->stream));
-    SV_CUDA(cudaMemcpyAsync(&ctl, s->d_ctl, sizeof ctl, cudaMemcpyDeviceToHost, s->stream));
-    SV_CUDA(cudaMemcpyAsync(&status, s->d_status, sizeof status, cudaMemcpyDeviceToHost, s->stream));
-    SV_CUDA(cudaMemcpyAsync(cnt, s->d_counters, sizeof cnt, cudaMemcpyDeviceToHost, s->stream));
-    SV_CUDA(cudaStreamSynchronize(s->stream));
-    s->next_round      = ctl.next_round;
+    SV_CUDA(cudaMemcpyAsync(s->h_ctl, s->d_ctl, sizeof(RegroupCtl), cudaMemcpyDeviceToHost, s->stream));
+    SV_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    SV_CUDA(cudaMemcpyAsync(s->h_counters, s->d_counters, 8 * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, s->stream));
+    SV_CUDA(cudaEventRecord(s->ev_b, s->stream));
+    s->launched = true;
+    return LOOM_B200_OK;
+}
+
+/// Waits for the slice started by slice_launch, then copies out the
+/// requests whose threads all finished and frees what they held.
+int
+slice_harvest(loom_b200_server* s)
+{
+    if(!s->launched) return LOOM_B200_OK;
+    s->launched = false;
+    const loom_b200_kernel_info& info = *s->e->info;
+    const uint64_t               ring = s->mask + 1;
+    SV_CUDA(cudaEventSynchronize(s->ev_b));
+    float ms = 0.f;
+    if(cudaEventElapsedTime(&ms, s->ev_a, s->ev_k) == cudaSuccess) s->st.busy_ms += ms;
+    const unsigned status = *s->h_status;
+    s->next_round      = s->h_ctl->next_round;
     s->st.slices      += 1;
     s->st.status      |= status;
-    s->st.thread_instr = cnt[0];
-    s->st.warp_instr   = cnt[1];
-    s->st.rounds       = cnt[5];
+    s->st.thread_instr = s->h_counters[0];
+    s->st.warp_instr   = s->h_counters[1];
+    s->st.rounds       = s->h_counters[5];
     if(status) return LOOM_B200_ERR_DEVICE;
 
     // harvest: requests whose threads all finished
-    uint32_t         k = 0;
+    uint32_t             k = 0;
     std::vector<Request> keep;
     keep.reserve(s->flight.size());
     for(Request& r: s->flight)
@@ -620,10 +704,12 @@ run_slice(loom_b200_server* s)
             keep.push_back(std::move(r));
             continue;
         }
+        budget_give(s->cfg.budget, r.bytes);
+        s->st.held_bytes -= r.bytes;
         if(r.fail)
         {
             // cancelled in flight: its threads have finished, so its slot,
-            // ring range and arena words are free; nothing is copied out
+            // ring range, arena words and budget are free; nothing is copied out
             s->arena.release(r.arena_at, r.body_words);
             s->free_slots.push_back(r.slot);
             s->failed_q.push_back({r.ticket, r.fail});
@@ -654,10 +740,15 @@ loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, ui
 {
     if(!s) return LOOM_B200_ERR_INVALID;
     if(n_done) *n_done = 0;
-    expire_requests(s->queued, s->flight, SteadyClock::now(), s->timeout_us, LOOM_B200_ERR_TIMEOUT,
-                    s->failed_q);
-    const int rc = run_slice(s);
-    uint32_t  k  = 0;
+    int rc = LOOM_B200_OK;
+    if(!s->launched)
+    {
+        expire_requests(s->queued, s->flight, SteadyClock::now(), s->timeout_us, LOOM_B200_ERR_TIMEOUT,
+                        s->failed_q);
+        rc = slice_launch(s, 0u);
+    }
+    if(!rc) rc = slice_harvest(s);
+    uint32_t k = 0;
     while(done && k < max_done && !s->done_q.empty())
     {
         done[k++] = s->done_q.front();
@@ -665,6 +756,16 @@ loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, ui
     }
     if(n_done) *n_done = k;
     return rc;
+}
+
+int
+loom_b200_server_launch(loom_b200_server* s, uint32_t ctas_per_sm)
+{
+    if(!s) return LOOM_B200_ERR_INVALID;
+    if(s->launched) return LOOM_B200_OK;
+    expire_requests(s->queued, s->flight, SteadyClock::now(), s->timeout_us, LOOM_B200_ERR_TIMEOUT,
+                    s->failed_q);
+    return slice_launch(s, ctas_per_sm);
 }
 
 int

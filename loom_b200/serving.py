@@ -1,24 +1,34 @@
 """A request loop over several kernels: one continuous-batching server
-(loom_b200_server_*) per kernel, all on one CUDA stream, stepped in turn.
+(loom_b200_server_*) per kernel, each on its own CUDA stream.
 
 Each ``step`` gives every server that has work one slice of its
 regrouping megakernel; a request admitted by a server joins the threads of
-that server's requests in flight.  Completions come back as
-``(kind, ticket)`` pairs; ``result`` hands out the outputs.  Requests
+that server's requests in flight.  When several servers have work, their
+slices are started together (``Server.launch`` with the CTAs per SM of
+``shared_ctas``, so that the cooperative grids fit on the SMs side by side)
+and then completed, so the kernels of different requests run on the GPU at
+the same time, as Loom's mp::Shop runs several kernels' streams at once
+(src/vm/mp.hpp:316-385).  Servers created with one ``api.Budget`` admit
+requests against that shared device-memory budget.  Completions come back
+as ``(kind, ticket)`` pairs; ``result`` hands out the outputs.  Requests
 cancelled by ``cancel`` or by a server's watchdog (``timeout``) come back
 from ``failures`` as ``(kind, ticket, code)``.
 """
 
 from __future__ import annotations
 
-from typing import Dict, List, Tuple
+from typing import Dict, List, Optional, Tuple
 
 from . import api
 
 
 class Pool:
-    def __init__(self, servers: Dict[str, api.Server], timeout: float = 0.0):
+    def __init__(self, servers: Dict[str, api.Server], timeout: float = 0.0,
+                 shared_ctas: Optional[Dict[str, int]] = None):
         self.servers = dict(servers)
+        # CTAs per SM of each server's slice while several servers run (None:
+        # one server after the other)
+        self.shared_ctas = shared_ctas
         self._work = {k: 0 for k in self.servers}  # submitted, not completed
         self._failed: List[Tuple[str, int, int]] = []
         if timeout:
@@ -35,12 +45,16 @@ class Pool:
 
     def step(self) -> List[Tuple[str, int]]:
         done = []
-        for k, srv in self.servers.items():
-            if self._work[k]:
-                for t in srv.step():
-                    done.append((k, t))
-                    self._work[k] -= 1
-                self._collect(k, srv)
+        busy = [k for k, srv in self.servers.items() if self._work[k]]
+        if self.shared_ctas and len(busy) > 1:
+            for k in busy:
+                self.servers[k].launch(self.shared_ctas.get(k, 1))
+        for k in busy:
+            srv = self.servers[k]
+            for t in srv.step():
+                done.append((k, t))
+                self._work[k] -= 1
+            self._collect(k, srv)
         return done
 
     def cancel(self, kind: str, ticket: int) -> bool:

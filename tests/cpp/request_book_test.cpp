@@ -1,6 +1,7 @@
-// The serving loop's failure bookkeeping (loom_b200/csrc/request_book.hpp)
-// on the host, without a GPU: cancelling queued and in-flight requests, the
-// watchdog's expiry by submission time, and the hand-out of failures.
+// The serving loop's bookkeeping (loom_b200/csrc/request_book.hpp) on the
+// host, without a GPU: cancelling queued and in-flight requests, the
+// watchdog's expiry by submission time, the hand-out of failures and the
+// device-memory budget of admitted requests.
 // Prints "ok" and returns 0 when every check holds.
 #include "request_book.hpp"
 
@@ -33,6 +34,32 @@ check(bool ok, const char* what)
 
 constexpr int kCancelled = -8;
 constexpr int kTimeout   = -9;
+
+struct Budget
+{
+    uint64_t limit = 0, used = 0;
+};
+
+void
+test_budget()
+{
+    Budget b{1000, 0};
+    check(request_bytes(10, 40, 25) == 500, "bytes: n x per-thread + 4 x table words");
+    check(budget_take(&b, 600), "take what fits");
+    check(!budget_take(&b, 500), "refuse what does not fit");
+    check(b.used == 600, "a refusal takes nothing");
+    check(budget_take(&b, 400) && b.used == 1000, "take up to the limit");
+    budget_give(&b, 600);
+    check(b.used == 400, "give back");
+    check(!budget_take(&b, 1001), "larger than the limit never fits");
+    budget_give(&b, 5000);
+    check(b.used == 0, "giving back more than held clamps at zero");
+    Budget* none = nullptr;
+    check(budget_take(none, ~0ull), "no budget: everything fits");
+    budget_give(none, 7);
+    Budget big{~0ull, ~0ull - 10};
+    check(!budget_take(&big, 11) && budget_take(&big, 10), "no overflow near the top");
+}
 } // namespace
 
 int
@@ -78,6 +105,7 @@ main()
     check(drain_failures(failed, tk, nullptr, 2) == 1 && tk[0] == 3, "the rest, codes skipped");
     check(drain_failures(failed, tk, cd, 2) == 0, "empty");
 
+    test_budget();
     if(failures == 0) std::printf("ok\n");
     return failures == 0 ? 0 : 1;
 }

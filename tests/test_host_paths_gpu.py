@@ -78,7 +78,8 @@ def test_launch_host_mean_rejects_ragged_groups(golden_extra):
     n = int(extra["starts"][-1])
     with api.Function("sphere_pt_f32", n, "regroup") as f:
         with pytest.raises(api.LoomError) as e:
-            f.launch_host_mean([api.Instance(), api.LocalIota()], n, group=3,
+            # 6144 threads are no multiple of 5
+            f.launch_host_mean([api.Instance(), api.LocalIota()], n, group=5,
                                instance_starts=extra["starts"], table=extra["table"])
         assert e.value.code == api.ERR_INVALID
     with api.Function("collatz_u64", 64, "regroup") as f:
