@@ -94,8 +94,8 @@ typedef struct loom_b200_opts
                              largest same-PC group has >= utr_lanes lanes
                              (the GPU form of Loom's UTR, simd.hpp:3273-3292) */
     uint32_t period;      /* regroup: max block steps per tile per round;
-                             LOOM_B200_PERIOD_UNBOUNDED with schedule 2: a
-                             warp never parks, so the launch runs one round,
+                             LOOM_B200_PERIOD_UNBOUNDED with schedule 2 or 3:
+                             a warp never parks, so the launch runs one round,
                              admits every input at once and needs no queue
                              state (a few KB instead of 2 x row bytes per
                              thread in flight) */
@@ -129,7 +129,11 @@ typedef struct loom_b200_opts
                              block earliest in program order, so lagging lanes
                              catch up and merge; 2 steps one block at a time
                              in that order without votes or parking (a
-                             reconvergence stack in software, plus refill) */
+                             reconvergence stack in software, plus refill);
+                             3 runs each warp's lanes along their own paths
+                             under the hardware's reconvergence, as the plain
+                             engine does, and gives the warp new threads when
+                             all its lanes have finished (use a large burst) */
     uint32_t host_chunks; /* launch_host: split the threads into this many
                              ranges whose host copies overlap the kernels of
                              the neighbouring ranges (0 = 8 ranges when the
@@ -137,6 +141,18 @@ typedef struct loom_b200_opts
     uint32_t max_regs;    /* regroup: registers per thread of the megakernel,
                              one of the caps compiled for the kernel
                              (loom_b200_kernel_reg_caps); 0 = its default */
+    uint64_t plain_below; /* regroup: launches of fewer threads run the plain
+                             engine, for workloads too small or too uniform
+                             for the persistent megakernel to pay (Loom's
+                             hybrid backend likewise falls back to predicated
+                             execution where regrouping does not pay,
+                             src/vm/simd.hpp:4163-4194); 0 = never */
+    uint32_t defer_lanes; /* regroup, schedule 2: a long block of the kernel
+                             (the longest few, >= 96 instructions) runs only
+                             once this many of the warp's lanes stand at it,
+                             or when no other block is left; its lanes wait
+                             while the others catch up (0 = off) */
+    uint32_t pad1;
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

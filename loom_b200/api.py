@@ -117,6 +117,9 @@ class Opts(ctypes.Structure):
         ("schedule", ctypes.c_uint32),
         ("host_chunks", ctypes.c_uint32),
         ("max_regs", ctypes.c_uint32),
+        ("plain_below", ctypes.c_uint64),
+        ("defer_lanes", ctypes.c_uint32),
+        ("pad1", ctypes.c_uint32),
     ]
 
 
@@ -513,6 +516,8 @@ def make_opts(
     schedule: int = 0,
     host_chunks: int = 0,
     max_regs: int = 0,
+    plain_below: int = 0,
+    defer_lanes: int = 0,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -536,6 +541,8 @@ def make_opts(
         schedule=int(schedule),
         host_chunks=int(host_chunks),
         max_regs=int(max_regs),
+        plain_below=int(plain_below),
+        defer_lanes=int(defer_lanes),
     )
 
 

@@ -46,14 +46,19 @@ SPACE: Dict[str, List] = {
     "ctas_per_sm": [0, 1, 2, 4],
     "prefetch": [True, False],
     "cost_model": [False, True],
-    "schedule": [0, 1, 2],
+    "schedule": [0, 1, 2, 3],
     # 0: the kernel's default cap; the others exist only for kernels large
     # enough to reach a cap (loom_b200_kernel_reg_caps), which the caller
     # passes as this option's values
     "max_regs": [0],
+    # launches below this many threads run the plain engine: 0 never, 2^40
+    # always (where the megakernel does not pay, the tuner may say so)
+    "plain_below": [0, 1 << 40],
+    # schedule 2: lanes a long block waits for (0: off)
+    "defer_lanes": [0, 4, 8, 12, 16, 24],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0, plain_below=0, defer_lanes=0)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:

@@ -58,6 +58,19 @@ REGROUP_MAX_REGS = 64
 REG_VARIANTS = (32, 40, 48, 56, 80, 96, 128)
 REG_VARIANT_MIN_INSTR = 300
 
+# Long blocks: at least this many instructions.  The software-stepped
+# schedule can hold lanes that reach one back until enough of the warp's
+# lanes stand there (opts.defer_lanes), so that its long code runs at a
+# higher lane efficiency (the path tracers' random-number subroutine).
+LONG_BLOCK_INSTR = 96
+
+
+def long_blocks(k: Kernel) -> List[int]:
+    """Blocks of at least LONG_BLOCK_INSTR instructions, longest first (at
+    most 4)."""
+    counts = k.instr_counts()
+    return sorted((b for b in range(k.num_blocks) if counts[b] >= LONG_BLOCK_INSTR), key=lambda b: -counts[b])[:4]
+
 
 def reg_caps(k: Kernel) -> List[int]:
     """Register caps of the megakernel compiled for `k`, default first."""
@@ -414,6 +427,22 @@ def generate(k: Kernel) -> str:
     w("    __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }")
     w("    __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }")
     w("    __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }")
+    lb = long_blocks(k)
+    w(f"    static constexpr int kNumLong = {len(lb)};")
+    w("    // j-th long block (most instructions first)")
+    w("    __device__ __forceinline__ static int long_block(const int j)")
+    w("    {")
+    if lb:
+        w("        switch(j)")
+        w("        {")
+        for j, b in enumerate(lb):
+            w(f"        case {j}: return {b};")
+        w("        default: return -1;")
+        w("        }")
+    else:
+        w("        (void)j;")
+        w("        return -1;")
+    w("    }")
     w("")
     per_block = [[qi for qi, (b, _) in enumerate(queues) if b == blk] for blk in range(nb)]
     maxq = max(len(x) for x in per_block)
@@ -466,13 +495,17 @@ def generate(k: Kernel) -> str:
     w("    // loop iterations (visits of a loop header); returns the block it")
     w("    // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is")
     w("    // above zero is entered only as the first block of the burst, when")
-    w("    // the warp's vote chose it.")
+    w("    // the warp's vote chose it.  A block that loops on itself takes up")
+    w("    // to `spin` further iterations without spending budget (a loop the")
+    w("    // warp's lanes run together needs no step of its own per iteration).")
     w("    template <bool kProf>")
     w("    __device__ __forceinline__ static int")
-    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)")
+    w("    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false,")
+    w("              unsigned spin = 0u)")
     w("    {")
     w("        (void)ctx;")
     w("        (void)stop_heavy;")
+    w("        (void)spin;")
     w("        bool fresh = true; // no block run yet in this burst")
     w("        (void)fresh;")
     w("        switch(entry)")
@@ -484,16 +517,23 @@ def generate(k: Kernel) -> str:
     for blk in k.blocks:
         w(f"    L_B{blk.idx}: // {blk.label}")
         transfer = L.goto_transfer(blk, "        ")
-        if blk.idx in heavy:
+        own = f"goto L_B{blk.idx};"
+        self_loop = blk.idx in headers and blk.idx in blk.successors()
+        if blk.idx in heavy or self_loop:
             # a lane that loops on the block keeps going; one that comes
             # from another block waits for the warp's vote
-            w(f"        if(stop_heavy && !fresh) return {blk.idx};")
+            if blk.idx in heavy:
+                w(f"        if(stop_heavy && !fresh) return {blk.idx};")
             w(f"    L_B{blk.idx}_again:")
-            own = f"goto L_B{blk.idx};"
-            transfer = [t.replace(own, f"goto L_B{blk.idx}_again;") for t in transfer]
+            back = f"goto L_B{blk.idx}_again;"
+            if self_loop:
+                back = f"{{ if(spin != 0u) {{ --spin; goto L_B{blk.idx}_spin; }} goto L_B{blk.idx}_again; }}"
+            transfer = [t.replace(own, back) for t in transfer]
         if blk.idx in headers:
             w(f"        if(budget == 0u) return {blk.idx};")
             w("        --budget;")
+        if self_loop:
+            w(f"    L_B{blk.idx}_spin:")
         if heavy:
             w("        fresh = false;")
         w(f"        if constexpr(kProf) count_block(ctx, {blk.idx}, {len(blk.instrs)}u);")

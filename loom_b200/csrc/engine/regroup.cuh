@@ -88,9 +88,19 @@ struct RegroupParams
     // the group at the block earliest in reverse post-order, so lanes that
     // lag catch up with the others and merge at join blocks and loop heads;
     // 2 steps one block at a time in that order with no vote and no quorum
-    // (lanes park only when the period ends).
+    // (lanes park only when the period ends); 3 runs every live lane along
+    // its own path under the hardware's reconvergence, as the plain engine
+    // does, and takes new threads for the whole warp once all its lanes have
+    // finished (for kernels whose lanes the hardware keeps together).
     unsigned            schedule;
+    // Schedule 2: a long block (K::long_block) runs only once this many of
+    // the warp's lanes stand at it, or when no other block is left (0: off).
+    unsigned            defer_lanes;
 };
+
+/// Iterations of a self-loop a lane runs within one step of schedules 2
+/// and 3 before the step ends at the loop's header.
+constexpr unsigned kSelfLoopSpin = 1024;
 
 __device__ __forceinline__ unsigned
 ld_volatile(const unsigned* p)
@@ -271,22 +281,41 @@ regroup_kernel(const RegroupParams p)
                         if(t != ~0ull) { pf_tid = t; K::load_in(pf, p.cols, t); }
                     }
                 }
-                if(p.schedule == 2u)
+                // Schedule 2 steps one loop iteration at a time, always the
+                // block earliest in reverse post-order among the warp's lanes:
+                // lanes that lag run until they reach the others (MinPC
+                // stepping, the order a reconvergence stack keeps); a long
+                // block waits until defer_lanes lanes stand at it or no
+                // other block is left.  Schedule 3 runs every live lane
+                // along its own path, the hardware reconverging the warp as
+                // in the plain engine; schedules 0 and 1 run the chosen group
+                // (or every live lane once the group has spread_lanes).
+                // One call site keeps one copy of the kernel's code.
+                const bool minpc = p.schedule == 2u;
+                for(unsigned i = 0; i < (minpc ? p.burst : 1u); ++i)
                 {
-                    // one block at a time, always the block earliest in
-                    // reverse post-order among the warp's lanes: lanes that
-                    // lag run until they reach the others (MinPC stepping,
-                    // the order a reconvergence stack keeps)
-                    for(unsigned i = 0; i < p.burst; ++i)
+                    bool run;
+                    if(minpc)
                     {
-                        const unsigned rk = pc >= 0 ? s_rank[pc] : 0xffffffffu;
+                        unsigned rk = pc >= 0 ? s_rank[pc] : 0xffffffffu;
+                        if(p.defer_lanes)
+                            for(int j = 0; j < K::kNumLong; ++j)
+                            {
+                                const int      h  = K::long_block(j);
+                                const unsigned at = __ballot_sync(FULL, pc == h);
+                                if(pc == h && static_cast<unsigned>(__popc(at)) < p.defer_lanes) rk |= 0x10000u;
+                            }
                         const unsigned lo = __reduce_min_sync(FULL, rk);
                         if(lo == 0xffffffffu) break;
-                        if(rk == lo) pc = K::template run_burst<kProf>(pc, R, ctx, 1u);
+                        run = rk == lo;
                     }
+                    else
+                        run = pc >= 0 && (p.schedule == 3u || mc >= p.spread || pc == m);
+                    if(run)
+                        pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
+                                                          cost_on && p.schedule < 2u,
+                                                          p.schedule >= 2u ? kSelfLoopSpin : 0u);
                 }
-                else if(pc >= 0 && (mc >= p.spread || pc == m))
-                    pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on);
                 if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
@@ -304,9 +333,9 @@ regroup_kernel(const RegroupParams p)
                                 atomicAdd(p.inst_done + id, static_cast<unsigned>(__popc(peers)));
                         }
                         pc = kEmpty;
-                        if(pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
+                        if(pf_tid != ~0ull && p.schedule != 3u) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
                     }
-                    if(!dry && p.refill)
+                    if(!dry && p.refill && p.schedule != 3u)
                     {
                         const unsigned need = __ballot_sync(FULL, pc == kEmpty);
                         if(need)
@@ -317,6 +346,23 @@ regroup_kernel(const RegroupParams p)
                     }
                 }
                 if(steps >= p.period) break;
+                if(p.schedule == 3u)
+                {
+                    // the warp takes new threads only when all its lanes
+                    // have finished, so that they start together at block 0
+                    // (the plain engine's lockstep, one warp of threads
+                    // after another)
+                    if(__ballot_sync(FULL, pc >= 0) != 0u) continue;
+                    if(pf_tid != ~0ull) { K::start(R, pf); tid = pf_tid; pf_tid = ~0ull; pc = 0; }
+                    const unsigned need = __ballot_sync(FULL, pc == kEmpty);
+                    if(need && !dry)
+                    {
+                        const unsigned long long t = claim_inputs(need, p.ctl, admit_end, dry);
+                        if(t != ~0ull) { typename K::In in; K::load_in(in, p.cols, t); K::start(R, in); tid = t; pc = 0; }
+                    }
+                    if(__ballot_sync(FULL, pc >= 0) == 0u) break;
+                    continue;
+                }
                 if(p.schedule == 2u)
                 {
                     // a lane left empty by a refill that found no input

@@ -66,6 +66,13 @@ struct K
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
     __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
+    static constexpr int kNumLong = 0;
+    // j-th long block (most instructions first)
+    __device__ __forceinline__ static int long_block(const int j)
+    {
+        (void)j;
+        return -1;
+    }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -88,13 +95,17 @@ struct K
     // loop iterations (visits of a loop header); returns the block it
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
-    // the warp's vote chose it.
+    // the warp's vote chose it.  A block that loops on itself takes up
+    // to `spin` further iterations without spending budget (a loop the
+    // warp's lanes run together needs no step of its own per iteration).
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false,
+              unsigned spin = 0u)
     {
         (void)ctx;
         (void)stop_heavy;
+        (void)spin;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -122,12 +133,13 @@ struct K
     L_B2_again:
         if(budget == 0u) return 2;
         --budget;
+    L_B2_spin:
         fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 4u);
         R.r1 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r1) * static_cast<unsigned long long>(R.r3)));
         R.r3 = static_cast<unsigned long long>(static_cast<unsigned long long>(static_cast<unsigned long long>(R.r3) - static_cast<unsigned long long>(((unsigned long long)0x1ull))));
         R.r2 = static_cast<unsigned long long>(static_cast<bool>(static_cast<unsigned long long>(R.r3) == static_cast<unsigned long long>(((unsigned long long)0x0ull))));
-        if(R.r2) goto L_HALT; else goto L_B2_again;
+        if(R.r2) goto L_HALT; else { if(spin != 0u) { --spin; goto L_B2_spin; } goto L_B2_again; }
     L_HALT:
         return kHalt;
     }

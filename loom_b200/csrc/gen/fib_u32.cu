@@ -69,6 +69,13 @@ struct K
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
     __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
+    static constexpr int kNumLong = 0;
+    // j-th long block (most instructions first)
+    __device__ __forceinline__ static int long_block(const int j)
+    {
+        (void)j;
+        return -1;
+    }
 
     static constexpr int kMaxQueuesPerBlock = 1;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -91,13 +98,17 @@ struct K
     // loop iterations (visits of a loop header); returns the block it
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
-    // the warp's vote chose it.
+    // the warp's vote chose it.  A block that loops on itself takes up
+    // to `spin` further iterations without spending budget (a loop the
+    // warp's lanes run together needs no step of its own per iteration).
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false,
+              unsigned spin = 0u)
     {
         (void)ctx;
         (void)stop_heavy;
+        (void)spin;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -129,6 +140,7 @@ struct K
     L_B2_again:
         if(budget == 0u) return 2;
         --budget;
+    L_B2_spin:
         fresh = false;
         if constexpr(kProf) count_block(ctx, 2, 6u);
         R.r6 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r4) + static_cast<unsigned int>(R.r2)));
@@ -136,7 +148,7 @@ struct K
         R.r2 = static_cast<unsigned int>(R.r6);
         R.r5 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r5) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r3 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r5) <= static_cast<unsigned int>(R.r1)));
-        if(R.r3) goto L_B2_again; else goto L_HALT;
+        if(R.r3) { if(spin != 0u) { --spin; goto L_B2_spin; } goto L_B2_again; } else goto L_HALT;
     L_HALT:
         return kHalt;
     }

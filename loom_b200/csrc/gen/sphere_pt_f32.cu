@@ -201,6 +201,16 @@ struct K
     __device__ __forceinline__ static int block_of(const int q) { return kQueueBlock[q]; }
     __device__ __forceinline__ static unsigned quorum(const int b) { return kQuorumTab[b]; }
     __device__ __forceinline__ static unsigned rank(const int b) { return kRankTab[b]; }
+    static constexpr int kNumLong = 1;
+    // j-th long block (most instructions first)
+    __device__ __forceinline__ static int long_block(const int j)
+    {
+        switch(j)
+        {
+        case 0: return 23;
+        default: return -1;
+        }
+    }
 
     static constexpr int kMaxQueuesPerBlock = 5;
     // j-th queue holding threads that stand at block b (-1: none).
@@ -246,13 +256,17 @@ struct K
     // loop iterations (visits of a loop header); returns the block it
     // stopped at, or kHalt.  With `stop_heavy`, a block whose quorum is
     // above zero is entered only as the first block of the burst, when
-    // the warp's vote chose it.
+    // the warp's vote chose it.  A block that loops on itself takes up
+    // to `spin` further iterations without spending budget (a loop the
+    // warp's lanes run together needs no step of its own per iteration).
     template <bool kProf>
     __device__ __forceinline__ static int
-    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false)
+    run_burst(const int entry, Regs& R, Ctx& ctx, unsigned budget, const bool stop_heavy = false,
+              unsigned spin = 0u)
     {
         (void)ctx;
         (void)stop_heavy;
+        (void)spin;
         bool fresh = true; // no block run yet in this burst
         (void)fresh;
         switch(entry)
@@ -403,6 +417,7 @@ struct K
     L_B3_again:
         if(budget == 0u) return 3;
         --budget;
+    L_B3_spin:
         fresh = false;
         if constexpr(kProf) count_block(ctx, 3, 38u);
         R.r57 = static_cast<float>(table_load<float>(*ctx.cols, static_cast<unsigned>(R.r56)));
@@ -442,7 +457,7 @@ struct K
         R.r55 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r55) + static_cast<unsigned int>(((unsigned int)0x1ull))));
         R.r56 = static_cast<unsigned int>(static_cast<unsigned int>(static_cast<unsigned int>(R.r56) + static_cast<unsigned int>(((unsigned int)0x8ull))));
         R.r33 = static_cast<unsigned int>(static_cast<bool>(static_cast<unsigned int>(R.r55) < static_cast<unsigned int>(R.r13)));
-        if(R.r33) goto L_B3_again; else goto L_B4;
+        if(R.r33) { if(spin != 0u) { --spin; goto L_B3_spin; } goto L_B3_again; } else goto L_B4;
     L_B4: // shade
         fresh = false;
         if constexpr(kProf) count_block(ctx, 4, 2u);

@@ -209,12 +209,13 @@ round_cap(uint64_t cap)
     return (cap + 31) / 32 * 32;
 }
 
-/// Whether a regrouping launch never parks a thread: schedule 2 with no
-/// period limit keeps every thread in its lane until it halts.
+/// Whether a regrouping launch never parks a thread: schedules 2 and 3 with
+/// no period limit keep every thread in its lane until it halts.
 bool
 never_parks(const loom_b200_opts& o)
 {
-    return o.mode == LOOM_B200_REGROUP && o.schedule == 2u && o.period == LOOM_B200_PERIOD_UNBOUNDED;
+    return o.mode == LOOM_B200_REGROUP && (o.schedule == 2u || o.schedule == 3u) &&
+           o.period == LOOM_B200_PERIOD_UNBOUNDED;
 }
 
 /// Threads in flight of a regrouping launch: the requested population, or
@@ -402,7 +403,10 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
     cols.table      = L.table;
     cols.tid_base   = first; // thread ids in flight lie in [first, first + n)
     const loom_b200_opts& o = h->opts;
-    if(o.mode == LOOM_B200_REGROUP)
+    // a regrouping handle runs launches below plain_below threads on the
+    // plain engine (the persistent megakernel does not pay for them)
+    const bool regroup = o.mode == LOOM_B200_REGROUP && n >= o.plain_below;
+    if(regroup)
     {
         // the workspace is reallocated only between launches
         const uint64_t cap = population(h, n);
@@ -414,7 +418,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         }
     }
     LB_CUDA(cudaEventRecord(h->ev0, stream));
-    if(o.mode == LOOM_B200_REGROUP)
+    if(regroup)
     {
         const uint64_t cap = population(h, n);
         // the largest CTA size up to the requested one that fits on an SM
@@ -459,6 +463,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.params.prefetch      = o.no_prefetch ? 0u : 1u;
         L.params.cost_model    = o.cost_model;
         L.params.schedule      = o.schedule;
+        L.params.defer_lanes   = o.defer_lanes;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
         L.regs                 = o.max_regs;
@@ -481,7 +486,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.cols      = cols;
         L.first     = first;
         L.n         = n;
-        L.max_steps = o.max_steps;
+        L.max_steps = o.mode == LOOM_B200_REGROUP ? kDefaultMaxSteps : o.max_steps; // regroup: max_steps counts rounds
         L.status    = h->d_status;
         L.counters  = h->d_counters;
         L.block     = o.block_size;

@@ -638,6 +638,7 @@ slice_launch(loom_b200_server* s, unsigned ctas_per_sm)
     L.params.prefetch      = o.no_prefetch ? 0u : 1u;
     L.params.cost_model    = o.cost_model;
     L.params.schedule      = o.schedule;
+    L.params.defer_lanes   = o.defer_lanes;
     L.params.round0        = static_cast<unsigned>(s->next_round);
     L.params.slice_rounds  = s->cfg.slice_rounds;
     L.params.inst_done     = s->d_done;

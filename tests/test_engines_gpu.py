@@ -115,6 +115,16 @@ REGROUP_VARIANTS = [
     # no period limit: schedule 2 never parks, one round, no queue state
     dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, prefetch=False),
     dict(schedule=2, burst=1, period=api.PERIOD_UNBOUNDED, prefetch=True, block_size=64),
+    # whole warps of threads run plain-fashion inside the persistent kernel
+    dict(schedule=3, burst=1 << 20, period=api.PERIOD_UNBOUNDED),
+    dict(schedule=3, burst=1 << 20, period=api.PERIOD_UNBOUNDED, prefetch=False, population=100),
+    dict(schedule=3, burst=2, period=9, population=300),
+    # launches below plain_below threads run the plain engine
+    dict(plain_below=1 << 40),
+    # schedule 2 holding long blocks back until 8 or all lanes stand there
+    dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, defer_lanes=8),
+    dict(schedule=2, burst=4, period=api.PERIOD_UNBOUNDED, defer_lanes=32, prefetch=True),
+    dict(schedule=2, burst=1, period=5, population=200, defer_lanes=12),
 ]
 
 
