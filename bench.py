@@ -924,9 +924,10 @@ class RegroupService:
         wi = sum(s["warp_instr"] for s in self.p.stats().values())
         return ti / (32.0 * wi) if wi else None
 
-    def busy_ms(self):
-        """Device time of every server's slices so far, summed over servers."""
-        return sum(s["busy_ms"] for s in self.p.stats().values())
+    def slice_times(self):
+        """(summed slice time, time any slice ran) so far, in ms, from the
+        slices' global-timer intervals."""
+        return self.p.slice_ns / 1e6, self.p.union_ns / 1e6
 
     def budget_waits(self):
         return sum(s["budget_waits"] for s in self.p.stats().values())
@@ -1067,7 +1068,7 @@ def serve_measure(seconds: float, rank: int = 0, local: int = 0, parity: bool = 
                 count = max(8, int(rate * seconds))
                 reqs = mix.draw(count)
                 arr = np.cumsum(mix.rng.exponential(1.0 / rate, size=count))
-                busy0 = svc.busy_ms() if hasattr(svc, "busy_ms") else None
+                t_0 = svc.slice_times() if hasattr(svc, "slice_times") else None
                 lat, span, threads = run_requests(svc, reqs, arr)
                 row = {
                     "offered_load": L,
@@ -1077,12 +1078,15 @@ def serve_measure(seconds: float, rank: int = 0, local: int = 0, parity: bool = 
                     "p99_ms": round(float(np.percentile(lat, 99)) * 1e3, 2),
                     "mean_ms": round(float(lat.mean()) * 1e3, 2),
                 }
-                if busy0 is not None:
-                    # device time of all servers' slices over the wall time:
-                    # above 1 when slices of different kernels ran together
-                    row["servers_busy_ms"] = round(svc.busy_ms() - busy0, 1)
+                if t_0 is not None:
+                    # the slices' device time summed over servers, against the
+                    # time during which any slice ran: above 1 when slices of
+                    # different kernels ran on the GPU together
+                    t_1 = svc.slice_times()
+                    row["slices_ms"] = round(t_1[0] - t_0[0], 1)
+                    row["any_slice_ms"] = round(t_1[1] - t_0[1], 1)
                     row["wall_ms"] = round(span * 1e3, 1)
-                    row["overlap"] = round((svc.busy_ms() - busy0) / (span * 1e3), 3)
+                    row["overlap"] = round((t_1[0] - t_0[0]) / max(1e-9, t_1[1] - t_0[1]), 3)
                 res["loads"].append(row)
             if parity and name == "regroup":
                 res["parity"] = serve_parity(svc, inputs)

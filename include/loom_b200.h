@@ -440,6 +440,9 @@ typedef struct loom_b200_server_stats
     uint64_t budget_waits; /* requests that waited for the budget at least once */
     uint64_t held_bytes;   /* budget bytes held by this server's requests in flight */
     double   busy_ms;      /* device time of the slices (CUDA events on the server's stream) */
+    uint64_t slice_t0_ns;  /* the last slice's first CTA start and its end, */
+    uint64_t slice_t1_ns;  /* on the GPU's global timer (ns): slices of
+                              servers whose intervals intersect ran at once */
 } loom_b200_server_stats;
 
 /* `opts`: engine options (population = resident threads; 0: 2^21);

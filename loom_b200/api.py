@@ -237,6 +237,8 @@ class ServerStatsC(ctypes.Structure):
         ("budget_waits", ctypes.c_uint64),
         ("held_bytes", ctypes.c_uint64),
         ("busy_ms", ctypes.c_double),
+        ("slice_t0_ns", ctypes.c_uint64),
+        ("slice_t1_ns", ctypes.c_uint64),
     ]
 
 

@@ -49,7 +49,17 @@ struct RegroupCtl
     unsigned long long cursor;     // next input index to admit
     unsigned long long admit_end;  // inputs below this index may enter this round
     unsigned long long next_round; // round number the next launch continues with
+    unsigned long long t_first;    // %globaltimer (ns) when the first CTA started
+    unsigned long long t_last;     // %globaltimer when the launch finished
 };
+
+__device__ __forceinline__ unsigned long long
+global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 struct RegroupParams
 {
@@ -201,6 +211,7 @@ regroup_kernel(const RegroupParams p)
     // block ranks in reverse post-order, for the schedules that order groups
     __shared__ unsigned s_rank[K::kNumBlocks];
     for(int i = threadIdx.x; i < K::kNumBlocks; i += blockDim.x) s_rank[i] = K::rank(i);
+    if(threadIdx.x == 0) atomicMin(&p.ctl->t_first, global_ns());
     __syncthreads();
     unsigned long long parks = 0, sbytes = 0, finished = 0;
     typename K::Regs   R;
@@ -449,6 +460,7 @@ regroup_kernel(const RegroupParams p)
                     done = 1u;
                 }
                 p.ctl->next_round = round + 1ull;
+                if(done) p.ctl->t_last = global_ns();
                 *reinterpret_cast<volatile unsigned*>(&p.ctl->done) = done;
                 if(done) atomicAdd(p.counters + 5, ran);
             });

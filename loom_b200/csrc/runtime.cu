@@ -80,6 +80,8 @@ regroup_reset(RegroupCtl*        ctl,
         ctl->pad0      = 0u;
         ctl->cursor    = first;
         ctl->admit_end = admit_end;
+        ctl->t_first   = ~0ull;
+        ctl->t_last    = 0ull;
     }
 }
 

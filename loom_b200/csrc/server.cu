@@ -81,6 +81,8 @@ serve_reset(RegroupCtl* ctl, unsigned* qcnt, unsigned* qhead, unsigned num_queue
         ctl->cursor     = 0ull;
         ctl->admit_end  = 0ull;
         ctl->next_round = 0ull;
+        ctl->t_first    = ~0ull;
+        ctl->t_last     = 0ull;
     }
 }
 
@@ -107,6 +109,8 @@ serve_resume(RegroupCtl*        ctl,
     }
     ctl->bar_count = 0u;
     ctl->done      = 0u;
+    ctl->t_first   = ~0ull;
+    ctl->t_last    = 0ull;
     const unsigned long long c    = ctl->cursor;
     const unsigned long long room = parked < cap ? cap - parked : 0ull;
     ctl->admit_end                = c + room < n ? c + room : n;
@@ -687,6 +691,8 @@ slice_harvest(loom_b200_server* s)
     if(cudaEventElapsedTime(&ms, s->ev_a, s->ev_k) == cudaSuccess) s->st.busy_ms += ms;
     const unsigned status = *s->h_status;
     s->next_round      = s->h_ctl->next_round;
+    s->st.slice_t0_ns  = s->h_ctl->t_first;
+    s->st.slice_t1_ns  = s->h_ctl->t_last;
     s->st.slices      += 1;
     s->st.status      |= status;
     s->st.thread_instr = s->h_counters[0];

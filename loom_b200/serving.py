@@ -29,6 +29,8 @@ class Pool:
         # CTAs per SM of each server's slice while several servers run (None:
         # one server after the other)
         self.shared_ctas = shared_ctas
+        self.slice_ns = 0  # device time of the slices, summed over servers
+        self.union_ns = 0  # time at least one slice ran
         self._work = {k: 0 for k in self.servers}  # submitted, not completed
         self._failed: List[Tuple[str, int, int]] = []
         if timeout:
@@ -46,16 +48,43 @@ class Pool:
     def step(self) -> List[Tuple[str, int]]:
         done = []
         busy = [k for k, srv in self.servers.items() if self._work[k]]
-        if self.shared_ctas and len(busy) > 1:
+        together = bool(self.shared_ctas) and len(busy) > 1
+        if together:
             for k in busy:
                 self.servers[k].launch(self.shared_ctas.get(k, 1))
+        spans = []
         for k in busy:
             srv = self.servers[k]
+            slices = srv.stats()["slices"]
             for t in srv.step():
                 done.append((k, t))
                 self._work[k] -= 1
+            st = srv.stats()
+            if st["slices"] > slices and st["slice_t1_ns"] > st["slice_t0_ns"]:
+                spans.append((st["slice_t0_ns"], st["slice_t1_ns"]))
             self._collect(k, srv)
+        self._account(spans)
         return done
+
+    def _account(self, spans) -> None:
+        """Adds this step's slice intervals (global-timer ns) to the device
+        time of the slices (their sum) and to the time any slice ran (their
+        union): sum / union above 1 means slices of different kernels ran on
+        the GPU at the same time."""
+        if not spans:
+            return
+        self.slice_ns += sum(b - a for a, b in spans)
+        union, end = 0, 0
+        for a, b in sorted(spans):
+            a = max(a, end)
+            if b > a:
+                union += b - a
+                end = b
+        self.union_ns += union
+
+    def overlap(self) -> float:
+        """Summed slice time over the time any slice ran (1.0: no overlap)."""
+        return self.slice_ns / self.union_ns if self.union_ns else 1.0
 
     def cancel(self, kind: str, ticket: int) -> bool:
         ok = self.servers[kind].cancel(ticket)

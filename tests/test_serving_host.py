@@ -9,11 +9,21 @@ CANCELLED, TIMEOUT = -8, -9
 
 
 class FakeServer:
-    def __init__(self):
+    def __init__(self, span=None, log=None):
         self.next = 0
         self.queued = []
         self.failed_q = []
         self.timeout = None
+        self.slices = 0
+        self.span = span  # (start, end) global-timer ns of every slice
+        self.log = log if log is not None else []
+
+    def stats(self):
+        a, b = self.span or (0, 0)
+        return {"slices": self.slices, "slice_t0_ns": a, "slice_t1_ns": b}
+
+    def launch(self, ctas):
+        self.log.append(("launch", self, ctas))
 
     def submit(self, n, **request):
         self.next += 1
@@ -22,6 +32,9 @@ class FakeServer:
 
     def step(self):
         # completes the oldest request each step
+        self.log.append(("step", self, None))
+        if self.queued:
+            self.slices += 1
         return [self.queued.pop(0)] if self.queued else []
 
     def cancel(self, ticket):
@@ -71,3 +84,25 @@ def test_watchdog_failures_are_collected_by_step():
         assert pool.step() == []
         assert pool.failures() == [("a", t[0], TIMEOUT), ("a", t[1], TIMEOUT)]
         assert not pool.busy()
+
+
+def test_busy_servers_start_their_slices_together():
+    """With shared_ctas, a step with several busy servers starts every
+    slice (launch with that server's CTAs per SM) before completing any; a
+    step with one busy server just steps it.  The slices' global-timer
+    intervals give the summed slice time and the time any slice ran."""
+    log = []
+    a = FakeServer(span=(100, 300), log=log)
+    b = FakeServer(span=(200, 500), log=log)
+    pool = Pool({"a": a, "b": b}, shared_ctas={"a": 1, "b": 2})
+    pool.submit("a", 4)
+    pool.submit("a", 4)
+    pool.submit("b", 4)
+    pool.step()
+    assert [(e[0], e[1], e[2]) for e in log] == [("launch", a, 1), ("launch", b, 2), ("step", a, None), ("step", b, None)]
+    assert (pool.slice_ns, pool.union_ns) == (200 + 300, 400)  # [100, 500] covered
+    assert abs(pool.overlap() - 500 / 400) < 1e-12
+    log.clear()
+    pool.step()  # only a is busy now: no launch ahead of the step
+    assert [e[0] for e in log] == ["step"]
+    assert (pool.slice_ns, pool.union_ns) == (700, 600)
