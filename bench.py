@@ -1296,6 +1296,10 @@ def workload_summary(w, res, world, cpu=None, want=None, e2e=None, tids=None):
         },
         "speedup_vs_plain": round(pl["ms"] / rg["ms"], 4),
     }
+    if rg["opts"].get("plain_below", 0) > w.n:
+        # the tuner measured that the persistent megakernel does not pay for
+        # this workload: the regrouping handle runs it on the plain engine
+        d["engine_used"] = "plain (regrouping handle's plain_below rule, set by the tuner)"
     for name, r in res.items():
         if name in ("plain", "regroup"):
             continue

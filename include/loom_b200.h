@@ -461,14 +461,14 @@ int loom_b200_server_submit(loom_b200_server* s, const loom_b200_request* r, uin
  * and returns up to max_done of their tickets (the rest on later calls).
  * After loom_b200_server_launch it completes the slice that call started. */
 int loom_b200_server_step(loom_b200_server* s, uint64_t* done, uint32_t max_done, uint32_t* n_done);
-/* Admits what fits and starts the next slice without waiting for it, with
- * ctas_per_sm CTAs per SM (0: the server's own launch shape), so that the
- * slices of several servers (each on its own stream) run on the GPU at the
- * same time; the next loom_b200_server_step completes it.  Servers whose
- * slices overlap must fit on the SMs together (registers, threads, shared
- * memory of one CTA each per SM), since each slice is a cooperative launch
- * whose CTAs are resident together.  Nothing is launched when no request is
- * in flight or admissible. */
+/* Admits what fits and starts the next slice without waiting for it, so
+ * that the slices of several servers (each on its own stream) run on the
+ * GPU at the same time; the next loom_b200_server_step completes it.  With
+ * ctas_per_sm > 0 the slice has that many CTAs per SM and runs one round as
+ * an ordinary launch (no grid barrier, so it shares the SMs with the other
+ * servers' slices; a cooperative launch would not); 0 keeps the server's
+ * own launch shape and slice length.  Nothing is launched when no request
+ * is in flight or admissible. */
 int loom_b200_server_launch(loom_b200_server* s, uint32_t ctas_per_sm);
 int loom_b200_server_get_stats(const loom_b200_server* s, loom_b200_server_stats* st);
 /* Cancels a request (no counterpart in Loom, whose streams have no request

@@ -657,6 +657,8 @@ def generate(k: Kernel) -> str:
     w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
     w("    const void* fn = regroup_fn(a.regs, a.profile);")
     w("    if(!fn) return cudaErrorInvalidValue;")
+    w("    if(a.ordinary && a.params.slice_rounds == 1u)")
+    w("        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
     w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
     w("}")
     w("")

@@ -136,6 +136,7 @@ grid_barrier(RegroupCtl*        ctl,
              unsigned*          status,
              unsigned long long spins,
              unsigned           phantoms,
+             bool               final_round,
              F&&                last)
 {
     __shared__ int ok;
@@ -152,6 +153,12 @@ grid_barrier(RegroupCtl*        ctl,
             ctl->bar_count = 0;
             __threadfence();
             atomicAdd(&ctl->bar_gen, 1u);
+        }
+        else if(final_round)
+        {
+            // the launch ends with this round whatever the last CTA finds:
+            // nothing to wait for (the CTAs need not be resident together)
+            go = 0;
         }
         else
         {
@@ -435,6 +442,7 @@ regroup_kernel(const RegroupParams p)
             p.status,
             p.barrier_spins,
             p.phantoms,
+            p.slice_rounds == 1u,
             [&]()
             {
                 unsigned long long parked = 0;

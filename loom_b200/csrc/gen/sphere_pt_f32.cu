@@ -2762,6 +2762,8 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.ordinary && a.params.slice_rounds == 1u)
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
     return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
 }
 

@@ -29,6 +29,11 @@ struct RegroupLaunch
     unsigned      block;
     unsigned      regs; // register cap of the megakernel (0: the kernel's default)
     bool          profile;
+    // a one-round slice (params.slice_rounds == 1) waits at no grid
+    // barrier, so it may be an ordinary launch, which can run on the GPU
+    // beside other kernels; every other launch is cooperative (its CTAs
+    // resident together, as the grid barrier between rounds needs)
+    bool          ordinary = false;
     cudaStream_t  stream;
 };
 

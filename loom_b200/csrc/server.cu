@@ -644,7 +644,11 @@ slice_launch(loom_b200_server* s, unsigned ctas_per_sm)
     L.params.schedule      = o.schedule;
     L.params.defer_lanes   = o.defer_lanes;
     L.params.round0        = static_cast<unsigned>(s->next_round);
-    L.params.slice_rounds  = s->cfg.slice_rounds;
+    // beside other servers' slices: one round, an ordinary launch (no grid
+    // barrier to wait at), so that the GPU runs the slices together;
+    // cooperative launches do not share the GPU with other kernels
+    L.params.slice_rounds  = ctas_per_sm ? 1u : s->cfg.slice_rounds;
+    L.ordinary             = ctas_per_sm != 0u;
     L.params.inst_done     = s->d_done;
     L.grid                 = s->grid;
     if(ctas_per_sm)
