@@ -108,8 +108,8 @@ struct RegroupParams
     unsigned            defer_lanes;
 };
 
-/// Iterations of a self-loop a lane runs within one step of schedules 2
-/// and 3 before the step ends at the loop's header.
+/// Iterations of a self-loop a lane runs within one step of schedule 2
+/// before the step ends at the loop's header.
 constexpr unsigned kSelfLoopSpin = 1024;
 
 __device__ __forceinline__ unsigned
@@ -124,12 +124,13 @@ ld_volatile64(const unsigned long long* p)
     return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
 
-/// Grid barrier with a bounded wait.  The last CTA to arrive runs `last`
-/// before releasing the others.  Returns whether the CTA should run another
-/// round: false when the launch is done or when the wait ran out (the status
-/// word then carries kStatusBarrierTimeout and ctl->done is set).  The value
-/// is decided by thread 0 and shared, so every thread of the CTA leaves the
-/// round loop together.
+/// Grid barrier with a bounded wait.  The first warp of the last CTA to
+/// arrive runs `last` (every lane of it: the round-end work is spread over
+/// the warp) before releasing the others.  Returns whether the CTA should
+/// run another round: false when the launch is done or when the wait ran
+/// out (the status word then carries kStatusBarrierTimeout and ctl->done is
+/// set).  The value is decided by thread 0 and shared, so every thread of
+/// the CTA leaves the round loop together.
 template <typename F>
 __device__ bool
 grid_barrier(RegroupCtl*        ctl,
@@ -139,22 +140,42 @@ grid_barrier(RegroupCtl*        ctl,
              bool               final_round,
              F&&                last)
 {
-    __shared__ int ok;
+    __shared__ int      ok;
+    __shared__ int      is_last;
+    __shared__ unsigned gen0;
     __syncthreads();
     if(threadIdx.x == 0)
     {
-        int            go  = 1;
-        const unsigned gen = ld_volatile(&ctl->bar_gen);
+        gen0 = ld_volatile(&ctl->bar_gen);
         __threadfence();
         const unsigned arrived = atomicAdd(&ctl->bar_count, 1u);
-        if(arrived == gridDim.x - 1 + phantoms)
+        is_last = arrived == gridDim.x - 1 + phantoms ? 1 : 0;
+    }
+    __syncthreads();
+    if(is_last)
+    {
+        if(threadIdx.x < 32)
         {
-            last();
-            ctl->bar_count = 0;
             __threadfence();
-            atomicAdd(&ctl->bar_gen, 1u);
+            last();
+            __threadfence(); // every lane's resets visible before the release
+            __syncwarp();
+            if(threadIdx.x == 0)
+            {
+                ctl->bar_count = 0;
+                __threadfence();
+                atomicAdd(&ctl->bar_gen, 1u);
+                ok = ld_volatile(&ctl->done) != 0u ? 0 : 1;
+            }
         }
-        else if(final_round)
+        __syncthreads();
+        return ok != 0;
+    }
+    if(threadIdx.x == 0)
+    {
+        int            go  = 1;
+        const unsigned gen = gen0;
+        if(final_round)
         {
             // the launch ends with this round whatever the last CTA finds:
             // nothing to wait for (the CTAs need not be resident together)
@@ -239,30 +260,45 @@ regroup_kernel(const RegroupParams p)
         bool                     dry  = false;
         for(;;)
         {
+            // a tile of the current round's queues: the warp reads 32
+            // queues' counts and pop cursors at once, and takes 32 entries
+            // from the first non-empty queue at or after bsel (warps start
+            // at different queues, so they contend less)
             int      tb = kEmpty;
             unsigned tk = 0, toff = 0;
-            if(lane == 0)
+            for(int c = 0; c < (B + 31) / 32 && tb < 0; ++c)
             {
-                for(int i = 0; i < B; ++i)
+                const int base = ((static_cast<int>(bsel) / 32 + c) % ((B + 31) / 32)) * 32;
+                const int b    = base + static_cast<int>(lane);
+                unsigned  cnt  = 0, head = 0;
+                if(b < B)
                 {
-                    const unsigned b = (bsel + i) % B;
-                    unsigned cnt     = ld_volatile(&p.qcnt[cur * B + b]);
-                    if(cnt > p.cap) cnt = p.cap;
-                    if(ld_volatile(&p.qhead[b]) >= cnt) continue;
-                    const unsigned off = atomicAdd(&p.qhead[b], 32u);
-                    if(off < cnt)
+                    cnt  = ld_volatile(&p.qcnt[cur * B + b]);
+                    cnt  = cnt > p.cap ? p.cap : cnt;
+                    head = ld_volatile(&p.qhead[b]);
+                }
+                unsigned avail = __ballot_sync(FULL, b < B && head < cnt);
+                const unsigned s0 = c == 0 ? bsel % 32u : 0u;
+                while(avail)
+                {
+                    // first available queue at or after s0, cyclically
+                    const unsigned rot  = s0 ? ((avail >> s0) | (avail << (32u - s0))) : avail;
+                    const unsigned pick = (static_cast<unsigned>(__ffs(rot)) - 1u + s0) & 31u;
+                    unsigned       off  = 0;
+                    if(lane == pick) off = atomicAdd(&p.qhead[b], 32u);
+                    off                = __shfl_sync(FULL, off, static_cast<int>(pick));
+                    const unsigned pc_ = __shfl_sync(FULL, cnt, static_cast<int>(pick));
+                    if(off < pc_)
                     {
-                        tb   = static_cast<int>(b);
+                        tb   = base + static_cast<int>(pick);
                         toff = off;
-                        tk   = cnt - off < 32u ? cnt - off : 32u;
-                        bsel = b;
+                        tk   = pc_ - off < 32u ? pc_ - off : 32u;
+                        bsel = static_cast<unsigned>(tb);
                         break;
                     }
+                    avail &= ~(1u << pick);
                 }
             }
-            tb   = __shfl_sync(FULL, tb, 0);
-            tk   = __shfl_sync(FULL, tk, 0);
-            toff = __shfl_sync(FULL, toff, 0);
             int                pc  = kEmpty;
             unsigned long long tid = 0;
             if(tb >= 0)
@@ -308,7 +344,9 @@ regroup_kernel(const RegroupParams p)
                 // along its own path, the hardware reconverging the warp as
                 // in the plain engine; schedules 0 and 1 run the chosen group
                 // (or every live lane once the group has spread_lanes).
-                // One call site keeps one copy of the kernel's code.
+                // Two call sites: the stepped schedule's (self-loops spin,
+                // budget 1) and the others' (no spin, so a tight self-loop
+                // pays no spin check per iteration).
                 const bool minpc = p.schedule == 2u;
                 for(unsigned i = 0; i < (minpc ? p.burst : 1u); ++i)
                 {
@@ -330,9 +368,12 @@ regroup_kernel(const RegroupParams p)
                     else
                         run = pc >= 0 && (p.schedule == 3u || mc >= p.spread || pc == m);
                     if(run)
-                        pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
-                                                          cost_on && p.schedule < 2u,
-                                                          p.schedule >= 2u ? kSelfLoopSpin : 0u);
+                    {
+                        if(minpc)
+                            pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, kSelfLoopSpin);
+                        else
+                            pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on && p.schedule < 2u);
+                    }
                 }
                 if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
@@ -445,13 +486,19 @@ regroup_kernel(const RegroupParams p)
             p.slice_rounds == 1u,
             [&]()
             {
+                // every lane of the first warp of the last CTA: the threads
+                // parked for the next round (summed over the queues), the
+                // current round's counts and pop cursors cleared; lane 0
+                // then sets the next admission limit and decides the end
                 unsigned long long parked = 0;
-                for(int b = 0; b < B; ++b)
+                for(int b = static_cast<int>(lane); b < B; b += 32)
                 {
                     parked += ld_volatile(&p.qcnt[nxt * B + b]);
                     p.qcnt[cur * B + b] = 0u;
                     p.qhead[b]          = 0u;
                 }
+                for(int o = 16; o > 0; o >>= 1) parked += __shfl_xor_sync(FULL, parked, o);
+                if(lane != 0) return;
                 // claims beyond the limit were refused: give them back
                 unsigned long long c = ld_volatile64(&p.ctl->cursor);
                 if(c > admit_end) c = admit_end;

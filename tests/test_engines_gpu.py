@@ -35,6 +35,17 @@ def _as_list(x):
 # units in the last place of the scalar backend's value, and integer outputs
 # (ray counts, pixel ids) stay exact.
 ULP_TOLERANCE = {"pt2_const_40": 4, "pt2_const_512": 4}
+# ... and the image those float outputs form (one radiance channel per
+# output, one pixel per thread) within this relative RMSE:
+# sqrt(mean((got - want)^2)) / sqrt(mean(want^2)).
+IMAGE_RMSE_TOLERANCE = 1e-6
+
+
+def image_rmse(got, want) -> float:
+    g = np.asarray(got, dtype=np.float64)
+    w = np.asarray(want, dtype=np.float64)
+    ref = float(np.sqrt(np.mean(w * w))) if w.size else 0.0
+    return float(np.sqrt(np.mean((g - w) ** 2))) / ref if ref > 0 else 0.0
 
 
 def _check(name, got, want):
@@ -43,6 +54,7 @@ def _check(name, got, want):
             g, w = np.asarray(g), np.asarray(w)
             ulps = np.abs(g.astype(np.float64) - w.astype(np.float64)) / np.spacing(np.abs(w)).astype(np.float64)
             assert float(ulps.max()) <= ULP_TOLERANCE[name], f"{name}: {float(ulps.max())} ulp apart"
+            assert image_rmse(g, w) <= IMAGE_RMSE_TOLERANCE, f"{name}: image RMSE {image_rmse(g, w):.3g}"
             continue
         assert np.array_equal(_bits(g), _bits(w)), f"{name}: {int((g != w).sum())} threads differ"
 
