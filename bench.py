@@ -1420,6 +1420,8 @@ def main() -> None:
     ap.add_argument("--only", metavar="FORM", default="",
                     help="time one engine or form alone (plain, regroup, majority_cost_model, "
                          "lane_efficiency_form): no counted launch, no end-to-end leg, no CPU leg (for profilers)")
+    ap.add_argument("--form-opts", default="", metavar="JSON",
+                    help="with --only: options merged into the form's tuned ones")
     ap.add_argument("--no-configs", action="store_true",
                     help="pt: skip the other configurations (fib, collatz, batch, serve) of the default run")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="serve: open-loop seconds per load")
@@ -1506,7 +1508,7 @@ def main() -> None:
     if args.only:
         # one engine or form, W + K launches and nothing else: the launch
         # sequence a profiler's -s/-c counts refer to
-        opts = {} if args.only == "plain" else forms[args.only]
+        opts = {} if args.only == "plain" else dict(forms[args.only], **json.loads(args.form_opts or "{}"))
         f = api.Function(w.kernel, 0, "plain" if args.only == "plain" else "regroup", **opts)
         ms = time_steps(lambda: w.launch(f, api, stream), args.steps, warmup, torch, dist)
         st = f.stats(raise_on_device_error=True)

@@ -57,6 +57,9 @@ REGROUP_MAX_REGS = 64
 # per workload (opts.max_regs), trading warps per SM against spills.
 REG_VARIANTS = (32, 40, 48, 56, 80, 96, 128)
 REG_VARIANT_MIN_INSTR = 300
+# Small kernels: the megakernel's own state dominates their registers, and a
+# cap that fits one more CTA per SM can pay for latency-bound loops.
+SMALL_REG_VARIANTS = (40, 48)
 
 # Long blocks: at least this many instructions.  The software-stepped
 # schedule can hold lanes that reach one back until enough of the warp's
@@ -74,9 +77,9 @@ def long_blocks(k: Kernel) -> List[int]:
 
 def reg_caps(k: Kernel) -> List[int]:
     """Register caps of the megakernel compiled for `k`, default first."""
-    if sum(k.instr_counts()) <= REG_VARIANT_MIN_INSTR:
-        return [REGROUP_MAX_REGS]
-    return [REGROUP_MAX_REGS] + [c for c in REG_VARIANTS if c != REGROUP_MAX_REGS]
+    extra = REG_VARIANTS if sum(k.instr_counts()) > REG_VARIANT_MIN_INSTR else SMALL_REG_VARIANTS
+    return [REGROUP_MAX_REGS] + [c for c in extra if c != REGROUP_MAX_REGS]
+
 
 CTYPE = {
     "b8": "bool",

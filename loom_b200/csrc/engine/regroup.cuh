@@ -241,7 +241,11 @@ regroup_kernel(const RegroupParams p)
     for(int i = threadIdx.x; i < K::kNumBlocks; i += blockDim.x) s_rank[i] = K::rank(i);
     if(threadIdx.x == 0) atomicMin(&p.ctl->t_first, global_ns());
     __syncthreads();
-    unsigned long long parks = 0, sbytes = 0, finished = 0;
+    // per-lane counters, 32 bits (a lane's share of one launch), summed into
+    // the 64-bit launch counters at the end
+    unsigned           parks = 0, sbytes = 0, finished = 0;
+    // the round's admission limit, read once per CTA
+    __shared__ unsigned long long s_admit_end;
     typename K::Regs   R;
     typename K::In     pf;
     unsigned long long pf_tid = ~0ull;
@@ -255,7 +259,9 @@ regroup_kernel(const RegroupParams p)
     for(unsigned round = p.round0;; ++round)
     {
         const unsigned           cur = round & 1u, nxt = cur ^ 1u;
-        const unsigned long long admit_end = ld_volatile64(&p.ctl->admit_end);
+        if(threadIdx.x == 0) s_admit_end = ld_volatile64(&p.ctl->admit_end);
+        __syncthreads();
+        const unsigned long long& admit_end = s_admit_end;
         unsigned                 bsel = gwarp % B;
         bool                     dry  = false;
         for(;;)
@@ -522,8 +528,8 @@ regroup_kernel(const RegroupParams p)
         if(!more) break;
     }
 
-    flush_counters(p.counters, ctx.thread_instr, ctx.warp_instr, parks);
-    flush_counters(p.counters + 3, sbytes, finished, 0ull);
+    flush_counters(p.counters, ctx.thread_instr, ctx.warp_instr, static_cast<unsigned long long>(parks));
+    flush_counters(p.counters + 3, static_cast<unsigned long long>(sbytes), static_cast<unsigned long long>(finished), 0ull);
     if constexpr(kProf) block_counters_flush(s_blk, K::kNumBlocks, p.counters + 8);
 }
 } // namespace loom_b200

@@ -209,7 +209,7 @@ cudaError_t launch_plain(const PlainLaunch& a)
     return cudaGetLastError();
 }
 
-const unsigned kRegCaps[] = {64u};
+const unsigned kRegCaps[] = {64u, 40u, 48u};
 
 /// The megakernel at register cap `regs` (0: the default); profiled
 /// launches use the default cap.  NULL: no such cap compiled.
@@ -220,6 +220,8 @@ const void* regroup_fn(unsigned regs, bool profile)
     {
     case 0u:
     case 64u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 64>);
+    case 40u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 40>);
+    case 48u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 48>);
     default: return nullptr;
     }
 }
@@ -249,4 +251,4 @@ const loom_b200::KernelEntry loom_b200_entry_arithmetic_f32 = {
     &loom_b200::k_arithmetic_f32::launch_plain, &loom_b200::k_arithmetic_f32::launch_regroup,
     &loom_b200::k_arithmetic_f32::regroup_occupancy,
     loom_b200::k_arithmetic_f32::kQueues, loom_b200::k_arithmetic_f32::kSegments,
-    loom_b200::k_arithmetic_f32::kRegCaps, 1u};
+    loom_b200::k_arithmetic_f32::kRegCaps, 3u};

@@ -192,7 +192,7 @@ cudaError_t launch_plain(const PlainLaunch& a)
     return cudaGetLastError();
 }
 
-const unsigned kRegCaps[] = {64u};
+const unsigned kRegCaps[] = {64u, 40u, 48u};
 
 /// The megakernel at register cap `regs` (0: the default); profiled
 /// launches use the default cap.  NULL: no such cap compiled.
@@ -203,6 +203,8 @@ const void* regroup_fn(unsigned regs, bool profile)
     {
     case 0u:
     case 64u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 64>);
+    case 40u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 40>);
+    case 48u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 48>);
     default: return nullptr;
     }
 }
@@ -232,4 +234,4 @@ const loom_b200::KernelEntry loom_b200_entry_sct_inv_u32 = {
     &loom_b200::k_sct_inv_u32::launch_plain, &loom_b200::k_sct_inv_u32::launch_regroup,
     &loom_b200::k_sct_inv_u32::regroup_occupancy,
     loom_b200::k_sct_inv_u32::kQueues, loom_b200::k_sct_inv_u32::kSegments,
-    loom_b200::k_sct_inv_u32::kRegCaps, 1u};
+    loom_b200::k_sct_inv_u32::kRegCaps, 3u};
