@@ -142,7 +142,8 @@ def test_register_caps_keep_results(name, golden, golden_extra):
 
 
 def test_register_cap_not_compiled_is_refused():
-    with api.Function("collatz_u64", 64, "regroup", max_regs=40) as f:
+    assert 72 not in api.reg_caps("collatz_u64")
+    with api.Function("collatz_u64", 64, "regroup", max_regs=72) as f:
         with pytest.raises(api.LoomError) as e:
             f(np.arange(64, dtype=np.uint64))
         assert e.value.code == api.ERR_INVALID
