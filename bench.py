@@ -1542,6 +1542,10 @@ def main() -> None:
                                         args.no_cpu)
         configs["batch"] = sub_config("batch", api, torch, stream, max(2, args.steps // 4), 3, dist, world,
                                       args.no_cpu)
+        # Loom's own path tracers at 512x512 (where the tuner found that the
+        # megakernel does not pay and set the regrouping handle's plain rule)
+        for name in ("loom_pt_512", "loom_pt2_512"):
+            configs[name] = sub_config(name, api, torch, stream, 3, 3, dist, world, args.no_cpu)
         sv, sv_clk = serve_measure(1.0, rank, local, parity=not args.no_cpu)
         full = sv["regroup"]["loads"][-1]
         configs["serve"] = {
