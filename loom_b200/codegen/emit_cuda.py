@@ -300,6 +300,46 @@ class Lowering:
         return "L_HALT" if t == HALT else f"L_B{t}"
 
 
+def pack_slots(items, start: int) -> Dict:
+    """Queue row layout from `start` (bytes per entry): items (register,
+    bytes) and the input index ("tid", 4).  Registers of 8 and 4 bytes and
+    the index are packed largest first into slots of 16 bytes, each at an
+    offset that is a multiple of its size; the last slot shrinks to 8 or 4
+    bytes when that holds its contents; registers of 1 or 2 bytes get a slot
+    each.  Returns {"slots": [(off, width, [(item, sub)])], "cols": {reg: (off,
+    sub, width)}, "tid": (off, sub, width), "end": next offset, a multiple
+    of 8}."""
+    wide = sorted([(r, n) for r, n in items if n >= 4], key=lambda x: (-x[1], x[0])) + [("tid", 4)]
+    narrow = sorted([(r, n) for r, n in items if n < 4], key=lambda x: (-x[1], x[0]))
+    slots = []
+    cur, used = [], 0
+    for it, n in wide:
+        if used + n > 16:
+            slots.append((cur, used))
+            cur, used = [], 0
+        cur.append((it, used, n))
+        used += n
+    if cur:
+        slots.append((cur, used))
+    out, off = [], start
+    for contents, used in slots:
+        width = 16 if used > 8 else (8 if used > 4 else 4)
+        out.append((off, width, [(it, sub) for it, sub, _ in contents]))
+        off += width
+    for it, n in narrow:
+        out.append((off, n, [(it, 0)]))
+        off += n
+    end = (off + 7) // 8 * 8
+    cols, tid = {}, None
+    for o, wdt, contents in out:
+        for it, sub in contents:
+            if it == "tid":
+                tid = (o, sub, wdt)
+            else:
+                cols[it] = (o, sub, wdt)
+    return {"slots": out, "cols": cols, "tid": tid, "end": end}
+
+
 def generate(k: Kernel) -> str:
     L = Lowering(k)
     name = k.name
@@ -319,22 +359,16 @@ def generate(k: Kernel) -> str:
     disp = k.dispatch_blocks()
     nq = len(queues)
     qbytes = [sum(L.regs[r].nbytes for r in li) for li in qlive]
-    # queue segments: per queue, live-in columns by decreasing size, then the
-    # u32 input index; each segment padded to 8 bytes per entry
+    # queue segments: per queue, the live-in registers and the u32 input
+    # index packed into slots of 16 bytes per entry (then 8, 4: the rest),
+    # so a lane saves or restores four 32-bit values with one 128-bit access
+    # and a warp's 32 entries of a slot are 512 contiguous bytes; registers
+    # of 1 or 2 bytes keep slots of their own
     layout = []
     row_total = 0
     for q in range(nq):
-        cols = sorted(qlive[q], key=lambda r: (-L.regs[r].nbytes, r))
-        off = row_total
-        placed = []
-        for r in cols:
-            placed.append((r, off))
-            off += L.regs[r].nbytes
-        tid_off = off
-        off += 4
-        off = (off + 7) // 8 * 8
-        layout.append({"cols": placed, "tid": tid_off})
-        row_total = off
+        layout.append(pack_slots([(r, L.regs[r].nbytes) for r in qlive[q]], row_total))
+        row_total = layout[-1]["end"]
 
     o: List[str] = []
     w = o.append
@@ -564,22 +598,55 @@ def generate(k: Kernel) -> str:
         w("        {")
         for qi, (b, kk) in enumerate(queues):
             w(f"        case {qi}: // {k.blocks[b].label}" + ("" if kk is None else f", context {kk}"))
+            w("        {")
             if fn == "restore" and kk is not None:
                 v = disp[b][0]
                 w(f"            R.r{v} = static_cast<{CTYPE[L.regs[v].storage]}>({kk});")
-            for r, off in layout[qi]["cols"]:
-                stt = CTYPE[L.regs[r].storage]
-                col = f"reinterpret_cast<{q}{stt}*>(base + {off}ull * cap)[idx]"
+            tid_expr = None
+            for si, (off, wdt, contents) in enumerate(layout[qi]["slots"]):
+                vt = {16: "uint4", 8: "uint2", 4: "unsigned", 2: "unsigned short", 1: "unsigned char"}[wdt]
+                slot = f"reinterpret_cast<{q}{vt}*>(base + {off}ull * cap)[idx]"
+                if wdt <= 2:
+                    # a narrow register alone in its slot
+                    (r, _), = contents
+                    stt = CTYPE[L.regs[r].storage]
+                    if fn == "save":
+                        w(f"            {slot} = bitcast<{vt}>(R.r{r});")
+                    else:
+                        w(f"            R.r{r} = bitcast<{stt}>({slot});")
+                    continue
+                words = ["x", "y", "z", "w"][: wdt // 4] if wdt > 4 else [None]
+                def word(sub):
+                    return f"v{si}" if words == [None] else f"v{si}.{words[sub // 4]}"
                 if fn == "save":
-                    w(f"            {col} = R.r{r};")
+                    w(f"            {{")
+                    w(f"                {vt} v{si};")
+                    for it, sub in contents:
+                        if it == "tid":
+                            w(f"                {word(sub)} = tid;")
+                        elif L.regs[it].nbytes == 8:
+                            w(f"                {{ const unsigned long long b = bitcast<unsigned long long>(R.r{it});")
+                            w(f"                  {word(sub)} = static_cast<unsigned>(b); {word(sub + 4)} = static_cast<unsigned>(b >> 32); }}")
+                        else:
+                            w(f"                {word(sub)} = bitcast<unsigned>(R.r{it});")
+                    w(f"                {slot} = v{si};")
+                    w(f"            }}")
                 else:
-                    w(f"            R.r{r} = {col};")
-            tcol = f"reinterpret_cast<{q}unsigned*>(base + {layout[qi]['tid']}ull * cap)[idx]"
+                    w(f"            const {vt} v{si} = {slot};")
+                    for it, sub in contents:
+                        if it == "tid":
+                            tid_expr = word(sub)
+                        elif L.regs[it].nbytes == 8:
+                            stt = CTYPE[L.regs[it].storage]
+                            w(f"            R.r{it} = bitcast<{stt}>((static_cast<unsigned long long>({word(sub + 4)}) << 32) | {word(sub)});")
+                        else:
+                            stt = CTYPE[L.regs[it].storage]
+                            w(f"            R.r{it} = bitcast<{stt}>({word(sub)});")
             if fn == "save":
-                w(f"            {tcol} = tid;")
                 w("            return;")
             else:
-                w(f"            return {tcol};")
+                w(f"            return {tid_expr};")
+            w("        }")
         w("        default: " + ("return;" if fn == "save" else "return 0xffffffffu;"))
         w("        }")
         w("    }")
@@ -604,16 +671,21 @@ def generate(k: Kernel) -> str:
     assert all(rg.idx == i for i, rg in enumerate(k.regs)), "registers out of order"
     assert all(qk is None or -(2**31) <= qk < 2**31 for _, qk in queues), "dispatch context out of range"
     for qi, (qb, qk) in enumerate(queues):
-        cols = layout[qi]["cols"]
+        # columns in register-size order (the order of the queue analysis)
+        cols = sorted(layout[qi]["cols"], key=lambda r: (-L.regs[r].nbytes, r))
+        layout[qi]["order"] = cols
         if cols:
-            w(f"const uint32_t kQRegs{qi}[] = {{{', '.join(f'{r}u' for r, _ in cols)}}};")
-            w(f"const int kQTypes{qi}[] = {{{', '.join(ABI_TYPE[L.regs[r].storage] for r, _ in cols)}}};")
-            names = ", ".join('"' + k.regs[r].name + '"' for r, _ in cols)
+            at = layout[qi]["cols"]
+            w(f"const uint32_t kQRegs{qi}[] = {{{', '.join(f'{r}u' for r in cols)}}};")
+            w(f"const int kQTypes{qi}[] = {{{', '.join(ABI_TYPE[L.regs[r].storage] for r in cols)}}};")
+            names = ", ".join('"' + k.regs[r].name + '"' for r in cols)
             w(f"const char* const kQNames{qi}[] = {{{names}}};")
-            w(f"const unsigned long long kQOffs{qi}[] = {{{', '.join(f'{off}ull' for _, off in cols)}}};")
+            w(f"const unsigned long long kQOffs{qi}[] = {{{', '.join(f'{at[r][0]}ull' for r in cols)}}};")
+            w(f"const unsigned kQSubs{qi}[] = {{{', '.join(f'{at[r][1]}u' for r in cols)}}};")
+            w(f"const unsigned kQWidths{qi}[] = {{{', '.join(f'{at[r][2]}u' for r in cols)}}};")
     w("const loom_b200_queue_layout kQueues[] = {")
     for qi, (qb, qk) in enumerate(queues):
-        cols = layout[qi]["cols"]
+        cols = layout[qi]["order"]
         if cols:
             w(f"    {{{qb}u, {-1 if qk is None else qk}, {len(cols)}u, kQRegs{qi}, kQTypes{qi}, kQNames{qi}}},")
         else:
@@ -621,8 +693,10 @@ def generate(k: Kernel) -> str:
     w("};")
     w("const QueueSegment kSegments[] = {")
     for qi in range(nq):
-        offs = f"kQOffs{qi}" if layout[qi]["cols"] else "nullptr"
-        w(f"    {{{offs}, {layout[qi]['tid']}ull}},")
+        has = bool(layout[qi]["order"])
+        offs = f"kQOffs{qi}, kQSubs{qi}, kQWidths{qi}" if has else "nullptr, nullptr, nullptr"
+        t = layout[qi]["tid"]
+        w(f"    {{{offs}, {t[0]}ull, {t[1]}u, {t[2]}u}},")
     w("};")
     w("")
     w("cudaError_t launch_plain(const PlainLaunch& a)")

@@ -350,9 +350,8 @@ regroup_kernel(const RegroupParams p)
                 // along its own path, the hardware reconverging the warp as
                 // in the plain engine; schedules 0 and 1 run the chosen group
                 // (or every live lane once the group has spread_lanes).
-                // Two call sites: the stepped schedule's (self-loops spin,
-                // budget 1) and the others' (no spin, so a tight self-loop
-                // pays no spin check per iteration).
+                // One call site keeps one copy of the kernel's code in the
+                // megakernel (self-loops spin only in the stepped schedule).
                 const bool minpc = p.schedule == 2u;
                 for(unsigned i = 0; i < (minpc ? p.burst : 1u); ++i)
                 {
@@ -374,12 +373,8 @@ regroup_kernel(const RegroupParams p)
                     else
                         run = pc >= 0 && (p.schedule == 3u || mc >= p.spread || pc == m);
                     if(run)
-                    {
-                        if(minpc)
-                            pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, kSelfLoopSpin);
-                        else
-                            pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on && p.schedule < 2u);
-                    }
+                        pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
+                                                          cost_on && p.schedule < 2u, minpc ? kSelfLoopSpin : 0u);
                 }
                 if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);

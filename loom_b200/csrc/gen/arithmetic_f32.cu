@@ -147,11 +147,17 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<float*>(base + 4ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned*>(base + 12ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r0);
+                v0.y = bitcast<unsigned>(R.r1);
+                v0.z = bitcast<unsigned>(R.r2);
+                v0.w = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -164,10 +170,13 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const float*>(base + 4ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 12ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned int>(v0.x);
+            R.r1 = bitcast<float>(v0.y);
+            R.r2 = bitcast<float>(v0.z);
+            return v0.w;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -188,12 +197,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u, 2u};
 const int kQTypes0[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames0[] = {"a", "b", "c"};
-const unsigned long long kQOffs0[] = {0ull, 4ull, 8ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull, 0ull};
+const unsigned kQSubs0[] = {0u, 4u, 8u};
+const unsigned kQWidths0[] = {16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 3u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 12ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 12u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

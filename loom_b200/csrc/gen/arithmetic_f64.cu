@@ -147,11 +147,24 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<double*>(base + 8ull * cap)[idx] = R.r1;
-            reinterpret_cast<double*>(base + 16ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r0);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.z = static_cast<unsigned>(b); v0.w = static_cast<unsigned>(b >> 32); }
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r2);
+                  v1.x = static_cast<unsigned>(b); v1.y = static_cast<unsigned>(b >> 32); }
+                v1.z = tid;
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -164,10 +177,14 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const double*>(base + 8ull * cap)[idx];
-            R.r2 = reinterpret_cast<const double*>(base + 16ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            R.r1 = bitcast<double>((static_cast<unsigned long long>(v0.w) << 32) | v0.z);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r2 = bitcast<double>((static_cast<unsigned long long>(v1.y) << 32) | v1.x);
+            return v1.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -188,12 +205,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u, 2u};
 const int kQTypes0[] = {LOOM_B200_U64, LOOM_B200_F64, LOOM_B200_F64};
 const char* const kQNames0[] = {"a", "b", "c"};
-const unsigned long long kQOffs0[] = {0ull, 8ull, 16ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull, 16ull};
+const unsigned kQSubs0[] = {0u, 8u, 0u};
+const unsigned kQWidths0[] = {16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 3u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 24ull},
+    {kQOffs0, kQSubs0, kQWidths0, 16ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

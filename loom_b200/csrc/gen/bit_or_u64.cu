@@ -132,10 +132,22 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<unsigned long long*>(base + 8ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r0);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.z = static_cast<unsigned>(b); v0.w = static_cast<unsigned>(b >> 32); }
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
+            {
+                unsigned v1;
+                v1 = tid;
+                reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -148,9 +160,13 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 8ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.w) << 32) | v0.z);
+            const unsigned v1 = reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+            return v1;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -171,12 +187,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u};
 const int kQTypes0[] = {LOOM_B200_U64, LOOM_B200_U64};
 const char* const kQNames0[] = {"a", "b"};
-const unsigned long long kQOffs0[] = {0ull, 8ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull};
+const unsigned kQSubs0[] = {0u, 8u};
+const unsigned kQWidths0[] = {16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 16ull},
+    {kQOffs0, kQSubs0, kQWidths0, 16ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

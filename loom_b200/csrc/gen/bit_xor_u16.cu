@@ -132,10 +132,16 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned short*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<unsigned short*>(base + 2ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 0ull * cap)[idx] = v0;
+            }
+            reinterpret_cast<unsigned short*>(base + 4ull * cap)[idx] = bitcast<unsigned short>(R.r0);
+            reinterpret_cast<unsigned short*>(base + 6ull * cap)[idx] = bitcast<unsigned short>(R.r1);
             return;
+        }
         default: return;
         }
     }
@@ -148,9 +154,12 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned short*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const unsigned short*>(base + 2ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned short>(reinterpret_cast<const unsigned short*>(base + 4ull * cap)[idx]);
+            R.r1 = bitcast<unsigned short>(reinterpret_cast<const unsigned short*>(base + 6ull * cap)[idx]);
+            return v0;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -171,12 +180,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u};
 const int kQTypes0[] = {LOOM_B200_U16, LOOM_B200_U16};
 const char* const kQNames0[] = {"a", "b"};
-const unsigned long long kQOffs0[] = {0ull, 2ull};
+const unsigned long long kQOffs0[] = {4ull, 6ull};
+const unsigned kQSubs0[] = {0u, 0u};
+const unsigned kQWidths0[] = {2u, 2u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 4ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -154,14 +154,28 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // loop
-            reinterpret_cast<unsigned long long*>(base + 16ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 24ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned*>(base + 28ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = bitcast<unsigned>(R.r2);
+                v0.w = tid;
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -174,12 +188,18 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            return v0.z;
+        }
         case 1: // loop
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 16ull * cap)[idx];
-            R.r2 = reinterpret_cast<const unsigned int*>(base + 24ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 28ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            R.r2 = bitcast<unsigned int>(v0.z);
+            return v0.w;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -201,17 +221,21 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U64};
 const char* const kQNames0[] = {"n"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {16u};
 const uint32_t kQRegs1[] = {1u, 2u};
 const int kQTypes1[] = {LOOM_B200_U64, LOOM_B200_U32};
 const char* const kQNames1[] = {"n", "steps"};
-const unsigned long long kQOffs1[] = {16ull, 24ull};
+const unsigned long long kQOffs1[] = {16ull, 16ull};
+const unsigned kQSubs1[] = {0u, 8u};
+const unsigned kQWidths1[] = {16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 2u, kQRegs1, kQTypes1, kQNames1},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
-    {kQOffs1, 28ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
+    {kQOffs1, kQSubs1, kQWidths1, 16ull, 12u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -159,14 +159,24 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<float*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<float*>(base + 4ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 12ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 16ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 20ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r0);
+                v0.y = bitcast<unsigned>(R.r1);
+                v0.z = bitcast<unsigned>(R.r2);
+                v0.w = bitcast<unsigned>(R.r3);
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r4);
+                v1.y = bitcast<unsigned>(R.r5);
+                v1.z = tid;
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -179,13 +189,17 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const float*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const float*>(base + 4ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 12ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 16ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 20ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<float>(v0.x);
+            R.r1 = bitcast<float>(v0.y);
+            R.r2 = bitcast<float>(v0.z);
+            R.r3 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r4 = bitcast<float>(v1.x);
+            R.r5 = bitcast<float>(v1.y);
+            return v1.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -206,12 +220,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u, 2u, 3u, 4u, 5u};
 const int kQTypes0[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames0[] = {"x0", "x1", "x2", "y0", "y1", "y2"};
-const unsigned long long kQOffs0[] = {0ull, 4ull, 8ull, 12ull, 16ull, 20ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull, 0ull, 0ull, 16ull, 16ull};
+const unsigned kQSubs0[] = {0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths0[] = {16u, 16u, 16u, 16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 6u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 24ull},
+    {kQOffs0, kQSubs0, kQWidths0, 16ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -153,18 +153,36 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // cinit
-            reinterpret_cast<unsigned int*>(base + 8ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 12ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 8ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 2: // loop
-            reinterpret_cast<unsigned int*>(base + 16ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 20ull * cap)[idx] = R.r3;
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r3);
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -177,15 +195,24 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         case 1: // cinit
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 12ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 8ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         case 2: // loop
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 16ull * cap)[idx];
-            R.r3 = reinterpret_cast<const unsigned int*>(base + 20ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r3 = bitcast<unsigned int>(v0.y);
+            return v0.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -207,23 +234,29 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U32};
 const char* const kQNames0[] = {"a"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {8u};
 const uint32_t kQRegs1[] = {1u};
 const int kQTypes1[] = {LOOM_B200_U32};
 const char* const kQNames1[] = {"a"};
 const unsigned long long kQOffs1[] = {8ull};
+const unsigned kQSubs1[] = {0u};
+const unsigned kQWidths1[] = {8u};
 const uint32_t kQRegs2[] = {1u, 3u};
 const int kQTypes2[] = {LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames2[] = {"a", "c"};
-const unsigned long long kQOffs2[] = {16ull, 20ull};
+const unsigned long long kQOffs2[] = {16ull, 16ull};
+const unsigned kQSubs2[] = {0u, 4u};
+const unsigned kQWidths2[] = {16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 1u, kQRegs1, kQTypes1, kQNames1},
     {2u, -1, 2u, kQRegs2, kQTypes2, kQNames2},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 4ull},
-    {kQOffs1, 12ull},
-    {kQOffs2, 24ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 4u, 8u},
+    {kQOffs1, kQSubs1, kQWidths1, 8ull, 4u, 8u},
+    {kQOffs2, kQSubs2, kQWidths2, 16ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -162,20 +162,42 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // work
-            reinterpret_cast<unsigned int*>(base + 8ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 12ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 8ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 2: // loop
-            reinterpret_cast<unsigned int*>(base + 16ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 20ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned int*>(base + 24ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 28ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r4);
+                v0.w = bitcast<unsigned>(R.r5);
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
+            {
+                unsigned v1;
+                v1 = tid;
+                reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -188,17 +210,27 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         case 1: // work
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 12ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 8ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         case 2: // loop
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 16ull * cap)[idx];
-            R.r2 = reinterpret_cast<const unsigned int*>(base + 20ull * cap)[idx];
-            R.r4 = reinterpret_cast<const unsigned int*>(base + 24ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 28ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<unsigned int>(v0.y);
+            R.r4 = bitcast<unsigned int>(v0.z);
+            R.r5 = bitcast<unsigned int>(v0.w);
+            const unsigned v1 = reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+            return v1;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -220,23 +252,29 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U32};
 const char* const kQNames0[] = {"n"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {8u};
 const uint32_t kQRegs1[] = {1u};
 const int kQTypes1[] = {LOOM_B200_U32};
 const char* const kQNames1[] = {"n"};
 const unsigned long long kQOffs1[] = {8ull};
+const unsigned kQSubs1[] = {0u};
+const unsigned kQWidths1[] = {8u};
 const uint32_t kQRegs2[] = {1u, 2u, 4u, 5u};
 const int kQTypes2[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames2[] = {"n", "c", "p", "i"};
-const unsigned long long kQOffs2[] = {16ull, 20ull, 24ull, 28ull};
+const unsigned long long kQOffs2[] = {16ull, 16ull, 16ull, 16ull};
+const unsigned kQSubs2[] = {0u, 4u, 8u, 12u};
+const unsigned kQWidths2[] = {16u, 16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 1u, kQRegs1, kQTypes1, kQNames1},
     {2u, -1, 4u, kQRegs2, kQTypes2, kQNames2},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 4ull},
-    {kQOffs1, 12ull},
-    {kQOffs2, 32ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 4u, 8u},
+    {kQOffs1, kQSubs1, kQWidths1, 8ull, 4u, 8u},
+    {kQOffs2, kQSubs2, kQWidths2, 32ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -162,20 +162,52 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // work
-            reinterpret_cast<unsigned long long*>(base + 16ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 2: // loop
-            reinterpret_cast<unsigned long long*>(base + 32ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned long long*>(base + 40ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned long long*>(base + 48ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned long long*>(base + 56ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned*>(base + 64ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                { const unsigned long long b = bitcast<unsigned long long>(R.r2);
+                  v0.z = static_cast<unsigned>(b); v0.w = static_cast<unsigned>(b >> 32); }
+                reinterpret_cast<uint4*>(base + 32ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r4);
+                  v1.x = static_cast<unsigned>(b); v1.y = static_cast<unsigned>(b >> 32); }
+                { const unsigned long long b = bitcast<unsigned long long>(R.r5);
+                  v1.z = static_cast<unsigned>(b); v1.w = static_cast<unsigned>(b >> 32); }
+                reinterpret_cast<uint4*>(base + 48ull * cap)[idx] = v1;
+            }
+            {
+                unsigned v2;
+                v2 = tid;
+                reinterpret_cast<unsigned*>(base + 64ull * cap)[idx] = v2;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -188,17 +220,28 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            return v0.z;
+        }
         case 1: // work
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 16ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            return v0.z;
+        }
         case 2: // loop
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 32ull * cap)[idx];
-            R.r2 = reinterpret_cast<const unsigned long long*>(base + 40ull * cap)[idx];
-            R.r4 = reinterpret_cast<const unsigned long long*>(base + 48ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned long long*>(base + 56ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 64ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 32ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            R.r2 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.w) << 32) | v0.z);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 48ull * cap)[idx];
+            R.r4 = bitcast<unsigned long long>((static_cast<unsigned long long>(v1.y) << 32) | v1.x);
+            R.r5 = bitcast<unsigned long long>((static_cast<unsigned long long>(v1.w) << 32) | v1.z);
+            const unsigned v2 = reinterpret_cast<const unsigned*>(base + 64ull * cap)[idx];
+            return v2;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -220,23 +263,29 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U64};
 const char* const kQNames0[] = {"n"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {16u};
 const uint32_t kQRegs1[] = {1u};
 const int kQTypes1[] = {LOOM_B200_U64};
 const char* const kQNames1[] = {"n"};
 const unsigned long long kQOffs1[] = {16ull};
+const unsigned kQSubs1[] = {0u};
+const unsigned kQWidths1[] = {16u};
 const uint32_t kQRegs2[] = {1u, 2u, 4u, 5u};
 const int kQTypes2[] = {LOOM_B200_U64, LOOM_B200_U64, LOOM_B200_U64, LOOM_B200_U64};
 const char* const kQNames2[] = {"n", "c", "p", "i"};
-const unsigned long long kQOffs2[] = {32ull, 40ull, 48ull, 56ull};
+const unsigned long long kQOffs2[] = {32ull, 32ull, 48ull, 48ull};
+const unsigned kQSubs2[] = {0u, 8u, 0u, 8u};
+const unsigned kQWidths2[] = {16u, 16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 1u, kQRegs1, kQTypes1, kQNames1},
     {2u, -1, 4u, kQRegs2, kQTypes2, kQNames2},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
-    {kQOffs1, 24ull},
-    {kQOffs2, 64ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
+    {kQOffs1, kQSubs1, kQWidths1, 16ull, 8u, 16u},
+    {kQOffs2, kQSubs2, kQWidths2, 64ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -128,9 +128,15 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned char*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<unsigned*>(base + 1ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 0ull * cap)[idx] = v0;
+            }
+            reinterpret_cast<unsigned char*>(base + 4ull * cap)[idx] = bitcast<unsigned char>(R.r0);
             return;
+        }
         default: return;
         }
     }
@@ -143,8 +149,11 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned char*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned char>(reinterpret_cast<const unsigned char*>(base + 4ull * cap)[idx]);
+            return v0;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -165,12 +174,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u};
 const int kQTypes0[] = {LOOM_B200_U8};
 const char* const kQNames0[] = {"val"};
-const unsigned long long kQOffs0[] = {0ull};
+const unsigned long long kQOffs0[] = {4ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {1u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 1ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

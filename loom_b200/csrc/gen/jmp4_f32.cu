@@ -166,21 +166,51 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // l0
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 2: // l1
-            reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 3: // l2
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 4: // l3
-            reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -193,16 +223,31 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         case 1: // l0
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+            return v0;
+        }
         case 2: // l1
-            return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+            return v0;
+        }
         case 3: // l2
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+            return v0;
+        }
         case 4: // l3
-            return reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+            return v0;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -224,6 +269,8 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U32};
 const char* const kQNames0[] = {"i"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {8u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 0u, nullptr, nullptr, nullptr},
@@ -232,11 +279,11 @@ const loom_b200_queue_layout kQueues[] = {
     {4u, -1, 0u, nullptr, nullptr, nullptr},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 4ull},
-    {nullptr, 8ull},
-    {nullptr, 16ull},
-    {nullptr, 24ull},
-    {nullptr, 32ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 4u, 8u},
+    {nullptr, nullptr, nullptr, 8ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 16ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 24ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 32ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

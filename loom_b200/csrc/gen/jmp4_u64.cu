@@ -166,21 +166,52 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned long long*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r1);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // l0
-            reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 16ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 2: // l1
-            reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 24ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 3: // l2
-            reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 32ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 4: // l3
-            reinterpret_cast<unsigned*>(base + 40ull * cap)[idx] = tid;
+        {
+            {
+                unsigned v0;
+                v0 = tid;
+                reinterpret_cast<unsigned*>(base + 40ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -193,16 +224,31 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned long long*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned long long>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            return v0.z;
+        }
         case 1: // l0
-            return reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 16ull * cap)[idx];
+            return v0;
+        }
         case 2: // l1
-            return reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 24ull * cap)[idx];
+            return v0;
+        }
         case 3: // l2
-            return reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 32ull * cap)[idx];
+            return v0;
+        }
         case 4: // l3
-            return reinterpret_cast<const unsigned*>(base + 40ull * cap)[idx];
+        {
+            const unsigned v0 = reinterpret_cast<const unsigned*>(base + 40ull * cap)[idx];
+            return v0;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -224,6 +270,8 @@ const uint32_t kQRegs0[] = {1u};
 const int kQTypes0[] = {LOOM_B200_U64};
 const char* const kQNames0[] = {"i"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 0u, nullptr, nullptr, nullptr},
@@ -232,11 +280,11 @@ const loom_b200_queue_layout kQueues[] = {
     {4u, -1, 0u, nullptr, nullptr, nullptr},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
-    {nullptr, 16ull},
-    {nullptr, 24ull},
-    {nullptr, 32ull},
-    {nullptr, 40ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
+    {nullptr, nullptr, nullptr, 16ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 24ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 32ull, 0u, 4u},
+    {nullptr, nullptr, nullptr, 40ull, 0u, 4u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -137,10 +137,16 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<float*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<float*>(base + 4ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r0);
+                v0.y = bitcast<unsigned>(R.r1);
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -153,9 +159,12 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const float*>(base + 0ull * cap)[idx];
-            R.r1 = reinterpret_cast<const float*>(base + 4ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<float>(v0.x);
+            R.r1 = bitcast<float>(v0.y);
+            return v0.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -176,12 +185,14 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {0u, 1u};
 const int kQTypes0[] = {LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames0[] = {"a", "b"};
-const unsigned long long kQOffs0[] = {0ull, 4ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull};
+const unsigned kQSubs0[] = {0u, 4u};
+const unsigned kQWidths0[] = {16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

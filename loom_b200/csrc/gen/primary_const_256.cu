@@ -1060,911 +1060,1869 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 4ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r53);
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // roll
-            reinterpret_cast<unsigned int*>(base + 16ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 20ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 24ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 28ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 32ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 36ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 40ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 44ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 48ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 52ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 56ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 60ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 64ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r8);
+                v1.z = bitcast<unsigned>(R.r9);
+                v1.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 32ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r13);
+                v2.y = bitcast<unsigned>(R.r15);
+                v2.z = bitcast<unsigned>(R.r17);
+                v2.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 48ull * cap)[idx] = v2;
+            }
+            {
+                unsigned v3;
+                v3 = tid;
+                reinterpret_cast<unsigned*>(base + 64ull * cap)[idx] = v3;
+            }
             return;
+        }
         case 2: // traverse_box
-            reinterpret_cast<unsigned int*>(base + 72ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 76ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 80ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 84ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 88ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 92ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 96ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 100ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 104ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 108ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 112ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 116ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 120ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 124ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 128ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 132ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 136ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 140ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 144ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 148ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 152ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 156ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 72ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 88ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 104ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 120ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 136ull * cap)[idx] = v4;
+            }
+            {
+                uint2 v5;
+                v5.x = bitcast<unsigned>(R.r53);
+                v5.y = tid;
+                reinterpret_cast<uint2*>(base + 152ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 3: // isect_quad_l1
-            reinterpret_cast<unsigned int*>(base + 160ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 164ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 168ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 172ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 176ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 180ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 184ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 188ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 192ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 196ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 200ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 204ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 208ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 212ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 216ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 220ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 224ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 228ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 232ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 236ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 240ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 244ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 248ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 252ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 256ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 260ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 264ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 268ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 272ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 276ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 280ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 284ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 288ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 292ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 296ull * cap)[idx] = R.r51;
-            reinterpret_cast<float*>(base + 300ull * cap)[idx] = R.r52;
-            reinterpret_cast<unsigned int*>(base + 304ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 308ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 160ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 176ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 192ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 208ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 224ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 240ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 256ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r38);
+                v7.y = bitcast<unsigned>(R.r39);
+                v7.z = bitcast<unsigned>(R.r40);
+                v7.w = bitcast<unsigned>(R.r41);
+                reinterpret_cast<uint4*>(base + 272ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r42);
+                v8.y = bitcast<unsigned>(R.r50);
+                v8.z = bitcast<unsigned>(R.r51);
+                v8.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 288ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r53);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 304ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 4: // isect_quad_l2
-            reinterpret_cast<unsigned int*>(base + 312ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 316ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 320ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 324ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 328ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 332ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 336ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 340ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 344ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 348ull * cap)[idx] = R.r10;
-            reinterpret_cast<float*>(base + 352ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 356ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 360ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 364ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 368ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 372ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 376ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 380ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 384ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 388ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 392ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 396ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 400ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 404ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 408ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 412ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 416ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 420ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 424ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 428ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 432ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 436ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 440ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 444ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 448ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 452ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 312ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 328ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r10);
+                v2.z = bitcast<unsigned>(R.r12);
+                v2.w = bitcast<unsigned>(R.r13);
+                reinterpret_cast<uint4*>(base + 344ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r14);
+                v3.y = bitcast<unsigned>(R.r15);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 360ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r21);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r27);
+                v4.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 376ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r29);
+                v5.y = bitcast<unsigned>(R.r30);
+                v5.z = bitcast<unsigned>(R.r31);
+                v5.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 392ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r33);
+                v6.y = bitcast<unsigned>(R.r34);
+                v6.z = bitcast<unsigned>(R.r35);
+                v6.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 408ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r37);
+                v7.y = bitcast<unsigned>(R.r38);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 424ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r42);
+                v8.z = bitcast<unsigned>(R.r53);
+                v8.w = tid;
+                reinterpret_cast<uint4*>(base + 440ull * cap)[idx] = v8;
+            }
             return;
+        }
         case 5: // isect_quad_l3
-            reinterpret_cast<unsigned int*>(base + 456ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 460ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 464ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 468ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 472ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 476ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 480ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 484ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 488ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 492ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 496ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 500ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 504ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 508ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 512ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 516ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 520ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 524ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 528ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 532ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 536ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 540ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 544ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 548ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 552ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 556ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 560ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 564ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 568ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 572ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 576ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 580ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 584ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 588ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 592ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned*>(base + 596ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 456ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 472ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r10);
+                v2.z = bitcast<unsigned>(R.r11);
+                v2.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 488ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r13);
+                v3.y = bitcast<unsigned>(R.r14);
+                v3.z = bitcast<unsigned>(R.r15);
+                v3.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 504ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r20);
+                v4.y = bitcast<unsigned>(R.r21);
+                v4.z = bitcast<unsigned>(R.r22);
+                v4.w = bitcast<unsigned>(R.r27);
+                reinterpret_cast<uint4*>(base + 520ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r28);
+                v5.y = bitcast<unsigned>(R.r29);
+                v5.z = bitcast<unsigned>(R.r30);
+                v5.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 536ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r32);
+                v6.y = bitcast<unsigned>(R.r33);
+                v6.z = bitcast<unsigned>(R.r34);
+                v6.w = bitcast<unsigned>(R.r35);
+                reinterpret_cast<uint4*>(base + 552ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r36);
+                v7.y = bitcast<unsigned>(R.r37);
+                v7.z = bitcast<unsigned>(R.r38);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 568ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r42);
+                v8.w = tid;
+                reinterpret_cast<uint4*>(base + 584ull * cap)[idx] = v8;
+            }
             return;
+        }
         case 6: // isect_quad_l4
-            reinterpret_cast<unsigned int*>(base + 600ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 604ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 608ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 612ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 616ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 620ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 624ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 628ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 632ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 636ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 640ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 644ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 648ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 652ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 656ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 660ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 664ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 668ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 672ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 676ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 680ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 684ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 688ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 692ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 696ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 700ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 704ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 708ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 712ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 716ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 720ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 724ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 728ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned*>(base + 732ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 600ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 616ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 632ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 648ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 664ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 680ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 696ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r38);
+                v7.y = bitcast<unsigned>(R.r39);
+                v7.z = bitcast<unsigned>(R.r40);
+                v7.w = bitcast<unsigned>(R.r41);
+                reinterpret_cast<uint4*>(base + 712ull * cap)[idx] = v7;
+            }
+            {
+                uint2 v8;
+                v8.x = bitcast<unsigned>(R.r42);
+                v8.y = tid;
+                reinterpret_cast<uint2*>(base + 728ull * cap)[idx] = v8;
+            }
             return;
+        }
         case 7: // isect_quad_l5
-            reinterpret_cast<unsigned int*>(base + 736ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 740ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 744ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 748ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 752ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 756ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 760ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 764ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 768ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 772ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 776ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 780ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 784ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 788ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 792ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 796ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 800ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 804ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 808ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 812ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 816ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 820ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 824ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 828ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 832ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 836ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 840ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 844ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 848ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 852ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 856ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 860ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 864ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 868ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 872ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 876ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 880ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 884ull * cap)[idx] = R.r51;
-            reinterpret_cast<float*>(base + 888ull * cap)[idx] = R.r52;
-            reinterpret_cast<unsigned int*>(base + 892ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 896ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 736ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 752ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 768ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 784ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 800ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 816ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 832ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r38);
+                v7.y = bitcast<unsigned>(R.r39);
+                v7.z = bitcast<unsigned>(R.r40);
+                v7.w = bitcast<unsigned>(R.r41);
+                reinterpret_cast<uint4*>(base + 848ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r42);
+                v8.y = bitcast<unsigned>(R.r43);
+                v8.z = bitcast<unsigned>(R.r44);
+                v8.w = bitcast<unsigned>(R.r45);
+                reinterpret_cast<uint4*>(base + 864ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r50);
+                v9.y = bitcast<unsigned>(R.r51);
+                v9.z = bitcast<unsigned>(R.r52);
+                v9.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 880ull * cap)[idx] = v9;
+            }
+            {
+                unsigned v10;
+                v10 = tid;
+                reinterpret_cast<unsigned*>(base + 896ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 8: // isect_quad_l6
-            reinterpret_cast<unsigned int*>(base + 904ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 908ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 912ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 916ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 920ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 924ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 928ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 932ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 936ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 940ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 944ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 948ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 952ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 956ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 960ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 964ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 968ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 972ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 976ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 980ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 984ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 988ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 992ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 996ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 1000ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 1004ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1008ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1012ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 1016ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1020ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1024ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1028ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1032ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 1036ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1040ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1044ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 1048ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1052ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 904ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 920ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 936ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 952ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 968ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 984ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 1000ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r41);
+                v7.y = bitcast<unsigned>(R.r42);
+                v7.z = bitcast<unsigned>(R.r43);
+                v7.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1016ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r45);
+                v8.y = bitcast<unsigned>(R.r46);
+                v8.z = bitcast<unsigned>(R.r47);
+                v8.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1032ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r53);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 1048ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 9: // isect_quad_l7
-            reinterpret_cast<unsigned int*>(base + 1056ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1060ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1064ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1068ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1072ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1076ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1080ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1084ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1088ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1092ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1096ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1100ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1104ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1108ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1112ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1116ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1120ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1124ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1128ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1132ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1136ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1140ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1144ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1148ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 1152ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 1156ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1160ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1164ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 1168ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1172ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned*>(base + 1176ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1056ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1072ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 1088ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 1104ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 1120ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1136ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 1152ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r41);
+                v7.y = bitcast<unsigned>(R.r42);
+                v7.z = tid;
+                reinterpret_cast<uint4*>(base + 1168ull * cap)[idx] = v7;
+            }
             return;
+        }
         case 10: // isect_quad_end
-            reinterpret_cast<unsigned int*>(base + 1184ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1188ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1192ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1196ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1200ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1204ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1208ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1212ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1216ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1220ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1224ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1228ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1232ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1236ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1240ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1244ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1248ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1252ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1256ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1260ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1264ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 1268ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1272ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1184ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1200ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1216ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1232ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1248ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r49);
+                v5.y = bitcast<unsigned>(R.r53);
+                v5.z = tid;
+                reinterpret_cast<uint4*>(base + 1264ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 11: // traverse_tetrahedron
-            reinterpret_cast<unsigned int*>(base + 1280ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1284ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1288ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1292ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1296ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1300ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1304ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1308ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1312ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1316ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1320ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1324ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1328ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1332ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1336ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1340ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1344ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1348ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1352ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1356ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned*>(base + 1360ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1280ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1296ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1312ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1328ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1344ull * cap)[idx] = v4;
+            }
+            {
+                unsigned v5;
+                v5 = tid;
+                reinterpret_cast<unsigned*>(base + 1360ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 12: // isect_triangle_mid1
-            reinterpret_cast<unsigned int*>(base + 1368ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1372ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1376ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1380ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1384ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1388ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1392ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1396ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1400ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1404ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1408ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1412ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1416ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1420ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1424ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1428ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1432ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1436ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1440ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1444ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1448ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1452ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1456ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 1460ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 1464ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1468ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1472ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1476ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1480ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 1484ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 1488ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1492ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1496ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1500ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1368ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1384ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1400ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1416ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r28);
+                v4.z = bitcast<unsigned>(R.r29);
+                v4.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 1432ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r31);
+                v5.y = bitcast<unsigned>(R.r32);
+                v5.z = bitcast<unsigned>(R.r33);
+                v5.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 1448ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r35);
+                v6.y = bitcast<unsigned>(R.r36);
+                v6.z = bitcast<unsigned>(R.r37);
+                v6.w = bitcast<unsigned>(R.r38);
+                reinterpret_cast<uint4*>(base + 1464ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r39);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r41);
+                v7.w = bitcast<unsigned>(R.r42);
+                reinterpret_cast<uint4*>(base + 1480ull * cap)[idx] = v7;
+            }
+            {
+                uint2 v8;
+                v8.x = bitcast<unsigned>(R.r53);
+                v8.y = tid;
+                reinterpret_cast<uint2*>(base + 1496ull * cap)[idx] = v8;
+            }
             return;
+        }
         case 13: // isect_triangle_mid2
-            reinterpret_cast<unsigned int*>(base + 1504ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1508ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1512ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1516ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1520ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1524ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1528ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1532ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1536ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1540ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1544ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1548ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1552ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1556ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1560ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1564ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1568ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1572ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1576ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1580ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1584ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1588ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1592ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1596ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 1600ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 1604ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1608ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1612ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1616ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1620ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 1624ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1628ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1504ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1520ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 1536ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 1552ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 1568ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1584ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 1600ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r38);
+                v7.y = bitcast<unsigned>(R.r39);
+                v7.z = bitcast<unsigned>(R.r53);
+                v7.w = tid;
+                reinterpret_cast<uint4*>(base + 1616ull * cap)[idx] = v7;
+            }
             return;
+        }
         case 14: // isect_triangle_mid3
-            reinterpret_cast<unsigned int*>(base + 1632ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1636ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1640ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1644ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1648ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1652ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1656ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1660ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1664ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1668ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1672ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1676ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1680ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1684ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1688ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1692ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1696ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1700ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1704ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1708ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 1712ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1716ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1720ull * cap)[idx] = R.r39;
-            reinterpret_cast<float*>(base + 1724ull * cap)[idx] = R.r40;
-            reinterpret_cast<float*>(base + 1728ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1732ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1736ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1740ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1632ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1648ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1664ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1680ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1696ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r37);
+                v5.y = bitcast<unsigned>(R.r38);
+                v5.z = bitcast<unsigned>(R.r39);
+                v5.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 1712ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r41);
+                v6.y = bitcast<unsigned>(R.r42);
+                v6.z = bitcast<unsigned>(R.r53);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 1728ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 15: // isect_triangle_end
-            reinterpret_cast<unsigned int*>(base + 1744ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1748ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1752ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1756ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1760ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1764ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1768ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1772ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1776ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1780ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1784ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1788ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1792ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1796ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1800ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1804ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1808ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1812ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1816ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1820ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1824ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 1828ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1832ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1744ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1760ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1776ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1792ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 1808ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r49);
+                v5.y = bitcast<unsigned>(R.r53);
+                v5.z = tid;
+                reinterpret_cast<uint4*>(base + 1824ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 16: // traverse_sphere
-            reinterpret_cast<unsigned int*>(base + 1840ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1844ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1848ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1852ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1856ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1860ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1864ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1868ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1872ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1876ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1880ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1884ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1888ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1892ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1896ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1900ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1904ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1908ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 1912ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 1916ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 1920ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1840ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1856ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1872ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1888ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 1904ull * cap)[idx] = v4;
+            }
+            {
+                unsigned v5;
+                v5 = tid;
+                reinterpret_cast<unsigned*>(base + 1920ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 17: // traverse_solve_quadratic
-            reinterpret_cast<unsigned int*>(base + 1928ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1932ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1936ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1940ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1944ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1948ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1952ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1956ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1960ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 1964ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1968ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 1972ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 1976ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 1980ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 1984ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 1988ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1992ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1996ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2000ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2004ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2008ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 2012ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 2016ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2020ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned int*>(base + 2024ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2028ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1928ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1944ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 1960ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1976ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 1992ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r34);
+                v5.z = bitcast<unsigned>(R.r35);
+                v5.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 2008ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r53);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 2024ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 18: // sq_head1
-            reinterpret_cast<unsigned int*>(base + 2032ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2036ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2040ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2044ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2048ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2052ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2056ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2060ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2064ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2068ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2072ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2076ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2080ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2084ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2088ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2092ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2096ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2100ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2104ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2108ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2112ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2116ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2120ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned int*>(base + 2124ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2128ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2032ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2048ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2064ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2080ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2096ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r35);
+                v5.z = bitcast<unsigned>(R.r36);
+                v5.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 2112ull * cap)[idx] = v5;
+            }
+            {
+                unsigned v6;
+                v6 = tid;
+                reinterpret_cast<unsigned*>(base + 2128ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 19: // sq_head2
-            reinterpret_cast<unsigned int*>(base + 2136ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2140ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2144ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2148ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2152ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2156ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2160ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2164ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2168ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2172ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2176ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2180ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2184ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2188ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2192ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2196ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2200ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2204ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2208ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2212ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2216ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2220ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2224ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned int*>(base + 2228ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned*>(base + 2232ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2136ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2152ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2168ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2184ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2200ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r35);
+                v5.z = bitcast<unsigned>(R.r36);
+                v5.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 2216ull * cap)[idx] = v5;
+            }
+            {
+                unsigned v6;
+                v6 = tid;
+                reinterpret_cast<unsigned*>(base + 2232ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 20: // sq_mid1
-            reinterpret_cast<unsigned int*>(base + 2240ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2244ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2248ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2252ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2256ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2260ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2264ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2268ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2272ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2276ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2280ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2284ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2288ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2292ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2296ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2300ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2304ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2308ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2312ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2316ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2320ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 2324ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 2328ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2332ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned int*>(base + 2336ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2340ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2240ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2256ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2272ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2288ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2304ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r34);
+                v5.z = bitcast<unsigned>(R.r35);
+                v5.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 2320ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r53);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 2336ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 21: // sq_mid2
-            reinterpret_cast<unsigned int*>(base + 2344ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2348ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2352ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2356ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2360ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2364ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2368ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2372ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2376ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2380ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2384ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2388ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2392ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2396ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2400ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2404ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2408ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2412ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2416ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2420ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2424ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2428ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 2432ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 2436ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2440ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned*>(base + 2444ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2344ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2360ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 2376ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 2392ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r29);
+                v4.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 2408ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r32);
+                v5.y = bitcast<unsigned>(R.r33);
+                v5.z = bitcast<unsigned>(R.r34);
+                v5.w = bitcast<unsigned>(R.r35);
+                reinterpret_cast<uint4*>(base + 2424ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r36);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 2440ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 22: // sq_mid
-            reinterpret_cast<unsigned int*>(base + 2448ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2452ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2456ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2460ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2464ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2468ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2472ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2476ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2480ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2484ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2488ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2492ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2496ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2500ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2504ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2508ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2512ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2516ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2520ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2524ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2528ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2532ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 2536ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned int*>(base + 2540ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2544ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2448ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2464ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 2480ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 2496ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r29);
+                v4.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 2512ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r32);
+                v5.y = bitcast<unsigned>(R.r33);
+                v5.z = bitcast<unsigned>(R.r36);
+                v5.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 2528ull * cap)[idx] = v5;
+            }
+            {
+                unsigned v6;
+                v6 = tid;
+                reinterpret_cast<unsigned*>(base + 2544ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 23: // sq_tail
-            reinterpret_cast<unsigned int*>(base + 2552ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2556ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2560ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2564ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2568ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2572ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2576ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2580ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2584ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2588ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2592ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2596ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2600ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2604ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2608ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2612ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2616ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2620ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2624ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2628ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2632ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2636ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2640ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2644ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2552ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2568ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 2584ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 2600ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r29);
+                v4.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 2616ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r32);
+                v5.y = bitcast<unsigned>(R.r33);
+                v5.z = bitcast<unsigned>(R.r53);
+                v5.w = tid;
+                reinterpret_cast<uint4*>(base + 2632ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 24: // sq_end
-            reinterpret_cast<unsigned int*>(base + 2648ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2652ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2656ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2660ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2664ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2668ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2672ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2676ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2680ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2684ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2688ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2692ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2696ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2700ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2704ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2708ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2712ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2716ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2720ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2724ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2728ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2732ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 2736ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2740ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2648ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2664ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2680ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2696ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2712ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r49);
+                v5.z = bitcast<unsigned>(R.r53);
+                v5.w = tid;
+                reinterpret_cast<uint4*>(base + 2728ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 25: // traverse_sphere_fin
-            reinterpret_cast<unsigned int*>(base + 2744ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2748ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2752ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2756ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2760ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2764ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2768ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2772ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2776ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2780ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2784ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2788ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2792ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2796ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2800ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2804ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2808ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2812ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2816ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2820ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2824ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 2828ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2832ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2744ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2760ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2776ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2792ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 2808ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r49);
+                v5.y = bitcast<unsigned>(R.r53);
+                v5.z = tid;
+                reinterpret_cast<uint4*>(base + 2824ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 26: // traverse_cylinder
-            reinterpret_cast<unsigned int*>(base + 2840ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2844ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2848ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2852ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2856ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2860ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2864ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2868ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2872ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2876ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2880ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2884ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2888ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2892ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2896ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2900ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2904ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2908ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 2912ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 2916ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 2920ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2840ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2856ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2872ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2888ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 2904ull * cap)[idx] = v4;
+            }
+            {
+                unsigned v5;
+                v5 = tid;
+                reinterpret_cast<unsigned*>(base + 2920ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 27: // traverse_cylinder_fin
-            reinterpret_cast<unsigned int*>(base + 2928ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2932ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2936ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2940ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2944ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2948ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2952ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2956ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 2960ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 2964ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2968ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2972ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 2976ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 2980ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 2984ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 2988ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2992ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2996ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3000ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 3004ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 3008ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3012ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 3016ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 3020ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2928ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 2944ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2960ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2976ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r29);
+                v4.z = bitcast<unsigned>(R.r31);
+                v4.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2992ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r33);
+                v5.y = bitcast<unsigned>(R.r49);
+                v5.z = bitcast<unsigned>(R.r53);
+                v5.w = tid;
+                reinterpret_cast<uint4*>(base + 3008ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 28: // traverse_disk
-            reinterpret_cast<unsigned int*>(base + 3024ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3028ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3032ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3036ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3040ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3044ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3048ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3052ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 3056ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 3060ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3064ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 3068ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 3072ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 3076ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 3080ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 3084ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 3088ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3092ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3096ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3100ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3104ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3108ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 3112ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 3116ull * cap)[idx] = R.r33;
-            reinterpret_cast<float*>(base + 3120ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 3124ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3128ull * cap)[idx] = R.r36;
-            reinterpret_cast<unsigned*>(base + 3132ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3024ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 3040ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 3056ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 3072ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3088ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3104ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r36);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 3120ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 29: // isect_disk_rest
-            reinterpret_cast<unsigned int*>(base + 3136ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3140ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3144ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3148ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3152ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3156ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3160ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3164ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 3168ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 3172ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3176ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 3180ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 3184ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 3188ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 3192ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 3196ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 3200ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3204ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3208ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3212ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3216ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3220ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 3224ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 3228ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3232ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 3236ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3136ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 3152ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 3168ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 3184ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r27);
+                v4.z = bitcast<unsigned>(R.r28);
+                v4.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3200ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r30);
+                v5.y = bitcast<unsigned>(R.r31);
+                v5.z = bitcast<unsigned>(R.r32);
+                v5.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3216ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r53);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 3232ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 30: // isect_disk_end
-            reinterpret_cast<unsigned int*>(base + 3240ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3244ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3248ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3252ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3256ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3260ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3264ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3268ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 3272ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 3276ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3280ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3284ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 3288ull * cap)[idx] = R.r17;
-            reinterpret_cast<float*>(base + 3292ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 3296ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 3300ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3304ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3308ull * cap)[idx] = R.r31;
-            reinterpret_cast<unsigned int*>(base + 3312ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 3316ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3320ull * cap)[idx] = R.r49;
-            reinterpret_cast<unsigned int*>(base + 3324ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 3328ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3240ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 3256ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 3272ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r17);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 3288ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r27);
+                v4.y = bitcast<unsigned>(R.r31);
+                v4.z = bitcast<unsigned>(R.r32);
+                v4.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3304ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r49);
+                v5.y = bitcast<unsigned>(R.r53);
+                v5.z = tid;
+                reinterpret_cast<uint4*>(base + 3320ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 31: // traverse_room_end
-            reinterpret_cast<unsigned int*>(base + 3336ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3340ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3344ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3348ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3352ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3356ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 3360ull * cap)[idx] = R.r9;
-            reinterpret_cast<float*>(base + 3364ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3368ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3372ull * cap)[idx] = R.r15;
-            reinterpret_cast<unsigned int*>(base + 3376ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3380ull * cap)[idx] = R.r32;
-            reinterpret_cast<unsigned int*>(base + 3384ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned*>(base + 3388ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3336ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r8);
+                v1.z = bitcast<unsigned>(R.r9);
+                v1.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 3352ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r13);
+                v2.y = bitcast<unsigned>(R.r15);
+                v2.z = bitcast<unsigned>(R.r17);
+                v2.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 3368ull * cap)[idx] = v2;
+            }
+            {
+                uint2 v3;
+                v3.x = bitcast<unsigned>(R.r53);
+                v3.y = tid;
+                reinterpret_cast<uint2*>(base + 3384ull * cap)[idx] = v3;
+            }
             return;
+        }
         case 32: // fin_pixel
-            reinterpret_cast<unsigned int*>(base + 3392ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3396ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3400ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3404ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3408ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned*>(base + 3412ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3392ull * cap)[idx] = v0;
+            }
+            {
+                uint2 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = tid;
+                reinterpret_cast<uint2*>(base + 3408ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -1977,878 +2935,1167 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 4ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r53 = bitcast<unsigned int>(v0.y);
+            return v0.z;
+        }
         case 1: // roll
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 16ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 20ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 24ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 28ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 32ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 36ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 40ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 44ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 48ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 52ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 56ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 60ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 64ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 32ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 48ull * cap)[idx];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r17 = bitcast<unsigned int>(v2.z);
+            R.r53 = bitcast<unsigned int>(v2.w);
+            const unsigned v3 = reinterpret_cast<const unsigned*>(base + 64ull * cap)[idx];
+            return v3;
+        }
         case 2: // traverse_box
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 72ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 76ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 80ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 84ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 88ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 92ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 96ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 100ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 104ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 108ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 112ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 116ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 120ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 124ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 128ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 132ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 136ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 140ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 144ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 148ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 152ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 156ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 72ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 88ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 104ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 120ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 136ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(base + 152ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
         case 3: // isect_quad_l1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 160ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 164ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 168ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 172ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 176ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 180ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 184ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 188ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 192ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 196ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 200ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 204ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 208ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 212ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 216ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 220ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 224ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 228ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 232ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 236ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 240ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 244ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 248ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 252ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 256ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 260ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 264ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 268ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 272ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 276ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 280ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 284ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 288ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 292ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 296ull * cap)[idx];
-            R.r52 = reinterpret_cast<const float*>(base + 300ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 304ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 308ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 160ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 176ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 192ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 208ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 224ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 240ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 256ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 272ull * cap)[idx];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 288ull * cap)[idx];
+            R.r42 = bitcast<float>(v8.x);
+            R.r50 = bitcast<float>(v8.y);
+            R.r51 = bitcast<float>(v8.z);
+            R.r52 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 304ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v9.x);
+            return v9.y;
+        }
         case 4: // isect_quad_l2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 312ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 316ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 320ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 324ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 328ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 332ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 336ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 340ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 344ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 348ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 352ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 356ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 360ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 364ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 368ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 372ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 376ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 380ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 384ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 388ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 392ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 396ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 400ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 404ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 408ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 412ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 416ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 420ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 424ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 428ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 432ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 436ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 440ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 444ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 448ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 452ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 312ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 328ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 344ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 360ull * cap)[idx];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r17 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 376ull * cap)[idx];
+            R.r21 = bitcast<float>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r27 = bitcast<float>(v4.z);
+            R.r28 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 392ull * cap)[idx];
+            R.r29 = bitcast<float>(v5.x);
+            R.r30 = bitcast<float>(v5.y);
+            R.r31 = bitcast<float>(v5.z);
+            R.r32 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 408ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v6.x);
+            R.r34 = bitcast<float>(v6.y);
+            R.r35 = bitcast<unsigned int>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 424ull * cap)[idx];
+            R.r37 = bitcast<float>(v7.x);
+            R.r38 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 440ull * cap)[idx];
+            R.r41 = bitcast<float>(v8.x);
+            R.r42 = bitcast<float>(v8.y);
+            R.r53 = bitcast<unsigned int>(v8.z);
+            return v8.w;
+        }
         case 5: // isect_quad_l3
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 456ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 460ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 464ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 468ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 472ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 476ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 480ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 484ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 488ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 492ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 496ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 500ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 504ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 508ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 512ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 516ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 520ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 524ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 528ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 532ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 536ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 540ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 544ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 548ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 552ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 556ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 560ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 564ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 568ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 572ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 576ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 580ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 584ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 588ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 592ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 596ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 456ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 472ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 488ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 504ull * cap)[idx];
+            R.r13 = bitcast<float>(v3.x);
+            R.r14 = bitcast<unsigned int>(v3.y);
+            R.r15 = bitcast<float>(v3.z);
+            R.r17 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 520ull * cap)[idx];
+            R.r20 = bitcast<float>(v4.x);
+            R.r21 = bitcast<float>(v4.y);
+            R.r22 = bitcast<float>(v4.z);
+            R.r27 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 536ull * cap)[idx];
+            R.r28 = bitcast<float>(v5.x);
+            R.r29 = bitcast<float>(v5.y);
+            R.r30 = bitcast<float>(v5.z);
+            R.r31 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 552ull * cap)[idx];
+            R.r32 = bitcast<unsigned int>(v6.x);
+            R.r33 = bitcast<unsigned int>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r35 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 568ull * cap)[idx];
+            R.r36 = bitcast<float>(v7.x);
+            R.r37 = bitcast<float>(v7.y);
+            R.r38 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 584ull * cap)[idx];
+            R.r40 = bitcast<float>(v8.x);
+            R.r41 = bitcast<float>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            return v8.w;
+        }
         case 6: // isect_quad_l4
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 600ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 604ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 608ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 612ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 616ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 620ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 624ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 628ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 632ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 636ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 640ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 644ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 648ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 652ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 656ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 660ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 664ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 668ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 672ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 676ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 680ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 684ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 688ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 692ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 696ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 700ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 704ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 708ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 712ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 716ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 720ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 724ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 728ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 732ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 600ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 616ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 632ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 648ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 664ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 680ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 696ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 712ull * cap)[idx];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint2 v8 = reinterpret_cast<const uint2*>(base + 728ull * cap)[idx];
+            R.r42 = bitcast<float>(v8.x);
+            return v8.y;
+        }
         case 7: // isect_quad_l5
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 736ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 740ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 744ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 748ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 752ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 756ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 760ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 764ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 768ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 772ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 776ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 780ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 784ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 788ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 792ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 796ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 800ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 804ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 808ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 812ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 816ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 820ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 824ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 828ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 832ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 836ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 840ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 844ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 848ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 852ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 856ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 860ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 864ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 868ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 872ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 876ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 880ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 884ull * cap)[idx];
-            R.r52 = reinterpret_cast<const float*>(base + 888ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 892ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 896ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 736ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 752ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 768ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 784ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 800ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 816ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 832ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 848ull * cap)[idx];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 864ull * cap)[idx];
+            R.r42 = bitcast<float>(v8.x);
+            R.r43 = bitcast<float>(v8.y);
+            R.r44 = bitcast<float>(v8.z);
+            R.r45 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 880ull * cap)[idx];
+            R.r50 = bitcast<float>(v9.x);
+            R.r51 = bitcast<float>(v9.y);
+            R.r52 = bitcast<float>(v9.z);
+            R.r53 = bitcast<unsigned int>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(base + 896ull * cap)[idx];
+            return v10;
+        }
         case 8: // isect_quad_l6
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 904ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 908ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 912ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 916ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 920ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 924ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 928ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 932ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 936ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 940ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 944ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 948ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 952ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 956ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 960ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 964ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 968ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 972ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 976ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 980ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 984ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 988ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 992ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 996ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 1000ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 1004ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1008ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 1012ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 1016ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1020ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1024ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1028ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 1032ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1036ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1040ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1044ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1048ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1052ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 904ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 920ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 936ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 952ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 968ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 984ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1000ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r40 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1016ull * cap)[idx];
+            R.r41 = bitcast<float>(v7.x);
+            R.r42 = bitcast<float>(v7.y);
+            R.r43 = bitcast<float>(v7.z);
+            R.r44 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 1032ull * cap)[idx];
+            R.r45 = bitcast<float>(v8.x);
+            R.r46 = bitcast<float>(v8.y);
+            R.r47 = bitcast<float>(v8.z);
+            R.r48 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 1048ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v9.x);
+            return v9.y;
+        }
         case 9: // isect_quad_l7
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1056ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1060ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1064ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1068ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1072ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1076ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1080ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1084ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1088ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1092ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1096ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1100ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1104ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1108ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1112ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1116ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1120ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1124ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1128ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1132ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1136ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1140ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1144ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1148ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 1152ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 1156ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1160ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 1164ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 1168ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1172ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1176ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1056ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1072ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1088ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1104ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1120ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1136ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1152ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r40 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1168ull * cap)[idx];
+            R.r41 = bitcast<float>(v7.x);
+            R.r42 = bitcast<float>(v7.y);
+            return v7.z;
+        }
         case 10: // isect_quad_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1184ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1188ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1192ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1196ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1200ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1204ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1208ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1212ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1216ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1220ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1224ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1228ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1232ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1236ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1240ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1244ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1248ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1252ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1256ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1260ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1264ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1268ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1272ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1184ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1200ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1216ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1232ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1248ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1264ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
         case 11: // traverse_tetrahedron
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1280ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1284ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1288ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1292ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1296ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1300ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1304ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1308ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1312ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1316ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1320ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1324ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1328ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1332ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1336ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1340ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1344ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1348ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1352ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1356ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1360ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1280ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1296ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1312ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1328ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1344ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(base + 1360ull * cap)[idx];
+            return v5;
+        }
         case 12: // isect_triangle_mid1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1368ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1372ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1376ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1380ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1384ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1388ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1392ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1396ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1400ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1404ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1408ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1412ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1416ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1420ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1424ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1428ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1432ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1436ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1440ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1444ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1448ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1452ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1456ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 1460ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 1464ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1468ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1472ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1476ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1480ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 1484ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 1488ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1492ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1496ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1500ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1368ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1384ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1400ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1416ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1432ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r28 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r30 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1448ull * cap)[idx];
+            R.r31 = bitcast<float>(v5.x);
+            R.r32 = bitcast<unsigned int>(v5.y);
+            R.r33 = bitcast<unsigned int>(v5.z);
+            R.r34 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1464ull * cap)[idx];
+            R.r35 = bitcast<unsigned int>(v6.x);
+            R.r36 = bitcast<float>(v6.y);
+            R.r37 = bitcast<float>(v6.z);
+            R.r38 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1480ull * cap)[idx];
+            R.r39 = bitcast<float>(v7.x);
+            R.r40 = bitcast<float>(v7.y);
+            R.r41 = bitcast<float>(v7.z);
+            R.r42 = bitcast<float>(v7.w);
+            const uint2 v8 = reinterpret_cast<const uint2*>(base + 1496ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v8.x);
+            return v8.y;
+        }
         case 13: // isect_triangle_mid2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1504ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1508ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1512ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1516ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1520ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1524ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1528ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1532ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1536ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1540ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1544ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1548ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1552ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1556ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1560ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1564ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1568ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1572ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1576ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1580ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1584ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1588ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1592ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1596ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 1600ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 1604ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1608ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1612ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1616ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1620ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1624ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1628ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1504ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1520ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1536ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1552ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1568ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1584ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1600ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1616ull * cap)[idx];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r53 = bitcast<unsigned int>(v7.z);
+            return v7.w;
+        }
         case 14: // isect_triangle_mid3
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1632ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1636ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1640ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1644ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1648ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1652ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1656ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1660ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1664ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1668ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1672ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1676ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1680ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1684ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1688ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1692ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1696ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1700ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1704ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1708ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1712ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1716ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1720ull * cap)[idx];
-            R.r40 = reinterpret_cast<const float*>(base + 1724ull * cap)[idx];
-            R.r41 = reinterpret_cast<const float*>(base + 1728ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1732ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1736ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1740ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1632ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1648ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1664ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1680ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1696ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1712ull * cap)[idx];
+            R.r37 = bitcast<float>(v5.x);
+            R.r38 = bitcast<float>(v5.y);
+            R.r39 = bitcast<float>(v5.z);
+            R.r40 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1728ull * cap)[idx];
+            R.r41 = bitcast<float>(v6.x);
+            R.r42 = bitcast<float>(v6.y);
+            R.r53 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
         case 15: // isect_triangle_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1744ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1748ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1752ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1756ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1760ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1764ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1768ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1772ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1776ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1780ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1784ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1788ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1792ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1796ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1800ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1804ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1808ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1812ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1816ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 1820ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1824ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1828ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1832ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1744ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1760ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1776ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1792ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1808ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1824ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
         case 16: // traverse_sphere
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1840ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1844ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1848ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1852ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1856ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1860ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1864ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1868ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1872ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1876ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1880ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1884ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1888ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1892ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1896ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1900ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1904ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1908ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 1912ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 1916ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1920ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1840ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1856ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1872ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1888ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1904ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(base + 1920ull * cap)[idx];
+            return v5;
+        }
         case 17: // traverse_solve_quadratic
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1928ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1932ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1936ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1940ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1944ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1948ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1952ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1956ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1960ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1964ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1968ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1972ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 1976ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 1980ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 1984ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1988ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1992ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1996ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2000ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2004ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2008ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 2012ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 2016ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2020ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2024ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2028ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1928ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1944ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1960ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1976ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1992ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2008ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r34 = bitcast<float>(v5.y);
+            R.r35 = bitcast<unsigned int>(v5.z);
+            R.r36 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 2024ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
         case 18: // sq_head1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2032ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2036ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2040ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2044ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2048ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2052ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2056ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2060ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2064ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2068ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2072ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2076ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2080ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2084ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2088ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2092ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2096ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2100ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2104ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2108ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2112ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 2116ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2120ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2124ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2128ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2032ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2048ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2064ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2080ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2096ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2112ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r35 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r53 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(base + 2128ull * cap)[idx];
+            return v6;
+        }
         case 19: // sq_head2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2136ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2140ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2144ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2148ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2152ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2156ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2160ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2164ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2168ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2172ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2176ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2180ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2184ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2188ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2192ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2196ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2200ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2204ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2208ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2212ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2216ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 2220ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2224ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2228ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2232ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2136ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2152ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2168ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2184ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2200ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2216ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r35 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r49 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(base + 2232ull * cap)[idx];
+            return v6;
+        }
         case 20: // sq_mid1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2240ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2244ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2248ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2252ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2256ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2260ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2264ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2268ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2272ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2276ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2280ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2284ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2288ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2292ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2296ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2300ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2304ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2308ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2312ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2316ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2320ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 2324ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 2328ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2332ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2336ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2340ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2240ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2256ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2272ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2288ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2304ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2320ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r34 = bitcast<float>(v5.y);
+            R.r35 = bitcast<unsigned int>(v5.z);
+            R.r36 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 2336ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
         case 21: // sq_mid2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2344ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2348ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2352ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2356ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2360ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2364ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2368ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2372ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2376ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2380ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2384ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 2388ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2392ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2396ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2400ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2404ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2408ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2412ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2416ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2420ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2424ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2428ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 2432ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 2436ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2440ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2444ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2344ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2360ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2376ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2392ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2408ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2424ull * cap)[idx];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r34 = bitcast<float>(v5.z);
+            R.r35 = bitcast<unsigned int>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 2440ull * cap)[idx];
+            R.r36 = bitcast<float>(v6.x);
+            return v6.y;
+        }
         case 22: // sq_mid
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2448ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2452ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2456ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2460ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2464ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2468ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2472ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2476ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2480ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2484ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2488ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 2492ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2496ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2500ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2504ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2508ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2512ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2516ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2520ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2524ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2528ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2532ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2536ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2540ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2544ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2448ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2464ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2480ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2496ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2512ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2528ull * cap)[idx];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r53 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(base + 2544ull * cap)[idx];
+            return v6;
+        }
         case 23: // sq_tail
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2552ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2556ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2560ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2564ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2568ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2572ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2576ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2580ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2584ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2588ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2592ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 2596ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2600ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2604ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2608ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2612ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2616ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2620ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2624ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2628ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2632ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2636ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2640ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2644ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2552ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2568ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2584ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2600ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2616ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2632ull * cap)[idx];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
         case 24: // sq_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2648ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2652ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2656ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2660ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2664ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2668ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2672ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2676ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2680ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2684ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2688ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2692ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2696ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2700ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2704ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2708ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2712ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2716ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2720ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2724ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2728ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2732ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2736ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2740ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2648ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2664ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2680ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2696ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2712ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2728ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r49 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
         case 25: // traverse_sphere_fin
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2744ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2748ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2752ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2756ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2760ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2764ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2768ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2772ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2776ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2780ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2784ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2788ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2792ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2796ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2800ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2804ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2808ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2812ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2816ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 2820ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2824ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2828ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2832ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2744ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2760ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2776ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2792ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2808ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2824ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
         case 26: // traverse_cylinder
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2840ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2844ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2848ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2852ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2856ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2860ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2864ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2868ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2872ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2876ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2880ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2884ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2888ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2892ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2896ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2900ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2904ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2908ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 2912ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2916ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2920ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2840ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2856ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2872ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2888ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2904ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(base + 2920ull * cap)[idx];
+            return v5;
+        }
         case 27: // traverse_cylinder_fin
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2928ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2932ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2936ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2940ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2944ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2948ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2952ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 2956ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2960ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2964ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2968ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2972ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 2976ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 2980ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 2984ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2988ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2992ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2996ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3000ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 3004ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 3008ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 3012ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 3016ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3020ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2928ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2944ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2960ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2976ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2992ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3008ull * cap)[idx];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r49 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
         case 28: // traverse_disk
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3024ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3028ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3032ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3036ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3040ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3044ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3048ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 3052ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 3056ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3060ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3064ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 3068ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3072ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 3076ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 3080ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 3084ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3088ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3092ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3096ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3100ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3104ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3108ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 3112ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 3116ull * cap)[idx];
-            R.r34 = reinterpret_cast<const float*>(base + 3120ull * cap)[idx];
-            R.r35 = reinterpret_cast<const unsigned int*>(base + 3124ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 3128ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3132ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3024ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3040ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3056ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3072ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3088ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3104ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3120ull * cap)[idx];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 29: // isect_disk_rest
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3136ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3140ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3144ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3148ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3152ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3156ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3160ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 3164ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 3168ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3172ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3176ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 3180ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3184ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 3188ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 3192ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 3196ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3200ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3204ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3208ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3212ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3216ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3220ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 3224ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 3228ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 3232ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3236ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3136ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3152ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3168ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3184ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3200ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3216ull * cap)[idx];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 3232ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
         case 30: // isect_disk_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3240ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3244ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3248ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3252ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3256ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3260ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3264ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 3268ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 3272ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3276ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3280ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3284ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 3288ull * cap)[idx];
-            R.r20 = reinterpret_cast<const float*>(base + 3292ull * cap)[idx];
-            R.r21 = reinterpret_cast<const float*>(base + 3296ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3300ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3304ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3308ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 3312ull * cap)[idx];
-            R.r33 = reinterpret_cast<const unsigned int*>(base + 3316ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 3320ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 3324ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3328ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3240ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3256ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3272ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3288ull * cap)[idx];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3304ull * cap)[idx];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3320ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
         case 31: // traverse_room_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3336ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3340ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3344ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3348ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3352ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 3356ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 3360ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3364ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3368ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3372ull * cap)[idx];
-            R.r17 = reinterpret_cast<const unsigned int*>(base + 3376ull * cap)[idx];
-            R.r32 = reinterpret_cast<const unsigned int*>(base + 3380ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 3384ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3388ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3336ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3352ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3368ull * cap)[idx];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r17 = bitcast<unsigned int>(v2.z);
+            R.r32 = bitcast<unsigned int>(v2.w);
+            const uint2 v3 = reinterpret_cast<const uint2*>(base + 3384ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v3.x);
+            return v3.y;
+        }
         case 32: // fin_pixel
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3392ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3396ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3400ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3404ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3408ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3412ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3392ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint2 v1 = reinterpret_cast<const uint2*>(base + 3408ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            return v1.y;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -2869,135 +4116,201 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {1u, 53u};
 const int kQTypes0[] = {LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames0[] = {"ppp", "ct"};
-const unsigned long long kQOffs0[] = {0ull, 4ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull};
+const unsigned kQSubs0[] = {0u, 4u};
+const unsigned kQWidths0[] = {16u, 16u};
 const uint32_t kQRegs1[] = {1u, 2u, 3u, 4u, 5u, 8u, 9u, 12u, 13u, 15u, 17u, 53u};
 const int kQTypes1[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames1[] = {"ppp", "L0", "L1", "L2", "rc", "c0", "c1", "pp0", "pp1", "pw", "sc", "ct"};
-const unsigned long long kQOffs1[] = {16ull, 20ull, 24ull, 28ull, 32ull, 36ull, 40ull, 44ull, 48ull, 52ull, 56ull, 60ull};
+const unsigned long long kQOffs1[] = {16ull, 16ull, 16ull, 16ull, 32ull, 32ull, 32ull, 32ull, 48ull, 48ull, 48ull, 48ull};
+const unsigned kQSubs1[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths1[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs2[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 53u};
 const int kQTypes2[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames2[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "ct"};
-const unsigned long long kQOffs2[] = {72ull, 76ull, 80ull, 84ull, 88ull, 92ull, 96ull, 100ull, 104ull, 108ull, 112ull, 116ull, 120ull, 124ull, 128ull, 132ull, 136ull, 140ull, 144ull, 148ull, 152ull};
+const unsigned long long kQOffs2[] = {72ull, 72ull, 72ull, 72ull, 88ull, 88ull, 88ull, 88ull, 104ull, 104ull, 104ull, 104ull, 120ull, 120ull, 120ull, 120ull, 136ull, 136ull, 136ull, 136ull, 152ull};
+const unsigned kQSubs2[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths2[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs3[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 50u, 51u, 52u, 53u};
 const int kQTypes3[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames3[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "vr60", "vr61", "vr62", "ct"};
-const unsigned long long kQOffs3[] = {160ull, 164ull, 168ull, 172ull, 176ull, 180ull, 184ull, 188ull, 192ull, 196ull, 200ull, 204ull, 208ull, 212ull, 216ull, 220ull, 224ull, 228ull, 232ull, 236ull, 240ull, 244ull, 248ull, 252ull, 256ull, 260ull, 264ull, 268ull, 272ull, 276ull, 280ull, 284ull, 288ull, 292ull, 296ull, 300ull, 304ull};
+const unsigned long long kQOffs3[] = {160ull, 160ull, 160ull, 160ull, 176ull, 176ull, 176ull, 176ull, 192ull, 192ull, 192ull, 192ull, 208ull, 208ull, 208ull, 208ull, 224ull, 224ull, 224ull, 224ull, 240ull, 240ull, 240ull, 240ull, 256ull, 256ull, 256ull, 256ull, 272ull, 272ull, 272ull, 272ull, 288ull, 288ull, 288ull, 288ull, 304ull};
+const unsigned kQSubs3[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths3[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs4[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 10u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 53u};
 const int kQTypes4[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames4[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "tmp1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct"};
-const unsigned long long kQOffs4[] = {312ull, 316ull, 320ull, 324ull, 328ull, 332ull, 336ull, 340ull, 344ull, 348ull, 352ull, 356ull, 360ull, 364ull, 368ull, 372ull, 376ull, 380ull, 384ull, 388ull, 392ull, 396ull, 400ull, 404ull, 408ull, 412ull, 416ull, 420ull, 424ull, 428ull, 432ull, 436ull, 440ull, 444ull, 448ull};
+const unsigned long long kQOffs4[] = {312ull, 312ull, 312ull, 312ull, 328ull, 328ull, 328ull, 328ull, 344ull, 344ull, 344ull, 344ull, 360ull, 360ull, 360ull, 360ull, 376ull, 376ull, 376ull, 376ull, 392ull, 392ull, 392ull, 392ull, 408ull, 408ull, 408ull, 408ull, 424ull, 424ull, 424ull, 424ull, 440ull, 440ull, 440ull};
+const unsigned kQSubs4[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths4[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs5[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 10u, 11u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u};
 const int kQTypes5[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames5[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "tmp1", "tmp2", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32"};
-const unsigned long long kQOffs5[] = {456ull, 460ull, 464ull, 468ull, 472ull, 476ull, 480ull, 484ull, 488ull, 492ull, 496ull, 500ull, 504ull, 508ull, 512ull, 516ull, 520ull, 524ull, 528ull, 532ull, 536ull, 540ull, 544ull, 548ull, 552ull, 556ull, 560ull, 564ull, 568ull, 572ull, 576ull, 580ull, 584ull, 588ull, 592ull};
+const unsigned long long kQOffs5[] = {456ull, 456ull, 456ull, 456ull, 472ull, 472ull, 472ull, 472ull, 488ull, 488ull, 488ull, 488ull, 504ull, 504ull, 504ull, 504ull, 520ull, 520ull, 520ull, 520ull, 536ull, 536ull, 536ull, 536ull, 552ull, 552ull, 552ull, 552ull, 568ull, 568ull, 568ull, 568ull, 584ull, 584ull, 584ull};
+const unsigned kQSubs5[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths5[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs6[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u};
 const int kQTypes6[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames6[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32"};
-const unsigned long long kQOffs6[] = {600ull, 604ull, 608ull, 612ull, 616ull, 620ull, 624ull, 628ull, 632ull, 636ull, 640ull, 644ull, 648ull, 652ull, 656ull, 660ull, 664ull, 668ull, 672ull, 676ull, 680ull, 684ull, 688ull, 692ull, 696ull, 700ull, 704ull, 708ull, 712ull, 716ull, 720ull, 724ull, 728ull};
+const unsigned long long kQOffs6[] = {600ull, 600ull, 600ull, 600ull, 616ull, 616ull, 616ull, 616ull, 632ull, 632ull, 632ull, 632ull, 648ull, 648ull, 648ull, 648ull, 664ull, 664ull, 664ull, 664ull, 680ull, 680ull, 680ull, 680ull, 696ull, 696ull, 696ull, 696ull, 712ull, 712ull, 712ull, 712ull, 728ull};
+const unsigned kQSubs6[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths6[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs7[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 50u, 51u, 52u, 53u};
 const int kQTypes7[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames7[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "vr40", "vr41", "vr42", "vr60", "vr61", "vr62", "ct"};
-const unsigned long long kQOffs7[] = {736ull, 740ull, 744ull, 748ull, 752ull, 756ull, 760ull, 764ull, 768ull, 772ull, 776ull, 780ull, 784ull, 788ull, 792ull, 796ull, 800ull, 804ull, 808ull, 812ull, 816ull, 820ull, 824ull, 828ull, 832ull, 836ull, 840ull, 844ull, 848ull, 852ull, 856ull, 860ull, 864ull, 868ull, 872ull, 876ull, 880ull, 884ull, 888ull, 892ull};
+const unsigned long long kQOffs7[] = {736ull, 736ull, 736ull, 736ull, 752ull, 752ull, 752ull, 752ull, 768ull, 768ull, 768ull, 768ull, 784ull, 784ull, 784ull, 784ull, 800ull, 800ull, 800ull, 800ull, 816ull, 816ull, 816ull, 816ull, 832ull, 832ull, 832ull, 832ull, 848ull, 848ull, 848ull, 848ull, 864ull, 864ull, 864ull, 864ull, 880ull, 880ull, 880ull, 880ull};
+const unsigned kQSubs7[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths7[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs8[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 53u};
 const int kQTypes8[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames8[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr30", "vr31", "vr32", "vr40", "vr41", "vr42", "vr50", "vr51", "vr52", "ct"};
-const unsigned long long kQOffs8[] = {904ull, 908ull, 912ull, 916ull, 920ull, 924ull, 928ull, 932ull, 936ull, 940ull, 944ull, 948ull, 952ull, 956ull, 960ull, 964ull, 968ull, 972ull, 976ull, 980ull, 984ull, 988ull, 992ull, 996ull, 1000ull, 1004ull, 1008ull, 1012ull, 1016ull, 1020ull, 1024ull, 1028ull, 1032ull, 1036ull, 1040ull, 1044ull, 1048ull};
+const unsigned long long kQOffs8[] = {904ull, 904ull, 904ull, 904ull, 920ull, 920ull, 920ull, 920ull, 936ull, 936ull, 936ull, 936ull, 952ull, 952ull, 952ull, 952ull, 968ull, 968ull, 968ull, 968ull, 984ull, 984ull, 984ull, 984ull, 1000ull, 1000ull, 1000ull, 1000ull, 1016ull, 1016ull, 1016ull, 1016ull, 1032ull, 1032ull, 1032ull, 1032ull, 1048ull};
+const unsigned kQSubs8[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths8[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs9[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 40u, 41u, 42u};
 const int kQTypes9[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames9[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr30", "vr31", "vr32"};
-const unsigned long long kQOffs9[] = {1056ull, 1060ull, 1064ull, 1068ull, 1072ull, 1076ull, 1080ull, 1084ull, 1088ull, 1092ull, 1096ull, 1100ull, 1104ull, 1108ull, 1112ull, 1116ull, 1120ull, 1124ull, 1128ull, 1132ull, 1136ull, 1140ull, 1144ull, 1148ull, 1152ull, 1156ull, 1160ull, 1164ull, 1168ull, 1172ull};
+const unsigned long long kQOffs9[] = {1056ull, 1056ull, 1056ull, 1056ull, 1072ull, 1072ull, 1072ull, 1072ull, 1088ull, 1088ull, 1088ull, 1088ull, 1104ull, 1104ull, 1104ull, 1104ull, 1120ull, 1120ull, 1120ull, 1120ull, 1136ull, 1136ull, 1136ull, 1136ull, 1152ull, 1152ull, 1152ull, 1152ull, 1168ull, 1168ull};
+const unsigned kQSubs9[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths9[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs10[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes10[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames10[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs10[] = {1184ull, 1188ull, 1192ull, 1196ull, 1200ull, 1204ull, 1208ull, 1212ull, 1216ull, 1220ull, 1224ull, 1228ull, 1232ull, 1236ull, 1240ull, 1244ull, 1248ull, 1252ull, 1256ull, 1260ull, 1264ull, 1268ull};
+const unsigned long long kQOffs10[] = {1184ull, 1184ull, 1184ull, 1184ull, 1200ull, 1200ull, 1200ull, 1200ull, 1216ull, 1216ull, 1216ull, 1216ull, 1232ull, 1232ull, 1232ull, 1232ull, 1248ull, 1248ull, 1248ull, 1248ull, 1264ull, 1264ull};
+const unsigned kQSubs10[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths10[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs11[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u};
 const int kQTypes11[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames11[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp"};
-const unsigned long long kQOffs11[] = {1280ull, 1284ull, 1288ull, 1292ull, 1296ull, 1300ull, 1304ull, 1308ull, 1312ull, 1316ull, 1320ull, 1324ull, 1328ull, 1332ull, 1336ull, 1340ull, 1344ull, 1348ull, 1352ull, 1356ull};
+const unsigned long long kQOffs11[] = {1280ull, 1280ull, 1280ull, 1280ull, 1296ull, 1296ull, 1296ull, 1296ull, 1312ull, 1312ull, 1312ull, 1312ull, 1328ull, 1328ull, 1328ull, 1328ull, 1344ull, 1344ull, 1344ull, 1344ull};
+const unsigned kQSubs11[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths11[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs12[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 53u};
 const int kQTypes12[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames12[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct"};
-const unsigned long long kQOffs12[] = {1368ull, 1372ull, 1376ull, 1380ull, 1384ull, 1388ull, 1392ull, 1396ull, 1400ull, 1404ull, 1408ull, 1412ull, 1416ull, 1420ull, 1424ull, 1428ull, 1432ull, 1436ull, 1440ull, 1444ull, 1448ull, 1452ull, 1456ull, 1460ull, 1464ull, 1468ull, 1472ull, 1476ull, 1480ull, 1484ull, 1488ull, 1492ull, 1496ull};
+const unsigned long long kQOffs12[] = {1368ull, 1368ull, 1368ull, 1368ull, 1384ull, 1384ull, 1384ull, 1384ull, 1400ull, 1400ull, 1400ull, 1400ull, 1416ull, 1416ull, 1416ull, 1416ull, 1432ull, 1432ull, 1432ull, 1432ull, 1448ull, 1448ull, 1448ull, 1448ull, 1464ull, 1464ull, 1464ull, 1464ull, 1480ull, 1480ull, 1480ull, 1480ull, 1496ull};
+const unsigned kQSubs12[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths12[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs13[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 53u};
 const int kQTypes13[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames13[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "ct"};
-const unsigned long long kQOffs13[] = {1504ull, 1508ull, 1512ull, 1516ull, 1520ull, 1524ull, 1528ull, 1532ull, 1536ull, 1540ull, 1544ull, 1548ull, 1552ull, 1556ull, 1560ull, 1564ull, 1568ull, 1572ull, 1576ull, 1580ull, 1584ull, 1588ull, 1592ull, 1596ull, 1600ull, 1604ull, 1608ull, 1612ull, 1616ull, 1620ull, 1624ull};
+const unsigned long long kQOffs13[] = {1504ull, 1504ull, 1504ull, 1504ull, 1520ull, 1520ull, 1520ull, 1520ull, 1536ull, 1536ull, 1536ull, 1536ull, 1552ull, 1552ull, 1552ull, 1552ull, 1568ull, 1568ull, 1568ull, 1568ull, 1584ull, 1584ull, 1584ull, 1584ull, 1600ull, 1600ull, 1600ull, 1600ull, 1616ull, 1616ull, 1616ull};
+const unsigned kQSubs13[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths13[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs14[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 37u, 38u, 39u, 40u, 41u, 42u, 53u};
 const int kQTypes14[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames14[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct"};
-const unsigned long long kQOffs14[] = {1632ull, 1636ull, 1640ull, 1644ull, 1648ull, 1652ull, 1656ull, 1660ull, 1664ull, 1668ull, 1672ull, 1676ull, 1680ull, 1684ull, 1688ull, 1692ull, 1696ull, 1700ull, 1704ull, 1708ull, 1712ull, 1716ull, 1720ull, 1724ull, 1728ull, 1732ull, 1736ull};
+const unsigned long long kQOffs14[] = {1632ull, 1632ull, 1632ull, 1632ull, 1648ull, 1648ull, 1648ull, 1648ull, 1664ull, 1664ull, 1664ull, 1664ull, 1680ull, 1680ull, 1680ull, 1680ull, 1696ull, 1696ull, 1696ull, 1696ull, 1712ull, 1712ull, 1712ull, 1712ull, 1728ull, 1728ull, 1728ull};
+const unsigned kQSubs14[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths14[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs15[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes15[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames15[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs15[] = {1744ull, 1748ull, 1752ull, 1756ull, 1760ull, 1764ull, 1768ull, 1772ull, 1776ull, 1780ull, 1784ull, 1788ull, 1792ull, 1796ull, 1800ull, 1804ull, 1808ull, 1812ull, 1816ull, 1820ull, 1824ull, 1828ull};
+const unsigned long long kQOffs15[] = {1744ull, 1744ull, 1744ull, 1744ull, 1760ull, 1760ull, 1760ull, 1760ull, 1776ull, 1776ull, 1776ull, 1776ull, 1792ull, 1792ull, 1792ull, 1792ull, 1808ull, 1808ull, 1808ull, 1808ull, 1824ull, 1824ull};
+const unsigned kQSubs15[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths15[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs16[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 53u};
 const int kQTypes16[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames16[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "ct"};
-const unsigned long long kQOffs16[] = {1840ull, 1844ull, 1848ull, 1852ull, 1856ull, 1860ull, 1864ull, 1868ull, 1872ull, 1876ull, 1880ull, 1884ull, 1888ull, 1892ull, 1896ull, 1900ull, 1904ull, 1908ull, 1912ull, 1916ull};
+const unsigned long long kQOffs16[] = {1840ull, 1840ull, 1840ull, 1840ull, 1856ull, 1856ull, 1856ull, 1856ull, 1872ull, 1872ull, 1872ull, 1872ull, 1888ull, 1888ull, 1888ull, 1888ull, 1904ull, 1904ull, 1904ull, 1904ull};
+const unsigned kQSubs16[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths16[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs17[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 34u, 35u, 36u, 53u};
 const int kQTypes17[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames17[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12", "ct"};
-const unsigned long long kQOffs17[] = {1928ull, 1932ull, 1936ull, 1940ull, 1944ull, 1948ull, 1952ull, 1956ull, 1960ull, 1964ull, 1968ull, 1972ull, 1976ull, 1980ull, 1984ull, 1988ull, 1992ull, 1996ull, 2000ull, 2004ull, 2008ull, 2012ull, 2016ull, 2020ull, 2024ull};
+const unsigned long long kQOffs17[] = {1928ull, 1928ull, 1928ull, 1928ull, 1944ull, 1944ull, 1944ull, 1944ull, 1960ull, 1960ull, 1960ull, 1960ull, 1976ull, 1976ull, 1976ull, 1976ull, 1992ull, 1992ull, 1992ull, 1992ull, 2008ull, 2008ull, 2008ull, 2008ull, 2024ull};
+const unsigned kQSubs17[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths17[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs18[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 35u, 36u, 53u};
 const int kQTypes18[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames18[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr11", "vr12", "ct"};
-const unsigned long long kQOffs18[] = {2032ull, 2036ull, 2040ull, 2044ull, 2048ull, 2052ull, 2056ull, 2060ull, 2064ull, 2068ull, 2072ull, 2076ull, 2080ull, 2084ull, 2088ull, 2092ull, 2096ull, 2100ull, 2104ull, 2108ull, 2112ull, 2116ull, 2120ull, 2124ull};
+const unsigned long long kQOffs18[] = {2032ull, 2032ull, 2032ull, 2032ull, 2048ull, 2048ull, 2048ull, 2048ull, 2064ull, 2064ull, 2064ull, 2064ull, 2080ull, 2080ull, 2080ull, 2080ull, 2096ull, 2096ull, 2096ull, 2096ull, 2112ull, 2112ull, 2112ull, 2112ull};
+const unsigned kQSubs18[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths18[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs19[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 35u, 36u, 49u};
 const int kQTypes19[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames19[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr11", "vr12", "hit"};
-const unsigned long long kQOffs19[] = {2136ull, 2140ull, 2144ull, 2148ull, 2152ull, 2156ull, 2160ull, 2164ull, 2168ull, 2172ull, 2176ull, 2180ull, 2184ull, 2188ull, 2192ull, 2196ull, 2200ull, 2204ull, 2208ull, 2212ull, 2216ull, 2220ull, 2224ull, 2228ull};
+const unsigned long long kQOffs19[] = {2136ull, 2136ull, 2136ull, 2136ull, 2152ull, 2152ull, 2152ull, 2152ull, 2168ull, 2168ull, 2168ull, 2168ull, 2184ull, 2184ull, 2184ull, 2184ull, 2200ull, 2200ull, 2200ull, 2200ull, 2216ull, 2216ull, 2216ull, 2216ull};
+const unsigned kQSubs19[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths19[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs20[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 34u, 35u, 36u, 53u};
 const int kQTypes20[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames20[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12", "ct"};
-const unsigned long long kQOffs20[] = {2240ull, 2244ull, 2248ull, 2252ull, 2256ull, 2260ull, 2264ull, 2268ull, 2272ull, 2276ull, 2280ull, 2284ull, 2288ull, 2292ull, 2296ull, 2300ull, 2304ull, 2308ull, 2312ull, 2316ull, 2320ull, 2324ull, 2328ull, 2332ull, 2336ull};
+const unsigned long long kQOffs20[] = {2240ull, 2240ull, 2240ull, 2240ull, 2256ull, 2256ull, 2256ull, 2256ull, 2272ull, 2272ull, 2272ull, 2272ull, 2288ull, 2288ull, 2288ull, 2288ull, 2304ull, 2304ull, 2304ull, 2304ull, 2320ull, 2320ull, 2320ull, 2320ull, 2336ull};
+const unsigned kQSubs20[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths20[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs21[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 34u, 35u, 36u};
 const int kQTypes21[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32};
 const char* const kQNames21[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12"};
-const unsigned long long kQOffs21[] = {2344ull, 2348ull, 2352ull, 2356ull, 2360ull, 2364ull, 2368ull, 2372ull, 2376ull, 2380ull, 2384ull, 2388ull, 2392ull, 2396ull, 2400ull, 2404ull, 2408ull, 2412ull, 2416ull, 2420ull, 2424ull, 2428ull, 2432ull, 2436ull, 2440ull};
+const unsigned long long kQOffs21[] = {2344ull, 2344ull, 2344ull, 2344ull, 2360ull, 2360ull, 2360ull, 2360ull, 2376ull, 2376ull, 2376ull, 2376ull, 2392ull, 2392ull, 2392ull, 2392ull, 2408ull, 2408ull, 2408ull, 2408ull, 2424ull, 2424ull, 2424ull, 2424ull, 2440ull};
+const unsigned kQSubs21[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths21[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs22[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 36u, 53u};
 const int kQTypes22[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames22[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "vr12", "ct"};
-const unsigned long long kQOffs22[] = {2448ull, 2452ull, 2456ull, 2460ull, 2464ull, 2468ull, 2472ull, 2476ull, 2480ull, 2484ull, 2488ull, 2492ull, 2496ull, 2500ull, 2504ull, 2508ull, 2512ull, 2516ull, 2520ull, 2524ull, 2528ull, 2532ull, 2536ull, 2540ull};
+const unsigned long long kQOffs22[] = {2448ull, 2448ull, 2448ull, 2448ull, 2464ull, 2464ull, 2464ull, 2464ull, 2480ull, 2480ull, 2480ull, 2480ull, 2496ull, 2496ull, 2496ull, 2496ull, 2512ull, 2512ull, 2512ull, 2512ull, 2528ull, 2528ull, 2528ull, 2528ull};
+const unsigned kQSubs22[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths22[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs23[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 53u};
 const int kQTypes23[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames23[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "ct"};
-const unsigned long long kQOffs23[] = {2552ull, 2556ull, 2560ull, 2564ull, 2568ull, 2572ull, 2576ull, 2580ull, 2584ull, 2588ull, 2592ull, 2596ull, 2600ull, 2604ull, 2608ull, 2612ull, 2616ull, 2620ull, 2624ull, 2628ull, 2632ull, 2636ull, 2640ull};
+const unsigned long long kQOffs23[] = {2552ull, 2552ull, 2552ull, 2552ull, 2568ull, 2568ull, 2568ull, 2568ull, 2584ull, 2584ull, 2584ull, 2584ull, 2600ull, 2600ull, 2600ull, 2600ull, 2616ull, 2616ull, 2616ull, 2616ull, 2632ull, 2632ull, 2632ull};
+const unsigned kQSubs23[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths23[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs24[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes24[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames24[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs24[] = {2648ull, 2652ull, 2656ull, 2660ull, 2664ull, 2668ull, 2672ull, 2676ull, 2680ull, 2684ull, 2688ull, 2692ull, 2696ull, 2700ull, 2704ull, 2708ull, 2712ull, 2716ull, 2720ull, 2724ull, 2728ull, 2732ull, 2736ull};
+const unsigned long long kQOffs24[] = {2648ull, 2648ull, 2648ull, 2648ull, 2664ull, 2664ull, 2664ull, 2664ull, 2680ull, 2680ull, 2680ull, 2680ull, 2696ull, 2696ull, 2696ull, 2696ull, 2712ull, 2712ull, 2712ull, 2712ull, 2728ull, 2728ull, 2728ull};
+const unsigned kQSubs24[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths24[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs25[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes25[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames25[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs25[] = {2744ull, 2748ull, 2752ull, 2756ull, 2760ull, 2764ull, 2768ull, 2772ull, 2776ull, 2780ull, 2784ull, 2788ull, 2792ull, 2796ull, 2800ull, 2804ull, 2808ull, 2812ull, 2816ull, 2820ull, 2824ull, 2828ull};
+const unsigned long long kQOffs25[] = {2744ull, 2744ull, 2744ull, 2744ull, 2760ull, 2760ull, 2760ull, 2760ull, 2776ull, 2776ull, 2776ull, 2776ull, 2792ull, 2792ull, 2792ull, 2792ull, 2808ull, 2808ull, 2808ull, 2808ull, 2824ull, 2824ull};
+const unsigned kQSubs25[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths25[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs26[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 53u};
 const int kQTypes26[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames26[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "ct"};
-const unsigned long long kQOffs26[] = {2840ull, 2844ull, 2848ull, 2852ull, 2856ull, 2860ull, 2864ull, 2868ull, 2872ull, 2876ull, 2880ull, 2884ull, 2888ull, 2892ull, 2896ull, 2900ull, 2904ull, 2908ull, 2912ull, 2916ull};
+const unsigned long long kQOffs26[] = {2840ull, 2840ull, 2840ull, 2840ull, 2856ull, 2856ull, 2856ull, 2856ull, 2872ull, 2872ull, 2872ull, 2872ull, 2888ull, 2888ull, 2888ull, 2888ull, 2904ull, 2904ull, 2904ull, 2904ull};
+const unsigned kQSubs26[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths26[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs27[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 29u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes27[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames27[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "vr01", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs27[] = {2928ull, 2932ull, 2936ull, 2940ull, 2944ull, 2948ull, 2952ull, 2956ull, 2960ull, 2964ull, 2968ull, 2972ull, 2976ull, 2980ull, 2984ull, 2988ull, 2992ull, 2996ull, 3000ull, 3004ull, 3008ull, 3012ull, 3016ull};
+const unsigned long long kQOffs27[] = {2928ull, 2928ull, 2928ull, 2928ull, 2944ull, 2944ull, 2944ull, 2944ull, 2960ull, 2960ull, 2960ull, 2960ull, 2976ull, 2976ull, 2976ull, 2976ull, 2992ull, 2992ull, 2992ull, 2992ull, 3008ull, 3008ull, 3008ull};
+const unsigned kQSubs27[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths27[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs28[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u};
 const int kQTypes28[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32};
 const char* const kQNames28[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12"};
-const unsigned long long kQOffs28[] = {3024ull, 3028ull, 3032ull, 3036ull, 3040ull, 3044ull, 3048ull, 3052ull, 3056ull, 3060ull, 3064ull, 3068ull, 3072ull, 3076ull, 3080ull, 3084ull, 3088ull, 3092ull, 3096ull, 3100ull, 3104ull, 3108ull, 3112ull, 3116ull, 3120ull, 3124ull, 3128ull};
+const unsigned long long kQOffs28[] = {3024ull, 3024ull, 3024ull, 3024ull, 3040ull, 3040ull, 3040ull, 3040ull, 3056ull, 3056ull, 3056ull, 3056ull, 3072ull, 3072ull, 3072ull, 3072ull, 3088ull, 3088ull, 3088ull, 3088ull, 3104ull, 3104ull, 3104ull, 3104ull, 3120ull, 3120ull, 3120ull};
+const unsigned kQSubs28[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths28[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs29[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 14u, 15u, 17u, 20u, 21u, 22u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 53u};
 const int kQTypes29[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames29[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "sc", "o0", "o1", "o2", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "ct"};
-const unsigned long long kQOffs29[] = {3136ull, 3140ull, 3144ull, 3148ull, 3152ull, 3156ull, 3160ull, 3164ull, 3168ull, 3172ull, 3176ull, 3180ull, 3184ull, 3188ull, 3192ull, 3196ull, 3200ull, 3204ull, 3208ull, 3212ull, 3216ull, 3220ull, 3224ull, 3228ull, 3232ull};
+const unsigned long long kQOffs29[] = {3136ull, 3136ull, 3136ull, 3136ull, 3152ull, 3152ull, 3152ull, 3152ull, 3168ull, 3168ull, 3168ull, 3168ull, 3184ull, 3184ull, 3184ull, 3184ull, 3200ull, 3200ull, 3200ull, 3200ull, 3216ull, 3216ull, 3216ull, 3216ull, 3232ull};
+const unsigned kQSubs29[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths29[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs30[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 12u, 13u, 15u, 17u, 20u, 21u, 22u, 27u, 31u, 32u, 33u, 49u, 53u};
 const int kQTypes30[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames30[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "sc", "o0", "o1", "o2", "d2", "t", "pid", "rp", "hit", "ct"};
-const unsigned long long kQOffs30[] = {3240ull, 3244ull, 3248ull, 3252ull, 3256ull, 3260ull, 3264ull, 3268ull, 3272ull, 3276ull, 3280ull, 3284ull, 3288ull, 3292ull, 3296ull, 3300ull, 3304ull, 3308ull, 3312ull, 3316ull, 3320ull, 3324ull};
+const unsigned long long kQOffs30[] = {3240ull, 3240ull, 3240ull, 3240ull, 3256ull, 3256ull, 3256ull, 3256ull, 3272ull, 3272ull, 3272ull, 3272ull, 3288ull, 3288ull, 3288ull, 3288ull, 3304ull, 3304ull, 3304ull, 3304ull, 3320ull, 3320ull};
+const unsigned kQSubs30[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths30[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs31[] = {1u, 2u, 3u, 4u, 5u, 8u, 9u, 12u, 13u, 15u, 17u, 32u, 53u};
 const int kQTypes31[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames31[] = {"ppp", "L0", "L1", "L2", "rc", "c0", "c1", "pp0", "pp1", "pw", "sc", "pid", "ct"};
-const unsigned long long kQOffs31[] = {3336ull, 3340ull, 3344ull, 3348ull, 3352ull, 3356ull, 3360ull, 3364ull, 3368ull, 3372ull, 3376ull, 3380ull, 3384ull};
+const unsigned long long kQOffs31[] = {3336ull, 3336ull, 3336ull, 3336ull, 3352ull, 3352ull, 3352ull, 3352ull, 3368ull, 3368ull, 3368ull, 3368ull, 3384ull};
+const unsigned kQSubs31[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths31[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs32[] = {1u, 2u, 3u, 4u, 5u};
 const int kQTypes32[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames32[] = {"ppp", "L0", "L1", "L2", "rc"};
-const unsigned long long kQOffs32[] = {3392ull, 3396ull, 3400ull, 3404ull, 3408ull};
+const unsigned long long kQOffs32[] = {3392ull, 3392ull, 3392ull, 3392ull, 3408ull};
+const unsigned kQSubs32[] = {0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths32[] = {16u, 16u, 16u, 16u, 8u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 12u, kQRegs1, kQTypes1, kQNames1},
@@ -3034,39 +4347,39 @@ const loom_b200_queue_layout kQueues[] = {
     {32u, -1, 5u, kQRegs32, kQTypes32, kQNames32},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
-    {kQOffs1, 64ull},
-    {kQOffs2, 156ull},
-    {kQOffs3, 308ull},
-    {kQOffs4, 452ull},
-    {kQOffs5, 596ull},
-    {kQOffs6, 732ull},
-    {kQOffs7, 896ull},
-    {kQOffs8, 1052ull},
-    {kQOffs9, 1176ull},
-    {kQOffs10, 1272ull},
-    {kQOffs11, 1360ull},
-    {kQOffs12, 1500ull},
-    {kQOffs13, 1628ull},
-    {kQOffs14, 1740ull},
-    {kQOffs15, 1832ull},
-    {kQOffs16, 1920ull},
-    {kQOffs17, 2028ull},
-    {kQOffs18, 2128ull},
-    {kQOffs19, 2232ull},
-    {kQOffs20, 2340ull},
-    {kQOffs21, 2444ull},
-    {kQOffs22, 2544ull},
-    {kQOffs23, 2644ull},
-    {kQOffs24, 2740ull},
-    {kQOffs25, 2832ull},
-    {kQOffs26, 2920ull},
-    {kQOffs27, 3020ull},
-    {kQOffs28, 3132ull},
-    {kQOffs29, 3236ull},
-    {kQOffs30, 3328ull},
-    {kQOffs31, 3388ull},
-    {kQOffs32, 3412ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
+    {kQOffs1, kQSubs1, kQWidths1, 64ull, 0u, 4u},
+    {kQOffs2, kQSubs2, kQWidths2, 152ull, 4u, 8u},
+    {kQOffs3, kQSubs3, kQWidths3, 304ull, 4u, 8u},
+    {kQOffs4, kQSubs4, kQWidths4, 440ull, 12u, 16u},
+    {kQOffs5, kQSubs5, kQWidths5, 584ull, 12u, 16u},
+    {kQOffs6, kQSubs6, kQWidths6, 728ull, 4u, 8u},
+    {kQOffs7, kQSubs7, kQWidths7, 896ull, 0u, 4u},
+    {kQOffs8, kQSubs8, kQWidths8, 1048ull, 4u, 8u},
+    {kQOffs9, kQSubs9, kQWidths9, 1168ull, 8u, 16u},
+    {kQOffs10, kQSubs10, kQWidths10, 1264ull, 8u, 16u},
+    {kQOffs11, kQSubs11, kQWidths11, 1360ull, 0u, 4u},
+    {kQOffs12, kQSubs12, kQWidths12, 1496ull, 4u, 8u},
+    {kQOffs13, kQSubs13, kQWidths13, 1616ull, 12u, 16u},
+    {kQOffs14, kQSubs14, kQWidths14, 1728ull, 12u, 16u},
+    {kQOffs15, kQSubs15, kQWidths15, 1824ull, 8u, 16u},
+    {kQOffs16, kQSubs16, kQWidths16, 1920ull, 0u, 4u},
+    {kQOffs17, kQSubs17, kQWidths17, 2024ull, 4u, 8u},
+    {kQOffs18, kQSubs18, kQWidths18, 2128ull, 0u, 4u},
+    {kQOffs19, kQSubs19, kQWidths19, 2232ull, 0u, 4u},
+    {kQOffs20, kQSubs20, kQWidths20, 2336ull, 4u, 8u},
+    {kQOffs21, kQSubs21, kQWidths21, 2440ull, 4u, 8u},
+    {kQOffs22, kQSubs22, kQWidths22, 2544ull, 0u, 4u},
+    {kQOffs23, kQSubs23, kQWidths23, 2632ull, 12u, 16u},
+    {kQOffs24, kQSubs24, kQWidths24, 2728ull, 12u, 16u},
+    {kQOffs25, kQSubs25, kQWidths25, 2824ull, 8u, 16u},
+    {kQOffs26, kQSubs26, kQWidths26, 2920ull, 0u, 4u},
+    {kQOffs27, kQSubs27, kQWidths27, 3008ull, 12u, 16u},
+    {kQOffs28, kQSubs28, kQWidths28, 3120ull, 12u, 16u},
+    {kQOffs29, kQSubs29, kQWidths29, 3232ull, 4u, 8u},
+    {kQOffs30, kQSubs30, kQWidths30, 3320ull, 8u, 16u},
+    {kQOffs31, kQSubs31, kQWidths31, 3384ull, 4u, 8u},
+    {kQOffs32, kQSubs32, kQWidths32, 3408ull, 4u, 8u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

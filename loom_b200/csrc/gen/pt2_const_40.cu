@@ -1976,2595 +1976,5273 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 4ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 8ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 12ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 16ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 20ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 24ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 28ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 32ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 36ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 40ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 44ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 48ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 52ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 56ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 60ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 64ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 68ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 72ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 76ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 80ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 84ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 88ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 92ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 96ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 100ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 104ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 108ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r14);
+                v0.z = bitcast<unsigned>(R.r22);
+                v0.w = bitcast<unsigned>(R.r23);
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r24);
+                v1.y = bitcast<unsigned>(R.r25);
+                v1.z = bitcast<unsigned>(R.r26);
+                v1.w = bitcast<unsigned>(R.r27);
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r28);
+                v2.y = bitcast<unsigned>(R.r29);
+                v2.z = bitcast<unsigned>(R.r30);
+                v2.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 32ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r32);
+                v3.y = bitcast<unsigned>(R.r33);
+                v3.z = bitcast<unsigned>(R.r34);
+                v3.w = bitcast<unsigned>(R.r35);
+                reinterpret_cast<uint4*>(base + 48ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r61);
+                v4.y = bitcast<unsigned>(R.r62);
+                v4.z = bitcast<unsigned>(R.r63);
+                v4.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 64ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r65);
+                v5.y = bitcast<unsigned>(R.r66);
+                v5.z = bitcast<unsigned>(R.r67);
+                v5.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 80ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r69);
+                v6.y = bitcast<unsigned>(R.r70);
+                v6.z = bitcast<unsigned>(R.r71);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 96ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 1: // roll
-            reinterpret_cast<unsigned int*>(base + 112ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 116ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 120ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 124ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 128ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 132ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 136ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 140ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 144ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 148ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 152ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 156ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 160ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 164ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 168ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 172ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 176ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 180ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 184ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 188ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 192ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 196ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 200ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 204ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 208ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 212ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 216ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 220ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 224ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 228ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 232ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 236ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 240ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 244ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 248ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 252ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 256ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 260ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 264ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 268ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 272ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 276ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 112ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 128ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 144ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 160ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 176ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 192ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 208ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 224ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 240ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r68);
+                v9.z = bitcast<unsigned>(R.r69);
+                v9.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 256ull * cap)[idx] = v9;
+            }
+            {
+                uint2 v10;
+                v10.x = bitcast<unsigned>(R.r71);
+                v10.y = tid;
+                reinterpret_cast<uint2*>(base + 272ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 2: // roll_split
-            reinterpret_cast<unsigned int*>(base + 280ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 284ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 288ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 292ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 296ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 300ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 304ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 308ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 312ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 316ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 320ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 324ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 328ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 332ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 336ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 340ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 344ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 348ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 352ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 356ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 360ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 364ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 368ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 372ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 376ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 380ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 384ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 388ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 392ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 396ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 400ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 404ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 408ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 412ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 416ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 420ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 424ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 428ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 432ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 436ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 440ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 444ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 448ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 452ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 456ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 460ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 280ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 296ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r10);
+                v2.z = bitcast<unsigned>(R.r11);
+                v2.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 312ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r13);
+                v3.y = bitcast<unsigned>(R.r15);
+                v3.z = bitcast<unsigned>(R.r16);
+                v3.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 328ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r18);
+                v4.y = bitcast<unsigned>(R.r19);
+                v4.z = bitcast<unsigned>(R.r20);
+                v4.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 344ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r22);
+                v5.y = bitcast<unsigned>(R.r23);
+                v5.z = bitcast<unsigned>(R.r24);
+                v5.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 360ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r26);
+                v6.y = bitcast<unsigned>(R.r27);
+                v6.z = bitcast<unsigned>(R.r28);
+                v6.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 376ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r30);
+                v7.y = bitcast<unsigned>(R.r31);
+                v7.z = bitcast<unsigned>(R.r32);
+                v7.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 392ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r34);
+                v8.y = bitcast<unsigned>(R.r35);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 408ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 424ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 440ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 456ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 3: // sample_pixel
-            reinterpret_cast<unsigned int*>(base + 464ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 468ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 472ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 476ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 480ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 484ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 488ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 492ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 496ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 500ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 504ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 508ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 512ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 516ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 520ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 524ull * cap)[idx] = R.r21;
-            reinterpret_cast<unsigned int*>(base + 528ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 532ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 536ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 540ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 544ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 548ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 552ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 556ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 560ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 564ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 568ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 572ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 464ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r10);
+                v1.z = bitcast<unsigned>(R.r11);
+                v1.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 480ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r13);
+                v2.y = bitcast<unsigned>(R.r15);
+                v2.z = bitcast<unsigned>(R.r16);
+                v2.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 496ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r18);
+                v3.y = bitcast<unsigned>(R.r19);
+                v3.z = bitcast<unsigned>(R.r20);
+                v3.w = bitcast<unsigned>(R.r21);
+                reinterpret_cast<uint4*>(base + 512ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r61);
+                v4.y = bitcast<unsigned>(R.r62);
+                v4.z = bitcast<unsigned>(R.r63);
+                v4.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 528ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r65);
+                v5.y = bitcast<unsigned>(R.r66);
+                v5.z = bitcast<unsigned>(R.r67);
+                v5.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 544ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r69);
+                v6.y = bitcast<unsigned>(R.r70);
+                v6.z = bitcast<unsigned>(R.r71);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 560ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 4: // traverse_scene
-            reinterpret_cast<unsigned int*>(base + 576ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 580ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 584ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 588ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 592ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 596ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 600ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 604ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 608ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 612ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 616ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 620ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 624ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 628ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 632ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 636ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 640ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 644ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 648ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 652ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 656ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 660ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 664ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 668ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 672ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 676ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 680ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 684ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 688ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 692ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 696ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 700ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 704ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 708ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 712ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 716ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 720ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 724ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 728ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 732ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 736ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 740ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 576ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 592ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 608ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 624ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 640ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 656ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 672ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 688ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 704ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r68);
+                v9.z = bitcast<unsigned>(R.r69);
+                v9.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 720ull * cap)[idx] = v9;
+            }
+            {
+                uint2 v10;
+                v10.x = bitcast<unsigned>(R.r71);
+                v10.y = tid;
+                reinterpret_cast<uint2*>(base + 736ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 5: // traverse_box
-            reinterpret_cast<unsigned int*>(base + 744ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 748ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 752ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 756ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 760ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 764ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 768ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 772ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 776ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 780ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 784ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 788ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 792ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 796ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 800ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 804ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 808ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 812ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 816ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 820ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 824ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 828ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 832ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 836ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 840ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 844ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 848ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 852ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 856ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 860ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 864ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 868ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 872ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 876ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 880ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 884ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 888ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 892ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 896ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 900ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 904ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 908ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 912ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 916ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 920ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 744ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 760ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 776ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 792ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 808ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 824ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 840ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 856ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r61);
+                v8.z = bitcast<unsigned>(R.r62);
+                v8.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 872ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r64);
+                v9.y = bitcast<unsigned>(R.r65);
+                v9.z = bitcast<unsigned>(R.r66);
+                v9.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 888ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r68);
+                v10.y = bitcast<unsigned>(R.r69);
+                v10.z = bitcast<unsigned>(R.r70);
+                v10.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 904ull * cap)[idx] = v10;
+            }
+            {
+                unsigned v11;
+                v11 = tid;
+                reinterpret_cast<unsigned*>(base + 920ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 6: // isect_quad_l1
-            reinterpret_cast<unsigned int*>(base + 928ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 932ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 936ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 940ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 944ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 948ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 952ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 956ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 960ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 964ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 968ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 972ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 976ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 980ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 984ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 988ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 992ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 996ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1000ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 1004ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 1008ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1012ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 1016ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1020ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1024ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1028ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1032ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 1036ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 1040ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1044ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 1048ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1052ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1056ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1060ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1064ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 1068ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 1072ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1076ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1080ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 1084ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1088ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 1092ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1096ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 1100ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 1104ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1108ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1112ull * cap)[idx] = R.r58;
-            reinterpret_cast<float*>(base + 1116ull * cap)[idx] = R.r59;
-            reinterpret_cast<float*>(base + 1120ull * cap)[idx] = R.r60;
-            reinterpret_cast<unsigned int*>(base + 1124ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 1128ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 1132ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 1136ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 1140ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 1144ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 1148ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 1152ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 1156ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 1160ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 1164ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 1168ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 928ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 944ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 960ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 976ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 992ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 1008ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 1024ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 1040ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 1056ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1072ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r45);
+                v10.y = bitcast<unsigned>(R.r46);
+                v10.z = bitcast<unsigned>(R.r47);
+                v10.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1088ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r49);
+                v11.y = bitcast<unsigned>(R.r50);
+                v11.z = bitcast<unsigned>(R.r58);
+                v11.w = bitcast<unsigned>(R.r59);
+                reinterpret_cast<uint4*>(base + 1104ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r60);
+                v12.y = bitcast<unsigned>(R.r61);
+                v12.z = bitcast<unsigned>(R.r62);
+                v12.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 1120ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r64);
+                v13.y = bitcast<unsigned>(R.r65);
+                v13.z = bitcast<unsigned>(R.r66);
+                v13.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 1136ull * cap)[idx] = v13;
+            }
+            {
+                uint4 v14;
+                v14.x = bitcast<unsigned>(R.r68);
+                v14.y = bitcast<unsigned>(R.r69);
+                v14.z = bitcast<unsigned>(R.r70);
+                v14.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 1152ull * cap)[idx] = v14;
+            }
+            {
+                unsigned v15;
+                v15 = tid;
+                reinterpret_cast<unsigned*>(base + 1168ull * cap)[idx] = v15;
+            }
             return;
+        }
         case 7: // isect_quad_l2
-            reinterpret_cast<unsigned int*>(base + 1176ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1180ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1184ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1188ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1192ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1196ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1200ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1204ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1208ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 1212ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 1216ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1220ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1224ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1228ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 1232ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 1236ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 1240ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 1244ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 1248ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1252ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 1256ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 1260ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1264ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 1268ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1272ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1276ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1280ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1284ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 1288ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 1292ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1296ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 1300ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1304ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1308ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1312ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1316ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 1320ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 1324ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1328ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1332ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 1336ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1340ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 1344ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1348ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 1352ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 1356ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1360ull * cap)[idx] = R.r50;
-            reinterpret_cast<unsigned int*>(base + 1364ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 1368ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 1372ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 1376ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 1380ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 1384ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 1388ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 1392ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 1396ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 1400ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 1404ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 1408ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1176ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1192ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r10);
+                v2.y = bitcast<unsigned>(R.r11);
+                v2.z = bitcast<unsigned>(R.r12);
+                v2.w = bitcast<unsigned>(R.r13);
+                reinterpret_cast<uint4*>(base + 1208ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r14);
+                v3.y = bitcast<unsigned>(R.r15);
+                v3.z = bitcast<unsigned>(R.r16);
+                v3.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 1224ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r18);
+                v4.y = bitcast<unsigned>(R.r19);
+                v4.z = bitcast<unsigned>(R.r22);
+                v4.w = bitcast<unsigned>(R.r23);
+                reinterpret_cast<uint4*>(base + 1240ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r24);
+                v5.y = bitcast<unsigned>(R.r25);
+                v5.z = bitcast<unsigned>(R.r26);
+                v5.w = bitcast<unsigned>(R.r27);
+                reinterpret_cast<uint4*>(base + 1256ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r28);
+                v6.y = bitcast<unsigned>(R.r29);
+                v6.z = bitcast<unsigned>(R.r30);
+                v6.w = bitcast<unsigned>(R.r31);
+                reinterpret_cast<uint4*>(base + 1272ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r32);
+                v7.y = bitcast<unsigned>(R.r33);
+                v7.z = bitcast<unsigned>(R.r34);
+                v7.w = bitcast<unsigned>(R.r35);
+                reinterpret_cast<uint4*>(base + 1288ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r36);
+                v8.y = bitcast<unsigned>(R.r37);
+                v8.z = bitcast<unsigned>(R.r38);
+                v8.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 1304ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r40);
+                v9.y = bitcast<unsigned>(R.r41);
+                v9.z = bitcast<unsigned>(R.r42);
+                v9.w = bitcast<unsigned>(R.r43);
+                reinterpret_cast<uint4*>(base + 1320ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r44);
+                v10.y = bitcast<unsigned>(R.r45);
+                v10.z = bitcast<unsigned>(R.r46);
+                v10.w = bitcast<unsigned>(R.r47);
+                reinterpret_cast<uint4*>(base + 1336ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r48);
+                v11.y = bitcast<unsigned>(R.r49);
+                v11.z = bitcast<unsigned>(R.r50);
+                v11.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 1352ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r62);
+                v12.y = bitcast<unsigned>(R.r63);
+                v12.z = bitcast<unsigned>(R.r64);
+                v12.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 1368ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r66);
+                v13.y = bitcast<unsigned>(R.r67);
+                v13.z = bitcast<unsigned>(R.r68);
+                v13.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 1384ull * cap)[idx] = v13;
+            }
+            {
+                uint4 v14;
+                v14.x = bitcast<unsigned>(R.r70);
+                v14.y = bitcast<unsigned>(R.r71);
+                v14.z = tid;
+                reinterpret_cast<uint4*>(base + 1400ull * cap)[idx] = v14;
+            }
             return;
+        }
         case 8: // isect_quad_l3
-            reinterpret_cast<unsigned int*>(base + 1416ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1420ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1424ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1428ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1432ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1436ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1440ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1444ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 1448ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 1452ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 1456ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 1460ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1464ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1468ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1472ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 1476ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 1480ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 1484ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 1488ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 1492ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1496ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 1500ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 1504ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1508ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 1512ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1516ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1520ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1524ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1528ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 1532ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 1536ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1540ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 1544ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1548ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1552ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1556ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1560ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 1564ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 1568ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1572ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1576ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 1580ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1584ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 1588ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1592ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 1596ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 1600ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1604ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1608ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 1612ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 1616ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 1620ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 1624ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 1628ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 1632ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 1636ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 1640ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 1644ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 1648ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1416ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 1432ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r10);
+                v2.z = bitcast<unsigned>(R.r11);
+                v2.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 1448ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r13);
+                v3.y = bitcast<unsigned>(R.r14);
+                v3.z = bitcast<unsigned>(R.r15);
+                v3.w = bitcast<unsigned>(R.r16);
+                reinterpret_cast<uint4*>(base + 1464ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r17);
+                v4.y = bitcast<unsigned>(R.r18);
+                v4.z = bitcast<unsigned>(R.r19);
+                v4.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 1480ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r23);
+                v5.y = bitcast<unsigned>(R.r24);
+                v5.z = bitcast<unsigned>(R.r25);
+                v5.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 1496ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r27);
+                v6.y = bitcast<unsigned>(R.r28);
+                v6.z = bitcast<unsigned>(R.r29);
+                v6.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 1512ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r31);
+                v7.y = bitcast<unsigned>(R.r32);
+                v7.z = bitcast<unsigned>(R.r33);
+                v7.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 1528ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r35);
+                v8.y = bitcast<unsigned>(R.r36);
+                v8.z = bitcast<unsigned>(R.r37);
+                v8.w = bitcast<unsigned>(R.r38);
+                reinterpret_cast<uint4*>(base + 1544ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r39);
+                v9.y = bitcast<unsigned>(R.r40);
+                v9.z = bitcast<unsigned>(R.r41);
+                v9.w = bitcast<unsigned>(R.r42);
+                reinterpret_cast<uint4*>(base + 1560ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r43);
+                v10.y = bitcast<unsigned>(R.r44);
+                v10.z = bitcast<unsigned>(R.r45);
+                v10.w = bitcast<unsigned>(R.r46);
+                reinterpret_cast<uint4*>(base + 1576ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r47);
+                v11.y = bitcast<unsigned>(R.r48);
+                v11.z = bitcast<unsigned>(R.r49);
+                v11.w = bitcast<unsigned>(R.r50);
+                reinterpret_cast<uint4*>(base + 1592ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r62);
+                v12.y = bitcast<unsigned>(R.r63);
+                v12.z = bitcast<unsigned>(R.r64);
+                v12.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 1608ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r66);
+                v13.y = bitcast<unsigned>(R.r67);
+                v13.z = bitcast<unsigned>(R.r68);
+                v13.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 1624ull * cap)[idx] = v13;
+            }
+            {
+                uint4 v14;
+                v14.x = bitcast<unsigned>(R.r70);
+                v14.y = bitcast<unsigned>(R.r71);
+                v14.z = tid;
+                reinterpret_cast<uint4*>(base + 1640ull * cap)[idx] = v14;
+            }
             return;
+        }
         case 9: // isect_quad_l4
-            reinterpret_cast<unsigned int*>(base + 1656ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1660ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1664ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1668ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1672ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1676ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1680ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1684ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 1688ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 1692ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1696ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1700ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1704ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 1708ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 1712ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 1716ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 1720ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 1724ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1728ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 1732ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 1736ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1740ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 1744ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1748ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1752ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1756ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1760ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 1764ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 1768ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 1772ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 1776ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 1780ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 1784ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 1788ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 1792ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 1796ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 1800ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 1804ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 1808ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 1812ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1816ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 1820ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1824ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 1828ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 1832ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1836ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1840ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 1844ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 1848ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 1852ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 1856ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 1860ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 1864ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 1868ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 1872ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 1876ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 1880ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1656ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 1672ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 1688ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 1704ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1720ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 1736ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 1752ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 1768ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 1784ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1800ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r45);
+                v10.y = bitcast<unsigned>(R.r46);
+                v10.z = bitcast<unsigned>(R.r47);
+                v10.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1816ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r49);
+                v11.y = bitcast<unsigned>(R.r50);
+                v11.z = bitcast<unsigned>(R.r62);
+                v11.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 1832ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r64);
+                v12.y = bitcast<unsigned>(R.r65);
+                v12.z = bitcast<unsigned>(R.r66);
+                v12.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 1848ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r68);
+                v13.y = bitcast<unsigned>(R.r69);
+                v13.z = bitcast<unsigned>(R.r70);
+                v13.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 1864ull * cap)[idx] = v13;
+            }
+            {
+                unsigned v14;
+                v14 = tid;
+                reinterpret_cast<unsigned*>(base + 1880ull * cap)[idx] = v14;
+            }
             return;
+        }
         case 10: // isect_quad_l5
-            reinterpret_cast<unsigned int*>(base + 1888ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 1892ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 1896ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1900ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 1904ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1908ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 1912ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 1916ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 1920ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 1924ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 1928ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1932ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 1936ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 1940ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 1944ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 1948ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 1952ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 1956ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 1960ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 1964ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 1968ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1972ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 1976ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 1980ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 1984ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 1988ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 1992ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 1996ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 2000ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2004ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 2008ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2012ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 2016ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 2020ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 2024ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 2028ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 2032ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 2036ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 2040ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 2044ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 2048ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 2052ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2056ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 2060ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 2064ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2068ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2072ull * cap)[idx] = R.r51;
-            reinterpret_cast<float*>(base + 2076ull * cap)[idx] = R.r52;
-            reinterpret_cast<unsigned int*>(base + 2080ull * cap)[idx] = R.r53;
-            reinterpret_cast<float*>(base + 2084ull * cap)[idx] = R.r58;
-            reinterpret_cast<float*>(base + 2088ull * cap)[idx] = R.r59;
-            reinterpret_cast<float*>(base + 2092ull * cap)[idx] = R.r60;
-            reinterpret_cast<unsigned int*>(base + 2096ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 2100ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 2104ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 2108ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 2112ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 2116ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 2120ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 2124ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 2128ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 2132ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 2136ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 2140ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 1888ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 1904ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 1920ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 1936ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1952ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 1968ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 1984ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 2000ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 2016ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2032ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r45);
+                v10.y = bitcast<unsigned>(R.r46);
+                v10.z = bitcast<unsigned>(R.r47);
+                v10.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 2048ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r49);
+                v11.y = bitcast<unsigned>(R.r50);
+                v11.z = bitcast<unsigned>(R.r51);
+                v11.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 2064ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r53);
+                v12.y = bitcast<unsigned>(R.r58);
+                v12.z = bitcast<unsigned>(R.r59);
+                v12.w = bitcast<unsigned>(R.r60);
+                reinterpret_cast<uint4*>(base + 2080ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r61);
+                v13.y = bitcast<unsigned>(R.r62);
+                v13.z = bitcast<unsigned>(R.r63);
+                v13.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 2096ull * cap)[idx] = v13;
+            }
+            {
+                uint4 v14;
+                v14.x = bitcast<unsigned>(R.r65);
+                v14.y = bitcast<unsigned>(R.r66);
+                v14.z = bitcast<unsigned>(R.r67);
+                v14.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 2112ull * cap)[idx] = v14;
+            }
+            {
+                uint4 v15;
+                v15.x = bitcast<unsigned>(R.r69);
+                v15.y = bitcast<unsigned>(R.r70);
+                v15.z = bitcast<unsigned>(R.r71);
+                v15.w = tid;
+                reinterpret_cast<uint4*>(base + 2128ull * cap)[idx] = v15;
+            }
             return;
+        }
         case 11: // isect_quad_l6
-            reinterpret_cast<unsigned int*>(base + 2144ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2148ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2152ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2156ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2160ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2164ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2168ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2172ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 2176ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 2180ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2184ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2188ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2192ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2196ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2200ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2204ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 2208ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 2212ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2216ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 2220ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 2224ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2228ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 2232ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2236ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 2240ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2244ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 2248ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 2252ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 2256ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2260ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 2264ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2268ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 2272ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 2276ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 2280ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 2284ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 2288ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 2292ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 2296ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 2300ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 2304ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 2308ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2312ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2316ull * cap)[idx] = R.r51;
-            reinterpret_cast<float*>(base + 2320ull * cap)[idx] = R.r52;
-            reinterpret_cast<unsigned int*>(base + 2324ull * cap)[idx] = R.r53;
-            reinterpret_cast<float*>(base + 2328ull * cap)[idx] = R.r54;
-            reinterpret_cast<float*>(base + 2332ull * cap)[idx] = R.r55;
-            reinterpret_cast<float*>(base + 2336ull * cap)[idx] = R.r56;
-            reinterpret_cast<unsigned int*>(base + 2340ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 2344ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 2348ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 2352ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 2356ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 2360ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 2364ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 2368ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 2372ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 2376ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 2380ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 2384ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2144ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 2160ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 2176ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 2192ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2208ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 2224ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2240ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 2256ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 2272ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2288ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r48);
+                v10.y = bitcast<unsigned>(R.r49);
+                v10.z = bitcast<unsigned>(R.r50);
+                v10.w = bitcast<unsigned>(R.r51);
+                reinterpret_cast<uint4*>(base + 2304ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r52);
+                v11.y = bitcast<unsigned>(R.r53);
+                v11.z = bitcast<unsigned>(R.r54);
+                v11.w = bitcast<unsigned>(R.r55);
+                reinterpret_cast<uint4*>(base + 2320ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r56);
+                v12.y = bitcast<unsigned>(R.r61);
+                v12.z = bitcast<unsigned>(R.r62);
+                v12.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 2336ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r64);
+                v13.y = bitcast<unsigned>(R.r65);
+                v13.z = bitcast<unsigned>(R.r66);
+                v13.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 2352ull * cap)[idx] = v13;
+            }
+            {
+                uint4 v14;
+                v14.x = bitcast<unsigned>(R.r68);
+                v14.y = bitcast<unsigned>(R.r69);
+                v14.z = bitcast<unsigned>(R.r70);
+                v14.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 2368ull * cap)[idx] = v14;
+            }
+            {
+                unsigned v15;
+                v15 = tid;
+                reinterpret_cast<unsigned*>(base + 2384ull * cap)[idx] = v15;
+            }
             return;
+        }
         case 12: // isect_quad_l7
-            reinterpret_cast<unsigned int*>(base + 2392ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2396ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2400ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2404ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2408ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2412ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2416ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2420ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 2424ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 2428ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2432ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2436ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2440ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2444ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2448ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2452ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 2456ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 2460ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2464ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 2468ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 2472ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2476ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 2480ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2484ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 2488ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2492ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 2496ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 2500ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 2504ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2508ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 2512ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2516ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 2520ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 2524ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 2528ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 2532ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 2536ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 2540ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 2544ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 2548ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 2552ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 2556ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2560ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2564ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 2568ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 2572ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 2576ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 2580ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 2584ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 2588ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 2592ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 2596ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 2600ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 2604ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2392ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 2408ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 2424ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 2440ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2456ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 2472ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 2488ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 2504ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 2520ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2536ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r48);
+                v10.y = bitcast<unsigned>(R.r49);
+                v10.z = bitcast<unsigned>(R.r50);
+                v10.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 2552ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r63);
+                v11.y = bitcast<unsigned>(R.r64);
+                v11.z = bitcast<unsigned>(R.r65);
+                v11.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 2568ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r67);
+                v12.y = bitcast<unsigned>(R.r68);
+                v12.z = bitcast<unsigned>(R.r69);
+                v12.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 2584ull * cap)[idx] = v12;
+            }
+            {
+                uint2 v13;
+                v13.x = bitcast<unsigned>(R.r71);
+                v13.y = tid;
+                reinterpret_cast<uint2*>(base + 2600ull * cap)[idx] = v13;
+            }
             return;
+        }
         case 13: // isect_quad_end
-            reinterpret_cast<unsigned int*>(base + 2608ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2612ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2616ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2620ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2624ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2628ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2632ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2636ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 2640ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 2644ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2648ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2652ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2656ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2660ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2664ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 2668ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 2672ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2676ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 2680ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 2684ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2688ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 2692ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2696ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 2700ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2704ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 2708ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 2712ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 2716ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2720ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 2724ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2728ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 2732ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 2736ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 2740ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 2744ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 2748ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 2752ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 2756ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 2760ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 2764ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 2768ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 2772ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 2776ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 2780ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 2784ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 2788ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2608ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 2624ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2640ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 2656ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 2672ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 2688ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 2704ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 2720ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r57);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 2736ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 2752ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 2768ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 2784ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 14: // traverse_tetrahedron
-            reinterpret_cast<unsigned int*>(base + 2792ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2796ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2800ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2804ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2808ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2812ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2816ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2820ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 2824ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 2828ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 2832ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2836ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2840ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2844ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2848ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 2852ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 2856ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 2860ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 2864ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 2868ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2872ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 2876ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 2880ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 2884ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 2888ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 2892ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 2896ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 2900ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 2904ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 2908ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 2912ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 2916ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 2920ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 2924ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 2928ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 2932ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 2936ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 2940ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 2944ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 2948ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 2952ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 2956ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 2960ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 2964ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2792ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 2808ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 2824ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 2840ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 2856ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 2872ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 2888ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 2904ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r62);
+                v8.z = bitcast<unsigned>(R.r63);
+                v8.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 2920ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r65);
+                v9.y = bitcast<unsigned>(R.r66);
+                v9.z = bitcast<unsigned>(R.r67);
+                v9.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 2936ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r69);
+                v10.y = bitcast<unsigned>(R.r70);
+                v10.z = bitcast<unsigned>(R.r71);
+                v10.w = tid;
+                reinterpret_cast<uint4*>(base + 2952ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 15: // isect_triangle_mid1
-            reinterpret_cast<unsigned int*>(base + 2968ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 2972ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 2976ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2980ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 2984ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2988ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 2992ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2996ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 3000ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 3004ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3008ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3012ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 3016ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 3020ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3024ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 3028ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 3032ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3036ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 3040ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 3044ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 3048ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 3052ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3056ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3060ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3064ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3068ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 3072ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 3076ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3080ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 3084ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3088ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 3092ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 3096ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 3100ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 3104ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 3108ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 3112ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 3116ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 3120ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 3124ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 3128ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 3132ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 3136ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 3140ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 3144ull * cap)[idx] = R.r50;
-            reinterpret_cast<unsigned int*>(base + 3148ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 3152ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 3156ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 3160ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 3164ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 3168ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 3172ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 3176ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 3180ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 3184ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 3188ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 3192ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 2968ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 2984ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 3000ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 3016ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 3032ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3048ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3064ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r36);
+                v7.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 3080ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r38);
+                v8.y = bitcast<unsigned>(R.r39);
+                v8.z = bitcast<unsigned>(R.r40);
+                v8.w = bitcast<unsigned>(R.r41);
+                reinterpret_cast<uint4*>(base + 3096ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r42);
+                v9.y = bitcast<unsigned>(R.r43);
+                v9.z = bitcast<unsigned>(R.r44);
+                v9.w = bitcast<unsigned>(R.r45);
+                reinterpret_cast<uint4*>(base + 3112ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r46);
+                v10.y = bitcast<unsigned>(R.r47);
+                v10.z = bitcast<unsigned>(R.r48);
+                v10.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 3128ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r50);
+                v11.y = bitcast<unsigned>(R.r61);
+                v11.z = bitcast<unsigned>(R.r62);
+                v11.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 3144ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r64);
+                v12.y = bitcast<unsigned>(R.r65);
+                v12.z = bitcast<unsigned>(R.r66);
+                v12.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 3160ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r68);
+                v13.y = bitcast<unsigned>(R.r69);
+                v13.z = bitcast<unsigned>(R.r70);
+                v13.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 3176ull * cap)[idx] = v13;
+            }
+            {
+                unsigned v14;
+                v14 = tid;
+                reinterpret_cast<unsigned*>(base + 3192ull * cap)[idx] = v14;
+            }
             return;
+        }
         case 16: // isect_triangle_mid2
-            reinterpret_cast<unsigned int*>(base + 3200ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3204ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3208ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3212ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3216ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3220ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3224ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3228ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 3232ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 3236ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3240ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 3244ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 3248ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 3252ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 3256ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3260ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 3264ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 3268ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3272ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 3276ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 3280ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 3284ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 3288ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3292ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3296ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3300ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3304ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 3308ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 3312ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3316ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 3320ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3324ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 3328ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 3332ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 3336ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 3340ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 3344ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 3348ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 3352ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 3356ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 3360ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 3364ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 3368ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 3372ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 3376ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 3380ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 3384ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 3388ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 3392ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 3396ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 3400ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 3404ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 3408ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 3412ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 3416ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3200ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 3216ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 3232ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 3248ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 3264ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 3280ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 3296ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 3312ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 3328ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 3344ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r45);
+                v10.y = bitcast<unsigned>(R.r46);
+                v10.z = bitcast<unsigned>(R.r47);
+                v10.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 3360ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r62);
+                v11.y = bitcast<unsigned>(R.r63);
+                v11.z = bitcast<unsigned>(R.r64);
+                v11.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 3376ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r66);
+                v12.y = bitcast<unsigned>(R.r67);
+                v12.z = bitcast<unsigned>(R.r68);
+                v12.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 3392ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r70);
+                v13.y = bitcast<unsigned>(R.r71);
+                v13.z = tid;
+                reinterpret_cast<uint4*>(base + 3408ull * cap)[idx] = v13;
+            }
             return;
+        }
         case 17: // isect_triangle_mid3
-            reinterpret_cast<unsigned int*>(base + 3424ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3428ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3432ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3436ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3440ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3444ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3448ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3452ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 3456ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 3460ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3464ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3468ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 3472ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 3476ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3480ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 3484ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 3488ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3492ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 3496ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 3500ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 3504ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 3508ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3512ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3516ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3520ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3524ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 3528ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 3532ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3536ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 3540ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3544ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 3548ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 3552ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 3556ull * cap)[idx] = R.r45;
-            reinterpret_cast<float*>(base + 3560ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 3564ull * cap)[idx] = R.r47;
-            reinterpret_cast<unsigned int*>(base + 3568ull * cap)[idx] = R.r48;
-            reinterpret_cast<unsigned int*>(base + 3572ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 3576ull * cap)[idx] = R.r50;
-            reinterpret_cast<unsigned int*>(base + 3580ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 3584ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 3588ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 3592ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 3596ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 3600ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 3604ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 3608ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 3612ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 3616ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 3620ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 3624ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3424ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 3440ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 3456ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 3472ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 3488ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3504ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3520ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 3536ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r45);
+                v8.z = bitcast<unsigned>(R.r46);
+                v8.w = bitcast<unsigned>(R.r47);
+                reinterpret_cast<uint4*>(base + 3552ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r48);
+                v9.y = bitcast<unsigned>(R.r49);
+                v9.z = bitcast<unsigned>(R.r50);
+                v9.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 3568ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r62);
+                v10.y = bitcast<unsigned>(R.r63);
+                v10.z = bitcast<unsigned>(R.r64);
+                v10.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 3584ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r66);
+                v11.y = bitcast<unsigned>(R.r67);
+                v11.z = bitcast<unsigned>(R.r68);
+                v11.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 3600ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r70);
+                v12.y = bitcast<unsigned>(R.r71);
+                v12.z = tid;
+                reinterpret_cast<uint4*>(base + 3616ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 18: // isect_triangle_end
-            reinterpret_cast<unsigned int*>(base + 3632ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3636ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3640ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3644ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3648ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3652ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3656ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3660ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 3664ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 3668ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3672ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3676ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 3680ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 3684ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3688ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 3692ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 3696ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3700ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 3704ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 3708ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 3712ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 3716ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3720ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3724ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3728ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3732ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 3736ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 3740ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3744ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 3748ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3752ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 3756ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 3760ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 3764ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 3768ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 3772ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 3776ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 3780ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 3784ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 3788ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 3792ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 3796ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 3800ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 3804ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 3808ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 3812ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3632ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 3648ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 3664ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 3680ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 3696ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3712ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3728ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 3744ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r57);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 3760ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 3776ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 3792ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 3808ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 19: // traverse_sphere
-            reinterpret_cast<unsigned int*>(base + 3816ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3820ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 3824ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 3828ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 3832ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 3836ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 3840ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 3844ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 3848ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 3852ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 3856ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 3860ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 3864ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 3868ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 3872ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 3876ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 3880ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 3884ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 3888ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 3892ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 3896ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 3900ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 3904ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 3908ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 3912ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 3916ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 3920ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 3924ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 3928ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 3932ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 3936ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 3940ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 3944ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 3948ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 3952ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 3956ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 3960ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 3964ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 3968ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 3972ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 3976ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 3980ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 3984ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 3988ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3816ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 3832ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 3848ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 3864ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 3880ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 3896ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 3912ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 3928ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r61);
+                v8.y = bitcast<unsigned>(R.r62);
+                v8.z = bitcast<unsigned>(R.r63);
+                v8.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 3944ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r65);
+                v9.y = bitcast<unsigned>(R.r66);
+                v9.z = bitcast<unsigned>(R.r67);
+                v9.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 3960ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r69);
+                v10.y = bitcast<unsigned>(R.r70);
+                v10.z = bitcast<unsigned>(R.r71);
+                v10.w = tid;
+                reinterpret_cast<uint4*>(base + 3976ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 20: // traverse_solve_quadratic
-            reinterpret_cast<unsigned int*>(base + 3992ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 3996ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4000ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4004ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4008ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4012ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 4016ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 4020ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 4024ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 4028ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 4032ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 4036ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 4040ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 4044ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 4048ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 4052ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 4056ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 4060ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 4064ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 4068ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 4072ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 4076ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 4080ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 4084ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 4088ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 4092ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 4096ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 4100ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 4104ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 4108ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 4112ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 4116ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 4120ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 4124ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 4128ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 4132ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 4136ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 4140ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 4144ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 4148ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 4152ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 4156ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 4160ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 4164ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 4168ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 4172ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 4176ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 4180ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 4184ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 3992ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4008ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 4024ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 4040ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 4056ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 4072ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 4088ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 4104ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r42);
+                v8.w = bitcast<unsigned>(R.r43);
+                reinterpret_cast<uint4*>(base + 4120ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r44);
+                v9.y = bitcast<unsigned>(R.r61);
+                v9.z = bitcast<unsigned>(R.r62);
+                v9.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 4136ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r64);
+                v10.y = bitcast<unsigned>(R.r65);
+                v10.z = bitcast<unsigned>(R.r66);
+                v10.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 4152ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r68);
+                v11.y = bitcast<unsigned>(R.r69);
+                v11.z = bitcast<unsigned>(R.r70);
+                v11.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 4168ull * cap)[idx] = v11;
+            }
+            {
+                unsigned v12;
+                v12 = tid;
+                reinterpret_cast<unsigned*>(base + 4184ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 21: // sq_head1
-            reinterpret_cast<unsigned int*>(base + 4192ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 4196ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4200ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4204ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4208ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4212ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 4216ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 4220ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 4224ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 4228ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 4232ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 4236ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 4240ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 4244ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 4248ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 4252ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 4256ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 4260ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 4264ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 4268ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 4272ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 4276ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 4280ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 4284ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 4288ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 4292ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 4296ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 4300ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 4304ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 4308ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 4312ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 4316ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 4320ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 4324ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 4328ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 4332ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 4336ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 4340ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 4344ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 4348ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 4352ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 4356ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 4360ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 4364ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 4368ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 4372ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 4376ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 4380ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 4192ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4208ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 4224ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 4240ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 4256ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 4272ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 4288ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 4304ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r43);
+                v8.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 4320ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r61);
+                v9.y = bitcast<unsigned>(R.r62);
+                v9.z = bitcast<unsigned>(R.r63);
+                v9.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 4336ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r65);
+                v10.y = bitcast<unsigned>(R.r66);
+                v10.z = bitcast<unsigned>(R.r67);
+                v10.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 4352ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r69);
+                v11.y = bitcast<unsigned>(R.r70);
+                v11.z = bitcast<unsigned>(R.r71);
+                v11.w = tid;
+                reinterpret_cast<uint4*>(base + 4368ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 22: // sq_head2
-            reinterpret_cast<unsigned int*>(base + 4384ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 4388ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4392ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4396ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4400ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4404ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 4408ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 4412ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 4416ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 4420ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 4424ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 4428ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 4432ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 4436ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 4440ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 4444ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 4448ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 4452ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 4456ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 4460ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 4464ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 4468ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 4472ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 4476ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 4480ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 4484ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 4488ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 4492ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 4496ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 4500ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 4504ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 4508ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 4512ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 4516ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 4520ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 4524ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 4528ull * cap)[idx] = R.r57;
-            reinterpret_cast<float*>(base + 4532ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 4536ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 4540ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 4544ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 4548ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 4552ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 4556ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 4560ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 4564ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 4568ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 4572ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 4384ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4400ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 4416ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 4432ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 4448ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 4464ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 4480ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 4496ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r43);
+                v8.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 4512ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r57);
+                v9.y = bitcast<unsigned>(R.r62);
+                v9.z = bitcast<unsigned>(R.r63);
+                v9.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 4528ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r65);
+                v10.y = bitcast<unsigned>(R.r66);
+                v10.z = bitcast<unsigned>(R.r67);
+                v10.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 4544ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r69);
+                v11.y = bitcast<unsigned>(R.r70);
+                v11.z = bitcast<unsigned>(R.r71);
+                v11.w = tid;
+                reinterpret_cast<uint4*>(base + 4560ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 23: // sq_mid1
-            reinterpret_cast<unsigned int*>(base + 4576ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 4580ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4584ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4588ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4592ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4596ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 4600ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 4604ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 4608ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 4612ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 4616ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 4620ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 4624ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 4628ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 4632ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 4636ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 4640ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 4644ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 4648ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 4652ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 4656ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 4660ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 4664ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 4668ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 4672ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 4676ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 4680ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 4684ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 4688ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 4692ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 4696ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 4700ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 4704ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 4708ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 4712ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 4716ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 4720ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 4724ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 4728ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 4732ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 4736ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 4740ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 4744ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 4748ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 4752ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 4756ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 4760ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 4764ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 4768ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 4576ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4592ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 4608ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 4624ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 4640ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 4656ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 4672ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 4688ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r42);
+                v8.w = bitcast<unsigned>(R.r43);
+                reinterpret_cast<uint4*>(base + 4704ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r44);
+                v9.y = bitcast<unsigned>(R.r61);
+                v9.z = bitcast<unsigned>(R.r62);
+                v9.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 4720ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r64);
+                v10.y = bitcast<unsigned>(R.r65);
+                v10.z = bitcast<unsigned>(R.r66);
+                v10.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 4736ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r68);
+                v11.y = bitcast<unsigned>(R.r69);
+                v11.z = bitcast<unsigned>(R.r70);
+                v11.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 4752ull * cap)[idx] = v11;
+            }
+            {
+                unsigned v12;
+                v12 = tid;
+                reinterpret_cast<unsigned*>(base + 4768ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 24: // sq_mid2
-            reinterpret_cast<unsigned int*>(base + 4776ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 4780ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4784ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4788ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4792ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4796ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 4800ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 4804ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 4808ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 4812ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 4816ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 4820ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 4824ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 4828ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 4832ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 4836ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 4840ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 4844ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 4848ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 4852ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 4856ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 4860ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 4864ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 4868ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 4872ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 4876ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 4880ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 4884ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 4888ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 4892ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 4896ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 4900ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 4904ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 4908ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 4912ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 4916ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 4920ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 4924ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 4928ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 4932ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 4936ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 4940ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 4944ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 4948ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 4952ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 4956ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 4960ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 4964ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 4968ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 4776ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4792ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 4808ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 4824ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 4840ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 4856ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 4872ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 4888ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r39);
+                v8.y = bitcast<unsigned>(R.r40);
+                v8.z = bitcast<unsigned>(R.r41);
+                v8.w = bitcast<unsigned>(R.r42);
+                reinterpret_cast<uint4*>(base + 4904ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r43);
+                v9.y = bitcast<unsigned>(R.r44);
+                v9.z = bitcast<unsigned>(R.r62);
+                v9.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 4920ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r64);
+                v10.y = bitcast<unsigned>(R.r65);
+                v10.z = bitcast<unsigned>(R.r66);
+                v10.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 4936ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r68);
+                v11.y = bitcast<unsigned>(R.r69);
+                v11.z = bitcast<unsigned>(R.r70);
+                v11.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 4952ull * cap)[idx] = v11;
+            }
+            {
+                unsigned v12;
+                v12 = tid;
+                reinterpret_cast<unsigned*>(base + 4968ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 25: // sq_mid
-            reinterpret_cast<unsigned int*>(base + 4976ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 4980ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 4984ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 4988ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 4992ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 4996ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5000ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5004ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5008ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5012ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5016ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 5020ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 5024ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5028ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5032ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5036ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5040ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5044ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5048ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5052ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5056ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5060ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5064ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 5068ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 5072ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 5076ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 5080ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 5084ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 5088ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 5092ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 5096ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 5100ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 5104ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 5108ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 5112ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 5116ull * cap)[idx] = R.r44;
-            reinterpret_cast<unsigned int*>(base + 5120ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 5124ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 5128ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 5132ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 5136ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 5140ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 5144ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 5148ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 5152ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 5156ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 5160ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 5164ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 4976ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 4992ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 5008ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 5024ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 5040ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 5056ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 5072ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 5088ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r39);
+                v8.y = bitcast<unsigned>(R.r40);
+                v8.z = bitcast<unsigned>(R.r41);
+                v8.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 5104ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r61);
+                v9.y = bitcast<unsigned>(R.r62);
+                v9.z = bitcast<unsigned>(R.r63);
+                v9.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 5120ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r65);
+                v10.y = bitcast<unsigned>(R.r66);
+                v10.z = bitcast<unsigned>(R.r67);
+                v10.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 5136ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r69);
+                v11.y = bitcast<unsigned>(R.r70);
+                v11.z = bitcast<unsigned>(R.r71);
+                v11.w = tid;
+                reinterpret_cast<uint4*>(base + 5152ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 26: // sq_tail
-            reinterpret_cast<unsigned int*>(base + 5168ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 5172ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 5176ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 5180ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 5184ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 5188ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5192ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5196ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5200ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5204ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5208ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 5212ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 5216ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5220ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5224ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5228ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5232ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5236ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5240ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5244ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5248ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5252ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5256ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 5260ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 5264ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 5268ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 5272ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 5276ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 5280ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 5284ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 5288ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 5292ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 5296ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 5300ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 5304ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 5308ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 5312ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 5316ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 5320ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 5324ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 5328ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 5332ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 5336ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 5340ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 5344ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 5348ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 5352ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 5168ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 5184ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 5200ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 5216ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 5232ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 5248ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 5264ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r37);
+                reinterpret_cast<uint4*>(base + 5280ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r39);
+                v8.y = bitcast<unsigned>(R.r40);
+                v8.z = bitcast<unsigned>(R.r41);
+                v8.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 5296ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r62);
+                v9.y = bitcast<unsigned>(R.r63);
+                v9.z = bitcast<unsigned>(R.r64);
+                v9.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 5312ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r66);
+                v10.y = bitcast<unsigned>(R.r67);
+                v10.z = bitcast<unsigned>(R.r68);
+                v10.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 5328ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r70);
+                v11.y = bitcast<unsigned>(R.r71);
+                v11.z = tid;
+                reinterpret_cast<uint4*>(base + 5344ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 27: // sq_end
-            reinterpret_cast<unsigned int*>(base + 5360ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 5364ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 5368ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 5372ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 5376ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 5380ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5384ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5388ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5392ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5396ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5400ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 5404ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5408ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5412ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5416ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5420ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5424ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5428ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5432ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5436ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5440ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5444ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 5448ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 5452ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 5456ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 5460ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 5464ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 5468ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 5472ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 5476ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 5480ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 5484ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 5488ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 5492ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 5496ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 5500ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 5504ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 5508ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 5512ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 5516ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 5520ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 5524ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 5528ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 5532ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 5536ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 5540ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 5544ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 5360ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 5376ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 5392ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 5408ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 5424ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 5440ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 5456ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 5472ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r57);
+                v8.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 5488ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r62);
+                v9.y = bitcast<unsigned>(R.r63);
+                v9.z = bitcast<unsigned>(R.r64);
+                v9.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 5504ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r66);
+                v10.y = bitcast<unsigned>(R.r67);
+                v10.z = bitcast<unsigned>(R.r68);
+                v10.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 5520ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r70);
+                v11.y = bitcast<unsigned>(R.r71);
+                v11.z = tid;
+                reinterpret_cast<uint4*>(base + 5536ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 28: // traverse_sphere_fin
-            reinterpret_cast<unsigned int*>(base + 5552ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 5556ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 5560ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 5564ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 5568ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 5572ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5576ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5580ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5584ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5588ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5592ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 5596ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5600ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5604ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5608ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5612ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5616ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5620ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5624ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5628ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5632ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5636ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 5640ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 5644ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 5648ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 5652ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 5656ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 5660ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 5664ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 5668ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 5672ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 5676ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 5680ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 5684ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 5688ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 5692ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 5696ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 5700ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 5704ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 5708ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 5712ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 5716ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 5720ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 5724ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 5728ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 5732ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 5552ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 5568ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 5584ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 5600ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 5616ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 5632ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 5648ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 5664ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r57);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 5680ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 5696ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 5712ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 5728ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 29: // traverse_cylinder
-            reinterpret_cast<unsigned int*>(base + 5736ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 5740ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 5744ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 5748ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 5752ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 5756ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5760ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5764ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5768ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5772ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5776ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 5780ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5784ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5788ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5792ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5796ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5800ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5804ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5808ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5812ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5816ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5820ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 5824ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 5828ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 5832ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 5836ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 5840ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 5844ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 5848ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 5852ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 5856ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 5860ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 5864ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 5868ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 5872ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 5876ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 5880ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 5884ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 5888ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 5892ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 5896ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 5900ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 5904ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 5908ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 5736ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 5752ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 5768ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 5784ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 5800ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 5816ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 5832ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 5848ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r61);
+                v8.y = bitcast<unsigned>(R.r62);
+                v8.z = bitcast<unsigned>(R.r63);
+                v8.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 5864ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r65);
+                v9.y = bitcast<unsigned>(R.r66);
+                v9.z = bitcast<unsigned>(R.r67);
+                v9.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 5880ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r69);
+                v10.y = bitcast<unsigned>(R.r70);
+                v10.z = bitcast<unsigned>(R.r71);
+                v10.w = tid;
+                reinterpret_cast<uint4*>(base + 5896ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 30: // traverse_cylinder_fin
-            reinterpret_cast<unsigned int*>(base + 5912ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 5916ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 5920ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 5924ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 5928ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 5932ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 5936ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 5940ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 5944ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 5948ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 5952ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 5956ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 5960ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 5964ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 5968ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 5972ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 5976ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 5980ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 5984ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 5988ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 5992ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 5996ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6000ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6004ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6008ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6012ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6016ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6020ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6024ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6028ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6032ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 6036ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6040ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6044ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 6048ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 6052ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 6056ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 6060ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 6064ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 6068ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 6072ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 6076ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 6080ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 6084ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 6088ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 6092ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 6096ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 5912ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 5928ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 5944ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 5960ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 5976ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 5992ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 6008ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r37);
+                v7.w = bitcast<unsigned>(R.r39);
+                reinterpret_cast<uint4*>(base + 6024ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r40);
+                v8.y = bitcast<unsigned>(R.r41);
+                v8.z = bitcast<unsigned>(R.r57);
+                v8.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 6040ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r62);
+                v9.y = bitcast<unsigned>(R.r63);
+                v9.z = bitcast<unsigned>(R.r64);
+                v9.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 6056ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r66);
+                v10.y = bitcast<unsigned>(R.r67);
+                v10.z = bitcast<unsigned>(R.r68);
+                v10.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 6072ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r70);
+                v11.y = bitcast<unsigned>(R.r71);
+                v11.z = tid;
+                reinterpret_cast<uint4*>(base + 6088ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 31: // traverse_disk
-            reinterpret_cast<unsigned int*>(base + 6104ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 6108ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 6112ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 6116ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 6120ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 6124ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 6128ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 6132ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 6136ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 6140ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 6144ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 6148ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 6152ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 6156ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 6160ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 6164ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 6168ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 6172ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 6176ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 6180ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 6184ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 6188ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 6192ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6196ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6200ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6204ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6208ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6212ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6216ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6220ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6224ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6228ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 6232ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 6236ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 6240ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6244ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6248ull * cap)[idx] = R.r41;
-            reinterpret_cast<float*>(base + 6252ull * cap)[idx] = R.r42;
-            reinterpret_cast<unsigned int*>(base + 6256ull * cap)[idx] = R.r43;
-            reinterpret_cast<unsigned int*>(base + 6260ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 6264ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 6268ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 6272ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 6276ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 6280ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 6284ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 6288ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 6292ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 6296ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 6300ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 6304ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 6104ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 6120ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 6136ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 6152ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 6168ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 6184ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 6200ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 6216ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 6232ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r42);
+                v9.z = bitcast<unsigned>(R.r43);
+                v9.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 6248ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r62);
+                v10.y = bitcast<unsigned>(R.r63);
+                v10.z = bitcast<unsigned>(R.r64);
+                v10.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 6264ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r66);
+                v11.y = bitcast<unsigned>(R.r67);
+                v11.z = bitcast<unsigned>(R.r68);
+                v11.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 6280ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r70);
+                v12.y = bitcast<unsigned>(R.r71);
+                v12.z = tid;
+                reinterpret_cast<uint4*>(base + 6296ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 32: // isect_disk_rest
-            reinterpret_cast<unsigned int*>(base + 6312ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 6316ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 6320ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 6324ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 6328ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 6332ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 6336ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 6340ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 6344ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 6348ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 6352ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 6356ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 6360ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 6364ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 6368ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 6372ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 6376ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 6380ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 6384ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 6388ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 6392ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 6396ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 6400ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6404ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6408ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6412ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6416ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6420ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6424ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6428ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6432ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6436ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 6440ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 6444ull * cap)[idx] = R.r38;
-            reinterpret_cast<float*>(base + 6448ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6452ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6456ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 6460ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 6464ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 6468ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 6472ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 6476ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 6480ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 6484ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 6488ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 6492ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 6496ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 6500ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 6504ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 6312ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 6328ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r14);
+                reinterpret_cast<uint4*>(base + 6344ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r15);
+                v3.y = bitcast<unsigned>(R.r16);
+                v3.z = bitcast<unsigned>(R.r17);
+                v3.w = bitcast<unsigned>(R.r18);
+                reinterpret_cast<uint4*>(base + 6360ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 6376ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 6392ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 6408ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 6424ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r39);
+                v8.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 6440ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r41);
+                v9.y = bitcast<unsigned>(R.r61);
+                v9.z = bitcast<unsigned>(R.r62);
+                v9.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 6456ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r64);
+                v10.y = bitcast<unsigned>(R.r65);
+                v10.z = bitcast<unsigned>(R.r66);
+                v10.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 6472ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r68);
+                v11.y = bitcast<unsigned>(R.r69);
+                v11.z = bitcast<unsigned>(R.r70);
+                v11.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 6488ull * cap)[idx] = v11;
+            }
+            {
+                unsigned v12;
+                v12 = tid;
+                reinterpret_cast<unsigned*>(base + 6504ull * cap)[idx] = v12;
+            }
             return;
+        }
         case 33: // isect_disk_end
-            reinterpret_cast<unsigned int*>(base + 6512ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 6516ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 6520ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 6524ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 6528ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 6532ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 6536ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 6540ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 6544ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 6548ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 6552ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 6556ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 6560ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 6564ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 6568ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 6572ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 6576ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 6580ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 6584ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 6588ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 6592ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 6596ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6600ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6604ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6608ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6612ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6616ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6620ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6624ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6628ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6632ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6636ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6640ull * cap)[idx] = R.r41;
-            reinterpret_cast<unsigned int*>(base + 6644ull * cap)[idx] = R.r57;
-            reinterpret_cast<unsigned int*>(base + 6648ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 6652ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 6656ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 6660ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 6664ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 6668ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 6672ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 6676ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 6680ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 6684ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 6688ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 6692ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 6512ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 6528ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 6544ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 6560ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 6576ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 6592ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 6608ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 6624ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r41);
+                v8.y = bitcast<unsigned>(R.r57);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 6640ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 6656ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 6672ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 6688ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 34: // traverse_room_end
-            reinterpret_cast<unsigned int*>(base + 6696ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 6700ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 6704ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 6708ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 6712ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 6716ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 6720ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 6724ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 6728ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 6732ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 6736ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 6740ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 6744ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 6748ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 6752ull * cap)[idx] = R.r18;
-            reinterpret_cast<unsigned int*>(base + 6756ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 6760ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 6764ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 6768ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 6772ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 6776ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 6780ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6784ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6788ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6792ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6796ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6800ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6804ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6808ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6812ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6816ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6820ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6824ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 6828ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 6832ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 6836ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 6840ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 6844ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 6848ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 6852ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 6856ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 6860ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 6864ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 6868ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 6696ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 6712ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 6728ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r18);
+                v3.w = bitcast<unsigned>(R.r19);
+                reinterpret_cast<uint4*>(base + 6744ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 6760ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 6776ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 6792ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r39);
+                v7.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 6808ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r61);
+                v8.y = bitcast<unsigned>(R.r62);
+                v8.z = bitcast<unsigned>(R.r63);
+                v8.w = bitcast<unsigned>(R.r64);
+                reinterpret_cast<uint4*>(base + 6824ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r65);
+                v9.y = bitcast<unsigned>(R.r66);
+                v9.z = bitcast<unsigned>(R.r67);
+                v9.w = bitcast<unsigned>(R.r68);
+                reinterpret_cast<uint4*>(base + 6840ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r69);
+                v10.y = bitcast<unsigned>(R.r70);
+                v10.z = bitcast<unsigned>(R.r71);
+                v10.w = tid;
+                reinterpret_cast<uint4*>(base + 6856ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 35: // radiance
-            reinterpret_cast<unsigned int*>(base + 6872ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 6876ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 6880ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 6884ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 6888ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 6892ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 6896ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 6900ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 6904ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 6908ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 6912ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 6916ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 6920ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 6924ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 6928ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 6932ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 6936ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 6940ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 6944ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 6948ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 6952ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 6956ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 6960ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 6964ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 6968ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 6972ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 6976ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 6980ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 6984ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 6988ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 6992ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 6996ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7000ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7004ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7008ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7012ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 7016ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 7020ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 7024ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 7028ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7032ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7036ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7040ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 6872ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 6888ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 6904ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 6920ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 6936ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 6952ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 6968ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r39);
+                v7.z = bitcast<unsigned>(R.r40);
+                v7.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 6984ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r62);
+                v8.y = bitcast<unsigned>(R.r63);
+                v8.z = bitcast<unsigned>(R.r64);
+                v8.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 7000ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r66);
+                v9.y = bitcast<unsigned>(R.r67);
+                v9.z = bitcast<unsigned>(R.r68);
+                v9.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 7016ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r70);
+                v10.y = bitcast<unsigned>(R.r71);
+                v10.z = tid;
+                reinterpret_cast<uint4*>(base + 7032ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 36: // set_materials
-            reinterpret_cast<unsigned int*>(base + 7048ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7052ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7056ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7060ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7064ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7068ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7072ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7076ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7080ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7084ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7088ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7092ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7096ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7100ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7104ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7108ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7112ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7116ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7120ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7124ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7128ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7132ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7136ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7140ull * cap)[idx] = R.r30;
-            reinterpret_cast<unsigned int*>(base + 7144ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7148ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 7152ull * cap)[idx] = R.r39;
-            reinterpret_cast<unsigned int*>(base + 7156ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7160ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7164ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7168ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7172ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7176ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7048ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7064ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7080ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7096ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7112ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7128ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r34);
+                v6.y = bitcast<unsigned>(R.r35);
+                v6.z = bitcast<unsigned>(R.r39);
+                v6.w = bitcast<unsigned>(R.r40);
+                reinterpret_cast<uint4*>(base + 7144ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r61);
+                v7.y = bitcast<unsigned>(R.r69);
+                v7.z = bitcast<unsigned>(R.r70);
+                v7.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 7160ull * cap)[idx] = v7;
+            }
+            {
+                unsigned v8;
+                v8 = tid;
+                reinterpret_cast<unsigned*>(base + 7176ull * cap)[idx] = v8;
+            }
             return;
+        }
         case 37: // set_polygon_normal
-            reinterpret_cast<unsigned int*>(base + 7184ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7188ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7192ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7196ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7200ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7204ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7208ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7212ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7216ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7220ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7224ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7228ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7232ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7236ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7240ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7244ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7248ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7252ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7256ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7260ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7264ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7268ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7272ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7276ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 7280ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 7284ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 7288ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 7292ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7296ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 7300ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7304ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7308ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7312ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7316ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7320ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7324ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7328ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7332ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7184ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7200ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7216ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7232ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7248ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7264ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 7280ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 7296ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r69);
+                v8.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 7312ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r71);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 7328ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 38: // set_disk_normal
-            reinterpret_cast<unsigned int*>(base + 7336ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7340ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7344ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7348ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7352ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7356ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7360ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7364ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7368ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7372ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7376ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7380ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7384ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7388ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7392ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7396ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7400ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7404ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7408ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7412ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7416ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7420ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7424ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7428ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 7432ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 7436ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 7440ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 7444ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7448ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 7452ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7456ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7460ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7464ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7468ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7472ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7476ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7480ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7484ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7336ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7352ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7368ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7384ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7400ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7416ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 7432ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 7448ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r69);
+                v8.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 7464ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r71);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 7480ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 39: // compute_sphere_normal
-            reinterpret_cast<unsigned int*>(base + 7488ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7492ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7496ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7500ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7504ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7508ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7512ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7516ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7520ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7524ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7528ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7532ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7536ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7540ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7544ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7548ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7552ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7556ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7560ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7564ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7568ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7572ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7576ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7580ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 7584ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 7588ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 7592ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 7596ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7600ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 7604ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7608ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7612ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7616ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7620ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7624ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7628ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7632ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7636ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7488ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7504ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7520ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7536ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7552ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7568ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 7584ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 7600ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r69);
+                v8.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 7616ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r71);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 7632ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 40: // compute_cylinder_normal
-            reinterpret_cast<unsigned int*>(base + 7640ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7644ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7648ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7652ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7656ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7660ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7664ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7668ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7672ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7676ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7680ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7684ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7688ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7692ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7696ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7700ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7704ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7708ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7712ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7716ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7720ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7724ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7728ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7732ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 7736ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 7740ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 7744ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 7748ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7752ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 7756ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7760ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7764ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7768ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7772ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7776ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7780ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7784ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7788ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7640ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7656ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7672ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7688ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7704ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7720ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 7736ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 7752ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r69);
+                v8.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 7768ull * cap)[idx] = v8;
+            }
+            {
+                uint2 v9;
+                v9.x = bitcast<unsigned>(R.r71);
+                v9.y = tid;
+                reinterpret_cast<uint2*>(base + 7784ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 41: // set_materials_end
-            reinterpret_cast<unsigned int*>(base + 7792ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7796ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7800ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7804ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7808ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7812ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7816ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7820ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7824ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7828ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 7832ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 7836ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 7840ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 7844ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 7848ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 7852ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 7856ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 7860ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 7864ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 7868ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 7872ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 7876ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 7880ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 7884ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 7888ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 7892ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 7896ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 7900ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 7904ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 7908ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 7912ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 7916ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 7920ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 7924ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 7928ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 7932ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 7936ull * cap)[idx] = R.r67;
-            reinterpret_cast<float*>(base + 7940ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 7944ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 7948ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 7952ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7792ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7808ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7824ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 7840ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 7856ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 7872ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 7888ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 7904ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 7920ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r69);
+                v9.z = bitcast<unsigned>(R.r70);
+                v9.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 7936ull * cap)[idx] = v9;
+            }
+            {
+                unsigned v10;
+                v10 = tid;
+                reinterpret_cast<unsigned*>(base + 7952ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 42: // test_direct
-            reinterpret_cast<unsigned int*>(base + 7960ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 7964ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 7968ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 7972ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 7976ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 7980ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 7984ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 7988ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 7992ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 7996ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8000ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8004ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8008ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8012ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8016ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 8020ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 8024ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8028ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8032ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8036ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8040ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8044ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8048ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8052ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8056ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8060ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8064ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8068ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8072ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 8076ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 8080ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8084ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 8088ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 8092ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 8096ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8100ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8104ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8108ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 8112ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 8116ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 8120ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 8124ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 7960ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 7976ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 7992ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 8008ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 8024ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 8040ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 8056ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 8072ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 8088ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r68);
+                v9.z = bitcast<unsigned>(R.r69);
+                v9.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 8104ull * cap)[idx] = v9;
+            }
+            {
+                uint2 v10;
+                v10.x = bitcast<unsigned>(R.r71);
+                v10.y = tid;
+                reinterpret_cast<uint2*>(base + 8120ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 43: // direct
-            reinterpret_cast<unsigned int*>(base + 8128ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8132ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8136ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8140ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8144ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8148ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 8152ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 8156ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8160ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8164ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8168ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8172ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8176ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8180ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8184ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 8188ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 8192ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 8196ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8200ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8204ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8208ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8212ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8216ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8220ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8224ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8228ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8232ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8236ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8240ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8244ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 8248ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 8252ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8256ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 8260ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 8264ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 8268ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8272ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8276ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8280ull * cap)[idx] = R.r68;
-            reinterpret_cast<unsigned*>(base + 8284ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8128ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 8144ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 8160ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 8176ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r21);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 8192ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 8208ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 8224ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 8240ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r62);
+                v8.y = bitcast<unsigned>(R.r63);
+                v8.z = bitcast<unsigned>(R.r64);
+                v8.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 8256ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r66);
+                v9.y = bitcast<unsigned>(R.r67);
+                v9.z = bitcast<unsigned>(R.r68);
+                v9.w = tid;
+                reinterpret_cast<uint4*>(base + 8272ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 44: // direct_pdf
-            reinterpret_cast<unsigned int*>(base + 8288ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8292ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8296ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8300ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8304ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8308ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 8312ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 8316ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8320ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8324ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8328ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8332ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8336ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8340ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8344ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 8348ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8352ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8356ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8360ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8364ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8368ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8372ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8376ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8380ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8384ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8388ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8392ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8396ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 8400ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 8404ull * cap)[idx] = R.r40;
-            reinterpret_cast<unsigned int*>(base + 8408ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8412ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 8416ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 8420ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 8424ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8428ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8432ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8436ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 8440ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 8444ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 8448ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 8452ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8288ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 8304ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 8320ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 8336ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 8352ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 8368ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 8384ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r40);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 8400ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 8416ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r68);
+                v9.z = bitcast<unsigned>(R.r69);
+                v9.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 8432ull * cap)[idx] = v9;
+            }
+            {
+                uint2 v10;
+                v10.x = bitcast<unsigned>(R.r71);
+                v10.y = tid;
+                reinterpret_cast<uint2*>(base + 8448ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 45: // direct_metal
-            reinterpret_cast<unsigned int*>(base + 8456ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8460ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8464ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8468ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8472ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8476ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 8480ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 8484ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 8488ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 8492ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8496ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8500ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8504ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8508ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8512ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8516ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8520ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 8524ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8528ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8532ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8536ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8540ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8544ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8548ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8552ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8556ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8560ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8564ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8568ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8572ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 8576ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 8580ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8584ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 8588ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 8592ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 8596ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8600ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8604ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8608ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 8612ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 8616ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 8620ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 8624ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8456ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 8472ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r9);
+                v2.y = bitcast<unsigned>(R.r10);
+                v2.z = bitcast<unsigned>(R.r11);
+                v2.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 8488ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r13);
+                v3.y = bitcast<unsigned>(R.r15);
+                v3.z = bitcast<unsigned>(R.r16);
+                v3.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 8504ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 8520ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 8536ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 8552ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 8568ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r62);
+                v8.y = bitcast<unsigned>(R.r63);
+                v8.z = bitcast<unsigned>(R.r64);
+                v8.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 8584ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r66);
+                v9.y = bitcast<unsigned>(R.r67);
+                v9.z = bitcast<unsigned>(R.r68);
+                v9.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 8600ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r70);
+                v10.y = bitcast<unsigned>(R.r71);
+                v10.z = tid;
+                reinterpret_cast<uint4*>(base + 8616ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 46: // window
-            reinterpret_cast<unsigned int*>(base + 8632ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8636ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8640ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8644ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8648ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8652ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 8656ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 8660ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8664ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8668ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8672ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8676ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8680ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8684ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8688ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 8692ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 8696ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 8700ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8704ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8708ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8712ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8716ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8720ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8724ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8728ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8732ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8736ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8740ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8744ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8748ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 8752ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 8756ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8760ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 8764ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 8768ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 8772ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8776ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8780ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8784ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 8788ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 8792ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 8796ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 8800ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8632ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 8648ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 8664ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 8680ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r21);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 8696ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 8712ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 8728ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 8744ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r62);
+                v8.y = bitcast<unsigned>(R.r63);
+                v8.z = bitcast<unsigned>(R.r64);
+                v8.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 8760ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r66);
+                v9.y = bitcast<unsigned>(R.r67);
+                v9.z = bitcast<unsigned>(R.r68);
+                v9.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 8776ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r70);
+                v10.y = bitcast<unsigned>(R.r71);
+                v10.z = tid;
+                reinterpret_cast<uint4*>(base + 8792ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 47: // lambert_indirect
-            reinterpret_cast<unsigned int*>(base + 8808ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8812ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8816ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8820ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8824ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8828ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8832ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8836ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 8840ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 8844ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 8848ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 8852ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 8856ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 8860ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 8864ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 8868ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 8872ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 8876ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 8880ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 8884ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 8888ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 8892ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 8896ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 8900ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 8904ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 8908ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 8912ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 8916ull * cap)[idx] = R.r34;
-            reinterpret_cast<unsigned int*>(base + 8920ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 8924ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 8928ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 8932ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 8936ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 8940ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 8944ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 8948ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 8952ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8808ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r10);
+                v1.z = bitcast<unsigned>(R.r11);
+                v1.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 8824ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r13);
+                v2.y = bitcast<unsigned>(R.r15);
+                v2.z = bitcast<unsigned>(R.r16);
+                v2.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 8840ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r19);
+                v3.y = bitcast<unsigned>(R.r20);
+                v3.z = bitcast<unsigned>(R.r21);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 8856ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 8872ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 8888ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 8904ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r61);
+                v7.y = bitcast<unsigned>(R.r65);
+                v7.z = bitcast<unsigned>(R.r66);
+                v7.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 8920ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r68);
+                v8.y = bitcast<unsigned>(R.r69);
+                v8.z = bitcast<unsigned>(R.r70);
+                v8.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 8936ull * cap)[idx] = v8;
+            }
+            {
+                unsigned v9;
+                v9 = tid;
+                reinterpret_cast<unsigned*>(base + 8952ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 48: // tth_begin
-            reinterpret_cast<unsigned int*>(base + 8960ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 8964ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 8968ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 8972ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 8976ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 8980ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 8984ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 8988ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 8992ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 8996ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9000ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 9004ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9008ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9012ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9016ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 9020ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 9024ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9028ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9032ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9036ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9040ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9044ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9048ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9052ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9056ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 9060ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 9064ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 9068ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 9072ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9076ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 9080ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9084ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9088ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9092ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9096ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9100ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9104ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9108ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9112ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9116ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9120ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9124ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 8960ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 8976ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 8992ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 9008ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 9024ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 9040ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r31);
+                v6.z = bitcast<unsigned>(R.r32);
+                v6.w = bitcast<unsigned>(R.r33);
+                reinterpret_cast<uint4*>(base + 9056ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r34);
+                v7.y = bitcast<unsigned>(R.r35);
+                v7.z = bitcast<unsigned>(R.r61);
+                v7.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 9072ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r63);
+                v8.y = bitcast<unsigned>(R.r64);
+                v8.z = bitcast<unsigned>(R.r65);
+                v8.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 9088ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r67);
+                v9.y = bitcast<unsigned>(R.r68);
+                v9.z = bitcast<unsigned>(R.r69);
+                v9.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 9104ull * cap)[idx] = v9;
+            }
+            {
+                uint2 v10;
+                v10.x = bitcast<unsigned>(R.r71);
+                v10.y = tid;
+                reinterpret_cast<uint2*>(base + 9120ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 49: // glass
-            reinterpret_cast<unsigned int*>(base + 9128ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 9132ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 9136ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 9140ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 9144ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 9148ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 9152ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 9156ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 9160ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 9164ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9168ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 9172ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9176ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9180ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9184ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 9188ull * cap)[idx] = R.r20;
-            reinterpret_cast<float*>(base + 9192ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9196ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9200ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9204ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9208ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9212ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9216ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9220ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9224ull * cap)[idx] = R.r30;
-            reinterpret_cast<unsigned int*>(base + 9228ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9232ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 9236ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9240ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9244ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9248ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9252ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9256ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9260ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9264ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9268ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9272ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9276ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9280ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 9128ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 9144ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 9160ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 9176ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r22);
+                v4.y = bitcast<unsigned>(R.r23);
+                v4.z = bitcast<unsigned>(R.r24);
+                v4.w = bitcast<unsigned>(R.r25);
+                reinterpret_cast<uint4*>(base + 9192ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r26);
+                v5.y = bitcast<unsigned>(R.r27);
+                v5.z = bitcast<unsigned>(R.r28);
+                v5.w = bitcast<unsigned>(R.r29);
+                reinterpret_cast<uint4*>(base + 9208ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r30);
+                v6.y = bitcast<unsigned>(R.r34);
+                v6.z = bitcast<unsigned>(R.r35);
+                v6.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 9224ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r62);
+                v7.y = bitcast<unsigned>(R.r63);
+                v7.z = bitcast<unsigned>(R.r64);
+                v7.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 9240ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r66);
+                v8.y = bitcast<unsigned>(R.r67);
+                v8.z = bitcast<unsigned>(R.r68);
+                v8.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 9256ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r70);
+                v9.y = bitcast<unsigned>(R.r71);
+                v9.z = tid;
+                reinterpret_cast<uint4*>(base + 9272ull * cap)[idx] = v9;
+            }
             return;
+        }
         case 50: // indirect_metal
-            reinterpret_cast<unsigned int*>(base + 9288ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 9292ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 9296ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 9300ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 9304ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 9308ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 9312ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 9316ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 9320ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 9324ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9328ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 9332ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9336ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9340ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9344ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 9348ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 9352ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 9356ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9360ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9364ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9368ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9372ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9376ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9380ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9384ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9388ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 9392ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 9396ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 9400ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 9404ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9408ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 9412ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9416ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9420ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9424ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9428ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9432ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9436ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9440ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9444ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9448ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9452ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9456ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 9288ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 9304ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 9320ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 9336ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r21);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 9352ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 9368ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 9384ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r61);
+                reinterpret_cast<uint4*>(base + 9400ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r62);
+                v8.y = bitcast<unsigned>(R.r63);
+                v8.z = bitcast<unsigned>(R.r64);
+                v8.w = bitcast<unsigned>(R.r65);
+                reinterpret_cast<uint4*>(base + 9416ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r66);
+                v9.y = bitcast<unsigned>(R.r67);
+                v9.z = bitcast<unsigned>(R.r68);
+                v9.w = bitcast<unsigned>(R.r69);
+                reinterpret_cast<uint4*>(base + 9432ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r70);
+                v10.y = bitcast<unsigned>(R.r71);
+                v10.z = tid;
+                reinterpret_cast<uint4*>(base + 9448ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 51: // get_slope_mid
-            reinterpret_cast<unsigned int*>(base + 9464ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 9468ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 9472ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 9476ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 9480ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 9484ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 9488ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 9492ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 9496ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 9500ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9504ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 9508ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9512ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9516ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9520ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned int*>(base + 9524ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 9528ull * cap)[idx] = R.r21;
-            reinterpret_cast<float*>(base + 9532ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9536ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9540ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9544ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9548ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9552ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9556ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9560ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9564ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 9568ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 9572ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 9576ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 9580ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9584ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 9588ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 9592ull * cap)[idx] = R.r37;
-            reinterpret_cast<float*>(base + 9596ull * cap)[idx] = R.r38;
-            reinterpret_cast<unsigned int*>(base + 9600ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9604ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9608ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9612ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9616ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9620ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9624ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9628ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9632ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9636ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9640ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9644ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 9464ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 9480ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 9496ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r20);
+                reinterpret_cast<uint4*>(base + 9512ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r21);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 9528ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 9544ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 9560ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 9576ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r38);
+                v8.z = bitcast<unsigned>(R.r61);
+                v8.w = bitcast<unsigned>(R.r62);
+                reinterpret_cast<uint4*>(base + 9592ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r63);
+                v9.y = bitcast<unsigned>(R.r64);
+                v9.z = bitcast<unsigned>(R.r65);
+                v9.w = bitcast<unsigned>(R.r66);
+                reinterpret_cast<uint4*>(base + 9608ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r67);
+                v10.y = bitcast<unsigned>(R.r68);
+                v10.z = bitcast<unsigned>(R.r69);
+                v10.w = bitcast<unsigned>(R.r70);
+                reinterpret_cast<uint4*>(base + 9624ull * cap)[idx] = v10;
+            }
+            {
+                uint2 v11;
+                v11.x = bitcast<unsigned>(R.r71);
+                v11.y = tid;
+                reinterpret_cast<uint2*>(base + 9640ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 52: // get_slope_end
-            reinterpret_cast<unsigned int*>(base + 9648ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 9652ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 9656ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 9660ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 9664ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 9668ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 9672ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 9676ull * cap)[idx] = R.r8;
-            reinterpret_cast<unsigned int*>(base + 9680ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 9684ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 9688ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9692ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 9696ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 9700ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9704ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9708ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9712ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 9716ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9720ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9724ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9728ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9732ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9736ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9740ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9744ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9748ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 9752ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 9756ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 9760ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 9764ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9768ull * cap)[idx] = R.r35;
-            reinterpret_cast<float*>(base + 9772ull * cap)[idx] = R.r36;
-            reinterpret_cast<float*>(base + 9776ull * cap)[idx] = R.r37;
-            reinterpret_cast<unsigned int*>(base + 9780ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9784ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9788ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9792ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9796ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9800ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9804ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9808ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9812ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9816ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9820ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9824ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 9648ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r8);
+                reinterpret_cast<uint4*>(base + 9664ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r10);
+                v2.y = bitcast<unsigned>(R.r11);
+                v2.z = bitcast<unsigned>(R.r12);
+                v2.w = bitcast<unsigned>(R.r13);
+                reinterpret_cast<uint4*>(base + 9680ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r14);
+                v3.y = bitcast<unsigned>(R.r15);
+                v3.z = bitcast<unsigned>(R.r16);
+                v3.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 9696ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r19);
+                v4.y = bitcast<unsigned>(R.r22);
+                v4.z = bitcast<unsigned>(R.r23);
+                v4.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 9712ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r25);
+                v5.y = bitcast<unsigned>(R.r26);
+                v5.z = bitcast<unsigned>(R.r27);
+                v5.w = bitcast<unsigned>(R.r28);
+                reinterpret_cast<uint4*>(base + 9728ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r29);
+                v6.y = bitcast<unsigned>(R.r30);
+                v6.z = bitcast<unsigned>(R.r31);
+                v6.w = bitcast<unsigned>(R.r32);
+                reinterpret_cast<uint4*>(base + 9744ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r33);
+                v7.y = bitcast<unsigned>(R.r34);
+                v7.z = bitcast<unsigned>(R.r35);
+                v7.w = bitcast<unsigned>(R.r36);
+                reinterpret_cast<uint4*>(base + 9760ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r37);
+                v8.y = bitcast<unsigned>(R.r61);
+                v8.z = bitcast<unsigned>(R.r62);
+                v8.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 9776ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r64);
+                v9.y = bitcast<unsigned>(R.r65);
+                v9.z = bitcast<unsigned>(R.r66);
+                v9.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 9792ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r68);
+                v10.y = bitcast<unsigned>(R.r69);
+                v10.z = bitcast<unsigned>(R.r70);
+                v10.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 9808ull * cap)[idx] = v10;
+            }
+            {
+                unsigned v11;
+                v11 = tid;
+                reinterpret_cast<unsigned*>(base + 9824ull * cap)[idx] = v11;
+            }
             return;
+        }
         case 53: // fin_sample
-            reinterpret_cast<unsigned int*>(base + 9832ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 9836ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 9840ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 9844ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 9848ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 9852ull * cap)[idx] = R.r6;
-            reinterpret_cast<unsigned int*>(base + 9856ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 9860ull * cap)[idx] = R.r10;
-            reinterpret_cast<unsigned int*>(base + 9864ull * cap)[idx] = R.r11;
-            reinterpret_cast<float*>(base + 9868ull * cap)[idx] = R.r12;
-            reinterpret_cast<float*>(base + 9872ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 9876ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 9880ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 9884ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 9888ull * cap)[idx] = R.r19;
-            reinterpret_cast<float*>(base + 9892ull * cap)[idx] = R.r22;
-            reinterpret_cast<float*>(base + 9896ull * cap)[idx] = R.r23;
-            reinterpret_cast<float*>(base + 9900ull * cap)[idx] = R.r24;
-            reinterpret_cast<float*>(base + 9904ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 9908ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 9912ull * cap)[idx] = R.r27;
-            reinterpret_cast<float*>(base + 9916ull * cap)[idx] = R.r28;
-            reinterpret_cast<float*>(base + 9920ull * cap)[idx] = R.r29;
-            reinterpret_cast<float*>(base + 9924ull * cap)[idx] = R.r30;
-            reinterpret_cast<float*>(base + 9928ull * cap)[idx] = R.r31;
-            reinterpret_cast<float*>(base + 9932ull * cap)[idx] = R.r32;
-            reinterpret_cast<float*>(base + 9936ull * cap)[idx] = R.r33;
-            reinterpret_cast<unsigned int*>(base + 9940ull * cap)[idx] = R.r34;
-            reinterpret_cast<float*>(base + 9944ull * cap)[idx] = R.r35;
-            reinterpret_cast<unsigned int*>(base + 9948ull * cap)[idx] = R.r61;
-            reinterpret_cast<float*>(base + 9952ull * cap)[idx] = R.r62;
-            reinterpret_cast<float*>(base + 9956ull * cap)[idx] = R.r63;
-            reinterpret_cast<float*>(base + 9960ull * cap)[idx] = R.r64;
-            reinterpret_cast<float*>(base + 9964ull * cap)[idx] = R.r65;
-            reinterpret_cast<float*>(base + 9968ull * cap)[idx] = R.r66;
-            reinterpret_cast<float*>(base + 9972ull * cap)[idx] = R.r67;
-            reinterpret_cast<unsigned int*>(base + 9976ull * cap)[idx] = R.r68;
-            reinterpret_cast<float*>(base + 9980ull * cap)[idx] = R.r69;
-            reinterpret_cast<float*>(base + 9984ull * cap)[idx] = R.r70;
-            reinterpret_cast<float*>(base + 9988ull * cap)[idx] = R.r71;
-            reinterpret_cast<unsigned*>(base + 9992ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 9832ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r6);
+                v1.z = bitcast<unsigned>(R.r7);
+                v1.w = bitcast<unsigned>(R.r10);
+                reinterpret_cast<uint4*>(base + 9848ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r11);
+                v2.y = bitcast<unsigned>(R.r12);
+                v2.z = bitcast<unsigned>(R.r13);
+                v2.w = bitcast<unsigned>(R.r15);
+                reinterpret_cast<uint4*>(base + 9864ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r16);
+                v3.y = bitcast<unsigned>(R.r17);
+                v3.z = bitcast<unsigned>(R.r19);
+                v3.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 9880ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r23);
+                v4.y = bitcast<unsigned>(R.r24);
+                v4.z = bitcast<unsigned>(R.r25);
+                v4.w = bitcast<unsigned>(R.r26);
+                reinterpret_cast<uint4*>(base + 9896ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r27);
+                v5.y = bitcast<unsigned>(R.r28);
+                v5.z = bitcast<unsigned>(R.r29);
+                v5.w = bitcast<unsigned>(R.r30);
+                reinterpret_cast<uint4*>(base + 9912ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r31);
+                v6.y = bitcast<unsigned>(R.r32);
+                v6.z = bitcast<unsigned>(R.r33);
+                v6.w = bitcast<unsigned>(R.r34);
+                reinterpret_cast<uint4*>(base + 9928ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r35);
+                v7.y = bitcast<unsigned>(R.r61);
+                v7.z = bitcast<unsigned>(R.r62);
+                v7.w = bitcast<unsigned>(R.r63);
+                reinterpret_cast<uint4*>(base + 9944ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r64);
+                v8.y = bitcast<unsigned>(R.r65);
+                v8.z = bitcast<unsigned>(R.r66);
+                v8.w = bitcast<unsigned>(R.r67);
+                reinterpret_cast<uint4*>(base + 9960ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r68);
+                v9.y = bitcast<unsigned>(R.r69);
+                v9.z = bitcast<unsigned>(R.r70);
+                v9.w = bitcast<unsigned>(R.r71);
+                reinterpret_cast<uint4*>(base + 9976ull * cap)[idx] = v9;
+            }
+            {
+                unsigned v10;
+                v10 = tid;
+                reinterpret_cast<unsigned*>(base + 9992ull * cap)[idx] = v10;
+            }
             return;
+        }
         case 54: // fin_pixel
-            reinterpret_cast<unsigned int*>(base + 10000ull * cap)[idx] = R.r1;
-            reinterpret_cast<float*>(base + 10004ull * cap)[idx] = R.r2;
-            reinterpret_cast<float*>(base + 10008ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 10012ull * cap)[idx] = R.r4;
-            reinterpret_cast<unsigned int*>(base + 10016ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 10020ull * cap)[idx] = R.r19;
-            reinterpret_cast<unsigned*>(base + 10024ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = bitcast<unsigned>(R.r3);
+                v0.w = bitcast<unsigned>(R.r4);
+                reinterpret_cast<uint4*>(base + 10000ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r5);
+                v1.y = bitcast<unsigned>(R.r19);
+                v1.z = tid;
+                reinterpret_cast<uint4*>(base + 10016ull * cap)[idx] = v1;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -4577,2540 +7255,3292 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 4ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 12ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 16ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 20ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 24ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 28ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 32ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 36ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 40ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 44ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 48ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 52ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 56ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 60ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 64ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 68ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 72ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 76ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 80ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 84ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 88ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 92ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 96ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 100ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 104ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 108ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r14 = bitcast<unsigned int>(v0.y);
+            R.r22 = bitcast<float>(v0.z);
+            R.r23 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r24 = bitcast<float>(v1.x);
+            R.r25 = bitcast<float>(v1.y);
+            R.r26 = bitcast<float>(v1.z);
+            R.r27 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 32ull * cap)[idx];
+            R.r28 = bitcast<float>(v2.x);
+            R.r29 = bitcast<float>(v2.y);
+            R.r30 = bitcast<float>(v2.z);
+            R.r31 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 48ull * cap)[idx];
+            R.r32 = bitcast<float>(v3.x);
+            R.r33 = bitcast<float>(v3.y);
+            R.r34 = bitcast<unsigned int>(v3.z);
+            R.r35 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 64ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v4.x);
+            R.r62 = bitcast<float>(v4.y);
+            R.r63 = bitcast<float>(v4.z);
+            R.r64 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 80ull * cap)[idx];
+            R.r65 = bitcast<float>(v5.x);
+            R.r66 = bitcast<float>(v5.y);
+            R.r67 = bitcast<float>(v5.z);
+            R.r68 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 96ull * cap)[idx];
+            R.r69 = bitcast<float>(v6.x);
+            R.r70 = bitcast<float>(v6.y);
+            R.r71 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 1: // roll
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 112ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 116ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 120ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 124ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 128ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 132ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 136ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 140ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 144ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 148ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 152ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 156ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 160ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 164ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 168ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 172ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 176ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 180ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 184ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 188ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 192ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 196ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 200ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 204ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 208ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 212ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 216ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 220ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 224ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 228ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 232ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 236ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 240ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 244ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 248ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 252ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 256ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 260ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 264ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 268ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 272ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 276ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 112ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 128ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 144ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 160ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 176ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 192ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 208ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 224ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 240ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 256ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(base + 272ull * cap)[idx];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
         case 2: // roll_split
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 280ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 284ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 288ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 292ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 296ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 300ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 304ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 308ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 312ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 316ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 320ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 324ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 328ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 332ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 336ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 340ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 344ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 348ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 352ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 356ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 360ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 364ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 368ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 372ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 376ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 380ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 384ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 388ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 392ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 396ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 400ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 404ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 408ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 412ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 416ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 420ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 424ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 428ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 432ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 436ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 440ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 444ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 448ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 452ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 456ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 460ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 280ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 296ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 312ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 328ull * cap)[idx];
+            R.r13 = bitcast<float>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 344ull * cap)[idx];
+            R.r18 = bitcast<unsigned int>(v4.x);
+            R.r19 = bitcast<unsigned int>(v4.y);
+            R.r20 = bitcast<unsigned int>(v4.z);
+            R.r21 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 360ull * cap)[idx];
+            R.r22 = bitcast<float>(v5.x);
+            R.r23 = bitcast<float>(v5.y);
+            R.r24 = bitcast<float>(v5.z);
+            R.r25 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 376ull * cap)[idx];
+            R.r26 = bitcast<float>(v6.x);
+            R.r27 = bitcast<float>(v6.y);
+            R.r28 = bitcast<float>(v6.z);
+            R.r29 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 392ull * cap)[idx];
+            R.r30 = bitcast<float>(v7.x);
+            R.r31 = bitcast<float>(v7.y);
+            R.r32 = bitcast<float>(v7.z);
+            R.r33 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 408ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v8.x);
+            R.r35 = bitcast<float>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 424ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 440ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 456ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 3: // sample_pixel
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 464ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 468ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 472ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 476ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 480ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 484ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 488ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 492ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 496ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 500ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 504ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 508ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 512ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 516ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 520ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 524ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 528ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 532ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 536ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 540ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 544ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 548ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 552ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 556ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 560ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 564ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 568ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 572ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 464ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 480ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r10 = bitcast<unsigned int>(v1.y);
+            R.r11 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 496ull * cap)[idx];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 512ull * cap)[idx];
+            R.r18 = bitcast<unsigned int>(v3.x);
+            R.r19 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<unsigned int>(v3.z);
+            R.r21 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 528ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v4.x);
+            R.r62 = bitcast<float>(v4.y);
+            R.r63 = bitcast<float>(v4.z);
+            R.r64 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 544ull * cap)[idx];
+            R.r65 = bitcast<float>(v5.x);
+            R.r66 = bitcast<float>(v5.y);
+            R.r67 = bitcast<float>(v5.z);
+            R.r68 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 560ull * cap)[idx];
+            R.r69 = bitcast<float>(v6.x);
+            R.r70 = bitcast<float>(v6.y);
+            R.r71 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 4: // traverse_scene
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 576ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 580ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 584ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 588ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 592ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 596ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 600ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 604ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 608ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 612ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 616ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 620ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 624ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 628ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 632ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 636ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 640ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 644ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 648ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 652ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 656ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 660ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 664ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 668ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 672ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 676ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 680ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 684ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 688ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 692ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 696ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 700ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 704ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 708ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 712ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 716ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 720ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 724ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 728ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 732ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 736ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 740ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 576ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 592ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 608ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 624ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 640ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 656ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 672ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 688ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 704ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 720ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(base + 736ull * cap)[idx];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
         case 5: // traverse_box
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 744ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 748ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 752ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 756ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 760ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 764ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 768ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 772ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 776ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 780ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 784ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 788ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 792ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 796ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 800ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 804ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 808ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 812ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 816ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 820ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 824ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 828ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 832ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 836ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 840ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 844ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 848ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 852ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 856ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 860ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 864ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 868ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 872ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 876ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 880ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 884ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 888ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 892ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 896ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 900ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 904ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 908ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 912ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 916ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 920ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 744ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 760ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 776ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 792ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 808ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 824ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 840ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 856ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 872ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r61 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 888ull * cap)[idx];
+            R.r64 = bitcast<float>(v9.x);
+            R.r65 = bitcast<float>(v9.y);
+            R.r66 = bitcast<float>(v9.z);
+            R.r67 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 904ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v10.x);
+            R.r69 = bitcast<float>(v10.y);
+            R.r70 = bitcast<float>(v10.z);
+            R.r71 = bitcast<float>(v10.w);
+            const unsigned v11 = reinterpret_cast<const unsigned*>(base + 920ull * cap)[idx];
+            return v11;
+        }
         case 6: // isect_quad_l1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 928ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 932ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 936ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 940ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 944ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 948ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 952ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 956ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 960ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 964ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 968ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 972ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 976ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 980ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 984ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 988ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 992ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 996ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 1000ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 1004ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 1008ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 1012ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1016ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1020ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1024ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1028ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1032ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 1036ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 1040ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 1044ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 1048ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1052ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1056ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1060ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1064ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 1068ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 1072ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1076ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 1080ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 1084ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 1088ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1092ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1096ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 1100ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1104ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1108ull * cap)[idx];
-            R.r58 = reinterpret_cast<const float*>(base + 1112ull * cap)[idx];
-            R.r59 = reinterpret_cast<const float*>(base + 1116ull * cap)[idx];
-            R.r60 = reinterpret_cast<const float*>(base + 1120ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 1124ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 1128ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 1132ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 1136ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 1140ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 1144ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 1148ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 1152ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 1156ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 1160ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 1164ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1168ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 928ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 944ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 960ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 976ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 992ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1008ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1024ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1040ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 1056ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 1072ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 1088ull * cap)[idx];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 1104ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r58 = bitcast<float>(v11.z);
+            R.r59 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 1120ull * cap)[idx];
+            R.r60 = bitcast<float>(v12.x);
+            R.r61 = bitcast<unsigned int>(v12.y);
+            R.r62 = bitcast<float>(v12.z);
+            R.r63 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 1136ull * cap)[idx];
+            R.r64 = bitcast<float>(v13.x);
+            R.r65 = bitcast<float>(v13.y);
+            R.r66 = bitcast<float>(v13.z);
+            R.r67 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(base + 1152ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v14.x);
+            R.r69 = bitcast<float>(v14.y);
+            R.r70 = bitcast<float>(v14.z);
+            R.r71 = bitcast<float>(v14.w);
+            const unsigned v15 = reinterpret_cast<const unsigned*>(base + 1168ull * cap)[idx];
+            return v15;
+        }
         case 7: // isect_quad_l2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1176ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1180ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1184ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1188ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1192ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1196ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1200ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1204ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 1208ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1212ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1216ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1220ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1224ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1228ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 1232ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 1236ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 1240ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 1244ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1248ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 1252ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 1256ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 1260ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 1264ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1268ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1272ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1276ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1280ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1284ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 1288ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 1292ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 1296ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 1300ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1304ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1308ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1312ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1316ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 1320ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 1324ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1328ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 1332ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 1336ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 1340ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1344ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1348ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 1352ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1356ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1360ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 1364ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 1368ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 1372ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 1376ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 1380ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 1384ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 1388ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 1392ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 1396ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 1400ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 1404ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1408ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1176ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1192ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1208ull * cap)[idx];
+            R.r10 = bitcast<unsigned int>(v2.x);
+            R.r11 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1224ull * cap)[idx];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1240ull * cap)[idx];
+            R.r18 = bitcast<unsigned int>(v4.x);
+            R.r19 = bitcast<unsigned int>(v4.y);
+            R.r22 = bitcast<float>(v4.z);
+            R.r23 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1256ull * cap)[idx];
+            R.r24 = bitcast<float>(v5.x);
+            R.r25 = bitcast<float>(v5.y);
+            R.r26 = bitcast<float>(v5.z);
+            R.r27 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1272ull * cap)[idx];
+            R.r28 = bitcast<float>(v6.x);
+            R.r29 = bitcast<float>(v6.y);
+            R.r30 = bitcast<float>(v6.z);
+            R.r31 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1288ull * cap)[idx];
+            R.r32 = bitcast<float>(v7.x);
+            R.r33 = bitcast<float>(v7.y);
+            R.r34 = bitcast<unsigned int>(v7.z);
+            R.r35 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 1304ull * cap)[idx];
+            R.r36 = bitcast<float>(v8.x);
+            R.r37 = bitcast<float>(v8.y);
+            R.r38 = bitcast<float>(v8.z);
+            R.r39 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 1320ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v9.x);
+            R.r41 = bitcast<unsigned int>(v9.y);
+            R.r42 = bitcast<float>(v9.z);
+            R.r43 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 1336ull * cap)[idx];
+            R.r44 = bitcast<unsigned int>(v10.x);
+            R.r45 = bitcast<float>(v10.y);
+            R.r46 = bitcast<float>(v10.z);
+            R.r47 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 1352ull * cap)[idx];
+            R.r48 = bitcast<unsigned int>(v11.x);
+            R.r49 = bitcast<unsigned int>(v11.y);
+            R.r50 = bitcast<float>(v11.z);
+            R.r61 = bitcast<unsigned int>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 1368ull * cap)[idx];
+            R.r62 = bitcast<float>(v12.x);
+            R.r63 = bitcast<float>(v12.y);
+            R.r64 = bitcast<float>(v12.z);
+            R.r65 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 1384ull * cap)[idx];
+            R.r66 = bitcast<float>(v13.x);
+            R.r67 = bitcast<float>(v13.y);
+            R.r68 = bitcast<unsigned int>(v13.z);
+            R.r69 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(base + 1400ull * cap)[idx];
+            R.r70 = bitcast<float>(v14.x);
+            R.r71 = bitcast<float>(v14.y);
+            return v14.z;
+        }
         case 8: // isect_quad_l3
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1416ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1420ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1424ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1428ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1432ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1436ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1440ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 1444ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 1448ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 1452ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1456ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1460ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1464ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1468ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1472ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 1476ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 1480ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 1484ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 1488ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1492ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 1496ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 1500ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 1504ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 1508ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1512ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1516ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1520ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1524ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1528ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 1532ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 1536ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 1540ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 1544ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1548ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1552ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1556ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1560ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 1564ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 1568ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1572ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 1576ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 1580ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 1584ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1588ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1592ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 1596ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1600ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1604ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 1608ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 1612ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 1616ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 1620ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 1624ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 1628ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 1632ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 1636ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 1640ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 1644ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1648ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1416ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1432ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1448ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1464ull * cap)[idx];
+            R.r13 = bitcast<float>(v3.x);
+            R.r14 = bitcast<unsigned int>(v3.y);
+            R.r15 = bitcast<float>(v3.z);
+            R.r16 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1480ull * cap)[idx];
+            R.r17 = bitcast<float>(v4.x);
+            R.r18 = bitcast<unsigned int>(v4.y);
+            R.r19 = bitcast<unsigned int>(v4.z);
+            R.r22 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1496ull * cap)[idx];
+            R.r23 = bitcast<float>(v5.x);
+            R.r24 = bitcast<float>(v5.y);
+            R.r25 = bitcast<float>(v5.z);
+            R.r26 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1512ull * cap)[idx];
+            R.r27 = bitcast<float>(v6.x);
+            R.r28 = bitcast<float>(v6.y);
+            R.r29 = bitcast<float>(v6.z);
+            R.r30 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1528ull * cap)[idx];
+            R.r31 = bitcast<float>(v7.x);
+            R.r32 = bitcast<float>(v7.y);
+            R.r33 = bitcast<float>(v7.z);
+            R.r34 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 1544ull * cap)[idx];
+            R.r35 = bitcast<float>(v8.x);
+            R.r36 = bitcast<float>(v8.y);
+            R.r37 = bitcast<float>(v8.z);
+            R.r38 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 1560ull * cap)[idx];
+            R.r39 = bitcast<float>(v9.x);
+            R.r40 = bitcast<unsigned int>(v9.y);
+            R.r41 = bitcast<unsigned int>(v9.z);
+            R.r42 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 1576ull * cap)[idx];
+            R.r43 = bitcast<unsigned int>(v10.x);
+            R.r44 = bitcast<unsigned int>(v10.y);
+            R.r45 = bitcast<float>(v10.z);
+            R.r46 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 1592ull * cap)[idx];
+            R.r47 = bitcast<float>(v11.x);
+            R.r48 = bitcast<unsigned int>(v11.y);
+            R.r49 = bitcast<unsigned int>(v11.z);
+            R.r50 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 1608ull * cap)[idx];
+            R.r62 = bitcast<float>(v12.x);
+            R.r63 = bitcast<float>(v12.y);
+            R.r64 = bitcast<float>(v12.z);
+            R.r65 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 1624ull * cap)[idx];
+            R.r66 = bitcast<float>(v13.x);
+            R.r67 = bitcast<float>(v13.y);
+            R.r68 = bitcast<unsigned int>(v13.z);
+            R.r69 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(base + 1640ull * cap)[idx];
+            R.r70 = bitcast<float>(v14.x);
+            R.r71 = bitcast<float>(v14.y);
+            return v14.z;
+        }
         case 9: // isect_quad_l4
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1656ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1660ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1664ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1668ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1672ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1676ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1680ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 1684ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1688ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1692ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1696ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1700ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1704ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 1708ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 1712ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 1716ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 1720ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1724ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 1728ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 1732ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 1736ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 1740ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1744ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1748ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1752ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1756ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1760ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 1764ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 1768ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 1772ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 1776ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 1780ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 1784ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 1788ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 1792ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 1796ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 1800ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1804ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 1808ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 1812ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 1816ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1820ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1824ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 1828ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 1832ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1836ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 1840ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 1844ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 1848ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 1852ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 1856ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 1860ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 1864ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 1868ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 1872ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 1876ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1880ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1656ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1672ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1688ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1704ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1720ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1736ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1752ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 1768ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 1784ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 1800ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 1816ull * cap)[idx];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 1832ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 1848ull * cap)[idx];
+            R.r64 = bitcast<float>(v12.x);
+            R.r65 = bitcast<float>(v12.y);
+            R.r66 = bitcast<float>(v12.z);
+            R.r67 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 1864ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v13.x);
+            R.r69 = bitcast<float>(v13.y);
+            R.r70 = bitcast<float>(v13.z);
+            R.r71 = bitcast<float>(v13.w);
+            const unsigned v14 = reinterpret_cast<const unsigned*>(base + 1880ull * cap)[idx];
+            return v14;
+        }
         case 10: // isect_quad_l5
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 1888ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 1892ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 1896ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1900ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 1904ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 1908ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 1912ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 1916ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1920ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 1924ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 1928ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 1932ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 1936ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 1940ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 1944ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 1948ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 1952ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 1956ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 1960ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 1964ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 1968ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 1972ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 1976ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 1980ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 1984ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 1988ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 1992ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 1996ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 2000ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 2004ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 2008ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2012ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 2016ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 2020ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 2024ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 2028ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 2032ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2036ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 2040ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 2044ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 2048ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2052ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2056ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 2060ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2064ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2068ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2072ull * cap)[idx];
-            R.r52 = reinterpret_cast<const float*>(base + 2076ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2080ull * cap)[idx];
-            R.r58 = reinterpret_cast<const float*>(base + 2084ull * cap)[idx];
-            R.r59 = reinterpret_cast<const float*>(base + 2088ull * cap)[idx];
-            R.r60 = reinterpret_cast<const float*>(base + 2092ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 2096ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 2100ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 2104ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 2108ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 2112ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 2116ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 2120ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 2124ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 2128ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 2132ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 2136ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2140ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1888ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1904ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1920ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1936ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1952ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1968ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1984ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2000ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2016ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2032ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2048ull * cap)[idx];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 2064ull * cap)[idx];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r51 = bitcast<float>(v11.z);
+            R.r52 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 2080ull * cap)[idx];
+            R.r53 = bitcast<unsigned int>(v12.x);
+            R.r58 = bitcast<float>(v12.y);
+            R.r59 = bitcast<float>(v12.z);
+            R.r60 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 2096ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v13.x);
+            R.r62 = bitcast<float>(v13.y);
+            R.r63 = bitcast<float>(v13.z);
+            R.r64 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(base + 2112ull * cap)[idx];
+            R.r65 = bitcast<float>(v14.x);
+            R.r66 = bitcast<float>(v14.y);
+            R.r67 = bitcast<float>(v14.z);
+            R.r68 = bitcast<unsigned int>(v14.w);
+            const uint4 v15 = reinterpret_cast<const uint4*>(base + 2128ull * cap)[idx];
+            R.r69 = bitcast<float>(v15.x);
+            R.r70 = bitcast<float>(v15.y);
+            R.r71 = bitcast<float>(v15.z);
+            return v15.w;
+        }
         case 11: // isect_quad_l6
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2144ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2148ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2152ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2156ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2160ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2164ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2168ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 2172ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2176ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2180ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2184ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 2188ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2192ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2196ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2200ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 2204ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 2208ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2212ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 2216ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 2220ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 2224ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 2228ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2232ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 2236ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2240ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 2244ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2248ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 2252ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 2256ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 2260ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 2264ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2268ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 2272ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 2276ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 2280ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 2284ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 2288ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2292ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 2296ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 2300ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 2304ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2308ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2312ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2316ull * cap)[idx];
-            R.r52 = reinterpret_cast<const float*>(base + 2320ull * cap)[idx];
-            R.r53 = reinterpret_cast<const unsigned int*>(base + 2324ull * cap)[idx];
-            R.r54 = reinterpret_cast<const float*>(base + 2328ull * cap)[idx];
-            R.r55 = reinterpret_cast<const float*>(base + 2332ull * cap)[idx];
-            R.r56 = reinterpret_cast<const float*>(base + 2336ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 2340ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 2344ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 2348ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 2352ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 2356ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 2360ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 2364ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 2368ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 2372ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 2376ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 2380ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2384ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2144ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2160ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2176ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2192ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2208ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2224ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2240ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2256ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2272ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2288ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2304ull * cap)[idx];
+            R.r48 = bitcast<unsigned int>(v10.x);
+            R.r49 = bitcast<unsigned int>(v10.y);
+            R.r50 = bitcast<float>(v10.z);
+            R.r51 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 2320ull * cap)[idx];
+            R.r52 = bitcast<float>(v11.x);
+            R.r53 = bitcast<unsigned int>(v11.y);
+            R.r54 = bitcast<float>(v11.z);
+            R.r55 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 2336ull * cap)[idx];
+            R.r56 = bitcast<float>(v12.x);
+            R.r61 = bitcast<unsigned int>(v12.y);
+            R.r62 = bitcast<float>(v12.z);
+            R.r63 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 2352ull * cap)[idx];
+            R.r64 = bitcast<float>(v13.x);
+            R.r65 = bitcast<float>(v13.y);
+            R.r66 = bitcast<float>(v13.z);
+            R.r67 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(base + 2368ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v14.x);
+            R.r69 = bitcast<float>(v14.y);
+            R.r70 = bitcast<float>(v14.z);
+            R.r71 = bitcast<float>(v14.w);
+            const unsigned v15 = reinterpret_cast<const unsigned*>(base + 2384ull * cap)[idx];
+            return v15;
+        }
         case 12: // isect_quad_l7
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2392ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2396ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2400ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2404ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2408ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2412ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2416ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 2420ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2424ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2428ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2432ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 2436ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2440ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2444ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2448ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 2452ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 2456ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2460ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 2464ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 2468ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 2472ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 2476ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2480ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 2484ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2488ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 2492ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2496ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 2500ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 2504ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 2508ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 2512ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 2516ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 2520ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 2524ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 2528ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 2532ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 2536ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2540ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 2544ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 2548ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 2552ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 2556ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2560ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 2564ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 2568ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 2572ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 2576ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 2580ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 2584ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 2588ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 2592ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 2596ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 2600ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2604ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2392ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2408ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2424ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2440ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2456ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2472ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2488ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2504ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2520ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2536ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2552ull * cap)[idx];
+            R.r48 = bitcast<unsigned int>(v10.x);
+            R.r49 = bitcast<unsigned int>(v10.y);
+            R.r50 = bitcast<float>(v10.z);
+            R.r62 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 2568ull * cap)[idx];
+            R.r63 = bitcast<float>(v11.x);
+            R.r64 = bitcast<float>(v11.y);
+            R.r65 = bitcast<float>(v11.z);
+            R.r66 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 2584ull * cap)[idx];
+            R.r67 = bitcast<float>(v12.x);
+            R.r68 = bitcast<unsigned int>(v12.y);
+            R.r69 = bitcast<float>(v12.z);
+            R.r70 = bitcast<float>(v12.w);
+            const uint2 v13 = reinterpret_cast<const uint2*>(base + 2600ull * cap)[idx];
+            R.r71 = bitcast<float>(v13.x);
+            return v13.y;
+        }
         case 13: // isect_quad_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2608ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2612ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2616ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2620ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2624ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2628ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2632ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 2636ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2640ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2644ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2648ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2652ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2656ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2660ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 2664ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 2668ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2672ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 2676ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 2680ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 2684ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 2688ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2692ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 2696ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2700ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 2704ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2708ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 2712ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 2716ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 2720ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 2724ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 2728ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 2732ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 2736ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 2740ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 2744ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 2748ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 2752ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 2756ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 2760ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 2764ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 2768ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 2772ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 2776ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 2780ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 2784ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2788ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2608ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2624ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2640ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2656ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2672ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2688ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2704ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2720ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2736ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2752ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2768ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 2784ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 14: // traverse_tetrahedron
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2792ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2796ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2800ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2804ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2808ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2812ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2816ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 2820ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2824ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 2828ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 2832ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2836ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2840ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2844ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 2848ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 2852ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 2856ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 2860ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 2864ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 2868ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 2872ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 2876ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 2880ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 2884ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 2888ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 2892ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 2896ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 2900ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 2904ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 2908ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 2912ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 2916ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 2920ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 2924ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 2928ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 2932ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 2936ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 2940ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 2944ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 2948ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 2952ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 2956ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 2960ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2964ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2792ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2808ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2824ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2840ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2856ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2872ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2888ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2904ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2920ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2936ull * cap)[idx];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2952ull * cap)[idx];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
         case 15: // isect_triangle_mid1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 2968ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 2972ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 2976ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2980ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 2984ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 2988ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2992ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 2996ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 3000ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3004ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3008ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3012ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 3016ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 3020ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 3024ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 3028ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3032ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 3036ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 3040ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 3044ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 3048ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3052ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3056ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3060ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3064ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3068ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 3072ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 3076ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 3080ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 3084ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 3088ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 3092ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 3096ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 3100ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 3104ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 3108ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 3112ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 3116ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 3120ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 3124ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 3128ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 3132ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 3136ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 3140ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 3144ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 3148ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 3152ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 3156ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 3160ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 3164ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 3168ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 3172ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 3176ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 3180ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 3184ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 3188ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3192ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2968ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2984ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3000ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3016ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3032ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3048ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3064ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 3080ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 3096ull * cap)[idx];
+            R.r38 = bitcast<float>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 3112ull * cap)[idx];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<unsigned int>(v9.y);
+            R.r44 = bitcast<unsigned int>(v9.z);
+            R.r45 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 3128ull * cap)[idx];
+            R.r46 = bitcast<float>(v10.x);
+            R.r47 = bitcast<float>(v10.y);
+            R.r48 = bitcast<unsigned int>(v10.z);
+            R.r49 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 3144ull * cap)[idx];
+            R.r50 = bitcast<float>(v11.x);
+            R.r61 = bitcast<unsigned int>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 3160ull * cap)[idx];
+            R.r64 = bitcast<float>(v12.x);
+            R.r65 = bitcast<float>(v12.y);
+            R.r66 = bitcast<float>(v12.z);
+            R.r67 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 3176ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v13.x);
+            R.r69 = bitcast<float>(v13.y);
+            R.r70 = bitcast<float>(v13.z);
+            R.r71 = bitcast<float>(v13.w);
+            const unsigned v14 = reinterpret_cast<const unsigned*>(base + 3192ull * cap)[idx];
+            return v14;
+        }
         case 16: // isect_triangle_mid2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3200ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3204ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3208ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3212ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3216ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3220ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3224ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 3228ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 3232ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3236ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3240ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 3244ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3248ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 3252ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 3256ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 3260ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 3264ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3268ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 3272ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 3276ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 3280ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 3284ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3288ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3292ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3296ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3300ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3304ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 3308ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 3312ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 3316ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 3320ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 3324ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 3328ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 3332ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 3336ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 3340ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 3344ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 3348ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 3352ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 3356ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 3360ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 3364ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 3368ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 3372ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 3376ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 3380ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 3384ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 3388ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 3392ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 3396ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 3400ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 3404ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 3408ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 3412ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3416ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3200ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3216ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3232ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3248ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3264ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3280ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3296ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 3312ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 3328ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 3344ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 3360ull * cap)[idx];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r61 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 3376ull * cap)[idx];
+            R.r62 = bitcast<float>(v11.x);
+            R.r63 = bitcast<float>(v11.y);
+            R.r64 = bitcast<float>(v11.z);
+            R.r65 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 3392ull * cap)[idx];
+            R.r66 = bitcast<float>(v12.x);
+            R.r67 = bitcast<float>(v12.y);
+            R.r68 = bitcast<unsigned int>(v12.z);
+            R.r69 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 3408ull * cap)[idx];
+            R.r70 = bitcast<float>(v13.x);
+            R.r71 = bitcast<float>(v13.y);
+            return v13.z;
+        }
         case 17: // isect_triangle_mid3
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3424ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3428ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3432ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3436ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3440ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3444ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3448ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 3452ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 3456ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3460ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3464ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3468ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 3472ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 3476ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 3480ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 3484ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3488ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 3492ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 3496ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 3500ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 3504ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3508ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3512ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3516ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3520ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3524ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 3528ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 3532ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 3536ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 3540ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 3544ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 3548ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 3552ull * cap)[idx];
-            R.r45 = reinterpret_cast<const float*>(base + 3556ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 3560ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 3564ull * cap)[idx];
-            R.r48 = reinterpret_cast<const unsigned int*>(base + 3568ull * cap)[idx];
-            R.r49 = reinterpret_cast<const unsigned int*>(base + 3572ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 3576ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 3580ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 3584ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 3588ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 3592ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 3596ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 3600ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 3604ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 3608ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 3612ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 3616ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 3620ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3624ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3424ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3440ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3456ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3472ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3488ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3504ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3520ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 3536ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 3552ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r45 = bitcast<float>(v8.y);
+            R.r46 = bitcast<float>(v8.z);
+            R.r47 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 3568ull * cap)[idx];
+            R.r48 = bitcast<unsigned int>(v9.x);
+            R.r49 = bitcast<unsigned int>(v9.y);
+            R.r50 = bitcast<float>(v9.z);
+            R.r61 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 3584ull * cap)[idx];
+            R.r62 = bitcast<float>(v10.x);
+            R.r63 = bitcast<float>(v10.y);
+            R.r64 = bitcast<float>(v10.z);
+            R.r65 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 3600ull * cap)[idx];
+            R.r66 = bitcast<float>(v11.x);
+            R.r67 = bitcast<float>(v11.y);
+            R.r68 = bitcast<unsigned int>(v11.z);
+            R.r69 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 3616ull * cap)[idx];
+            R.r70 = bitcast<float>(v12.x);
+            R.r71 = bitcast<float>(v12.y);
+            return v12.z;
+        }
         case 18: // isect_triangle_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3632ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3636ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3640ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3644ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3648ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3652ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3656ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 3660ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 3664ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3668ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3672ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3676ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 3680ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 3684ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 3688ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 3692ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3696ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 3700ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 3704ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 3708ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 3712ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3716ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3720ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3724ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3728ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3732ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 3736ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 3740ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 3744ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 3748ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 3752ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 3756ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 3760ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 3764ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 3768ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 3772ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 3776ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 3780ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 3784ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 3788ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 3792ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 3796ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 3800ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 3804ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 3808ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3812ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3632ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3648ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3664ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3680ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3696ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3712ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3728ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 3744ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 3760ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 3776ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 3792ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 3808ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 19: // traverse_sphere
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3816ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3820ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 3824ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 3828ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 3832ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 3836ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 3840ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 3844ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 3848ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 3852ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 3856ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 3860ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 3864ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 3868ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 3872ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 3876ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 3880ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 3884ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 3888ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 3892ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 3896ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 3900ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 3904ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 3908ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 3912ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 3916ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 3920ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 3924ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 3928ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 3932ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 3936ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 3940ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 3944ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 3948ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 3952ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 3956ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 3960ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 3964ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 3968ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 3972ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 3976ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 3980ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 3984ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 3988ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3816ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 3832ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 3848ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 3864ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 3880ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 3896ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 3912ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 3928ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 3944ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 3960ull * cap)[idx];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 3976ull * cap)[idx];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
         case 20: // traverse_solve_quadratic
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 3992ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 3996ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4000ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4004ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4008ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4012ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 4016ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 4020ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 4024ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 4028ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 4032ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 4036ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 4040ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 4044ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 4048ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 4052ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 4056ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 4060ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 4064ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 4068ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 4072ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 4076ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 4080ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 4084ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 4088ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 4092ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 4096ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 4100ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 4104ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 4108ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 4112ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 4116ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 4120ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 4124ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 4128ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 4132ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 4136ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 4140ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 4144ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 4148ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 4152ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 4156ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 4160ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 4164ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 4168ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 4172ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 4176ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 4180ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4184ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 3992ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4008ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 4024ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 4040ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 4056ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 4072ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 4088ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 4104ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 4120ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            R.r43 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 4136ull * cap)[idx];
+            R.r44 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 4152ull * cap)[idx];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 4168ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(base + 4184ull * cap)[idx];
+            return v12;
+        }
         case 21: // sq_head1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 4192ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 4196ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4200ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4204ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4208ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4212ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 4216ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 4220ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 4224ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 4228ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 4232ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 4236ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 4240ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 4244ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 4248ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 4252ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 4256ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 4260ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 4264ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 4268ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 4272ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 4276ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 4280ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 4284ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 4288ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 4292ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 4296ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 4300ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 4304ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 4308ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 4312ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 4316ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 4320ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 4324ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 4328ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 4332ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 4336ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 4340ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 4344ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 4348ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 4352ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 4356ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 4360ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 4364ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 4368ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 4372ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 4376ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4380ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 4192ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4208ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 4224ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 4240ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 4256ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 4272ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 4288ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 4304ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 4320ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r43 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 4336ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 4352ull * cap)[idx];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 4368ull * cap)[idx];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
         case 22: // sq_head2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 4384ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 4388ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4392ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4396ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4400ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4404ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 4408ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 4412ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 4416ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 4420ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 4424ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 4428ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 4432ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 4436ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 4440ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 4444ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 4448ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 4452ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 4456ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 4460ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 4464ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 4468ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 4472ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 4476ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 4480ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 4484ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 4488ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 4492ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 4496ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 4500ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 4504ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 4508ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 4512ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 4516ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 4520ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 4524ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 4528ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 4532ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 4536ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 4540ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 4544ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 4548ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 4552ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 4556ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 4560ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 4564ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 4568ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4572ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 4384ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4400ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 4416ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 4432ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 4448ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 4464ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 4480ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 4496ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 4512ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r43 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 4528ull * cap)[idx];
+            R.r57 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 4544ull * cap)[idx];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 4560ull * cap)[idx];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
         case 23: // sq_mid1
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 4576ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 4580ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4584ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4588ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4592ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4596ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 4600ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 4604ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 4608ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 4612ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 4616ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 4620ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 4624ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 4628ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 4632ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 4636ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 4640ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 4644ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 4648ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 4652ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 4656ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 4660ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 4664ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 4668ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 4672ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 4676ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 4680ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 4684ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 4688ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 4692ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 4696ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 4700ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 4704ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 4708ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 4712ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 4716ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 4720ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 4724ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 4728ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 4732ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 4736ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 4740ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 4744ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 4748ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 4752ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 4756ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 4760ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 4764ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4768ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 4576ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4592ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 4608ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 4624ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 4640ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 4656ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 4672ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 4688ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 4704ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            R.r43 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 4720ull * cap)[idx];
+            R.r44 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 4736ull * cap)[idx];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 4752ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(base + 4768ull * cap)[idx];
+            return v12;
+        }
         case 24: // sq_mid2
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 4776ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 4780ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4784ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4788ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4792ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4796ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 4800ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 4804ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 4808ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 4812ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 4816ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 4820ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 4824ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 4828ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 4832ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 4836ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 4840ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 4844ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 4848ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 4852ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 4856ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 4860ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 4864ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 4868ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 4872ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 4876ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 4880ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 4884ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 4888ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 4892ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 4896ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 4900ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 4904ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 4908ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 4912ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 4916ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 4920ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 4924ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 4928ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 4932ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 4936ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 4940ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 4944ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 4948ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 4952ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 4956ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 4960ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 4964ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4968ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 4776ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4792ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 4808ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 4824ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 4840ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 4856ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 4872ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 4888ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 4904ull * cap)[idx];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r42 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 4920ull * cap)[idx];
+            R.r43 = bitcast<unsigned int>(v9.x);
+            R.r44 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 4936ull * cap)[idx];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 4952ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(base + 4968ull * cap)[idx];
+            return v12;
+        }
         case 25: // sq_mid
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 4976ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 4980ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 4984ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 4988ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 4992ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 4996ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5000ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5004ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5008ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5012ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5016ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 5020ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5024ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5028ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5032ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5036ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5040ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5044ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5048ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5052ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5056ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5060ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5064ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 5068ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 5072ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 5076ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 5080ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 5084ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 5088ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 5092ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 5096ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 5100ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 5104ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 5108ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 5112ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 5116ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 5120ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 5124ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 5128ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 5132ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 5136ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 5140ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 5144ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 5148ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 5152ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 5156ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 5160ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 5164ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 4976ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 4992ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5008ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5024ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5040ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5056ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 5072ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 5088ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 5104ull * cap)[idx];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 5120ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 5136ull * cap)[idx];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 5152ull * cap)[idx];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
         case 26: // sq_tail
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 5168ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 5172ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 5176ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 5180ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 5184ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 5188ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5192ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5196ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5200ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5204ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5208ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 5212ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5216ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5220ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5224ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5228ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5232ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5236ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5240ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5244ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5248ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5252ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5256ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 5260ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 5264ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 5268ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 5272ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 5276ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 5280ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 5284ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 5288ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 5292ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 5296ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 5300ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 5304ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 5308ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 5312ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 5316ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 5320ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 5324ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 5328ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 5332ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 5336ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 5340ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 5344ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 5348ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 5352ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 5168ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 5184ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5200ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5216ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5232ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5248ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 5264ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 5280ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 5296ull * cap)[idx];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 5312ull * cap)[idx];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 5328ull * cap)[idx];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 5344ull * cap)[idx];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
         case 27: // sq_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 5360ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 5364ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 5368ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 5372ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 5376ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 5380ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5384ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5388ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5392ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5396ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5400ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5404ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5408ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5412ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5416ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5420ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5424ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5428ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5432ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5436ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5440ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5444ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 5448ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 5452ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 5456ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 5460ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 5464ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 5468ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 5472ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 5476ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 5480ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 5484ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 5488ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 5492ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 5496ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 5500ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 5504ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 5508ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 5512ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 5516ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 5520ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 5524ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 5528ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 5532ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 5536ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 5540ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 5544ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 5360ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 5376ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5392ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5408ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5424ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5440ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 5456ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 5472ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 5488ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r57 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 5504ull * cap)[idx];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 5520ull * cap)[idx];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 5536ull * cap)[idx];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
         case 28: // traverse_sphere_fin
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 5552ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 5556ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 5560ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 5564ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 5568ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 5572ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5576ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5580ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5584ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5588ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5592ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5596ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5600ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5604ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5608ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5612ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5616ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5620ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5624ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5628ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5632ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5636ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 5640ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 5644ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 5648ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 5652ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 5656ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 5660ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 5664ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 5668ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 5672ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 5676ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 5680ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 5684ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 5688ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 5692ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 5696ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 5700ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 5704ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 5708ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 5712ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 5716ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 5720ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 5724ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 5728ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 5732ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 5552ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 5568ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5584ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5600ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5616ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5632ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 5648ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 5664ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 5680ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 5696ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 5712ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 5728ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 29: // traverse_cylinder
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 5736ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 5740ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 5744ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 5748ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 5752ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 5756ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5760ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5764ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5768ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5772ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5776ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5780ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5784ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5788ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5792ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5796ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5800ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5804ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5808ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5812ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5816ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5820ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 5824ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 5828ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 5832ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 5836ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 5840ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 5844ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 5848ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 5852ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 5856ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 5860ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 5864ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 5868ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 5872ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 5876ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 5880ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 5884ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 5888ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 5892ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 5896ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 5900ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 5904ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 5908ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 5736ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 5752ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5768ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5784ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5800ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5816ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 5832ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 5848ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 5864ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 5880ull * cap)[idx];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 5896ull * cap)[idx];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
         case 30: // traverse_cylinder_fin
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 5912ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 5916ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 5920ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 5924ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 5928ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 5932ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 5936ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 5940ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 5944ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 5948ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 5952ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 5956ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 5960ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 5964ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 5968ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 5972ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 5976ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 5980ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 5984ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 5988ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 5992ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 5996ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6000ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6004ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6008ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6012ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6016ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6020ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6024ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6028ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 6032ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6036ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6040ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 6044ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 6048ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 6052ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 6056ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 6060ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 6064ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 6068ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 6072ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 6076ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 6080ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 6084ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 6088ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 6092ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 6096ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 5912ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 5928ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 5944ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 5960ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 5976ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 5992ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6008ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6024ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 6040ull * cap)[idx];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r57 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 6056ull * cap)[idx];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 6072ull * cap)[idx];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 6088ull * cap)[idx];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
         case 31: // traverse_disk
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 6104ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 6108ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 6112ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 6116ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 6120ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 6124ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 6128ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 6132ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 6136ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 6140ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 6144ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 6148ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 6152ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 6156ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 6160ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 6164ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 6168ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 6172ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 6176ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 6180ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 6184ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 6188ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 6192ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6196ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6200ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6204ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6208ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6212ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6216ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6220ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6224ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 6228ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 6232ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 6236ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6240ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6244ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 6248ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 6252ull * cap)[idx];
-            R.r43 = reinterpret_cast<const unsigned int*>(base + 6256ull * cap)[idx];
-            R.r44 = reinterpret_cast<const unsigned int*>(base + 6260ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 6264ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 6268ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 6272ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 6276ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 6280ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 6284ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 6288ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 6292ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 6296ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 6300ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 6304ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 6104ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 6120ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 6136ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 6152ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 6168ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 6184ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6200ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6216ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 6232ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 6248ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 6264ull * cap)[idx];
+            R.r62 = bitcast<float>(v10.x);
+            R.r63 = bitcast<float>(v10.y);
+            R.r64 = bitcast<float>(v10.z);
+            R.r65 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 6280ull * cap)[idx];
+            R.r66 = bitcast<float>(v11.x);
+            R.r67 = bitcast<float>(v11.y);
+            R.r68 = bitcast<unsigned int>(v11.z);
+            R.r69 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 6296ull * cap)[idx];
+            R.r70 = bitcast<float>(v12.x);
+            R.r71 = bitcast<float>(v12.y);
+            return v12.z;
+        }
         case 32: // isect_disk_rest
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 6312ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 6316ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 6320ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 6324ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 6328ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 6332ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 6336ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 6340ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 6344ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 6348ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 6352ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 6356ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 6360ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 6364ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 6368ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 6372ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 6376ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 6380ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 6384ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 6388ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 6392ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 6396ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 6400ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6404ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6408ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6412ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6416ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6420ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6424ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6428ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6432ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 6436ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 6440ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 6444ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6448ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6452ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 6456ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 6460ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 6464ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 6468ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 6472ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 6476ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 6480ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 6484ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 6488ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 6492ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 6496ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 6500ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 6504ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 6312ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 6328ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 6344ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 6360ull * cap)[idx];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 6376ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 6392ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6408ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6424ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 6440ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 6456ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 6472ull * cap)[idx];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 6488ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(base + 6504ull * cap)[idx];
+            return v12;
+        }
         case 33: // isect_disk_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 6512ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 6516ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 6520ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 6524ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 6528ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 6532ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 6536ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 6540ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 6544ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 6548ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 6552ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 6556ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 6560ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 6564ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 6568ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 6572ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 6576ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 6580ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 6584ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 6588ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 6592ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 6596ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6600ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6604ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6608ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6612ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6616ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6620ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6624ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6628ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6632ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6636ull * cap)[idx];
-            R.r41 = reinterpret_cast<const unsigned int*>(base + 6640ull * cap)[idx];
-            R.r57 = reinterpret_cast<const unsigned int*>(base + 6644ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 6648ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 6652ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 6656ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 6660ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 6664ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 6668ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 6672ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 6676ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 6680ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 6684ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 6688ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 6692ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 6512ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 6528ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 6544ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 6560ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 6576ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 6592ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6608ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6624ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 6640ull * cap)[idx];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 6656ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 6672ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 6688ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 34: // traverse_room_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 6696ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 6700ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 6704ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 6708ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 6712ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 6716ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 6720ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 6724ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 6728ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 6732ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 6736ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 6740ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 6744ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 6748ull * cap)[idx];
-            R.r18 = reinterpret_cast<const unsigned int*>(base + 6752ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 6756ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 6760ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 6764ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 6768ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 6772ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 6776ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 6780ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6784ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6788ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6792ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6796ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6800ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6804ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6808ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6812ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6816ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6820ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 6824ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 6828ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 6832ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 6836ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 6840ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 6844ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 6848ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 6852ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 6856ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 6860ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 6864ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 6868ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 6696ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 6712ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 6728ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 6744ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 6760ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 6776ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6792ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6808ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 6824ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 6840ull * cap)[idx];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 6856ull * cap)[idx];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
         case 35: // radiance
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 6872ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 6876ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 6880ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 6884ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 6888ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 6892ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 6896ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 6900ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 6904ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 6908ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 6912ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 6916ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 6920ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 6924ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 6928ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 6932ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 6936ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 6940ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 6944ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 6948ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 6952ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 6956ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 6960ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 6964ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 6968ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 6972ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 6976ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 6980ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 6984ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 6988ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 6992ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 6996ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7000ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7004ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7008ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 7012ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 7016ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 7020ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 7024ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7028ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7032ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7036ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7040ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 6872ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 6888ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 6904ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 6920ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 6936ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 6952ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 6968ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 6984ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<unsigned int>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7000ull * cap)[idx];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 7016ull * cap)[idx];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 7032ull * cap)[idx];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
         case 36: // set_materials
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7048ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7052ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7056ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7060ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7064ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7068ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7072ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7076ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7080ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7084ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7088ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7092ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7096ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7100ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7104ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7108ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7112ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7116ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7120ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7124ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7128ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7132ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7136ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7140ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7144ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7148ull * cap)[idx];
-            R.r39 = reinterpret_cast<const float*>(base + 7152ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7156ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7160ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7164ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7168ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7172ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7176ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7048ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7064ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7080ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7096ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7112ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7128ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7144ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v6.x);
+            R.r35 = bitcast<float>(v6.y);
+            R.r39 = bitcast<float>(v6.z);
+            R.r40 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7160ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v7.x);
+            R.r69 = bitcast<float>(v7.y);
+            R.r70 = bitcast<float>(v7.z);
+            R.r71 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(base + 7176ull * cap)[idx];
+            return v8;
+        }
         case 37: // set_polygon_normal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7184ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7188ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7192ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7196ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7200ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7204ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7208ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7212ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7216ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7220ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7224ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7228ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7232ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7236ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7240ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7244ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7248ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7252ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7256ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7260ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7264ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7268ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7272ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7276ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 7280ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 7284ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 7288ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7292ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7296ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7300ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7304ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7308ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7312ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7316ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7320ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7324ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7328ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7332ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7184ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7200ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7216ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7232ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7248ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7264ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7280ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7296ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7312ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 7328ull * cap)[idx];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
         case 38: // set_disk_normal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7336ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7340ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7344ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7348ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7352ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7356ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7360ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7364ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7368ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7372ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7376ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7380ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7384ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7388ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7392ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7396ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7400ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7404ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7408ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7412ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7416ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7420ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7424ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7428ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 7432ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 7436ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 7440ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7444ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7448ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7452ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7456ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7460ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7464ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7468ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7472ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7476ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7480ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7484ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7336ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7352ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7368ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7384ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7400ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7416ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7432ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7448ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7464ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 7480ull * cap)[idx];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
         case 39: // compute_sphere_normal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7488ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7492ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7496ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7500ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7504ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7508ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7512ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7516ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7520ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7524ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7528ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7532ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7536ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7540ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7544ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7548ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7552ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7556ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7560ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7564ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7568ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7572ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7576ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7580ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 7584ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 7588ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 7592ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7596ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7600ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7604ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7608ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7612ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7616ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7620ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7624ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7628ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7632ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7636ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7488ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7504ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7520ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7536ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7552ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7568ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7584ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7600ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7616ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 7632ull * cap)[idx];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
         case 40: // compute_cylinder_normal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7640ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7644ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7648ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7652ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7656ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7660ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7664ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7668ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7672ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7676ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7680ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7684ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7688ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7692ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7696ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7700ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7704ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7708ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7712ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7716ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7720ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7724ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7728ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7732ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 7736ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 7740ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 7744ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7748ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7752ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7756ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7760ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7764ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7768ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7772ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7776ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7780ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7784ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7788ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7640ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7656ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7672ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7688ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7704ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7720ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7736ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7752ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7768ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(base + 7784ull * cap)[idx];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
         case 41: // set_materials_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7792ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7796ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7800ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7804ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7808ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7812ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7816ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7820ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7824ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7828ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 7832ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 7836ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 7840ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 7844ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 7848ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 7852ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 7856ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 7860ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 7864ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 7868ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 7872ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 7876ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 7880ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 7884ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 7888ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 7892ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 7896ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 7900ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 7904ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 7908ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 7912ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 7916ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 7920ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 7924ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 7928ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 7932ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 7936ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 7940ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 7944ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 7948ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 7952ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7792ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7808ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7824ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 7840ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 7856ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 7872ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 7888ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 7904ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 7920ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 7936ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r69 = bitcast<float>(v9.y);
+            R.r70 = bitcast<float>(v9.z);
+            R.r71 = bitcast<float>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(base + 7952ull * cap)[idx];
+            return v10;
+        }
         case 42: // test_direct
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 7960ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 7964ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 7968ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 7972ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 7976ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 7980ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 7984ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 7988ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 7992ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 7996ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8000ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8004ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8008ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8012ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8016ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 8020ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8024ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8028ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8032ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8036ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8040ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8044ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8048ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8052ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8056ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8060ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8064ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8068ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8072ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 8076ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8080ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 8084ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 8088ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 8092ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8096ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8100ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8104ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8108ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 8112ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 8116ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 8120ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8124ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 7960ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 7976ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 7992ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8008ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8024ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8040ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8056ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8072ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8088ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 8104ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(base + 8120ull * cap)[idx];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
         case 43: // direct
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8128ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8132ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8136ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8140ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8144ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 8148ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 8152ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8156ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8160ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8164ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8168ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8172ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8176ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8180ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8184ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 8188ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 8192ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8196ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8200ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8204ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8208ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8212ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8216ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8220ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8224ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8228ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8232ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8236ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8240ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8244ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 8248ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8252ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 8256ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 8260ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 8264ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8268ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8272ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8276ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8280ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8284ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8128ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8144ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8160ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8176ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8192ull * cap)[idx];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8208ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8224ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8240ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8256ull * cap)[idx];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 8272ull * cap)[idx];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            return v9.w;
+        }
         case 44: // direct_pdf
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8288ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8292ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8296ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8300ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8304ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 8308ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 8312ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8316ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8320ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8324ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8328ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8332ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8336ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8340ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8344ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8348ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8352ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8356ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8360ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8364ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8368ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8372ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8376ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8380ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8384ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8388ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8392ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8396ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 8400ull * cap)[idx];
-            R.r40 = reinterpret_cast<const unsigned int*>(base + 8404ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8408ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 8412ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 8416ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 8420ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8424ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8428ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8432ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8436ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 8440ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 8444ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 8448ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8452ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8288ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8304ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8320ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8336ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8352ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8368ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8384ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8400ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8416ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 8432ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(base + 8448ull * cap)[idx];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
         case 45: // direct_metal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8456ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8460ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8464ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8468ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8472ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 8476ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 8480ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 8484ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 8488ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8492ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8496ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8500ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8504ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8508ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8512ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8516ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8520ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8524ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8528ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8532ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8536ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8540ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8544ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8548ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8552ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8556ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8560ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8564ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8568ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8572ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 8576ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8580ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 8584ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 8588ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 8592ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8596ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8600ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8604ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8608ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 8612ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 8616ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 8620ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8624ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8456ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8472ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8488ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8504ull * cap)[idx];
+            R.r13 = bitcast<float>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8520ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8536ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8552ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8568ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8584ull * cap)[idx];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 8600ull * cap)[idx];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 8616ull * cap)[idx];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
         case 46: // window
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8632ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8636ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8640ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8644ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8648ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 8652ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 8656ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8660ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8664ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8668ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8672ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8676ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8680ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8684ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8688ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 8692ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 8696ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8700ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8704ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8708ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8712ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8716ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8720ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8724ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8728ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8732ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8736ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8740ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8744ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8748ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 8752ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8756ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 8760ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 8764ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 8768ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8772ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8776ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8780ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8784ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 8788ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 8792ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 8796ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8800ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8632ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8648ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8664ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8680ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8696ull * cap)[idx];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8712ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8728ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8744ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8760ull * cap)[idx];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 8776ull * cap)[idx];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 8792ull * cap)[idx];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
         case 47: // lambert_indirect
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8808ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8812ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8816ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8820ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8824ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8828ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8832ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8836ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 8840ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 8844ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 8848ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 8852ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 8856ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 8860ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 8864ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 8868ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 8872ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 8876ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 8880ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 8884ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 8888ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 8892ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 8896ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 8900ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 8904ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 8908ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 8912ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 8916ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 8920ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 8924ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 8928ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 8932ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 8936ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 8940ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 8944ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 8948ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8952ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8808ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8824ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r10 = bitcast<unsigned int>(v1.y);
+            R.r11 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8840ull * cap)[idx];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 8856ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<unsigned int>(v3.y);
+            R.r21 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 8872ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 8888ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 8904ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 8920ull * cap)[idx];
+            R.r61 = bitcast<unsigned int>(v7.x);
+            R.r65 = bitcast<float>(v7.y);
+            R.r66 = bitcast<float>(v7.z);
+            R.r67 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 8936ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v8.x);
+            R.r69 = bitcast<float>(v8.y);
+            R.r70 = bitcast<float>(v8.z);
+            R.r71 = bitcast<float>(v8.w);
+            const unsigned v9 = reinterpret_cast<const unsigned*>(base + 8952ull * cap)[idx];
+            return v9;
+        }
         case 48: // tth_begin
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 8960ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 8964ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 8968ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 8972ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 8976ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 8980ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 8984ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 8988ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 8992ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 8996ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9000ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9004ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9008ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9012ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9016ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 9020ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9024ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9028ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9032ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9036ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9040ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9044ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9048ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9052ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9056ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 9060ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 9064ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 9068ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9072ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9076ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9080ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9084ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9088ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9092ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9096ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9100ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9104ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9108ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9112ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9116ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9120ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9124ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 8960ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 8976ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 8992ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9008ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9024ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9040ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9056ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9072ull * cap)[idx];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9088ull * cap)[idx];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9104ull * cap)[idx];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(base + 9120ull * cap)[idx];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
         case 49: // glass
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 9128ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 9132ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 9136ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 9140ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 9144ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 9148ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 9152ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 9156ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 9160ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 9164ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9168ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9172ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9176ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9180ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9184ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 9188ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9192ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9196ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9200ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9204ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9208ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9212ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9216ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9220ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9224ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9228ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9232ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9236ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9240ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9244ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9248ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9252ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9256ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9260ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9264ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9268ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9272ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9276ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9280ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 9128ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 9144ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 9160ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9176ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9192ull * cap)[idx];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9208ull * cap)[idx];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9224ull * cap)[idx];
+            R.r30 = bitcast<float>(v6.x);
+            R.r34 = bitcast<unsigned int>(v6.y);
+            R.r35 = bitcast<float>(v6.z);
+            R.r61 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9240ull * cap)[idx];
+            R.r62 = bitcast<float>(v7.x);
+            R.r63 = bitcast<float>(v7.y);
+            R.r64 = bitcast<float>(v7.z);
+            R.r65 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9256ull * cap)[idx];
+            R.r66 = bitcast<float>(v8.x);
+            R.r67 = bitcast<float>(v8.y);
+            R.r68 = bitcast<unsigned int>(v8.z);
+            R.r69 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9272ull * cap)[idx];
+            R.r70 = bitcast<float>(v9.x);
+            R.r71 = bitcast<float>(v9.y);
+            return v9.z;
+        }
         case 50: // indirect_metal
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 9288ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 9292ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 9296ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 9300ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 9304ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 9308ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 9312ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 9316ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 9320ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 9324ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9328ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9332ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9336ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9340ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9344ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 9348ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 9352ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9356ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9360ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9364ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9368ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9372ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9376ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9380ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9384ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9388ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 9392ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 9396ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 9400ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9404ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9408ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9412ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9416ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9420ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9424ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9428ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9432ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9436ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9440ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9444ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9448ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9452ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9456ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 9288ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 9304ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 9320ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9336ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9352ull * cap)[idx];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9368ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9384ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9400ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9416ull * cap)[idx];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9432ull * cap)[idx];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 9448ull * cap)[idx];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
         case 51: // get_slope_mid
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 9464ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 9468ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 9472ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 9476ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 9480ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 9484ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 9488ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 9492ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 9496ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 9500ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9504ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9508ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9512ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9516ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9520ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 9524ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 9528ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9532ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9536ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9540ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9544ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9548ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9552ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9556ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9560ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9564ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 9568ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 9572ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 9576ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9580ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9584ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 9588ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 9592ull * cap)[idx];
-            R.r38 = reinterpret_cast<const float*>(base + 9596ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9600ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9604ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9608ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9612ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9616ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9620ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9624ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9628ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9632ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9636ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9640ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9644ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 9464ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 9480ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 9496ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9512ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9528ull * cap)[idx];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9544ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9560ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9576ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9592ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9608ull * cap)[idx];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 9624ull * cap)[idx];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(base + 9640ull * cap)[idx];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
         case 52: // get_slope_end
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 9648ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 9652ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 9656ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 9660ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 9664ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 9668ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 9672ull * cap)[idx];
-            R.r8 = reinterpret_cast<const unsigned int*>(base + 9676ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 9680ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 9684ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 9688ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9692ull * cap)[idx];
-            R.r14 = reinterpret_cast<const unsigned int*>(base + 9696ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9700ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9704ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9708ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9712ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9716ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9720ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9724ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9728ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9732ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9736ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9740ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9744ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9748ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 9752ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 9756ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 9760ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9764ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9768ull * cap)[idx];
-            R.r36 = reinterpret_cast<const float*>(base + 9772ull * cap)[idx];
-            R.r37 = reinterpret_cast<const float*>(base + 9776ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9780ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9784ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9788ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9792ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9796ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9800ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9804ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9808ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9812ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9816ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9820ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9824ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 9648ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 9664ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 9680ull * cap)[idx];
+            R.r10 = bitcast<unsigned int>(v2.x);
+            R.r11 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9696ull * cap)[idx];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9712ull * cap)[idx];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9728ull * cap)[idx];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9744ull * cap)[idx];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9760ull * cap)[idx];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9776ull * cap)[idx];
+            R.r37 = bitcast<float>(v8.x);
+            R.r61 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9792ull * cap)[idx];
+            R.r64 = bitcast<float>(v9.x);
+            R.r65 = bitcast<float>(v9.y);
+            R.r66 = bitcast<float>(v9.z);
+            R.r67 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 9808ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v10.x);
+            R.r69 = bitcast<float>(v10.y);
+            R.r70 = bitcast<float>(v10.z);
+            R.r71 = bitcast<float>(v10.w);
+            const unsigned v11 = reinterpret_cast<const unsigned*>(base + 9824ull * cap)[idx];
+            return v11;
+        }
         case 53: // fin_sample
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 9832ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 9836ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 9840ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 9844ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 9848ull * cap)[idx];
-            R.r6 = reinterpret_cast<const unsigned int*>(base + 9852ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 9856ull * cap)[idx];
-            R.r10 = reinterpret_cast<const unsigned int*>(base + 9860ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 9864ull * cap)[idx];
-            R.r12 = reinterpret_cast<const float*>(base + 9868ull * cap)[idx];
-            R.r13 = reinterpret_cast<const float*>(base + 9872ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 9876ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 9880ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 9884ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 9888ull * cap)[idx];
-            R.r22 = reinterpret_cast<const float*>(base + 9892ull * cap)[idx];
-            R.r23 = reinterpret_cast<const float*>(base + 9896ull * cap)[idx];
-            R.r24 = reinterpret_cast<const float*>(base + 9900ull * cap)[idx];
-            R.r25 = reinterpret_cast<const float*>(base + 9904ull * cap)[idx];
-            R.r26 = reinterpret_cast<const float*>(base + 9908ull * cap)[idx];
-            R.r27 = reinterpret_cast<const float*>(base + 9912ull * cap)[idx];
-            R.r28 = reinterpret_cast<const float*>(base + 9916ull * cap)[idx];
-            R.r29 = reinterpret_cast<const float*>(base + 9920ull * cap)[idx];
-            R.r30 = reinterpret_cast<const float*>(base + 9924ull * cap)[idx];
-            R.r31 = reinterpret_cast<const float*>(base + 9928ull * cap)[idx];
-            R.r32 = reinterpret_cast<const float*>(base + 9932ull * cap)[idx];
-            R.r33 = reinterpret_cast<const float*>(base + 9936ull * cap)[idx];
-            R.r34 = reinterpret_cast<const unsigned int*>(base + 9940ull * cap)[idx];
-            R.r35 = reinterpret_cast<const float*>(base + 9944ull * cap)[idx];
-            R.r61 = reinterpret_cast<const unsigned int*>(base + 9948ull * cap)[idx];
-            R.r62 = reinterpret_cast<const float*>(base + 9952ull * cap)[idx];
-            R.r63 = reinterpret_cast<const float*>(base + 9956ull * cap)[idx];
-            R.r64 = reinterpret_cast<const float*>(base + 9960ull * cap)[idx];
-            R.r65 = reinterpret_cast<const float*>(base + 9964ull * cap)[idx];
-            R.r66 = reinterpret_cast<const float*>(base + 9968ull * cap)[idx];
-            R.r67 = reinterpret_cast<const float*>(base + 9972ull * cap)[idx];
-            R.r68 = reinterpret_cast<const unsigned int*>(base + 9976ull * cap)[idx];
-            R.r69 = reinterpret_cast<const float*>(base + 9980ull * cap)[idx];
-            R.r70 = reinterpret_cast<const float*>(base + 9984ull * cap)[idx];
-            R.r71 = reinterpret_cast<const float*>(base + 9988ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 9992ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 9832ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 9848ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 9864ull * cap)[idx];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 9880ull * cap)[idx];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 9896ull * cap)[idx];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 9912ull * cap)[idx];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 9928ull * cap)[idx];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 9944ull * cap)[idx];
+            R.r35 = bitcast<float>(v7.x);
+            R.r61 = bitcast<unsigned int>(v7.y);
+            R.r62 = bitcast<float>(v7.z);
+            R.r63 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 9960ull * cap)[idx];
+            R.r64 = bitcast<float>(v8.x);
+            R.r65 = bitcast<float>(v8.y);
+            R.r66 = bitcast<float>(v8.z);
+            R.r67 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 9976ull * cap)[idx];
+            R.r68 = bitcast<unsigned int>(v9.x);
+            R.r69 = bitcast<float>(v9.y);
+            R.r70 = bitcast<float>(v9.z);
+            R.r71 = bitcast<float>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(base + 9992ull * cap)[idx];
+            return v10;
+        }
         case 54: // fin_pixel
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 10000ull * cap)[idx];
-            R.r2 = reinterpret_cast<const float*>(base + 10004ull * cap)[idx];
-            R.r3 = reinterpret_cast<const float*>(base + 10008ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 10012ull * cap)[idx];
-            R.r5 = reinterpret_cast<const unsigned int*>(base + 10016ull * cap)[idx];
-            R.r19 = reinterpret_cast<const unsigned int*>(base + 10020ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 10024ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 10000ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 10016ull * cap)[idx];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r19 = bitcast<unsigned int>(v1.y);
+            return v1.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -7131,223 +10561,333 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {1u, 14u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes0[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames0[] = {"ppp", "tmp0", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs0[] = {0ull, 4ull, 8ull, 12ull, 16ull, 20ull, 24ull, 28ull, 32ull, 36ull, 40ull, 44ull, 48ull, 52ull, 56ull, 60ull, 64ull, 68ull, 72ull, 76ull, 80ull, 84ull, 88ull, 92ull, 96ull, 100ull, 104ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull, 0ull, 0ull, 16ull, 16ull, 16ull, 16ull, 32ull, 32ull, 32ull, 32ull, 48ull, 48ull, 48ull, 48ull, 64ull, 64ull, 64ull, 64ull, 80ull, 80ull, 80ull, 80ull, 96ull, 96ull, 96ull};
+const unsigned kQSubs0[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths0[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs1[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes1[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames1[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs1[] = {112ull, 116ull, 120ull, 124ull, 128ull, 132ull, 136ull, 140ull, 144ull, 148ull, 152ull, 156ull, 160ull, 164ull, 168ull, 172ull, 176ull, 180ull, 184ull, 188ull, 192ull, 196ull, 200ull, 204ull, 208ull, 212ull, 216ull, 220ull, 224ull, 228ull, 232ull, 236ull, 240ull, 244ull, 248ull, 252ull, 256ull, 260ull, 264ull, 268ull, 272ull};
+const unsigned long long kQOffs1[] = {112ull, 112ull, 112ull, 112ull, 128ull, 128ull, 128ull, 128ull, 144ull, 144ull, 144ull, 144ull, 160ull, 160ull, 160ull, 160ull, 176ull, 176ull, 176ull, 176ull, 192ull, 192ull, 192ull, 192ull, 208ull, 208ull, 208ull, 208ull, 224ull, 224ull, 224ull, 224ull, 240ull, 240ull, 240ull, 240ull, 256ull, 256ull, 256ull, 256ull, 272ull};
+const unsigned kQSubs1[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths1[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs2[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes2[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames2[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "tmp1", "tmp2", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs2[] = {280ull, 284ull, 288ull, 292ull, 296ull, 300ull, 304ull, 308ull, 312ull, 316ull, 320ull, 324ull, 328ull, 332ull, 336ull, 340ull, 344ull, 348ull, 352ull, 356ull, 360ull, 364ull, 368ull, 372ull, 376ull, 380ull, 384ull, 388ull, 392ull, 396ull, 400ull, 404ull, 408ull, 412ull, 416ull, 420ull, 424ull, 428ull, 432ull, 436ull, 440ull, 444ull, 448ull, 452ull, 456ull};
+const unsigned long long kQOffs2[] = {280ull, 280ull, 280ull, 280ull, 296ull, 296ull, 296ull, 296ull, 312ull, 312ull, 312ull, 312ull, 328ull, 328ull, 328ull, 328ull, 344ull, 344ull, 344ull, 344ull, 360ull, 360ull, 360ull, 360ull, 376ull, 376ull, 376ull, 376ull, 392ull, 392ull, 392ull, 392ull, 408ull, 408ull, 408ull, 408ull, 424ull, 424ull, 424ull, 424ull, 440ull, 440ull, 440ull, 440ull, 456ull};
+const unsigned kQSubs2[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths2[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs3[] = {1u, 2u, 3u, 4u, 5u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 20u, 21u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes3[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames3[] = {"ppp", "L0", "L1", "L2", "rc", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "u0", "u1", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs3[] = {464ull, 468ull, 472ull, 476ull, 480ull, 484ull, 488ull, 492ull, 496ull, 500ull, 504ull, 508ull, 512ull, 516ull, 520ull, 524ull, 528ull, 532ull, 536ull, 540ull, 544ull, 548ull, 552ull, 556ull, 560ull, 564ull, 568ull};
+const unsigned long long kQOffs3[] = {464ull, 464ull, 464ull, 464ull, 480ull, 480ull, 480ull, 480ull, 496ull, 496ull, 496ull, 496ull, 512ull, 512ull, 512ull, 512ull, 528ull, 528ull, 528ull, 528ull, 544ull, 544ull, 544ull, 544ull, 560ull, 560ull, 560ull};
+const unsigned kQSubs3[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths3[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs4[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes4[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames4[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs4[] = {576ull, 580ull, 584ull, 588ull, 592ull, 596ull, 600ull, 604ull, 608ull, 612ull, 616ull, 620ull, 624ull, 628ull, 632ull, 636ull, 640ull, 644ull, 648ull, 652ull, 656ull, 660ull, 664ull, 668ull, 672ull, 676ull, 680ull, 684ull, 688ull, 692ull, 696ull, 700ull, 704ull, 708ull, 712ull, 716ull, 720ull, 724ull, 728ull, 732ull, 736ull};
+const unsigned long long kQOffs4[] = {576ull, 576ull, 576ull, 576ull, 592ull, 592ull, 592ull, 592ull, 608ull, 608ull, 608ull, 608ull, 624ull, 624ull, 624ull, 624ull, 640ull, 640ull, 640ull, 640ull, 656ull, 656ull, 656ull, 656ull, 672ull, 672ull, 672ull, 672ull, 688ull, 688ull, 688ull, 688ull, 704ull, 704ull, 704ull, 704ull, 720ull, 720ull, 720ull, 720ull, 736ull};
+const unsigned kQSubs4[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths4[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs5[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes5[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames5[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs5[] = {744ull, 748ull, 752ull, 756ull, 760ull, 764ull, 768ull, 772ull, 776ull, 780ull, 784ull, 788ull, 792ull, 796ull, 800ull, 804ull, 808ull, 812ull, 816ull, 820ull, 824ull, 828ull, 832ull, 836ull, 840ull, 844ull, 848ull, 852ull, 856ull, 860ull, 864ull, 868ull, 872ull, 876ull, 880ull, 884ull, 888ull, 892ull, 896ull, 900ull, 904ull, 908ull, 912ull, 916ull};
+const unsigned long long kQOffs5[] = {744ull, 744ull, 744ull, 744ull, 760ull, 760ull, 760ull, 760ull, 776ull, 776ull, 776ull, 776ull, 792ull, 792ull, 792ull, 792ull, 808ull, 808ull, 808ull, 808ull, 824ull, 824ull, 824ull, 824ull, 840ull, 840ull, 840ull, 840ull, 856ull, 856ull, 856ull, 856ull, 872ull, 872ull, 872ull, 872ull, 888ull, 888ull, 888ull, 888ull, 904ull, 904ull, 904ull, 904ull};
+const unsigned kQSubs5[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths5[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs6[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 58u, 59u, 60u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes6[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames6[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "vr60", "vr61", "vr62", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs6[] = {928ull, 932ull, 936ull, 940ull, 944ull, 948ull, 952ull, 956ull, 960ull, 964ull, 968ull, 972ull, 976ull, 980ull, 984ull, 988ull, 992ull, 996ull, 1000ull, 1004ull, 1008ull, 1012ull, 1016ull, 1020ull, 1024ull, 1028ull, 1032ull, 1036ull, 1040ull, 1044ull, 1048ull, 1052ull, 1056ull, 1060ull, 1064ull, 1068ull, 1072ull, 1076ull, 1080ull, 1084ull, 1088ull, 1092ull, 1096ull, 1100ull, 1104ull, 1108ull, 1112ull, 1116ull, 1120ull, 1124ull, 1128ull, 1132ull, 1136ull, 1140ull, 1144ull, 1148ull, 1152ull, 1156ull, 1160ull, 1164ull};
+const unsigned long long kQOffs6[] = {928ull, 928ull, 928ull, 928ull, 944ull, 944ull, 944ull, 944ull, 960ull, 960ull, 960ull, 960ull, 976ull, 976ull, 976ull, 976ull, 992ull, 992ull, 992ull, 992ull, 1008ull, 1008ull, 1008ull, 1008ull, 1024ull, 1024ull, 1024ull, 1024ull, 1040ull, 1040ull, 1040ull, 1040ull, 1056ull, 1056ull, 1056ull, 1056ull, 1072ull, 1072ull, 1072ull, 1072ull, 1088ull, 1088ull, 1088ull, 1088ull, 1104ull, 1104ull, 1104ull, 1104ull, 1120ull, 1120ull, 1120ull, 1120ull, 1136ull, 1136ull, 1136ull, 1136ull, 1152ull, 1152ull, 1152ull, 1152ull};
+const unsigned kQSubs6[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths6[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs7[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes7[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames7[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "tmp1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs7[] = {1176ull, 1180ull, 1184ull, 1188ull, 1192ull, 1196ull, 1200ull, 1204ull, 1208ull, 1212ull, 1216ull, 1220ull, 1224ull, 1228ull, 1232ull, 1236ull, 1240ull, 1244ull, 1248ull, 1252ull, 1256ull, 1260ull, 1264ull, 1268ull, 1272ull, 1276ull, 1280ull, 1284ull, 1288ull, 1292ull, 1296ull, 1300ull, 1304ull, 1308ull, 1312ull, 1316ull, 1320ull, 1324ull, 1328ull, 1332ull, 1336ull, 1340ull, 1344ull, 1348ull, 1352ull, 1356ull, 1360ull, 1364ull, 1368ull, 1372ull, 1376ull, 1380ull, 1384ull, 1388ull, 1392ull, 1396ull, 1400ull, 1404ull};
+const unsigned long long kQOffs7[] = {1176ull, 1176ull, 1176ull, 1176ull, 1192ull, 1192ull, 1192ull, 1192ull, 1208ull, 1208ull, 1208ull, 1208ull, 1224ull, 1224ull, 1224ull, 1224ull, 1240ull, 1240ull, 1240ull, 1240ull, 1256ull, 1256ull, 1256ull, 1256ull, 1272ull, 1272ull, 1272ull, 1272ull, 1288ull, 1288ull, 1288ull, 1288ull, 1304ull, 1304ull, 1304ull, 1304ull, 1320ull, 1320ull, 1320ull, 1320ull, 1336ull, 1336ull, 1336ull, 1336ull, 1352ull, 1352ull, 1352ull, 1352ull, 1368ull, 1368ull, 1368ull, 1368ull, 1384ull, 1384ull, 1384ull, 1384ull, 1400ull, 1400ull};
+const unsigned kQSubs7[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths7[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs8[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes8[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames8[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "tmp1", "tmp2", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs8[] = {1416ull, 1420ull, 1424ull, 1428ull, 1432ull, 1436ull, 1440ull, 1444ull, 1448ull, 1452ull, 1456ull, 1460ull, 1464ull, 1468ull, 1472ull, 1476ull, 1480ull, 1484ull, 1488ull, 1492ull, 1496ull, 1500ull, 1504ull, 1508ull, 1512ull, 1516ull, 1520ull, 1524ull, 1528ull, 1532ull, 1536ull, 1540ull, 1544ull, 1548ull, 1552ull, 1556ull, 1560ull, 1564ull, 1568ull, 1572ull, 1576ull, 1580ull, 1584ull, 1588ull, 1592ull, 1596ull, 1600ull, 1604ull, 1608ull, 1612ull, 1616ull, 1620ull, 1624ull, 1628ull, 1632ull, 1636ull, 1640ull, 1644ull};
+const unsigned long long kQOffs8[] = {1416ull, 1416ull, 1416ull, 1416ull, 1432ull, 1432ull, 1432ull, 1432ull, 1448ull, 1448ull, 1448ull, 1448ull, 1464ull, 1464ull, 1464ull, 1464ull, 1480ull, 1480ull, 1480ull, 1480ull, 1496ull, 1496ull, 1496ull, 1496ull, 1512ull, 1512ull, 1512ull, 1512ull, 1528ull, 1528ull, 1528ull, 1528ull, 1544ull, 1544ull, 1544ull, 1544ull, 1560ull, 1560ull, 1560ull, 1560ull, 1576ull, 1576ull, 1576ull, 1576ull, 1592ull, 1592ull, 1592ull, 1592ull, 1608ull, 1608ull, 1608ull, 1608ull, 1624ull, 1624ull, 1624ull, 1624ull, 1640ull, 1640ull};
+const unsigned kQSubs8[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths8[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs9[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes9[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames9[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs9[] = {1656ull, 1660ull, 1664ull, 1668ull, 1672ull, 1676ull, 1680ull, 1684ull, 1688ull, 1692ull, 1696ull, 1700ull, 1704ull, 1708ull, 1712ull, 1716ull, 1720ull, 1724ull, 1728ull, 1732ull, 1736ull, 1740ull, 1744ull, 1748ull, 1752ull, 1756ull, 1760ull, 1764ull, 1768ull, 1772ull, 1776ull, 1780ull, 1784ull, 1788ull, 1792ull, 1796ull, 1800ull, 1804ull, 1808ull, 1812ull, 1816ull, 1820ull, 1824ull, 1828ull, 1832ull, 1836ull, 1840ull, 1844ull, 1848ull, 1852ull, 1856ull, 1860ull, 1864ull, 1868ull, 1872ull, 1876ull};
+const unsigned long long kQOffs9[] = {1656ull, 1656ull, 1656ull, 1656ull, 1672ull, 1672ull, 1672ull, 1672ull, 1688ull, 1688ull, 1688ull, 1688ull, 1704ull, 1704ull, 1704ull, 1704ull, 1720ull, 1720ull, 1720ull, 1720ull, 1736ull, 1736ull, 1736ull, 1736ull, 1752ull, 1752ull, 1752ull, 1752ull, 1768ull, 1768ull, 1768ull, 1768ull, 1784ull, 1784ull, 1784ull, 1784ull, 1800ull, 1800ull, 1800ull, 1800ull, 1816ull, 1816ull, 1816ull, 1816ull, 1832ull, 1832ull, 1832ull, 1832ull, 1848ull, 1848ull, 1848ull, 1848ull, 1864ull, 1864ull, 1864ull, 1864ull};
+const unsigned kQSubs9[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths9[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs10[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 58u, 59u, 60u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes10[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames10[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "vr40", "vr41", "vr42", "vr60", "vr61", "vr62", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs10[] = {1888ull, 1892ull, 1896ull, 1900ull, 1904ull, 1908ull, 1912ull, 1916ull, 1920ull, 1924ull, 1928ull, 1932ull, 1936ull, 1940ull, 1944ull, 1948ull, 1952ull, 1956ull, 1960ull, 1964ull, 1968ull, 1972ull, 1976ull, 1980ull, 1984ull, 1988ull, 1992ull, 1996ull, 2000ull, 2004ull, 2008ull, 2012ull, 2016ull, 2020ull, 2024ull, 2028ull, 2032ull, 2036ull, 2040ull, 2044ull, 2048ull, 2052ull, 2056ull, 2060ull, 2064ull, 2068ull, 2072ull, 2076ull, 2080ull, 2084ull, 2088ull, 2092ull, 2096ull, 2100ull, 2104ull, 2108ull, 2112ull, 2116ull, 2120ull, 2124ull, 2128ull, 2132ull, 2136ull};
+const unsigned long long kQOffs10[] = {1888ull, 1888ull, 1888ull, 1888ull, 1904ull, 1904ull, 1904ull, 1904ull, 1920ull, 1920ull, 1920ull, 1920ull, 1936ull, 1936ull, 1936ull, 1936ull, 1952ull, 1952ull, 1952ull, 1952ull, 1968ull, 1968ull, 1968ull, 1968ull, 1984ull, 1984ull, 1984ull, 1984ull, 2000ull, 2000ull, 2000ull, 2000ull, 2016ull, 2016ull, 2016ull, 2016ull, 2032ull, 2032ull, 2032ull, 2032ull, 2048ull, 2048ull, 2048ull, 2048ull, 2064ull, 2064ull, 2064ull, 2064ull, 2080ull, 2080ull, 2080ull, 2080ull, 2096ull, 2096ull, 2096ull, 2096ull, 2112ull, 2112ull, 2112ull, 2112ull, 2128ull, 2128ull, 2128ull};
+const unsigned kQSubs10[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths10[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs11[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 48u, 49u, 50u, 51u, 52u, 53u, 54u, 55u, 56u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes11[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames11[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr30", "vr31", "vr32", "vr40", "vr41", "vr42", "vr50", "vr51", "vr52", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs11[] = {2144ull, 2148ull, 2152ull, 2156ull, 2160ull, 2164ull, 2168ull, 2172ull, 2176ull, 2180ull, 2184ull, 2188ull, 2192ull, 2196ull, 2200ull, 2204ull, 2208ull, 2212ull, 2216ull, 2220ull, 2224ull, 2228ull, 2232ull, 2236ull, 2240ull, 2244ull, 2248ull, 2252ull, 2256ull, 2260ull, 2264ull, 2268ull, 2272ull, 2276ull, 2280ull, 2284ull, 2288ull, 2292ull, 2296ull, 2300ull, 2304ull, 2308ull, 2312ull, 2316ull, 2320ull, 2324ull, 2328ull, 2332ull, 2336ull, 2340ull, 2344ull, 2348ull, 2352ull, 2356ull, 2360ull, 2364ull, 2368ull, 2372ull, 2376ull, 2380ull};
+const unsigned long long kQOffs11[] = {2144ull, 2144ull, 2144ull, 2144ull, 2160ull, 2160ull, 2160ull, 2160ull, 2176ull, 2176ull, 2176ull, 2176ull, 2192ull, 2192ull, 2192ull, 2192ull, 2208ull, 2208ull, 2208ull, 2208ull, 2224ull, 2224ull, 2224ull, 2224ull, 2240ull, 2240ull, 2240ull, 2240ull, 2256ull, 2256ull, 2256ull, 2256ull, 2272ull, 2272ull, 2272ull, 2272ull, 2288ull, 2288ull, 2288ull, 2288ull, 2304ull, 2304ull, 2304ull, 2304ull, 2320ull, 2320ull, 2320ull, 2320ull, 2336ull, 2336ull, 2336ull, 2336ull, 2352ull, 2352ull, 2352ull, 2352ull, 2368ull, 2368ull, 2368ull, 2368ull};
+const unsigned kQSubs11[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths11[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs12[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 48u, 49u, 50u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes12[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames12[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr30", "vr31", "vr32", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs12[] = {2392ull, 2396ull, 2400ull, 2404ull, 2408ull, 2412ull, 2416ull, 2420ull, 2424ull, 2428ull, 2432ull, 2436ull, 2440ull, 2444ull, 2448ull, 2452ull, 2456ull, 2460ull, 2464ull, 2468ull, 2472ull, 2476ull, 2480ull, 2484ull, 2488ull, 2492ull, 2496ull, 2500ull, 2504ull, 2508ull, 2512ull, 2516ull, 2520ull, 2524ull, 2528ull, 2532ull, 2536ull, 2540ull, 2544ull, 2548ull, 2552ull, 2556ull, 2560ull, 2564ull, 2568ull, 2572ull, 2576ull, 2580ull, 2584ull, 2588ull, 2592ull, 2596ull, 2600ull};
+const unsigned long long kQOffs12[] = {2392ull, 2392ull, 2392ull, 2392ull, 2408ull, 2408ull, 2408ull, 2408ull, 2424ull, 2424ull, 2424ull, 2424ull, 2440ull, 2440ull, 2440ull, 2440ull, 2456ull, 2456ull, 2456ull, 2456ull, 2472ull, 2472ull, 2472ull, 2472ull, 2488ull, 2488ull, 2488ull, 2488ull, 2504ull, 2504ull, 2504ull, 2504ull, 2520ull, 2520ull, 2520ull, 2520ull, 2536ull, 2536ull, 2536ull, 2536ull, 2552ull, 2552ull, 2552ull, 2552ull, 2568ull, 2568ull, 2568ull, 2568ull, 2584ull, 2584ull, 2584ull, 2584ull, 2600ull};
+const unsigned kQSubs12[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths12[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs13[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes13[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames13[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs13[] = {2608ull, 2612ull, 2616ull, 2620ull, 2624ull, 2628ull, 2632ull, 2636ull, 2640ull, 2644ull, 2648ull, 2652ull, 2656ull, 2660ull, 2664ull, 2668ull, 2672ull, 2676ull, 2680ull, 2684ull, 2688ull, 2692ull, 2696ull, 2700ull, 2704ull, 2708ull, 2712ull, 2716ull, 2720ull, 2724ull, 2728ull, 2732ull, 2736ull, 2740ull, 2744ull, 2748ull, 2752ull, 2756ull, 2760ull, 2764ull, 2768ull, 2772ull, 2776ull, 2780ull, 2784ull};
+const unsigned long long kQOffs13[] = {2608ull, 2608ull, 2608ull, 2608ull, 2624ull, 2624ull, 2624ull, 2624ull, 2640ull, 2640ull, 2640ull, 2640ull, 2656ull, 2656ull, 2656ull, 2656ull, 2672ull, 2672ull, 2672ull, 2672ull, 2688ull, 2688ull, 2688ull, 2688ull, 2704ull, 2704ull, 2704ull, 2704ull, 2720ull, 2720ull, 2720ull, 2720ull, 2736ull, 2736ull, 2736ull, 2736ull, 2752ull, 2752ull, 2752ull, 2752ull, 2768ull, 2768ull, 2768ull, 2768ull, 2784ull};
+const unsigned kQSubs13[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths13[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs14[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes14[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames14[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs14[] = {2792ull, 2796ull, 2800ull, 2804ull, 2808ull, 2812ull, 2816ull, 2820ull, 2824ull, 2828ull, 2832ull, 2836ull, 2840ull, 2844ull, 2848ull, 2852ull, 2856ull, 2860ull, 2864ull, 2868ull, 2872ull, 2876ull, 2880ull, 2884ull, 2888ull, 2892ull, 2896ull, 2900ull, 2904ull, 2908ull, 2912ull, 2916ull, 2920ull, 2924ull, 2928ull, 2932ull, 2936ull, 2940ull, 2944ull, 2948ull, 2952ull, 2956ull, 2960ull};
+const unsigned long long kQOffs14[] = {2792ull, 2792ull, 2792ull, 2792ull, 2808ull, 2808ull, 2808ull, 2808ull, 2824ull, 2824ull, 2824ull, 2824ull, 2840ull, 2840ull, 2840ull, 2840ull, 2856ull, 2856ull, 2856ull, 2856ull, 2872ull, 2872ull, 2872ull, 2872ull, 2888ull, 2888ull, 2888ull, 2888ull, 2904ull, 2904ull, 2904ull, 2904ull, 2920ull, 2920ull, 2920ull, 2920ull, 2936ull, 2936ull, 2936ull, 2936ull, 2952ull, 2952ull, 2952ull};
+const unsigned kQSubs14[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths14[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs15[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 48u, 49u, 50u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes15[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames15[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs15[] = {2968ull, 2972ull, 2976ull, 2980ull, 2984ull, 2988ull, 2992ull, 2996ull, 3000ull, 3004ull, 3008ull, 3012ull, 3016ull, 3020ull, 3024ull, 3028ull, 3032ull, 3036ull, 3040ull, 3044ull, 3048ull, 3052ull, 3056ull, 3060ull, 3064ull, 3068ull, 3072ull, 3076ull, 3080ull, 3084ull, 3088ull, 3092ull, 3096ull, 3100ull, 3104ull, 3108ull, 3112ull, 3116ull, 3120ull, 3124ull, 3128ull, 3132ull, 3136ull, 3140ull, 3144ull, 3148ull, 3152ull, 3156ull, 3160ull, 3164ull, 3168ull, 3172ull, 3176ull, 3180ull, 3184ull, 3188ull};
+const unsigned long long kQOffs15[] = {2968ull, 2968ull, 2968ull, 2968ull, 2984ull, 2984ull, 2984ull, 2984ull, 3000ull, 3000ull, 3000ull, 3000ull, 3016ull, 3016ull, 3016ull, 3016ull, 3032ull, 3032ull, 3032ull, 3032ull, 3048ull, 3048ull, 3048ull, 3048ull, 3064ull, 3064ull, 3064ull, 3064ull, 3080ull, 3080ull, 3080ull, 3080ull, 3096ull, 3096ull, 3096ull, 3096ull, 3112ull, 3112ull, 3112ull, 3112ull, 3128ull, 3128ull, 3128ull, 3128ull, 3144ull, 3144ull, 3144ull, 3144ull, 3160ull, 3160ull, 3160ull, 3160ull, 3176ull, 3176ull, 3176ull, 3176ull};
+const unsigned kQSubs15[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths15[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs16[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 45u, 46u, 47u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes16[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames16[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "vr20", "vr21", "vr22", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs16[] = {3200ull, 3204ull, 3208ull, 3212ull, 3216ull, 3220ull, 3224ull, 3228ull, 3232ull, 3236ull, 3240ull, 3244ull, 3248ull, 3252ull, 3256ull, 3260ull, 3264ull, 3268ull, 3272ull, 3276ull, 3280ull, 3284ull, 3288ull, 3292ull, 3296ull, 3300ull, 3304ull, 3308ull, 3312ull, 3316ull, 3320ull, 3324ull, 3328ull, 3332ull, 3336ull, 3340ull, 3344ull, 3348ull, 3352ull, 3356ull, 3360ull, 3364ull, 3368ull, 3372ull, 3376ull, 3380ull, 3384ull, 3388ull, 3392ull, 3396ull, 3400ull, 3404ull, 3408ull, 3412ull};
+const unsigned long long kQOffs16[] = {3200ull, 3200ull, 3200ull, 3200ull, 3216ull, 3216ull, 3216ull, 3216ull, 3232ull, 3232ull, 3232ull, 3232ull, 3248ull, 3248ull, 3248ull, 3248ull, 3264ull, 3264ull, 3264ull, 3264ull, 3280ull, 3280ull, 3280ull, 3280ull, 3296ull, 3296ull, 3296ull, 3296ull, 3312ull, 3312ull, 3312ull, 3312ull, 3328ull, 3328ull, 3328ull, 3328ull, 3344ull, 3344ull, 3344ull, 3344ull, 3360ull, 3360ull, 3360ull, 3360ull, 3376ull, 3376ull, 3376ull, 3376ull, 3392ull, 3392ull, 3392ull, 3392ull, 3408ull, 3408ull};
+const unsigned kQSubs16[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths16[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs17[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 45u, 46u, 47u, 48u, 49u, 50u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes17[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames17[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "vr20", "vr21", "vr22", "vr30", "vr31", "vr32", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs17[] = {3424ull, 3428ull, 3432ull, 3436ull, 3440ull, 3444ull, 3448ull, 3452ull, 3456ull, 3460ull, 3464ull, 3468ull, 3472ull, 3476ull, 3480ull, 3484ull, 3488ull, 3492ull, 3496ull, 3500ull, 3504ull, 3508ull, 3512ull, 3516ull, 3520ull, 3524ull, 3528ull, 3532ull, 3536ull, 3540ull, 3544ull, 3548ull, 3552ull, 3556ull, 3560ull, 3564ull, 3568ull, 3572ull, 3576ull, 3580ull, 3584ull, 3588ull, 3592ull, 3596ull, 3600ull, 3604ull, 3608ull, 3612ull, 3616ull, 3620ull};
+const unsigned long long kQOffs17[] = {3424ull, 3424ull, 3424ull, 3424ull, 3440ull, 3440ull, 3440ull, 3440ull, 3456ull, 3456ull, 3456ull, 3456ull, 3472ull, 3472ull, 3472ull, 3472ull, 3488ull, 3488ull, 3488ull, 3488ull, 3504ull, 3504ull, 3504ull, 3504ull, 3520ull, 3520ull, 3520ull, 3520ull, 3536ull, 3536ull, 3536ull, 3536ull, 3552ull, 3552ull, 3552ull, 3552ull, 3568ull, 3568ull, 3568ull, 3568ull, 3584ull, 3584ull, 3584ull, 3584ull, 3600ull, 3600ull, 3600ull, 3600ull, 3616ull, 3616ull};
+const unsigned kQSubs17[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths17[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs18[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes18[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames18[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs18[] = {3632ull, 3636ull, 3640ull, 3644ull, 3648ull, 3652ull, 3656ull, 3660ull, 3664ull, 3668ull, 3672ull, 3676ull, 3680ull, 3684ull, 3688ull, 3692ull, 3696ull, 3700ull, 3704ull, 3708ull, 3712ull, 3716ull, 3720ull, 3724ull, 3728ull, 3732ull, 3736ull, 3740ull, 3744ull, 3748ull, 3752ull, 3756ull, 3760ull, 3764ull, 3768ull, 3772ull, 3776ull, 3780ull, 3784ull, 3788ull, 3792ull, 3796ull, 3800ull, 3804ull, 3808ull};
+const unsigned long long kQOffs18[] = {3632ull, 3632ull, 3632ull, 3632ull, 3648ull, 3648ull, 3648ull, 3648ull, 3664ull, 3664ull, 3664ull, 3664ull, 3680ull, 3680ull, 3680ull, 3680ull, 3696ull, 3696ull, 3696ull, 3696ull, 3712ull, 3712ull, 3712ull, 3712ull, 3728ull, 3728ull, 3728ull, 3728ull, 3744ull, 3744ull, 3744ull, 3744ull, 3760ull, 3760ull, 3760ull, 3760ull, 3776ull, 3776ull, 3776ull, 3776ull, 3792ull, 3792ull, 3792ull, 3792ull, 3808ull};
+const unsigned kQSubs18[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths18[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs19[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes19[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames19[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs19[] = {3816ull, 3820ull, 3824ull, 3828ull, 3832ull, 3836ull, 3840ull, 3844ull, 3848ull, 3852ull, 3856ull, 3860ull, 3864ull, 3868ull, 3872ull, 3876ull, 3880ull, 3884ull, 3888ull, 3892ull, 3896ull, 3900ull, 3904ull, 3908ull, 3912ull, 3916ull, 3920ull, 3924ull, 3928ull, 3932ull, 3936ull, 3940ull, 3944ull, 3948ull, 3952ull, 3956ull, 3960ull, 3964ull, 3968ull, 3972ull, 3976ull, 3980ull, 3984ull};
+const unsigned long long kQOffs19[] = {3816ull, 3816ull, 3816ull, 3816ull, 3832ull, 3832ull, 3832ull, 3832ull, 3848ull, 3848ull, 3848ull, 3848ull, 3864ull, 3864ull, 3864ull, 3864ull, 3880ull, 3880ull, 3880ull, 3880ull, 3896ull, 3896ull, 3896ull, 3896ull, 3912ull, 3912ull, 3912ull, 3912ull, 3928ull, 3928ull, 3928ull, 3928ull, 3944ull, 3944ull, 3944ull, 3944ull, 3960ull, 3960ull, 3960ull, 3960ull, 3976ull, 3976ull, 3976ull};
+const unsigned kQSubs19[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths19[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs20[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 42u, 43u, 44u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes20[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames20[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs20[] = {3992ull, 3996ull, 4000ull, 4004ull, 4008ull, 4012ull, 4016ull, 4020ull, 4024ull, 4028ull, 4032ull, 4036ull, 4040ull, 4044ull, 4048ull, 4052ull, 4056ull, 4060ull, 4064ull, 4068ull, 4072ull, 4076ull, 4080ull, 4084ull, 4088ull, 4092ull, 4096ull, 4100ull, 4104ull, 4108ull, 4112ull, 4116ull, 4120ull, 4124ull, 4128ull, 4132ull, 4136ull, 4140ull, 4144ull, 4148ull, 4152ull, 4156ull, 4160ull, 4164ull, 4168ull, 4172ull, 4176ull, 4180ull};
+const unsigned long long kQOffs20[] = {3992ull, 3992ull, 3992ull, 3992ull, 4008ull, 4008ull, 4008ull, 4008ull, 4024ull, 4024ull, 4024ull, 4024ull, 4040ull, 4040ull, 4040ull, 4040ull, 4056ull, 4056ull, 4056ull, 4056ull, 4072ull, 4072ull, 4072ull, 4072ull, 4088ull, 4088ull, 4088ull, 4088ull, 4104ull, 4104ull, 4104ull, 4104ull, 4120ull, 4120ull, 4120ull, 4120ull, 4136ull, 4136ull, 4136ull, 4136ull, 4152ull, 4152ull, 4152ull, 4152ull, 4168ull, 4168ull, 4168ull, 4168ull};
+const unsigned kQSubs20[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths20[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs21[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 43u, 44u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes21[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames21[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr11", "vr12", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs21[] = {4192ull, 4196ull, 4200ull, 4204ull, 4208ull, 4212ull, 4216ull, 4220ull, 4224ull, 4228ull, 4232ull, 4236ull, 4240ull, 4244ull, 4248ull, 4252ull, 4256ull, 4260ull, 4264ull, 4268ull, 4272ull, 4276ull, 4280ull, 4284ull, 4288ull, 4292ull, 4296ull, 4300ull, 4304ull, 4308ull, 4312ull, 4316ull, 4320ull, 4324ull, 4328ull, 4332ull, 4336ull, 4340ull, 4344ull, 4348ull, 4352ull, 4356ull, 4360ull, 4364ull, 4368ull, 4372ull, 4376ull};
+const unsigned long long kQOffs21[] = {4192ull, 4192ull, 4192ull, 4192ull, 4208ull, 4208ull, 4208ull, 4208ull, 4224ull, 4224ull, 4224ull, 4224ull, 4240ull, 4240ull, 4240ull, 4240ull, 4256ull, 4256ull, 4256ull, 4256ull, 4272ull, 4272ull, 4272ull, 4272ull, 4288ull, 4288ull, 4288ull, 4288ull, 4304ull, 4304ull, 4304ull, 4304ull, 4320ull, 4320ull, 4320ull, 4320ull, 4336ull, 4336ull, 4336ull, 4336ull, 4352ull, 4352ull, 4352ull, 4352ull, 4368ull, 4368ull, 4368ull};
+const unsigned kQSubs21[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths21[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs22[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 43u, 44u, 57u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes22[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames22[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr11", "vr12", "hit", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs22[] = {4384ull, 4388ull, 4392ull, 4396ull, 4400ull, 4404ull, 4408ull, 4412ull, 4416ull, 4420ull, 4424ull, 4428ull, 4432ull, 4436ull, 4440ull, 4444ull, 4448ull, 4452ull, 4456ull, 4460ull, 4464ull, 4468ull, 4472ull, 4476ull, 4480ull, 4484ull, 4488ull, 4492ull, 4496ull, 4500ull, 4504ull, 4508ull, 4512ull, 4516ull, 4520ull, 4524ull, 4528ull, 4532ull, 4536ull, 4540ull, 4544ull, 4548ull, 4552ull, 4556ull, 4560ull, 4564ull, 4568ull};
+const unsigned long long kQOffs22[] = {4384ull, 4384ull, 4384ull, 4384ull, 4400ull, 4400ull, 4400ull, 4400ull, 4416ull, 4416ull, 4416ull, 4416ull, 4432ull, 4432ull, 4432ull, 4432ull, 4448ull, 4448ull, 4448ull, 4448ull, 4464ull, 4464ull, 4464ull, 4464ull, 4480ull, 4480ull, 4480ull, 4480ull, 4496ull, 4496ull, 4496ull, 4496ull, 4512ull, 4512ull, 4512ull, 4512ull, 4528ull, 4528ull, 4528ull, 4528ull, 4544ull, 4544ull, 4544ull, 4544ull, 4560ull, 4560ull, 4560ull};
+const unsigned kQSubs22[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths22[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs23[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 42u, 43u, 44u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes23[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames23[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs23[] = {4576ull, 4580ull, 4584ull, 4588ull, 4592ull, 4596ull, 4600ull, 4604ull, 4608ull, 4612ull, 4616ull, 4620ull, 4624ull, 4628ull, 4632ull, 4636ull, 4640ull, 4644ull, 4648ull, 4652ull, 4656ull, 4660ull, 4664ull, 4668ull, 4672ull, 4676ull, 4680ull, 4684ull, 4688ull, 4692ull, 4696ull, 4700ull, 4704ull, 4708ull, 4712ull, 4716ull, 4720ull, 4724ull, 4728ull, 4732ull, 4736ull, 4740ull, 4744ull, 4748ull, 4752ull, 4756ull, 4760ull, 4764ull};
+const unsigned long long kQOffs23[] = {4576ull, 4576ull, 4576ull, 4576ull, 4592ull, 4592ull, 4592ull, 4592ull, 4608ull, 4608ull, 4608ull, 4608ull, 4624ull, 4624ull, 4624ull, 4624ull, 4640ull, 4640ull, 4640ull, 4640ull, 4656ull, 4656ull, 4656ull, 4656ull, 4672ull, 4672ull, 4672ull, 4672ull, 4688ull, 4688ull, 4688ull, 4688ull, 4704ull, 4704ull, 4704ull, 4704ull, 4720ull, 4720ull, 4720ull, 4720ull, 4736ull, 4736ull, 4736ull, 4736ull, 4752ull, 4752ull, 4752ull, 4752ull};
+const unsigned kQSubs23[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths23[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs24[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 42u, 43u, 44u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes24[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames24[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr10", "vr11", "vr12", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs24[] = {4776ull, 4780ull, 4784ull, 4788ull, 4792ull, 4796ull, 4800ull, 4804ull, 4808ull, 4812ull, 4816ull, 4820ull, 4824ull, 4828ull, 4832ull, 4836ull, 4840ull, 4844ull, 4848ull, 4852ull, 4856ull, 4860ull, 4864ull, 4868ull, 4872ull, 4876ull, 4880ull, 4884ull, 4888ull, 4892ull, 4896ull, 4900ull, 4904ull, 4908ull, 4912ull, 4916ull, 4920ull, 4924ull, 4928ull, 4932ull, 4936ull, 4940ull, 4944ull, 4948ull, 4952ull, 4956ull, 4960ull, 4964ull};
+const unsigned long long kQOffs24[] = {4776ull, 4776ull, 4776ull, 4776ull, 4792ull, 4792ull, 4792ull, 4792ull, 4808ull, 4808ull, 4808ull, 4808ull, 4824ull, 4824ull, 4824ull, 4824ull, 4840ull, 4840ull, 4840ull, 4840ull, 4856ull, 4856ull, 4856ull, 4856ull, 4872ull, 4872ull, 4872ull, 4872ull, 4888ull, 4888ull, 4888ull, 4888ull, 4904ull, 4904ull, 4904ull, 4904ull, 4920ull, 4920ull, 4920ull, 4920ull, 4936ull, 4936ull, 4936ull, 4936ull, 4952ull, 4952ull, 4952ull, 4952ull};
+const unsigned kQSubs24[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths24[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs25[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 44u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes25[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames25[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "vr12", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs25[] = {4976ull, 4980ull, 4984ull, 4988ull, 4992ull, 4996ull, 5000ull, 5004ull, 5008ull, 5012ull, 5016ull, 5020ull, 5024ull, 5028ull, 5032ull, 5036ull, 5040ull, 5044ull, 5048ull, 5052ull, 5056ull, 5060ull, 5064ull, 5068ull, 5072ull, 5076ull, 5080ull, 5084ull, 5088ull, 5092ull, 5096ull, 5100ull, 5104ull, 5108ull, 5112ull, 5116ull, 5120ull, 5124ull, 5128ull, 5132ull, 5136ull, 5140ull, 5144ull, 5148ull, 5152ull, 5156ull, 5160ull};
+const unsigned long long kQOffs25[] = {4976ull, 4976ull, 4976ull, 4976ull, 4992ull, 4992ull, 4992ull, 4992ull, 5008ull, 5008ull, 5008ull, 5008ull, 5024ull, 5024ull, 5024ull, 5024ull, 5040ull, 5040ull, 5040ull, 5040ull, 5056ull, 5056ull, 5056ull, 5056ull, 5072ull, 5072ull, 5072ull, 5072ull, 5088ull, 5088ull, 5088ull, 5088ull, 5104ull, 5104ull, 5104ull, 5104ull, 5120ull, 5120ull, 5120ull, 5120ull, 5136ull, 5136ull, 5136ull, 5136ull, 5152ull, 5152ull, 5152ull};
+const unsigned kQSubs25[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths25[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs26[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes26[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames26[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs26[] = {5168ull, 5172ull, 5176ull, 5180ull, 5184ull, 5188ull, 5192ull, 5196ull, 5200ull, 5204ull, 5208ull, 5212ull, 5216ull, 5220ull, 5224ull, 5228ull, 5232ull, 5236ull, 5240ull, 5244ull, 5248ull, 5252ull, 5256ull, 5260ull, 5264ull, 5268ull, 5272ull, 5276ull, 5280ull, 5284ull, 5288ull, 5292ull, 5296ull, 5300ull, 5304ull, 5308ull, 5312ull, 5316ull, 5320ull, 5324ull, 5328ull, 5332ull, 5336ull, 5340ull, 5344ull, 5348ull};
+const unsigned long long kQOffs26[] = {5168ull, 5168ull, 5168ull, 5168ull, 5184ull, 5184ull, 5184ull, 5184ull, 5200ull, 5200ull, 5200ull, 5200ull, 5216ull, 5216ull, 5216ull, 5216ull, 5232ull, 5232ull, 5232ull, 5232ull, 5248ull, 5248ull, 5248ull, 5248ull, 5264ull, 5264ull, 5264ull, 5264ull, 5280ull, 5280ull, 5280ull, 5280ull, 5296ull, 5296ull, 5296ull, 5296ull, 5312ull, 5312ull, 5312ull, 5312ull, 5328ull, 5328ull, 5328ull, 5328ull, 5344ull, 5344ull};
+const unsigned kQSubs26[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths26[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs27[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes27[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames27[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs27[] = {5360ull, 5364ull, 5368ull, 5372ull, 5376ull, 5380ull, 5384ull, 5388ull, 5392ull, 5396ull, 5400ull, 5404ull, 5408ull, 5412ull, 5416ull, 5420ull, 5424ull, 5428ull, 5432ull, 5436ull, 5440ull, 5444ull, 5448ull, 5452ull, 5456ull, 5460ull, 5464ull, 5468ull, 5472ull, 5476ull, 5480ull, 5484ull, 5488ull, 5492ull, 5496ull, 5500ull, 5504ull, 5508ull, 5512ull, 5516ull, 5520ull, 5524ull, 5528ull, 5532ull, 5536ull, 5540ull};
+const unsigned long long kQOffs27[] = {5360ull, 5360ull, 5360ull, 5360ull, 5376ull, 5376ull, 5376ull, 5376ull, 5392ull, 5392ull, 5392ull, 5392ull, 5408ull, 5408ull, 5408ull, 5408ull, 5424ull, 5424ull, 5424ull, 5424ull, 5440ull, 5440ull, 5440ull, 5440ull, 5456ull, 5456ull, 5456ull, 5456ull, 5472ull, 5472ull, 5472ull, 5472ull, 5488ull, 5488ull, 5488ull, 5488ull, 5504ull, 5504ull, 5504ull, 5504ull, 5520ull, 5520ull, 5520ull, 5520ull, 5536ull, 5536ull};
+const unsigned kQSubs27[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths27[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs28[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes28[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames28[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs28[] = {5552ull, 5556ull, 5560ull, 5564ull, 5568ull, 5572ull, 5576ull, 5580ull, 5584ull, 5588ull, 5592ull, 5596ull, 5600ull, 5604ull, 5608ull, 5612ull, 5616ull, 5620ull, 5624ull, 5628ull, 5632ull, 5636ull, 5640ull, 5644ull, 5648ull, 5652ull, 5656ull, 5660ull, 5664ull, 5668ull, 5672ull, 5676ull, 5680ull, 5684ull, 5688ull, 5692ull, 5696ull, 5700ull, 5704ull, 5708ull, 5712ull, 5716ull, 5720ull, 5724ull, 5728ull};
+const unsigned long long kQOffs28[] = {5552ull, 5552ull, 5552ull, 5552ull, 5568ull, 5568ull, 5568ull, 5568ull, 5584ull, 5584ull, 5584ull, 5584ull, 5600ull, 5600ull, 5600ull, 5600ull, 5616ull, 5616ull, 5616ull, 5616ull, 5632ull, 5632ull, 5632ull, 5632ull, 5648ull, 5648ull, 5648ull, 5648ull, 5664ull, 5664ull, 5664ull, 5664ull, 5680ull, 5680ull, 5680ull, 5680ull, 5696ull, 5696ull, 5696ull, 5696ull, 5712ull, 5712ull, 5712ull, 5712ull, 5728ull};
+const unsigned kQSubs28[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths28[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs29[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes29[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames29[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs29[] = {5736ull, 5740ull, 5744ull, 5748ull, 5752ull, 5756ull, 5760ull, 5764ull, 5768ull, 5772ull, 5776ull, 5780ull, 5784ull, 5788ull, 5792ull, 5796ull, 5800ull, 5804ull, 5808ull, 5812ull, 5816ull, 5820ull, 5824ull, 5828ull, 5832ull, 5836ull, 5840ull, 5844ull, 5848ull, 5852ull, 5856ull, 5860ull, 5864ull, 5868ull, 5872ull, 5876ull, 5880ull, 5884ull, 5888ull, 5892ull, 5896ull, 5900ull, 5904ull};
+const unsigned long long kQOffs29[] = {5736ull, 5736ull, 5736ull, 5736ull, 5752ull, 5752ull, 5752ull, 5752ull, 5768ull, 5768ull, 5768ull, 5768ull, 5784ull, 5784ull, 5784ull, 5784ull, 5800ull, 5800ull, 5800ull, 5800ull, 5816ull, 5816ull, 5816ull, 5816ull, 5832ull, 5832ull, 5832ull, 5832ull, 5848ull, 5848ull, 5848ull, 5848ull, 5864ull, 5864ull, 5864ull, 5864ull, 5880ull, 5880ull, 5880ull, 5880ull, 5896ull, 5896ull, 5896ull};
+const unsigned kQSubs29[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths29[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs30[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 37u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes30[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames30[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr01", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs30[] = {5912ull, 5916ull, 5920ull, 5924ull, 5928ull, 5932ull, 5936ull, 5940ull, 5944ull, 5948ull, 5952ull, 5956ull, 5960ull, 5964ull, 5968ull, 5972ull, 5976ull, 5980ull, 5984ull, 5988ull, 5992ull, 5996ull, 6000ull, 6004ull, 6008ull, 6012ull, 6016ull, 6020ull, 6024ull, 6028ull, 6032ull, 6036ull, 6040ull, 6044ull, 6048ull, 6052ull, 6056ull, 6060ull, 6064ull, 6068ull, 6072ull, 6076ull, 6080ull, 6084ull, 6088ull, 6092ull};
+const unsigned long long kQOffs30[] = {5912ull, 5912ull, 5912ull, 5912ull, 5928ull, 5928ull, 5928ull, 5928ull, 5944ull, 5944ull, 5944ull, 5944ull, 5960ull, 5960ull, 5960ull, 5960ull, 5976ull, 5976ull, 5976ull, 5976ull, 5992ull, 5992ull, 5992ull, 5992ull, 6008ull, 6008ull, 6008ull, 6008ull, 6024ull, 6024ull, 6024ull, 6024ull, 6040ull, 6040ull, 6040ull, 6040ull, 6056ull, 6056ull, 6056ull, 6056ull, 6072ull, 6072ull, 6072ull, 6072ull, 6088ull, 6088ull};
+const unsigned kQSubs30[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths30[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs31[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 42u, 43u, 44u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes31[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames31[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "vr10", "vr11", "vr12", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs31[] = {6104ull, 6108ull, 6112ull, 6116ull, 6120ull, 6124ull, 6128ull, 6132ull, 6136ull, 6140ull, 6144ull, 6148ull, 6152ull, 6156ull, 6160ull, 6164ull, 6168ull, 6172ull, 6176ull, 6180ull, 6184ull, 6188ull, 6192ull, 6196ull, 6200ull, 6204ull, 6208ull, 6212ull, 6216ull, 6220ull, 6224ull, 6228ull, 6232ull, 6236ull, 6240ull, 6244ull, 6248ull, 6252ull, 6256ull, 6260ull, 6264ull, 6268ull, 6272ull, 6276ull, 6280ull, 6284ull, 6288ull, 6292ull, 6296ull, 6300ull};
+const unsigned long long kQOffs31[] = {6104ull, 6104ull, 6104ull, 6104ull, 6120ull, 6120ull, 6120ull, 6120ull, 6136ull, 6136ull, 6136ull, 6136ull, 6152ull, 6152ull, 6152ull, 6152ull, 6168ull, 6168ull, 6168ull, 6168ull, 6184ull, 6184ull, 6184ull, 6184ull, 6200ull, 6200ull, 6200ull, 6200ull, 6216ull, 6216ull, 6216ull, 6216ull, 6232ull, 6232ull, 6232ull, 6232ull, 6248ull, 6248ull, 6248ull, 6248ull, 6264ull, 6264ull, 6264ull, 6264ull, 6280ull, 6280ull, 6280ull, 6280ull, 6296ull, 6296ull};
+const unsigned kQSubs31[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths31[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs32[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 39u, 40u, 41u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes32[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames32[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "t", "pid", "rp", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs32[] = {6312ull, 6316ull, 6320ull, 6324ull, 6328ull, 6332ull, 6336ull, 6340ull, 6344ull, 6348ull, 6352ull, 6356ull, 6360ull, 6364ull, 6368ull, 6372ull, 6376ull, 6380ull, 6384ull, 6388ull, 6392ull, 6396ull, 6400ull, 6404ull, 6408ull, 6412ull, 6416ull, 6420ull, 6424ull, 6428ull, 6432ull, 6436ull, 6440ull, 6444ull, 6448ull, 6452ull, 6456ull, 6460ull, 6464ull, 6468ull, 6472ull, 6476ull, 6480ull, 6484ull, 6488ull, 6492ull, 6496ull, 6500ull};
+const unsigned long long kQOffs32[] = {6312ull, 6312ull, 6312ull, 6312ull, 6328ull, 6328ull, 6328ull, 6328ull, 6344ull, 6344ull, 6344ull, 6344ull, 6360ull, 6360ull, 6360ull, 6360ull, 6376ull, 6376ull, 6376ull, 6376ull, 6392ull, 6392ull, 6392ull, 6392ull, 6408ull, 6408ull, 6408ull, 6408ull, 6424ull, 6424ull, 6424ull, 6424ull, 6440ull, 6440ull, 6440ull, 6440ull, 6456ull, 6456ull, 6456ull, 6456ull, 6472ull, 6472ull, 6472ull, 6472ull, 6488ull, 6488ull, 6488ull, 6488ull};
+const unsigned kQSubs32[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths32[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs33[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 41u, 57u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes33[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames33[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "rp", "hit", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs33[] = {6512ull, 6516ull, 6520ull, 6524ull, 6528ull, 6532ull, 6536ull, 6540ull, 6544ull, 6548ull, 6552ull, 6556ull, 6560ull, 6564ull, 6568ull, 6572ull, 6576ull, 6580ull, 6584ull, 6588ull, 6592ull, 6596ull, 6600ull, 6604ull, 6608ull, 6612ull, 6616ull, 6620ull, 6624ull, 6628ull, 6632ull, 6636ull, 6640ull, 6644ull, 6648ull, 6652ull, 6656ull, 6660ull, 6664ull, 6668ull, 6672ull, 6676ull, 6680ull, 6684ull, 6688ull};
+const unsigned long long kQOffs33[] = {6512ull, 6512ull, 6512ull, 6512ull, 6528ull, 6528ull, 6528ull, 6528ull, 6544ull, 6544ull, 6544ull, 6544ull, 6560ull, 6560ull, 6560ull, 6560ull, 6576ull, 6576ull, 6576ull, 6576ull, 6592ull, 6592ull, 6592ull, 6592ull, 6608ull, 6608ull, 6608ull, 6608ull, 6624ull, 6624ull, 6624ull, 6624ull, 6640ull, 6640ull, 6640ull, 6640ull, 6656ull, 6656ull, 6656ull, 6656ull, 6672ull, 6672ull, 6672ull, 6672ull, 6688ull};
+const unsigned kQSubs33[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths33[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs34[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 18u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes34[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames34[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "rpt", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs34[] = {6696ull, 6700ull, 6704ull, 6708ull, 6712ull, 6716ull, 6720ull, 6724ull, 6728ull, 6732ull, 6736ull, 6740ull, 6744ull, 6748ull, 6752ull, 6756ull, 6760ull, 6764ull, 6768ull, 6772ull, 6776ull, 6780ull, 6784ull, 6788ull, 6792ull, 6796ull, 6800ull, 6804ull, 6808ull, 6812ull, 6816ull, 6820ull, 6824ull, 6828ull, 6832ull, 6836ull, 6840ull, 6844ull, 6848ull, 6852ull, 6856ull, 6860ull, 6864ull};
+const unsigned long long kQOffs34[] = {6696ull, 6696ull, 6696ull, 6696ull, 6712ull, 6712ull, 6712ull, 6712ull, 6728ull, 6728ull, 6728ull, 6728ull, 6744ull, 6744ull, 6744ull, 6744ull, 6760ull, 6760ull, 6760ull, 6760ull, 6776ull, 6776ull, 6776ull, 6776ull, 6792ull, 6792ull, 6792ull, 6792ull, 6808ull, 6808ull, 6808ull, 6808ull, 6824ull, 6824ull, 6824ull, 6824ull, 6840ull, 6840ull, 6840ull, 6840ull, 6856ull, 6856ull, 6856ull};
+const unsigned kQSubs34[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths34[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs35[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 39u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes35[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames35[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "t", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs35[] = {6872ull, 6876ull, 6880ull, 6884ull, 6888ull, 6892ull, 6896ull, 6900ull, 6904ull, 6908ull, 6912ull, 6916ull, 6920ull, 6924ull, 6928ull, 6932ull, 6936ull, 6940ull, 6944ull, 6948ull, 6952ull, 6956ull, 6960ull, 6964ull, 6968ull, 6972ull, 6976ull, 6980ull, 6984ull, 6988ull, 6992ull, 6996ull, 7000ull, 7004ull, 7008ull, 7012ull, 7016ull, 7020ull, 7024ull, 7028ull, 7032ull, 7036ull};
+const unsigned long long kQOffs35[] = {6872ull, 6872ull, 6872ull, 6872ull, 6888ull, 6888ull, 6888ull, 6888ull, 6904ull, 6904ull, 6904ull, 6904ull, 6920ull, 6920ull, 6920ull, 6920ull, 6936ull, 6936ull, 6936ull, 6936ull, 6952ull, 6952ull, 6952ull, 6952ull, 6968ull, 6968ull, 6968ull, 6968ull, 6984ull, 6984ull, 6984ull, 6984ull, 7000ull, 7000ull, 7000ull, 7000ull, 7016ull, 7016ull, 7016ull, 7016ull, 7032ull, 7032ull};
+const unsigned kQSubs35[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths35[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs36[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 34u, 35u, 39u, 40u, 61u, 69u, 70u, 71u};
 const int kQTypes36[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames36[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "depth", "d2", "t", "pid", "ct", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs36[] = {7048ull, 7052ull, 7056ull, 7060ull, 7064ull, 7068ull, 7072ull, 7076ull, 7080ull, 7084ull, 7088ull, 7092ull, 7096ull, 7100ull, 7104ull, 7108ull, 7112ull, 7116ull, 7120ull, 7124ull, 7128ull, 7132ull, 7136ull, 7140ull, 7144ull, 7148ull, 7152ull, 7156ull, 7160ull, 7164ull, 7168ull, 7172ull};
+const unsigned long long kQOffs36[] = {7048ull, 7048ull, 7048ull, 7048ull, 7064ull, 7064ull, 7064ull, 7064ull, 7080ull, 7080ull, 7080ull, 7080ull, 7096ull, 7096ull, 7096ull, 7096ull, 7112ull, 7112ull, 7112ull, 7112ull, 7128ull, 7128ull, 7128ull, 7128ull, 7144ull, 7144ull, 7144ull, 7144ull, 7160ull, 7160ull, 7160ull, 7160ull};
+const unsigned kQSubs36[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths36[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs37[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 69u, 70u, 71u};
 const int kQTypes37[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames37[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs37[] = {7184ull, 7188ull, 7192ull, 7196ull, 7200ull, 7204ull, 7208ull, 7212ull, 7216ull, 7220ull, 7224ull, 7228ull, 7232ull, 7236ull, 7240ull, 7244ull, 7248ull, 7252ull, 7256ull, 7260ull, 7264ull, 7268ull, 7272ull, 7276ull, 7280ull, 7284ull, 7288ull, 7292ull, 7296ull, 7300ull, 7304ull, 7308ull, 7312ull, 7316ull, 7320ull, 7324ull, 7328ull};
+const unsigned long long kQOffs37[] = {7184ull, 7184ull, 7184ull, 7184ull, 7200ull, 7200ull, 7200ull, 7200ull, 7216ull, 7216ull, 7216ull, 7216ull, 7232ull, 7232ull, 7232ull, 7232ull, 7248ull, 7248ull, 7248ull, 7248ull, 7264ull, 7264ull, 7264ull, 7264ull, 7280ull, 7280ull, 7280ull, 7280ull, 7296ull, 7296ull, 7296ull, 7296ull, 7312ull, 7312ull, 7312ull, 7312ull, 7328ull};
+const unsigned kQSubs37[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths37[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs38[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 69u, 70u, 71u};
 const int kQTypes38[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames38[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs38[] = {7336ull, 7340ull, 7344ull, 7348ull, 7352ull, 7356ull, 7360ull, 7364ull, 7368ull, 7372ull, 7376ull, 7380ull, 7384ull, 7388ull, 7392ull, 7396ull, 7400ull, 7404ull, 7408ull, 7412ull, 7416ull, 7420ull, 7424ull, 7428ull, 7432ull, 7436ull, 7440ull, 7444ull, 7448ull, 7452ull, 7456ull, 7460ull, 7464ull, 7468ull, 7472ull, 7476ull, 7480ull};
+const unsigned long long kQOffs38[] = {7336ull, 7336ull, 7336ull, 7336ull, 7352ull, 7352ull, 7352ull, 7352ull, 7368ull, 7368ull, 7368ull, 7368ull, 7384ull, 7384ull, 7384ull, 7384ull, 7400ull, 7400ull, 7400ull, 7400ull, 7416ull, 7416ull, 7416ull, 7416ull, 7432ull, 7432ull, 7432ull, 7432ull, 7448ull, 7448ull, 7448ull, 7448ull, 7464ull, 7464ull, 7464ull, 7464ull, 7480ull};
+const unsigned kQSubs38[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths38[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs39[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 69u, 70u, 71u};
 const int kQTypes39[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames39[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs39[] = {7488ull, 7492ull, 7496ull, 7500ull, 7504ull, 7508ull, 7512ull, 7516ull, 7520ull, 7524ull, 7528ull, 7532ull, 7536ull, 7540ull, 7544ull, 7548ull, 7552ull, 7556ull, 7560ull, 7564ull, 7568ull, 7572ull, 7576ull, 7580ull, 7584ull, 7588ull, 7592ull, 7596ull, 7600ull, 7604ull, 7608ull, 7612ull, 7616ull, 7620ull, 7624ull, 7628ull, 7632ull};
+const unsigned long long kQOffs39[] = {7488ull, 7488ull, 7488ull, 7488ull, 7504ull, 7504ull, 7504ull, 7504ull, 7520ull, 7520ull, 7520ull, 7520ull, 7536ull, 7536ull, 7536ull, 7536ull, 7552ull, 7552ull, 7552ull, 7552ull, 7568ull, 7568ull, 7568ull, 7568ull, 7584ull, 7584ull, 7584ull, 7584ull, 7600ull, 7600ull, 7600ull, 7600ull, 7616ull, 7616ull, 7616ull, 7616ull, 7632ull};
+const unsigned kQSubs39[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths39[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs40[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 69u, 70u, 71u};
 const int kQTypes40[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames40[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs40[] = {7640ull, 7644ull, 7648ull, 7652ull, 7656ull, 7660ull, 7664ull, 7668ull, 7672ull, 7676ull, 7680ull, 7684ull, 7688ull, 7692ull, 7696ull, 7700ull, 7704ull, 7708ull, 7712ull, 7716ull, 7720ull, 7724ull, 7728ull, 7732ull, 7736ull, 7740ull, 7744ull, 7748ull, 7752ull, 7756ull, 7760ull, 7764ull, 7768ull, 7772ull, 7776ull, 7780ull, 7784ull};
+const unsigned long long kQOffs40[] = {7640ull, 7640ull, 7640ull, 7640ull, 7656ull, 7656ull, 7656ull, 7656ull, 7672ull, 7672ull, 7672ull, 7672ull, 7688ull, 7688ull, 7688ull, 7688ull, 7704ull, 7704ull, 7704ull, 7704ull, 7720ull, 7720ull, 7720ull, 7720ull, 7736ull, 7736ull, 7736ull, 7736ull, 7752ull, 7752ull, 7752ull, 7752ull, 7768ull, 7768ull, 7768ull, 7768ull, 7784ull};
+const unsigned kQSubs40[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths40[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs41[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 69u, 70u, 71u};
 const int kQTypes41[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames41[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs41[] = {7792ull, 7796ull, 7800ull, 7804ull, 7808ull, 7812ull, 7816ull, 7820ull, 7824ull, 7828ull, 7832ull, 7836ull, 7840ull, 7844ull, 7848ull, 7852ull, 7856ull, 7860ull, 7864ull, 7868ull, 7872ull, 7876ull, 7880ull, 7884ull, 7888ull, 7892ull, 7896ull, 7900ull, 7904ull, 7908ull, 7912ull, 7916ull, 7920ull, 7924ull, 7928ull, 7932ull, 7936ull, 7940ull, 7944ull, 7948ull};
+const unsigned long long kQOffs41[] = {7792ull, 7792ull, 7792ull, 7792ull, 7808ull, 7808ull, 7808ull, 7808ull, 7824ull, 7824ull, 7824ull, 7824ull, 7840ull, 7840ull, 7840ull, 7840ull, 7856ull, 7856ull, 7856ull, 7856ull, 7872ull, 7872ull, 7872ull, 7872ull, 7888ull, 7888ull, 7888ull, 7888ull, 7904ull, 7904ull, 7904ull, 7904ull, 7920ull, 7920ull, 7920ull, 7920ull, 7936ull, 7936ull, 7936ull, 7936ull};
+const unsigned kQSubs41[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths41[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs42[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes42[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames42[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs42[] = {7960ull, 7964ull, 7968ull, 7972ull, 7976ull, 7980ull, 7984ull, 7988ull, 7992ull, 7996ull, 8000ull, 8004ull, 8008ull, 8012ull, 8016ull, 8020ull, 8024ull, 8028ull, 8032ull, 8036ull, 8040ull, 8044ull, 8048ull, 8052ull, 8056ull, 8060ull, 8064ull, 8068ull, 8072ull, 8076ull, 8080ull, 8084ull, 8088ull, 8092ull, 8096ull, 8100ull, 8104ull, 8108ull, 8112ull, 8116ull, 8120ull};
+const unsigned long long kQOffs42[] = {7960ull, 7960ull, 7960ull, 7960ull, 7976ull, 7976ull, 7976ull, 7976ull, 7992ull, 7992ull, 7992ull, 7992ull, 8008ull, 8008ull, 8008ull, 8008ull, 8024ull, 8024ull, 8024ull, 8024ull, 8040ull, 8040ull, 8040ull, 8040ull, 8056ull, 8056ull, 8056ull, 8056ull, 8072ull, 8072ull, 8072ull, 8072ull, 8088ull, 8088ull, 8088ull, 8088ull, 8104ull, 8104ull, 8104ull, 8104ull, 8120ull};
+const unsigned kQSubs42[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths42[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs43[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u};
 const int kQTypes43[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames43[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal"};
-const unsigned long long kQOffs43[] = {8128ull, 8132ull, 8136ull, 8140ull, 8144ull, 8148ull, 8152ull, 8156ull, 8160ull, 8164ull, 8168ull, 8172ull, 8176ull, 8180ull, 8184ull, 8188ull, 8192ull, 8196ull, 8200ull, 8204ull, 8208ull, 8212ull, 8216ull, 8220ull, 8224ull, 8228ull, 8232ull, 8236ull, 8240ull, 8244ull, 8248ull, 8252ull, 8256ull, 8260ull, 8264ull, 8268ull, 8272ull, 8276ull, 8280ull};
+const unsigned long long kQOffs43[] = {8128ull, 8128ull, 8128ull, 8128ull, 8144ull, 8144ull, 8144ull, 8144ull, 8160ull, 8160ull, 8160ull, 8160ull, 8176ull, 8176ull, 8176ull, 8176ull, 8192ull, 8192ull, 8192ull, 8192ull, 8208ull, 8208ull, 8208ull, 8208ull, 8224ull, 8224ull, 8224ull, 8224ull, 8240ull, 8240ull, 8240ull, 8240ull, 8256ull, 8256ull, 8256ull, 8256ull, 8272ull, 8272ull, 8272ull};
+const unsigned kQSubs43[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths43[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs44[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 40u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes44[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames44[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "pid", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs44[] = {8288ull, 8292ull, 8296ull, 8300ull, 8304ull, 8308ull, 8312ull, 8316ull, 8320ull, 8324ull, 8328ull, 8332ull, 8336ull, 8340ull, 8344ull, 8348ull, 8352ull, 8356ull, 8360ull, 8364ull, 8368ull, 8372ull, 8376ull, 8380ull, 8384ull, 8388ull, 8392ull, 8396ull, 8400ull, 8404ull, 8408ull, 8412ull, 8416ull, 8420ull, 8424ull, 8428ull, 8432ull, 8436ull, 8440ull, 8444ull, 8448ull};
+const unsigned long long kQOffs44[] = {8288ull, 8288ull, 8288ull, 8288ull, 8304ull, 8304ull, 8304ull, 8304ull, 8320ull, 8320ull, 8320ull, 8320ull, 8336ull, 8336ull, 8336ull, 8336ull, 8352ull, 8352ull, 8352ull, 8352ull, 8368ull, 8368ull, 8368ull, 8368ull, 8384ull, 8384ull, 8384ull, 8384ull, 8400ull, 8400ull, 8400ull, 8400ull, 8416ull, 8416ull, 8416ull, 8416ull, 8432ull, 8432ull, 8432ull, 8432ull, 8448ull};
+const unsigned kQSubs44[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths44[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs45[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 9u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes45[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames45[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "tmp1", "tmp2", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs45[] = {8456ull, 8460ull, 8464ull, 8468ull, 8472ull, 8476ull, 8480ull, 8484ull, 8488ull, 8492ull, 8496ull, 8500ull, 8504ull, 8508ull, 8512ull, 8516ull, 8520ull, 8524ull, 8528ull, 8532ull, 8536ull, 8540ull, 8544ull, 8548ull, 8552ull, 8556ull, 8560ull, 8564ull, 8568ull, 8572ull, 8576ull, 8580ull, 8584ull, 8588ull, 8592ull, 8596ull, 8600ull, 8604ull, 8608ull, 8612ull, 8616ull, 8620ull};
+const unsigned long long kQOffs45[] = {8456ull, 8456ull, 8456ull, 8456ull, 8472ull, 8472ull, 8472ull, 8472ull, 8488ull, 8488ull, 8488ull, 8488ull, 8504ull, 8504ull, 8504ull, 8504ull, 8520ull, 8520ull, 8520ull, 8520ull, 8536ull, 8536ull, 8536ull, 8536ull, 8552ull, 8552ull, 8552ull, 8552ull, 8568ull, 8568ull, 8568ull, 8568ull, 8584ull, 8584ull, 8584ull, 8584ull, 8600ull, 8600ull, 8600ull, 8600ull, 8616ull, 8616ull};
+const unsigned kQSubs45[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths45[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs46[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes46[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames46[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs46[] = {8632ull, 8636ull, 8640ull, 8644ull, 8648ull, 8652ull, 8656ull, 8660ull, 8664ull, 8668ull, 8672ull, 8676ull, 8680ull, 8684ull, 8688ull, 8692ull, 8696ull, 8700ull, 8704ull, 8708ull, 8712ull, 8716ull, 8720ull, 8724ull, 8728ull, 8732ull, 8736ull, 8740ull, 8744ull, 8748ull, 8752ull, 8756ull, 8760ull, 8764ull, 8768ull, 8772ull, 8776ull, 8780ull, 8784ull, 8788ull, 8792ull, 8796ull};
+const unsigned long long kQOffs46[] = {8632ull, 8632ull, 8632ull, 8632ull, 8648ull, 8648ull, 8648ull, 8648ull, 8664ull, 8664ull, 8664ull, 8664ull, 8680ull, 8680ull, 8680ull, 8680ull, 8696ull, 8696ull, 8696ull, 8696ull, 8712ull, 8712ull, 8712ull, 8712ull, 8728ull, 8728ull, 8728ull, 8728ull, 8744ull, 8744ull, 8744ull, 8744ull, 8760ull, 8760ull, 8760ull, 8760ull, 8776ull, 8776ull, 8776ull, 8776ull, 8792ull, 8792ull};
+const unsigned kQSubs46[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths46[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs47[] = {1u, 2u, 3u, 4u, 5u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 61u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes47[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames47[] = {"ppp", "L0", "L1", "L2", "rc", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "ct", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs47[] = {8808ull, 8812ull, 8816ull, 8820ull, 8824ull, 8828ull, 8832ull, 8836ull, 8840ull, 8844ull, 8848ull, 8852ull, 8856ull, 8860ull, 8864ull, 8868ull, 8872ull, 8876ull, 8880ull, 8884ull, 8888ull, 8892ull, 8896ull, 8900ull, 8904ull, 8908ull, 8912ull, 8916ull, 8920ull, 8924ull, 8928ull, 8932ull, 8936ull, 8940ull, 8944ull, 8948ull};
+const unsigned long long kQOffs47[] = {8808ull, 8808ull, 8808ull, 8808ull, 8824ull, 8824ull, 8824ull, 8824ull, 8840ull, 8840ull, 8840ull, 8840ull, 8856ull, 8856ull, 8856ull, 8856ull, 8872ull, 8872ull, 8872ull, 8872ull, 8888ull, 8888ull, 8888ull, 8888ull, 8904ull, 8904ull, 8904ull, 8904ull, 8920ull, 8920ull, 8920ull, 8920ull, 8936ull, 8936ull, 8936ull, 8936ull};
+const unsigned kQSubs47[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths47[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs48[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes48[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames48[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs48[] = {8960ull, 8964ull, 8968ull, 8972ull, 8976ull, 8980ull, 8984ull, 8988ull, 8992ull, 8996ull, 9000ull, 9004ull, 9008ull, 9012ull, 9016ull, 9020ull, 9024ull, 9028ull, 9032ull, 9036ull, 9040ull, 9044ull, 9048ull, 9052ull, 9056ull, 9060ull, 9064ull, 9068ull, 9072ull, 9076ull, 9080ull, 9084ull, 9088ull, 9092ull, 9096ull, 9100ull, 9104ull, 9108ull, 9112ull, 9116ull, 9120ull};
+const unsigned long long kQOffs48[] = {8960ull, 8960ull, 8960ull, 8960ull, 8976ull, 8976ull, 8976ull, 8976ull, 8992ull, 8992ull, 8992ull, 8992ull, 9008ull, 9008ull, 9008ull, 9008ull, 9024ull, 9024ull, 9024ull, 9024ull, 9040ull, 9040ull, 9040ull, 9040ull, 9056ull, 9056ull, 9056ull, 9056ull, 9072ull, 9072ull, 9072ull, 9072ull, 9088ull, 9088ull, 9088ull, 9088ull, 9104ull, 9104ull, 9104ull, 9104ull, 9120ull};
+const unsigned kQSubs48[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths48[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs49[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes49[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames49[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs49[] = {9128ull, 9132ull, 9136ull, 9140ull, 9144ull, 9148ull, 9152ull, 9156ull, 9160ull, 9164ull, 9168ull, 9172ull, 9176ull, 9180ull, 9184ull, 9188ull, 9192ull, 9196ull, 9200ull, 9204ull, 9208ull, 9212ull, 9216ull, 9220ull, 9224ull, 9228ull, 9232ull, 9236ull, 9240ull, 9244ull, 9248ull, 9252ull, 9256ull, 9260ull, 9264ull, 9268ull, 9272ull, 9276ull};
+const unsigned long long kQOffs49[] = {9128ull, 9128ull, 9128ull, 9128ull, 9144ull, 9144ull, 9144ull, 9144ull, 9160ull, 9160ull, 9160ull, 9160ull, 9176ull, 9176ull, 9176ull, 9176ull, 9192ull, 9192ull, 9192ull, 9192ull, 9208ull, 9208ull, 9208ull, 9208ull, 9224ull, 9224ull, 9224ull, 9224ull, 9240ull, 9240ull, 9240ull, 9240ull, 9256ull, 9256ull, 9256ull, 9256ull, 9272ull, 9272ull};
+const unsigned kQSubs49[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths49[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs50[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes50[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames50[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs50[] = {9288ull, 9292ull, 9296ull, 9300ull, 9304ull, 9308ull, 9312ull, 9316ull, 9320ull, 9324ull, 9328ull, 9332ull, 9336ull, 9340ull, 9344ull, 9348ull, 9352ull, 9356ull, 9360ull, 9364ull, 9368ull, 9372ull, 9376ull, 9380ull, 9384ull, 9388ull, 9392ull, 9396ull, 9400ull, 9404ull, 9408ull, 9412ull, 9416ull, 9420ull, 9424ull, 9428ull, 9432ull, 9436ull, 9440ull, 9444ull, 9448ull, 9452ull};
+const unsigned long long kQOffs50[] = {9288ull, 9288ull, 9288ull, 9288ull, 9304ull, 9304ull, 9304ull, 9304ull, 9320ull, 9320ull, 9320ull, 9320ull, 9336ull, 9336ull, 9336ull, 9336ull, 9352ull, 9352ull, 9352ull, 9352ull, 9368ull, 9368ull, 9368ull, 9368ull, 9384ull, 9384ull, 9384ull, 9384ull, 9400ull, 9400ull, 9400ull, 9400ull, 9416ull, 9416ull, 9416ull, 9416ull, 9432ull, 9432ull, 9432ull, 9432ull, 9448ull, 9448ull};
+const unsigned kQSubs50[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths50[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs51[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 38u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes51[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames51[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "u0", "u1", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "vr02", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs51[] = {9464ull, 9468ull, 9472ull, 9476ull, 9480ull, 9484ull, 9488ull, 9492ull, 9496ull, 9500ull, 9504ull, 9508ull, 9512ull, 9516ull, 9520ull, 9524ull, 9528ull, 9532ull, 9536ull, 9540ull, 9544ull, 9548ull, 9552ull, 9556ull, 9560ull, 9564ull, 9568ull, 9572ull, 9576ull, 9580ull, 9584ull, 9588ull, 9592ull, 9596ull, 9600ull, 9604ull, 9608ull, 9612ull, 9616ull, 9620ull, 9624ull, 9628ull, 9632ull, 9636ull, 9640ull};
+const unsigned long long kQOffs51[] = {9464ull, 9464ull, 9464ull, 9464ull, 9480ull, 9480ull, 9480ull, 9480ull, 9496ull, 9496ull, 9496ull, 9496ull, 9512ull, 9512ull, 9512ull, 9512ull, 9528ull, 9528ull, 9528ull, 9528ull, 9544ull, 9544ull, 9544ull, 9544ull, 9560ull, 9560ull, 9560ull, 9560ull, 9576ull, 9576ull, 9576ull, 9576ull, 9592ull, 9592ull, 9592ull, 9592ull, 9608ull, 9608ull, 9608ull, 9608ull, 9624ull, 9624ull, 9624ull, 9624ull, 9640ull};
+const unsigned kQSubs51[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths51[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs52[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 8u, 10u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 36u, 37u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes52[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames52[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "tmp1", "c0", "c1", "pp0", "pp1", "tmp0", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "vr00", "vr01", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs52[] = {9648ull, 9652ull, 9656ull, 9660ull, 9664ull, 9668ull, 9672ull, 9676ull, 9680ull, 9684ull, 9688ull, 9692ull, 9696ull, 9700ull, 9704ull, 9708ull, 9712ull, 9716ull, 9720ull, 9724ull, 9728ull, 9732ull, 9736ull, 9740ull, 9744ull, 9748ull, 9752ull, 9756ull, 9760ull, 9764ull, 9768ull, 9772ull, 9776ull, 9780ull, 9784ull, 9788ull, 9792ull, 9796ull, 9800ull, 9804ull, 9808ull, 9812ull, 9816ull, 9820ull};
+const unsigned long long kQOffs52[] = {9648ull, 9648ull, 9648ull, 9648ull, 9664ull, 9664ull, 9664ull, 9664ull, 9680ull, 9680ull, 9680ull, 9680ull, 9696ull, 9696ull, 9696ull, 9696ull, 9712ull, 9712ull, 9712ull, 9712ull, 9728ull, 9728ull, 9728ull, 9728ull, 9744ull, 9744ull, 9744ull, 9744ull, 9760ull, 9760ull, 9760ull, 9760ull, 9776ull, 9776ull, 9776ull, 9776ull, 9792ull, 9792ull, 9792ull, 9792ull, 9808ull, 9808ull, 9808ull, 9808ull};
+const unsigned kQSubs52[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths52[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs53[] = {1u, 2u, 3u, 4u, 5u, 6u, 7u, 10u, 11u, 12u, 13u, 15u, 16u, 17u, 19u, 22u, 23u, 24u, 25u, 26u, 27u, 28u, 29u, 30u, 31u, 32u, 33u, 34u, 35u, 61u, 62u, 63u, 64u, 65u, 66u, 67u, 68u, 69u, 70u, 71u};
 const int kQTypes53[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames53[] = {"ppp", "L0", "L1", "L2", "rc", "d0", "d1", "c0", "c1", "pp0", "pp1", "pw", "mean", "m2", "ns", "o0", "o1", "o2", "TP0", "TP1", "TP2", "SL0", "SL1", "SL2", "clr0", "clr1", "clr2", "depth", "d2", "ct", "t0", "t1", "t2", "n0", "n1", "n2", "metal", "wi0", "wi1", "wi2"};
-const unsigned long long kQOffs53[] = {9832ull, 9836ull, 9840ull, 9844ull, 9848ull, 9852ull, 9856ull, 9860ull, 9864ull, 9868ull, 9872ull, 9876ull, 9880ull, 9884ull, 9888ull, 9892ull, 9896ull, 9900ull, 9904ull, 9908ull, 9912ull, 9916ull, 9920ull, 9924ull, 9928ull, 9932ull, 9936ull, 9940ull, 9944ull, 9948ull, 9952ull, 9956ull, 9960ull, 9964ull, 9968ull, 9972ull, 9976ull, 9980ull, 9984ull, 9988ull};
+const unsigned long long kQOffs53[] = {9832ull, 9832ull, 9832ull, 9832ull, 9848ull, 9848ull, 9848ull, 9848ull, 9864ull, 9864ull, 9864ull, 9864ull, 9880ull, 9880ull, 9880ull, 9880ull, 9896ull, 9896ull, 9896ull, 9896ull, 9912ull, 9912ull, 9912ull, 9912ull, 9928ull, 9928ull, 9928ull, 9928ull, 9944ull, 9944ull, 9944ull, 9944ull, 9960ull, 9960ull, 9960ull, 9960ull, 9976ull, 9976ull, 9976ull, 9976ull};
+const unsigned kQSubs53[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths53[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs54[] = {1u, 2u, 3u, 4u, 5u, 19u};
 const int kQTypes54[] = {LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames54[] = {"ppp", "L0", "L1", "L2", "rc", "ns"};
-const unsigned long long kQOffs54[] = {10000ull, 10004ull, 10008ull, 10012ull, 10016ull, 10020ull};
+const unsigned long long kQOffs54[] = {10000ull, 10000ull, 10000ull, 10000ull, 10016ull, 10016ull};
+const unsigned kQSubs54[] = {0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths54[] = {16u, 16u, 16u, 16u, 16u, 16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 27u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 41u, kQRegs1, kQTypes1, kQNames1},
@@ -7406,61 +10946,61 @@ const loom_b200_queue_layout kQueues[] = {
     {54u, -1, 6u, kQRegs54, kQTypes54, kQNames54},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 108ull},
-    {kQOffs1, 276ull},
-    {kQOffs2, 460ull},
-    {kQOffs3, 572ull},
-    {kQOffs4, 740ull},
-    {kQOffs5, 920ull},
-    {kQOffs6, 1168ull},
-    {kQOffs7, 1408ull},
-    {kQOffs8, 1648ull},
-    {kQOffs9, 1880ull},
-    {kQOffs10, 2140ull},
-    {kQOffs11, 2384ull},
-    {kQOffs12, 2604ull},
-    {kQOffs13, 2788ull},
-    {kQOffs14, 2964ull},
-    {kQOffs15, 3192ull},
-    {kQOffs16, 3416ull},
-    {kQOffs17, 3624ull},
-    {kQOffs18, 3812ull},
-    {kQOffs19, 3988ull},
-    {kQOffs20, 4184ull},
-    {kQOffs21, 4380ull},
-    {kQOffs22, 4572ull},
-    {kQOffs23, 4768ull},
-    {kQOffs24, 4968ull},
-    {kQOffs25, 5164ull},
-    {kQOffs26, 5352ull},
-    {kQOffs27, 5544ull},
-    {kQOffs28, 5732ull},
-    {kQOffs29, 5908ull},
-    {kQOffs30, 6096ull},
-    {kQOffs31, 6304ull},
-    {kQOffs32, 6504ull},
-    {kQOffs33, 6692ull},
-    {kQOffs34, 6868ull},
-    {kQOffs35, 7040ull},
-    {kQOffs36, 7176ull},
-    {kQOffs37, 7332ull},
-    {kQOffs38, 7484ull},
-    {kQOffs39, 7636ull},
-    {kQOffs40, 7788ull},
-    {kQOffs41, 7952ull},
-    {kQOffs42, 8124ull},
-    {kQOffs43, 8284ull},
-    {kQOffs44, 8452ull},
-    {kQOffs45, 8624ull},
-    {kQOffs46, 8800ull},
-    {kQOffs47, 8952ull},
-    {kQOffs48, 9124ull},
-    {kQOffs49, 9280ull},
-    {kQOffs50, 9456ull},
-    {kQOffs51, 9644ull},
-    {kQOffs52, 9824ull},
-    {kQOffs53, 9992ull},
-    {kQOffs54, 10024ull},
+    {kQOffs0, kQSubs0, kQWidths0, 96ull, 12u, 16u},
+    {kQOffs1, kQSubs1, kQWidths1, 272ull, 4u, 8u},
+    {kQOffs2, kQSubs2, kQWidths2, 456ull, 4u, 8u},
+    {kQOffs3, kQSubs3, kQWidths3, 560ull, 12u, 16u},
+    {kQOffs4, kQSubs4, kQWidths4, 736ull, 4u, 8u},
+    {kQOffs5, kQSubs5, kQWidths5, 920ull, 0u, 4u},
+    {kQOffs6, kQSubs6, kQWidths6, 1168ull, 0u, 4u},
+    {kQOffs7, kQSubs7, kQWidths7, 1400ull, 8u, 16u},
+    {kQOffs8, kQSubs8, kQWidths8, 1640ull, 8u, 16u},
+    {kQOffs9, kQSubs9, kQWidths9, 1880ull, 0u, 4u},
+    {kQOffs10, kQSubs10, kQWidths10, 2128ull, 12u, 16u},
+    {kQOffs11, kQSubs11, kQWidths11, 2384ull, 0u, 4u},
+    {kQOffs12, kQSubs12, kQWidths12, 2600ull, 4u, 8u},
+    {kQOffs13, kQSubs13, kQWidths13, 2784ull, 4u, 8u},
+    {kQOffs14, kQSubs14, kQWidths14, 2952ull, 12u, 16u},
+    {kQOffs15, kQSubs15, kQWidths15, 3192ull, 0u, 4u},
+    {kQOffs16, kQSubs16, kQWidths16, 3408ull, 8u, 16u},
+    {kQOffs17, kQSubs17, kQWidths17, 3616ull, 8u, 16u},
+    {kQOffs18, kQSubs18, kQWidths18, 3808ull, 4u, 8u},
+    {kQOffs19, kQSubs19, kQWidths19, 3976ull, 12u, 16u},
+    {kQOffs20, kQSubs20, kQWidths20, 4184ull, 0u, 4u},
+    {kQOffs21, kQSubs21, kQWidths21, 4368ull, 12u, 16u},
+    {kQOffs22, kQSubs22, kQWidths22, 4560ull, 12u, 16u},
+    {kQOffs23, kQSubs23, kQWidths23, 4768ull, 0u, 4u},
+    {kQOffs24, kQSubs24, kQWidths24, 4968ull, 0u, 4u},
+    {kQOffs25, kQSubs25, kQWidths25, 5152ull, 12u, 16u},
+    {kQOffs26, kQSubs26, kQWidths26, 5344ull, 8u, 16u},
+    {kQOffs27, kQSubs27, kQWidths27, 5536ull, 8u, 16u},
+    {kQOffs28, kQSubs28, kQWidths28, 5728ull, 4u, 8u},
+    {kQOffs29, kQSubs29, kQWidths29, 5896ull, 12u, 16u},
+    {kQOffs30, kQSubs30, kQWidths30, 6088ull, 8u, 16u},
+    {kQOffs31, kQSubs31, kQWidths31, 6296ull, 8u, 16u},
+    {kQOffs32, kQSubs32, kQWidths32, 6504ull, 0u, 4u},
+    {kQOffs33, kQSubs33, kQWidths33, 6688ull, 4u, 8u},
+    {kQOffs34, kQSubs34, kQWidths34, 6856ull, 12u, 16u},
+    {kQOffs35, kQSubs35, kQWidths35, 7032ull, 8u, 16u},
+    {kQOffs36, kQSubs36, kQWidths36, 7176ull, 0u, 4u},
+    {kQOffs37, kQSubs37, kQWidths37, 7328ull, 4u, 8u},
+    {kQOffs38, kQSubs38, kQWidths38, 7480ull, 4u, 8u},
+    {kQOffs39, kQSubs39, kQWidths39, 7632ull, 4u, 8u},
+    {kQOffs40, kQSubs40, kQWidths40, 7784ull, 4u, 8u},
+    {kQOffs41, kQSubs41, kQWidths41, 7952ull, 0u, 4u},
+    {kQOffs42, kQSubs42, kQWidths42, 8120ull, 4u, 8u},
+    {kQOffs43, kQSubs43, kQWidths43, 8272ull, 12u, 16u},
+    {kQOffs44, kQSubs44, kQWidths44, 8448ull, 4u, 8u},
+    {kQOffs45, kQSubs45, kQWidths45, 8616ull, 8u, 16u},
+    {kQOffs46, kQSubs46, kQWidths46, 8792ull, 8u, 16u},
+    {kQOffs47, kQSubs47, kQWidths47, 8952ull, 0u, 4u},
+    {kQOffs48, kQSubs48, kQWidths48, 9120ull, 4u, 8u},
+    {kQOffs49, kQSubs49, kQWidths49, 9272ull, 8u, 16u},
+    {kQOffs50, kQSubs50, kQWidths50, 9448ull, 8u, 16u},
+    {kQOffs51, kQSubs51, kQWidths51, 9640ull, 4u, 8u},
+    {kQOffs52, kQSubs52, kQWidths52, 9824ull, 0u, 4u},
+    {kQOffs53, kQSubs53, kQWidths53, 9992ull, 0u, 4u},
+    {kQOffs54, kQSubs54, kQWidths54, 10016ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

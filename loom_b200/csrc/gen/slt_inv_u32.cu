@@ -142,9 +142,15 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<unsigned*>(base + 4ull * cap)[idx] = tid;
+        {
+            {
+                uint2 v0;
+                v0.x = bitcast<unsigned>(R.r0);
+                v0.y = tid;
+                reinterpret_cast<uint2*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -157,8 +163,11 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 4ull * cap)[idx];
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<unsigned int>(v0.x);
+            return v0.y;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -180,11 +189,13 @@ const uint32_t kQRegs0[] = {0u};
 const int kQTypes0[] = {LOOM_B200_U32};
 const char* const kQNames0[] = {"i"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {8u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 4ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 4u, 8u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

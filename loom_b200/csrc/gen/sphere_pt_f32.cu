@@ -1038,759 +1038,1543 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<unsigned int*>(base + 0ull * cap)[idx] = R.r1;
-            reinterpret_cast<unsigned int*>(base + 4ull * cap)[idx] = R.r2;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r1);
+                v0.y = bitcast<unsigned>(R.r2);
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         case 1: // prim
-            reinterpret_cast<unsigned int*>(base + 16ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 20ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 24ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 28ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 32ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 36ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 40ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 44ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 48ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 52ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 56ull * cap)[idx] = R.r21;
-            reinterpret_cast<unsigned int*>(base + 60ull * cap)[idx] = R.r22;
-            reinterpret_cast<unsigned int*>(base + 64ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 68ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 72ull * cap)[idx] = R.r25;
-            reinterpret_cast<unsigned int*>(base + 76ull * cap)[idx] = R.r130;
-            reinterpret_cast<unsigned int*>(base + 80ull * cap)[idx] = R.r131;
-            reinterpret_cast<unsigned*>(base + 84ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r7);
+                v0.y = bitcast<unsigned>(R.r9);
+                v0.z = bitcast<unsigned>(R.r11);
+                v0.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 16ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r13);
+                v1.y = bitcast<unsigned>(R.r14);
+                v1.z = bitcast<unsigned>(R.r15);
+                v1.w = bitcast<unsigned>(R.r16);
+                reinterpret_cast<uint4*>(base + 32ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r17);
+                v2.y = bitcast<unsigned>(R.r20);
+                v2.z = bitcast<unsigned>(R.r21);
+                v2.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 48ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r23);
+                v3.y = bitcast<unsigned>(R.r24);
+                v3.z = bitcast<unsigned>(R.r25);
+                v3.w = bitcast<unsigned>(R.r130);
+                reinterpret_cast<uint4*>(base + 64ull * cap)[idx] = v3;
+            }
+            {
+                uint2 v4;
+                v4.x = bitcast<unsigned>(R.r131);
+                v4.y = tid;
+                reinterpret_cast<uint2*>(base + 80ull * cap)[idx] = v4;
+            }
             return;
+        }
         case 2: // bounce
-            reinterpret_cast<float*>(base + 88ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 92ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 96ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 100ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 104ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 108ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 112ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 116ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 120ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 124ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 128ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 132ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 136ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 140ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 144ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 148ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 152ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 156ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 160ull * cap)[idx] = R.r52;
-            reinterpret_cast<unsigned*>(base + 164ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 88ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 104ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 120ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 136ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = tid;
+                reinterpret_cast<uint4*>(base + 152ull * cap)[idx] = v4;
+            }
             return;
+        }
         case 3: // isect
-            reinterpret_cast<float*>(base + 168ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 172ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 176ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 180ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 184ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 188ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 192ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 196ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 200ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 204ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 208ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 212ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 216ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 220ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 224ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 228ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 232ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 236ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 240ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 244ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned int*>(base + 248ull * cap)[idx] = R.r54;
-            reinterpret_cast<unsigned int*>(base + 252ull * cap)[idx] = R.r55;
-            reinterpret_cast<unsigned int*>(base + 256ull * cap)[idx] = R.r56;
-            reinterpret_cast<unsigned*>(base + 260ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 168ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 184ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 200ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 216ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 232ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r54);
+                v5.y = bitcast<unsigned>(R.r55);
+                v5.z = bitcast<unsigned>(R.r56);
+                v5.w = tid;
+                reinterpret_cast<uint4*>(base + 248ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 4: // shade
-            reinterpret_cast<float*>(base + 264ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 268ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 272ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 276ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 280ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 284ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 288ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 292ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 296ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 300ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 304ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 308ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 312ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 316ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 320ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 324ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 328ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 332ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 336ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 340ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned int*>(base + 344ull * cap)[idx] = R.r54;
-            reinterpret_cast<unsigned*>(base + 348ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 264ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 280ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 296ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 312ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 328ull * cap)[idx] = v4;
+            }
+            {
+                uint2 v5;
+                v5.x = bitcast<unsigned>(R.r54);
+                v5.y = tid;
+                reinterpret_cast<uint2*>(base + 344ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 5: // hitp
-            reinterpret_cast<float*>(base + 352ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 356ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 360ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 364ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 368ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 372ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 376ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 380ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 384ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 388ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 392ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 396ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 400ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 404ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 408ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 412ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 416ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 420ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 424ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 428ull * cap)[idx] = R.r53;
-            reinterpret_cast<unsigned int*>(base + 432ull * cap)[idx] = R.r54;
-            reinterpret_cast<unsigned*>(base + 436ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 352ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 368ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 384ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 400ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r53);
+                reinterpret_cast<uint4*>(base + 416ull * cap)[idx] = v4;
+            }
+            {
+                uint2 v5;
+                v5.x = bitcast<unsigned>(R.r54);
+                v5.y = tid;
+                reinterpret_cast<uint2*>(base + 432ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 6: // emit
-            reinterpret_cast<float*>(base + 440ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 444ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 448ull * cap)[idx] = R.r5;
-            reinterpret_cast<float*>(base + 452ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 456ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 460ull * cap)[idx] = R.r51;
-            reinterpret_cast<float*>(base + 464ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 468ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 472ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned*>(base + 476ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 440ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r50);
+                v1.y = bitcast<unsigned>(R.r51);
+                v1.z = bitcast<unsigned>(R.r76);
+                v1.w = bitcast<unsigned>(R.r77);
+                reinterpret_cast<uint4*>(base + 456ull * cap)[idx] = v1;
+            }
+            {
+                uint2 v2;
+                v2.x = bitcast<unsigned>(R.r78);
+                v2.y = tid;
+                reinterpret_cast<uint2*>(base + 472ull * cap)[idx] = v2;
+            }
             return;
+        }
         case 7: // surf
-            reinterpret_cast<float*>(base + 480ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 484ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 488ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 492ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 496ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 500ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 504ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 508ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 512ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 516ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 520ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 524ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 528ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 532ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 536ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 540ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 544ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 548ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 552ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 556ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 560ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 564ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 568ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 572ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 576ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 580ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned*>(base + 584ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 480ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 496ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 512ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 528ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 544ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 560ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = tid;
+                reinterpret_cast<uint4*>(base + 576ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 8: // rrchk
-            reinterpret_cast<float*>(base + 592ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 596ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 600ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 604ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 608ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 612ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 616ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 620ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 624ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 628ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 632ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 636ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 640ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 644ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 648ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 652ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 656ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 660ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 664ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 668ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 672ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 676ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 680ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 684ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 688ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 692ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned*>(base + 696ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 592ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 608ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 624ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 640ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 656ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 672ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = tid;
+                reinterpret_cast<uint4*>(base + 688ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 9: // rr_roll
-            reinterpret_cast<float*>(base + 704ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 708ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 712ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 716ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 720ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 724ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 728ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 732ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 736ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 740ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 744ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 748ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 752ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 756ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 760ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 764ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 768ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 772ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 776ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 780ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 784ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 788ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 792ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 796ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 800ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 804ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned*>(base + 808ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 704ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 720ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 736ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 752ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 768ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 784ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = tid;
+                reinterpret_cast<uint4*>(base + 800ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 10: // rr
-            reinterpret_cast<float*>(base + 816ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 820ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 824ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 828ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 832ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 836ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 840ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 844ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 848ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 852ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 856ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 860ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 864ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 868ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 872ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 876ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 880ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 884ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 888ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 892ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 896ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 900ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 904ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 908ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 912ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 916ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned int*>(base + 920ull * cap)[idx] = R.r130;
-            reinterpret_cast<unsigned*>(base + 924ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 816ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 832ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 848ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 864ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 880ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 896ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = bitcast<unsigned>(R.r130);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 912ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 11: // rr_keep
-            reinterpret_cast<float*>(base + 928ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 932ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 936ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 940ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 944ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 948ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 952ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 956ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 960ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 964ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 968ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 972ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 976ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 980ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 984ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 988ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 992ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 996ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 1000ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 1004ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 1008ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 1012ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 1016ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 1020ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1024ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1028ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 1032ull * cap)[idx] = R.r86;
-            reinterpret_cast<unsigned*>(base + 1036ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 928ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 944ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 960ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 976ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 992ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1008ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = bitcast<unsigned>(R.r86);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 1024ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 12: // scatter
-            reinterpret_cast<float*>(base + 1040ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1044ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1048ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1052ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1056ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1060ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1064ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1068ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1072ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1076ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1080ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1084ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1088ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1092ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1096ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1100ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1104ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 1108ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 1112ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 1116ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 1120ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 1124ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 1128ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 1132ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1136ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1140ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned*>(base + 1144ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1040ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1056ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1072ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 1088ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 1104ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1120ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = tid;
+                reinterpret_cast<uint4*>(base + 1136ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 13: // mirror
-            reinterpret_cast<float*>(base + 1152ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1156ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1160ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1164ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1168ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1172ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1176ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1180ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1184ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1188ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1192ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1196ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1200ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1204ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1208ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1212ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1216ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1220ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1224ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1228ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1232ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1236ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 1240ull * cap)[idx] = R.r87;
-            reinterpret_cast<unsigned*>(base + 1244ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1152ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1168ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1184ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 1200ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1216ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = tid;
+                reinterpret_cast<uint4*>(base + 1232ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 14: // diffuse
-            reinterpret_cast<float*>(base + 1248ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1252ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1256ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1260ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1264ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1268ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1272ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1276ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1280ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1284ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1288ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1292ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1296ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1300ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1304ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1308ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1312ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 1316ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 1320ull * cap)[idx] = R.r94;
-            reinterpret_cast<unsigned*>(base + 1324ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1248ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1264ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1280ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 1296ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r92);
+                v4.y = bitcast<unsigned>(R.r93);
+                v4.z = bitcast<unsigned>(R.r94);
+                v4.w = tid;
+                reinterpret_cast<uint4*>(base + 1312ull * cap)[idx] = v4;
+            }
             return;
+        }
         case 15: // disk_roll
-            reinterpret_cast<float*>(base + 1328ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1332ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1336ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1340ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1344ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1348ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1352ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1356ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1360ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1364ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1368ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1372ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1376ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1380ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1384ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1388ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1392ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 1396ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 1400ull * cap)[idx] = R.r94;
-            reinterpret_cast<float*>(base + 1404ull * cap)[idx] = R.r100;
-            reinterpret_cast<float*>(base + 1408ull * cap)[idx] = R.r101;
-            reinterpret_cast<float*>(base + 1412ull * cap)[idx] = R.r102;
-            reinterpret_cast<float*>(base + 1416ull * cap)[idx] = R.r103;
-            reinterpret_cast<float*>(base + 1420ull * cap)[idx] = R.r104;
-            reinterpret_cast<float*>(base + 1424ull * cap)[idx] = R.r105;
-            reinterpret_cast<unsigned*>(base + 1428ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1328ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1344ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1360ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 1376ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r92);
+                v4.y = bitcast<unsigned>(R.r93);
+                v4.z = bitcast<unsigned>(R.r94);
+                v4.w = bitcast<unsigned>(R.r100);
+                reinterpret_cast<uint4*>(base + 1392ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r101);
+                v5.y = bitcast<unsigned>(R.r102);
+                v5.z = bitcast<unsigned>(R.r103);
+                v5.w = bitcast<unsigned>(R.r104);
+                reinterpret_cast<uint4*>(base + 1408ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r105);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 1424ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 16: // disk
-            reinterpret_cast<float*>(base + 1432ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1436ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1440ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1444ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1448ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1452ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1456ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1460ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1464ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1468ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1472ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1476ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1480ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1484ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1488ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1492ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1496ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 1500ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 1504ull * cap)[idx] = R.r94;
-            reinterpret_cast<float*>(base + 1508ull * cap)[idx] = R.r100;
-            reinterpret_cast<float*>(base + 1512ull * cap)[idx] = R.r101;
-            reinterpret_cast<float*>(base + 1516ull * cap)[idx] = R.r102;
-            reinterpret_cast<float*>(base + 1520ull * cap)[idx] = R.r103;
-            reinterpret_cast<float*>(base + 1524ull * cap)[idx] = R.r104;
-            reinterpret_cast<float*>(base + 1528ull * cap)[idx] = R.r105;
-            reinterpret_cast<unsigned int*>(base + 1532ull * cap)[idx] = R.r130;
-            reinterpret_cast<unsigned int*>(base + 1536ull * cap)[idx] = R.r131;
-            reinterpret_cast<unsigned*>(base + 1540ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1432ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1448ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1464ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 1480ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r92);
+                v4.y = bitcast<unsigned>(R.r93);
+                v4.z = bitcast<unsigned>(R.r94);
+                v4.w = bitcast<unsigned>(R.r100);
+                reinterpret_cast<uint4*>(base + 1496ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r101);
+                v5.y = bitcast<unsigned>(R.r102);
+                v5.z = bitcast<unsigned>(R.r103);
+                v5.w = bitcast<unsigned>(R.r104);
+                reinterpret_cast<uint4*>(base + 1512ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r105);
+                v6.y = bitcast<unsigned>(R.r130);
+                v6.z = bitcast<unsigned>(R.r131);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 1528ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 17: // disk_ok
-            reinterpret_cast<float*>(base + 1544ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1548ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1552ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1556ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1560ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1564ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1568ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1572ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1576ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1580ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1584ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1588ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1592ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1596ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1600ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1604ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1608ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 1612ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 1616ull * cap)[idx] = R.r94;
-            reinterpret_cast<float*>(base + 1620ull * cap)[idx] = R.r100;
-            reinterpret_cast<float*>(base + 1624ull * cap)[idx] = R.r101;
-            reinterpret_cast<float*>(base + 1628ull * cap)[idx] = R.r102;
-            reinterpret_cast<float*>(base + 1632ull * cap)[idx] = R.r103;
-            reinterpret_cast<float*>(base + 1636ull * cap)[idx] = R.r104;
-            reinterpret_cast<float*>(base + 1640ull * cap)[idx] = R.r105;
-            reinterpret_cast<float*>(base + 1644ull * cap)[idx] = R.r106;
-            reinterpret_cast<float*>(base + 1648ull * cap)[idx] = R.r107;
-            reinterpret_cast<float*>(base + 1652ull * cap)[idx] = R.r108;
-            reinterpret_cast<unsigned*>(base + 1656ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1544ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1560ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 1576ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 1592ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r92);
+                v4.y = bitcast<unsigned>(R.r93);
+                v4.z = bitcast<unsigned>(R.r94);
+                v4.w = bitcast<unsigned>(R.r100);
+                reinterpret_cast<uint4*>(base + 1608ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r101);
+                v5.y = bitcast<unsigned>(R.r102);
+                v5.z = bitcast<unsigned>(R.r103);
+                v5.w = bitcast<unsigned>(R.r104);
+                reinterpret_cast<uint4*>(base + 1624ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r105);
+                v6.y = bitcast<unsigned>(R.r106);
+                v6.z = bitcast<unsigned>(R.r107);
+                v6.w = bitcast<unsigned>(R.r108);
+                reinterpret_cast<uint4*>(base + 1640ull * cap)[idx] = v6;
+            }
+            {
+                unsigned v7;
+                v7 = tid;
+                reinterpret_cast<unsigned*>(base + 1656ull * cap)[idx] = v7;
+            }
             return;
+        }
         case 18: // glass
-            reinterpret_cast<float*>(base + 1664ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1668ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1672ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1676ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1680ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1684ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1688ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1692ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1696ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1700ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1704ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1708ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1712ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1716ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1720ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1724ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1728ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1732ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1736ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1740ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1744ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1748ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 1752ull * cap)[idx] = R.r87;
-            reinterpret_cast<unsigned int*>(base + 1756ull * cap)[idx] = R.r88;
-            reinterpret_cast<float*>(base + 1760ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 1764ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 1768ull * cap)[idx] = R.r94;
-            reinterpret_cast<unsigned*>(base + 1772ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1664ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1680ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1696ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 1712ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1728ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = bitcast<unsigned>(R.r88);
+                reinterpret_cast<uint4*>(base + 1744ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r92);
+                v6.y = bitcast<unsigned>(R.r93);
+                v6.z = bitcast<unsigned>(R.r94);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 1760ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 19: // refr
-            reinterpret_cast<float*>(base + 1776ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1780ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1784ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1788ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1792ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1796ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1800ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1804ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1808ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1812ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1816ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1820ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1824ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1828ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1832ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1836ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1840ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1844ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1848ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1852ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1856ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1860ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 1864ull * cap)[idx] = R.r87;
-            reinterpret_cast<unsigned int*>(base + 1868ull * cap)[idx] = R.r88;
-            reinterpret_cast<float*>(base + 1872ull * cap)[idx] = R.r111;
-            reinterpret_cast<float*>(base + 1876ull * cap)[idx] = R.r112;
-            reinterpret_cast<float*>(base + 1880ull * cap)[idx] = R.r113;
-            reinterpret_cast<unsigned*>(base + 1884ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1776ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1792ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1808ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 1824ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1840ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = bitcast<unsigned>(R.r88);
+                reinterpret_cast<uint4*>(base + 1856ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r111);
+                v6.y = bitcast<unsigned>(R.r112);
+                v6.z = bitcast<unsigned>(R.r113);
+                v6.w = tid;
+                reinterpret_cast<uint4*>(base + 1872ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 20: // fres
-            reinterpret_cast<float*>(base + 1888ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 1892ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 1896ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 1900ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 1904ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 1908ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 1912ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 1916ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 1920ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 1924ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 1928ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 1932ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 1936ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 1940ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 1944ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 1948ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 1952ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 1956ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 1960ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 1964ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 1968ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 1972ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 1976ull * cap)[idx] = R.r87;
-            reinterpret_cast<float*>(base + 1980ull * cap)[idx] = R.r117;
-            reinterpret_cast<float*>(base + 1984ull * cap)[idx] = R.r118;
-            reinterpret_cast<float*>(base + 1988ull * cap)[idx] = R.r119;
-            reinterpret_cast<float*>(base + 1992ull * cap)[idx] = R.r127;
-            reinterpret_cast<float*>(base + 1996ull * cap)[idx] = R.r128;
-            reinterpret_cast<float*>(base + 2000ull * cap)[idx] = R.r129;
-            reinterpret_cast<unsigned int*>(base + 2004ull * cap)[idx] = R.r130;
-            reinterpret_cast<unsigned*>(base + 2008ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 1888ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 1904ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 1920ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 1936ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 1952ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = bitcast<unsigned>(R.r117);
+                reinterpret_cast<uint4*>(base + 1968ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r118);
+                v6.y = bitcast<unsigned>(R.r119);
+                v6.z = bitcast<unsigned>(R.r127);
+                v6.w = bitcast<unsigned>(R.r128);
+                reinterpret_cast<uint4*>(base + 1984ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r129);
+                v7.y = bitcast<unsigned>(R.r130);
+                v7.z = tid;
+                reinterpret_cast<uint4*>(base + 2000ull * cap)[idx] = v7;
+            }
             return;
+        }
         case 21: // take_refl
-            reinterpret_cast<float*>(base + 2016ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2020ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2024ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2028ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2032ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2036ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2040ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2044ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2048ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2052ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 2056ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 2060ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 2064ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2068ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 2072ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 2076ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2080ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2084ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2088ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2092ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 2096ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 2100ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 2104ull * cap)[idx] = R.r87;
-            reinterpret_cast<float*>(base + 2108ull * cap)[idx] = R.r128;
-            reinterpret_cast<unsigned*>(base + 2112ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 2016ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2032ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2048ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 2064ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 2080ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = bitcast<unsigned>(R.r128);
+                reinterpret_cast<uint4*>(base + 2096ull * cap)[idx] = v5;
+            }
+            {
+                unsigned v6;
+                v6 = tid;
+                reinterpret_cast<unsigned*>(base + 2112ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 22: // take_refr
-            reinterpret_cast<float*>(base + 2120ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2124ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2128ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2132ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2136ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2140ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2144ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2148ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2152ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2156ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2160ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 2164ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 2168ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2172ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2176ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2180ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2184ull * cap)[idx] = R.r117;
-            reinterpret_cast<float*>(base + 2188ull * cap)[idx] = R.r118;
-            reinterpret_cast<float*>(base + 2192ull * cap)[idx] = R.r119;
-            reinterpret_cast<float*>(base + 2196ull * cap)[idx] = R.r129;
-            reinterpret_cast<unsigned*>(base + 2200ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 2120ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2136ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 2152ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 2168ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r117);
+                v4.y = bitcast<unsigned>(R.r118);
+                v4.z = bitcast<unsigned>(R.r119);
+                v4.w = bitcast<unsigned>(R.r129);
+                reinterpret_cast<uint4*>(base + 2184ull * cap)[idx] = v4;
+            }
+            {
+                unsigned v5;
+                v5 = tid;
+                reinterpret_cast<unsigned*>(base + 2200ull * cap)[idx] = v5;
+            }
             return;
+        }
         case 23: // roll
-            reinterpret_cast<float*>(base + 2208ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2212ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2216ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2220ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2224ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 2228ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2232ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2236ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2240ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2244ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2248ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2252ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2256ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 2260ull * cap)[idx] = R.r21;
-            reinterpret_cast<unsigned int*>(base + 2264ull * cap)[idx] = R.r22;
-            reinterpret_cast<unsigned int*>(base + 2268ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2272ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2276ull * cap)[idx] = R.r25;
-            reinterpret_cast<unsigned int*>(base + 2280ull * cap)[idx] = R.r26;
-            reinterpret_cast<float*>(base + 2284ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 2288ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 2292ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 2296ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2300ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 2304ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 2308ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2312ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2316ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2320ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2324ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 2328ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 2332ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 2336ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 2340ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 2344ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 2348ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 2352ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 2356ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 2360ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 2364ull * cap)[idx] = R.r87;
-            reinterpret_cast<float*>(base + 2368ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 2372ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 2376ull * cap)[idx] = R.r94;
-            reinterpret_cast<float*>(base + 2380ull * cap)[idx] = R.r100;
-            reinterpret_cast<float*>(base + 2384ull * cap)[idx] = R.r101;
-            reinterpret_cast<float*>(base + 2388ull * cap)[idx] = R.r102;
-            reinterpret_cast<float*>(base + 2392ull * cap)[idx] = R.r103;
-            reinterpret_cast<float*>(base + 2396ull * cap)[idx] = R.r104;
-            reinterpret_cast<float*>(base + 2400ull * cap)[idx] = R.r105;
-            reinterpret_cast<float*>(base + 2404ull * cap)[idx] = R.r117;
-            reinterpret_cast<float*>(base + 2408ull * cap)[idx] = R.r118;
-            reinterpret_cast<float*>(base + 2412ull * cap)[idx] = R.r119;
-            reinterpret_cast<float*>(base + 2416ull * cap)[idx] = R.r127;
-            reinterpret_cast<float*>(base + 2420ull * cap)[idx] = R.r128;
-            reinterpret_cast<float*>(base + 2424ull * cap)[idx] = R.r129;
-            reinterpret_cast<unsigned*>(base + 2428ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r7);
+                reinterpret_cast<uint4*>(base + 2208ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r9);
+                v1.y = bitcast<unsigned>(R.r11);
+                v1.z = bitcast<unsigned>(R.r12);
+                v1.w = bitcast<unsigned>(R.r13);
+                reinterpret_cast<uint4*>(base + 2224ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r14);
+                v2.y = bitcast<unsigned>(R.r15);
+                v2.z = bitcast<unsigned>(R.r16);
+                v2.w = bitcast<unsigned>(R.r17);
+                reinterpret_cast<uint4*>(base + 2240ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r20);
+                v3.y = bitcast<unsigned>(R.r21);
+                v3.z = bitcast<unsigned>(R.r22);
+                v3.w = bitcast<unsigned>(R.r23);
+                reinterpret_cast<uint4*>(base + 2256ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r24);
+                v4.y = bitcast<unsigned>(R.r25);
+                v4.z = bitcast<unsigned>(R.r26);
+                v4.w = bitcast<unsigned>(R.r42);
+                reinterpret_cast<uint4*>(base + 2272ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r43);
+                v5.y = bitcast<unsigned>(R.r44);
+                v5.z = bitcast<unsigned>(R.r46);
+                v5.w = bitcast<unsigned>(R.r47);
+                reinterpret_cast<uint4*>(base + 2288ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r48);
+                v6.y = bitcast<unsigned>(R.r49);
+                v6.z = bitcast<unsigned>(R.r50);
+                v6.w = bitcast<unsigned>(R.r51);
+                reinterpret_cast<uint4*>(base + 2304ull * cap)[idx] = v6;
+            }
+            {
+                uint4 v7;
+                v7.x = bitcast<unsigned>(R.r52);
+                v7.y = bitcast<unsigned>(R.r76);
+                v7.z = bitcast<unsigned>(R.r77);
+                v7.w = bitcast<unsigned>(R.r78);
+                reinterpret_cast<uint4*>(base + 2320ull * cap)[idx] = v7;
+            }
+            {
+                uint4 v8;
+                v8.x = bitcast<unsigned>(R.r79);
+                v8.y = bitcast<unsigned>(R.r80);
+                v8.z = bitcast<unsigned>(R.r81);
+                v8.w = bitcast<unsigned>(R.r82);
+                reinterpret_cast<uint4*>(base + 2336ull * cap)[idx] = v8;
+            }
+            {
+                uint4 v9;
+                v9.x = bitcast<unsigned>(R.r83);
+                v9.y = bitcast<unsigned>(R.r84);
+                v9.z = bitcast<unsigned>(R.r85);
+                v9.w = bitcast<unsigned>(R.r87);
+                reinterpret_cast<uint4*>(base + 2352ull * cap)[idx] = v9;
+            }
+            {
+                uint4 v10;
+                v10.x = bitcast<unsigned>(R.r92);
+                v10.y = bitcast<unsigned>(R.r93);
+                v10.z = bitcast<unsigned>(R.r94);
+                v10.w = bitcast<unsigned>(R.r100);
+                reinterpret_cast<uint4*>(base + 2368ull * cap)[idx] = v10;
+            }
+            {
+                uint4 v11;
+                v11.x = bitcast<unsigned>(R.r101);
+                v11.y = bitcast<unsigned>(R.r102);
+                v11.z = bitcast<unsigned>(R.r103);
+                v11.w = bitcast<unsigned>(R.r104);
+                reinterpret_cast<uint4*>(base + 2384ull * cap)[idx] = v11;
+            }
+            {
+                uint4 v12;
+                v12.x = bitcast<unsigned>(R.r105);
+                v12.y = bitcast<unsigned>(R.r117);
+                v12.z = bitcast<unsigned>(R.r118);
+                v12.w = bitcast<unsigned>(R.r119);
+                reinterpret_cast<uint4*>(base + 2400ull * cap)[idx] = v12;
+            }
+            {
+                uint4 v13;
+                v13.x = bitcast<unsigned>(R.r127);
+                v13.y = bitcast<unsigned>(R.r128);
+                v13.z = bitcast<unsigned>(R.r129);
+                v13.w = tid;
+                reinterpret_cast<uint4*>(base + 2416ull * cap)[idx] = v13;
+            }
             return;
+        }
         case 24: // roll, context 0
-            reinterpret_cast<unsigned int*>(base + 2432ull * cap)[idx] = R.r7;
-            reinterpret_cast<unsigned int*>(base + 2436ull * cap)[idx] = R.r9;
-            reinterpret_cast<unsigned int*>(base + 2440ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2444ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2448ull * cap)[idx] = R.r13;
-            reinterpret_cast<float*>(base + 2452ull * cap)[idx] = R.r14;
-            reinterpret_cast<float*>(base + 2456ull * cap)[idx] = R.r15;
-            reinterpret_cast<float*>(base + 2460ull * cap)[idx] = R.r16;
-            reinterpret_cast<float*>(base + 2464ull * cap)[idx] = R.r17;
-            reinterpret_cast<unsigned int*>(base + 2468ull * cap)[idx] = R.r20;
-            reinterpret_cast<unsigned int*>(base + 2472ull * cap)[idx] = R.r21;
-            reinterpret_cast<unsigned int*>(base + 2476ull * cap)[idx] = R.r22;
-            reinterpret_cast<unsigned int*>(base + 2480ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2484ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2488ull * cap)[idx] = R.r25;
-            reinterpret_cast<unsigned*>(base + 2492ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r7);
+                v0.y = bitcast<unsigned>(R.r9);
+                v0.z = bitcast<unsigned>(R.r11);
+                v0.w = bitcast<unsigned>(R.r12);
+                reinterpret_cast<uint4*>(base + 2432ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r13);
+                v1.y = bitcast<unsigned>(R.r14);
+                v1.z = bitcast<unsigned>(R.r15);
+                v1.w = bitcast<unsigned>(R.r16);
+                reinterpret_cast<uint4*>(base + 2448ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r17);
+                v2.y = bitcast<unsigned>(R.r20);
+                v2.z = bitcast<unsigned>(R.r21);
+                v2.w = bitcast<unsigned>(R.r22);
+                reinterpret_cast<uint4*>(base + 2464ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r23);
+                v3.y = bitcast<unsigned>(R.r24);
+                v3.z = bitcast<unsigned>(R.r25);
+                v3.w = tid;
+                reinterpret_cast<uint4*>(base + 2480ull * cap)[idx] = v3;
+            }
             return;
+        }
         case 25: // roll, context 1
-            reinterpret_cast<float*>(base + 2496ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2500ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2504ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2508ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2512ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2516ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2520ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2524ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2528ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2532ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 2536ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 2540ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 2544ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2548ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2552ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2556ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2560ull * cap)[idx] = R.r76;
-            reinterpret_cast<float*>(base + 2564ull * cap)[idx] = R.r77;
-            reinterpret_cast<float*>(base + 2568ull * cap)[idx] = R.r78;
-            reinterpret_cast<unsigned int*>(base + 2572ull * cap)[idx] = R.r79;
-            reinterpret_cast<float*>(base + 2576ull * cap)[idx] = R.r80;
-            reinterpret_cast<float*>(base + 2580ull * cap)[idx] = R.r81;
-            reinterpret_cast<float*>(base + 2584ull * cap)[idx] = R.r82;
-            reinterpret_cast<float*>(base + 2588ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 2592ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 2596ull * cap)[idx] = R.r85;
-            reinterpret_cast<unsigned*>(base + 2600ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 2496ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2512ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2528ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 2544ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r76);
+                v4.y = bitcast<unsigned>(R.r77);
+                v4.z = bitcast<unsigned>(R.r78);
+                v4.w = bitcast<unsigned>(R.r79);
+                reinterpret_cast<uint4*>(base + 2560ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r80);
+                v5.y = bitcast<unsigned>(R.r81);
+                v5.z = bitcast<unsigned>(R.r82);
+                v5.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 2576ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r84);
+                v6.y = bitcast<unsigned>(R.r85);
+                v6.z = tid;
+                reinterpret_cast<uint4*>(base + 2592ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 26: // roll, context 2
-            reinterpret_cast<float*>(base + 2608ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2612ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2616ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2620ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2624ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2628ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2632ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2636ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2640ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2644ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2648ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 2652ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 2656ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2660ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2664ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2668ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2672ull * cap)[idx] = R.r92;
-            reinterpret_cast<float*>(base + 2676ull * cap)[idx] = R.r93;
-            reinterpret_cast<float*>(base + 2680ull * cap)[idx] = R.r94;
-            reinterpret_cast<float*>(base + 2684ull * cap)[idx] = R.r100;
-            reinterpret_cast<float*>(base + 2688ull * cap)[idx] = R.r101;
-            reinterpret_cast<float*>(base + 2692ull * cap)[idx] = R.r102;
-            reinterpret_cast<float*>(base + 2696ull * cap)[idx] = R.r103;
-            reinterpret_cast<float*>(base + 2700ull * cap)[idx] = R.r104;
-            reinterpret_cast<float*>(base + 2704ull * cap)[idx] = R.r105;
-            reinterpret_cast<unsigned*>(base + 2708ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 2608ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2624ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r46);
+                v2.z = bitcast<unsigned>(R.r47);
+                v2.w = bitcast<unsigned>(R.r48);
+                reinterpret_cast<uint4*>(base + 2640ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r49);
+                v3.y = bitcast<unsigned>(R.r50);
+                v3.z = bitcast<unsigned>(R.r51);
+                v3.w = bitcast<unsigned>(R.r52);
+                reinterpret_cast<uint4*>(base + 2656ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r92);
+                v4.y = bitcast<unsigned>(R.r93);
+                v4.z = bitcast<unsigned>(R.r94);
+                v4.w = bitcast<unsigned>(R.r100);
+                reinterpret_cast<uint4*>(base + 2672ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r101);
+                v5.y = bitcast<unsigned>(R.r102);
+                v5.z = bitcast<unsigned>(R.r103);
+                v5.w = bitcast<unsigned>(R.r104);
+                reinterpret_cast<uint4*>(base + 2688ull * cap)[idx] = v5;
+            }
+            {
+                uint2 v6;
+                v6.x = bitcast<unsigned>(R.r105);
+                v6.y = tid;
+                reinterpret_cast<uint2*>(base + 2704ull * cap)[idx] = v6;
+            }
             return;
+        }
         case 27: // roll, context 3
-            reinterpret_cast<float*>(base + 2712ull * cap)[idx] = R.r3;
-            reinterpret_cast<float*>(base + 2716ull * cap)[idx] = R.r4;
-            reinterpret_cast<float*>(base + 2720ull * cap)[idx] = R.r5;
-            reinterpret_cast<unsigned int*>(base + 2724ull * cap)[idx] = R.r11;
-            reinterpret_cast<unsigned int*>(base + 2728ull * cap)[idx] = R.r12;
-            reinterpret_cast<unsigned int*>(base + 2732ull * cap)[idx] = R.r13;
-            reinterpret_cast<unsigned int*>(base + 2736ull * cap)[idx] = R.r23;
-            reinterpret_cast<unsigned int*>(base + 2740ull * cap)[idx] = R.r24;
-            reinterpret_cast<unsigned int*>(base + 2744ull * cap)[idx] = R.r25;
-            reinterpret_cast<float*>(base + 2748ull * cap)[idx] = R.r42;
-            reinterpret_cast<float*>(base + 2752ull * cap)[idx] = R.r43;
-            reinterpret_cast<float*>(base + 2756ull * cap)[idx] = R.r44;
-            reinterpret_cast<float*>(base + 2760ull * cap)[idx] = R.r46;
-            reinterpret_cast<float*>(base + 2764ull * cap)[idx] = R.r47;
-            reinterpret_cast<float*>(base + 2768ull * cap)[idx] = R.r48;
-            reinterpret_cast<float*>(base + 2772ull * cap)[idx] = R.r49;
-            reinterpret_cast<float*>(base + 2776ull * cap)[idx] = R.r50;
-            reinterpret_cast<float*>(base + 2780ull * cap)[idx] = R.r51;
-            reinterpret_cast<unsigned int*>(base + 2784ull * cap)[idx] = R.r52;
-            reinterpret_cast<float*>(base + 2788ull * cap)[idx] = R.r83;
-            reinterpret_cast<float*>(base + 2792ull * cap)[idx] = R.r84;
-            reinterpret_cast<float*>(base + 2796ull * cap)[idx] = R.r85;
-            reinterpret_cast<float*>(base + 2800ull * cap)[idx] = R.r87;
-            reinterpret_cast<float*>(base + 2804ull * cap)[idx] = R.r117;
-            reinterpret_cast<float*>(base + 2808ull * cap)[idx] = R.r118;
-            reinterpret_cast<float*>(base + 2812ull * cap)[idx] = R.r119;
-            reinterpret_cast<float*>(base + 2816ull * cap)[idx] = R.r127;
-            reinterpret_cast<float*>(base + 2820ull * cap)[idx] = R.r128;
-            reinterpret_cast<float*>(base + 2824ull * cap)[idx] = R.r129;
-            reinterpret_cast<unsigned*>(base + 2828ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                v0.x = bitcast<unsigned>(R.r3);
+                v0.y = bitcast<unsigned>(R.r4);
+                v0.z = bitcast<unsigned>(R.r5);
+                v0.w = bitcast<unsigned>(R.r11);
+                reinterpret_cast<uint4*>(base + 2712ull * cap)[idx] = v0;
+            }
+            {
+                uint4 v1;
+                v1.x = bitcast<unsigned>(R.r12);
+                v1.y = bitcast<unsigned>(R.r13);
+                v1.z = bitcast<unsigned>(R.r23);
+                v1.w = bitcast<unsigned>(R.r24);
+                reinterpret_cast<uint4*>(base + 2728ull * cap)[idx] = v1;
+            }
+            {
+                uint4 v2;
+                v2.x = bitcast<unsigned>(R.r25);
+                v2.y = bitcast<unsigned>(R.r42);
+                v2.z = bitcast<unsigned>(R.r43);
+                v2.w = bitcast<unsigned>(R.r44);
+                reinterpret_cast<uint4*>(base + 2744ull * cap)[idx] = v2;
+            }
+            {
+                uint4 v3;
+                v3.x = bitcast<unsigned>(R.r46);
+                v3.y = bitcast<unsigned>(R.r47);
+                v3.z = bitcast<unsigned>(R.r48);
+                v3.w = bitcast<unsigned>(R.r49);
+                reinterpret_cast<uint4*>(base + 2760ull * cap)[idx] = v3;
+            }
+            {
+                uint4 v4;
+                v4.x = bitcast<unsigned>(R.r50);
+                v4.y = bitcast<unsigned>(R.r51);
+                v4.z = bitcast<unsigned>(R.r52);
+                v4.w = bitcast<unsigned>(R.r83);
+                reinterpret_cast<uint4*>(base + 2776ull * cap)[idx] = v4;
+            }
+            {
+                uint4 v5;
+                v5.x = bitcast<unsigned>(R.r84);
+                v5.y = bitcast<unsigned>(R.r85);
+                v5.z = bitcast<unsigned>(R.r87);
+                v5.w = bitcast<unsigned>(R.r117);
+                reinterpret_cast<uint4*>(base + 2792ull * cap)[idx] = v5;
+            }
+            {
+                uint4 v6;
+                v6.x = bitcast<unsigned>(R.r118);
+                v6.y = bitcast<unsigned>(R.r119);
+                v6.z = bitcast<unsigned>(R.r127);
+                v6.w = bitcast<unsigned>(R.r128);
+                reinterpret_cast<uint4*>(base + 2808ull * cap)[idx] = v6;
+            }
+            {
+                uint2 v7;
+                v7.x = bitcast<unsigned>(R.r129);
+                v7.y = tid;
+                reinterpret_cast<uint2*>(base + 2824ull * cap)[idx] = v7;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -1803,735 +2587,973 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r1 = reinterpret_cast<const unsigned int*>(base + 0ull * cap)[idx];
-            R.r2 = reinterpret_cast<const unsigned int*>(base + 4ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<unsigned int>(v0.y);
+            return v0.z;
+        }
         case 1: // prim
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 16ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 20ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 24ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 28ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 32ull * cap)[idx];
-            R.r14 = reinterpret_cast<const float*>(base + 36ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 40ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 44ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 48ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 52ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 56ull * cap)[idx];
-            R.r22 = reinterpret_cast<const unsigned int*>(base + 60ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 64ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 68ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 72ull * cap)[idx];
-            R.r130 = reinterpret_cast<const unsigned int*>(base + 76ull * cap)[idx];
-            R.r131 = reinterpret_cast<const unsigned int*>(base + 80ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 84ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 16ull * cap)[idx];
+            R.r7 = bitcast<unsigned int>(v0.x);
+            R.r9 = bitcast<unsigned int>(v0.y);
+            R.r11 = bitcast<unsigned int>(v0.z);
+            R.r12 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 32ull * cap)[idx];
+            R.r13 = bitcast<unsigned int>(v1.x);
+            R.r14 = bitcast<float>(v1.y);
+            R.r15 = bitcast<float>(v1.z);
+            R.r16 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 48ull * cap)[idx];
+            R.r17 = bitcast<float>(v2.x);
+            R.r20 = bitcast<unsigned int>(v2.y);
+            R.r21 = bitcast<unsigned int>(v2.z);
+            R.r22 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 64ull * cap)[idx];
+            R.r23 = bitcast<unsigned int>(v3.x);
+            R.r24 = bitcast<unsigned int>(v3.y);
+            R.r25 = bitcast<unsigned int>(v3.z);
+            R.r130 = bitcast<unsigned int>(v3.w);
+            const uint2 v4 = reinterpret_cast<const uint2*>(base + 80ull * cap)[idx];
+            R.r131 = bitcast<unsigned int>(v4.x);
+            return v4.y;
+        }
         case 2: // bounce
-            R.r3 = reinterpret_cast<const float*>(base + 88ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 92ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 96ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 100ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 104ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 108ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 112ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 116ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 120ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 124ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 128ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 132ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 136ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 140ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 144ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 148ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 152ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 156ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 160ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 164ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 88ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 104ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 120ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 136ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 152ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            return v4.w;
+        }
         case 3: // isect
-            R.r3 = reinterpret_cast<const float*>(base + 168ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 172ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 176ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 180ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 184ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 188ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 192ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 196ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 200ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 204ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 208ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 212ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 216ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 220ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 224ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 228ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 232ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 236ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 240ull * cap)[idx];
-            R.r53 = reinterpret_cast<const float*>(base + 244ull * cap)[idx];
-            R.r54 = reinterpret_cast<const unsigned int*>(base + 248ull * cap)[idx];
-            R.r55 = reinterpret_cast<const unsigned int*>(base + 252ull * cap)[idx];
-            R.r56 = reinterpret_cast<const unsigned int*>(base + 256ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 260ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 168ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 184ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 200ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 216ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 232ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 248ull * cap)[idx];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            R.r55 = bitcast<unsigned int>(v5.y);
+            R.r56 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
         case 4: // shade
-            R.r3 = reinterpret_cast<const float*>(base + 264ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 268ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 272ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 276ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 280ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 284ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 288ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 292ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 296ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 300ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 304ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 308ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 312ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 316ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 320ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 324ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 328ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 332ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 336ull * cap)[idx];
-            R.r53 = reinterpret_cast<const float*>(base + 340ull * cap)[idx];
-            R.r54 = reinterpret_cast<const unsigned int*>(base + 344ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 348ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 264ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 280ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 296ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 312ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 328ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(base + 344ull * cap)[idx];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
         case 5: // hitp
-            R.r3 = reinterpret_cast<const float*>(base + 352ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 356ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 360ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 364ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 368ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 372ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 376ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 380ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 384ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 388ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 392ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 396ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 400ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 404ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 408ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 412ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 416ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 420ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 424ull * cap)[idx];
-            R.r53 = reinterpret_cast<const float*>(base + 428ull * cap)[idx];
-            R.r54 = reinterpret_cast<const unsigned int*>(base + 432ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 436ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 352ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 368ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 384ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 400ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 416ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(base + 432ull * cap)[idx];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
         case 6: // emit
-            R.r3 = reinterpret_cast<const float*>(base + 440ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 444ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 448ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 452ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 456ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 460ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 464ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 468ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 472ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 476ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 440ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r49 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 456ull * cap)[idx];
+            R.r50 = bitcast<float>(v1.x);
+            R.r51 = bitcast<float>(v1.y);
+            R.r76 = bitcast<float>(v1.z);
+            R.r77 = bitcast<float>(v1.w);
+            const uint2 v2 = reinterpret_cast<const uint2*>(base + 472ull * cap)[idx];
+            R.r78 = bitcast<float>(v2.x);
+            return v2.y;
+        }
         case 7: // surf
-            R.r3 = reinterpret_cast<const float*>(base + 480ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 484ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 488ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 492ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 496ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 500ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 504ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 508ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 512ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 516ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 520ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 524ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 528ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 532ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 536ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 540ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 544ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 548ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 552ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 556ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 560ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 564ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 568ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 572ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 576ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 580ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 584ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 480ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 496ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 512ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 528ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 544ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 560ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 576ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
         case 8: // rrchk
-            R.r3 = reinterpret_cast<const float*>(base + 592ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 596ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 600ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 604ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 608ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 612ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 616ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 620ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 624ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 628ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 632ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 636ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 640ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 644ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 648ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 652ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 656ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 660ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 664ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 668ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 672ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 676ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 680ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 684ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 688ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 692ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 696ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 592ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 608ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 624ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 640ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 656ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 672ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 688ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
         case 9: // rr_roll
-            R.r3 = reinterpret_cast<const float*>(base + 704ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 708ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 712ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 716ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 720ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 724ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 728ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 732ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 736ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 740ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 744ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 748ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 752ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 756ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 760ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 764ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 768ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 772ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 776ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 780ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 784ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 788ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 792ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 796ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 800ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 804ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 808ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 704ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 720ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 736ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 752ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 768ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 784ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 800ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
         case 10: // rr
-            R.r3 = reinterpret_cast<const float*>(base + 816ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 820ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 824ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 828ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 832ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 836ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 840ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 844ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 848ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 852ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 856ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 860ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 864ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 868ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 872ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 876ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 880ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 884ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 888ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 892ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 896ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 900ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 904ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 908ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 912ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 916ull * cap)[idx];
-            R.r130 = reinterpret_cast<const unsigned int*>(base + 920ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 924ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 816ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 832ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 848ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 864ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 880ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 896ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 912ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            R.r130 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
         case 11: // rr_keep
-            R.r3 = reinterpret_cast<const float*>(base + 928ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 932ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 936ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 940ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 944ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 948ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 952ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 956ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 960ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 964ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 968ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 972ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 976ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 980ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 984ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 988ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 992ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 996ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 1000ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 1004ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 1008ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 1012ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 1016ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1020ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1024ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1028ull * cap)[idx];
-            R.r86 = reinterpret_cast<const float*>(base + 1032ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1036ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 928ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 944ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 960ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 976ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 992ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1008ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1024ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            R.r86 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 12: // scatter
-            R.r3 = reinterpret_cast<const float*>(base + 1040ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1044ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1048ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1052ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1056ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1060ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1064ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1068ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1072ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1076ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1080ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1084ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1088ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1092ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1096ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1100ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 1104ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 1108ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 1112ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 1116ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 1120ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 1124ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 1128ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1132ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1136ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1140ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1144ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1040ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1056ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1072ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1088ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1104ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1120ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1136ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
         case 13: // mirror
-            R.r3 = reinterpret_cast<const float*>(base + 1152ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1156ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1160ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1164ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1168ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1172ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1176ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1180ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1184ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1188ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1192ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1196ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1200ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1204ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1208ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1212ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1216ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1220ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1224ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1228ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1232ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1236ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 1240ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1244ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1152ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1168ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1184ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1200ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1216ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1232ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            return v5.w;
+        }
         case 14: // diffuse
-            R.r3 = reinterpret_cast<const float*>(base + 1248ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1252ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1256ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1260ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1264ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1268ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1272ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1276ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1280ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1284ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1288ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1292ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1296ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1300ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1304ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1308ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 1312ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 1316ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 1320ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1324ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1248ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1264ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1280ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1296ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1312ull * cap)[idx];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            return v4.w;
+        }
         case 15: // disk_roll
-            R.r3 = reinterpret_cast<const float*>(base + 1328ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1332ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1336ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1340ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1344ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1348ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1352ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1356ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1360ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1364ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1368ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1372ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1376ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1380ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1384ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1388ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 1392ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 1396ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 1400ull * cap)[idx];
-            R.r100 = reinterpret_cast<const float*>(base + 1404ull * cap)[idx];
-            R.r101 = reinterpret_cast<const float*>(base + 1408ull * cap)[idx];
-            R.r102 = reinterpret_cast<const float*>(base + 1412ull * cap)[idx];
-            R.r103 = reinterpret_cast<const float*>(base + 1416ull * cap)[idx];
-            R.r104 = reinterpret_cast<const float*>(base + 1420ull * cap)[idx];
-            R.r105 = reinterpret_cast<const float*>(base + 1424ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1428ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1328ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1344ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1360ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1376ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1392ull * cap)[idx];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1408ull * cap)[idx];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 1424ull * cap)[idx];
+            R.r105 = bitcast<float>(v6.x);
+            return v6.y;
+        }
         case 16: // disk
-            R.r3 = reinterpret_cast<const float*>(base + 1432ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1436ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1440ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1444ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1448ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1452ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1456ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1460ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1464ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1468ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1472ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1476ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1480ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1484ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1488ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1492ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 1496ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 1500ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 1504ull * cap)[idx];
-            R.r100 = reinterpret_cast<const float*>(base + 1508ull * cap)[idx];
-            R.r101 = reinterpret_cast<const float*>(base + 1512ull * cap)[idx];
-            R.r102 = reinterpret_cast<const float*>(base + 1516ull * cap)[idx];
-            R.r103 = reinterpret_cast<const float*>(base + 1520ull * cap)[idx];
-            R.r104 = reinterpret_cast<const float*>(base + 1524ull * cap)[idx];
-            R.r105 = reinterpret_cast<const float*>(base + 1528ull * cap)[idx];
-            R.r130 = reinterpret_cast<const unsigned int*>(base + 1532ull * cap)[idx];
-            R.r131 = reinterpret_cast<const unsigned int*>(base + 1536ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1540ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1432ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1448ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1464ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1480ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1496ull * cap)[idx];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1512ull * cap)[idx];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1528ull * cap)[idx];
+            R.r105 = bitcast<float>(v6.x);
+            R.r130 = bitcast<unsigned int>(v6.y);
+            R.r131 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
         case 17: // disk_ok
-            R.r3 = reinterpret_cast<const float*>(base + 1544ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1548ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1552ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1556ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1560ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1564ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1568ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1572ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1576ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1580ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1584ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1588ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1592ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1596ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1600ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1604ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 1608ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 1612ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 1616ull * cap)[idx];
-            R.r100 = reinterpret_cast<const float*>(base + 1620ull * cap)[idx];
-            R.r101 = reinterpret_cast<const float*>(base + 1624ull * cap)[idx];
-            R.r102 = reinterpret_cast<const float*>(base + 1628ull * cap)[idx];
-            R.r103 = reinterpret_cast<const float*>(base + 1632ull * cap)[idx];
-            R.r104 = reinterpret_cast<const float*>(base + 1636ull * cap)[idx];
-            R.r105 = reinterpret_cast<const float*>(base + 1640ull * cap)[idx];
-            R.r106 = reinterpret_cast<const float*>(base + 1644ull * cap)[idx];
-            R.r107 = reinterpret_cast<const float*>(base + 1648ull * cap)[idx];
-            R.r108 = reinterpret_cast<const float*>(base + 1652ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1656ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1544ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1560ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1576ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1592ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1608ull * cap)[idx];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1624ull * cap)[idx];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1640ull * cap)[idx];
+            R.r105 = bitcast<float>(v6.x);
+            R.r106 = bitcast<float>(v6.y);
+            R.r107 = bitcast<float>(v6.z);
+            R.r108 = bitcast<float>(v6.w);
+            const unsigned v7 = reinterpret_cast<const unsigned*>(base + 1656ull * cap)[idx];
+            return v7;
+        }
         case 18: // glass
-            R.r3 = reinterpret_cast<const float*>(base + 1664ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1668ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1672ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1676ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1680ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1684ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1688ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1692ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1696ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1700ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1704ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1708ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1712ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1716ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1720ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1724ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1728ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1732ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1736ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1740ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1744ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1748ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 1752ull * cap)[idx];
-            R.r88 = reinterpret_cast<const unsigned int*>(base + 1756ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 1760ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 1764ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 1768ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1772ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1664ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1680ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1696ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1712ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1728ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1744ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r88 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1760ull * cap)[idx];
+            R.r92 = bitcast<float>(v6.x);
+            R.r93 = bitcast<float>(v6.y);
+            R.r94 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 19: // refr
-            R.r3 = reinterpret_cast<const float*>(base + 1776ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1780ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1784ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1788ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1792ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1796ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1800ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1804ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1808ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1812ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1816ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1820ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1824ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1828ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1832ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1836ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1840ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1844ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1848ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1852ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1856ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1860ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 1864ull * cap)[idx];
-            R.r88 = reinterpret_cast<const unsigned int*>(base + 1868ull * cap)[idx];
-            R.r111 = reinterpret_cast<const float*>(base + 1872ull * cap)[idx];
-            R.r112 = reinterpret_cast<const float*>(base + 1876ull * cap)[idx];
-            R.r113 = reinterpret_cast<const float*>(base + 1880ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 1884ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1776ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1792ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1808ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1824ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1840ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1856ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r88 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1872ull * cap)[idx];
+            R.r111 = bitcast<float>(v6.x);
+            R.r112 = bitcast<float>(v6.y);
+            R.r113 = bitcast<float>(v6.z);
+            return v6.w;
+        }
         case 20: // fres
-            R.r3 = reinterpret_cast<const float*>(base + 1888ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 1892ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 1896ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 1900ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 1904ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 1908ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 1912ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 1916ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 1920ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 1924ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 1928ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 1932ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 1936ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 1940ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 1944ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 1948ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 1952ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 1956ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 1960ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 1964ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 1968ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 1972ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 1976ull * cap)[idx];
-            R.r117 = reinterpret_cast<const float*>(base + 1980ull * cap)[idx];
-            R.r118 = reinterpret_cast<const float*>(base + 1984ull * cap)[idx];
-            R.r119 = reinterpret_cast<const float*>(base + 1988ull * cap)[idx];
-            R.r127 = reinterpret_cast<const float*>(base + 1992ull * cap)[idx];
-            R.r128 = reinterpret_cast<const float*>(base + 1996ull * cap)[idx];
-            R.r129 = reinterpret_cast<const float*>(base + 2000ull * cap)[idx];
-            R.r130 = reinterpret_cast<const unsigned int*>(base + 2004ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2008ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 1888ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 1904ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 1920ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 1936ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 1952ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 1968ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r117 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 1984ull * cap)[idx];
+            R.r118 = bitcast<float>(v6.x);
+            R.r119 = bitcast<float>(v6.y);
+            R.r127 = bitcast<float>(v6.z);
+            R.r128 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2000ull * cap)[idx];
+            R.r129 = bitcast<float>(v7.x);
+            R.r130 = bitcast<unsigned int>(v7.y);
+            return v7.z;
+        }
         case 21: // take_refl
-            R.r3 = reinterpret_cast<const float*>(base + 2016ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2020ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2024ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2028ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2032ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2036ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2040ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2044ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2048ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2052ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 2056ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 2060ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2064ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2068ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 2072ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2076ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2080ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2084ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2088ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 2092ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 2096ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 2100ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 2104ull * cap)[idx];
-            R.r128 = reinterpret_cast<const float*>(base + 2108ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2112ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2016ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2032ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2048ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2064ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2080ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2096ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r128 = bitcast<float>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(base + 2112ull * cap)[idx];
+            return v6;
+        }
         case 22: // take_refr
-            R.r3 = reinterpret_cast<const float*>(base + 2120ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2124ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2128ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2132ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2136ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2140ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2144ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2148ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2152ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2156ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2160ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 2164ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2168ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2172ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2176ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2180ull * cap)[idx];
-            R.r117 = reinterpret_cast<const float*>(base + 2184ull * cap)[idx];
-            R.r118 = reinterpret_cast<const float*>(base + 2188ull * cap)[idx];
-            R.r119 = reinterpret_cast<const float*>(base + 2192ull * cap)[idx];
-            R.r129 = reinterpret_cast<const float*>(base + 2196ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2200ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2120ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2136ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2152ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2168ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2184ull * cap)[idx];
+            R.r117 = bitcast<float>(v4.x);
+            R.r118 = bitcast<float>(v4.y);
+            R.r119 = bitcast<float>(v4.z);
+            R.r129 = bitcast<float>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(base + 2200ull * cap)[idx];
+            return v5;
+        }
         case 23: // roll
-            R.r3 = reinterpret_cast<const float*>(base + 2208ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2212ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2216ull * cap)[idx];
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2220ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2224ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2228ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2232ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2236ull * cap)[idx];
-            R.r14 = reinterpret_cast<const float*>(base + 2240ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2244ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2248ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2252ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 2256ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 2260ull * cap)[idx];
-            R.r22 = reinterpret_cast<const unsigned int*>(base + 2264ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2268ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2272ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2276ull * cap)[idx];
-            R.r26 = reinterpret_cast<const unsigned int*>(base + 2280ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2284ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 2288ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 2292ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2296ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2300ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 2304ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2308ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2312ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2316ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2320ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 2324ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 2328ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 2332ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 2336ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 2340ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 2344ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 2348ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 2352ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 2356ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 2360ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 2364ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 2368ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 2372ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 2376ull * cap)[idx];
-            R.r100 = reinterpret_cast<const float*>(base + 2380ull * cap)[idx];
-            R.r101 = reinterpret_cast<const float*>(base + 2384ull * cap)[idx];
-            R.r102 = reinterpret_cast<const float*>(base + 2388ull * cap)[idx];
-            R.r103 = reinterpret_cast<const float*>(base + 2392ull * cap)[idx];
-            R.r104 = reinterpret_cast<const float*>(base + 2396ull * cap)[idx];
-            R.r105 = reinterpret_cast<const float*>(base + 2400ull * cap)[idx];
-            R.r117 = reinterpret_cast<const float*>(base + 2404ull * cap)[idx];
-            R.r118 = reinterpret_cast<const float*>(base + 2408ull * cap)[idx];
-            R.r119 = reinterpret_cast<const float*>(base + 2412ull * cap)[idx];
-            R.r127 = reinterpret_cast<const float*>(base + 2416ull * cap)[idx];
-            R.r128 = reinterpret_cast<const float*>(base + 2420ull * cap)[idx];
-            R.r129 = reinterpret_cast<const float*>(base + 2424ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2428ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2208ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r7 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2224ull * cap)[idx];
+            R.r9 = bitcast<unsigned int>(v1.x);
+            R.r11 = bitcast<unsigned int>(v1.y);
+            R.r12 = bitcast<unsigned int>(v1.z);
+            R.r13 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2240ull * cap)[idx];
+            R.r14 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2256ull * cap)[idx];
+            R.r20 = bitcast<unsigned int>(v3.x);
+            R.r21 = bitcast<unsigned int>(v3.y);
+            R.r22 = bitcast<unsigned int>(v3.z);
+            R.r23 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2272ull * cap)[idx];
+            R.r24 = bitcast<unsigned int>(v4.x);
+            R.r25 = bitcast<unsigned int>(v4.y);
+            R.r26 = bitcast<unsigned int>(v4.z);
+            R.r42 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2288ull * cap)[idx];
+            R.r43 = bitcast<float>(v5.x);
+            R.r44 = bitcast<float>(v5.y);
+            R.r46 = bitcast<float>(v5.z);
+            R.r47 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2304ull * cap)[idx];
+            R.r48 = bitcast<float>(v6.x);
+            R.r49 = bitcast<float>(v6.y);
+            R.r50 = bitcast<float>(v6.z);
+            R.r51 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(base + 2320ull * cap)[idx];
+            R.r52 = bitcast<unsigned int>(v7.x);
+            R.r76 = bitcast<float>(v7.y);
+            R.r77 = bitcast<float>(v7.z);
+            R.r78 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(base + 2336ull * cap)[idx];
+            R.r79 = bitcast<unsigned int>(v8.x);
+            R.r80 = bitcast<float>(v8.y);
+            R.r81 = bitcast<float>(v8.z);
+            R.r82 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(base + 2352ull * cap)[idx];
+            R.r83 = bitcast<float>(v9.x);
+            R.r84 = bitcast<float>(v9.y);
+            R.r85 = bitcast<float>(v9.z);
+            R.r87 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(base + 2368ull * cap)[idx];
+            R.r92 = bitcast<float>(v10.x);
+            R.r93 = bitcast<float>(v10.y);
+            R.r94 = bitcast<float>(v10.z);
+            R.r100 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(base + 2384ull * cap)[idx];
+            R.r101 = bitcast<float>(v11.x);
+            R.r102 = bitcast<float>(v11.y);
+            R.r103 = bitcast<float>(v11.z);
+            R.r104 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(base + 2400ull * cap)[idx];
+            R.r105 = bitcast<float>(v12.x);
+            R.r117 = bitcast<float>(v12.y);
+            R.r118 = bitcast<float>(v12.z);
+            R.r119 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(base + 2416ull * cap)[idx];
+            R.r127 = bitcast<float>(v13.x);
+            R.r128 = bitcast<float>(v13.y);
+            R.r129 = bitcast<float>(v13.z);
+            return v13.w;
+        }
         case 24: // roll, context 0
+        {
             R.r26 = static_cast<unsigned int>(0);
-            R.r7 = reinterpret_cast<const unsigned int*>(base + 2432ull * cap)[idx];
-            R.r9 = reinterpret_cast<const unsigned int*>(base + 2436ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2440ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2444ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2448ull * cap)[idx];
-            R.r14 = reinterpret_cast<const float*>(base + 2452ull * cap)[idx];
-            R.r15 = reinterpret_cast<const float*>(base + 2456ull * cap)[idx];
-            R.r16 = reinterpret_cast<const float*>(base + 2460ull * cap)[idx];
-            R.r17 = reinterpret_cast<const float*>(base + 2464ull * cap)[idx];
-            R.r20 = reinterpret_cast<const unsigned int*>(base + 2468ull * cap)[idx];
-            R.r21 = reinterpret_cast<const unsigned int*>(base + 2472ull * cap)[idx];
-            R.r22 = reinterpret_cast<const unsigned int*>(base + 2476ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2480ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2484ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2488ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2492ull * cap)[idx];
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2432ull * cap)[idx];
+            R.r7 = bitcast<unsigned int>(v0.x);
+            R.r9 = bitcast<unsigned int>(v0.y);
+            R.r11 = bitcast<unsigned int>(v0.z);
+            R.r12 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2448ull * cap)[idx];
+            R.r13 = bitcast<unsigned int>(v1.x);
+            R.r14 = bitcast<float>(v1.y);
+            R.r15 = bitcast<float>(v1.z);
+            R.r16 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2464ull * cap)[idx];
+            R.r17 = bitcast<float>(v2.x);
+            R.r20 = bitcast<unsigned int>(v2.y);
+            R.r21 = bitcast<unsigned int>(v2.z);
+            R.r22 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2480ull * cap)[idx];
+            R.r23 = bitcast<unsigned int>(v3.x);
+            R.r24 = bitcast<unsigned int>(v3.y);
+            R.r25 = bitcast<unsigned int>(v3.z);
+            return v3.w;
+        }
         case 25: // roll, context 1
+        {
             R.r26 = static_cast<unsigned int>(1);
-            R.r3 = reinterpret_cast<const float*>(base + 2496ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2500ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2504ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2508ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2512ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2516ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2520ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2524ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2528ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2532ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 2536ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 2540ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2544ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2548ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2552ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2556ull * cap)[idx];
-            R.r76 = reinterpret_cast<const float*>(base + 2560ull * cap)[idx];
-            R.r77 = reinterpret_cast<const float*>(base + 2564ull * cap)[idx];
-            R.r78 = reinterpret_cast<const float*>(base + 2568ull * cap)[idx];
-            R.r79 = reinterpret_cast<const unsigned int*>(base + 2572ull * cap)[idx];
-            R.r80 = reinterpret_cast<const float*>(base + 2576ull * cap)[idx];
-            R.r81 = reinterpret_cast<const float*>(base + 2580ull * cap)[idx];
-            R.r82 = reinterpret_cast<const float*>(base + 2584ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 2588ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 2592ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 2596ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2600ull * cap)[idx];
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2496ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2512ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2528ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2544ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2560ull * cap)[idx];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2576ull * cap)[idx];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2592ull * cap)[idx];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
         case 26: // roll, context 2
+        {
             R.r26 = static_cast<unsigned int>(2);
-            R.r3 = reinterpret_cast<const float*>(base + 2608ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2612ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2616ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2620ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2624ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2628ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2632ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2636ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2640ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2644ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2648ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 2652ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2656ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2660ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2664ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2668ull * cap)[idx];
-            R.r92 = reinterpret_cast<const float*>(base + 2672ull * cap)[idx];
-            R.r93 = reinterpret_cast<const float*>(base + 2676ull * cap)[idx];
-            R.r94 = reinterpret_cast<const float*>(base + 2680ull * cap)[idx];
-            R.r100 = reinterpret_cast<const float*>(base + 2684ull * cap)[idx];
-            R.r101 = reinterpret_cast<const float*>(base + 2688ull * cap)[idx];
-            R.r102 = reinterpret_cast<const float*>(base + 2692ull * cap)[idx];
-            R.r103 = reinterpret_cast<const float*>(base + 2696ull * cap)[idx];
-            R.r104 = reinterpret_cast<const float*>(base + 2700ull * cap)[idx];
-            R.r105 = reinterpret_cast<const float*>(base + 2704ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2708ull * cap)[idx];
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2608ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2624ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2640ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2656ull * cap)[idx];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2672ull * cap)[idx];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2688ull * cap)[idx];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(base + 2704ull * cap)[idx];
+            R.r105 = bitcast<float>(v6.x);
+            return v6.y;
+        }
         case 27: // roll, context 3
+        {
             R.r26 = static_cast<unsigned int>(3);
-            R.r3 = reinterpret_cast<const float*>(base + 2712ull * cap)[idx];
-            R.r4 = reinterpret_cast<const float*>(base + 2716ull * cap)[idx];
-            R.r5 = reinterpret_cast<const float*>(base + 2720ull * cap)[idx];
-            R.r11 = reinterpret_cast<const unsigned int*>(base + 2724ull * cap)[idx];
-            R.r12 = reinterpret_cast<const unsigned int*>(base + 2728ull * cap)[idx];
-            R.r13 = reinterpret_cast<const unsigned int*>(base + 2732ull * cap)[idx];
-            R.r23 = reinterpret_cast<const unsigned int*>(base + 2736ull * cap)[idx];
-            R.r24 = reinterpret_cast<const unsigned int*>(base + 2740ull * cap)[idx];
-            R.r25 = reinterpret_cast<const unsigned int*>(base + 2744ull * cap)[idx];
-            R.r42 = reinterpret_cast<const float*>(base + 2748ull * cap)[idx];
-            R.r43 = reinterpret_cast<const float*>(base + 2752ull * cap)[idx];
-            R.r44 = reinterpret_cast<const float*>(base + 2756ull * cap)[idx];
-            R.r46 = reinterpret_cast<const float*>(base + 2760ull * cap)[idx];
-            R.r47 = reinterpret_cast<const float*>(base + 2764ull * cap)[idx];
-            R.r48 = reinterpret_cast<const float*>(base + 2768ull * cap)[idx];
-            R.r49 = reinterpret_cast<const float*>(base + 2772ull * cap)[idx];
-            R.r50 = reinterpret_cast<const float*>(base + 2776ull * cap)[idx];
-            R.r51 = reinterpret_cast<const float*>(base + 2780ull * cap)[idx];
-            R.r52 = reinterpret_cast<const unsigned int*>(base + 2784ull * cap)[idx];
-            R.r83 = reinterpret_cast<const float*>(base + 2788ull * cap)[idx];
-            R.r84 = reinterpret_cast<const float*>(base + 2792ull * cap)[idx];
-            R.r85 = reinterpret_cast<const float*>(base + 2796ull * cap)[idx];
-            R.r87 = reinterpret_cast<const float*>(base + 2800ull * cap)[idx];
-            R.r117 = reinterpret_cast<const float*>(base + 2804ull * cap)[idx];
-            R.r118 = reinterpret_cast<const float*>(base + 2808ull * cap)[idx];
-            R.r119 = reinterpret_cast<const float*>(base + 2812ull * cap)[idx];
-            R.r127 = reinterpret_cast<const float*>(base + 2816ull * cap)[idx];
-            R.r128 = reinterpret_cast<const float*>(base + 2820ull * cap)[idx];
-            R.r129 = reinterpret_cast<const float*>(base + 2824ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 2828ull * cap)[idx];
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 2712ull * cap)[idx];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(base + 2728ull * cap)[idx];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(base + 2744ull * cap)[idx];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(base + 2760ull * cap)[idx];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(base + 2776ull * cap)[idx];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(base + 2792ull * cap)[idx];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r117 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(base + 2808ull * cap)[idx];
+            R.r118 = bitcast<float>(v6.x);
+            R.r119 = bitcast<float>(v6.y);
+            R.r127 = bitcast<float>(v6.z);
+            R.r128 = bitcast<float>(v6.w);
+            const uint2 v7 = reinterpret_cast<const uint2*>(base + 2824ull * cap)[idx];
+            R.r129 = bitcast<float>(v7.x);
+            return v7.y;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -2552,115 +3574,171 @@ const loom_b200_kernel_info kInfo = {
 const uint32_t kQRegs0[] = {1u, 2u};
 const int kQTypes0[] = {LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames0[] = {"inst", "sid"};
-const unsigned long long kQOffs0[] = {0ull, 4ull};
+const unsigned long long kQOffs0[] = {0ull, 0ull};
+const unsigned kQSubs0[] = {0u, 4u};
+const unsigned kQWidths0[] = {16u, 16u};
 const uint32_t kQRegs1[] = {7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u, 130u, 131u};
 const int kQTypes1[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames1[] = {"w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1", "u0", "u1"};
-const unsigned long long kQOffs1[] = {16ull, 20ull, 24ull, 28ull, 32ull, 36ull, 40ull, 44ull, 48ull, 52ull, 56ull, 60ull, 64ull, 68ull, 72ull, 76ull, 80ull};
+const unsigned long long kQOffs1[] = {16ull, 16ull, 16ull, 16ull, 32ull, 32ull, 32ull, 32ull, 48ull, 48ull, 48ull, 48ull, 64ull, 64ull, 64ull, 64ull, 80ull};
+const unsigned kQSubs1[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths1[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs2[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u};
 const int kQTypes2[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames2[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth"};
-const unsigned long long kQOffs2[] = {88ull, 92ull, 96ull, 100ull, 104ull, 108ull, 112ull, 116ull, 120ull, 124ull, 128ull, 132ull, 136ull, 140ull, 144ull, 148ull, 152ull, 156ull, 160ull};
+const unsigned long long kQOffs2[] = {88ull, 88ull, 88ull, 88ull, 104ull, 104ull, 104ull, 104ull, 120ull, 120ull, 120ull, 120ull, 136ull, 136ull, 136ull, 136ull, 152ull, 152ull, 152ull};
+const unsigned kQSubs2[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths2[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs3[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u, 55u, 56u};
 const int kQTypes3[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames3[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid", "i", "sp"};
-const unsigned long long kQOffs3[] = {168ull, 172ull, 176ull, 180ull, 184ull, 188ull, 192ull, 196ull, 200ull, 204ull, 208ull, 212ull, 216ull, 220ull, 224ull, 228ull, 232ull, 236ull, 240ull, 244ull, 248ull, 252ull, 256ull};
+const unsigned long long kQOffs3[] = {168ull, 168ull, 168ull, 168ull, 184ull, 184ull, 184ull, 184ull, 200ull, 200ull, 200ull, 200ull, 216ull, 216ull, 216ull, 216ull, 232ull, 232ull, 232ull, 232ull, 248ull, 248ull, 248ull};
+const unsigned kQSubs3[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths3[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs4[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u};
 const int kQTypes4[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames4[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid"};
-const unsigned long long kQOffs4[] = {264ull, 268ull, 272ull, 276ull, 280ull, 284ull, 288ull, 292ull, 296ull, 300ull, 304ull, 308ull, 312ull, 316ull, 320ull, 324ull, 328ull, 332ull, 336ull, 340ull, 344ull};
+const unsigned long long kQOffs4[] = {264ull, 264ull, 264ull, 264ull, 280ull, 280ull, 280ull, 280ull, 296ull, 296ull, 296ull, 296ull, 312ull, 312ull, 312ull, 312ull, 328ull, 328ull, 328ull, 328ull, 344ull};
+const unsigned kQSubs4[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths4[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs5[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 53u, 54u};
 const int kQTypes5[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames5[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "tmin", "hid"};
-const unsigned long long kQOffs5[] = {352ull, 356ull, 360ull, 364ull, 368ull, 372ull, 376ull, 380ull, 384ull, 388ull, 392ull, 396ull, 400ull, 404ull, 408ull, 412ull, 416ull, 420ull, 424ull, 428ull, 432ull};
+const unsigned long long kQOffs5[] = {352ull, 352ull, 352ull, 352ull, 368ull, 368ull, 368ull, 368ull, 384ull, 384ull, 384ull, 384ull, 400ull, 400ull, 400ull, 400ull, 416ull, 416ull, 416ull, 416ull, 432ull};
+const unsigned kQSubs5[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths5[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs6[] = {3u, 4u, 5u, 49u, 50u, 51u, 76u, 77u, 78u};
 const int kQTypes6[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames6[] = {"L0", "L1", "L2", "T0", "T1", "T2", "cr", "cg", "cb"};
-const unsigned long long kQOffs6[] = {440ull, 444ull, 448ull, 452ull, 456ull, 460ull, 464ull, 468ull, 472ull};
+const unsigned long long kQOffs6[] = {440ull, 440ull, 440ull, 440ull, 456ull, 456ull, 456ull, 456ull, 472ull};
+const unsigned kQSubs6[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths6[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs7[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
 const int kQTypes7[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames7[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
-const unsigned long long kQOffs7[] = {480ull, 484ull, 488ull, 492ull, 496ull, 500ull, 504ull, 508ull, 512ull, 516ull, 520ull, 524ull, 528ull, 532ull, 536ull, 540ull, 544ull, 548ull, 552ull, 556ull, 560ull, 564ull, 568ull, 572ull, 576ull, 580ull};
+const unsigned long long kQOffs7[] = {480ull, 480ull, 480ull, 480ull, 496ull, 496ull, 496ull, 496ull, 512ull, 512ull, 512ull, 512ull, 528ull, 528ull, 528ull, 528ull, 544ull, 544ull, 544ull, 544ull, 560ull, 560ull, 560ull, 560ull, 576ull, 576ull};
+const unsigned kQSubs7[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths7[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs8[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
 const int kQTypes8[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames8[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
-const unsigned long long kQOffs8[] = {592ull, 596ull, 600ull, 604ull, 608ull, 612ull, 616ull, 620ull, 624ull, 628ull, 632ull, 636ull, 640ull, 644ull, 648ull, 652ull, 656ull, 660ull, 664ull, 668ull, 672ull, 676ull, 680ull, 684ull, 688ull, 692ull};
+const unsigned long long kQOffs8[] = {592ull, 592ull, 592ull, 592ull, 608ull, 608ull, 608ull, 608ull, 624ull, 624ull, 624ull, 624ull, 640ull, 640ull, 640ull, 640ull, 656ull, 656ull, 656ull, 656ull, 672ull, 672ull, 672ull, 672ull, 688ull, 688ull};
+const unsigned kQSubs8[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths8[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs9[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
 const int kQTypes9[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames9[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
-const unsigned long long kQOffs9[] = {704ull, 708ull, 712ull, 716ull, 720ull, 724ull, 728ull, 732ull, 736ull, 740ull, 744ull, 748ull, 752ull, 756ull, 760ull, 764ull, 768ull, 772ull, 776ull, 780ull, 784ull, 788ull, 792ull, 796ull, 800ull, 804ull};
+const unsigned long long kQOffs9[] = {704ull, 704ull, 704ull, 704ull, 720ull, 720ull, 720ull, 720ull, 736ull, 736ull, 736ull, 736ull, 752ull, 752ull, 752ull, 752ull, 768ull, 768ull, 768ull, 768ull, 784ull, 784ull, 784ull, 784ull, 800ull, 800ull};
+const unsigned kQSubs9[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths9[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs10[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 130u};
 const int kQTypes10[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames10[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "u0"};
-const unsigned long long kQOffs10[] = {816ull, 820ull, 824ull, 828ull, 832ull, 836ull, 840ull, 844ull, 848ull, 852ull, 856ull, 860ull, 864ull, 868ull, 872ull, 876ull, 880ull, 884ull, 888ull, 892ull, 896ull, 900ull, 904ull, 908ull, 912ull, 916ull, 920ull};
+const unsigned long long kQOffs10[] = {816ull, 816ull, 816ull, 816ull, 832ull, 832ull, 832ull, 832ull, 848ull, 848ull, 848ull, 848ull, 864ull, 864ull, 864ull, 864ull, 880ull, 880ull, 880ull, 880ull, 896ull, 896ull, 896ull, 896ull, 912ull, 912ull, 912ull};
+const unsigned kQSubs10[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths10[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs11[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 86u};
 const int kQTypes11[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames11[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "p"};
-const unsigned long long kQOffs11[] = {928ull, 932ull, 936ull, 940ull, 944ull, 948ull, 952ull, 956ull, 960ull, 964ull, 968ull, 972ull, 976ull, 980ull, 984ull, 988ull, 992ull, 996ull, 1000ull, 1004ull, 1008ull, 1012ull, 1016ull, 1020ull, 1024ull, 1028ull, 1032ull};
+const unsigned long long kQOffs11[] = {928ull, 928ull, 928ull, 928ull, 944ull, 944ull, 944ull, 944ull, 960ull, 960ull, 960ull, 960ull, 976ull, 976ull, 976ull, 976ull, 992ull, 992ull, 992ull, 992ull, 1008ull, 1008ull, 1008ull, 1008ull, 1024ull, 1024ull, 1024ull};
+const unsigned kQSubs11[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths11[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs12[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
 const int kQTypes12[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames12[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
-const unsigned long long kQOffs12[] = {1040ull, 1044ull, 1048ull, 1052ull, 1056ull, 1060ull, 1064ull, 1068ull, 1072ull, 1076ull, 1080ull, 1084ull, 1088ull, 1092ull, 1096ull, 1100ull, 1104ull, 1108ull, 1112ull, 1116ull, 1120ull, 1124ull, 1128ull, 1132ull, 1136ull, 1140ull};
+const unsigned long long kQOffs12[] = {1040ull, 1040ull, 1040ull, 1040ull, 1056ull, 1056ull, 1056ull, 1056ull, 1072ull, 1072ull, 1072ull, 1072ull, 1088ull, 1088ull, 1088ull, 1088ull, 1104ull, 1104ull, 1104ull, 1104ull, 1120ull, 1120ull, 1120ull, 1120ull, 1136ull, 1136ull};
+const unsigned kQSubs12[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths12[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs13[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u};
 const int kQTypes13[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames13[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn"};
-const unsigned long long kQOffs13[] = {1152ull, 1156ull, 1160ull, 1164ull, 1168ull, 1172ull, 1176ull, 1180ull, 1184ull, 1188ull, 1192ull, 1196ull, 1200ull, 1204ull, 1208ull, 1212ull, 1216ull, 1220ull, 1224ull, 1228ull, 1232ull, 1236ull, 1240ull};
+const unsigned long long kQOffs13[] = {1152ull, 1152ull, 1152ull, 1152ull, 1168ull, 1168ull, 1168ull, 1168ull, 1184ull, 1184ull, 1184ull, 1184ull, 1200ull, 1200ull, 1200ull, 1200ull, 1216ull, 1216ull, 1216ull, 1216ull, 1232ull, 1232ull, 1232ull};
+const unsigned kQSubs13[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths13[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs14[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u};
 const int kQTypes14[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames14[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2"};
-const unsigned long long kQOffs14[] = {1248ull, 1252ull, 1256ull, 1260ull, 1264ull, 1268ull, 1272ull, 1276ull, 1280ull, 1284ull, 1288ull, 1292ull, 1296ull, 1300ull, 1304ull, 1308ull, 1312ull, 1316ull, 1320ull};
+const unsigned long long kQOffs14[] = {1248ull, 1248ull, 1248ull, 1248ull, 1264ull, 1264ull, 1264ull, 1264ull, 1280ull, 1280ull, 1280ull, 1280ull, 1296ull, 1296ull, 1296ull, 1296ull, 1312ull, 1312ull, 1312ull};
+const unsigned kQSubs14[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths14[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs15[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u};
 const int kQTypes15[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames15[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2"};
-const unsigned long long kQOffs15[] = {1328ull, 1332ull, 1336ull, 1340ull, 1344ull, 1348ull, 1352ull, 1356ull, 1360ull, 1364ull, 1368ull, 1372ull, 1376ull, 1380ull, 1384ull, 1388ull, 1392ull, 1396ull, 1400ull, 1404ull, 1408ull, 1412ull, 1416ull, 1420ull, 1424ull};
+const unsigned long long kQOffs15[] = {1328ull, 1328ull, 1328ull, 1328ull, 1344ull, 1344ull, 1344ull, 1344ull, 1360ull, 1360ull, 1360ull, 1360ull, 1376ull, 1376ull, 1376ull, 1376ull, 1392ull, 1392ull, 1392ull, 1392ull, 1408ull, 1408ull, 1408ull, 1408ull, 1424ull};
+const unsigned kQSubs15[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths15[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs16[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 130u, 131u};
 const int kQTypes16[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames16[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "u0", "u1"};
-const unsigned long long kQOffs16[] = {1432ull, 1436ull, 1440ull, 1444ull, 1448ull, 1452ull, 1456ull, 1460ull, 1464ull, 1468ull, 1472ull, 1476ull, 1480ull, 1484ull, 1488ull, 1492ull, 1496ull, 1500ull, 1504ull, 1508ull, 1512ull, 1516ull, 1520ull, 1524ull, 1528ull, 1532ull, 1536ull};
+const unsigned long long kQOffs16[] = {1432ull, 1432ull, 1432ull, 1432ull, 1448ull, 1448ull, 1448ull, 1448ull, 1464ull, 1464ull, 1464ull, 1464ull, 1480ull, 1480ull, 1480ull, 1480ull, 1496ull, 1496ull, 1496ull, 1496ull, 1512ull, 1512ull, 1512ull, 1512ull, 1528ull, 1528ull, 1528ull};
+const unsigned kQSubs16[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths16[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs17[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 106u, 107u, 108u};
 const int kQTypes17[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames17[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "dx", "dy", "rr2"};
-const unsigned long long kQOffs17[] = {1544ull, 1548ull, 1552ull, 1556ull, 1560ull, 1564ull, 1568ull, 1572ull, 1576ull, 1580ull, 1584ull, 1588ull, 1592ull, 1596ull, 1600ull, 1604ull, 1608ull, 1612ull, 1616ull, 1620ull, 1624ull, 1628ull, 1632ull, 1636ull, 1640ull, 1644ull, 1648ull, 1652ull};
+const unsigned long long kQOffs17[] = {1544ull, 1544ull, 1544ull, 1544ull, 1560ull, 1560ull, 1560ull, 1560ull, 1576ull, 1576ull, 1576ull, 1576ull, 1592ull, 1592ull, 1592ull, 1592ull, 1608ull, 1608ull, 1608ull, 1608ull, 1624ull, 1624ull, 1624ull, 1624ull, 1640ull, 1640ull, 1640ull, 1640ull};
+const unsigned kQSubs17[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths17[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs18[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 88u, 92u, 93u, 94u};
 const int kQTypes18[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames18[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "into", "nl0", "nl1", "nl2"};
-const unsigned long long kQOffs18[] = {1664ull, 1668ull, 1672ull, 1676ull, 1680ull, 1684ull, 1688ull, 1692ull, 1696ull, 1700ull, 1704ull, 1708ull, 1712ull, 1716ull, 1720ull, 1724ull, 1728ull, 1732ull, 1736ull, 1740ull, 1744ull, 1748ull, 1752ull, 1756ull, 1760ull, 1764ull, 1768ull};
+const unsigned long long kQOffs18[] = {1664ull, 1664ull, 1664ull, 1664ull, 1680ull, 1680ull, 1680ull, 1680ull, 1696ull, 1696ull, 1696ull, 1696ull, 1712ull, 1712ull, 1712ull, 1712ull, 1728ull, 1728ull, 1728ull, 1728ull, 1744ull, 1744ull, 1744ull, 1744ull, 1760ull, 1760ull, 1760ull};
+const unsigned kQSubs18[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths18[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs19[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 88u, 111u, 112u, 113u};
 const int kQTypes19[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames19[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "into", "nnt", "ddn", "c2"};
-const unsigned long long kQOffs19[] = {1776ull, 1780ull, 1784ull, 1788ull, 1792ull, 1796ull, 1800ull, 1804ull, 1808ull, 1812ull, 1816ull, 1820ull, 1824ull, 1828ull, 1832ull, 1836ull, 1840ull, 1844ull, 1848ull, 1852ull, 1856ull, 1860ull, 1864ull, 1868ull, 1872ull, 1876ull, 1880ull};
+const unsigned long long kQOffs19[] = {1776ull, 1776ull, 1776ull, 1776ull, 1792ull, 1792ull, 1792ull, 1792ull, 1808ull, 1808ull, 1808ull, 1808ull, 1824ull, 1824ull, 1824ull, 1824ull, 1840ull, 1840ull, 1840ull, 1840ull, 1856ull, 1856ull, 1856ull, 1856ull, 1872ull, 1872ull, 1872ull};
+const unsigned kQSubs19[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths19[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs20[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 117u, 118u, 119u, 127u, 128u, 129u, 130u};
 const int kQTypes20[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32};
 const char* const kQNames20[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "td0", "td1", "td2", "pp", "rp", "tp", "u0"};
-const unsigned long long kQOffs20[] = {1888ull, 1892ull, 1896ull, 1900ull, 1904ull, 1908ull, 1912ull, 1916ull, 1920ull, 1924ull, 1928ull, 1932ull, 1936ull, 1940ull, 1944ull, 1948ull, 1952ull, 1956ull, 1960ull, 1964ull, 1968ull, 1972ull, 1976ull, 1980ull, 1984ull, 1988ull, 1992ull, 1996ull, 2000ull, 2004ull};
+const unsigned long long kQOffs20[] = {1888ull, 1888ull, 1888ull, 1888ull, 1904ull, 1904ull, 1904ull, 1904ull, 1920ull, 1920ull, 1920ull, 1920ull, 1936ull, 1936ull, 1936ull, 1936ull, 1952ull, 1952ull, 1952ull, 1952ull, 1968ull, 1968ull, 1968ull, 1968ull, 1984ull, 1984ull, 1984ull, 1984ull, 2000ull, 2000ull};
+const unsigned kQSubs20[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths20[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs21[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 128u};
 const int kQTypes21[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames21[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "rp"};
-const unsigned long long kQOffs21[] = {2016ull, 2020ull, 2024ull, 2028ull, 2032ull, 2036ull, 2040ull, 2044ull, 2048ull, 2052ull, 2056ull, 2060ull, 2064ull, 2068ull, 2072ull, 2076ull, 2080ull, 2084ull, 2088ull, 2092ull, 2096ull, 2100ull, 2104ull, 2108ull};
+const unsigned long long kQOffs21[] = {2016ull, 2016ull, 2016ull, 2016ull, 2032ull, 2032ull, 2032ull, 2032ull, 2048ull, 2048ull, 2048ull, 2048ull, 2064ull, 2064ull, 2064ull, 2064ull, 2080ull, 2080ull, 2080ull, 2080ull, 2096ull, 2096ull, 2096ull, 2096ull};
+const unsigned kQSubs21[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths21[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs22[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 117u, 118u, 119u, 129u};
 const int kQTypes22[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames22[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "td0", "td1", "td2", "tp"};
-const unsigned long long kQOffs22[] = {2120ull, 2124ull, 2128ull, 2132ull, 2136ull, 2140ull, 2144ull, 2148ull, 2152ull, 2156ull, 2160ull, 2164ull, 2168ull, 2172ull, 2176ull, 2180ull, 2184ull, 2188ull, 2192ull, 2196ull};
+const unsigned long long kQOffs22[] = {2120ull, 2120ull, 2120ull, 2120ull, 2136ull, 2136ull, 2136ull, 2136ull, 2152ull, 2152ull, 2152ull, 2152ull, 2168ull, 2168ull, 2168ull, 2168ull, 2184ull, 2184ull, 2184ull, 2184ull};
+const unsigned kQSubs22[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u};
+const unsigned kQWidths22[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs23[] = {3u, 4u, 5u, 7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u, 26u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u, 87u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u, 117u, 118u, 119u, 127u, 128u, 129u};
 const int kQTypes23[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames23[] = {"L0", "L1", "L2", "w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1", "rpt", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2", "dn", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2", "td0", "td1", "td2", "pp", "rp", "tp"};
-const unsigned long long kQOffs23[] = {2208ull, 2212ull, 2216ull, 2220ull, 2224ull, 2228ull, 2232ull, 2236ull, 2240ull, 2244ull, 2248ull, 2252ull, 2256ull, 2260ull, 2264ull, 2268ull, 2272ull, 2276ull, 2280ull, 2284ull, 2288ull, 2292ull, 2296ull, 2300ull, 2304ull, 2308ull, 2312ull, 2316ull, 2320ull, 2324ull, 2328ull, 2332ull, 2336ull, 2340ull, 2344ull, 2348ull, 2352ull, 2356ull, 2360ull, 2364ull, 2368ull, 2372ull, 2376ull, 2380ull, 2384ull, 2388ull, 2392ull, 2396ull, 2400ull, 2404ull, 2408ull, 2412ull, 2416ull, 2420ull, 2424ull};
+const unsigned long long kQOffs23[] = {2208ull, 2208ull, 2208ull, 2208ull, 2224ull, 2224ull, 2224ull, 2224ull, 2240ull, 2240ull, 2240ull, 2240ull, 2256ull, 2256ull, 2256ull, 2256ull, 2272ull, 2272ull, 2272ull, 2272ull, 2288ull, 2288ull, 2288ull, 2288ull, 2304ull, 2304ull, 2304ull, 2304ull, 2320ull, 2320ull, 2320ull, 2320ull, 2336ull, 2336ull, 2336ull, 2336ull, 2352ull, 2352ull, 2352ull, 2352ull, 2368ull, 2368ull, 2368ull, 2368ull, 2384ull, 2384ull, 2384ull, 2384ull, 2400ull, 2400ull, 2400ull, 2400ull, 2416ull, 2416ull, 2416ull};
+const unsigned kQSubs23[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths23[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs24[] = {7u, 9u, 11u, 12u, 13u, 14u, 15u, 16u, 17u, 20u, 21u, 22u, 23u, 24u, 25u};
 const int kQTypes24[] = {LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32};
 const char* const kQNames24[] = {"w", "h", "k0", "soff", "scnt", "cam0", "cam1", "cam2", "tanf", "smp", "px", "py", "k2", "c0", "c1"};
-const unsigned long long kQOffs24[] = {2432ull, 2436ull, 2440ull, 2444ull, 2448ull, 2452ull, 2456ull, 2460ull, 2464ull, 2468ull, 2472ull, 2476ull, 2480ull, 2484ull, 2488ull};
+const unsigned long long kQOffs24[] = {2432ull, 2432ull, 2432ull, 2432ull, 2448ull, 2448ull, 2448ull, 2448ull, 2464ull, 2464ull, 2464ull, 2464ull, 2480ull, 2480ull, 2480ull};
+const unsigned kQSubs24[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u};
+const unsigned kQWidths24[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs25[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 49u, 50u, 51u, 52u, 76u, 77u, 78u, 79u, 80u, 81u, 82u, 83u, 84u, 85u};
 const int kQTypes25[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames25[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "T0", "T1", "T2", "depth", "cr", "cg", "cb", "mat", "x0", "x1", "x2", "n0", "n1", "n2"};
-const unsigned long long kQOffs25[] = {2496ull, 2500ull, 2504ull, 2508ull, 2512ull, 2516ull, 2520ull, 2524ull, 2528ull, 2532ull, 2536ull, 2540ull, 2544ull, 2548ull, 2552ull, 2556ull, 2560ull, 2564ull, 2568ull, 2572ull, 2576ull, 2580ull, 2584ull, 2588ull, 2592ull, 2596ull};
+const unsigned long long kQOffs25[] = {2496ull, 2496ull, 2496ull, 2496ull, 2512ull, 2512ull, 2512ull, 2512ull, 2528ull, 2528ull, 2528ull, 2528ull, 2544ull, 2544ull, 2544ull, 2544ull, 2560ull, 2560ull, 2560ull, 2560ull, 2576ull, 2576ull, 2576ull, 2576ull, 2592ull, 2592ull};
+const unsigned kQSubs25[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u};
+const unsigned kQWidths25[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u};
 const uint32_t kQRegs26[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 92u, 93u, 94u, 100u, 101u, 102u, 103u, 104u, 105u};
 const int kQTypes26[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames26[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "nl0", "nl1", "nl2", "uu0", "uu1", "uu2", "vv0", "vv1", "vv2"};
-const unsigned long long kQOffs26[] = {2608ull, 2612ull, 2616ull, 2620ull, 2624ull, 2628ull, 2632ull, 2636ull, 2640ull, 2644ull, 2648ull, 2652ull, 2656ull, 2660ull, 2664ull, 2668ull, 2672ull, 2676ull, 2680ull, 2684ull, 2688ull, 2692ull, 2696ull, 2700ull, 2704ull};
+const unsigned long long kQOffs26[] = {2608ull, 2608ull, 2608ull, 2608ull, 2624ull, 2624ull, 2624ull, 2624ull, 2640ull, 2640ull, 2640ull, 2640ull, 2656ull, 2656ull, 2656ull, 2656ull, 2672ull, 2672ull, 2672ull, 2672ull, 2688ull, 2688ull, 2688ull, 2688ull, 2704ull};
+const unsigned kQSubs26[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths26[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const uint32_t kQRegs27[] = {3u, 4u, 5u, 11u, 12u, 13u, 23u, 24u, 25u, 42u, 43u, 44u, 46u, 47u, 48u, 49u, 50u, 51u, 52u, 83u, 84u, 85u, 87u, 117u, 118u, 119u, 127u, 128u, 129u};
 const int kQTypes27[] = {LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_U32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32, LOOM_B200_F32};
 const char* const kQNames27[] = {"L0", "L1", "L2", "k0", "soff", "scnt", "k2", "c0", "c1", "d0", "d1", "d2", "o0", "o1", "o2", "T0", "T1", "T2", "depth", "n0", "n1", "n2", "dn", "td0", "td1", "td2", "pp", "rp", "tp"};
-const unsigned long long kQOffs27[] = {2712ull, 2716ull, 2720ull, 2724ull, 2728ull, 2732ull, 2736ull, 2740ull, 2744ull, 2748ull, 2752ull, 2756ull, 2760ull, 2764ull, 2768ull, 2772ull, 2776ull, 2780ull, 2784ull, 2788ull, 2792ull, 2796ull, 2800ull, 2804ull, 2808ull, 2812ull, 2816ull, 2820ull, 2824ull};
+const unsigned long long kQOffs27[] = {2712ull, 2712ull, 2712ull, 2712ull, 2728ull, 2728ull, 2728ull, 2728ull, 2744ull, 2744ull, 2744ull, 2744ull, 2760ull, 2760ull, 2760ull, 2760ull, 2776ull, 2776ull, 2776ull, 2776ull, 2792ull, 2792ull, 2792ull, 2792ull, 2808ull, 2808ull, 2808ull, 2808ull, 2824ull};
+const unsigned kQSubs27[] = {0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u, 4u, 8u, 12u, 0u};
+const unsigned kQWidths27[] = {16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 16u, 8u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 2u, kQRegs0, kQTypes0, kQNames0},
     {1u, -1, 17u, kQRegs1, kQTypes1, kQNames1},
@@ -2692,34 +3770,34 @@ const loom_b200_queue_layout kQueues[] = {
     {23u, 3, 29u, kQRegs27, kQTypes27, kQNames27},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
-    {kQOffs1, 84ull},
-    {kQOffs2, 164ull},
-    {kQOffs3, 260ull},
-    {kQOffs4, 348ull},
-    {kQOffs5, 436ull},
-    {kQOffs6, 476ull},
-    {kQOffs7, 584ull},
-    {kQOffs8, 696ull},
-    {kQOffs9, 808ull},
-    {kQOffs10, 924ull},
-    {kQOffs11, 1036ull},
-    {kQOffs12, 1144ull},
-    {kQOffs13, 1244ull},
-    {kQOffs14, 1324ull},
-    {kQOffs15, 1428ull},
-    {kQOffs16, 1540ull},
-    {kQOffs17, 1656ull},
-    {kQOffs18, 1772ull},
-    {kQOffs19, 1884ull},
-    {kQOffs20, 2008ull},
-    {kQOffs21, 2112ull},
-    {kQOffs22, 2200ull},
-    {kQOffs23, 2428ull},
-    {kQOffs24, 2492ull},
-    {kQOffs25, 2600ull},
-    {kQOffs26, 2708ull},
-    {kQOffs27, 2828ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
+    {kQOffs1, kQSubs1, kQWidths1, 80ull, 4u, 8u},
+    {kQOffs2, kQSubs2, kQWidths2, 152ull, 12u, 16u},
+    {kQOffs3, kQSubs3, kQWidths3, 248ull, 12u, 16u},
+    {kQOffs4, kQSubs4, kQWidths4, 344ull, 4u, 8u},
+    {kQOffs5, kQSubs5, kQWidths5, 432ull, 4u, 8u},
+    {kQOffs6, kQSubs6, kQWidths6, 472ull, 4u, 8u},
+    {kQOffs7, kQSubs7, kQWidths7, 576ull, 8u, 16u},
+    {kQOffs8, kQSubs8, kQWidths8, 688ull, 8u, 16u},
+    {kQOffs9, kQSubs9, kQWidths9, 800ull, 8u, 16u},
+    {kQOffs10, kQSubs10, kQWidths10, 912ull, 12u, 16u},
+    {kQOffs11, kQSubs11, kQWidths11, 1024ull, 12u, 16u},
+    {kQOffs12, kQSubs12, kQWidths12, 1136ull, 8u, 16u},
+    {kQOffs13, kQSubs13, kQWidths13, 1232ull, 12u, 16u},
+    {kQOffs14, kQSubs14, kQWidths14, 1312ull, 12u, 16u},
+    {kQOffs15, kQSubs15, kQWidths15, 1424ull, 4u, 8u},
+    {kQOffs16, kQSubs16, kQWidths16, 1528ull, 12u, 16u},
+    {kQOffs17, kQSubs17, kQWidths17, 1656ull, 0u, 4u},
+    {kQOffs18, kQSubs18, kQWidths18, 1760ull, 12u, 16u},
+    {kQOffs19, kQSubs19, kQWidths19, 1872ull, 12u, 16u},
+    {kQOffs20, kQSubs20, kQWidths20, 2000ull, 8u, 16u},
+    {kQOffs21, kQSubs21, kQWidths21, 2112ull, 0u, 4u},
+    {kQOffs22, kQSubs22, kQWidths22, 2200ull, 0u, 4u},
+    {kQOffs23, kQSubs23, kQWidths23, 2416ull, 12u, 16u},
+    {kQOffs24, kQSubs24, kQWidths24, 2480ull, 12u, 16u},
+    {kQOffs25, kQSubs25, kQWidths25, 2592ull, 8u, 16u},
+    {kQOffs26, kQSubs26, kQWidths26, 2704ull, 4u, 8u},
+    {kQOffs27, kQSubs27, kQWidths27, 2824ull, 4u, 8u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

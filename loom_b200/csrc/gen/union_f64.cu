@@ -130,9 +130,16 @@ struct K
         switch(q)
         {
         case 0: // START
-            reinterpret_cast<double*>(base + 0ull * cap)[idx] = R.r0;
-            reinterpret_cast<unsigned*>(base + 8ull * cap)[idx] = tid;
+        {
+            {
+                uint4 v0;
+                { const unsigned long long b = bitcast<unsigned long long>(R.r0);
+                  v0.x = static_cast<unsigned>(b); v0.y = static_cast<unsigned>(b >> 32); }
+                v0.z = tid;
+                reinterpret_cast<uint4*>(base + 0ull * cap)[idx] = v0;
+            }
             return;
+        }
         default: return;
         }
     }
@@ -145,8 +152,11 @@ struct K
         switch(q)
         {
         case 0: // START
-            R.r0 = reinterpret_cast<const double*>(base + 0ull * cap)[idx];
-            return reinterpret_cast<const unsigned*>(base + 8ull * cap)[idx];
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(base + 0ull * cap)[idx];
+            R.r0 = bitcast<double>((static_cast<unsigned long long>(v0.y) << 32) | v0.x);
+            return v0.z;
+        }
         default: return 0xffffffffu;
         }
     }
@@ -168,11 +178,13 @@ const uint32_t kQRegs0[] = {0u};
 const int kQTypes0[] = {LOOM_B200_F64};
 const char* const kQNames0[] = {"i"};
 const unsigned long long kQOffs0[] = {0ull};
+const unsigned kQSubs0[] = {0u};
+const unsigned kQWidths0[] = {16u};
 const loom_b200_queue_layout kQueues[] = {
     {0u, -1, 1u, kQRegs0, kQTypes0, kQNames0},
 };
 const QueueSegment kSegments[] = {
-    {kQOffs0, 8ull},
+    {kQOffs0, kQSubs0, kQWidths0, 0ull, 8u, 16u},
 };
 
 cudaError_t launch_plain(const PlainLaunch& a)

@@ -1142,9 +1142,12 @@ loom_b200_parked_dump(loom_b200_handle* h,
     {
         if(!cols[k]) continue;
         const size_t width = type_bytes(ql.types[k]);
-        LB_CUDA(cudaMemcpy(cols[k], half + seg.col_off[k] * cap, n * width, cudaMemcpyDeviceToHost));
+        LB_CUDA(cudaMemcpy2D(cols[k], width, half + seg.col_off[k] * cap + seg.col_sub[k], seg.col_width[k],
+                             width, n, cudaMemcpyDeviceToHost));
     }
-    if(tids) LB_CUDA(cudaMemcpy(tids, half + seg.tid_off * cap, n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if(tids)
+        LB_CUDA(cudaMemcpy2D(tids, sizeof(uint32_t), half + seg.tid_off * cap + seg.tid_sub, seg.tid_width,
+                             sizeof(uint32_t), n, cudaMemcpyDeviceToHost));
     *rows = n;
     return LOOM_B200_OK;
 }

@@ -37,14 +37,20 @@ struct RegroupLaunch
     cudaStream_t  stream;
 };
 
-/// Where one queue's columns lie in a row of the regrouping state: column c
-/// of queue q holds `cap` values from byte `col_off[c] * cap` of the state
-/// half of the round's parity, the thread ids (low 32 bits) from
-/// `tid_off * cap`.
+/// Where one queue's columns lie in a row of the regrouping state: the
+/// values of column c sit in slots of col_width[c] bytes per entry (16 for
+/// four 32-bit values packed together), `cap` slots from byte
+/// `col_off[c] * cap` of the state half of the round's parity, at byte
+/// col_sub[c] of each slot; the thread ids (low 32 bits) likewise at
+/// tid_off / tid_sub / tid_width.
 struct QueueSegment
 {
     const unsigned long long* col_off;
+    const unsigned*           col_sub;
+    const unsigned*           col_width;
     unsigned long long        tid_off;
+    unsigned                  tid_sub;
+    unsigned                  tid_width;
 };
 
 /// One compiled kernel: its descriptor and the launchers of both engines.
