@@ -401,6 +401,8 @@ def generate(k: Kernel) -> str:
     w(f"    static constexpr int kNumBlocks = {nb};")
     w(f"    static constexpr int kNumQueues = {nq};")
     w(f"    static constexpr int kRegroupMaxRegs = {REGROUP_MAX_REGS};")
+    # small kernels: two inlined copies of their code in the megakernel
+    w(f"    static constexpr bool kSplitCallSites = {'true' if sum(counts) <= REG_VARIANT_MIN_INSTR else 'false'};")
     w("    struct Regs")
     w("    {")
     for r in regs:

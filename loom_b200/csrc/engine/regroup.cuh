@@ -350,8 +350,10 @@ regroup_kernel(const RegroupParams p)
                 // along its own path, the hardware reconverging the warp as
                 // in the plain engine; schedules 0 and 1 run the chosen group
                 // (or every live lane once the group has spread_lanes).
-                // One call site keeps one copy of the kernel's code in the
-                // megakernel (self-loops spin only in the stepped schedule).
+                // Large kernels keep one copy of their code in the megakernel
+                // (one call site, the spin count a runtime value); small ones
+                // get a call site per kind of step, so that a tight
+                // self-loop is compiled with its spin count known.
                 const bool minpc = p.schedule == 2u;
                 for(unsigned i = 0; i < (minpc ? p.burst : 1u); ++i)
                 {
@@ -373,8 +375,18 @@ regroup_kernel(const RegroupParams p)
                     else
                         run = pc >= 0 && (p.schedule == 3u || mc >= p.spread || pc == m);
                     if(run)
-                        pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
-                                                          cost_on && p.schedule < 2u, minpc ? kSelfLoopSpin : 0u);
+                    {
+                        if constexpr(K::kSplitCallSites)
+                        {
+                            if(minpc)
+                                pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, kSelfLoopSpin);
+                            else
+                                pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on && p.schedule < 2u);
+                        }
+                        else
+                            pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
+                                                              cost_on && p.schedule < 2u, minpc ? kSelfLoopSpin : 0u);
+                    }
                 }
                 if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);

@@ -17,6 +17,7 @@ struct K
     static constexpr int kNumBlocks = 1;
     static constexpr int kNumQueues = 1;
     static constexpr int kRegroupMaxRegs = 64;
+    static constexpr bool kSplitCallSites = true;
     struct Regs
     {
         unsigned char r0; // a: u8

@@ -17,6 +17,7 @@ struct K
     static constexpr int kNumBlocks = 3;
     static constexpr int kNumQueues = 3;
     static constexpr int kRegroupMaxRegs = 64;
+    static constexpr bool kSplitCallSites = true;
     struct Regs
     {
         unsigned int r1; // a: u32

@@ -17,6 +17,7 @@ struct K
     static constexpr int kNumBlocks = 5;
     static constexpr int kNumQueues = 5;
     static constexpr int kRegroupMaxRegs = 64;
+    static constexpr bool kSplitCallSites = true;
     struct Regs
     {
         unsigned short r1; // i: u16

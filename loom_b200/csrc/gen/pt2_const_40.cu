@@ -17,6 +17,7 @@ struct K
     static constexpr int kNumBlocks = 55;
     static constexpr int kNumQueues = 55;
     static constexpr int kRegroupMaxRegs = 64;
+    static constexpr bool kSplitCallSites = false;
     struct Regs
     {
         unsigned int r1; // ppp: u32
