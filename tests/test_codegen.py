@@ -84,3 +84,49 @@ def test_collatz_loop_header_and_quorum():
     # START: 3 instructions, 1 live register (n) -> ceil(32 * 1 / 5) = 7;
     # loop: 8 instructions, 2 live registers (n, steps) -> ceil(32 * 5 / 11) = 15
     assert _table(src, "kQuorumTab") == [7, 15]
+
+
+@pytest.mark.parametrize("name", KERNELS)
+def test_queue_rows_pack_every_live_register_once(name):
+    """The queue row layout (16-byte slots): every live register of every
+    queue and the thread id sit in exactly one slot, at an offset inside the
+    slot that is a multiple of their size, without overlapping; slots of 16,
+    8 or 4 bytes hold only 4- and 8-byte values, narrow registers get slots
+    of their own; the segments of the queues follow one another and every
+    segment ends on 8 bytes."""
+    k = ir.load(name)
+    L = E.Lowering(k)
+    qlive = k.queue_liveness()
+    start = 0
+    for q in range(len(k.queues())):
+        lay = E.pack_slots([(r, L.regs[r].nbytes) for r in qlive[q]], start)
+        seen = {}
+        used = {}
+        for off, width, contents in lay["slots"]:
+            assert width in (1, 2, 4, 8, 16) and off >= start
+            for it, sub in contents:
+                n = 4 if it == "tid" else L.regs[it].nbytes
+                assert it not in seen
+                seen[it] = (off, sub, width)
+                assert sub % n == 0 and sub + n <= width
+                if width >= 4:
+                    assert n in (4, 8)
+                for byte in range(off + sub, off + sub + n):
+                    assert byte not in used, (name, q, it)
+                    used[byte] = it
+        assert set(seen) == set(qlive[q]) | {"tid"}
+        assert lay["cols"] == {r: seen[r] for r in qlive[q]} and lay["tid"] == seen["tid"]
+        assert lay["end"] % 8 == 0 and lay["end"] >= max(used) + 1
+        start = lay["end"]
+    src = (GEN / f"{name}.cu").read_text()
+    assert f"static constexpr unsigned long long kRowBytes = {start}ull;" in src
+
+
+def test_slot_packing_of_a_mixed_row():
+    """Two 8-byte and five 4-byte registers with the thread id: one slot of
+    the two 8-byte values, one of four 4-byte values, one of the fifth and
+    the id; a 1-byte register on its own."""
+    lay = E.pack_slots([(0, 8), (1, 4), (2, 8), (3, 4), (4, 4), (5, 4), (6, 4), (7, 1)], 0)
+    assert [(o, w, [i for i, _ in c]) for o, w, c in lay["slots"]] == [
+        (0, 16, [0, 2]), (16, 16, [1, 3, 4, 5]), (32, 8, [6, "tid"]), (40, 1, [7])]
+    assert lay["end"] == 48
