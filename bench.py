@@ -1139,7 +1139,7 @@ def serve_main(args, warmup, world, rank, local):
     if world > 1:
         torch.cuda.set_device(local)
     out, clocks = serve_measure(args.serve_seconds, rank, local)
-    full = out["regroup"]["loads"][-1]
+    full = out["regroup_serial"]["loads"][-1]
     line = base_line(
         args, warmup, world,
         "serving: Poisson arrivals at 25/50/75/100 % of measured capacity; mix 60 % render requests "
@@ -1152,9 +1152,9 @@ def serve_main(args, warmup, world, rank, local):
             "value": full["msamples_s"],
             "p50_ms": full["p50_ms"],
             "p99_ms": full["p99_ms"],
-            "fraction_of_capacity": round(full["msamples_s"] / out["regroup"]["capacity_msamples_s"], 4),
-            "regroup": out["regroup"],
+            "fraction_of_capacity": round(full["msamples_s"] / out["regroup_serial"]["capacity_msamples_s"], 4),
             "regroup_serial": out["regroup_serial"],
+            "regroup_overlapping": out["regroup"],
             "plain": out["plain"],
             "gpu_launches": None,
             "clocks": clocks,
@@ -1547,18 +1547,18 @@ def main() -> None:
         for name in ("loom_pt_512", "loom_pt2_512"):
             configs[name] = sub_config(name, api, torch, stream, 3, 3, dist, world, args.no_cpu)
         sv, sv_clk = serve_measure(1.0, rank, local, parity=not args.no_cpu)
-        full = sv["regroup"]["loads"][-1]
+        full = sv["regroup_serial"]["loads"][-1]
         configs["serve"] = {
             "workload": "serving: Poisson arrivals at 25/50/75/100 % of measured capacity (1 s per load); mix "
                         "60 % render requests (batched-workload distribution), 20 % Collatz batches 2^16-2^22, "
-                        "20 % Fibonacci batches 2^16-2^20",
+                        "20 % Fibonacci batches 2^16-2^20; 100 GB thread-state budget shared by the servers",
             "value": full["msamples_s"],
-            "unit": "Msamples/s at 100 % offered load",
+            "unit": "Msamples/s at 100 % offered load (regrouping servers stepped one after the other)",
             "p50_ms": full["p50_ms"],
             "p99_ms": full["p99_ms"],
-            "fraction_of_capacity": round(full["msamples_s"] / sv["regroup"]["capacity_msamples_s"], 4),
-            "regroup": sv["regroup"],
+            "fraction_of_capacity": round(full["msamples_s"] / sv["regroup_serial"]["capacity_msamples_s"], 4),
             "regroup_serial": sv["regroup_serial"],
+            "regroup_overlapping": sv["regroup"],
             "plain": sv["plain"],
             "parity": sv["regroup"].pop("parity", None),
             "clocks": sv_clk,

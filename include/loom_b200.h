@@ -152,7 +152,12 @@ typedef struct loom_b200_opts
                              once this many of the warp's lanes stand at it,
                              or when no other block is left; its lanes wait
                              while the others catch up (0 = off) */
-    uint32_t pad1;
+    uint32_t bulk_restore; /* regroup: full tiles of parked threads come back
+                              through shared memory, one bulk copy (TMA,
+                              cp.async.bulk, no multicast) per 16-byte slot
+                              column, instead of 128-bit loads from HBM; the
+                              CTA size is halved until the staging area
+                              fits in shared memory */
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

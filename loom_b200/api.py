@@ -119,7 +119,7 @@ class Opts(ctypes.Structure):
         ("max_regs", ctypes.c_uint32),
         ("plain_below", ctypes.c_uint64),
         ("defer_lanes", ctypes.c_uint32),
-        ("pad1", ctypes.c_uint32),
+        ("bulk_restore", ctypes.c_uint32),
     ]
 
 
@@ -520,6 +520,7 @@ def make_opts(
     max_regs: int = 0,
     plain_below: int = 0,
     defer_lanes: int = 0,
+    bulk_restore: bool = False,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -545,6 +546,7 @@ def make_opts(
         max_regs=int(max_regs),
         plain_below=int(plain_below),
         defer_lanes=int(defer_lanes),
+        bulk_restore=1 if bulk_restore else 0,
     )
 
 

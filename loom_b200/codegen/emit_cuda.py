@@ -653,6 +653,88 @@ def generate(k: Kernel) -> str:
         w("        }")
         w("    }")
         w("")
+    # ---- bulk-copy restore: a tile's 32 entries of every slot column are 32
+    # consecutive slots, so one cp.async.bulk per slot column brings the
+    # tile into shared memory, where each lane reads its own entries
+    stage_rows = []
+    for qi in range(nq):
+        stage_rows.append(sum(wdt for _, wdt, _ in layout[qi]["slots"]))
+    max_stage = max(stage_rows) if stage_rows else 16
+    max_stage = (max_stage + 15) // 16 * 16
+    w("    // bytes of one queue entry's slots, the largest over the queues")
+    w(f"    static constexpr unsigned kMaxStageRow = {max_stage}u;")
+    w("    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q")
+    w("    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared")
+    w("    // memory) with one bulk copy per slot column, completing on the")
+    w("    // mbarrier at `mbar`; false (nothing issued) when an address is not on")
+    w("    // a 16-byte boundary.")
+    w("    __device__ __forceinline__ static bool")
+    w("    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,")
+    w("               unsigned long long* mbar)")
+    w("    {")
+    w("        unsigned bytes = 0;")
+    w("        switch(q)")
+    w("        {")
+    for qi in range(nq):
+        w(f"        case {qi}: bytes = {32 * stage_rows[qi]}u; break;")
+    w("        default: return false;")
+    w("        }")
+    w("        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;")
+    w("        bulk_expect(mbar, bytes);")
+    w("        switch(q)")
+    w("        {")
+    for qi in range(nq):
+        w(f"        case {qi}:")
+        so = 0
+        for off, wdt, _ in layout[qi]["slots"]:
+            w(f"            bulk_copy(stage + {so}u, base + {off}ull * cap + static_cast<unsigned long long>(toff) * {wdt}u, {32 * wdt}u, mbar);")
+            so += 32 * wdt
+        w("            break;")
+    w("        default: break;")
+    w("        }")
+    w("        return true;")
+    w("    }")
+    w("")
+    w("    // A lane's entry of a tile staged by bulk_issue; returns its thread id.")
+    w("    __device__ __forceinline__ static unsigned")
+    w("    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)")
+    w("    {")
+    w("        switch(q)")
+    w("        {")
+    for qi, (b, kk) in enumerate(queues):
+        w(f"        case {qi}:")
+        w("        {")
+        if kk is not None:
+            v = disp[b][0]
+            w(f"            R.r{v} = static_cast<{CTYPE[L.regs[v].storage]}>({kk});")
+        tid_expr = None
+        so = 0
+        for si, (off, wdt, contents) in enumerate(layout[qi]["slots"]):
+            vt = {16: "uint4", 8: "uint2", 4: "unsigned", 2: "unsigned short", 1: "unsigned char"}[wdt]
+            slot = f"reinterpret_cast<const {vt}*>(stage + {so}u)[lane]"
+            so += 32 * wdt
+            if wdt <= 2:
+                (r, _), = contents
+                w(f"            R.r{r} = bitcast<{CTYPE[L.regs[r].storage]}>({slot});")
+                continue
+            words = ["x", "y", "z", "w"][: wdt // 4] if wdt > 4 else [None]
+
+            def word(sub, si=si, words=words):
+                return f"v{si}" if words == [None] else f"v{si}.{words[sub // 4]}"
+
+            w(f"            const {vt} v{si} = {slot};")
+            for it, sub in contents:
+                if it == "tid":
+                    tid_expr = word(sub)
+                elif L.regs[it].nbytes == 8:
+                    w(f"            R.r{it} = bitcast<{CTYPE[L.regs[it].storage]}>((static_cast<unsigned long long>({word(sub + 4)}) << 32) | {word(sub)});")
+                else:
+                    w(f"            R.r{it} = bitcast<{CTYPE[L.regs[it].storage]}>({word(sub)});")
+        w(f"            return {tid_expr};")
+        w("        }")
+    w("        default: return 0xffffffffu;")
+    w("        }")
+    w("    }")
     w("};")
     w("")
     # ---- host side
@@ -736,16 +818,28 @@ def generate(k: Kernel) -> str:
     w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
     w("    const void* fn = regroup_fn(a.regs, a.profile);")
     w("    if(!fn) return cudaErrorInvalidValue;")
+    w("    if(a.dyn_smem)")
+    w("    {")
+    w("        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,")
+    w("                                                   static_cast<int>(a.dyn_smem));")
+    w("        if(e != cudaSuccess) return e;")
+    w("    }")
     w("    if(a.ordinary && a.params.slice_rounds == 1u)")
-    w("        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
-    w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);")
+    w("        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);")
+    w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);")
     w("}")
     w("")
-    w("cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)")
+    w("cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)")
     w("{")
     w("    const void* fn = regroup_fn(regs, profile);")
     w("    if(!fn) return cudaErrorInvalidValue;")
-    w("    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);")
+    w("    if(dyn_smem)")
+    w("    {")
+    w("        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,")
+    w("                                                   static_cast<int>(dyn_smem));")
+    w("        if(e != cudaSuccess) return e;")
+    w("    }")
+    w("    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);")
     w("}")
     w("")
     w(f"}} }} // namespace loom_b200::k_{name}")
@@ -756,7 +850,7 @@ def generate(k: Kernel) -> str:
     w(f"    &loom_b200::k_{name}::launch_plain, &loom_b200::k_{name}::launch_regroup,")
     w(f"    &loom_b200::k_{name}::regroup_occupancy,")
     w(f"    loom_b200::k_{name}::kQueues, loom_b200::k_{name}::kSegments,")
-    w(f"    loom_b200::k_{name}::kRegCaps, {len(caps)}u}};")
+    w(f"    loom_b200::k_{name}::kRegCaps, {len(caps)}u, loom_b200::k_{name}::K::kMaxStageRow}};")
     return "\n".join(o) + "\n"
 
 

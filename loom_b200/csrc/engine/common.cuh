@@ -247,6 +247,60 @@ table_load(const Columns& c, const unsigned idx)
     return bitcast<T>(__ldg(c.table + idx));
 }
 
+// ---- bulk copies (TMA, untiled, no multicast) into shared memory, for the
+// regrouping engine's staged tile restore.  Addresses on 16-byte boundaries
+// and sizes in multiples of 16 bytes (checked by the caller).
+
+__device__ __forceinline__ unsigned
+smem_addr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+/// An mbarrier with one expected arrival, visible to the bulk-copy unit.
+__device__ __forceinline__ void
+mbar_init(unsigned long long* mbar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+/// The one arrival of the mbarrier's current phase, which then completes
+/// once `bytes` have been copied into shared memory.
+__device__ __forceinline__ void
+bulk_expect(unsigned long long* mbar, const unsigned bytes)
+{
+    unsigned long long state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                 : "=l"(state)
+                 : "r"(smem_addr(mbar)), "r"(bytes)
+                 : "memory");
+    (void)state;
+}
+
+/// One bulk copy of `bytes` from global to shared memory, counted on `mbar`.
+__device__ __forceinline__ void
+bulk_copy(void* dst, const void* src, const unsigned bytes, unsigned long long* mbar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+                 : "memory");
+}
+
+/// Whether the mbarrier's phase of parity `phase` has completed.
+__device__ __forceinline__ bool
+mbar_try_wait(unsigned long long* mbar, const unsigned phase)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(mbar)), "r"(phase)
+                 : "memory");
+    return ok != 0u;
+}
+
 /// Block-wide sum of three counters into global memory, one atomic per warp.
 __device__ __forceinline__ void
 flush_counters(unsigned long long* dst,

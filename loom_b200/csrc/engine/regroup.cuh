@@ -106,7 +106,20 @@ struct RegroupParams
     // Schedule 2: a long block (K::long_block) runs only once this many of
     // the warp's lanes stand at it, or when no other block is left (0: off).
     unsigned            defer_lanes;
+    // Full tiles come back through shared memory: one bulk copy (TMA,
+    // cp.async.bulk) per slot column of the tile, then each lane reads its
+    // entry there (the launch's dynamic shared memory holds a staging area
+    // and an mbarrier per warp); 0 restores with 128-bit loads from HBM.
+    unsigned            bulk_restore;
 };
+
+/// Dynamic shared memory of a launch with bulk_restore: an mbarrier per warp
+/// (16-byte aligned block), then 32 entries of the largest queue row per warp.
+__host__ __device__ constexpr unsigned
+bulk_stage_bytes(const unsigned warps, const unsigned max_stage_row)
+{
+    return (warps * 8u + 15u) / 16u * 16u + warps * 32u * max_stage_row;
+}
 
 /// Iterations of a self-loop a lane runs within one step of schedule 2
 /// before the step ends at the loop's header.
@@ -250,6 +263,18 @@ regroup_kernel(const RegroupParams p)
     typename K::In     pf;
     unsigned long long pf_tid = ~0ull;
     const bool         cost_on = p.cost_model != 0u;
+    // staged restore: this warp's mbarrier and staging area
+    extern __shared__ __align__(16) unsigned char s_dyn[];
+    const unsigned      wib   = threadIdx.x >> 5;
+    unsigned long long* mbar  = reinterpret_cast<unsigned long long*>(s_dyn) + wib;
+    unsigned char*      stage = s_dyn + (blockDim.x / 32u * 8u + 15u) / 16u * 16u + wib * 32u * K::kMaxStageRow;
+    bool                bulk_ok    = p.bulk_restore != 0u;
+    unsigned            bulk_phase = 0;
+    if(bulk_ok)
+    {
+        if(lane == 0) mbar_init(mbar);
+        __syncwarp();
+    }
     // lanes a group at block b needs to keep running
     auto need = [&](const int b) -> unsigned
     {
@@ -309,10 +334,48 @@ regroup_kernel(const RegroupParams p)
             unsigned long long tid = 0;
             if(tb >= 0)
             {
+                bool staged = false;
+                if(bulk_ok && tk == 32u)
+                {
+                    // the tile through shared memory: lane 0 issues a bulk
+                    // copy per slot column, every lane waits (bounded) for
+                    // the mbarrier's phase
+                    bool issued = false;
+                    __syncwarp(); // the lanes' reads of the previous tile are done
+                    if(lane == 0)
+                    {
+                        // order those generic-proxy reads before the bulk
+                        // copies' writes to the same shared memory
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        issued = K::bulk_issue(tb, stage, p.state + static_cast<unsigned long long>(cur) * K::kRowBytes * p.cap,
+                                               p.cap, toff, mbar);
+                    }
+                    issued = __shfl_sync(FULL, issued ? 1u : 0u, 0) != 0u;
+                    if(issued)
+                    {
+                        bool     done = false;
+                        unsigned i    = 0;
+                        while(!(done = mbar_try_wait(mbar, bulk_phase)) && ++i < (1u << 20)) {}
+                        if(__all_sync(FULL, done))
+                        {
+                            bulk_phase ^= 1u;
+                            staged = true;
+                        }
+                        else
+                        {
+                            // the copy did not complete in time: restore from
+                            // HBM, and stage no more tiles in this launch
+                            ctx.flag(kStatusBarrierTimeout);
+                            bulk_ok = false;
+                        }
+                    }
+                    __syncwarp();
+                }
                 if(lane < tk)
                 {
                     // the queue keeps the low 32 bits of the thread id
-                    const unsigned t32 = K::restore(tb, R, p.state, p.cap, cur, toff + lane);
+                    const unsigned t32 = staged ? K::restore_stage(tb, R, stage, lane)
+                                                : K::restore(tb, R, p.state, p.cap, cur, toff + lane);
                     tid = p.cols.tid_base + static_cast<unsigned>(t32 - static_cast<unsigned>(p.cols.tid_base));
                     if(tid < p.n) { pc = K::block_of(tb); sbytes += K::live_bytes(tb) + 4u; }
                     else ctx.flag(kStatusQueueOverrun);

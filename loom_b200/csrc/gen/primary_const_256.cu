@@ -4101,6 +4101,1524 @@ struct K
         }
     }
 
+    // bytes of one queue entry's slots, the largest over the queues
+    static constexpr unsigned kMaxStageRow = 176u;
+    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q
+    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared
+    // memory) with one bulk copy per slot column, completing on the
+    // mbarrier at `mbar`; false (nothing issued) when an address is not on
+    // a 16-byte boundary.
+    __device__ __forceinline__ static bool
+    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,
+               unsigned long long* mbar)
+    {
+        unsigned bytes = 0;
+        switch(q)
+        {
+        case 0: bytes = 512u; break;
+        case 1: bytes = 1664u; break;
+        case 2: bytes = 2816u; break;
+        case 3: bytes = 4864u; break;
+        case 4: bytes = 4608u; break;
+        case 5: bytes = 4608u; break;
+        case 6: bytes = 4352u; break;
+        case 7: bytes = 5248u; break;
+        case 8: bytes = 4864u; break;
+        case 9: bytes = 4096u; break;
+        case 10: bytes = 3072u; break;
+        case 11: bytes = 2688u; break;
+        case 12: bytes = 4352u; break;
+        case 13: bytes = 4096u; break;
+        case 14: bytes = 3584u; break;
+        case 15: bytes = 3072u; break;
+        case 16: bytes = 2688u; break;
+        case 17: bytes = 3328u; break;
+        case 18: bytes = 3200u; break;
+        case 19: bytes = 3200u; break;
+        case 20: bytes = 3328u; break;
+        case 21: bytes = 3328u; break;
+        case 22: bytes = 3200u; break;
+        case 23: bytes = 3072u; break;
+        case 24: bytes = 3072u; break;
+        case 25: bytes = 3072u; break;
+        case 26: bytes = 2688u; break;
+        case 27: bytes = 3072u; break;
+        case 28: bytes = 3584u; break;
+        case 29: bytes = 3328u; break;
+        case 30: bytes = 3072u; break;
+        case 31: bytes = 1792u; break;
+        case 32: bytes = 768u; break;
+        default: return false;
+        }
+        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;
+        bulk_expect(mbar, bytes);
+        switch(q)
+        {
+        case 0:
+            bulk_copy(stage + 0u, base + 0ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 1:
+            bulk_copy(stage + 0u, base + 16ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 32ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 48ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 64ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 2:
+            bulk_copy(stage + 0u, base + 72ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 88ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 152ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 3:
+            bulk_copy(stage + 0u, base + 160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 304ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 4:
+            bulk_copy(stage + 0u, base + 312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 5:
+            bulk_copy(stage + 0u, base + 456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 6:
+            bulk_copy(stage + 0u, base + 600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 728ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 7:
+            bulk_copy(stage + 0u, base + 736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 896ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 8:
+            bulk_copy(stage + 0u, base + 904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1048ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 9:
+            bulk_copy(stage + 0u, base + 1056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 10:
+            bulk_copy(stage + 0u, base + 1184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 11:
+            bulk_copy(stage + 0u, base + 1280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1360ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 12:
+            bulk_copy(stage + 0u, base + 1368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1496ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 13:
+            bulk_copy(stage + 0u, base + 1504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 14:
+            bulk_copy(stage + 0u, base + 1632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 15:
+            bulk_copy(stage + 0u, base + 1744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 16:
+            bulk_copy(stage + 0u, base + 1840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1920ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 17:
+            bulk_copy(stage + 0u, base + 1928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2024ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 18:
+            bulk_copy(stage + 0u, base + 2032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2128ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 19:
+            bulk_copy(stage + 0u, base + 2136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2232ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 20:
+            bulk_copy(stage + 0u, base + 2240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2336ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 21:
+            bulk_copy(stage + 0u, base + 2344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2440ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 22:
+            bulk_copy(stage + 0u, base + 2448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2544ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 23:
+            bulk_copy(stage + 0u, base + 2552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 24:
+            bulk_copy(stage + 0u, base + 2648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 25:
+            bulk_copy(stage + 0u, base + 2744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 26:
+            bulk_copy(stage + 0u, base + 2840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2920ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 27:
+            bulk_copy(stage + 0u, base + 2928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 28:
+            bulk_copy(stage + 0u, base + 3024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 29:
+            bulk_copy(stage + 0u, base + 3136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3232ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 30:
+            bulk_copy(stage + 0u, base + 3240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 31:
+            bulk_copy(stage + 0u, base + 3336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3384ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 32:
+            bulk_copy(stage + 0u, base + 3392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3408ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        default: break;
+        }
+        return true;
+    }
+
+    // A lane's entry of a tile staged by bulk_issue; returns its thread id.
+    __device__ __forceinline__ static unsigned
+    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)
+    {
+        switch(q)
+        {
+        case 0:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r53 = bitcast<unsigned int>(v0.y);
+            return v0.z;
+        }
+        case 1:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r17 = bitcast<unsigned int>(v2.z);
+            R.r53 = bitcast<unsigned int>(v2.w);
+            const unsigned v3 = reinterpret_cast<const unsigned*>(stage + 1536u)[lane];
+            return v3;
+        }
+        case 2:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(stage + 2560u)[lane];
+            R.r53 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
+        case 3:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r42 = bitcast<float>(v8.x);
+            R.r50 = bitcast<float>(v8.y);
+            R.r51 = bitcast<float>(v8.z);
+            R.r52 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r53 = bitcast<unsigned int>(v9.x);
+            return v9.y;
+        }
+        case 4:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r17 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r21 = bitcast<float>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r27 = bitcast<float>(v4.z);
+            R.r28 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r29 = bitcast<float>(v5.x);
+            R.r30 = bitcast<float>(v5.y);
+            R.r31 = bitcast<float>(v5.z);
+            R.r32 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r33 = bitcast<unsigned int>(v6.x);
+            R.r34 = bitcast<float>(v6.y);
+            R.r35 = bitcast<unsigned int>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<float>(v7.x);
+            R.r38 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<float>(v8.x);
+            R.r42 = bitcast<float>(v8.y);
+            R.r53 = bitcast<unsigned int>(v8.z);
+            return v8.w;
+        }
+        case 5:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r13 = bitcast<float>(v3.x);
+            R.r14 = bitcast<unsigned int>(v3.y);
+            R.r15 = bitcast<float>(v3.z);
+            R.r17 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r20 = bitcast<float>(v4.x);
+            R.r21 = bitcast<float>(v4.y);
+            R.r22 = bitcast<float>(v4.z);
+            R.r27 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r28 = bitcast<float>(v5.x);
+            R.r29 = bitcast<float>(v5.y);
+            R.r30 = bitcast<float>(v5.z);
+            R.r31 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r32 = bitcast<unsigned int>(v6.x);
+            R.r33 = bitcast<unsigned int>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r35 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r36 = bitcast<float>(v7.x);
+            R.r37 = bitcast<float>(v7.y);
+            R.r38 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<float>(v8.x);
+            R.r41 = bitcast<float>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            return v8.w;
+        }
+        case 6:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint2 v8 = reinterpret_cast<const uint2*>(stage + 4096u)[lane];
+            R.r42 = bitcast<float>(v8.x);
+            return v8.y;
+        }
+        case 7:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<float>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r42 = bitcast<float>(v8.x);
+            R.r43 = bitcast<float>(v8.y);
+            R.r44 = bitcast<float>(v8.z);
+            R.r45 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r50 = bitcast<float>(v9.x);
+            R.r51 = bitcast<float>(v9.y);
+            R.r52 = bitcast<float>(v9.z);
+            R.r53 = bitcast<unsigned int>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(stage + 5120u)[lane];
+            return v10;
+        }
+        case 8:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r40 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r41 = bitcast<float>(v7.x);
+            R.r42 = bitcast<float>(v7.y);
+            R.r43 = bitcast<float>(v7.z);
+            R.r44 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r45 = bitcast<float>(v8.x);
+            R.r46 = bitcast<float>(v8.y);
+            R.r47 = bitcast<float>(v8.z);
+            R.r48 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r53 = bitcast<unsigned int>(v9.x);
+            return v9.y;
+        }
+        case 9:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r40 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r41 = bitcast<float>(v7.x);
+            R.r42 = bitcast<float>(v7.y);
+            return v7.z;
+        }
+        case 10:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
+        case 11:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(stage + 2560u)[lane];
+            return v5;
+        }
+        case 12:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r28 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r30 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r31 = bitcast<float>(v5.x);
+            R.r32 = bitcast<unsigned int>(v5.y);
+            R.r33 = bitcast<unsigned int>(v5.z);
+            R.r34 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r35 = bitcast<unsigned int>(v6.x);
+            R.r36 = bitcast<float>(v6.y);
+            R.r37 = bitcast<float>(v6.z);
+            R.r38 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r39 = bitcast<float>(v7.x);
+            R.r40 = bitcast<float>(v7.y);
+            R.r41 = bitcast<float>(v7.z);
+            R.r42 = bitcast<float>(v7.w);
+            const uint2 v8 = reinterpret_cast<const uint2*>(stage + 4096u)[lane];
+            R.r53 = bitcast<unsigned int>(v8.x);
+            return v8.y;
+        }
+        case 13:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r53 = bitcast<unsigned int>(v7.z);
+            return v7.w;
+        }
+        case 14:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r37 = bitcast<float>(v5.x);
+            R.r38 = bitcast<float>(v5.y);
+            R.r39 = bitcast<float>(v5.z);
+            R.r40 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r41 = bitcast<float>(v6.x);
+            R.r42 = bitcast<float>(v6.y);
+            R.r53 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
+        case 15:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
+        case 16:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(stage + 2560u)[lane];
+            return v5;
+        }
+        case 17:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r34 = bitcast<float>(v5.y);
+            R.r35 = bitcast<unsigned int>(v5.z);
+            R.r36 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
+        case 18:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r35 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r53 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(stage + 3072u)[lane];
+            return v6;
+        }
+        case 19:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r35 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r49 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(stage + 3072u)[lane];
+            return v6;
+        }
+        case 20:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r34 = bitcast<float>(v5.y);
+            R.r35 = bitcast<unsigned int>(v5.z);
+            R.r36 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
+        case 21:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r34 = bitcast<float>(v5.z);
+            R.r35 = bitcast<unsigned int>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r36 = bitcast<float>(v6.x);
+            return v6.y;
+        }
+        case 22:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r36 = bitcast<float>(v5.z);
+            R.r53 = bitcast<unsigned int>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(stage + 3072u)[lane];
+            return v6;
+        }
+        case 23:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r29 = bitcast<float>(v4.z);
+            R.r31 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r32 = bitcast<unsigned int>(v5.x);
+            R.r33 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
+        case 24:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r49 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
+        case 25:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
+        case 26:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<unsigned int>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(stage + 2560u)[lane];
+            return v5;
+        }
+        case 27:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r29 = bitcast<float>(v4.y);
+            R.r31 = bitcast<float>(v4.z);
+            R.r32 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r33 = bitcast<unsigned int>(v5.x);
+            R.r49 = bitcast<unsigned int>(v5.y);
+            R.r53 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
+        case 28:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<float>(v6.x);
+            R.r35 = bitcast<unsigned int>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 29:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r17 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<float>(v3.z);
+            R.r21 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r27 = bitcast<float>(v4.y);
+            R.r28 = bitcast<float>(v4.z);
+            R.r29 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r30 = bitcast<float>(v5.x);
+            R.r31 = bitcast<float>(v5.y);
+            R.r32 = bitcast<unsigned int>(v5.z);
+            R.r33 = bitcast<unsigned int>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r53 = bitcast<unsigned int>(v6.x);
+            return v6.y;
+        }
+        case 30:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r17 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<float>(v3.y);
+            R.r21 = bitcast<float>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r27 = bitcast<float>(v4.x);
+            R.r31 = bitcast<float>(v4.y);
+            R.r32 = bitcast<unsigned int>(v4.z);
+            R.r33 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r49 = bitcast<unsigned int>(v5.x);
+            R.r53 = bitcast<unsigned int>(v5.y);
+            return v5.z;
+        }
+        case 31:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r17 = bitcast<unsigned int>(v2.z);
+            R.r32 = bitcast<unsigned int>(v2.w);
+            const uint2 v3 = reinterpret_cast<const uint2*>(stage + 1536u)[lane];
+            R.r53 = bitcast<unsigned int>(v3.x);
+            return v3.y;
+        }
+        case 32:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint2 v1 = reinterpret_cast<const uint2*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            return v1.y;
+        }
+        default: return 0xffffffffu;
+        }
+    }
 };
 
 const int kInTypes[] = {LOOM_B200_U32};
@@ -4423,16 +5941,28 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(a.dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
     if(a.ordinary && a.params.slice_rounds == 1u)
-        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
-    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
 {
     const void* fn = regroup_fn(regs, profile);
     if(!fn) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
+    if(dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);
 }
 
 } } // namespace loom_b200::k_primary_const_256
@@ -4443,4 +5973,4 @@ const loom_b200::KernelEntry loom_b200_entry_primary_const_256 = {
     &loom_b200::k_primary_const_256::launch_plain, &loom_b200::k_primary_const_256::launch_regroup,
     &loom_b200::k_primary_const_256::regroup_occupancy,
     loom_b200::k_primary_const_256::kQueues, loom_b200::k_primary_const_256::kSegments,
-    loom_b200::k_primary_const_256::kRegCaps, 8u};
+    loom_b200::k_primary_const_256::kRegCaps, 8u, loom_b200::k_primary_const_256::K::kMaxStageRow};

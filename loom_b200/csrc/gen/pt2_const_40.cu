@@ -10546,6 +10546,4134 @@ struct K
         }
     }
 
+    // bytes of one queue entry's slots, the largest over the queues
+    static constexpr unsigned kMaxStageRow = 256u;
+    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q
+    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared
+    // memory) with one bulk copy per slot column, completing on the
+    // mbarrier at `mbar`; false (nothing issued) when an address is not on
+    // a 16-byte boundary.
+    __device__ __forceinline__ static bool
+    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,
+               unsigned long long* mbar)
+    {
+        unsigned bytes = 0;
+        switch(q)
+        {
+        case 0: bytes = 3584u; break;
+        case 1: bytes = 5376u; break;
+        case 2: bytes = 5888u; break;
+        case 3: bytes = 3584u; break;
+        case 4: bytes = 5376u; break;
+        case 5: bytes = 5760u; break;
+        case 6: bytes = 7808u; break;
+        case 7: bytes = 7680u; break;
+        case 8: bytes = 7680u; break;
+        case 9: bytes = 7296u; break;
+        case 10: bytes = 8192u; break;
+        case 11: bytes = 7808u; break;
+        case 12: bytes = 6912u; break;
+        case 13: bytes = 5888u; break;
+        case 14: bytes = 5632u; break;
+        case 15: bytes = 7296u; break;
+        case 16: bytes = 7168u; break;
+        case 17: bytes = 6656u; break;
+        case 18: bytes = 5888u; break;
+        case 19: bytes = 5632u; break;
+        case 20: bytes = 6272u; break;
+        case 21: bytes = 6144u; break;
+        case 22: bytes = 6144u; break;
+        case 23: bytes = 6272u; break;
+        case 24: bytes = 6272u; break;
+        case 25: bytes = 6144u; break;
+        case 26: bytes = 6144u; break;
+        case 27: bytes = 6144u; break;
+        case 28: bytes = 5888u; break;
+        case 29: bytes = 5632u; break;
+        case 30: bytes = 6144u; break;
+        case 31: bytes = 6656u; break;
+        case 32: bytes = 6272u; break;
+        case 33: bytes = 5888u; break;
+        case 34: bytes = 5632u; break;
+        case 35: bytes = 5632u; break;
+        case 36: bytes = 4224u; break;
+        case 37: bytes = 4864u; break;
+        case 38: bytes = 4864u; break;
+        case 39: bytes = 4864u; break;
+        case 40: bytes = 4864u; break;
+        case 41: bytes = 5248u; break;
+        case 42: bytes = 5376u; break;
+        case 43: bytes = 5120u; break;
+        case 44: bytes = 5376u; break;
+        case 45: bytes = 5632u; break;
+        case 46: bytes = 5632u; break;
+        case 47: bytes = 4736u; break;
+        case 48: bytes = 5376u; break;
+        case 49: bytes = 5120u; break;
+        case 50: bytes = 5632u; break;
+        case 51: bytes = 5888u; break;
+        case 52: bytes = 5760u; break;
+        case 53: bytes = 5248u; break;
+        case 54: bytes = 1024u; break;
+        default: return false;
+        }
+        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;
+        bulk_expect(mbar, bytes);
+        switch(q)
+        {
+        case 0:
+            bulk_copy(stage + 0u, base + 0ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 16ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 32ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 48ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 64ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 80ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 96ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 1:
+            bulk_copy(stage + 0u, base + 112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 272ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 2:
+            bulk_copy(stage + 0u, base + 280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 456ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 3:
+            bulk_copy(stage + 0u, base + 464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 4:
+            bulk_copy(stage + 0u, base + 576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 736ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 5:
+            bulk_copy(stage + 0u, base + 744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 920ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 6:
+            bulk_copy(stage + 0u, base + 928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 1136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 1152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7680u, base + 1168ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 7:
+            bulk_copy(stage + 0u, base + 1176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 1384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 1400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 8:
+            bulk_copy(stage + 0u, base + 1416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 1624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 1640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 9:
+            bulk_copy(stage + 0u, base + 1656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 1864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 1880ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 10:
+            bulk_copy(stage + 0u, base + 1888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 2080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 2096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 2112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7680u, base + 2128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 11:
+            bulk_copy(stage + 0u, base + 2144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 2336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 2352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 2368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7680u, base + 2384ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 12:
+            bulk_copy(stage + 0u, base + 2392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 2584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 2600ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 13:
+            bulk_copy(stage + 0u, base + 2608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2784ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 14:
+            bulk_copy(stage + 0u, base + 2792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 15:
+            bulk_copy(stage + 0u, base + 2968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 3128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 3144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 3160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 3176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 7168u, base + 3192ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 16:
+            bulk_copy(stage + 0u, base + 3200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 3360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 3376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 3392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 3408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 17:
+            bulk_copy(stage + 0u, base + 3424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 3584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 3600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 3616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 18:
+            bulk_copy(stage + 0u, base + 3632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 3792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 3808ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 19:
+            bulk_copy(stage + 0u, base + 3816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 3976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 20:
+            bulk_copy(stage + 0u, base + 3992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 4152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 4168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 4184ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 21:
+            bulk_copy(stage + 0u, base + 4192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 4352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 4368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 22:
+            bulk_copy(stage + 0u, base + 4384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 4544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 4560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 23:
+            bulk_copy(stage + 0u, base + 4576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 4736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 4752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 4768ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 24:
+            bulk_copy(stage + 0u, base + 4776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 4936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 4952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 4968ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 25:
+            bulk_copy(stage + 0u, base + 4976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 5120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 5136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 5152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 26:
+            bulk_copy(stage + 0u, base + 5168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 5312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 5328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 5344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 27:
+            bulk_copy(stage + 0u, base + 5360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 5504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 5520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 5536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 28:
+            bulk_copy(stage + 0u, base + 5552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 5696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 5712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 5728ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 29:
+            bulk_copy(stage + 0u, base + 5736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 5880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 5896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 30:
+            bulk_copy(stage + 0u, base + 5912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 6040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 6056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 6072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 6088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 31:
+            bulk_copy(stage + 0u, base + 6104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 6232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 6248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 6264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 6280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 6296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 32:
+            bulk_copy(stage + 0u, base + 6312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 6440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 6456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 6472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 6488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 6504ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 33:
+            bulk_copy(stage + 0u, base + 6512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 6640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 6656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 6672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 6688ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 34:
+            bulk_copy(stage + 0u, base + 6696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 6824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 6840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 6856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 35:
+            bulk_copy(stage + 0u, base + 6872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 7032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 36:
+            bulk_copy(stage + 0u, base + 7048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7176ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 37:
+            bulk_copy(stage + 0u, base + 7184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7328ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 38:
+            bulk_copy(stage + 0u, base + 7336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7480ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 39:
+            bulk_copy(stage + 0u, base + 7488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7632ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 40:
+            bulk_copy(stage + 0u, base + 7640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7784ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 41:
+            bulk_copy(stage + 0u, base + 7792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 7840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 7856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 7872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 7888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 7904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 7920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 7936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 7952ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 42:
+            bulk_copy(stage + 0u, base + 7960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 7976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 7992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 8120ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 43:
+            bulk_copy(stage + 0u, base + 8128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 44:
+            bulk_copy(stage + 0u, base + 8288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 8448ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 45:
+            bulk_copy(stage + 0u, base + 8456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 8616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 46:
+            bulk_copy(stage + 0u, base + 8632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 8792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 47:
+            bulk_copy(stage + 0u, base + 8808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 8856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 8872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 8888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 8904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 8920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 8936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 8952ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 48:
+            bulk_copy(stage + 0u, base + 8960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 8976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 8992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 9120ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 49:
+            bulk_copy(stage + 0u, base + 9128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 9144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 9160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 50:
+            bulk_copy(stage + 0u, base + 9288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 9304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 9320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 9448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 51:
+            bulk_copy(stage + 0u, base + 9464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 9480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 9496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 9624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 9640ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 52:
+            bulk_copy(stage + 0u, base + 9648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 9664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 9680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 9808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 9824ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 53:
+            bulk_copy(stage + 0u, base + 9832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 9848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 9864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 9880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 9896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 9912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 9928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 9944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 9960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 9976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 9992ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 54:
+            bulk_copy(stage + 0u, base + 10000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 10016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        default: break;
+        }
+        return true;
+    }
+
+    // A lane's entry of a tile staged by bulk_issue; returns its thread id.
+    __device__ __forceinline__ static unsigned
+    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)
+    {
+        switch(q)
+        {
+        case 0:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r14 = bitcast<unsigned int>(v0.y);
+            R.r22 = bitcast<float>(v0.z);
+            R.r23 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r24 = bitcast<float>(v1.x);
+            R.r25 = bitcast<float>(v1.y);
+            R.r26 = bitcast<float>(v1.z);
+            R.r27 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r28 = bitcast<float>(v2.x);
+            R.r29 = bitcast<float>(v2.y);
+            R.r30 = bitcast<float>(v2.z);
+            R.r31 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r32 = bitcast<float>(v3.x);
+            R.r33 = bitcast<float>(v3.y);
+            R.r34 = bitcast<unsigned int>(v3.z);
+            R.r35 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r61 = bitcast<unsigned int>(v4.x);
+            R.r62 = bitcast<float>(v4.y);
+            R.r63 = bitcast<float>(v4.z);
+            R.r64 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r65 = bitcast<float>(v5.x);
+            R.r66 = bitcast<float>(v5.y);
+            R.r67 = bitcast<float>(v5.z);
+            R.r68 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r69 = bitcast<float>(v6.x);
+            R.r70 = bitcast<float>(v6.y);
+            R.r71 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 1:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(stage + 5120u)[lane];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
+        case 2:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r13 = bitcast<float>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r18 = bitcast<unsigned int>(v4.x);
+            R.r19 = bitcast<unsigned int>(v4.y);
+            R.r20 = bitcast<unsigned int>(v4.z);
+            R.r21 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r22 = bitcast<float>(v5.x);
+            R.r23 = bitcast<float>(v5.y);
+            R.r24 = bitcast<float>(v5.z);
+            R.r25 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r26 = bitcast<float>(v6.x);
+            R.r27 = bitcast<float>(v6.y);
+            R.r28 = bitcast<float>(v6.z);
+            R.r29 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r30 = bitcast<float>(v7.x);
+            R.r31 = bitcast<float>(v7.y);
+            R.r32 = bitcast<float>(v7.z);
+            R.r33 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r34 = bitcast<unsigned int>(v8.x);
+            R.r35 = bitcast<float>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 3:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r10 = bitcast<unsigned int>(v1.y);
+            R.r11 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r18 = bitcast<unsigned int>(v3.x);
+            R.r19 = bitcast<unsigned int>(v3.y);
+            R.r20 = bitcast<unsigned int>(v3.z);
+            R.r21 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r61 = bitcast<unsigned int>(v4.x);
+            R.r62 = bitcast<float>(v4.y);
+            R.r63 = bitcast<float>(v4.z);
+            R.r64 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r65 = bitcast<float>(v5.x);
+            R.r66 = bitcast<float>(v5.y);
+            R.r67 = bitcast<float>(v5.z);
+            R.r68 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r69 = bitcast<float>(v6.x);
+            R.r70 = bitcast<float>(v6.y);
+            R.r71 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 4:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(stage + 5120u)[lane];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
+        case 5:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r61 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            R.r65 = bitcast<float>(v9.y);
+            R.r66 = bitcast<float>(v9.z);
+            R.r67 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r68 = bitcast<unsigned int>(v10.x);
+            R.r69 = bitcast<float>(v10.y);
+            R.r70 = bitcast<float>(v10.z);
+            R.r71 = bitcast<float>(v10.w);
+            const unsigned v11 = reinterpret_cast<const unsigned*>(stage + 5632u)[lane];
+            return v11;
+        }
+        case 6:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r58 = bitcast<float>(v11.z);
+            R.r59 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r60 = bitcast<float>(v12.x);
+            R.r61 = bitcast<unsigned int>(v12.y);
+            R.r62 = bitcast<float>(v12.z);
+            R.r63 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r64 = bitcast<float>(v13.x);
+            R.r65 = bitcast<float>(v13.y);
+            R.r66 = bitcast<float>(v13.z);
+            R.r67 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(stage + 7168u)[lane];
+            R.r68 = bitcast<unsigned int>(v14.x);
+            R.r69 = bitcast<float>(v14.y);
+            R.r70 = bitcast<float>(v14.z);
+            R.r71 = bitcast<float>(v14.w);
+            const unsigned v15 = reinterpret_cast<const unsigned*>(stage + 7680u)[lane];
+            return v15;
+        }
+        case 7:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r10 = bitcast<unsigned int>(v2.x);
+            R.r11 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r18 = bitcast<unsigned int>(v4.x);
+            R.r19 = bitcast<unsigned int>(v4.y);
+            R.r22 = bitcast<float>(v4.z);
+            R.r23 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r24 = bitcast<float>(v5.x);
+            R.r25 = bitcast<float>(v5.y);
+            R.r26 = bitcast<float>(v5.z);
+            R.r27 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r28 = bitcast<float>(v6.x);
+            R.r29 = bitcast<float>(v6.y);
+            R.r30 = bitcast<float>(v6.z);
+            R.r31 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r32 = bitcast<float>(v7.x);
+            R.r33 = bitcast<float>(v7.y);
+            R.r34 = bitcast<unsigned int>(v7.z);
+            R.r35 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r36 = bitcast<float>(v8.x);
+            R.r37 = bitcast<float>(v8.y);
+            R.r38 = bitcast<float>(v8.z);
+            R.r39 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r40 = bitcast<unsigned int>(v9.x);
+            R.r41 = bitcast<unsigned int>(v9.y);
+            R.r42 = bitcast<float>(v9.z);
+            R.r43 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r44 = bitcast<unsigned int>(v10.x);
+            R.r45 = bitcast<float>(v10.y);
+            R.r46 = bitcast<float>(v10.z);
+            R.r47 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r48 = bitcast<unsigned int>(v11.x);
+            R.r49 = bitcast<unsigned int>(v11.y);
+            R.r50 = bitcast<float>(v11.z);
+            R.r61 = bitcast<unsigned int>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r62 = bitcast<float>(v12.x);
+            R.r63 = bitcast<float>(v12.y);
+            R.r64 = bitcast<float>(v12.z);
+            R.r65 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r66 = bitcast<float>(v13.x);
+            R.r67 = bitcast<float>(v13.y);
+            R.r68 = bitcast<unsigned int>(v13.z);
+            R.r69 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(stage + 7168u)[lane];
+            R.r70 = bitcast<float>(v14.x);
+            R.r71 = bitcast<float>(v14.y);
+            return v14.z;
+        }
+        case 8:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r13 = bitcast<float>(v3.x);
+            R.r14 = bitcast<unsigned int>(v3.y);
+            R.r15 = bitcast<float>(v3.z);
+            R.r16 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r17 = bitcast<float>(v4.x);
+            R.r18 = bitcast<unsigned int>(v4.y);
+            R.r19 = bitcast<unsigned int>(v4.z);
+            R.r22 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r23 = bitcast<float>(v5.x);
+            R.r24 = bitcast<float>(v5.y);
+            R.r25 = bitcast<float>(v5.z);
+            R.r26 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r27 = bitcast<float>(v6.x);
+            R.r28 = bitcast<float>(v6.y);
+            R.r29 = bitcast<float>(v6.z);
+            R.r30 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r31 = bitcast<float>(v7.x);
+            R.r32 = bitcast<float>(v7.y);
+            R.r33 = bitcast<float>(v7.z);
+            R.r34 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r35 = bitcast<float>(v8.x);
+            R.r36 = bitcast<float>(v8.y);
+            R.r37 = bitcast<float>(v8.z);
+            R.r38 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r39 = bitcast<float>(v9.x);
+            R.r40 = bitcast<unsigned int>(v9.y);
+            R.r41 = bitcast<unsigned int>(v9.z);
+            R.r42 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r43 = bitcast<unsigned int>(v10.x);
+            R.r44 = bitcast<unsigned int>(v10.y);
+            R.r45 = bitcast<float>(v10.z);
+            R.r46 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r47 = bitcast<float>(v11.x);
+            R.r48 = bitcast<unsigned int>(v11.y);
+            R.r49 = bitcast<unsigned int>(v11.z);
+            R.r50 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r62 = bitcast<float>(v12.x);
+            R.r63 = bitcast<float>(v12.y);
+            R.r64 = bitcast<float>(v12.z);
+            R.r65 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r66 = bitcast<float>(v13.x);
+            R.r67 = bitcast<float>(v13.y);
+            R.r68 = bitcast<unsigned int>(v13.z);
+            R.r69 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(stage + 7168u)[lane];
+            R.r70 = bitcast<float>(v14.x);
+            R.r71 = bitcast<float>(v14.y);
+            return v14.z;
+        }
+        case 9:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r64 = bitcast<float>(v12.x);
+            R.r65 = bitcast<float>(v12.y);
+            R.r66 = bitcast<float>(v12.z);
+            R.r67 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r68 = bitcast<unsigned int>(v13.x);
+            R.r69 = bitcast<float>(v13.y);
+            R.r70 = bitcast<float>(v13.z);
+            R.r71 = bitcast<float>(v13.w);
+            const unsigned v14 = reinterpret_cast<const unsigned*>(stage + 7168u)[lane];
+            return v14;
+        }
+        case 10:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r48 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r49 = bitcast<unsigned int>(v11.x);
+            R.r50 = bitcast<float>(v11.y);
+            R.r51 = bitcast<float>(v11.z);
+            R.r52 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r53 = bitcast<unsigned int>(v12.x);
+            R.r58 = bitcast<float>(v12.y);
+            R.r59 = bitcast<float>(v12.z);
+            R.r60 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r61 = bitcast<unsigned int>(v13.x);
+            R.r62 = bitcast<float>(v13.y);
+            R.r63 = bitcast<float>(v13.z);
+            R.r64 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(stage + 7168u)[lane];
+            R.r65 = bitcast<float>(v14.x);
+            R.r66 = bitcast<float>(v14.y);
+            R.r67 = bitcast<float>(v14.z);
+            R.r68 = bitcast<unsigned int>(v14.w);
+            const uint4 v15 = reinterpret_cast<const uint4*>(stage + 7680u)[lane];
+            R.r69 = bitcast<float>(v15.x);
+            R.r70 = bitcast<float>(v15.y);
+            R.r71 = bitcast<float>(v15.z);
+            return v15.w;
+        }
+        case 11:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r48 = bitcast<unsigned int>(v10.x);
+            R.r49 = bitcast<unsigned int>(v10.y);
+            R.r50 = bitcast<float>(v10.z);
+            R.r51 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r52 = bitcast<float>(v11.x);
+            R.r53 = bitcast<unsigned int>(v11.y);
+            R.r54 = bitcast<float>(v11.z);
+            R.r55 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r56 = bitcast<float>(v12.x);
+            R.r61 = bitcast<unsigned int>(v12.y);
+            R.r62 = bitcast<float>(v12.z);
+            R.r63 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r64 = bitcast<float>(v13.x);
+            R.r65 = bitcast<float>(v13.y);
+            R.r66 = bitcast<float>(v13.z);
+            R.r67 = bitcast<float>(v13.w);
+            const uint4 v14 = reinterpret_cast<const uint4*>(stage + 7168u)[lane];
+            R.r68 = bitcast<unsigned int>(v14.x);
+            R.r69 = bitcast<float>(v14.y);
+            R.r70 = bitcast<float>(v14.z);
+            R.r71 = bitcast<float>(v14.w);
+            const unsigned v15 = reinterpret_cast<const unsigned*>(stage + 7680u)[lane];
+            return v15;
+        }
+        case 12:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r48 = bitcast<unsigned int>(v10.x);
+            R.r49 = bitcast<unsigned int>(v10.y);
+            R.r50 = bitcast<float>(v10.z);
+            R.r62 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r63 = bitcast<float>(v11.x);
+            R.r64 = bitcast<float>(v11.y);
+            R.r65 = bitcast<float>(v11.z);
+            R.r66 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r67 = bitcast<float>(v12.x);
+            R.r68 = bitcast<unsigned int>(v12.y);
+            R.r69 = bitcast<float>(v12.z);
+            R.r70 = bitcast<float>(v12.w);
+            const uint2 v13 = reinterpret_cast<const uint2*>(stage + 6656u)[lane];
+            R.r71 = bitcast<float>(v13.x);
+            return v13.y;
+        }
+        case 13:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 14:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
+        case 15:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<float>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<unsigned int>(v9.y);
+            R.r44 = bitcast<unsigned int>(v9.z);
+            R.r45 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r46 = bitcast<float>(v10.x);
+            R.r47 = bitcast<float>(v10.y);
+            R.r48 = bitcast<unsigned int>(v10.z);
+            R.r49 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r50 = bitcast<float>(v11.x);
+            R.r61 = bitcast<unsigned int>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r64 = bitcast<float>(v12.x);
+            R.r65 = bitcast<float>(v12.y);
+            R.r66 = bitcast<float>(v12.z);
+            R.r67 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r68 = bitcast<unsigned int>(v13.x);
+            R.r69 = bitcast<float>(v13.y);
+            R.r70 = bitcast<float>(v13.z);
+            R.r71 = bitcast<float>(v13.w);
+            const unsigned v14 = reinterpret_cast<const unsigned*>(stage + 7168u)[lane];
+            return v14;
+        }
+        case 16:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r61 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r62 = bitcast<float>(v11.x);
+            R.r63 = bitcast<float>(v11.y);
+            R.r64 = bitcast<float>(v11.z);
+            R.r65 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r66 = bitcast<float>(v12.x);
+            R.r67 = bitcast<float>(v12.y);
+            R.r68 = bitcast<unsigned int>(v12.z);
+            R.r69 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r70 = bitcast<float>(v13.x);
+            R.r71 = bitcast<float>(v13.y);
+            return v13.z;
+        }
+        case 17:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r45 = bitcast<float>(v8.y);
+            R.r46 = bitcast<float>(v8.z);
+            R.r47 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r48 = bitcast<unsigned int>(v9.x);
+            R.r49 = bitcast<unsigned int>(v9.y);
+            R.r50 = bitcast<float>(v9.z);
+            R.r61 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r62 = bitcast<float>(v10.x);
+            R.r63 = bitcast<float>(v10.y);
+            R.r64 = bitcast<float>(v10.z);
+            R.r65 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r66 = bitcast<float>(v11.x);
+            R.r67 = bitcast<float>(v11.y);
+            R.r68 = bitcast<unsigned int>(v11.z);
+            R.r69 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r70 = bitcast<float>(v12.x);
+            R.r71 = bitcast<float>(v12.y);
+            return v12.z;
+        }
+        case 18:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 19:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
+        case 20:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            R.r43 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r44 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(stage + 6144u)[lane];
+            return v12;
+        }
+        case 21:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r43 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r61 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
+        case 22:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r43 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r57 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
+        case 23:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r42 = bitcast<float>(v8.z);
+            R.r43 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r44 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(stage + 6144u)[lane];
+            return v12;
+        }
+        case 24:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r42 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r43 = bitcast<unsigned int>(v9.x);
+            R.r44 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(stage + 6144u)[lane];
+            return v12;
+        }
+        case 25:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r44 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r61 = bitcast<unsigned int>(v9.x);
+            R.r62 = bitcast<float>(v9.y);
+            R.r63 = bitcast<float>(v9.z);
+            R.r64 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r65 = bitcast<float>(v10.x);
+            R.r66 = bitcast<float>(v10.y);
+            R.r67 = bitcast<float>(v10.z);
+            R.r68 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r69 = bitcast<float>(v11.x);
+            R.r70 = bitcast<float>(v11.y);
+            R.r71 = bitcast<float>(v11.z);
+            return v11.w;
+        }
+        case 26:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r37 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
+        case 27:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r57 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
+        case 28:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 29:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
+        case 30:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r37 = bitcast<float>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<unsigned int>(v8.y);
+            R.r57 = bitcast<unsigned int>(v8.z);
+            R.r61 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            R.r65 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r66 = bitcast<float>(v10.x);
+            R.r67 = bitcast<float>(v10.y);
+            R.r68 = bitcast<unsigned int>(v10.z);
+            R.r69 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r70 = bitcast<float>(v11.x);
+            R.r71 = bitcast<float>(v11.y);
+            return v11.z;
+        }
+        case 31:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<unsigned int>(v9.z);
+            R.r44 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r62 = bitcast<float>(v10.x);
+            R.r63 = bitcast<float>(v10.y);
+            R.r64 = bitcast<float>(v10.z);
+            R.r65 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r66 = bitcast<float>(v11.x);
+            R.r67 = bitcast<float>(v11.y);
+            R.r68 = bitcast<unsigned int>(v11.z);
+            R.r69 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r70 = bitcast<float>(v12.x);
+            R.r71 = bitcast<float>(v12.y);
+            return v12.z;
+        }
+        case 32:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r18 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<unsigned int>(v9.x);
+            R.r61 = bitcast<unsigned int>(v9.y);
+            R.r62 = bitcast<float>(v9.z);
+            R.r63 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r64 = bitcast<float>(v10.x);
+            R.r65 = bitcast<float>(v10.y);
+            R.r66 = bitcast<float>(v10.z);
+            R.r67 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r68 = bitcast<unsigned int>(v11.x);
+            R.r69 = bitcast<float>(v11.y);
+            R.r70 = bitcast<float>(v11.z);
+            R.r71 = bitcast<float>(v11.w);
+            const unsigned v12 = reinterpret_cast<const unsigned*>(stage + 6144u)[lane];
+            return v12;
+        }
+        case 33:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<unsigned int>(v8.x);
+            R.r57 = bitcast<unsigned int>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 34:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r61 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r65 = bitcast<float>(v9.x);
+            R.r66 = bitcast<float>(v9.y);
+            R.r67 = bitcast<float>(v9.z);
+            R.r68 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r69 = bitcast<float>(v10.x);
+            R.r70 = bitcast<float>(v10.y);
+            R.r71 = bitcast<float>(v10.z);
+            return v10.w;
+        }
+        case 35:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r39 = bitcast<float>(v7.y);
+            R.r40 = bitcast<unsigned int>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
+        case 36:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r34 = bitcast<unsigned int>(v6.x);
+            R.r35 = bitcast<float>(v6.y);
+            R.r39 = bitcast<float>(v6.z);
+            R.r40 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r61 = bitcast<unsigned int>(v7.x);
+            R.r69 = bitcast<float>(v7.y);
+            R.r70 = bitcast<float>(v7.z);
+            R.r71 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 37:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 38:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 39:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 40:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r69 = bitcast<float>(v8.z);
+            R.r70 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r71 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 41:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r69 = bitcast<float>(v9.y);
+            R.r70 = bitcast<float>(v9.z);
+            R.r71 = bitcast<float>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(stage + 5120u)[lane];
+            return v10;
+        }
+        case 42:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(stage + 5120u)[lane];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
+        case 43:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            return v9.w;
+        }
+        case 44:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r40 = bitcast<unsigned int>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(stage + 5120u)[lane];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
+        case 45:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r13 = bitcast<float>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
+        case 46:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
+        case 47:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r10 = bitcast<unsigned int>(v1.y);
+            R.r11 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r19 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<unsigned int>(v3.y);
+            R.r21 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r61 = bitcast<unsigned int>(v7.x);
+            R.r65 = bitcast<float>(v7.y);
+            R.r66 = bitcast<float>(v7.z);
+            R.r67 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r68 = bitcast<unsigned int>(v8.x);
+            R.r69 = bitcast<float>(v8.y);
+            R.r70 = bitcast<float>(v8.z);
+            R.r71 = bitcast<float>(v8.w);
+            const unsigned v9 = reinterpret_cast<const unsigned*>(stage + 4608u)[lane];
+            return v9;
+        }
+        case 48:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<float>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<unsigned int>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r61 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            R.r65 = bitcast<float>(v8.z);
+            R.r66 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r67 = bitcast<float>(v9.x);
+            R.r68 = bitcast<unsigned int>(v9.y);
+            R.r69 = bitcast<float>(v9.z);
+            R.r70 = bitcast<float>(v9.w);
+            const uint2 v10 = reinterpret_cast<const uint2*>(stage + 5120u)[lane];
+            R.r71 = bitcast<float>(v10.x);
+            return v10.y;
+        }
+        case 49:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r34 = bitcast<unsigned int>(v6.y);
+            R.r35 = bitcast<float>(v6.z);
+            R.r61 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r62 = bitcast<float>(v7.x);
+            R.r63 = bitcast<float>(v7.y);
+            R.r64 = bitcast<float>(v7.z);
+            R.r65 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r66 = bitcast<float>(v8.x);
+            R.r67 = bitcast<float>(v8.y);
+            R.r68 = bitcast<unsigned int>(v8.z);
+            R.r69 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r70 = bitcast<float>(v9.x);
+            R.r71 = bitcast<float>(v9.y);
+            return v9.z;
+        }
+        case 50:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r61 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            R.r65 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r66 = bitcast<float>(v9.x);
+            R.r67 = bitcast<float>(v9.y);
+            R.r68 = bitcast<unsigned int>(v9.z);
+            R.r69 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r70 = bitcast<float>(v10.x);
+            R.r71 = bitcast<float>(v10.y);
+            return v10.z;
+        }
+        case 51:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r20 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r21 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r38 = bitcast<float>(v8.y);
+            R.r61 = bitcast<unsigned int>(v8.z);
+            R.r62 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r63 = bitcast<float>(v9.x);
+            R.r64 = bitcast<float>(v9.y);
+            R.r65 = bitcast<float>(v9.z);
+            R.r66 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r67 = bitcast<float>(v10.x);
+            R.r68 = bitcast<unsigned int>(v10.y);
+            R.r69 = bitcast<float>(v10.z);
+            R.r70 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r71 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 52:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r10 = bitcast<unsigned int>(v2.x);
+            R.r11 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<float>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<unsigned int>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<float>(v8.x);
+            R.r61 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            R.r65 = bitcast<float>(v9.y);
+            R.r66 = bitcast<float>(v9.z);
+            R.r67 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r68 = bitcast<unsigned int>(v10.x);
+            R.r69 = bitcast<float>(v10.y);
+            R.r70 = bitcast<float>(v10.z);
+            R.r71 = bitcast<float>(v10.w);
+            const unsigned v11 = reinterpret_cast<const unsigned*>(stage + 5632u)[lane];
+            return v11;
+        }
+        case 53:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r10 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r11 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<float>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r61 = bitcast<unsigned int>(v7.y);
+            R.r62 = bitcast<float>(v7.z);
+            R.r63 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r64 = bitcast<float>(v8.x);
+            R.r65 = bitcast<float>(v8.y);
+            R.r66 = bitcast<float>(v8.z);
+            R.r67 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r68 = bitcast<unsigned int>(v9.x);
+            R.r69 = bitcast<float>(v9.y);
+            R.r70 = bitcast<float>(v9.z);
+            R.r71 = bitcast<float>(v9.w);
+            const unsigned v10 = reinterpret_cast<const unsigned*>(stage + 5120u)[lane];
+            return v10;
+        }
+        case 54:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r19 = bitcast<unsigned int>(v1.y);
+            return v1.z;
+        }
+        default: return 0xffffffffu;
+        }
+    }
 };
 
 const int kInTypes[] = {LOOM_B200_U32};
@@ -11044,16 +15172,28 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(a.dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
     if(a.ordinary && a.params.slice_rounds == 1u)
-        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
-    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
 {
     const void* fn = regroup_fn(regs, profile);
     if(!fn) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
+    if(dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);
 }
 
 } } // namespace loom_b200::k_pt2_const_40
@@ -11064,4 +15204,4 @@ const loom_b200::KernelEntry loom_b200_entry_pt2_const_40 = {
     &loom_b200::k_pt2_const_40::launch_plain, &loom_b200::k_pt2_const_40::launch_regroup,
     &loom_b200::k_pt2_const_40::regroup_occupancy,
     loom_b200::k_pt2_const_40::kQueues, loom_b200::k_pt2_const_40::kSegments,
-    loom_b200::k_pt2_const_40::kRegCaps, 8u};
+    loom_b200::k_pt2_const_40::kRegCaps, 8u, loom_b200::k_pt2_const_40::K::kMaxStageRow};

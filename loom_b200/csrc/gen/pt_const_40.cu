@@ -6786,6 +6786,2677 @@ struct K
         }
     }
 
+    // bytes of one queue entry's slots, the largest over the queues
+    static constexpr unsigned kMaxStageRow = 224u;
+    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q
+    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared
+    // memory) with one bulk copy per slot column, completing on the
+    // mbarrier at `mbar`; false (nothing issued) when an address is not on
+    // a 16-byte boundary.
+    __device__ __forceinline__ static bool
+    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,
+               unsigned long long* mbar)
+    {
+        unsigned bytes = 0;
+        switch(q)
+        {
+        case 0: bytes = 2176u; break;
+        case 1: bytes = 4096u; break;
+        case 2: bytes = 2560u; break;
+        case 3: bytes = 4096u; break;
+        case 4: bytes = 4352u; break;
+        case 5: bytes = 6400u; break;
+        case 6: bytes = 6144u; break;
+        case 7: bytes = 6144u; break;
+        case 8: bytes = 5888u; break;
+        case 9: bytes = 6784u; break;
+        case 10: bytes = 6400u; break;
+        case 11: bytes = 5632u; break;
+        case 12: bytes = 4608u; break;
+        case 13: bytes = 4224u; break;
+        case 14: bytes = 5888u; break;
+        case 15: bytes = 5632u; break;
+        case 16: bytes = 5120u; break;
+        case 17: bytes = 4608u; break;
+        case 18: bytes = 4224u; break;
+        case 19: bytes = 4864u; break;
+        case 20: bytes = 4736u; break;
+        case 21: bytes = 4736u; break;
+        case 22: bytes = 4864u; break;
+        case 23: bytes = 4864u; break;
+        case 24: bytes = 4736u; break;
+        case 25: bytes = 4608u; break;
+        case 26: bytes = 4608u; break;
+        case 27: bytes = 4608u; break;
+        case 28: bytes = 4224u; break;
+        case 29: bytes = 4608u; break;
+        case 30: bytes = 5120u; break;
+        case 31: bytes = 4864u; break;
+        case 32: bytes = 4608u; break;
+        case 33: bytes = 4224u; break;
+        case 34: bytes = 4224u; break;
+        case 35: bytes = 3584u; break;
+        case 36: bytes = 3712u; break;
+        case 37: bytes = 4096u; break;
+        case 38: bytes = 3584u; break;
+        case 39: bytes = 3584u; break;
+        case 40: bytes = 4096u; break;
+        case 41: bytes = 3840u; break;
+        case 42: bytes = 4096u; break;
+        case 43: bytes = 1024u; break;
+        default: return false;
+        }
+        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;
+        bulk_expect(mbar, bytes);
+        switch(q)
+        {
+        case 0:
+            bulk_copy(stage + 0u, base + 0ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 16ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 32ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 48ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 64ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 1:
+            bulk_copy(stage + 0u, base + 72ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 88ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 2:
+            bulk_copy(stage + 0u, base + 200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 3:
+            bulk_copy(stage + 0u, base + 280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 4:
+            bulk_copy(stage + 0u, base + 408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 536ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 5:
+            bulk_copy(stage + 0u, base + 544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 736ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 6:
+            bulk_copy(stage + 0u, base + 744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 7:
+            bulk_copy(stage + 0u, base + 936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 8:
+            bulk_copy(stage + 0u, base + 1128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1192ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1304ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 9:
+            bulk_copy(stage + 0u, base + 1312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 1520ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 10:
+            bulk_copy(stage + 0u, base + 1528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 1704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 1720ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 11:
+            bulk_copy(stage + 0u, base + 1728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 1856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 1872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 1888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 12:
+            bulk_copy(stage + 0u, base + 1904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 13:
+            bulk_copy(stage + 0u, base + 2048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2176ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 14:
+            bulk_copy(stage + 0u, base + 2184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2360ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 15:
+            bulk_copy(stage + 0u, base + 2368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 16:
+            bulk_copy(stage + 0u, base + 2544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 17:
+            bulk_copy(stage + 0u, base + 2704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 18:
+            bulk_copy(stage + 0u, base + 2848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2976ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 19:
+            bulk_copy(stage + 0u, base + 2984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3128ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 20:
+            bulk_copy(stage + 0u, base + 3136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3280ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 21:
+            bulk_copy(stage + 0u, base + 3288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3432ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 22:
+            bulk_copy(stage + 0u, base + 3440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3472ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3488ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3504ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3520ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3536ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3552ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3584ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 23:
+            bulk_copy(stage + 0u, base + 3592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3736ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 24:
+            bulk_copy(stage + 0u, base + 3744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 3856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 3872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 3888ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 25:
+            bulk_copy(stage + 0u, base + 3896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 3912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 3928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 3944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 3960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 3976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 3992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 26:
+            bulk_copy(stage + 0u, base + 4040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 27:
+            bulk_copy(stage + 0u, base + 4184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 28:
+            bulk_copy(stage + 0u, base + 4328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4424ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4456ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 29:
+            bulk_copy(stage + 0u, base + 4464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 30:
+            bulk_copy(stage + 0u, base + 4608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 31:
+            bulk_copy(stage + 0u, base + 4768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 4848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 4864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 4880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 4896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 4912ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 32:
+            bulk_copy(stage + 0u, base + 4920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 4936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 4952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 4968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 4984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 33:
+            bulk_copy(stage + 0u, base + 5064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5160ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5176ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5192ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 34:
+            bulk_copy(stage + 0u, base + 5200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 5328ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 35:
+            bulk_copy(stage + 0u, base + 5336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 36:
+            bulk_copy(stage + 0u, base + 5448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5560ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 37:
+            bulk_copy(stage + 0u, base + 5568ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5584ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5600ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5616ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5632ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5648ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 5680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 38:
+            bulk_copy(stage + 0u, base + 5696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 39:
+            bulk_copy(stage + 0u, base + 5808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 5888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 5904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 40:
+            bulk_copy(stage + 0u, base + 5920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 5936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 5952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 5968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 5984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 41:
+            bulk_copy(stage + 0u, base + 6048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6112ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6128ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6144ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6160ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 42:
+            bulk_copy(stage + 0u, base + 6168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 6200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 6216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 6232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 6248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 6264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 6280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 43:
+            bulk_copy(stage + 0u, base + 6296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 6312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        default: break;
+        }
+        return true;
+    }
+
+    // A lane's entry of a tile staged by bulk_issue; returns its thread id.
+    __device__ __forceinline__ static unsigned
+    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)
+    {
+        switch(q)
+        {
+        case 0:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r22 = bitcast<float>(v0.y);
+            R.r23 = bitcast<float>(v0.z);
+            R.r24 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r25 = bitcast<float>(v1.x);
+            R.r26 = bitcast<float>(v1.y);
+            R.r27 = bitcast<float>(v1.z);
+            R.r28 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r29 = bitcast<float>(v2.x);
+            R.r30 = bitcast<float>(v2.y);
+            R.r31 = bitcast<unsigned int>(v2.z);
+            R.r32 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r58 = bitcast<unsigned int>(v3.x);
+            R.r62 = bitcast<float>(v3.y);
+            R.r63 = bitcast<float>(v3.z);
+            R.r64 = bitcast<float>(v3.w);
+            const unsigned v4 = reinterpret_cast<const unsigned*>(stage + 2048u)[lane];
+            return v4;
+        }
+        case 1:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r18 = bitcast<unsigned int>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r58 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r62 = bitcast<float>(v7.x);
+            R.r63 = bitcast<float>(v7.y);
+            R.r64 = bitcast<float>(v7.z);
+            return v7.w;
+        }
+        case 2:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r19 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<unsigned int>(v3.y);
+            R.r21 = bitcast<unsigned int>(v3.z);
+            R.r58 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r62 = bitcast<float>(v4.x);
+            R.r63 = bitcast<float>(v4.y);
+            R.r64 = bitcast<float>(v4.z);
+            return v4.w;
+        }
+        case 3:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r58 = bitcast<unsigned int>(v6.z);
+            R.r62 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r63 = bitcast<float>(v7.x);
+            R.r64 = bitcast<float>(v7.y);
+            return v7.z;
+        }
+        case 4:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r58 = bitcast<unsigned int>(v7.y);
+            R.r62 = bitcast<float>(v7.z);
+            R.r63 = bitcast<float>(v7.w);
+            const uint2 v8 = reinterpret_cast<const uint2*>(stage + 4096u)[lane];
+            R.r64 = bitcast<float>(v8.x);
+            return v8.y;
+        }
+        case 5:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<float>(v9.y);
+            R.r44 = bitcast<float>(v9.z);
+            R.r45 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r46 = bitcast<float>(v10.x);
+            R.r47 = bitcast<float>(v10.y);
+            R.r55 = bitcast<float>(v10.z);
+            R.r56 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r57 = bitcast<float>(v11.x);
+            R.r58 = bitcast<unsigned int>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint2 v12 = reinterpret_cast<const uint2*>(stage + 6144u)[lane];
+            R.r64 = bitcast<float>(v12.x);
+            return v12.y;
+        }
+        case 6:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r12 = bitcast<float>(v2.z);
+            R.r13 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r14 = bitcast<unsigned int>(v3.x);
+            R.r15 = bitcast<float>(v3.y);
+            R.r16 = bitcast<float>(v3.z);
+            R.r17 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r19 = bitcast<unsigned int>(v4.x);
+            R.r22 = bitcast<float>(v4.y);
+            R.r23 = bitcast<float>(v4.z);
+            R.r24 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r25 = bitcast<float>(v5.x);
+            R.r26 = bitcast<float>(v5.y);
+            R.r27 = bitcast<float>(v5.z);
+            R.r28 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r29 = bitcast<float>(v6.x);
+            R.r30 = bitcast<float>(v6.y);
+            R.r31 = bitcast<unsigned int>(v6.z);
+            R.r32 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r33 = bitcast<float>(v7.x);
+            R.r34 = bitcast<float>(v7.y);
+            R.r35 = bitcast<float>(v7.z);
+            R.r36 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r37 = bitcast<unsigned int>(v8.x);
+            R.r38 = bitcast<unsigned int>(v8.y);
+            R.r39 = bitcast<float>(v8.z);
+            R.r40 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r41 = bitcast<float>(v9.x);
+            R.r42 = bitcast<float>(v9.y);
+            R.r43 = bitcast<float>(v9.z);
+            R.r44 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r45 = bitcast<float>(v10.x);
+            R.r46 = bitcast<float>(v10.y);
+            R.r47 = bitcast<float>(v10.z);
+            R.r58 = bitcast<unsigned int>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r62 = bitcast<float>(v11.x);
+            R.r63 = bitcast<float>(v11.y);
+            R.r64 = bitcast<float>(v11.z);
+            return v11.w;
+        }
+        case 7:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r10 = bitcast<unsigned int>(v2.y);
+            R.r11 = bitcast<unsigned int>(v2.z);
+            R.r12 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r13 = bitcast<float>(v3.x);
+            R.r14 = bitcast<unsigned int>(v3.y);
+            R.r15 = bitcast<float>(v3.z);
+            R.r16 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r17 = bitcast<float>(v4.x);
+            R.r19 = bitcast<unsigned int>(v4.y);
+            R.r22 = bitcast<float>(v4.z);
+            R.r23 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r24 = bitcast<float>(v5.x);
+            R.r25 = bitcast<float>(v5.y);
+            R.r26 = bitcast<float>(v5.z);
+            R.r27 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r28 = bitcast<float>(v6.x);
+            R.r29 = bitcast<float>(v6.y);
+            R.r30 = bitcast<float>(v6.z);
+            R.r31 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r32 = bitcast<float>(v7.x);
+            R.r33 = bitcast<float>(v7.y);
+            R.r34 = bitcast<float>(v7.z);
+            R.r35 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r36 = bitcast<float>(v8.x);
+            R.r37 = bitcast<unsigned int>(v8.y);
+            R.r38 = bitcast<unsigned int>(v8.z);
+            R.r39 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r40 = bitcast<unsigned int>(v9.x);
+            R.r41 = bitcast<float>(v9.y);
+            R.r42 = bitcast<float>(v9.z);
+            R.r43 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r44 = bitcast<float>(v10.x);
+            R.r45 = bitcast<float>(v10.y);
+            R.r46 = bitcast<float>(v10.z);
+            R.r47 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r62 = bitcast<float>(v11.x);
+            R.r63 = bitcast<float>(v11.y);
+            R.r64 = bitcast<float>(v11.z);
+            return v11.w;
+        }
+        case 8:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<float>(v9.y);
+            R.r44 = bitcast<float>(v9.z);
+            R.r45 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r46 = bitcast<float>(v10.x);
+            R.r47 = bitcast<float>(v10.y);
+            R.r62 = bitcast<float>(v10.z);
+            R.r63 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r64 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 9:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<float>(v9.y);
+            R.r44 = bitcast<float>(v9.z);
+            R.r45 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r46 = bitcast<float>(v10.x);
+            R.r47 = bitcast<float>(v10.y);
+            R.r48 = bitcast<float>(v10.z);
+            R.r49 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r50 = bitcast<float>(v11.x);
+            R.r55 = bitcast<float>(v11.y);
+            R.r56 = bitcast<float>(v11.z);
+            R.r57 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r58 = bitcast<unsigned int>(v12.x);
+            R.r62 = bitcast<float>(v12.y);
+            R.r63 = bitcast<float>(v12.z);
+            R.r64 = bitcast<float>(v12.w);
+            const unsigned v13 = reinterpret_cast<const unsigned*>(stage + 6656u)[lane];
+            return v13;
+        }
+        case 10:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r45 = bitcast<float>(v9.x);
+            R.r46 = bitcast<float>(v9.y);
+            R.r47 = bitcast<float>(v9.z);
+            R.r48 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r49 = bitcast<float>(v10.x);
+            R.r50 = bitcast<float>(v10.y);
+            R.r51 = bitcast<float>(v10.z);
+            R.r52 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r53 = bitcast<float>(v11.x);
+            R.r58 = bitcast<unsigned int>(v11.y);
+            R.r62 = bitcast<float>(v11.z);
+            R.r63 = bitcast<float>(v11.w);
+            const uint2 v12 = reinterpret_cast<const uint2*>(stage + 6144u)[lane];
+            R.r64 = bitcast<float>(v12.x);
+            return v12.y;
+        }
+        case 11:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r45 = bitcast<float>(v9.x);
+            R.r46 = bitcast<float>(v9.y);
+            R.r47 = bitcast<float>(v9.z);
+            R.r62 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r63 = bitcast<float>(v10.x);
+            R.r64 = bitcast<float>(v10.y);
+            return v10.z;
+        }
+        case 12:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r54 = bitcast<unsigned int>(v7.y);
+            R.r58 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            return v8.z;
+        }
+        case 13:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r62 = bitcast<float>(v7.y);
+            R.r63 = bitcast<float>(v7.z);
+            R.r64 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 14:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r33 = bitcast<float>(v6.z);
+            R.r34 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r35 = bitcast<float>(v7.x);
+            R.r36 = bitcast<float>(v7.y);
+            R.r37 = bitcast<unsigned int>(v7.z);
+            R.r38 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r39 = bitcast<float>(v8.x);
+            R.r40 = bitcast<unsigned int>(v8.y);
+            R.r41 = bitcast<float>(v8.z);
+            R.r42 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r43 = bitcast<float>(v9.x);
+            R.r44 = bitcast<float>(v9.y);
+            R.r45 = bitcast<float>(v9.z);
+            R.r46 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r47 = bitcast<float>(v10.x);
+            R.r58 = bitcast<unsigned int>(v10.y);
+            R.r62 = bitcast<float>(v10.z);
+            R.r63 = bitcast<float>(v10.w);
+            const uint2 v11 = reinterpret_cast<const uint2*>(stage + 5632u)[lane];
+            R.r64 = bitcast<float>(v11.x);
+            return v11.y;
+        }
+        case 15:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r42 = bitcast<float>(v9.x);
+            R.r43 = bitcast<float>(v9.y);
+            R.r44 = bitcast<float>(v9.z);
+            R.r58 = bitcast<unsigned int>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r62 = bitcast<float>(v10.x);
+            R.r63 = bitcast<float>(v10.y);
+            R.r64 = bitcast<float>(v10.z);
+            return v10.w;
+        }
+        case 16:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r42 = bitcast<float>(v7.y);
+            R.r43 = bitcast<float>(v7.z);
+            R.r44 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r45 = bitcast<float>(v8.x);
+            R.r46 = bitcast<float>(v8.y);
+            R.r47 = bitcast<float>(v8.z);
+            R.r58 = bitcast<unsigned int>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            return v9.w;
+        }
+        case 17:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r54 = bitcast<unsigned int>(v7.y);
+            R.r58 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            return v8.z;
+        }
+        case 18:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r58 = bitcast<unsigned int>(v7.x);
+            R.r62 = bitcast<float>(v7.y);
+            R.r63 = bitcast<float>(v7.z);
+            R.r64 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 19:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<float>(v8.x);
+            R.r58 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 20:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r40 = bitcast<unsigned int>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r58 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const unsigned v9 = reinterpret_cast<const unsigned*>(stage + 4608u)[lane];
+            return v9;
+        }
+        case 21:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r40 = bitcast<unsigned int>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r54 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const unsigned v9 = reinterpret_cast<const unsigned*>(stage + 4608u)[lane];
+            return v9;
+        }
+        case 22:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r39 = bitcast<float>(v7.z);
+            R.r40 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r41 = bitcast<float>(v8.x);
+            R.r58 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 23:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r34 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r36 = bitcast<float>(v7.x);
+            R.r37 = bitcast<unsigned int>(v7.y);
+            R.r38 = bitcast<unsigned int>(v7.z);
+            R.r39 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r40 = bitcast<unsigned int>(v8.x);
+            R.r41 = bitcast<float>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 24:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r34 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r36 = bitcast<float>(v7.x);
+            R.r37 = bitcast<unsigned int>(v7.y);
+            R.r38 = bitcast<unsigned int>(v7.z);
+            R.r41 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r58 = bitcast<unsigned int>(v8.x);
+            R.r62 = bitcast<float>(v8.y);
+            R.r63 = bitcast<float>(v8.z);
+            R.r64 = bitcast<float>(v8.w);
+            const unsigned v9 = reinterpret_cast<const unsigned*>(stage + 4608u)[lane];
+            return v9;
+        }
+        case 25:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r34 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r36 = bitcast<float>(v7.x);
+            R.r37 = bitcast<unsigned int>(v7.y);
+            R.r38 = bitcast<unsigned int>(v7.z);
+            R.r58 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            return v8.w;
+        }
+        case 26:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r54 = bitcast<unsigned int>(v7.z);
+            R.r58 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            return v8.w;
+        }
+        case 27:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r54 = bitcast<unsigned int>(v7.y);
+            R.r58 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            return v8.z;
+        }
+        case 28:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r58 = bitcast<unsigned int>(v7.x);
+            R.r62 = bitcast<float>(v7.y);
+            R.r63 = bitcast<float>(v7.z);
+            R.r64 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 29:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r34 = bitcast<float>(v6.z);
+            R.r36 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r37 = bitcast<unsigned int>(v7.x);
+            R.r38 = bitcast<unsigned int>(v7.y);
+            R.r54 = bitcast<unsigned int>(v7.z);
+            R.r58 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r62 = bitcast<float>(v8.x);
+            R.r63 = bitcast<float>(v8.y);
+            R.r64 = bitcast<float>(v8.z);
+            return v8.w;
+        }
+        case 30:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r39 = bitcast<float>(v8.y);
+            R.r40 = bitcast<unsigned int>(v8.z);
+            R.r41 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r62 = bitcast<float>(v9.x);
+            R.r63 = bitcast<float>(v9.y);
+            R.r64 = bitcast<float>(v9.z);
+            return v9.w;
+        }
+        case 31:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r14 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r15 = bitcast<float>(v3.x);
+            R.r16 = bitcast<float>(v3.y);
+            R.r17 = bitcast<float>(v3.z);
+            R.r19 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r22 = bitcast<float>(v4.x);
+            R.r23 = bitcast<float>(v4.y);
+            R.r24 = bitcast<float>(v4.z);
+            R.r25 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r26 = bitcast<float>(v5.x);
+            R.r27 = bitcast<float>(v5.y);
+            R.r28 = bitcast<float>(v5.z);
+            R.r29 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r30 = bitcast<float>(v6.x);
+            R.r31 = bitcast<unsigned int>(v6.y);
+            R.r32 = bitcast<float>(v6.z);
+            R.r33 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r34 = bitcast<float>(v7.x);
+            R.r35 = bitcast<float>(v7.y);
+            R.r36 = bitcast<float>(v7.z);
+            R.r37 = bitcast<unsigned int>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r38 = bitcast<unsigned int>(v8.x);
+            R.r58 = bitcast<unsigned int>(v8.y);
+            R.r62 = bitcast<float>(v8.z);
+            R.r63 = bitcast<float>(v8.w);
+            const uint2 v9 = reinterpret_cast<const uint2*>(stage + 4608u)[lane];
+            R.r64 = bitcast<float>(v9.x);
+            return v9.y;
+        }
+        case 32:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r38 = bitcast<unsigned int>(v7.x);
+            R.r54 = bitcast<unsigned int>(v7.y);
+            R.r58 = bitcast<unsigned int>(v7.z);
+            R.r62 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r63 = bitcast<float>(v8.x);
+            R.r64 = bitcast<float>(v8.y);
+            return v8.z;
+        }
+        case 33:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r58 = bitcast<unsigned int>(v7.x);
+            R.r62 = bitcast<float>(v7.y);
+            R.r63 = bitcast<float>(v7.z);
+            R.r64 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 34:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r36 = bitcast<float>(v6.z);
+            R.r37 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r58 = bitcast<unsigned int>(v7.x);
+            R.r62 = bitcast<float>(v7.y);
+            R.r63 = bitcast<float>(v7.z);
+            R.r64 = bitcast<float>(v7.w);
+            const unsigned v8 = reinterpret_cast<const unsigned*>(stage + 4096u)[lane];
+            return v8;
+        }
+        case 35:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r31 = bitcast<unsigned int>(v5.y);
+            R.r32 = bitcast<float>(v5.z);
+            R.r36 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r37 = bitcast<unsigned int>(v6.x);
+            R.r58 = bitcast<unsigned int>(v6.y);
+            return v6.z;
+        }
+        case 36:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r37 = bitcast<unsigned int>(v6.z);
+            R.r58 = bitcast<unsigned int>(v6.w);
+            const unsigned v7 = reinterpret_cast<const unsigned*>(stage + 3584u)[lane];
+            return v7;
+        }
+        case 37:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r37 = bitcast<unsigned int>(v6.z);
+            R.r58 = bitcast<unsigned int>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r59 = bitcast<float>(v7.x);
+            R.r60 = bitcast<float>(v7.y);
+            R.r61 = bitcast<float>(v7.z);
+            return v7.w;
+        }
+        case 38:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r58 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
+        case 39:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r58 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
+        case 40:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r58 = bitcast<unsigned int>(v6.z);
+            R.r62 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r63 = bitcast<float>(v7.x);
+            R.r64 = bitcast<float>(v7.y);
+            return v7.z;
+        }
+        case 41:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r8 = bitcast<unsigned int>(v1.y);
+            R.r9 = bitcast<unsigned int>(v1.z);
+            R.r12 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r13 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r19 = bitcast<unsigned int>(v3.x);
+            R.r20 = bitcast<unsigned int>(v3.y);
+            R.r21 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r58 = bitcast<unsigned int>(v6.y);
+            R.r62 = bitcast<float>(v6.z);
+            R.r63 = bitcast<float>(v6.w);
+            const uint2 v7 = reinterpret_cast<const uint2*>(stage + 3584u)[lane];
+            R.r64 = bitcast<float>(v7.x);
+            return v7.y;
+        }
+        case 42:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r6 = bitcast<unsigned int>(v1.y);
+            R.r7 = bitcast<unsigned int>(v1.z);
+            R.r8 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r9 = bitcast<unsigned int>(v2.x);
+            R.r12 = bitcast<float>(v2.y);
+            R.r13 = bitcast<float>(v2.z);
+            R.r15 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r16 = bitcast<float>(v3.x);
+            R.r17 = bitcast<float>(v3.y);
+            R.r19 = bitcast<unsigned int>(v3.z);
+            R.r22 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r23 = bitcast<float>(v4.x);
+            R.r24 = bitcast<float>(v4.y);
+            R.r25 = bitcast<float>(v4.z);
+            R.r26 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r27 = bitcast<float>(v5.x);
+            R.r28 = bitcast<float>(v5.y);
+            R.r29 = bitcast<float>(v5.z);
+            R.r30 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r31 = bitcast<unsigned int>(v6.x);
+            R.r32 = bitcast<float>(v6.y);
+            R.r58 = bitcast<unsigned int>(v6.z);
+            R.r62 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r63 = bitcast<float>(v7.x);
+            R.r64 = bitcast<float>(v7.y);
+            return v7.z;
+        }
+        case 43:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<float>(v0.y);
+            R.r3 = bitcast<float>(v0.z);
+            R.r4 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r5 = bitcast<unsigned int>(v1.x);
+            R.r19 = bitcast<unsigned int>(v1.y);
+            return v1.z;
+        }
+        default: return 0xffffffffu;
+        }
+    }
 };
 
 const int kInTypes[] = {LOOM_B200_U32};
@@ -7196,16 +9867,28 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(a.dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
     if(a.ordinary && a.params.slice_rounds == 1u)
-        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
-    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
 {
     const void* fn = regroup_fn(regs, profile);
     if(!fn) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
+    if(dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);
 }
 
 } } // namespace loom_b200::k_pt_const_40
@@ -7216,4 +9899,4 @@ const loom_b200::KernelEntry loom_b200_entry_pt_const_40 = {
     &loom_b200::k_pt_const_40::launch_plain, &loom_b200::k_pt_const_40::launch_regroup,
     &loom_b200::k_pt_const_40::regroup_occupancy,
     loom_b200::k_pt_const_40::kQueues, loom_b200::k_pt_const_40::kSegments,
-    loom_b200::k_pt_const_40::kRegCaps, 8u};
+    loom_b200::k_pt_const_40::kRegCaps, 8u, loom_b200::k_pt_const_40::K::kMaxStageRow};

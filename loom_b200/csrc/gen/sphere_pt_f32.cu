@@ -3559,6 +3559,1274 @@ struct K
         }
     }
 
+    // bytes of one queue entry's slots, the largest over the queues
+    static constexpr unsigned kMaxStageRow = 224u;
+    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q
+    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared
+    // memory) with one bulk copy per slot column, completing on the
+    // mbarrier at `mbar`; false (nothing issued) when an address is not on
+    // a 16-byte boundary.
+    __device__ __forceinline__ static bool
+    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,
+               unsigned long long* mbar)
+    {
+        unsigned bytes = 0;
+        switch(q)
+        {
+        case 0: bytes = 512u; break;
+        case 1: bytes = 2304u; break;
+        case 2: bytes = 2560u; break;
+        case 3: bytes = 3072u; break;
+        case 4: bytes = 2816u; break;
+        case 5: bytes = 2816u; break;
+        case 6: bytes = 1280u; break;
+        case 7: bytes = 3584u; break;
+        case 8: bytes = 3584u; break;
+        case 9: bytes = 3584u; break;
+        case 10: bytes = 3584u; break;
+        case 11: bytes = 3584u; break;
+        case 12: bytes = 3584u; break;
+        case 13: bytes = 3072u; break;
+        case 14: bytes = 2560u; break;
+        case 15: bytes = 3328u; break;
+        case 16: bytes = 3584u; break;
+        case 17: bytes = 3712u; break;
+        case 18: bytes = 3584u; break;
+        case 19: bytes = 3584u; break;
+        case 20: bytes = 4096u; break;
+        case 21: bytes = 3200u; break;
+        case 22: bytes = 2688u; break;
+        case 23: bytes = 7168u; break;
+        case 24: bytes = 2048u; break;
+        case 25: bytes = 3584u; break;
+        case 26: bytes = 3328u; break;
+        case 27: bytes = 3840u; break;
+        default: return false;
+        }
+        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;
+        bulk_expect(mbar, bytes);
+        switch(q)
+        {
+        case 0:
+            bulk_copy(stage + 0u, base + 0ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 1:
+            bulk_copy(stage + 0u, base + 16ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 32ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 48ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 64ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 80ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 2:
+            bulk_copy(stage + 0u, base + 88ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 3:
+            bulk_copy(stage + 0u, base + 168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 4:
+            bulk_copy(stage + 0u, base + 264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 344ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 5:
+            bulk_copy(stage + 0u, base + 352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 432ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 6:
+            bulk_copy(stage + 0u, base + 440ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 456ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 472ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 7:
+            bulk_copy(stage + 0u, base + 480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 8:
+            bulk_copy(stage + 0u, base + 592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 9:
+            bulk_copy(stage + 0u, base + 704ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 720ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 736ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 752ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 768ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 784ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 800ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 10:
+            bulk_copy(stage + 0u, base + 816ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 832ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 848ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 864ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 880ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 896ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 912ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 11:
+            bulk_copy(stage + 0u, base + 928ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 944ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 960ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 976ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 992ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1008ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1024ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 12:
+            bulk_copy(stage + 0u, base + 1040ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1056ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1072ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1088ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1104ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 13:
+            bulk_copy(stage + 0u, base + 1152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1200ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1216ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1232ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 14:
+            bulk_copy(stage + 0u, base + 1248ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1264ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1280ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1296ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1312ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 15:
+            bulk_copy(stage + 0u, base + 1328ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1344ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1360ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1376ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1392ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1408ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1424ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 16:
+            bulk_copy(stage + 0u, base + 1432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 17:
+            bulk_copy(stage + 0u, base + 1544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 1656ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 18:
+            bulk_copy(stage + 0u, base + 1664ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1680ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1696ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 19:
+            bulk_copy(stage + 0u, base + 1776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1824ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1840ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1856ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1872ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 20:
+            bulk_copy(stage + 0u, base + 1888ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 1904ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 1920ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 1936ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 1952ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 1968ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 1984ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2000ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 21:
+            bulk_copy(stage + 0u, base + 2016ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2032ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2048ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2064ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2080ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2096ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2112ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 22:
+            bulk_copy(stage + 0u, base + 2120ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2136ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2152ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2168ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2184ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2200ull * cap + static_cast<unsigned long long>(toff) * 4u, 128u, mbar);
+            break;
+        case 23:
+            bulk_copy(stage + 0u, base + 2208ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2224ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2240ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2256ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2272ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2288ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2304ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2320ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4096u, base + 2336ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 4608u, base + 2352ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5120u, base + 2368ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 5632u, base + 2384ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6144u, base + 2400ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 6656u, base + 2416ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 24:
+            bulk_copy(stage + 0u, base + 2432ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2448ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2464ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2480ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 25:
+            bulk_copy(stage + 0u, base + 2496ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2512ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2528ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2544ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2560ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2576ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2592ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            break;
+        case 26:
+            bulk_copy(stage + 0u, base + 2608ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2624ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2640ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2656ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2672ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2688ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2704ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        case 27:
+            bulk_copy(stage + 0u, base + 2712ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 512u, base + 2728ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1024u, base + 2744ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 1536u, base + 2760ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2048u, base + 2776ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 2560u, base + 2792ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3072u, base + 2808ull * cap + static_cast<unsigned long long>(toff) * 16u, 512u, mbar);
+            bulk_copy(stage + 3584u, base + 2824ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        default: break;
+        }
+        return true;
+    }
+
+    // A lane's entry of a tile staged by bulk_issue; returns its thread id.
+    __device__ __forceinline__ static unsigned
+    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)
+    {
+        switch(q)
+        {
+        case 0:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r1 = bitcast<unsigned int>(v0.x);
+            R.r2 = bitcast<unsigned int>(v0.y);
+            return v0.z;
+        }
+        case 1:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r7 = bitcast<unsigned int>(v0.x);
+            R.r9 = bitcast<unsigned int>(v0.y);
+            R.r11 = bitcast<unsigned int>(v0.z);
+            R.r12 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r13 = bitcast<unsigned int>(v1.x);
+            R.r14 = bitcast<float>(v1.y);
+            R.r15 = bitcast<float>(v1.z);
+            R.r16 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r17 = bitcast<float>(v2.x);
+            R.r20 = bitcast<unsigned int>(v2.y);
+            R.r21 = bitcast<unsigned int>(v2.z);
+            R.r22 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r23 = bitcast<unsigned int>(v3.x);
+            R.r24 = bitcast<unsigned int>(v3.y);
+            R.r25 = bitcast<unsigned int>(v3.z);
+            R.r130 = bitcast<unsigned int>(v3.w);
+            const uint2 v4 = reinterpret_cast<const uint2*>(stage + 2048u)[lane];
+            R.r131 = bitcast<unsigned int>(v4.x);
+            return v4.y;
+        }
+        case 2:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            return v4.w;
+        }
+        case 3:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            R.r55 = bitcast<unsigned int>(v5.y);
+            R.r56 = bitcast<unsigned int>(v5.z);
+            return v5.w;
+        }
+        case 4:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(stage + 2560u)[lane];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
+        case 5:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r53 = bitcast<float>(v4.w);
+            const uint2 v5 = reinterpret_cast<const uint2*>(stage + 2560u)[lane];
+            R.r54 = bitcast<unsigned int>(v5.x);
+            return v5.y;
+        }
+        case 6:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r49 = bitcast<float>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r50 = bitcast<float>(v1.x);
+            R.r51 = bitcast<float>(v1.y);
+            R.r76 = bitcast<float>(v1.z);
+            R.r77 = bitcast<float>(v1.w);
+            const uint2 v2 = reinterpret_cast<const uint2*>(stage + 1024u)[lane];
+            R.r78 = bitcast<float>(v2.x);
+            return v2.y;
+        }
+        case 7:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
+        case 8:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
+        case 9:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
+        case 10:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            R.r130 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
+        case 11:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            R.r86 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 12:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
+        case 13:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            return v5.w;
+        }
+        case 14:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            return v4.w;
+        }
+        case 15:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r105 = bitcast<float>(v6.x);
+            return v6.y;
+        }
+        case 16:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r105 = bitcast<float>(v6.x);
+            R.r130 = bitcast<unsigned int>(v6.y);
+            R.r131 = bitcast<unsigned int>(v6.z);
+            return v6.w;
+        }
+        case 17:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r105 = bitcast<float>(v6.x);
+            R.r106 = bitcast<float>(v6.y);
+            R.r107 = bitcast<float>(v6.z);
+            R.r108 = bitcast<float>(v6.w);
+            const unsigned v7 = reinterpret_cast<const unsigned*>(stage + 3584u)[lane];
+            return v7;
+        }
+        case 18:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r88 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r92 = bitcast<float>(v6.x);
+            R.r93 = bitcast<float>(v6.y);
+            R.r94 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 19:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r88 = bitcast<unsigned int>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r111 = bitcast<float>(v6.x);
+            R.r112 = bitcast<float>(v6.y);
+            R.r113 = bitcast<float>(v6.z);
+            return v6.w;
+        }
+        case 20:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r117 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r118 = bitcast<float>(v6.x);
+            R.r119 = bitcast<float>(v6.y);
+            R.r127 = bitcast<float>(v6.z);
+            R.r128 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r129 = bitcast<float>(v7.x);
+            R.r130 = bitcast<unsigned int>(v7.y);
+            return v7.z;
+        }
+        case 21:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r128 = bitcast<float>(v5.w);
+            const unsigned v6 = reinterpret_cast<const unsigned*>(stage + 3072u)[lane];
+            return v6;
+        }
+        case 22:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r117 = bitcast<float>(v4.x);
+            R.r118 = bitcast<float>(v4.y);
+            R.r119 = bitcast<float>(v4.z);
+            R.r129 = bitcast<float>(v4.w);
+            const unsigned v5 = reinterpret_cast<const unsigned*>(stage + 2560u)[lane];
+            return v5;
+        }
+        case 23:
+        {
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r7 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r9 = bitcast<unsigned int>(v1.x);
+            R.r11 = bitcast<unsigned int>(v1.y);
+            R.r12 = bitcast<unsigned int>(v1.z);
+            R.r13 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r14 = bitcast<float>(v2.x);
+            R.r15 = bitcast<float>(v2.y);
+            R.r16 = bitcast<float>(v2.z);
+            R.r17 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r20 = bitcast<unsigned int>(v3.x);
+            R.r21 = bitcast<unsigned int>(v3.y);
+            R.r22 = bitcast<unsigned int>(v3.z);
+            R.r23 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r24 = bitcast<unsigned int>(v4.x);
+            R.r25 = bitcast<unsigned int>(v4.y);
+            R.r26 = bitcast<unsigned int>(v4.z);
+            R.r42 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r43 = bitcast<float>(v5.x);
+            R.r44 = bitcast<float>(v5.y);
+            R.r46 = bitcast<float>(v5.z);
+            R.r47 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r48 = bitcast<float>(v6.x);
+            R.r49 = bitcast<float>(v6.y);
+            R.r50 = bitcast<float>(v6.z);
+            R.r51 = bitcast<float>(v6.w);
+            const uint4 v7 = reinterpret_cast<const uint4*>(stage + 3584u)[lane];
+            R.r52 = bitcast<unsigned int>(v7.x);
+            R.r76 = bitcast<float>(v7.y);
+            R.r77 = bitcast<float>(v7.z);
+            R.r78 = bitcast<float>(v7.w);
+            const uint4 v8 = reinterpret_cast<const uint4*>(stage + 4096u)[lane];
+            R.r79 = bitcast<unsigned int>(v8.x);
+            R.r80 = bitcast<float>(v8.y);
+            R.r81 = bitcast<float>(v8.z);
+            R.r82 = bitcast<float>(v8.w);
+            const uint4 v9 = reinterpret_cast<const uint4*>(stage + 4608u)[lane];
+            R.r83 = bitcast<float>(v9.x);
+            R.r84 = bitcast<float>(v9.y);
+            R.r85 = bitcast<float>(v9.z);
+            R.r87 = bitcast<float>(v9.w);
+            const uint4 v10 = reinterpret_cast<const uint4*>(stage + 5120u)[lane];
+            R.r92 = bitcast<float>(v10.x);
+            R.r93 = bitcast<float>(v10.y);
+            R.r94 = bitcast<float>(v10.z);
+            R.r100 = bitcast<float>(v10.w);
+            const uint4 v11 = reinterpret_cast<const uint4*>(stage + 5632u)[lane];
+            R.r101 = bitcast<float>(v11.x);
+            R.r102 = bitcast<float>(v11.y);
+            R.r103 = bitcast<float>(v11.z);
+            R.r104 = bitcast<float>(v11.w);
+            const uint4 v12 = reinterpret_cast<const uint4*>(stage + 6144u)[lane];
+            R.r105 = bitcast<float>(v12.x);
+            R.r117 = bitcast<float>(v12.y);
+            R.r118 = bitcast<float>(v12.z);
+            R.r119 = bitcast<float>(v12.w);
+            const uint4 v13 = reinterpret_cast<const uint4*>(stage + 6656u)[lane];
+            R.r127 = bitcast<float>(v13.x);
+            R.r128 = bitcast<float>(v13.y);
+            R.r129 = bitcast<float>(v13.z);
+            return v13.w;
+        }
+        case 24:
+        {
+            R.r26 = static_cast<unsigned int>(0);
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r7 = bitcast<unsigned int>(v0.x);
+            R.r9 = bitcast<unsigned int>(v0.y);
+            R.r11 = bitcast<unsigned int>(v0.z);
+            R.r12 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r13 = bitcast<unsigned int>(v1.x);
+            R.r14 = bitcast<float>(v1.y);
+            R.r15 = bitcast<float>(v1.z);
+            R.r16 = bitcast<float>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r17 = bitcast<float>(v2.x);
+            R.r20 = bitcast<unsigned int>(v2.y);
+            R.r21 = bitcast<unsigned int>(v2.z);
+            R.r22 = bitcast<unsigned int>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r23 = bitcast<unsigned int>(v3.x);
+            R.r24 = bitcast<unsigned int>(v3.y);
+            R.r25 = bitcast<unsigned int>(v3.z);
+            return v3.w;
+        }
+        case 25:
+        {
+            R.r26 = static_cast<unsigned int>(1);
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r76 = bitcast<float>(v4.x);
+            R.r77 = bitcast<float>(v4.y);
+            R.r78 = bitcast<float>(v4.z);
+            R.r79 = bitcast<unsigned int>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r80 = bitcast<float>(v5.x);
+            R.r81 = bitcast<float>(v5.y);
+            R.r82 = bitcast<float>(v5.z);
+            R.r83 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r84 = bitcast<float>(v6.x);
+            R.r85 = bitcast<float>(v6.y);
+            return v6.z;
+        }
+        case 26:
+        {
+            R.r26 = static_cast<unsigned int>(2);
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r46 = bitcast<float>(v2.y);
+            R.r47 = bitcast<float>(v2.z);
+            R.r48 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r49 = bitcast<float>(v3.x);
+            R.r50 = bitcast<float>(v3.y);
+            R.r51 = bitcast<float>(v3.z);
+            R.r52 = bitcast<unsigned int>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r92 = bitcast<float>(v4.x);
+            R.r93 = bitcast<float>(v4.y);
+            R.r94 = bitcast<float>(v4.z);
+            R.r100 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r101 = bitcast<float>(v5.x);
+            R.r102 = bitcast<float>(v5.y);
+            R.r103 = bitcast<float>(v5.z);
+            R.r104 = bitcast<float>(v5.w);
+            const uint2 v6 = reinterpret_cast<const uint2*>(stage + 3072u)[lane];
+            R.r105 = bitcast<float>(v6.x);
+            return v6.y;
+        }
+        case 27:
+        {
+            R.r26 = static_cast<unsigned int>(3);
+            const uint4 v0 = reinterpret_cast<const uint4*>(stage + 0u)[lane];
+            R.r3 = bitcast<float>(v0.x);
+            R.r4 = bitcast<float>(v0.y);
+            R.r5 = bitcast<float>(v0.z);
+            R.r11 = bitcast<unsigned int>(v0.w);
+            const uint4 v1 = reinterpret_cast<const uint4*>(stage + 512u)[lane];
+            R.r12 = bitcast<unsigned int>(v1.x);
+            R.r13 = bitcast<unsigned int>(v1.y);
+            R.r23 = bitcast<unsigned int>(v1.z);
+            R.r24 = bitcast<unsigned int>(v1.w);
+            const uint4 v2 = reinterpret_cast<const uint4*>(stage + 1024u)[lane];
+            R.r25 = bitcast<unsigned int>(v2.x);
+            R.r42 = bitcast<float>(v2.y);
+            R.r43 = bitcast<float>(v2.z);
+            R.r44 = bitcast<float>(v2.w);
+            const uint4 v3 = reinterpret_cast<const uint4*>(stage + 1536u)[lane];
+            R.r46 = bitcast<float>(v3.x);
+            R.r47 = bitcast<float>(v3.y);
+            R.r48 = bitcast<float>(v3.z);
+            R.r49 = bitcast<float>(v3.w);
+            const uint4 v4 = reinterpret_cast<const uint4*>(stage + 2048u)[lane];
+            R.r50 = bitcast<float>(v4.x);
+            R.r51 = bitcast<float>(v4.y);
+            R.r52 = bitcast<unsigned int>(v4.z);
+            R.r83 = bitcast<float>(v4.w);
+            const uint4 v5 = reinterpret_cast<const uint4*>(stage + 2560u)[lane];
+            R.r84 = bitcast<float>(v5.x);
+            R.r85 = bitcast<float>(v5.y);
+            R.r87 = bitcast<float>(v5.z);
+            R.r117 = bitcast<float>(v5.w);
+            const uint4 v6 = reinterpret_cast<const uint4*>(stage + 3072u)[lane];
+            R.r118 = bitcast<float>(v6.x);
+            R.r119 = bitcast<float>(v6.y);
+            R.r127 = bitcast<float>(v6.z);
+            R.r128 = bitcast<float>(v6.w);
+            const uint2 v7 = reinterpret_cast<const uint2*>(stage + 3584u)[lane];
+            R.r129 = bitcast<float>(v7.x);
+            return v7.y;
+        }
+        default: return 0xffffffffu;
+        }
+    }
 };
 
 const int kInTypes[] = {LOOM_B200_U32, LOOM_B200_U32};
@@ -3841,16 +5109,28 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(a.dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
     if(a.ordinary && a.params.slice_rounds == 1u)
-        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
-    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
 {
     const void* fn = regroup_fn(regs, profile);
     if(!fn) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
+    if(dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);
 }
 
 } } // namespace loom_b200::k_sphere_pt_f32
@@ -3861,4 +5141,4 @@ const loom_b200::KernelEntry loom_b200_entry_sphere_pt_f32 = {
     &loom_b200::k_sphere_pt_f32::launch_plain, &loom_b200::k_sphere_pt_f32::launch_regroup,
     &loom_b200::k_sphere_pt_f32::regroup_occupancy,
     loom_b200::k_sphere_pt_f32::kQueues, loom_b200::k_sphere_pt_f32::kSegments,
-    loom_b200::k_sphere_pt_f32::kRegCaps, 8u};
+    loom_b200::k_sphere_pt_f32::kRegCaps, 8u, loom_b200::k_sphere_pt_f32::K::kMaxStageRow};

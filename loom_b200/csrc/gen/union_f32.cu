@@ -161,6 +161,50 @@ struct K
         }
     }
 
+    // bytes of one queue entry's slots, the largest over the queues
+    static constexpr unsigned kMaxStageRow = 16u;
+    // Lane 0 of a warp: copies the full tile [toff, toff + 32) of queue q
+    // (state half `base`) into `stage` (32 x kMaxStageRow bytes of shared
+    // memory) with one bulk copy per slot column, completing on the
+    // mbarrier at `mbar`; false (nothing issued) when an address is not on
+    // a 16-byte boundary.
+    __device__ __forceinline__ static bool
+    bulk_issue(const int q, unsigned char* stage, const char* base, const unsigned cap, const unsigned toff,
+               unsigned long long* mbar)
+    {
+        unsigned bytes = 0;
+        switch(q)
+        {
+        case 0: bytes = 256u; break;
+        default: return false;
+        }
+        if((reinterpret_cast<unsigned long long>(base) | reinterpret_cast<unsigned long long>(stage)) & 15ull) return false;
+        bulk_expect(mbar, bytes);
+        switch(q)
+        {
+        case 0:
+            bulk_copy(stage + 0u, base + 0ull * cap + static_cast<unsigned long long>(toff) * 8u, 256u, mbar);
+            break;
+        default: break;
+        }
+        return true;
+    }
+
+    // A lane's entry of a tile staged by bulk_issue; returns its thread id.
+    __device__ __forceinline__ static unsigned
+    restore_stage(const int q, Regs& R, const unsigned char* stage, const unsigned lane)
+    {
+        switch(q)
+        {
+        case 0:
+        {
+            const uint2 v0 = reinterpret_cast<const uint2*>(stage + 0u)[lane];
+            R.r0 = bitcast<float>(v0.x);
+            return v0.y;
+        }
+        default: return 0xffffffffu;
+        }
+    }
 };
 
 const int kInTypes[] = {LOOM_B200_F32};
@@ -222,16 +266,28 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
     const void* fn = regroup_fn(a.regs, a.profile);
     if(!fn) return cudaErrorInvalidValue;
+    if(a.dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(a.dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
     if(a.ordinary && a.params.slice_rounds == 1u)
-        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
-    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, 0, a.stream);
+        return cudaLaunchKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
+    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
 {
     const void* fn = regroup_fn(regs, profile);
     if(!fn) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, 0);
+    if(dyn_smem)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   static_cast<int>(dyn_smem));
+        if(e != cudaSuccess) return e;
+    }
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, fn, block, dyn_smem);
 }
 
 } } // namespace loom_b200::k_union_f32
@@ -242,4 +298,4 @@ const loom_b200::KernelEntry loom_b200_entry_union_f32 = {
     &loom_b200::k_union_f32::launch_plain, &loom_b200::k_union_f32::launch_regroup,
     &loom_b200::k_union_f32::regroup_occupancy,
     loom_b200::k_union_f32::kQueues, loom_b200::k_union_f32::kSegments,
-    loom_b200::k_union_f32::kRegCaps, 3u};
+    loom_b200::k_union_f32::kRegCaps, 3u, loom_b200::k_union_f32::K::kMaxStageRow};

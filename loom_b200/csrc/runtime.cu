@@ -139,6 +139,7 @@ constexpr unsigned           kDefaultUtr         = 16;
 constexpr unsigned           kDefaultPeriod      = 1024;
 constexpr unsigned           kDefaultBurst       = 32;
 constexpr unsigned           kDefaultSpread      = 33;
+constexpr unsigned           kMaxDynSmem         = 227u * 1024u; // shared memory one CTA may use
 } // namespace
 
 struct loom_b200_handle
@@ -428,10 +429,19 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         int      ctas  = 0;
         for(;;)
         {
-            const cudaError_t oe = e.regroup_occupancy(static_cast<int>(block), o.profile != 0, o.max_regs, &ctas);
+            const unsigned    dyn = o.bulk_restore ? bulk_stage_bytes(block / 32u, e.max_stage_row) : 0u;
+            const cudaError_t oe  = dyn > kMaxDynSmem ? cudaErrorInvalidValue
+                                                      : e.regroup_occupancy(static_cast<int>(block), o.profile != 0,
+                                                                            o.max_regs, dyn, &ctas);
+            if(oe == cudaErrorInvalidValue && dyn > kMaxDynSmem && block > 32)
+            {
+                block /= 2; // the staging area of this many warps does not fit
+                continue;
+            }
             if(oe == cudaErrorInvalidValue)
             {
-                g_last_error = "register cap not compiled for this kernel (loom_b200_kernel_reg_caps)";
+                g_last_error = dyn ? "bulk_restore: the staging area does not fit in shared memory"
+                                   : "register cap not compiled for this kernel (loom_b200_kernel_reg_caps)";
                 return LOOM_B200_ERR_INVALID;
             }
             LB_CUDA(oe);
@@ -466,6 +476,8 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.params.cost_model    = o.cost_model;
         L.params.schedule      = o.schedule;
         L.params.defer_lanes   = o.defer_lanes;
+        L.params.bulk_restore  = o.bulk_restore;
+        L.dyn_smem             = o.bulk_restore ? bulk_stage_bytes(block / 32u, e.max_stage_row) : 0u;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
         L.regs                 = o.max_regs;

@@ -34,6 +34,7 @@ struct RegroupLaunch
     // beside other kernels; every other launch is cooperative (its CTAs
     // resident together, as the grid barrier between rounds needs)
     bool          ordinary = false;
+    unsigned      dyn_smem = 0; // dynamic shared memory (bulk_restore's staging)
     cudaStream_t  stream;
 };
 
@@ -61,11 +62,12 @@ struct KernelEntry
     unsigned                     num_queues; // work queues of the regrouping engine
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
-    cudaError_t (*regroup_occupancy)(int block, bool profile, unsigned regs, int* ctas_per_sm);
+    cudaError_t (*regroup_occupancy)(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas_per_sm);
     const loom_b200_queue_layout* queues;   // num_queues entries
     const QueueSegment*           segments; // num_queues entries
     const unsigned*               reg_caps; // compiled register caps, default first
     unsigned                      num_reg_caps;
+    unsigned                      max_stage_row; // K::kMaxStageRow (bulk_restore staging per entry)
 };
 
 extern const KernelEntry* const kRegistry[];
