@@ -158,6 +158,13 @@ typedef struct loom_b200_opts
                               column, instead of 128-bit loads from HBM; the
                               CTA size is halved until the staging area
                               fits in shared memory */
+    uint32_t spin_iters;  /* regroup, schedule 2, kernels of more than 300
+                             instructions: iterations of a loop on one block
+                             a lane runs within one step (0 = 1024; smaller
+                             kernels always run 1024, compiled in): a few let
+                             the warp re-form sooner, many save the step's
+                             cost */
+    uint32_t pad1;
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

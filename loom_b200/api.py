@@ -120,6 +120,8 @@ class Opts(ctypes.Structure):
         ("plain_below", ctypes.c_uint64),
         ("defer_lanes", ctypes.c_uint32),
         ("bulk_restore", ctypes.c_uint32),
+        ("spin_iters", ctypes.c_uint32),
+        ("pad1", ctypes.c_uint32),
     ]
 
 
@@ -521,6 +523,7 @@ def make_opts(
     plain_below: int = 0,
     defer_lanes: int = 0,
     bulk_restore: bool = False,
+    spin_iters: int = 0,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -547,6 +550,7 @@ def make_opts(
         plain_below=int(plain_below),
         defer_lanes=int(defer_lanes),
         bulk_restore=1 if bulk_restore else 0,
+        spin_iters=int(spin_iters),
     )
 
 

@@ -56,9 +56,11 @@ SPACE: Dict[str, List] = {
     "plain_below": [0, 1 << 40],
     # schedule 2: lanes a long block waits for (0: off)
     "defer_lanes": [0, 4, 8, 12, 16, 24],
+    # schedule 2: self-loop iterations per step (0: 1024)
+    "spin_iters": [0, 8, 32, 128],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0, plain_below=0, defer_lanes=0)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0, plain_below=0, defer_lanes=0, spin_iters=0)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:

@@ -106,6 +106,11 @@ struct RegroupParams
     // Schedule 2: a long block (K::long_block) runs only once this many of
     // the warp's lanes stand at it, or when no other block is left (0: off).
     unsigned            defer_lanes;
+    // Schedule 2, kernels with one call site (K::kSplitCallSites false):
+    // iterations of a self-loop a lane runs within one step before the step
+    // ends at the loop's header (0: kSelfLoopSpin; small kernels always run
+    // kSelfLoopSpin, a constant their tight loops are compiled with).
+    unsigned            spin_iters;
     // Full tiles come back through shared memory: one bulk copy (TMA,
     // cp.async.bulk) per slot column of the tile, then each lane reads its
     // entry there (the launch's dynamic shared memory holds a staging area
@@ -122,7 +127,7 @@ bulk_stage_bytes(const unsigned warps, const unsigned max_stage_row)
 }
 
 /// Iterations of a self-loop a lane runs within one step of schedule 2
-/// before the step ends at the loop's header.
+/// before the step ends at the loop's header (opts.spin_iters: 0).
 constexpr unsigned kSelfLoopSpin = 1024;
 
 __device__ __forceinline__ unsigned
@@ -448,7 +453,8 @@ regroup_kernel(const RegroupParams p)
                         }
                         else
                             pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
-                                                              cost_on && p.schedule < 2u, minpc ? kSelfLoopSpin : 0u);
+                                                              cost_on && p.schedule < 2u,
+                                                              minpc ? (p.spin_iters ? p.spin_iters : kSelfLoopSpin) : 0u);
                     }
                 }
                 if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;

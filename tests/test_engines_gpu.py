@@ -137,6 +137,8 @@ REGROUP_VARIANTS = [
     dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, defer_lanes=8),
     dict(schedule=2, burst=4, period=api.PERIOD_UNBOUNDED, defer_lanes=32, prefetch=True),
     dict(schedule=2, burst=1, period=5, population=200, defer_lanes=12),
+    # few self-loop iterations per step
+    dict(schedule=2, burst=4, period=api.PERIOD_UNBOUNDED, spin_iters=3),
     # full tiles restored through shared memory with bulk copies
     dict(bulk_restore=True, utr_lanes=24, period=3, population=256),
     dict(bulk_restore=True, cost_model=True, burst=8, population=512, block_size=512),
