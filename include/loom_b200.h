@@ -157,7 +157,8 @@ typedef struct loom_b200_opts
                               cp.async.bulk, no multicast) per 16-byte slot
                               column, instead of 128-bit loads from HBM; the
                               CTA size is halved until the staging area
-                              fits in shared memory */
+                              fits in shared memory; runs at the default
+                              register cap (max_regs is ignored) */
     uint32_t spin_iters;  /* regroup, schedule 2, kernels of more than 300
                              instructions: iterations of a loop on one block
                              a lane runs within one step (0 = 1024; smaller

@@ -799,16 +799,20 @@ def generate(k: Kernel) -> str:
     caps = reg_caps(k)
     w(f"const unsigned kRegCaps[] = {{{', '.join(f'{c}u' for c in caps)}}};")
     w("")
-    w("/// The megakernel at register cap `regs` (0: the default); profiled")
-    w("/// launches use the default cap.  NULL: no such cap compiled.")
-    w("const void* regroup_fn(unsigned regs, bool profile)")
+    w("/// The megakernel at register cap `regs` (0: the default), in its form")
+    w("/// for launches that never park when `park` is false; profiled launches")
+    w("/// and launches with the staged restore (`bulk`) use the default cap and")
+    w("/// the parking form.  NULL: no such cap compiled.")
+    w("const void* regroup_fn(unsigned regs, bool profile, bool bulk, bool park)")
     w("{")
-    w("    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs>);")
+    w("    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs, true>);")
+    w("    if(bulk) return reinterpret_cast<const void*>(&regroup_kernel<K, false, K::kRegroupMaxRegs, true>);")
     w("    switch(regs)")
     w("    {")
     w("    case 0u:")
     for c in caps:
-        w(f"    case {c}u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, {c}>);")
+        w(f"    case {c}u: return park ? reinterpret_cast<const void*>(&regroup_kernel<K, false, {c}, false, true>)")
+        w(f"                          : reinterpret_cast<const void*>(&regroup_kernel<K, false, {c}, false, false>);")
     w("    default: return nullptr;")
     w("    }")
     w("}")
@@ -816,7 +820,7 @@ def generate(k: Kernel) -> str:
     w("cudaError_t launch_regroup(const RegroupLaunch& a)")
     w("{")
     w("    void* args[] = {const_cast<RegroupParams*>(&a.params)};")
-    w("    const void* fn = regroup_fn(a.regs, a.profile);")
+    w("    const void* fn = regroup_fn(a.regs, a.profile, a.params.bulk_restore != 0u, a.park);")
     w("    if(!fn) return cudaErrorInvalidValue;")
     w("    if(a.dyn_smem)")
     w("    {")
@@ -829,9 +833,9 @@ def generate(k: Kernel) -> str:
     w("    return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);")
     w("}")
     w("")
-    w("cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)")
+    w("cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, bool park, int* ctas)")
     w("{")
-    w("    const void* fn = regroup_fn(regs, profile);")
+    w("    const void* fn = regroup_fn(regs, profile, dyn_smem != 0u, park);")
     w("    if(!fn) return cudaErrorInvalidValue;")
     w("    if(dyn_smem)")
     w("    {")

@@ -242,8 +242,12 @@ claim_inputs(const unsigned need, RegroupCtl* ctl, unsigned long long admit_end,
 
 /// The megakernel.  `__maxnreg__` holds it to a register cap (`kRegs`, by
 /// default `K::kRegroupMaxRegs`) so that enough warps stay resident to hide
-/// the latency of the lanes it keeps running.
-template <typename K, bool kProf, int kRegs = K::kRegroupMaxRegs>
+/// the latency of the lanes it keeps running; `kBulk` compiles the staged
+/// (bulk-copy) tile restore in.  With `kPark` false the kernel serves only
+/// launches that never park (schedule 2 or 3, no period): it has no queue
+/// pop, restore or park code and no group selection of schedules 0 and 1,
+/// code that such launches never run but that would still cost registers.
+template <typename K, bool kProf, int kRegs = K::kRegroupMaxRegs, bool kBulk = false, bool kPark = true>
 __global__ void __maxnreg__(kRegs)
 regroup_kernel(const RegroupParams p)
 {
@@ -273,7 +277,9 @@ regroup_kernel(const RegroupParams p)
     const unsigned      wib   = threadIdx.x >> 5;
     unsigned long long* mbar  = reinterpret_cast<unsigned long long*>(s_dyn) + wib;
     unsigned char*      stage = s_dyn + (blockDim.x / 32u * 8u + 15u) / 16u * 16u + wib * 32u * K::kMaxStageRow;
-    bool                bulk_ok    = p.bulk_restore != 0u;
+    // the staged restore is compiled into its own instantiation (kBulk):
+    // its code would cost the other launches registers
+    bool                bulk_ok    = kBulk && p.bulk_restore != 0u;
     unsigned            bulk_phase = 0;
     if(bulk_ok)
     {
@@ -302,7 +308,7 @@ regroup_kernel(const RegroupParams p)
             // at different queues, so they contend less)
             int      tb = kEmpty;
             unsigned tk = 0, toff = 0;
-            for(int c = 0; c < (B + 31) / 32 && tb < 0; ++c)
+            for(int c = 0; kPark && c < (B + 31) / 32 && tb < 0; ++c)
             {
                 const int base = ((static_cast<int>(bsel) / 32 + c) % ((B + 31) / 32)) * 32;
                 const int b    = base + static_cast<int>(lane);
@@ -337,7 +343,7 @@ regroup_kernel(const RegroupParams p)
             }
             int                pc  = kEmpty;
             unsigned long long tid = 0;
-            if(tb >= 0)
+            if(kPark && tb >= 0)
             {
                 bool staged = false;
                 if(bulk_ok && tk == 32u)
@@ -457,7 +463,7 @@ regroup_kernel(const RegroupParams p)
                                                               minpc ? (p.spin_iters ? p.spin_iters : kSelfLoopSpin) : 0u);
                     }
                 }
-                if(p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
+                if(kPark && p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);
                 if(hm != 0u)
                 {
@@ -486,7 +492,7 @@ regroup_kernel(const RegroupParams p)
                         }
                     }
                 }
-                if(steps >= p.period) break;
+                if(kPark && steps >= p.period) break;
                 if(p.schedule == 3u)
                 {
                     // the warp takes new threads only when all its lanes
@@ -515,6 +521,7 @@ regroup_kernel(const RegroupParams p)
                     if(__ballot_sync(FULL, pc >= 0) == 0u) break;
                     continue;
                 }
+                if constexpr(!kPark) break; // schedules 0 and 1 always park
                 const unsigned cm = __popc(__ballot_sync(FULL, pc == m));
                 if(!p.schedule && cm >= need(m)) { mc = cm; continue; }
                 // the group to run next among those that meet their block's
@@ -528,6 +535,13 @@ regroup_kernel(const RegroupParams p)
                 if(best == 0u) break;
                 m  = static_cast<int>(best & 0xffffu);
                 mc = p.schedule ? static_cast<unsigned>(__popc(__ballot_sync(FULL, pc == m))) : best >> 16;
+            }
+            if constexpr(!kPark)
+            {
+                // nothing to park: a lane still live here means the launch
+                // was not one that never parks
+                if(pc >= 0 || pf_tid != ~0ull) ctx.flag(kStatusQueueOverrun);
+                continue;
             }
             for(int pass = 0; pass < 2; ++pass)
             {

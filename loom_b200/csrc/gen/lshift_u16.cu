@@ -253,17 +253,23 @@ cudaError_t launch_plain(const PlainLaunch& a)
 
 const unsigned kRegCaps[] = {64u, 40u, 48u};
 
-/// The megakernel at register cap `regs` (0: the default); profiled
-/// launches use the default cap.  NULL: no such cap compiled.
-const void* regroup_fn(unsigned regs, bool profile)
+/// The megakernel at register cap `regs` (0: the default), in its form
+/// for launches that never park when `park` is false; profiled launches
+/// and launches with the staged restore (`bulk`) use the default cap and
+/// the parking form.  NULL: no such cap compiled.
+const void* regroup_fn(unsigned regs, bool profile, bool bulk, bool park)
 {
-    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs>);
+    if(profile) return reinterpret_cast<const void*>(&regroup_kernel<K, true, K::kRegroupMaxRegs, true>);
+    if(bulk) return reinterpret_cast<const void*>(&regroup_kernel<K, false, K::kRegroupMaxRegs, true>);
     switch(regs)
     {
     case 0u:
-    case 64u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 64>);
-    case 40u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 40>);
-    case 48u: return reinterpret_cast<const void*>(&regroup_kernel<K, false, 48>);
+    case 64u: return park ? reinterpret_cast<const void*>(&regroup_kernel<K, false, 64, false, true>)
+                          : reinterpret_cast<const void*>(&regroup_kernel<K, false, 64, false, false>);
+    case 40u: return park ? reinterpret_cast<const void*>(&regroup_kernel<K, false, 40, false, true>)
+                          : reinterpret_cast<const void*>(&regroup_kernel<K, false, 40, false, false>);
+    case 48u: return park ? reinterpret_cast<const void*>(&regroup_kernel<K, false, 48, false, true>)
+                          : reinterpret_cast<const void*>(&regroup_kernel<K, false, 48, false, false>);
     default: return nullptr;
     }
 }
@@ -271,7 +277,7 @@ const void* regroup_fn(unsigned regs, bool profile)
 cudaError_t launch_regroup(const RegroupLaunch& a)
 {
     void* args[] = {const_cast<RegroupParams*>(&a.params)};
-    const void* fn = regroup_fn(a.regs, a.profile);
+    const void* fn = regroup_fn(a.regs, a.profile, a.params.bulk_restore != 0u, a.park);
     if(!fn) return cudaErrorInvalidValue;
     if(a.dyn_smem)
     {
@@ -284,9 +290,9 @@ cudaError_t launch_regroup(const RegroupLaunch& a)
     return cudaLaunchCooperativeKernel(fn, dim3(a.grid), dim3(a.block), args, a.dyn_smem, a.stream);
 }
 
-cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas)
+cudaError_t regroup_occupancy(int block, bool profile, unsigned regs, unsigned dyn_smem, bool park, int* ctas)
 {
-    const void* fn = regroup_fn(regs, profile);
+    const void* fn = regroup_fn(regs, profile, dyn_smem != 0u, park);
     if(!fn) return cudaErrorInvalidValue;
     if(dyn_smem)
     {

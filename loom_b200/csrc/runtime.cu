@@ -432,7 +432,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
             const unsigned    dyn = o.bulk_restore ? bulk_stage_bytes(block / 32u, e.max_stage_row) : 0u;
             const cudaError_t oe  = dyn > kMaxDynSmem ? cudaErrorInvalidValue
                                                       : e.regroup_occupancy(static_cast<int>(block), o.profile != 0,
-                                                                            o.max_regs, dyn, &ctas);
+                                                                            o.max_regs, dyn, !never_parks(o), &ctas);
             if(oe == cudaErrorInvalidValue && dyn > kMaxDynSmem && block > 32)
             {
                 block /= 2; // the staging area of this many warps does not fit
@@ -482,6 +482,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
         L.regs                 = o.max_regs;
+        L.park                 = !never_parks(o);
         L.profile              = o.profile != 0;
         L.stream               = stream;
         const uint64_t admit = first + (never_parks(o) ? n : std::min<uint64_t>(n, cap));

@@ -35,6 +35,9 @@ struct RegroupLaunch
     // resident together, as the grid barrier between rounds needs)
     bool          ordinary = false;
     unsigned      dyn_smem = 0; // dynamic shared memory (bulk_restore's staging)
+    // false: the launch never parks (schedule 2 or 3, no period) and runs
+    // the megakernel compiled without queue code
+    bool          park = true;
     cudaStream_t  stream;
 };
 
@@ -62,7 +65,8 @@ struct KernelEntry
     unsigned                     num_queues; // work queues of the regrouping engine
     cudaError_t (*plain)(const PlainLaunch&);
     cudaError_t (*regroup)(const RegroupLaunch&);
-    cudaError_t (*regroup_occupancy)(int block, bool profile, unsigned regs, unsigned dyn_smem, int* ctas_per_sm);
+    cudaError_t (*regroup_occupancy)(int block, bool profile, unsigned regs, unsigned dyn_smem, bool park,
+                                     int* ctas_per_sm);
     const loom_b200_queue_layout* queues;   // num_queues entries
     const QueueSegment*           segments; // num_queues entries
     const unsigned*               reg_caps; // compiled register caps, default first

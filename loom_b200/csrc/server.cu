@@ -450,7 +450,7 @@ loom_b200_server_create(const char*                 kernel,
     int      ctas  = 0;
     for(;;)
     {
-        if(e->regroup_occupancy(static_cast<int>(block), o.profile != 0, o.max_regs, 0u, &ctas) != cudaSuccess)
+        if(e->regroup_occupancy(static_cast<int>(block), o.profile != 0, o.max_regs, 0u, true, &ctas) != cudaSuccess)
         {
             delete s;
             return LOOM_B200_ERR_CUDA;
@@ -657,7 +657,7 @@ slice_launch(loom_b200_server* s, unsigned ctas_per_sm)
         // never more CTAs per SM than fit (cooperative launches need every
         // CTA resident at once)
         int fit = 0;
-        SV_CUDA(s->e->regroup_occupancy(static_cast<int>(s->block), o.profile != 0, o.max_regs, 0u, &fit));
+        SV_CUDA(s->e->regroup_occupancy(static_cast<int>(s->block), o.profile != 0, o.max_regs, 0u, true, &fit));
         const unsigned c = std::min<unsigned>(ctas_per_sm, static_cast<unsigned>(std::max(fit, 1)));
         L.grid           = c * static_cast<unsigned>(s->sms);
     }

@@ -203,7 +203,7 @@ loom_b200_launch_static(const char*             kernel,
     int      ctas  = 0;
     for(;;)
     {
-        if(e->regroup_occupancy(static_cast<int>(block), false, 0u, 0u, &ctas) != cudaSuccess)
+        if(e->regroup_occupancy(static_cast<int>(block), false, 0u, 0u, true, &ctas) != cudaSuccess)
             return LOOM_B200_ERR_CUDA;
         if(ctas > 0 || block <= 32) break;
         block /= 2;

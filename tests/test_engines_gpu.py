@@ -139,6 +139,11 @@ REGROUP_VARIANTS = [
     dict(schedule=2, burst=1, period=5, population=200, defer_lanes=12),
     # few self-loop iterations per step
     dict(schedule=2, burst=4, period=api.PERIOD_UNBOUNDED, spin_iters=3),
+    # the never-park instantiation at another register cap, and a never-park
+    # launch that asks for the staged restore (which then runs the parking form)
+    dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, max_regs=48),
+    dict(schedule=3, burst=1 << 20, period=api.PERIOD_UNBOUNDED, max_regs=40, block_size=128),
+    dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, bulk_restore=True),
     # full tiles restored through shared memory with bulk copies
     dict(bulk_restore=True, utr_lanes=24, period=3, population=256),
     dict(bulk_restore=True, cost_model=True, burst=8, population=512, block_size=512),
