@@ -455,11 +455,11 @@ regroup_kernel(const RegroupParams p)
                             if(minpc)
                                 pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, kSelfLoopSpin);
                             else
-                                pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, cost_on && p.schedule < 2u);
+                                pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, kPark && cost_on && p.schedule < 2u);
                         }
                         else
                             pc = K::template run_burst<kProf>(pc, R, ctx, minpc ? 1u : p.burst,
-                                                              cost_on && p.schedule < 2u,
+                                                              kPark && cost_on && p.schedule < 2u,
                                                               minpc ? (p.spin_iters ? p.spin_iters : kSelfLoopSpin) : 0u);
                     }
                 }
