@@ -575,6 +575,61 @@ def cpu_reference(w, check_tids=None, target_s: float = 2.0):
     return m / dt / 1e6, info, want
 
 
+def cpu_hybrid_port(w, target_s: float = 2.0, stream: int = 288, utr_den: int = 16):
+    """Loom's hybrid method on all host cores, as the gang port restates it
+    (oracle/gang_engine.hpp: N-lane gangs, threaded dispatch, counting sort
+    by PC, one stream of `stream` threads per worker in the manner of
+    mp::Shop; Loom's best published path-tracer configuration is a stream of
+    288 and a 1/16 threshold, site-docs/bm-results.md:40).  Timed like
+    cpu_reference on a bounded random sample (seed 7); checked bit for bit
+    against bse on the first 1024 of those threads.  None when the port is
+    not built."""
+    from oracle import oracle as O
+
+    if not O.gang_available():
+        return None
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    pool = rng.integers(0, w.n, size=min(w.n, 1 << 26))
+    m = 1 << 12
+    while True:
+        ins, table = w.ref_inputs(pool[:m])
+        t0 = time.perf_counter()
+        O.gang_run(w.kernel, ins, len(ins[0]), threads=cores, table=table, stream=stream, utr_den=utr_den)
+        dt = time.perf_counter() - t0
+        if dt > target_s / 8 or m >= len(pool):
+            break
+        m = min(len(pool), m * 4)
+    m = min(len(pool), max(m, int(m * target_s / max(dt, 1e-9))))
+    ins, table = w.ref_inputs(pool[:m])
+    st = {}
+    t0 = time.perf_counter()
+    got = O.gang_run(w.kernel, ins, len(ins[0]), threads=cores, table=table, stream=stream, utr_den=utr_den,
+                     stats=st)
+    dt = time.perf_counter() - t0
+    k = min(1024, len(ins[0]))
+    ok = None
+    if O.ref_available():
+        want = O.ref_run(w.kernel, [a[:k] for a in ins], k, threads=cores, table=table)
+        ok = bool(same_bits([g[:k] for g in got], want, w.kernel))
+    from loom_b200.codegen import ir as _ir
+    from oracle import gang_emit
+
+    lanes = gang_emit.lanes_of(_ir.load(w.kernel))
+    return {
+        "value": round(m / dt / 1e6, 3),
+        "unit": "Msamples/s",
+        "cores": cores,
+        "kind": "port",
+        "method": f"hybrid stream, {stream} threads per worker, threshold 1/{utr_den}, {lanes}-lane gangs",
+        "lane_efficiency": round(st["lanes"] / max(1, st["blocks"] * lanes), 4),
+        "sample": f"{m} threads drawn at random (seed 7) from the workload's {w.n}, on {_cpu_model()}; Loom's "
+                  "hybrid method restated for g++ (oracle/gang_engine.hpp), one worker per core",
+        "seconds": round(dt, 3),
+        "equals_bse_on_first_1024": ok,
+    }
+
+
 # Float outputs that pass through the host libm's sinf/cosf (Loom's
 # pt2_const) are held within this many ulp of the reference; everything else
 # is compared bit for bit.
@@ -1388,6 +1443,8 @@ def sub_config(name, api, torch, stream, steps, warmup, dist, world, no_cpu, ext
         v, info, want = cpu_reference(w, check_tids=tids, target_s=1.0)
         cpu = dict(info, value=round(v, 3))
     d = workload_summary(w, res, world, cpu, want, e2e, tids)
+    if not no_cpu:
+        d["cpu_hybrid_port"] = cpu_hybrid_port(w, target_s=1.0)
     d["steps"], d["warmup"] = steps, warmup
     if extra_check:
         d["parity"].update(extra_check(w))
@@ -1523,10 +1580,11 @@ def main() -> None:
     clocks = rg["clocks"]
     e2e = run_e2e(w, api, torch, args.steps, warmup, dist, world)
 
-    cpu = want = None
+    cpu = want = hyb = None
     if rank == 0 and not args.no_cpu:
         v, info, want = cpu_reference(w, check_tids=tids)
         cpu = dict(info, value=round(v, 3))
+        hyb = cpu_hybrid_port(w)
     summary = workload_summary(w, res, world, cpu, want, e2e, tids)
 
     # the other configurations of the default run, each with its parity check
@@ -1632,6 +1690,7 @@ def main() -> None:
             "roofline": roof,
             "sass_issue": sass,
             "cpu_baseline": cpu,
+            "cpu_hybrid_port": hyb,
             "e2e": {k: v for k, v in e2e.items() if k != "equals_device"},
             "gpu_launches": w.launches_per_step * args.steps,
             "clocks": clocks,

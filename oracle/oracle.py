@@ -215,6 +215,70 @@ def ref_run(
     return outs
 
 
+# ---------------------------------------------------------------- gang port
+GANG_SO = HERE / "_lib" / "libloomgang.so"
+GANG_METHODS = {"compact": 0, "hybrid": 1}
+_gang_lib = None
+
+
+def gang_available() -> bool:
+    return GANG_SO.exists()
+
+
+def gang_run(
+    name: str,
+    inputs: Sequence[Optional[np.ndarray]],
+    n: int,
+    threads: int = 1,
+    table: Optional[np.ndarray] = None,
+    method: str = "hybrid",
+    stream: int = 288,
+    utr_den: int = 16,
+    stats: Optional[Dict[str, int]] = None,
+):
+    """Run the CPU gang port (oracle/gang_engine.hpp, Loom's compact or
+    hybrid method restated) on threads [0, n) with `threads` workers, each
+    with a hybrid stream of `stream` threads and utilisation threshold
+    1/utr_den; a None input is the thread index.  With `stats`, fills in the
+    gang block executions, the lanes active in them and the sorts."""
+    global _gang_lib
+    if _gang_lib is None:
+        if not GANG_SO.exists():
+            raise FileNotFoundError(f"{GANG_SO} not built (oracle/build_gang.py)")
+        lib = ctypes.CDLL(str(GANG_SO))
+        lib.loom_gang_run.restype = ctypes.c_int
+        lib.loom_gang_run.argtypes = [
+            ctypes.c_char_p,
+            ctypes.POINTER(ctypes.c_void_p),
+            ctypes.POINTER(ctypes.c_void_p),
+            ctypes.c_uint64,
+            ctypes.c_int,
+            ctypes.c_void_p,
+            ctypes.c_int,
+            ctypes.c_uint,
+            ctypes.c_uint,
+            ctypes.POINTER(ctypes.c_uint64),
+        ]
+        _gang_lib = lib
+    text = (IR_DIR / f"{name}.lir").read_text()
+    in_decl, out_decl = _parse_io(text)
+    ins = [None if a is None else np.ascontiguousarray(a, dtype=NP_TYPE[t]) for a, (_, t) in zip(inputs, in_decl)]
+    outs = [np.zeros(n, dtype=NP_TYPE[t]) for _, t in out_decl]
+    pin = (ctypes.c_void_p * max(1, len(ins)))(*[None if a is None else a.ctypes.data for a in ins])
+    pout = (ctypes.c_void_p * max(1, len(outs)))(*[o.ctypes.data for o in outs])
+    tab = None if table is None else np.ascontiguousarray(table, dtype=np.uint32)
+    st = (ctypes.c_uint64 * 3)()
+    rc = _gang_lib.loom_gang_run(
+        name.encode(), pin, pout, n, threads, None if tab is None else tab.ctypes.data,
+        GANG_METHODS[method], stream, utr_den, st,
+    )
+    if rc != 0:
+        raise KeyError(f"{name} not in the gang port")
+    if stats is not None:
+        stats.update(blocks=int(st[0]), lanes=int(st[1]), sorts=int(st[2]))
+    return outs
+
+
 # ---------------------------------------------------------------- numpy refs
 def val_fib(n: np.ndarray) -> np.ndarray:
     """Loom src/tests/programs.hpp:353-368: fib(n) for n <= 1 is n, else the
