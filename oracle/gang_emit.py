@@ -40,6 +40,9 @@ from loom_b200.codegen.emit_cuda import CTYPE, Lowering  # noqa: E402
 # computed in every lane and blended)
 _TRAPPING = {"div", "mod"}
 
+# libm calls stay scalar: made only for the lanes that run the block
+_LIBM = {"sin", "cos"}
+
 # signed lane-mask type of each register width
 _MASK_T = {1: "signed char", 2: "short", 4: "int", 8: "long long"}
 
@@ -225,7 +228,7 @@ def generate(k: ir.Kernel) -> str:
             expr = L.value(ins.dst, L.expr(ins))
             d = f"R.r{ins.dst.reg}[l]"
             mw = L.regs[ins.dst.reg].nbytes
-            if ins.op in _TRAPPING and ins.optype and ins.optype[0] in ir.INT_TYPES:
+            if ins.op in _LIBM or (ins.op in _TRAPPING and ins.optype and ins.optype[0] in ir.INT_TYPES):
                 w(f"        {_LOOP} if(m{mw}[l]) {d} = {expr};")
             else:
                 w(f"        {_LOOP} {{ const auto v = {expr}; {d} = m{mw}[l] ? v : {d}; }}")
