@@ -165,7 +165,11 @@ typedef struct loom_b200_opts
                              kernels always run 1024, compiled in): a few let
                              the warp re-form sooner, many save the step's
                              cost */
-    uint32_t pad1;
+    uint32_t refill_lanes; /* regroup, schedule 2: a warp's burst of steps
+                              ends as soon as this many of its lanes have
+                              halted, so that the threads that replace them
+                              start together (0: every burst runs its full
+                              length) */
 } loom_b200_opts;
 
 /* Counters of the launches since the last reset. */

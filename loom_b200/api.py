@@ -121,7 +121,7 @@ class Opts(ctypes.Structure):
         ("defer_lanes", ctypes.c_uint32),
         ("bulk_restore", ctypes.c_uint32),
         ("spin_iters", ctypes.c_uint32),
-        ("pad1", ctypes.c_uint32),
+        ("refill_lanes", ctypes.c_uint32),
     ]
 
 
@@ -524,6 +524,7 @@ def make_opts(
     defer_lanes: int = 0,
     bulk_restore: bool = False,
     spin_iters: int = 0,
+    refill_lanes: int = 0,
 ) -> Opts:
     if isinstance(mode, str):
         mode = {"plain": PLAIN, "regroup": REGROUP}[mode]
@@ -551,6 +552,7 @@ def make_opts(
         defer_lanes=int(defer_lanes),
         bulk_restore=1 if bulk_restore else 0,
         spin_iters=int(spin_iters),
+        refill_lanes=int(refill_lanes),
     )
 
 

@@ -36,7 +36,10 @@ HERE = pathlib.Path(__file__).resolve().parent
 TUNING_FILE = HERE / "tuning.json"
 
 SPACE: Dict[str, List] = {
-    "burst": [1, 2, 4, 8, 16, 32, 64],
+    # between 8 and 16 the lane efficiency of schedule 2 on the path tracer
+    # moves by a few per cent from one value to the next (when halted lanes
+    # refill, against the loop's step count), so the grid is fine there
+    "burst": [1, 2, 4, 8, 10, 12, 14, 16, 20, 24, 32, 64],
     "utr_lanes": [1, 4, 8, 12, 16, 20, 24],
     "spread_lanes": [1, 8, 16, 24, 33],
     # 0xffffffff: no period limit (schedule 2 then never parks)
@@ -55,12 +58,14 @@ SPACE: Dict[str, List] = {
     # always (where the megakernel does not pay, the tuner may say so)
     "plain_below": [0, 1 << 40],
     # schedule 2: lanes a long block waits for (0: off)
-    "defer_lanes": [0, 4, 8, 12, 16, 24],
+    "defer_lanes": [0, 2, 4, 5, 6, 8, 12, 16, 24],
     # schedule 2: self-loop iterations per step (0: 1024)
     "spin_iters": [0, 8, 32, 128],
+    # schedule 2: halted lanes that end a burst early (0: off)
+    "refill_lanes": [0, 1, 2, 4, 6, 8, 10, 12, 16],
 }
 
-DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0, plain_below=0, defer_lanes=0, spin_iters=0)
+DEFAULT = dict(burst=32, utr_lanes=16, spread_lanes=33, period=1024, block_size=256, population=0, ctas_per_sm=0, prefetch=True, cost_model=False, schedule=0, max_regs=0, plain_below=0, defer_lanes=0, spin_iters=0, refill_lanes=0)
 
 
 def time_launch(fn: Callable[[], None], reps: int = 2) -> float:

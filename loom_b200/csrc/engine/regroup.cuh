@@ -111,6 +111,9 @@ struct RegroupParams
     // ends at the loop's header (0: kSelfLoopSpin; small kernels always run
     // kSelfLoopSpin, a constant their tight loops are compiled with).
     unsigned            spin_iters;
+    // Schedule 2: a burst ends once this many of the warp's lanes have
+    // halted (their replacements then start together; 0: full bursts).
+    unsigned            refill_lanes;
     // Full tiles come back through shared memory: one bulk copy (TMA,
     // cp.async.bulk) per slot column of the tile, then each lane reads its
     // entry there (the launch's dynamic shared memory holds a staging area
@@ -462,6 +465,9 @@ regroup_kernel(const RegroupParams p)
                                                               kPark && cost_on && p.schedule < 2u,
                                                               minpc ? (p.spin_iters ? p.spin_iters : kSelfLoopSpin) : 0u);
                     }
+                    if(minpc && p.refill_lanes &&
+                       static_cast<unsigned>(__popc(__ballot_sync(FULL, pc == kHalt))) >= p.refill_lanes)
+                        break;
                 }
                 if(kPark && p.period != LOOM_B200_PERIOD_UNBOUNDED) steps += p.burst;
                 const unsigned hm = __ballot_sync(FULL, pc == kHalt);

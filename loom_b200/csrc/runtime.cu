@@ -478,6 +478,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.params.defer_lanes   = o.defer_lanes;
         L.params.bulk_restore  = o.bulk_restore;
         L.params.spin_iters    = o.spin_iters;
+        L.params.refill_lanes  = o.refill_lanes;
         L.dyn_smem             = o.bulk_restore ? bulk_stage_bytes(block / 32u, e.max_stage_row) : 0u;
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;

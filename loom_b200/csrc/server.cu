@@ -644,6 +644,7 @@ slice_launch(loom_b200_server* s, unsigned ctas_per_sm)
     L.params.schedule      = o.schedule;
     L.params.defer_lanes   = o.defer_lanes;
     L.params.spin_iters    = o.spin_iters;
+    L.params.refill_lanes  = o.refill_lanes;
     L.params.round0        = static_cast<unsigned>(s->next_round);
     // beside other servers' slices: one round, an ordinary launch (no grid
     // barrier to wait at), so that the GPU runs the slices together;

@@ -139,6 +139,9 @@ REGROUP_VARIANTS = [
     dict(schedule=2, burst=1, period=5, population=200, defer_lanes=12),
     # few self-loop iterations per step
     dict(schedule=2, burst=4, period=api.PERIOD_UNBOUNDED, spin_iters=3),
+    # bursts that end once lanes have halted
+    dict(schedule=2, burst=64, period=api.PERIOD_UNBOUNDED, refill_lanes=1),
+    dict(schedule=2, burst=16, period=7, population=300, refill_lanes=4),
     # the never-park instantiation at another register cap, and a never-park
     # launch that asks for the staged restore (which then runs the parking form)
     dict(schedule=2, burst=2, period=api.PERIOD_UNBOUNDED, max_regs=48),
