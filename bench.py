@@ -1282,12 +1282,14 @@ def tune_main(args) -> None:
     f.close()
 
 
-def measure(w, api, torch, stream, steps, warmup, dist, tids, forms, clocks_for=None):
+def measure(w, api, torch, stream, steps, warmup, dist, tids, forms, clocks_for=None, full_for=()):
     """The plain engine and each regrouping form of workload `w`: CUDA-event
     time of `steps` steps after `warmup`, one counted launch (VM-instruction
     counters, lane efficiency) and the outputs at `tids`.  `forms` maps a
     name to regrouping options; the form named `clocks_for` is timed again
-    with the clocks sampled.  Returns a dict per engine and form."""
+    with the clocks sampled; the engines and forms named in `full_for` keep
+    every output of their last timed step (host arrays, "full").  Returns a
+    dict per engine and form."""
     res = {}
     for name, mode, opts in [("plain", "plain", {})] + [(k, "regroup", o) for k, o in forms.items()]:
         run_opts = dict(opts, graph=True) if mode == "regroup" else {}
@@ -1302,6 +1304,8 @@ def measure(w, api, torch, stream, steps, warmup, dist, tids, forms, clocks_for=
         st_t = f.stats(raise_on_device_error=True)
         out = w.outputs_at(tids)
         extra = {}
+        if name in full_for:
+            extra["full"] = [o.cpu().numpy() for o in w.d_out]
         if hasattr(w, "image_rows_ok"):
             extra["image"] = [img[:].clone() for img in getattr(w, "d_img", [])]
         dev_bytes = f.device_bytes()
@@ -1344,7 +1348,7 @@ def issue_roofline(vm_instr: float, kern_ms: float, sm_mhz: float) -> dict:
             "frac": round(got / top, 4)}
 
 
-def workload_summary(w, res, world, cpu=None, want=None, e2e=None, tids=None):
+def workload_summary(w, res, world, cpu=None, want=None, e2e=None, tids=None, full=None):
     """The figures of one workload: value and ms per step of the tuned
     regrouping form, the plain engine and the other forms beside it, lane
     efficiencies, parity against the reference on the sampled threads."""
@@ -1407,8 +1411,12 @@ def workload_summary(w, res, world, cpu=None, want=None, e2e=None, tids=None):
             w.d_img = rg["image"]
             par["image_ok"] = w.image_rows_ok(want, tids)
             par["image_pixels_checked"] = int(len(tids) // getattr(w, "spp", 1))
+    if full is not None:
+        par["full_size"] = full
+    full_ok = all(v for k, v in (full or {}).items() if k.endswith("_ok"))
     par["parity"] = bool(par.get("regroup_ok", par["plain_equals_regroup"]) and par["plain_equals_regroup"]
-                         and par.get("image_ok", True) is not False and not par.get("requests_failed"))
+                         and par.get("image_ok", True) is not False and not par.get("requests_failed")
+                         and full_ok)
     d["parity"] = par
     if cpu is not None:
         d["cpu_baseline"] = cpu
@@ -1429,20 +1437,24 @@ def run_e2e(w, api, torch, steps, warmup, dist, world):
     }
 
 
-def sub_config(name, api, torch, stream, steps, warmup, dist, world, no_cpu, extra_check=None):
+def sub_config(name, api, torch, stream, steps, warmup, dist, world, no_cpu, extra_check=None, full_check=False):
     """One more configuration of the default run, measured like the
-    headline with its own (smaller) step count."""
+    headline with its own (smaller) step count; with `full_check`, every
+    output is checked against bse (full_parity)."""
     w = make_workload(name)
     w.opts = regroup_opts(w.kernel, w.tune_key)
     w.device_buffers(torch)
     tids = w.check_tids()
-    res = measure(w, api, torch, stream, steps, warmup, dist, tids, regroup_forms(w))
+    full_for = ("regroup", "plain") if full_check and not no_cpu else ()
+    res = measure(w, api, torch, stream, steps, warmup, dist, tids, regroup_forms(w), full_for=full_for)
     e2e = run_e2e(w, api, torch, steps, warmup, dist, world)
-    cpu = want = None
+    cpu = want = full = None
     if not no_cpu:
         v, info, want = cpu_reference(w, check_tids=tids, target_s=1.0)
         cpu = dict(info, value=round(v, 3))
-    d = workload_summary(w, res, world, cpu, want, e2e, tids)
+        if full_for:
+            full = full_parity(w, res)
+    d = workload_summary(w, res, world, cpu, want, e2e, tids, full)
     if not no_cpu:
         d["cpu_hybrid_port"] = cpu_hybrid_port(w, target_s=1.0)
     d["steps"], d["warmup"] = steps, warmup
@@ -1454,6 +1466,38 @@ def sub_config(name, api, torch, stream, steps, warmup, dist, world, no_cpu, ext
         if hasattr(w, attr):
             delattr(w, attr)
     torch.cuda.empty_cache()
+    return d
+
+
+def full_parity(w, res, names=("regroup", "plain")):
+    """Every output of the full workload against Loom's bse, run on all host
+    cores over every thread: the last timed step's outputs of the engines
+    and forms in `names` (kept by measure(full_for=...)), bit for bit (float
+    outputs through libm sin/cos within the stated ulp and image bounds),
+    and, for the path tracer, every pixel of the device image against the
+    per-pixel means of bse's samples in sample order."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        return None
+    cores = os.cpu_count() or 1
+    ins, table = w.ref_inputs(np.arange(w.n, dtype=np.int64))
+    t0 = time.perf_counter()
+    want = O.ref_run(w.kernel, ins, w.n, threads=cores, table=table)
+    dt = time.perf_counter() - t0
+    d = {"threads": int(w.n), "reference": "Loom bse on every thread", "reference_seconds": round(dt, 3),
+         "cores": cores}
+    for name in names:
+        if res.get(name, {}).get("full") is not None:
+            d[f"{name}_ok"] = bool(same_bits(res[name]["full"], want, w.kernel))
+    if res["regroup"].get("image") and hasattr(w, "spp"):
+        from loom_b200 import scenes as S
+
+        img = np.stack([c.cpu().numpy() for c in res["regroup"]["image"]], axis=1)
+        d["image_ok"] = bool(np.array_equal(img.view(np.uint32), S.pixel_average(want, w.spp).view(np.uint32)))
+        d["image_pixels"] = int(img.shape[0])
+    for name in names:
+        res.get(name, {}).pop("full", None)
     return d
 
 
@@ -1575,17 +1619,21 @@ def main() -> None:
                               "ms_per_step": round(ms / args.steps, 4), "kernel_ms": round(st["ms"], 4),
                               "value": round(world * w.n / (ms / args.steps / 1e3) / 1e6, 3)}))
         return
-    res = measure(w, api, torch, stream, args.steps, warmup, dist, tids, forms, clocks_for="regroup")
+    full_for = ("regroup", "plain") if rank == 0 and not args.no_cpu and args.workload == "pt" else ()
+    res = measure(w, api, torch, stream, args.steps, warmup, dist, tids, forms, clocks_for="regroup",
+                  full_for=full_for)
     rg = res["regroup"]
     clocks = rg["clocks"]
     e2e = run_e2e(w, api, torch, args.steps, warmup, dist, world)
 
-    cpu = want = hyb = None
+    cpu = want = hyb = full = None
     if rank == 0 and not args.no_cpu:
         v, info, want = cpu_reference(w, check_tids=tids)
         cpu = dict(info, value=round(v, 3))
         hyb = cpu_hybrid_port(w)
-    summary = workload_summary(w, res, world, cpu, want, e2e, tids)
+        if full_for:
+            full = full_parity(w, res)
+    summary = workload_summary(w, res, world, cpu, want, e2e, tids, full)
 
     # the other configurations of the default run, each with its parity check
     configs = {}
@@ -1597,7 +1645,7 @@ def main() -> None:
         configs["fib"] = sub_config("fib", api, torch, stream, args.steps, warmup, dist, world, args.no_cpu,
                                     fib_full_check)
         configs["collatz"] = sub_config("collatz", api, torch, stream, args.steps, warmup, dist, world,
-                                        args.no_cpu)
+                                        args.no_cpu, full_check=True)
         configs["batch"] = sub_config("batch", api, torch, stream, max(2, args.steps // 4), 3, dist, world,
                                       args.no_cpu)
         # Loom's own path tracers at 512x512 (where the tuner found that the

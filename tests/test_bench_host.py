@@ -182,3 +182,35 @@ def test_reference_arm_under_torchrun_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["kind"] in ("reference", "port")
+
+
+class _FibFull:
+    """A workload stand-in for full_parity: 3000 Fibonacci threads."""
+
+    kernel = "fib_u64"
+
+    def __init__(self):
+        from oracle import oracle as O
+
+        self.n = 3000
+        self.x = O.uniform_int(9, self.n, 0, 93).astype(np.uint64)
+
+    def ref_inputs(self, tids):
+        return [self.x[np.asarray(tids, dtype=np.int64)]], None
+
+
+def test_full_parity_checks_every_thread():
+    """full_parity runs bse on every thread and compares each kept engine's
+    outputs bit for bit; one wrong output anywhere fails that engine."""
+    from oracle import oracle as O
+
+    if not O.ref_available():
+        pytest.skip("Loom's bse not built here")
+    w = _FibFull()
+    good = O.val_fib(w.x)
+    bad = good.copy()
+    bad[2999] ^= np.uint64(1)
+    res = {"regroup": {"full": [good]}, "plain": {"full": [bad]}}
+    d = bench.full_parity(w, res)
+    assert d["threads"] == 3000 and d["regroup_ok"] is True and d["plain_ok"] is False
+    assert "full" not in res["regroup"]  # the host copies are released
