@@ -633,7 +633,9 @@ def cpu_hybrid_port(w, target_s: float = 2.0, stream: int = 288, utr_den: int = 
 # Float outputs that pass through the host libm's sinf/cosf (Loom's
 # pt2_const) are held within this many ulp of the reference; everything else
 # is compared bit for bit.
-ULP_TOLERANCE = {"pt2_const_40": 4, "pt2_const_512": 4}
+# A libm value one ulp apart is carried through the rest of the path's
+# arithmetic: at 512x512 about 0.4 % of pixels differ, by at most 14 ulp.
+ULP_TOLERANCE = {"pt2_const_40": 16, "pt2_const_512": 16}
 IMAGE_RMSE_TOLERANCE = 1e-6  # relative RMSE of each float output (radiance channel) as an image
 
 
@@ -1651,7 +1653,7 @@ def main() -> None:
         # Loom's own path tracers at 512x512 (where the tuner found that the
         # megakernel does not pay and set the regrouping handle's plain rule)
         for name in ("loom_pt_512", "loom_pt2_512"):
-            configs[name] = sub_config(name, api, torch, stream, 3, 3, dist, world, args.no_cpu)
+            configs[name] = sub_config(name, api, torch, stream, 3, 3, dist, world, args.no_cpu, full_check=True)
         sv, sv_clk = serve_measure(1.0, rank, local, parity=not args.no_cpu)
         full = sv["regroup_serial"]["loads"][-1]
         configs["serve"] = {
