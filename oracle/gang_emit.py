@@ -43,9 +43,6 @@ _TRAPPING = {"div", "mod"}
 # libm calls stay scalar: made only for the lanes that run the block
 _LIBM = {"sin", "cos"}
 
-# signed lane-mask type of each register width
-_MASK_T = {1: "signed char", 2: "short", 4: "int", 8: "long long"}
-
 # a loop over the gang's lanes, kept as a loop (not unrolled) so that g++
 # vectorises it whole
 _LOOP = '_Pragma("GCC ivdep") _Pragma("GCC unroll 1") for(int l = 0; l < N; ++l)'
@@ -212,28 +209,21 @@ def generate(k: ir.Kernel) -> str:
         w(f"    static void block_{b}(Regs& R, const Ctx& ctx)")
         w("    {")
         w("        (void)ctx;")
-        # the block's lane mask at each width the block writes, so that
-        # every lane loop selects between values of one width (and
-        # vectorises): 0 or all ones.  One loop per instruction: g++
-        # vectorises these short loops reliably (a whole block fused into
-        # one lane loop measured slower: parts of it stayed scalar)
-        widths = sorted({L.regs[i.dst.reg].nbytes for i in blk.instrs if isinstance(i, ir.Compute)} | {4})
-        for wd in widths:
-            mt = _MASK_T[wd]
-            w(f"        alignas(64) {mt} m{wd}[N];")
-            w(f"        {_LOOP} m{wd}[l] = R.pc[l] == {b} ? static_cast<{mt}>(-1) : static_cast<{mt}>(0);")
+        # every lane loop selects by comparing the lane's PC with the block
+        # (PCs change only in the block's last loop): one vector compare
+        # per loop, at whatever width the destination has
+        on = f"R.pc[l] == {b}"
         for ins in blk.instrs:
             if not isinstance(ins, ir.Compute):
                 continue
             expr = L.value(ins.dst, L.expr(ins))
             d = f"R.r{ins.dst.reg}[l]"
-            mw = L.regs[ins.dst.reg].nbytes
             if ins.op in _LIBM or (ins.op in _TRAPPING and ins.optype and ins.optype[0] in ir.INT_TYPES):
-                w(f"        {_LOOP} if(m{mw}[l]) {d} = {expr};")
+                w(f"        {_LOOP} if({on}) {d} = {expr};")
             else:
-                w(f"        {_LOOP} {{ const auto v = {expr}; {d} = m{mw}[l] ? v : {d}; }}")
+                w(f"        {_LOOP} {{ const auto v = {expr}; {d} = ({on}) ? v : {d}; }}")
         nx = L.next_expr(blk).replace("kHalt", "kNumBlocks")
-        w(f"        {_LOOP} {{ const int nx = {nx}; R.pc[l] = m4[l] ? nx : R.pc[l]; }}")
+        w(f"        {_LOOP} {{ const int nx = {nx}; R.pc[l] = ({on}) ? nx : R.pc[l]; }}")
         w("    }")
         w("")
     w("    static void exec(const int b, Regs& R, const Ctx& ctx)")
