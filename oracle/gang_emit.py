@@ -40,6 +40,10 @@ from loom_b200.codegen.emit_cuda import CTYPE, Lowering  # noqa: E402
 # computed in every lane and blended)
 _TRAPPING = {"div", "mod"}
 
+# kernels of at most this many instructions have their blocks inlined into
+# the dispatch
+_SMALL_KERNEL = 64
+
 # libm calls stay scalar: made only for the lanes that run the block
 _LIBM = {"sin", "cos"}
 
@@ -72,6 +76,7 @@ def lanes_of(k: ir.Kernel) -> int:
 
 def generate(k: ir.Kernel) -> str:
     L = LaneLowering(k)
+    small = sum(k.instr_counts()) <= _SMALL_KERNEL
     name = k.name
     nb = k.num_blocks
     N = lanes_of(k)
@@ -206,7 +211,11 @@ def generate(k: ir.Kernel) -> str:
     # ---- blocks
     for b, blk in enumerate(k.blocks):
         w(f"    // block {b}: {blk.label}")
-        w(f"    static void block_{b}(Regs& R, const Ctx& ctx)")
+        # the blocks of a large kernel stay functions of their own: inlined
+        # into its dispatch, g++ compiled their lane loops worse (the path
+        # tracers ran 3x slower); a small kernel's dispatch keeps them inline
+        attr = "" if small else "__attribute__((noinline)) "
+        w(f"    {attr}static void block_{b}(Regs& R, const Ctx& ctx)")
         w("    {")
         w("        (void)ctx;")
         # every lane loop selects by comparing the lane's PC with the block
@@ -226,6 +235,57 @@ def generate(k: ir.Kernel) -> str:
         w(f"        {_LOOP} {{ const int nx = {nx}; R.pc[l] = ({on}) ? nx : R.pc[l]; }}")
         w("    }")
         w("")
+    # ---- threaded dispatch with the successors compiled in
+    w("    /// Loom's threaded dispatch (threaded_dispatch::eval) over this kernel:")
+    w("    /// each block's exit counts the lanes at its successors (in jump-table")
+    w("    /// order), adds those with lanes to the pending set and jumps to the")
+    w("    /// fullest one while it holds more lanes than the threshold.")
+    w("    static std::uint64_t run_from(int b, unsigned pops, Regs& R, std::uint64_t pending,")
+    w("                                  const unsigned threshold, const Ctx& ctx, Counters& c)")
+    w("    {")
+    w("        switch(b)")
+    w("        {")
+    for b in range(nb):
+        w(f"        case {b}: goto B{b};")
+    w("        default: return pending;")
+    w("        }")
+    for b in range(nb):
+        ss = succ[b]
+        w(f"    B{b}:")
+        w("        c.blocks += 1;")
+        w("        c.lanes += pops;")
+        w(f"        block_{b}(R, ctx);")
+        w(f"        pending &= ~(1ull << {b});")
+        if len(ss) == 1:
+            t = ss[0]
+            if t == ir.HALT:
+                w("        return pending;")
+            else:
+                w(f"        {{ const unsigned p = pops_at<N>(R.pc, {t}); if(p > threshold) {{ pops = p; goto B{t}; }} }}")
+                w("        return pending;")
+        else:
+            w("        {")
+            w("            unsigned bp = 0;")
+            w("            int bi = -1;")
+            for i, t in enumerate(ss):
+                tid = nb if t == ir.HALT else t
+                keep = "" if t == ir.HALT else f" if(p) pending |= 1ull << {t};"
+                w(f"            {{ const unsigned p = pops_at<N>(R.pc, {tid});{keep} if(p > bp) {{ bp = p; bi = {i}; }} }}")
+            w("            if(bp > threshold)")
+            w("            {")
+            w("                pops = bp;")
+            w("                switch(bi)")
+            w("                {")
+            for i, t in enumerate(ss):
+                if t != ir.HALT:
+                    w(f"                case {i}: goto B{t};")
+            w("                default: break;")
+            w("                }")
+            w("            }")
+            w("        }")
+            w("        return pending;")
+    w("    }")
+    w("")
     w("    static void exec(const int b, Regs& R, const Ctx& ctx)")
     w("    {")
     w("        switch(b)")

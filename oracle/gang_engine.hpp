@@ -137,6 +137,45 @@ enum Method
 
 // ---- gang execution
 
+/// Gang block executions and the lanes active in them.
+struct Counters
+{
+    std::uint64_t blocks = 0;
+    std::uint64_t lanes  = 0;
+};
+
+/// Bit l set when lane l of an N-lane gang stands at block b (an AVX-512
+/// compare per 16 lanes; the PCs are 32-bit).
+template <int N>
+inline std::uint64_t
+lanes_at(const int* pc, const int b)
+{
+    if constexpr(N == 8)
+        return _mm256_cmpeq_epi32_mask(_mm256_load_si256(reinterpret_cast<const __m256i*>(pc)), _mm256_set1_epi32(b));
+    else if constexpr(N % 16 == 0)
+    {
+        std::uint64_t m = 0;
+        for(int i = 0; i < N / 16; ++i)
+            m |= static_cast<std::uint64_t>(_mm512_cmpeq_epi32_mask(_mm512_load_si512(pc + 16 * i), _mm512_set1_epi32(b)))
+                 << (16 * i);
+        return m;
+    }
+    else
+    {
+        std::uint64_t m = 0;
+        for(int l = 0; l < N; ++l) m |= static_cast<std::uint64_t>(pc[l] == b) << l;
+        return m;
+    }
+}
+
+/// Lanes of an N-lane gang at block b.
+template <int N>
+inline unsigned
+pops_at(const int* pc, const int b)
+{
+    return static_cast<unsigned>(std::popcount(lanes_at<N>(pc, b)));
+}
+
 template <typename G>
 struct Gang
 {
@@ -144,30 +183,12 @@ struct Gang
     static constexpr int NB   = G::kNumBlocks;
     static constexpr int HALT = NB;
     using Regs                = typename G::Regs;
+    using Counters            = loom_gang::Counters;
 
-    /// Bit l set when lane l stands at block b (an AVX-512 compare per 16
-    /// lanes; the PCs are 32-bit).
     static std::uint64_t
     lanes_at(const Regs& R, const int b)
     {
-        if constexpr(N == 8)
-            return _mm256_cmpeq_epi32_mask(_mm256_load_si256(reinterpret_cast<const __m256i*>(R.pc)),
-                                           _mm256_set1_epi32(b));
-        else if constexpr(N % 16 == 0)
-        {
-            std::uint64_t m = 0;
-            for(int i = 0; i < N / 16; ++i)
-                m |= static_cast<std::uint64_t>(_mm512_cmpeq_epi32_mask(_mm512_load_si512(R.pc + 16 * i),
-                                                                        _mm512_set1_epi32(b)))
-                     << (16 * i);
-            return m;
-        }
-        else
-        {
-            std::uint64_t m = 0;
-            for(int l = 0; l < N; ++l) m |= static_cast<std::uint64_t>(R.pc[l] == b) << l;
-            return m;
-        }
+        return loom_gang::lanes_at<N>(R.pc, b);
     }
 
     /// Blocks some non-halted lane stands at (greedy_groups, ignore_halt).
@@ -200,59 +221,18 @@ struct Gang
         return pc;
     }
 
-    struct Counters
-    {
-        std::uint64_t blocks = 0; // gang block executions
-        std::uint64_t lanes  = 0; // lanes active in them
-    };
-
-    /// Threaded dispatch from block b, which `pops` lanes stand at:
-    /// returns the pending set.
+    /// Threaded dispatch from block b, which `pops` lanes stand at: run the
+    /// block for its lanes, drop it from the pending set, add every
+    /// successor that has lanes, and go on into the successor with the most
+    /// lanes (the first in jump-table order on a tie) while that group is
+    /// larger than the threshold; returns the pending set.  The kernel's
+    /// generated `run_from` does this with its successors compiled into
+    /// each block's exit (direct jumps, no tables).
     static std::uint64_t
     dispatch(int b, unsigned pops, Regs& R, std::uint64_t pending, const unsigned threshold, const Ctx& ctx,
              Counters& c)
     {
-        for(;;)
-        {
-            c.blocks += 1;
-            c.lanes += pops;
-            G::exec(b, R, ctx);
-            pending &= ~(1ull << b);
-            const int ns = G::kNumSucc[b];
-            if(ns == 1)
-            {
-                const int nx = G::kSucc[b][0];
-                if(nx == HALT) return pending;
-                const unsigned p = static_cast<unsigned>(std::popcount(lanes_at(R, nx)));
-                if(p > threshold)
-                {
-                    b    = nx;
-                    pops = p;
-                    continue;
-                }
-                return pending;
-            }
-            int      best  = HALT;
-            unsigned bpops = 0;
-            for(int i = 0; i < ns; ++i)
-            {
-                const int      nx = G::kSucc[b][i];
-                const unsigned p  = static_cast<unsigned>(std::popcount(lanes_at(R, nx)));
-                if(p > 0 && nx != HALT) pending |= 1ull << nx;
-                if(p > bpops)
-                {
-                    bpops = p;
-                    best  = nx;
-                }
-            }
-            if(bpops > threshold && best != HALT)
-            {
-                b    = best;
-                pops = bpops;
-                continue;
-            }
-            return pending;
-        }
+        return G::run_from(b, pops, R, pending, threshold, ctx, c);
     }
 
     /// Compact execution of one gang until every lane has halted.
