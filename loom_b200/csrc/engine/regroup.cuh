@@ -247,9 +247,10 @@ claim_inputs(const unsigned need, RegroupCtl* ctl, unsigned long long admit_end,
 /// default `K::kRegroupMaxRegs`) so that enough warps stay resident to hide
 /// the latency of the lanes it keeps running; `kBulk` compiles the staged
 /// (bulk-copy) tile restore in.  With `kPark` false the kernel serves only
-/// launches that never park (schedule 2 or 3, no period): it has no queue
-/// pop, restore or park code and no group selection of schedules 0 and 1,
-/// code that such launches never run but that would still cost registers.
+/// launches that never park (schedule 2 or 3, no period) and do not
+/// prefetch: it has no queue pop, restore or park code, no group selection
+/// of schedules 0 and 1 and no input prefetch, code that such launches never
+/// run but that would still cost registers.
 template <typename K, bool kProf, int kRegs = K::kRegroupMaxRegs, bool kBulk = false, bool kPark = true>
 __global__ void __maxnreg__(kRegs)
 regroup_kernel(const RegroupParams p)
@@ -409,7 +410,7 @@ regroup_kernel(const RegroupParams p)
             unsigned steps = 0;
             for(;;)
             {
-                if(p.prefetch && !dry)
+                if(kPark && p.prefetch && !dry)
                 {
                     const unsigned need = __ballot_sync(FULL, pf_tid == ~0ull);
                     if(need)

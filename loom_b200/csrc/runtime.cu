@@ -221,6 +221,15 @@ never_parks(const loom_b200_opts& o)
            o.period == LOOM_B200_PERIOD_UNBOUNDED;
 }
 
+/// Whether a regrouping launch runs the megakernel's parking form: every
+/// launch but those that never park and do not prefetch (the never-park
+/// form is compiled without prefetch).
+bool
+park_form(const loom_b200_opts& o)
+{
+    return !(never_parks(o) && o.no_prefetch);
+}
+
 /// Threads in flight of a regrouping launch: the requested population, or
 /// as many as the queue state of kDefaultStateBudget bytes holds.  A launch
 /// that never parks keeps its threads in registers: its queues get one tile
@@ -432,7 +441,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
             const unsigned    dyn = o.bulk_restore ? bulk_stage_bytes(block / 32u, e.max_stage_row) : 0u;
             const cudaError_t oe  = dyn > kMaxDynSmem ? cudaErrorInvalidValue
                                                       : e.regroup_occupancy(static_cast<int>(block), o.profile != 0,
-                                                                            o.max_regs, dyn, !never_parks(o), &ctas);
+                                                                            o.max_regs, dyn, park_form(o), &ctas);
             if(oe == cudaErrorInvalidValue && dyn > kMaxDynSmem && block > 32)
             {
                 block /= 2; // the staging area of this many warps does not fit
@@ -483,7 +492,7 @@ launch(loom_b200_handle* h, const loom_b200_launch& L, cudaStream_t stream, uint
         L.grid                 = static_cast<unsigned>(ctas * h->sms);
         L.block                = block;
         L.regs                 = o.max_regs;
-        L.park                 = !never_parks(o);
+        L.park                 = park_form(o);
         L.profile              = o.profile != 0;
         L.stream               = stream;
         const uint64_t admit = first + (never_parks(o) ? n : std::min<uint64_t>(n, cap));

@@ -35,8 +35,8 @@ struct RegroupLaunch
     // resident together, as the grid barrier between rounds needs)
     bool          ordinary = false;
     unsigned      dyn_smem = 0; // dynamic shared memory (bulk_restore's staging)
-    // false: the launch never parks (schedule 2 or 3, no period) and runs
-    // the megakernel compiled without queue code
+    // false: the launch never parks (schedule 2 or 3, no period), does not
+    // prefetch and runs the megakernel compiled without queue code
     bool          park = true;
     cudaStream_t  stream;
 };
