@@ -898,14 +898,15 @@ class RegroupService:
         self.budget = api.Budget(SERVE_BUDGET)
         mk = dict(profile=profile, budget=self.budget)
         # collatz and fib servers run 256-thread CTAs, so that one CTA of each
-        # fits on an SM beside one 512-thread CTA of the path tracer (64 + 40
-        # + 48 registers per thread: 54 K of the SM's 64 K registers)
+        # fits on an SM beside one 512-thread CTA of the path tracer (512 x 56
+        # + 256 x 48 + 256 x 48 registers: 53 K of the SM's 64 K)
         self.p = serving.Pool(
             {
                 "pt": api.Server(
                     "sphere_pt_f32", ring_threads=1 << 26, max_requests=512, slice_rounds=4,
                     forms=["instance", "local_iota"], header_words=S.HEADER_WORDS, reloc_word=4,
-                    table_words=1 << 20, **regroup_opts("sphere_pt_f32", "batch"), stream=self.streams["pt"], **mk,
+                    table_words=1 << 20, **{**regroup_opts("sphere_pt_f32", "batch"), "block_size": 512},
+                    stream=self.streams["pt"], **mk,
                 ),
                 "collatz": api.Server(
                     "collatz_u64", ring_threads=1 << 25, max_requests=512, slice_rounds=2,
