@@ -897,20 +897,21 @@ class RegroupService:
         self.streams = {k: torch.cuda.Stream() for k in SERVE_KERNELS}
         self.budget = api.Budget(SERVE_BUDGET)
         mk = dict(profile=profile, budget=self.budget)
-        # collatz and fib servers run 256-thread CTAs, so that one CTA of each
-        # fits on an SM beside one 512-thread CTA of the path tracer (512 x 56
-        # + 256 x 48 + 256 x 48 registers: 53 K of the SM's 64 K)
+        # the servers' own tuned options ("serve": the options of short
+        # slices, which are not those of one long launch); collatz and fib
+        # servers run 256-thread CTAs, so that one CTA of each fits on an SM
+        # beside one 512-thread CTA of the path tracer (512 x 64 + 256 x 40 +
+        # 256 x 48 registers: 54 K of the SM's 64 K)
         self.p = serving.Pool(
             {
                 "pt": api.Server(
                     "sphere_pt_f32", ring_threads=1 << 26, max_requests=512, slice_rounds=4,
                     forms=["instance", "local_iota"], header_words=S.HEADER_WORDS, reloc_word=4,
-                    table_words=1 << 20, **{**regroup_opts("sphere_pt_f32", "batch"), "block_size": 512},
-                    stream=self.streams["pt"], **mk,
+                    table_words=1 << 20, **regroup_opts("sphere_pt_f32", "serve"), stream=self.streams["pt"], **mk,
                 ),
                 "collatz": api.Server(
                     "collatz_u64", ring_threads=1 << 25, max_requests=512, slice_rounds=2,
-                    **{**regroup_opts("collatz_u64"), "population": 1 << 22, "block_size": 256, "ctas_per_sm": 0},
+                    **{**regroup_opts("collatz_u64", "serve"), "population": 1 << 22, "block_size": 256, "ctas_per_sm": 0},
                     stream=self.streams["collatz"], **mk,
                 ),
                 "fib": api.Server(
