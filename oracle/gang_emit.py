@@ -82,7 +82,6 @@ def generate(k: ir.Kernel) -> str:
     N = lanes_of(k)
     regs = [r for r in k.regs if r.idx != L.pc]
     succ = k.succ_table()
-    max_succ = max((len(s) for s in succ), default=1)
     o: List[str] = []
     w = o.append
     w(f"// Generated by oracle/gang_emit.py from loom_b200/ir/{name}.lir.")
@@ -95,18 +94,8 @@ def generate(k: ir.Kernel) -> str:
     w("{")
     w(f"    static constexpr int N = {N};")
     w(f"    static constexpr int kNumBlocks = {nb};")
-    w(f"    static constexpr int kMaxSucc = {max_succ};")
     w(f"    static constexpr int kNumIn = {len(k.inputs)};")
     w(f"    static constexpr int kNumOut = {len(k.outputs)};")
-    # successor lists in the order of the block's jump table, HALT as
-    # kNumBlocks (Loom core.hpp:418-441, threaded_dispatch's table)
-    rows = []
-    for s in succ:
-        ids = [nb if t == ir.HALT else t for t in s]
-        ids += [nb] * (max_succ - len(ids))
-        rows.append("{" + ", ".join(map(str, ids)) + "}")
-    w(f"    static constexpr int kSucc[{nb}][{max_succ}] = {{{', '.join(rows)}}};")
-    w(f"    static constexpr int kNumSucc[{nb}] = {{{', '.join(str(len(s)) for s in succ)}}};")
     w("")
     # ---- gang registers and the stream's columns
     w("    struct Regs")
@@ -235,7 +224,9 @@ def generate(k: ir.Kernel) -> str:
         w(f"        {_LOOP} {{ const int nx = {nx}; R.pc[l] = ({on}) ? nx : R.pc[l]; }}")
         w("    }")
         w("")
-    # ---- threaded dispatch with the successors compiled in
+    # ---- threaded dispatch with the successors compiled in: each block's
+    # successors in the order of its jump table, HALT as kNumBlocks (Loom
+    # src/vm/core.hpp:418-441, the table threaded_dispatch::eval walks)
     w("    /// Loom's threaded dispatch (threaded_dispatch::eval) over this kernel:")
     w("    /// each block's exit counts the lanes at its successors (in jump-table")
     w("    /// order), adds those with lanes to the pending set and jumps to the")
@@ -284,16 +275,6 @@ def generate(k: ir.Kernel) -> str:
             w("            }")
             w("        }")
             w("        return pending;")
-    w("    }")
-    w("")
-    w("    static void exec(const int b, Regs& R, const Ctx& ctx)")
-    w("    {")
-    w("        switch(b)")
-    w("        {")
-    for b in range(nb):
-        w(f"        case {b}: block_{b}(R, ctx); break;")
-    w("        default: break;")
-    w("        }")
     w("    }")
     w("};")
     w("")
