@@ -88,22 +88,32 @@ regroup_reset(RegroupCtl*        ctl,
 /// Per-group means of a float column, summed in thread order: output row r
 /// of instance i covers threads starts[i] + (r - out_starts[i]) * group[i]
 /// and the group[i] - 1 after it; without instances every row covers
-/// `group` threads from r * group.  One CUDA thread per row.
+/// `group` threads from r * group.  Each warp takes 32 consecutive rows.
+/// Where they lie in one instance, their group is a power of two from 4 to
+/// kTileGroupMax and their samples start on a 16-byte boundary (f32), the
+/// warp reads those samples with coalesced 16-byte loads into a padded
+/// shared-memory tile (row stride group + 1: no bank conflicts) and each
+/// lane then sums its row from there; otherwise each lane reads its row
+/// from global memory.  Either way a row's samples are added one after the
+/// other in thread order, so the means are the same bits.
+constexpr unsigned kTileGroupMax = 64;
+constexpr unsigned kMeanWarps    = 4; // warps per CTA of group_mean
+
 template <typename T>
-__global__ void
-group_mean(const T* __restrict__                  in,
-           T* __restrict__                        out,
-           const unsigned long long               rows,
-           const unsigned                         group,
-           const unsigned long long* __restrict__ starts,
-           const unsigned* __restrict__           inst_group,
-           const unsigned long long* __restrict__ out_starts,
-           const unsigned                         num_inst)
+__device__ __forceinline__ void
+row_of(const unsigned long long          r,
+       const unsigned                    group,
+       const unsigned long long* __restrict__ starts,
+       const unsigned* __restrict__           inst_group,
+       const unsigned long long* __restrict__ out_starts,
+       const unsigned                    num_inst,
+       unsigned long long&               t0,
+       unsigned&                         g,
+       unsigned&                         inst)
 {
-    const unsigned long long r = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if(r >= rows) return;
-    unsigned long long t0 = r * group;
-    unsigned           g  = group;
+    t0   = r * group;
+    g    = group;
+    inst = 0;
     if(num_inst)
     {
         unsigned lo = 0, hi = num_inst; // out_starts[lo] <= r < out_starts[hi]
@@ -115,12 +125,84 @@ group_mean(const T* __restrict__                  in,
             else
                 hi = mid;
         }
-        g  = inst_group[lo];
-        t0 = starts[lo] + (r - out_starts[lo]) * g;
+        g    = inst_group[lo];
+        t0   = starts[lo] + (r - out_starts[lo]) * g;
+        inst = lo;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kMeanWarps)
+group_mean(const T* __restrict__                  in,
+           T* __restrict__                        out,
+           const unsigned long long               rows,
+           const unsigned                         group,
+           const unsigned long long* __restrict__ starts,
+           const unsigned* __restrict__           inst_group,
+           const unsigned long long* __restrict__ out_starts,
+           const unsigned                         num_inst)
+{
+    __shared__ float          s_tile[kMeanWarps][32 * (kTileGroupMax + 1)];
+    const unsigned            lane = threadIdx.x & 31u;
+    const unsigned            wib  = threadIdx.x >> 5;
+    const unsigned long long  r0   = (static_cast<unsigned long long>(blockIdx.x) * kMeanWarps + wib) * 32ull;
+    if(r0 >= rows) return;
+    const unsigned            nr = rows - r0 < 32ull ? static_cast<unsigned>(rows - r0) : 32u;
+    const unsigned long long  r  = r0 + lane;
+    unsigned long long        t0 = 0;
+    unsigned                  g = 0, inst = 0;
+    if(lane < nr) row_of<T>(r, group, starts, inst_group, out_starts, num_inst, t0, g, inst);
+    // the tile applies when every row of the warp has the first row's
+    // instance (hence group), the group is a power of two in [4, 64] and
+    // the first row's samples start on a 16-byte boundary
+    const unsigned long long base = __shfl_sync(0xffffffffu, t0, 0);
+    const unsigned           g0   = __shfl_sync(0xffffffffu, g, 0);
+    const unsigned           i0   = __shfl_sync(0xffffffffu, inst, 0);
+    bool tiled = sizeof(T) == 4 && g0 >= 4u && g0 <= kTileGroupMax && (g0 & (g0 - 1u)) == 0u &&
+                 (reinterpret_cast<unsigned long long>(in + base) & 15ull) == 0ull;
+    tiled = __all_sync(0xffffffffu, !tiled || lane >= nr || inst == i0) && tiled;
+    if(tiled)
+    {
+        if constexpr(sizeof(T) == 4)
+        {
+            float*         tile = s_tile[wib];
+            const unsigned sh   = static_cast<unsigned>(__ffs(static_cast<int>(g0))) - 1u; // log2(g0)
+            const unsigned n4   = nr * g0 / 4u;                                           // float4 of the tile
+            const float4*  src  = reinterpret_cast<const float4*>(in + base);
+            for(unsigned e4 = lane; e4 < n4; e4 += 32u)
+            {
+                const float4   v   = __ldg(src + e4);
+                const unsigned e   = 4u * e4;
+                const unsigned row = e >> sh;
+                const unsigned j   = e & (g0 - 1u);
+                float*         d   = tile + row * (g0 + 1u) + j;
+                d[0]               = v.x;
+                d[1]               = v.y;
+                d[2]               = v.z;
+                d[3]               = v.w;
+            }
+            __syncwarp();
+            if(lane < nr)
+            {
+                const float* row = tile + lane * (g0 + 1u);
+                float        acc = 0.0f;
+                for(unsigned j = 0; j < g0; ++j) acc = acc + row[j];
+                out[r] = static_cast<T>(acc / static_cast<float>(g0));
+            }
+        }
+        return;
+    }
+    if(lane >= nr) return;
     T acc = T(0);
     for(unsigned j = 0; j < g; ++j) acc = acc + __ldg(in + t0 + j);
     out[r] = acc / static_cast<T>(g);
+}
+
+/// Grid of group_mean over `rows` rows.
+unsigned
+mean_blocks(const unsigned long long rows)
+{
+    return static_cast<unsigned>((rows + 32ull * kMeanWarps - 1) / (32ull * kMeanWarps));
 }
 
 /// Launch counters: 8 totals, then thread and warp instructions per block.
@@ -850,13 +932,13 @@ loom_b200_group_mean(uint32_t type, const void* in, void* out, uint64_t rows, ui
     if(!in || !out || group == 0 || (type != LOOM_B200_F32 && type != LOOM_B200_F64))
         return LOOM_B200_ERR_INVALID;
     if(rows == 0) return LOOM_B200_OK;
-    const unsigned blocks = static_cast<unsigned>((rows + 255) / 256);
+    const unsigned blocks = mean_blocks(rows);
     auto           st     = static_cast<cudaStream_t>(stream);
     if(type == LOOM_B200_F32)
-        group_mean<float><<<blocks, 256, 0, st>>>(static_cast<const float*>(in), static_cast<float*>(out), rows,
-                                                  group, nullptr, nullptr, nullptr, 0u);
+        group_mean<float><<<blocks, 32 * kMeanWarps, 0, st>>>(static_cast<const float*>(in), static_cast<float*>(out),
+                                                             rows, group, nullptr, nullptr, nullptr, 0u);
     else
-        group_mean<double><<<blocks, 256, 0, st>>>(static_cast<const double*>(in), static_cast<double*>(out),
+        group_mean<double><<<blocks, 32 * kMeanWarps, 0, st>>>(static_cast<const double*>(in), static_cast<double*>(out),
                                                    rows, group, nullptr, nullptr, nullptr, 0u);
     LB_CUDA(cudaGetLastError());
     return LOOM_B200_OK;
@@ -954,17 +1036,17 @@ loom_b200_launch_host_mean(loom_b200_handle* h, const loom_b200_launch* L, const
         d_g  = reinterpret_cast<const unsigned*>(m + out_starts.size() * 8);
     }
     const auto*    d_st   = static_cast<const unsigned long long*>(h->d_starts);
-    const unsigned blocks = static_cast<unsigned>((rows + 255) / 256);
+    const unsigned blocks = mean_blocks(rows);
     size_t         off    = 0;
     for(uint32_t j = 0; j < info.num_outputs; ++j)
     {
         const size_t eb = type_bytes(info.output_types[j]);
         if(info.output_types[j] == LOOM_B200_F32)
-            group_mean<float><<<blocks, 256, 0, h->stream>>>(
+            group_mean<float><<<blocks, 32 * kMeanWarps, 0, h->stream>>>(
                 static_cast<const float*>(h->d_out[j]), reinterpret_cast<float*>(base + off), rows, M->group,
                 d_os ? d_st : nullptr, d_g, d_os, d_os ? L->num_instances : 0u);
         else
-            group_mean<double><<<blocks, 256, 0, h->stream>>>(
+            group_mean<double><<<blocks, 32 * kMeanWarps, 0, h->stream>>>(
                 static_cast<const double*>(h->d_out[j]), reinterpret_cast<double*>(base + off), rows, M->group,
                 d_os ? d_st : nullptr, d_g, d_os, d_os ? L->num_instances : 0u);
         LB_CUDA(cudaGetLastError());
