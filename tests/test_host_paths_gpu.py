@@ -168,3 +168,52 @@ def test_never_parking_form_holds_no_queue_state():
     assert d["never"][1] == 1 and d["never"][2] == 0
     assert d["parks"][0] - cols > (1 << 18) * 8
     assert np.array_equal(d["never"][3], d["parks"][3])
+
+
+def test_group_mean_tiles_and_fallbacks():
+    """The means' shared-memory tiles (groups of 8, 16 and 32 here) and
+    their fallbacks: a column that does not start on a 16-byte boundary and
+    an f64 column, each against the host mean in order."""
+    import torch
+
+    rng = np.random.default_rng(6)
+    rows = 1000
+    for g, dtype, shift in ((8, np.float32, 0), (16, np.float32, 0), (32, np.float32, 0), (16, np.float32, 1),
+                            (16, np.float64, 0)):
+        x = (rng.standard_normal(rows * g + shift) * 1e3).astype(dtype)
+        d_x = torch.from_numpy(x).cuda()
+        d_y = torch.empty(rows, dtype=torch.from_numpy(x[:1]).dtype, device="cuda")
+        api.group_mean(d_x[shift:], d_y, rows, g)
+        torch.cuda.synchronize()
+        want = _ordered_means(x[shift:], g)
+        assert np.array_equal(d_y.cpu().numpy(), want), (g, dtype, shift)
+
+
+def _ordered_means(x, g):
+    """Means of consecutive groups of g, summed in order in x's type."""
+    s = np.asarray(x).reshape(-1, g)
+    acc = np.zeros(s.shape[0], dtype=s.dtype)
+    for j in range(g):
+        acc = acc + s[:, j]
+    return acc / s.dtype.type(g)
+
+
+def test_launch_host_mean_warps_across_instances():
+    """Instances whose rows do not fill whole warps, with groups from 1 to 64:
+    the warps whose 32 rows straddle two instances read their rows lane by
+    lane, the others through the shared-memory tile; every mean equals the
+    in-order mean of the engine's own per-thread outputs."""
+    rng = np.random.default_rng(8)
+    groups = np.array([4, 16, 1, 64, 8, 2, 32, 4], dtype=np.uint32)
+    rows = np.array([33, 5, 70, 3, 41, 17, 9, 64], dtype=np.int64)
+    starts = np.concatenate([[0], np.cumsum(groups.astype(np.int64) * rows)]).astype(np.uint64)
+    n = int(starts[-1])
+    x = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    with api.Function("canonical_f32", n, "plain") as f:
+        per = f.launch_host([x], n)  # one output: the array itself
+        (got,) = f.launch_host_mean([x], n, instance_group=groups, instance_starts=starts)
+        f.stats(raise_on_device_error=True)
+    want = np.concatenate([_ordered_means(per[int(starts[i]):int(starts[i + 1])], int(groups[i]))
+                           for i in range(len(groups))])
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
