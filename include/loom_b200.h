@@ -159,12 +159,13 @@ typedef struct loom_b200_opts
                               CTA size is halved until the staging area
                               fits in shared memory; runs at the default
                               register cap (max_regs is ignored) */
-    uint32_t spin_iters;  /* regroup, schedule 2, kernels of more than 300
-                             instructions: iterations of a loop on one block
-                             a lane runs within one step (0 = 1024; smaller
-                             kernels always run 1024, compiled in): a few let
-                             the warp re-form sooner, many save the step's
-                             cost */
+    uint32_t spin_iters;  /* regroup, schedule 2: iterations of a loop on one
+                             block a lane runs within one step (0 = 1024);
+                             kernels of at most 300 instructions run 16
+                             (spin_iters 1-16), 64 (17-64) or 1024, counts
+                             compiled into their code: a few let halted
+                             lanes take new threads sooner, many save the
+                             step's cost */
     uint32_t refill_lanes; /* regroup, schedule 2: a warp's burst of steps
                               ends as soon as this many of its lanes have
                               halted, so that the threads that replace them

@@ -60,7 +60,9 @@ SPACE: Dict[str, List] = {
     # schedule 2: lanes a long block waits for (0: off)
     "defer_lanes": [0, 2, 4, 5, 6, 8, 12, 16, 24],
     # schedule 2: self-loop iterations per step (0: 1024)
-    "spin_iters": [0, 8, 32, 128],
+    # (kernels of at most 300 instructions round to their compiled 16, 64
+    # or 1024)
+    "spin_iters": [0, 8, 16, 32, 64, 128],
     # schedule 2: halted lanes that end a burst early (0: off)
     "refill_lanes": [0, 1, 2, 4, 6, 8, 10, 12, 16],
 }

@@ -108,8 +108,9 @@ struct RegroupParams
     unsigned            defer_lanes;
     // Schedule 2, kernels with one call site (K::kSplitCallSites false):
     // iterations of a self-loop a lane runs within one step before the step
-    // ends at the loop's header (0: kSelfLoopSpin; small kernels always run
-    // kSelfLoopSpin, a constant their tight loops are compiled with).
+    // ends at the loop's header (0: kSelfLoopSpin; small kernels run 16, 64
+    // or kSelfLoopSpin, constants their tight loops are compiled with: up to
+    // 16, up to 64, more).
     unsigned            spin_iters;
     // Schedule 2: a burst ends once this many of the warp's lanes have
     // halted (their replacements then start together; 0: full bursts).
@@ -456,7 +457,15 @@ regroup_kernel(const RegroupParams p)
                     {
                         if constexpr(K::kSplitCallSites)
                         {
-                            if(minpc)
+                            // a self-loop's spin count is compiled into each
+                            // call site: spin_iters picks 16, 64 or the
+                            // default (a few iterations let halted lanes take
+                            // new threads while the others keep looping)
+                            if(minpc && p.spin_iters && p.spin_iters <= 16u)
+                                pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, 16u);
+                            else if(minpc && p.spin_iters && p.spin_iters <= 64u)
+                                pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, 64u);
+                            else if(minpc)
                                 pc = K::template run_burst<kProf>(pc, R, ctx, 1u, false, kSelfLoopSpin);
                             else
                                 pc = K::template run_burst<kProf>(pc, R, ctx, p.burst, kPark && cost_on && p.schedule < 2u);
